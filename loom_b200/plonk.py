@@ -1,0 +1,89 @@
+"""Seeded synthetic plonk-like workloads (the prove benchmark's inputs).
+
+Each instance i is one module "plonk_i" of N rows with base columns
+L_i, R_i, O_i (wires a, b, c) and QL_i, QR_i, QM_i, QO_i, QK_i (selectors),
+named as the reference benchmark names them (bench/main.go:86-106,
+integration_test/gnark_plonk/plonk_gnark_utils.go:221-233).  The gate is
+QL.L + QR.R + QM.L.R + QO.O + QK = 0 and a copy constraint covers the three
+wires (arguments.CopyConstraint).
+
+Witness: a and b uniform in [0, p); selectors are seeded 0/1 patterns; c is
+solved so every gate holds (QO = 1 wherever another selector is set).  The
+copy permutation links positions that hold equal values: random cycles of
+length 2..4 over the a/b positions (their values made equal), c positions
+fixed points.  Everything is deterministic in (seed, instance).
+"""
+from __future__ import annotations
+
+from typing import Dict, List, Tuple
+
+import numpy as np
+
+from . import field as F
+from .program import Builder, Compiled, Module, col, copy_constraint
+
+
+def _ith(s: str, i: int) -> str:
+    return f"{s}_{i}"
+
+
+def instance_witness(n: int, seed: int, instance: int) -> Tuple[Dict[str, np.ndarray], np.ndarray]:
+    rng = np.random.Generator(np.random.PCG64([seed, instance]))
+    a = rng.integers(0, F.P, n, dtype=np.uint64)
+    b = rng.integers(0, F.P, n, dtype=np.uint64)
+    ql, qr, qm, qc = (rng.integers(0, 2, n, dtype=np.uint64) for _ in range(4))
+    any_sel = (ql | qr | qm | qc) > 0
+    qo = np.where(any_sel, 1, rng.integers(0, 2, n, dtype=np.uint64)).astype(np.uint64)
+    # copy cycles over a/b positions (0..2n-1), values equalised along each cycle
+    S = np.arange(3 * n, dtype=np.int64)
+    vals = np.concatenate([a, b])
+    perm = rng.permutation(2 * n)
+    pos, covered = 0, int(n)  # link about half of the a/b positions
+    while pos < covered:
+        k = int(rng.integers(2, 5))
+        cyc = perm[pos:pos + k]
+        pos += k
+        if len(cyc) < 2:
+            break
+        vals[cyc] = vals[cyc[0]]
+        for j in range(len(cyc)):
+            S[cyc[j]] = cyc[(j + 1) % len(cyc)]
+    a, b = vals[:n], vals[n:]
+    p = np.uint64(F.P)
+    lin = (ql * a % p + qr * b % p + (qm * (a * b % p)) % p + qc) % p
+    c = np.where(qo == 1, (p - lin) % p, rng.integers(0, F.P, n, dtype=np.uint64))
+    # rows with qo == 0 have no other selector set, so the gate is 0 there
+    cols = {
+        _ith("L", instance): a, _ith("R", instance): b, _ith("O", instance): c,
+        _ith("QL", instance): ql, _ith("QR", instance): qr, _ith("QM", instance): qm,
+        _ith("QO", instance): qo, _ith("QK", instance): qc,
+    }
+    return {k: v.astype(np.uint32) for k, v in cols.items()}, S
+
+
+def build(n_instances: int, n: int, seed: int = 0x10AD) -> Tuple[Compiled, List[np.ndarray]]:
+    """Program and witness (canonical values, descriptor order) of
+    `n_instances` plonk-like modules of `n` rows."""
+    b = Builder()
+    trace: Dict[str, np.ndarray] = {}
+    for i in range(n_instances):
+        m = Module(_ith("plonk", i), n)
+        L, R, O = col(_ith("L", i)), col(_ith("R", i)), col(_ith("O", i))
+        QL, QR, QM, QO, QK = (col(_ith(s, i)) for s in ("QL", "QR", "QM", "QO", "QK"))
+        m.assert_zero(QL * L + QR * R + QM * L * R + QO * O + QK)
+        b.add_module(m)
+        w, S = instance_witness(n, seed, i)
+        trace.update(w)
+        copy_constraint(b, m.name, [L, R, O], S, _ith("plonk.S", i))
+    trace.update(b.generated)
+    compiled = b.compile()
+    witness = [np.ascontiguousarray(trace[name], dtype=np.uint32) for (name, fld, rows) in compiled.witness_columns]
+    return compiled, witness
+
+
+def check_gates(witness_by_name: Dict[str, np.ndarray], i: int) -> bool:
+    g = lambda s: witness_by_name[_ith(s, i)].astype(np.uint64)
+    p = np.uint64(F.P)
+    v = (g("QL") * g("L") % p + g("QR") * g("R") % p + (g("QM") * (g("L") * g("R") % p)) % p
+         + g("QO") * g("O") % p + g("QK")) % p
+    return bool(np.all(v == 0))

@@ -1,0 +1,341 @@
+"""Host-side program builder: the part of loom's board/expr front end that the
+Poseidon2 prove path consumes, compiled to this repository's flat program
+descriptor (documented in include/loom_gpu.h).
+
+It mirrors the reference's construction API so that a program built here is
+the program the Go prover would build:
+  * ``Expr`` / ``col`` / ``coin`` / ``const`` / ``fold``  — expr/ast.go,
+    expr/utils.go:21-33 (Horner fold C0 + v(C1 + v(C2 + ...))).
+  * ``Module.assert_zero`` / ``assert_zero_at`` / ``assert_equal_at`` —
+    board/module.go:183-251 (Lagrange verifier columns "<module>.Lagrange_i").
+  * ``Builder.stage_leaves`` / ``add_grand_product_step`` / ``fresh_name`` —
+    board/rounds.go:108-135, board/board.go:66-69,251-267.
+  * ``copy_constraint`` — arguments/permutation.go:37-127 (ID support and
+    permutation columns generated as in board/module.go:229-293).
+  * ``Builder.compile`` — board/program.go:45-89 and the last-round sweep of
+    board/rounds.go:219-292.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field as dfield
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import field as F
+
+ROUND_FOLD, ROUND_LOG_DERIVATIVE, ROUND_RUNNING_SUMS = 0, 1, 2
+BASE, EXT = 0, 1
+KIND_WITNESS, KIND_STEP, KIND_LAGRANGE = 0, 1, 2
+OP_COL, OP_COIN, OP_CONST, OP_ADD, OP_SUB, OP_MUL = range(6)
+MAGIC = 0x3150474C
+
+
+class Expr:
+    """Immutable expression tree over columns, round coins and constants."""
+
+    __slots__ = ("op", "a", "b")
+
+    def __init__(self, op, a=None, b=None):
+        self.op, self.a, self.b = op, a, b
+
+    def __add__(self, o): return Expr(OP_ADD, self, _lift(o))
+    def __sub__(self, o): return Expr(OP_SUB, self, _lift(o))
+    def __mul__(self, o): return Expr(OP_MUL, self, _lift(o))
+    add = __add__
+    sub = __sub__
+    mul = __mul__
+
+    def leaves(self) -> List["Expr"]:
+        """Leaves in left-to-right order (expr/ast.go:602-639)."""
+        if self.op in (OP_ADD, OP_SUB, OP_MUL):
+            return self.a.leaves() + self.b.leaves()
+        return [self]
+
+    def key(self):
+        if self.op == OP_COL:
+            return ("c", self.a, self.b)
+        if self.op == OP_COIN:
+            return ("k", self.a)
+        if self.op == OP_CONST:
+            return ("v", self.a)
+        return (self.op, self.a.key(), self.b.key())
+
+
+def _lift(o):
+    return o if isinstance(o, Expr) else const(int(o))
+
+
+def col(name: str, shift: int = 0) -> Expr:
+    return Expr(OP_COL, name, int(shift))
+
+
+def coin(r: int) -> Expr:
+    """Round challenge "challenge@loom_r" (board/rounds.go:70-72)."""
+    return Expr(OP_COIN, int(r))
+
+
+def const(v: int) -> Expr:
+    return Expr(OP_CONST, int(v) % F.P)
+
+
+def fold(v: Expr, cs: Sequence[Expr]) -> Expr:
+    if not cs:
+        return const(0)
+    res = cs[-1]
+    for c in reversed(cs[:-1]):
+        res = c + (v * res)
+    return res
+
+
+def lagrange_name(module: str, i: int) -> str:
+    return f"{module}.Lagrange_{i}"
+
+
+@dataclass
+class Module:
+    name: str
+    n: int
+    relations: List[Expr] = dfield(default_factory=list)
+    lagrange: Dict[str, int] = dfield(default_factory=dict)  # verifier column -> row
+
+    def lagrange_col(self, i: int) -> Expr:
+        nm = lagrange_name(self.name, i)
+        self.lagrange[nm] = i
+        return col(nm)
+
+    def assert_zero(self, rel: Expr):
+        self.relations.append(rel)
+
+    def assert_zero_at(self, rel: Expr, *rows: int):
+        disj = self.lagrange_col(rows[0])
+        for r in rows[1:]:
+            disj = disj + self.lagrange_col(r)
+        self.assert_zero(rel * disj)
+
+    def assert_equal_at(self, a: Expr, b: Expr, i: int):
+        self.assert_zero((a - b) * self.lagrange_col(i))
+
+    def id_support_name(self, i: int) -> str:
+        return f"{self.name}.ID_{i}_{self.n}"
+
+
+@dataclass
+class GrandProductStep:
+    round: int
+    module: str
+    num: Expr
+    den: Expr
+    out: str
+
+
+@dataclass
+class Compiled:
+    words: np.ndarray              # descriptor, uint32
+    witness_columns: List[Tuple[str, int, int]]  # (name, field, rows), in descriptor order
+    modules: Dict[str, int]        # name -> N
+    n_rounds: int
+
+
+class Builder:
+    def __init__(self):
+        self.modules: Dict[str, Module] = {}
+        self.rounds: List[dict] = []
+        self.names = 0
+        self.generated: Dict[str, np.ndarray] = {}  # generated base columns (ID support, permutation)
+
+    def add_module(self, m: Module):
+        self.modules[m.name] = m
+
+    def fresh_name(self, prefix: str) -> str:
+        self.names += 1
+        return f"{prefix}{self.names}"
+
+    def _grow(self, r: int):
+        while len(self.rounds) <= r:
+            self.rounds.append({"steps": [], "staged": []})
+
+    def stage_columns(self, r: int, *names: str):
+        self._grow(r)
+        for n in names:
+            if n not in self.rounds[r]["staged"]:
+                self.rounds[r]["staged"].append(n)
+
+    def stage_leaves(self, r: int, *exprs: Expr):
+        for e in exprs:
+            for lf in e.leaves():
+                if lf.op == OP_COL and not self._is_verifier(lf.a):
+                    self.stage_columns(r, lf.a)
+
+    def _is_verifier(self, name: str) -> bool:
+        return any(name in m.lagrange for m in self.modules.values())
+
+    def add_grand_product_step(self, r: int, module: str, num: Expr, den: Expr, out: str):
+        self._grow(r)
+        self.rounds[r]["steps"].append(GrandProductStep(r, module, num, den, out))
+        m = self.modules[module]
+        gp, gps = col(out), col(out, 1)
+        m.assert_zero(gps * den - gp * num)
+        m.assert_zero_at(gp - const(1), 0)
+
+    # ------------------------------------------------------------------ compile
+    def compile(self) -> Compiled:
+        if not self.rounds:
+            self.rounds = [{"steps": [], "staged": []}]
+        n_rounds = len(self.rounds)
+        verifier = {nm: (mname, row) for mname, m in self.modules.items() for nm, row in m.lagrange.items()}
+        owner: Dict[str, str] = {}
+        for mname, m in self.modules.items():
+            for rel in m.relations:
+                for lf in rel.leaves():
+                    if lf.op == OP_COL and lf.a not in verifier:
+                        owner[lf.a] = mname
+        step_out = {s.out: s for rd in self.rounds for s in rd["steps"]}
+        staged: List[List[str]] = []
+        seen = {}
+        for r, rd in enumerate(self.rounds):
+            lst = []
+            for nm in rd["staged"]:
+                if nm in seen:
+                    raise ValueError(f"column {nm} staged twice")
+                if nm not in owner:
+                    raise ValueError(f"column {nm} staged at round {r} is not referenced by any relation")
+                seen[nm] = r
+                lst.append(nm)
+            staged.append(lst)
+        for nm in sorted(owner):  # sweep into the last round, sorted by name
+            if nm not in seen:
+                seen[nm] = n_rounds - 1
+                staged[-1].append(nm)
+
+        # column table: committed columns (witness or step outputs), then the
+        # Lagrange verifier columns
+        def field_of(e: Expr, fields) -> int:
+            if e.op == OP_COL:
+                return fields.get(e.a, BASE)
+            if e.op == OP_COIN:
+                return EXT
+            if e.op == OP_CONST:
+                return BASE
+            return max(field_of(e.a, fields), field_of(e.b, fields))
+
+        fields: Dict[str, int] = {}
+        for s in step_out.values():
+            fields[s.out] = max(field_of(s.num, fields), field_of(s.den, fields))
+        columns: List[Tuple[str, int, int, int, int]] = []  # name, module idx, field, kind, param
+        mod_names = list(self.modules)
+        mod_idx = {n: i for i, n in enumerate(mod_names)}
+        col_idx: Dict[str, int] = {}
+        for nm in sorted(owner):
+            kind = KIND_STEP if nm in step_out else KIND_WITNESS
+            col_idx[nm] = len(columns)
+            columns.append((nm, mod_idx[owner[nm]], fields.get(nm, BASE), kind, 0))
+        for nm, (mname, row) in sorted(verifier.items()):
+            col_idx[nm] = len(columns)
+            columns.append((nm, mod_idx[mname], BASE, KIND_LAGRANGE, row))
+
+        nodes: List[Tuple[int, int, int]] = []
+        memo: Dict[tuple, int] = {}
+
+        def emit(e: Expr) -> int:
+            k = e.key()
+            if k in memo:
+                return memo[k]
+            if e.op == OP_COL:
+                if e.a not in col_idx:
+                    raise ValueError(f"column {e.a} is not part of the program")
+                t = (OP_COL, col_idx[e.a], e.b & 0xFFFFFFFF)
+            elif e.op == OP_COIN:
+                if e.a >= n_rounds:
+                    raise ValueError(f"coin {e.a} beyond the {n_rounds} rounds")
+                t = (OP_COIN, e.a, 0)
+            elif e.op == OP_CONST:
+                t = (OP_CONST, e.a, 0)
+            else:
+                a, b = emit(e.a), emit(e.b)
+                t = (e.op, a, b)
+            nodes.append(t)
+            memo[k] = len(nodes) - 1
+            return memo[k]
+
+        mod_rels = [[emit(r) for r in self.modules[n].relations] for n in mod_names]
+        steps = []
+        for rd in self.rounds:
+            for s in rd["steps"]:
+                steps.append((0, s.round, mod_idx[s.module], emit(s.num), emit(s.den), col_idx[s.out]))
+
+        w: List[int] = [MAGIC, n_rounds, len(mod_names), len(columns), len(nodes), len(steps)]
+
+        def wstr(s: str):
+            b = s.encode()
+            w.append(len(b))
+            b += b"\0" * (-len(b) % 4)
+            w.extend(int.from_bytes(b[i:i + 4], "little") for i in range(0, len(b), 4))
+
+        for i, n in enumerate(mod_names):
+            m = self.modules[n]
+            logn = m.n.bit_length() - 1
+            if m.n != 1 << logn:
+                raise ValueError(f"module {n}: size {m.n} is not a power of two")
+            w.append(logn)
+            wstr(n)
+            w.append(len(mod_rels[i]))
+            w.extend(mod_rels[i])
+        for (nm, mi, fld, kind, param) in columns:
+            wstr(nm)
+            w.extend([mi, fld, kind, param & 0xFFFFFFFF])
+        for t in nodes:
+            w.extend(t)
+        for s in steps:
+            w.extend(s)
+        for lst in staged:
+            w.append(len(lst))
+            w.extend(col_idx[nm] for nm in lst)
+        witness = [(nm, fld, self.modules[mod_names[mi]].n) for (nm, mi, fld, kind, _) in columns if kind == KIND_WITNESS]
+        return Compiled(np.array(w, dtype=np.uint32), witness, {n: self.modules[n].n for n in mod_names}, n_rounds)
+
+
+# ---------------------------------------------------------------------- arguments
+def permutation_within_module(b: Builder, module: str, A: Sequence[Expr], B: Sequence[Expr]):
+    """arguments/permutation.go:37-68."""
+    b.stage_leaves(ROUND_FOLD, *A)
+    b.stage_leaves(ROUND_FOLD, *B)
+    gamma = coin(ROUND_LOG_DERIVATIVE)
+    amul, bmul = A[0] - gamma, B[0] - gamma
+    for x in A[1:]:
+        amul = amul * (x - gamma)
+    for x in B[1:]:
+        bmul = bmul * (x - gamma)
+    gp = b.fresh_name("gp_")
+    b.add_grand_product_step(ROUND_RUNNING_SUMS, module, amul, bmul, gp)
+    b.modules[module].assert_equal_at(const(1), col(gp), 0)
+
+
+def id_support(n_chunks: int, n: int) -> List[np.ndarray]:
+    """ID_k[j] = g^k w^j, g = 3 (board/module.go:262-281); canonical values."""
+    w = F.root_of_unity(n)
+    res = [F.powers(w, n)]
+    for _ in range(1, n_chunks):
+        res.append(((res[-1].astype(np.uint64) * F.MULT_GEN) % F.P).astype(np.uint32))
+    return res
+
+
+def copy_constraint(b: Builder, module: str, A: Sequence[Expr], S: np.ndarray, perm_name: str):
+    """arguments/permutation.go:101-127 with board.PermutationGen: sigma_k[j] is
+    the ID-support value at position S[k*N + j]."""
+    m = b.modules[module]
+    n = m.n
+    if len(S) != n * len(A):
+        raise ValueError("len(S) must equal N * len(A)")
+    sup = id_support(len(A), n)
+    flat = np.concatenate(sup)
+    alpha = coin(ROUND_FOLD)
+    fa, fb = [], []
+    for i, a in enumerate(A):
+        idn = m.id_support_name(i)
+        sgn = f"{perm_name}_{i}"
+        b.generated[idn] = sup[i]
+        b.generated[sgn] = flat[np.asarray(S[i * n:(i + 1) * n], dtype=np.int64)]
+        fa.append(fold(alpha, [a, col(idn)]))
+        fb.append(fold(alpha, [a, col(sgn)]))
+    permutation_within_module(b, module, fa, fb)
