@@ -1,0 +1,120 @@
+/*
+ * loom_gpu.h — C ABI of the B200 (sm_100a) implementation of loom's
+ * Poseidon2-backend prove phase (github.com/consensys/loom).
+ *
+ * The Go prover binds these functions through cgo;
+ * Python binds them through ctypes.  Signatures use plain pointers and
+ * sizes only.  Every function returns an int status (LG_OK = 0) and never
+ * aborts; lg_last_error() describes the last failure on a context.
+ *
+ * Field data: KoalaBear (p = 2^31 - 2^24 + 1) elements are 32-bit
+ * Montgomery words (R = 2^32), the in-memory layout of gnark-crypto's
+ * koalabear.Element, so Go slices are passed as they are.  An E6 element is
+ * 6 such words [B0.A0, B0.A1, B1.A0, B1.A1, B2.A0, B2.A1] (ext.E6).  A
+ * digest is 8 words (hash.Digest).
+ *
+ * Buffers flagged `on_device` are device pointers on the context's GPU;
+ * otherwise host pointers.  Input pointers are only read during the call.
+ *
+ * Program descriptor (lg_prove): little-endian u32 words —
+ *   magic 0x3150474C, n_rounds, n_modules, n_columns, n_nodes, n_steps
+ *   module  : log2(N), str name, n_rel, rel_root[n_rel]
+ *   column  : str name, module, field (0 base | 1 ext),
+ *             kind (0 witness | 1 prover-step output | 2 Lagrange verifier
+ *             column), param (int32 row for kind 2; negative -(i+1) counts
+ *             from the last row)
+ *   node    : op (0 column | 1 round coin | 2 constant | 3 add | 4 sub |
+ *             5 mul), a, b — column: a = column, b = int32 shift; coin:
+ *             a = round; constant: a = canonical value; add/sub/mul: a, b =
+ *             earlier nodes
+ *   step    : type (0 grand product), round, module, numerator node,
+ *             denominator node, output column
+ *   round   : n_staged, staged column indices (board.Compile's order,
+ *             including the sweep of unstaged columns into the last round)
+ *   str     : byte length, then the bytes packed 4 per word
+ * This is the part of a compiled board.Program (board/program.go:21-89)
+ * that the prove phase reads.  Witness columns (kind 0) are passed to
+ * lg_prove in descriptor order, N words each, Lagrange form.
+ *
+ * Proof bytes: the canonical encoding defined by this project — 4-byte
+ * big-endian words, field elements in canonical (non-Montgomery) form, in
+ * the field order of proof.Proof / fri.OpeningProof / fri.Proof; lists are
+ * a count followed by the items (see loom_b200/proof.py for a decoder).
+ */
+#ifndef LOOM_GPU_H
+#define LOOM_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  LG_OK = 0,
+  LG_ERR_INVALID = 1,     /* malformed arguments or program */
+  LG_ERR_CUDA = 2,        /* CUDA runtime failure */
+  LG_ERR_OOM = 3,         /* device allocation failed */
+  LG_ERR_UNSUPPORTED = 4, /* shape or hash backend this build does not handle */
+  LG_ERR_BUFFER = 5       /* output buffer too small; size written back */
+};
+
+typedef struct lg_ctx lg_ctx;
+
+/* Creates a context (one CUDA stream, twiddle caches, memory pool) on
+ * `device`.  Replaces nothing in the reference: the Go prover has no device
+ * state; the cgo shim creates one context per GPU. */
+int lg_ctx_create(int device, lg_ctx** out);
+void lg_ctx_destroy(lg_ctx* ctx);
+/* NUL-terminated description of the last failure on `ctx` (never NULL). */
+const char* lg_last_error(lg_ctx* ctx);
+
+/* Whole prove phase for the Poseidon2 backend: replaces prover.Prove
+ * (prover/prover.go:655-719) called with fri.Poseidon2HashBackend()
+ * (internal/fri/hash_backend.go:21-40) and WithNumFriQueries(num_queries)
+ * (prover/prover.go:74-80), no setup columns, no public inputs.
+ * `hash_backend` must be "poseidon2" (or "" = default); "sha256" and
+ * "blake3" return LG_ERR_UNSUPPORTED.  On LG_ERR_BUFFER the proof is kept
+ * in the context and lg_last_proof() copies it. */
+int lg_prove(lg_ctx* ctx, const char* hash_backend, const uint32_t* program, size_t program_words,
+             const uint32_t* const* witness, int witness_on_device, uint32_t num_queries, uint8_t* proof,
+             size_t* proof_len);
+int lg_last_proof(lg_ctx* ctx, uint8_t* proof, size_t* proof_len);
+
+/* PCS.Commit of one batch (internal/fri/pcs.go:145-168 →
+ * internal/fri/commitment.go:259-386): RS-encode every polynomial at rate 4,
+ * hash adjacent row pairs into leaves with Poseidon2LeafHasher.HashLeafPairs
+ * (internal/fri/hash.go:63-120) and build the mixed-height tree
+ * (internal/merkle/tree.go:117-327).  Group g has rows[g] Lagrange rows,
+ * n_base[g] base columns then n_ext[g] ext columns (6 words per row) in
+ * `cols`, group by group.  Writes the root. */
+int lg_commit_root(lg_ctx* ctx, uint32_t n_groups, const uint64_t* rows, const uint32_t* n_base,
+                   const uint32_t* n_ext, const uint32_t* const* cols, int on_device, uint32_t root[8]);
+
+/* reedsolomon.Encoder.Encode (internal/reedsolomon/rs.go:52-70) on
+ * `n_cols` base columns of n_rows rows stored one after another in `in`;
+ * writes 4 * n_rows bit-reversed evaluations per column to `out`. */
+int lg_rs_encode(lg_ctx* ctx, const uint32_t* in, uint64_t n_rows, uint32_t n_cols, uint32_t* out, int on_device);
+
+/* poseidon2.Permutation (width 24) applied in place to n_states states of
+ * 24 words (the permutation behind internal/hash/poseidon2.go:165-449). */
+int lg_poseidon2_permute(lg_ctx* ctx, uint32_t* states, uint64_t n_states, int on_device);
+
+/* Merkle root over n_leaves digests with level injections
+ * (merkle.NewWithInjections + Build, internal/merkle/tree.go:117-296):
+ * n_inj injections of widths inj_widths[k] (non-increasing), their leaves
+ * concatenated in `inj`. */
+int lg_merkle_root(lg_ctx* ctx, const uint32_t* leaves, uint64_t n_leaves, uint32_t n_inj,
+                   const uint64_t* inj_widths, const uint32_t* inj, int on_device, uint32_t root[8]);
+
+/* One FRI fold of n E6 evaluations in bit-reversed order
+ * (foldLayerExt, internal/fri/fri.go:1177-1198); writes n/2 E6 values. */
+int lg_fri_fold(lg_ctx* ctx, const uint32_t* layer, uint64_t n, const uint32_t alpha[6], uint32_t* out,
+                int on_device);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LOOM_GPU_H */

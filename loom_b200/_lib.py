@@ -1,0 +1,160 @@
+"""ctypes binding of libloom_gpu.so (the C ABI in include/loom_gpu.h).
+
+The shared library is built in-tree (``python -m loom_b200.build``).  There
+is no CPU fallback: when the library or a GPU is missing, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libloom_gpu.so")
+
+LG_OK, LG_ERR_INVALID, LG_ERR_CUDA, LG_ERR_OOM, LG_ERR_UNSUPPORTED, LG_ERR_BUFFER = range(6)
+EXPORTS = ["lg_ctx_create", "lg_ctx_destroy", "lg_last_error", "lg_prove", "lg_last_proof", "lg_commit_root",
+           "lg_rs_encode", "lg_poseidon2_permute", "lg_merkle_root", "lg_fri_fold"]
+
+u32p = ctypes.POINTER(ctypes.c_uint32)
+u64p = ctypes.POINTER(ctypes.c_uint64)
+_lib = None
+_lock = threading.Lock()
+
+
+class LoomError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def load():
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise LoomError(LG_ERR_UNSUPPORTED, f"{LIB_PATH} is not built; run python -m loom_b200.build")
+        L = ctypes.CDLL(LIB_PATH)
+        vp = ctypes.c_void_p
+        L.lg_ctx_create.argtypes = [ctypes.c_int, ctypes.POINTER(vp)]
+        L.lg_ctx_destroy.argtypes = [vp]
+        L.lg_ctx_destroy.restype = None
+        L.lg_last_error.argtypes = [vp]
+        L.lg_last_error.restype = ctypes.c_char_p
+        L.lg_prove.argtypes = [vp, ctypes.c_char_p, u32p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
+                               ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_size_t)]
+        L.lg_last_proof.argtypes = [vp, ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_size_t)]
+        L.lg_commit_root.argtypes = [vp, ctypes.c_uint32, u64p, u32p, u32p, ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, u32p]
+        L.lg_rs_encode.argtypes = [vp, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_int]
+        L.lg_poseidon2_permute.argtypes = [vp, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int]
+        L.lg_merkle_root.argtypes = [vp, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, u64p, ctypes.c_void_p,
+                                     ctypes.c_int, u32p]
+        L.lg_fri_fold.argtypes = [vp, ctypes.c_void_p, ctypes.c_uint64, u32p, ctypes.c_void_p, ctypes.c_int]
+        _lib = L
+        return L
+
+
+def _u32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class Context:
+    """A device context (lg_ctx): one CUDA stream, caches and memory pool."""
+
+    def __init__(self, device: int = 0):
+        self.L = load()
+        self.h = ctypes.c_void_p()
+        rc = self.L.lg_ctx_create(device, ctypes.byref(self.h))
+        if rc != LG_OK:
+            raise LoomError(rc, f"lg_ctx_create failed on device {device}")
+        self._proof_cap = 1 << 22
+        self._proof_buf = (ctypes.c_uint8 * self._proof_cap)()
+
+    def close(self):
+        if self.h:
+            self.L.lg_ctx_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int):
+        if rc != LG_OK:
+            raise LoomError(rc, self.L.lg_last_error(self.h).decode())
+
+    # ------------------------------------------------------------------ prove
+    def prove(self, program_words: np.ndarray, witness: Sequence, num_queries: int, on_device: bool = False,
+              hash_backend: str = "poseidon2") -> bytes:
+        """prover.Prove with the Poseidon2 backend.  `witness`: Montgomery
+        columns in descriptor order — numpy arrays (host) or, with
+        on_device=True, integer device addresses (e.g. torch data_ptr())."""
+        prog = _u32(program_words)
+        if on_device:
+            arr = (ctypes.c_void_p * max(1, len(witness)))(*[int(p) for p in witness])
+        else:
+            cols = [_u32(c) for c in witness]
+            arr = (ctypes.c_void_p * max(1, len(cols)))(*[c.ctypes.data for c in cols])
+        n = ctypes.c_size_t(self._proof_cap)
+        rc = self.L.lg_prove(self.h, hash_backend.encode(), prog.ctypes.data_as(u32p), prog.size, arr, int(on_device),
+                             num_queries, self._proof_buf, ctypes.byref(n))
+        if rc == LG_ERR_BUFFER:
+            self._proof_cap = int(n.value) * 2
+            self._proof_buf = (ctypes.c_uint8 * self._proof_cap)()
+            n = ctypes.c_size_t(self._proof_cap)
+            rc = self.L.lg_last_proof(self.h, self._proof_buf, ctypes.byref(n))
+        self._check(rc)
+        return bytes(memoryview(self._proof_buf)[:n.value])
+
+    # ------------------------------------------------------------------ phase entry points
+    def commit_root(self, groups: List[dict]) -> np.ndarray:
+        rows = np.array([g["rows"] for g in groups], dtype=np.uint64)
+        nb = np.array([len(g.get("base", [])) for g in groups], dtype=np.uint32)
+        ne = np.array([len(g.get("ext", [])) for g in groups], dtype=np.uint32)
+        cols = []
+        for g in groups:
+            cols += [_u32(c) for c in g.get("base", [])] + [_u32(c).reshape(-1) for c in g.get("ext", [])]
+        arr = (ctypes.c_void_p * max(1, len(cols)))(*[c.ctypes.data for c in cols])
+        root = np.zeros(8, dtype=np.uint32)
+        self._check(self.L.lg_commit_root(self.h, len(groups), rows.ctypes.data_as(u64p), nb.ctypes.data_as(u32p),
+                                          ne.ctypes.data_as(u32p), arr, 0, root.ctypes.data_as(u32p)))
+        return root
+
+    def rs_encode(self, cols: np.ndarray) -> np.ndarray:
+        c = _u32(cols)
+        if c.ndim == 1:
+            c = c[None, :]
+        out = np.zeros((c.shape[0], 4 * c.shape[1]), dtype=np.uint32)
+        self._check(self.L.lg_rs_encode(self.h, _ptr(c), c.shape[1], c.shape[0], _ptr(out), 0))
+        return out
+
+    def poseidon2_permute(self, states: np.ndarray) -> np.ndarray:
+        s = _u32(states).reshape(-1, 24).copy()
+        self._check(self.L.lg_poseidon2_permute(self.h, _ptr(s), s.shape[0], 0))
+        return s
+
+    def merkle_root(self, leaves: np.ndarray, injections: Sequence[np.ndarray] = ()) -> np.ndarray:
+        lv = _u32(leaves).reshape(-1, 8)
+        widths = np.array([_u32(x).reshape(-1, 8).shape[0] for x in injections], dtype=np.uint64)
+        inj = np.concatenate([_u32(x).reshape(-1) for x in injections]) if injections else np.zeros(8, dtype=np.uint32)
+        root = np.zeros(8, dtype=np.uint32)
+        self._check(self.L.lg_merkle_root(self.h, _ptr(lv), lv.shape[0], len(injections), widths.ctypes.data_as(u64p),
+                                          _ptr(inj), 0, root.ctypes.data_as(u32p)))
+        return root
+
+    def fri_fold(self, layer: np.ndarray, alpha) -> np.ndarray:
+        x = _u32(layer).reshape(-1, 6)
+        a = _u32(alpha)
+        out = np.zeros((x.shape[0] // 2, 6), dtype=np.uint32)
+        self._check(self.L.lg_fri_fold(self.h, _ptr(x), x.shape[0], a.ctypes.data_as(u32p), _ptr(out), 0))
+        return out

@@ -1,0 +1,257 @@
+// Host-side pieces of the prover: device memory, program descriptor,
+// Fiat-Shamir transcript (internal/fiat-shamir/transcript.go:124-355) and the
+// canonical proof writer.  Errors are C++ exceptions inside the library and
+// become status codes at the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/loom_gpu.h"
+#include "kernels.cuh"
+
+namespace lg {
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define LG_CK(x)                                                                                      \
+  do {                                                                                                \
+    cudaError_t e_ = (x);                                                                             \
+    if (e_ != cudaSuccess)                                                                            \
+      throw ::lg::Error(e_ == cudaErrorMemoryAllocation ? LG_ERR_OOM : LG_ERR_CUDA,     \
+                        std::string(#x) + ": " + cudaGetErrorString(e_));                             \
+  } while (0)
+#define LG_LAUNCH() LG_CK(cudaGetLastError())
+
+// Device buffer of u32 words, stream-ordered allocation.
+struct DBuf {
+  uint32_t* p = nullptr;
+  size_t words = 0;
+  cudaStream_t st = nullptr;
+  DBuf() = default;
+  DBuf(size_t w, cudaStream_t s) : words(w), st(s) {
+    if (w) LG_CK(cudaMallocAsync((void**)&p, w * 4, s));
+  }
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  DBuf(DBuf&& o) noexcept { *this = std::move(o); }
+  DBuf& operator=(DBuf&& o) noexcept {
+    if (this != &o) { release(); p = o.p; words = o.words; st = o.st; o.p = nullptr; o.words = 0; }
+    return *this;
+  }
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFreeAsync(p, st);
+    p = nullptr;
+    words = 0;
+  }
+};
+using DBufP = std::shared_ptr<DBuf>;
+
+struct Ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::map<int, DBufP> tw;       // log n -> w_n^j, j < n
+  std::map<int, DBufP> gpow;     // log n -> g^k, k < n
+  std::map<int, DBufP> ginvpow;  // log n -> g^-k, k < n
+  std::string err;
+  uint32_t* pinned = nullptr;    // host staging
+  size_t pinned_words = 0;
+  int sm_count = 148;
+
+  const uint32_t* twiddles(int logn) {
+    auto it = tw.find(logn);
+    if (it != tw.end()) return it->second->p;
+    size_t n = (size_t)1 << logn;
+    auto b = std::make_shared<DBuf>(n, stream);
+    k_fill_powers<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(b->p, n, root_of_unity_mont(logn), MONT_ONE);
+    LG_LAUNCH();
+    tw[logn] = b;
+    return b->p;
+  }
+  const uint32_t* gpowers(int logn, bool inverse) {
+    auto& m = inverse ? ginvpow : gpow;
+    auto it = m.find(logn);
+    if (it != m.end()) return it->second->p;
+    size_t n = (size_t)1 << logn;
+    auto b = std::make_shared<DBuf>(n, stream);
+    uint32_t g = to_mont(3);
+    if (inverse) g = inv(g);
+    k_fill_powers<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(b->p, n, g, MONT_ONE);
+    LG_LAUNCH();
+    m[logn] = b;
+    return b->p;
+  }
+  uint32_t* host_staging(size_t words) {
+    if (words > pinned_words) {
+      if (pinned) cudaFreeHost(pinned);
+      pinned = nullptr;
+      size_t w = std::max(words, (size_t)1 << 20);
+      LG_CK(cudaMallocHost((void**)&pinned, w * 4));
+      pinned_words = w;
+    }
+    return pinned;
+  }
+  void d2h(uint32_t* host, const uint32_t* dev, size_t words) {
+    LG_CK(cudaMemcpyAsync(host, dev, words * 4, cudaMemcpyDeviceToHost, stream));
+    LG_CK(cudaStreamSynchronize(stream));
+  }
+  void h2d(uint32_t* dev, const void* host, size_t bytes) {
+    LG_CK(cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, stream));
+  }
+};
+
+// ---------------------------------------------------------------- program
+// Flat descriptor; the format is documented in include/loom_gpu.h.
+enum { OP_COL = 0, OP_COIN = 1, OP_CONST = 2, OP_ADD = 3, OP_SUB = 4, OP_MUL = 5 };
+enum { KIND_WITNESS = 0, KIND_STEP = 1, KIND_LAGRANGE = 2 };
+struct Module { uint32_t log_n; std::string name; std::vector<uint32_t> rels; };
+struct Column { std::string name; uint32_t module, field, kind; int32_t param; };
+struct Node { uint32_t op, a, b; };
+struct Step { uint32_t type, round, module, num, den, out; };
+struct Program {
+  uint32_t n_rounds = 0;
+  std::vector<Module> modules;
+  std::vector<Column> columns;
+  std::vector<Node> nodes;
+  std::vector<Step> steps;
+  std::vector<std::vector<uint32_t>> staged;
+};
+
+inline Program parse_program(const uint32_t* w, size_t n) {
+  size_t pos = 0;
+  auto rd = [&]() -> uint32_t {
+    if (pos >= n) throw Error(LG_ERR_INVALID, "program descriptor truncated");
+    return w[pos++];
+  };
+  auto rds = [&]() {
+    uint32_t len = rd();
+    if (len > (n - pos) * 4) throw Error(LG_ERR_INVALID, "program descriptor: bad string length");
+    std::string s(len, '\0');
+    for (uint32_t i = 0; i < len; i += 4) {
+      uint32_t x = rd();
+      for (uint32_t j = 0; j < 4 && i + j < len; j++) s[i + j] = (char)((x >> (8 * j)) & 0xff);
+    }
+    return s;
+  };
+  Program p;
+  if (rd() != 0x3150474Cu) throw Error(LG_ERR_INVALID, "program descriptor: bad magic");
+  p.n_rounds = rd();
+  uint32_t nm = rd(), nc = rd(), nn = rd(), ns = rd();
+  if (p.n_rounds == 0) throw Error(LG_ERR_INVALID, "program descriptor: no rounds");
+  for (uint32_t i = 0; i < nm; i++) {
+    Module m;
+    m.log_n = rd();
+    if (m.log_n < 1 || m.log_n > 22) throw Error(LG_ERR_INVALID, "module size out of range (2 .. 2^22 rows)");
+    m.name = rds();
+    uint32_t nr = rd();
+    for (uint32_t k = 0; k < nr; k++) m.rels.push_back(rd());
+    p.modules.push_back(m);
+  }
+  for (uint32_t i = 0; i < nc; i++) {
+    Column c;
+    c.name = rds();
+    c.module = rd(); c.field = rd(); c.kind = rd(); c.param = (int32_t)rd();
+    if (c.module >= nm || c.field > 1 || c.kind > 2) throw Error(LG_ERR_INVALID, "bad column " + c.name);
+    p.columns.push_back(c);
+  }
+  for (uint32_t i = 0; i < nn; i++) {
+    Node x{rd(), rd(), rd()};
+    if (x.op > OP_MUL) throw Error(LG_ERR_INVALID, "bad node op");
+    if (x.op >= OP_ADD && (x.a >= i || x.b >= i)) throw Error(LG_ERR_INVALID, "node children must precede parents");
+    if (x.op == OP_COL && x.a >= nc) throw Error(LG_ERR_INVALID, "node column out of range");
+    if (x.op == OP_COIN && x.a >= p.n_rounds) throw Error(LG_ERR_INVALID, "node coin out of range");
+    p.nodes.push_back(x);
+  }
+  for (uint32_t i = 0; i < ns; i++) {
+    Step s{rd(), rd(), rd(), rd(), rd(), rd()};
+    if (s.type != 0 || s.round >= p.n_rounds || s.module >= nm || s.num >= nn || s.den >= nn || s.out >= nc)
+      throw Error(LG_ERR_INVALID, "bad step");
+    p.steps.push_back(s);
+  }
+  for (uint32_t r = 0; r < p.n_rounds; r++) {
+    uint32_t k = rd();
+    std::vector<uint32_t> v;
+    for (uint32_t i = 0; i < k; i++) {
+      uint32_t c = rd();
+      if (c >= nc) throw Error(LG_ERR_INVALID, "staged column out of range");
+      v.push_back(c);
+    }
+    p.staged.push_back(v);
+  }
+  for (auto& m : p.modules)
+    for (uint32_t r : m.rels)
+      if (r >= nn) throw Error(LG_ERR_INVALID, "relation root out of range");
+  return p;
+}
+
+// ---------------------------------------------------------------- transcript
+inline std::vector<uint32_t> string_to_elements(uint32_t tag, const std::string& s) {
+  std::vector<uint32_t> r = {to_mont(tag), to_mont((uint32_t)s.size())};
+  for (size_t i = 0; i < s.size(); i += 3) {
+    uint32_t limb = 0;
+    for (size_t j = 0; j < 3 && i + j < s.size(); j++) limb |= (uint32_t)(uint8_t)s[i + j] << (8 * j);
+    r.push_back(to_mont(limb));
+  }
+  return r;
+}
+
+struct Digest { uint32_t v[8]; };
+
+struct Transcript {
+  struct Ch { std::string name; std::vector<uint32_t> bindings; Digest value; bool done = false; };
+  std::vector<Ch> chs;
+  std::map<std::string, size_t> index;
+  void add(const std::string& n) {
+    if (index.count(n)) throw Error(LG_ERR_INVALID, "duplicate challenge " + n);
+    index[n] = chs.size();
+    Ch c; c.name = n; chs.push_back(c);
+  }
+  void bind(const std::string& n, const uint32_t* v, size_t len) {
+    auto it = index.find(n);
+    if (it == index.end()) throw Error(LG_ERR_INVALID, "unknown challenge " + n);
+    if (chs[it->second].done) throw Error(LG_ERR_INVALID, "challenge already computed " + n);
+    chs[it->second].bindings.insert(chs[it->second].bindings.end(), v, v + len);
+  }
+  Digest compute(const std::string& n) {
+    auto it = index.find(n);
+    if (it == index.end()) throw Error(LG_ERR_INVALID, "unknown challenge " + n);
+    size_t i = it->second;
+    if (chs[i].done) return chs[i].value;
+    HostSponge h;
+    for (uint32_t x : string_to_elements(0x46534944u, n)) h.write(x);
+    if (i) {
+      if (!chs[i - 1].done) throw Error(LG_ERR_INVALID, "previous challenge not computed for " + n);
+      for (int k = 0; k < 8; k++) h.write(chs[i - 1].value.v[k]);
+    }
+    for (uint32_t x : chs[i].bindings) h.write(x);
+    h.sum(chs[i].value.v);
+    chs[i].done = true;
+    return chs[i].value;
+  }
+};
+inline E6 digest_e6(const Digest& d) { E6 r; for (int i = 0; i < 6; i++) r.c[i] = d.v[i]; return r; }
+
+// ---------------------------------------------------------------- proof writer
+// Canonical encoding: 4-byte big-endian words, field elements canonical.
+struct Writer {
+  std::vector<uint8_t> b;
+  void u32(uint32_t x) { for (int i = 3; i >= 0; i--) b.push_back((uint8_t)(x >> (8 * i))); }
+  void el(uint32_t m) { u32(from_mont(m)); }
+  void e6(const E6& x) { for (int i = 0; i < 6; i++) el(x.c[i]); }
+  void e6w(const uint32_t* w) { for (int i = 0; i < 6; i++) el(w[i]); }
+  void dg(const Digest& d) { for (int i = 0; i < 8; i++) el(d.v[i]); }
+  void dgw(const uint32_t* w) { for (int i = 0; i < 8; i++) el(w[i]); }
+  void str(const std::string& s) { u32((uint32_t)s.size()); b.insert(b.end(), s.begin(), s.end()); }
+};
+
+}  // namespace lg

@@ -1,0 +1,545 @@
+// sm_100a kernels of the Poseidon2 prove path.  All field data is Montgomery
+// words; an E6 column is stored as 6 base "lanes" (structure of arrays), so
+// every transform and gather works on plain u32 columns.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "field.cuh"
+#include "poseidon2.cuh"
+
+namespace lg {
+
+constexpr int RATE_LOG = 2;  // blowup 4 (internal/constants/const.go:24)
+constexpr int SMEM_NTT_MAX_LOG = 14;
+constexpr uint32_t LEAF_TAG = 0x4c454146u, NODE_TAG = 0x4e4f4445u;
+
+// ---------------------------------------------------------------- twiddles
+// tw[j] = w_n^j for j < n, w_n = root_of_unity(log n).
+__global__ void k_fill_powers(uint32_t* out, uint64_t n, uint32_t base, uint32_t start) {
+  uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (j < n) out[j] = mul(start, mont_pow(base, j));
+}
+
+// ---------------------------------------------------------------- smem NTT
+// Radix-2 stages over a block-resident array A of n = 2^logn words.
+// tw: table of w_n^j (j < n) for this n; `inverse` uses w_n^-j = w_n^(n-j).
+__device__ __forceinline__ uint32_t tw_at(const uint32_t* tw, uint32_t idx, uint32_t mask, bool inverse) {
+  return inverse ? __ldg(tw + ((0u - idx) & mask)) : __ldg(tw + idx);
+}
+
+// DIT: bit-reversed input, natural output.
+__device__ void smem_dit(uint32_t* A, int logn, const uint32_t* tw, bool inverse) {
+  const uint32_t n = 1u << logn, mask = n - 1;
+  for (int s = 1; s <= logn; s++) {
+    const uint32_t half = 1u << (s - 1);
+    for (uint32_t t = threadIdx.x; t < n / 2; t += blockDim.x) {
+      uint32_t j = t & (half - 1);
+      uint32_t i0 = ((t >> (s - 1)) << s) | j, i1 = i0 + half;
+      uint32_t w = tw_at(tw, j << (logn - s), mask, inverse);
+      uint32_t u = A[i0], v = mul(A[i1], w);
+      A[i0] = add(u, v);
+      A[i1] = sub(u, v);
+    }
+    __syncthreads();
+  }
+}
+
+// DIF: natural input, bit-reversed output.
+__device__ void smem_dif(uint32_t* A, int logn, const uint32_t* tw, bool inverse) {
+  const uint32_t n = 1u << logn, mask = n - 1;
+  for (int s = logn; s >= 1; s--) {
+    const uint32_t half = 1u << (s - 1);
+    for (uint32_t t = threadIdx.x; t < n / 2; t += blockDim.x) {
+      uint32_t j = t & (half - 1);
+      uint32_t i0 = ((t >> (s - 1)) << s) | j, i1 = i0 + half;
+      uint32_t w = tw_at(tw, j << (logn - s), mask, inverse);
+      uint32_t u = A[i0], v = A[i1];
+      A[i0] = add(u, v);
+      A[i1] = mul(sub(u, v), w);
+    }
+    __syncthreads();
+  }
+}
+
+// Inverse transform of natural-order values to natural-order coefficients
+// (scaled by 1/n), in place per lane.
+__global__ void k_intt_inplace(uint32_t* data, uint64_t lane_stride, int logn, const uint32_t* tw_n, uint32_t n_inv) {
+  extern __shared__ uint32_t sm[];
+  const uint32_t n = 1u << logn;
+  uint32_t* d = data + blockIdx.x * lane_stride;
+  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) sm[bitrev32(k, logn)] = d[k];
+  __syncthreads();
+  smem_dit(sm, logn, tw_n, true);
+  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) d[k] = mul(sm[k], n_inv);
+}
+
+// ---------------------------------------------------------------- leaves
+// leaf k = Sponge(LEAF, 2nB, 2nE, lo.base, hi.base, lo.ext, hi.ext) over
+// rows 2k, 2k+1 (internal/fri/hash.go:39-57).  Base lanes at base + c*stride,
+// ext column e lane l at ext + (6e + l)*stride.
+struct LeafGroup {
+  const uint32_t* base;
+  const uint32_t* ext;
+  uint64_t stride;      // words between lanes
+  uint32_t nb, ne;
+  uint32_t n_leaves;    // rows / 2
+  uint32_t* out;        // n_leaves digests of 8 words
+};
+
+__device__ __forceinline__ uint32_t leaf_elem(const LeafGroup& g, uint32_t idx, uint32_t k, uint32_t hdr0,
+                                              uint32_t hdr1, uint32_t hdr2) {
+  if (idx == 0) return hdr0;
+  if (idx == 1) return hdr1;
+  if (idx == 2) return hdr2;
+  idx -= 3;
+  if (idx < 2 * g.nb) {
+    uint32_t h = idx >= g.nb;
+    uint32_t c = idx - h * g.nb;
+    return g.base[c * g.stride + 2 * k + h];
+  }
+  idx -= 2 * g.nb;
+  uint32_t h = idx >= 6 * g.ne;
+  uint32_t e = idx - h * 6 * g.ne;
+  return g.ext[e * g.stride + 2 * k + h];
+}
+
+__global__ void k_hash_leaves(LeafGroup g) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= g.n_leaves) return;
+  const uint32_t total = 3 + 2 * g.nb + 12 * g.ne;
+  const uint32_t h0 = to_mont(LEAF_TAG), h1 = to_mont(2 * g.nb), h2 = to_mont(2 * g.ne);
+  uint32_t s[24];
+#pragma unroll
+  for (int i = 0; i < 24; i++) s[i] = 0;
+  for (uint32_t b = 0; b < total; b += 16) {
+#pragma unroll
+    for (uint32_t i = 0; i < 16; i++)
+      if (b + i < total) s[i] = leaf_elem(g, b + i, k, h0, h1, h2);
+    p2_permute(s);
+  }
+  uint32_t* o = g.out + (uint64_t)k * 8;
+#pragma unroll
+  for (int i = 0; i < 8; i++) o[i] = s[i];
+}
+
+// ---------------------------------------------------------------- Merkle
+// nodes: 1-indexed, 8 words per node.  Level step: node i = H(2i, 2i+1) for
+// i in [start, 2 start); injection fold: node start+j = H(node, inj[j]),
+// several injections of the same width chained in schedule order
+// (internal/merkle/tree.go:210-327).
+__global__ void k_merkle_level(uint32_t* nodes, uint32_t start) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= start) return;
+  uint64_t id = start + i;
+  uint32_t l[8], r[8], o[8];
+#pragma unroll
+  for (int q = 0; q < 8; q++) { l[q] = nodes[2 * id * 8 + q]; r[q] = nodes[(2 * id + 1) * 8 + q]; }
+  p2_compress(to_mont(NODE_TAG), l, r, o);
+#pragma unroll
+  for (int q = 0; q < 8; q++) nodes[id * 8 + q] = o[q];
+}
+
+__global__ void k_merkle_inject(uint32_t* nodes, uint32_t start, const uint32_t* const* inj, uint32_t n_inj) {
+  uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= start) return;
+  uint64_t id = start + j;
+  uint32_t cur[8], r[8];
+#pragma unroll
+  for (int q = 0; q < 8; q++) cur[q] = nodes[id * 8 + q];
+  const uint32_t tag = to_mont(NODE_TAG);
+  for (uint32_t t = 0; t < n_inj; t++) {
+    const uint32_t* leaf = inj[t] + (uint64_t)j * 8;
+#pragma unroll
+    for (int q = 0; q < 8; q++) r[q] = leaf[q];
+    p2_compress(tag, cur, r, cur);
+  }
+#pragma unroll
+  for (int q = 0; q < 8; q++) nodes[id * 8 + q] = cur[q];
+}
+
+// Permutation test hook: one state of 24 words per thread.
+__global__ void k_p2_permute(uint32_t* states, uint64_t n) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t s[24];
+#pragma unroll
+  for (int q = 0; q < 24; q++) s[q] = states[i * 24 + q];
+  p2_permute(s);
+#pragma unroll
+  for (int q = 0; q < 24; q++) states[i * 24 + q] = s[q];
+}
+
+// ---------------------------------------------------------------- expressions
+// Register bytecode for the constraint DAG (compiled on the host from the
+// program's folded relation): typed ops over a per-thread register file of
+// E6 slots held in shared memory.
+enum : uint8_t {
+  X_LOAD_B = 0,  // r[d] = col lane imm at row (j + shift) mod n (base)
+  X_LOAD_E,      // r[d] = 6 lanes starting at lane imm (ext)
+  X_COIN,        // r[d] = coins[imm]
+  X_CONST,       // r[d] = imm (base, Montgomery)
+  X_ADD_BB, X_ADD_EB, X_ADD_EE,
+  X_SUB_BB, X_SUB_BE, X_SUB_EB, X_SUB_EE,
+  X_MUL_BB, X_MUL_EB, X_MUL_EE,
+};
+struct XInst { uint8_t op, d, a, b; uint32_t imm; int32_t shift; };
+constexpr int X_MAX_REGS = 24;
+constexpr int X_MAX_INST = 512;
+
+struct XProgram {
+  const XInst* code;
+  uint32_t n_inst;
+  uint32_t n_regs;
+  uint32_t result;      // register holding the value
+  uint32_t result_ext;  // 1 when the result is an E6
+};
+
+// Evaluates one row.  lane(l, row) returns column lane l at `row`.
+template <class LaneFn>
+__device__ __forceinline__ E6 x_eval(const XProgram& p, const E6* coins, uint32_t* regs, uint32_t stride, uint32_t j,
+                                     uint32_t n, LaneFn lane) {
+  // regs: register r word w at regs[(r * 6 + w) * stride]
+  auto R = [&](uint32_t r, int w) -> uint32_t& { return regs[(r * 6 + w) * stride]; };
+  for (uint32_t pc = 0; pc < p.n_inst; pc++) {
+    XInst in = p.code[pc];
+    switch (in.op) {
+      case X_LOAD_B: {
+        uint32_t row = (uint32_t)(((int64_t)j + in.shift) & (int64_t)(n - 1));
+        R(in.d, 0) = lane(in.imm, row);
+        break;
+      }
+      case X_LOAD_E: {
+        uint32_t row = (uint32_t)(((int64_t)j + in.shift) & (int64_t)(n - 1));
+        for (int w = 0; w < 6; w++) R(in.d, w) = lane(in.imm + w, row);
+        break;
+      }
+      case X_COIN:
+        for (int w = 0; w < 6; w++) R(in.d, w) = coins[in.imm].c[w];
+        break;
+      case X_CONST: R(in.d, 0) = in.imm; break;
+      case X_ADD_BB: R(in.d, 0) = add(R(in.a, 0), R(in.b, 0)); break;
+      case X_ADD_EB: {  // a ext, b base
+        uint32_t b0 = R(in.b, 0);
+        for (int w = 1; w < 6; w++) R(in.d, w) = R(in.a, w);
+        R(in.d, 0) = add(R(in.a, 0), b0);
+        break;
+      }
+      case X_ADD_EE: for (int w = 0; w < 6; w++) R(in.d, w) = add(R(in.a, w), R(in.b, w)); break;
+      case X_SUB_BB: R(in.d, 0) = sub(R(in.a, 0), R(in.b, 0)); break;
+      case X_SUB_BE: {  // a base, b ext
+        uint32_t a0 = R(in.a, 0);
+        for (int w = 1; w < 6; w++) R(in.d, w) = neg(R(in.b, w));
+        R(in.d, 0) = sub(a0, R(in.b, 0));
+        break;
+      }
+      case X_SUB_EB: {
+        uint32_t b0 = R(in.b, 0);
+        for (int w = 1; w < 6; w++) R(in.d, w) = R(in.a, w);
+        R(in.d, 0) = sub(R(in.a, 0), b0);
+        break;
+      }
+      case X_SUB_EE: for (int w = 0; w < 6; w++) R(in.d, w) = sub(R(in.a, w), R(in.b, w)); break;
+      case X_MUL_BB: R(in.d, 0) = mul(R(in.a, 0), R(in.b, 0)); break;
+      case X_MUL_EB: {
+        uint32_t b0 = R(in.b, 0);
+        for (int w = 0; w < 6; w++) R(in.d, w) = mul(R(in.a, w), b0);
+        break;
+      }
+      case X_MUL_EE: {
+        E6 x, y;
+        for (int w = 0; w < 6; w++) { x.c[w] = R(in.a, w); y.c[w] = R(in.b, w); }
+        E6 z = e6_mul(x, y);
+        for (int w = 0; w < 6; w++) R(in.d, w) = z.c[w];
+        break;
+      }
+    }
+  }
+  E6 r;
+  if (p.result_ext) { for (int w = 0; w < 6; w++) r.c[w] = R(p.result, w); }
+  else r = e6_base(R(p.result, 0));
+  return r;
+}
+
+// Quotient numerator on coset c, row j: V(...) / (s_c^n - 1), written as 6
+// lanes qv[w][c n + j] (lane stride 4n).  cv: coset values, lane l coset c at
+// cv[l * 4n + c n + j].
+__global__ void k_quotient_eval(XProgram p, const E6* coins, const uint32_t* cv, int logn, const uint32_t* zinv,
+                                uint32_t* qv) {
+  extern __shared__ uint32_t regs[];
+  const uint32_t n = 1u << logn;
+  const uint32_t c = blockIdx.y;
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const uint64_t big = (uint64_t)n << RATE_LOG;
+  auto lane = [&](uint32_t l, uint32_t row) -> uint32_t { return cv[l * big + (uint64_t)c * n + row]; };
+  E6 v = x_eval(p, coins, regs + threadIdx.x, blockDim.x, j, n, lane);
+  v = e6_mul_base(v, zinv[c]);
+  for (int w = 0; w < 6; w++) qv[w * big + (uint64_t)c * n + j] = v.c[w];
+}
+
+// Quotient chunk coefficients from the inverse-transformed coset values.
+// After k_intt_inplace, r[w][c n + k] holds [Y^k] R_c(Y) where
+// R_c(Y) = sum_d s_c^(dn) q_d(s_c Y).  With t_c = r_c[k] s_c^-k,
+// u_d = g^(dn) q_(d,k) = 1/4 sum_c t_c w_4^(-cd).
+// out: chunk d, lane w at out[(d * 6 + w) * n + k].
+__global__ void k_quotient_chunks(const uint32_t* r, int logn, const uint32_t* ginv_pow, const uint32_t* tw_4n,
+                                  uint32_t* out, uint32_t quarter, uint32_t gn_inv, int lanes) {
+  const uint32_t n = 1u << logn;
+  const uint64_t big = (uint64_t)n << RATE_LOG;
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t w = blockIdx.y;
+  if (k >= n || (int)w >= lanes) return;
+  uint32_t t[4];
+  const uint32_t gk = ginv_pow[k];
+  for (int c = 0; c < 4; c++) {
+    // s_c^-k = g^-k w_4n^-(c k)
+    uint32_t e = (uint32_t)((big - ((uint64_t)c * k) % big) % big);
+    t[c] = mul(mul(r[w * big + (uint64_t)c * n + k], gk), __ldg(tw_4n + e));
+  }
+  // inverse 4-point DFT: u_d = 1/4 sum_c t_c w4^(-c d); w4^-1 = tw_4n[3n]
+  const uint32_t w4i = __ldg(tw_4n + 3 * n), w4i2 = mul(w4i, w4i), w4i3 = mul(w4i2, w4i);
+  uint32_t u[4];
+  u[0] = add(add(t[0], t[1]), add(t[2], t[3]));
+  u[1] = add(add(t[0], mul(t[1], w4i)), add(mul(t[2], w4i2), mul(t[3], w4i3)));
+  u[2] = add(add(t[0], mul(t[1], w4i2)), add(t[2], mul(t[3], w4i2)));
+  u[3] = add(add(t[0], mul(t[1], w4i3)), add(mul(t[2], w4i2), mul(t[3], w4i)));
+  uint32_t scale = quarter;  // 1/4, then times g^-(d n) per chunk
+  for (int d = 0; d < 4; d++) {
+    out[((uint64_t)d * lanes + w) * n + k] = mul(u[d], scale);
+    scale = mul(scale, gn_inv);
+  }
+}
+
+// ---------------------------------------------------------------- grand product
+// ratio[j] = num(j) / den(j) on Lagrange rows (internal/poly/iop_utils.go:170-192).
+struct LaneTable { const uint32_t* const* lanes; };
+__global__ void k_gp_ratio(XProgram pn, XProgram pd, const E6* coins, LaneTable t, int logn, uint32_t* ratio) {
+  extern __shared__ uint32_t regs[];
+  const uint32_t n = 1u << logn;
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  auto lane = [&](uint32_t l, uint32_t row) -> uint32_t { return t.lanes[l][row]; };
+  E6 a = x_eval(pn, coins, regs + threadIdx.x, blockDim.x, j, n, lane);
+  E6 b = x_eval(pd, coins, regs + threadIdx.x, blockDim.x, j, n, lane);
+  E6 q = e6_mul(a, e6_inv(b));
+  for (int w = 0; w < 6; w++) ratio[(uint64_t)w * n + j] = q.c[w];
+}
+
+constexpr int SCAN_BLOCK = 256, SCAN_PER_THREAD = 8, SCAN_TILE = SCAN_BLOCK * SCAN_PER_THREAD;
+
+__device__ __forceinline__ E6 ld6(const uint32_t* p, uint64_t stride, uint64_t i) {
+  E6 r;
+  for (int w = 0; w < 6; w++) r.c[w] = p[w * stride + i];
+  return r;
+}
+__device__ __forceinline__ void st6(uint32_t* p, uint64_t stride, uint64_t i, const E6& v) {
+  for (int w = 0; w < 6; w++) p[w * stride + i] = v.c[w];
+}
+
+// Per-tile inclusive product scan of ratio (in place); tile totals out.
+__global__ void k_scan_tiles(uint32_t* x, uint64_t n, uint32_t* totals) {
+  __shared__ E6 part[SCAN_BLOCK];
+  const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_PER_THREAD;
+  E6 acc = e6_one();
+  E6 v[SCAN_PER_THREAD];
+  for (int i = 0; i < SCAN_PER_THREAD; i++) {
+    uint64_t idx = base + i;
+    v[i] = idx < n ? ld6(x, n, idx) : e6_one();
+    acc = e6_mul(acc, v[i]);
+    v[i] = acc;
+  }
+  part[threadIdx.x] = acc;
+  __syncthreads();
+  // exclusive product of the thread partials (Hillis-Steele on smem)
+  for (int off = 1; off < SCAN_BLOCK; off <<= 1) {
+    E6 t = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : e6_one();
+    __syncthreads();
+    if (threadIdx.x >= (unsigned)off) part[threadIdx.x] = e6_mul(part[threadIdx.x], t);
+    __syncthreads();
+  }
+  E6 pre = threadIdx.x ? part[threadIdx.x - 1] : e6_one();
+  for (int i = 0; i < SCAN_PER_THREAD; i++) {
+    uint64_t idx = base + i;
+    if (idx < n) st6(x, n, idx, e6_mul(pre, v[i]));
+  }
+  if (threadIdx.x == SCAN_BLOCK - 1) {
+    uint32_t nt = gridDim.x;
+    for (int w = 0; w < 6; w++) totals[w * nt + blockIdx.x] = part[SCAN_BLOCK - 1].c[w];
+  }
+}
+
+// Exclusive prefix products of the tile totals (totals[w * nt + t]) into
+// pre[t * 6 + w]; nt is small (n / 2048), one thread walks it.
+__global__ void k_tile_prefix(const uint32_t* totals, uint32_t nt, uint32_t* pre) {
+  E6 acc = e6_one();
+  for (uint32_t t = 0; t < nt; t++) {
+    for (int w = 0; w < 6; w++) pre[t * 6 + w] = acc.c[w];
+    E6 v;
+    for (int w = 0; w < 6; w++) v.c[w] = totals[w * nt + t];
+    acc = e6_mul(acc, v);
+  }
+}
+
+// Grand product from the tile-local inclusive scan s: out[0] = 1,
+// out[i] = s[i-1] times the product of the earlier tiles' totals.
+__global__ void k_gp_finish(const uint32_t* s, uint64_t n, const uint32_t* tile_pre, uint32_t* out) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  E6 v;
+  if (i == 0) v = e6_one();
+  else {
+    uint64_t k = i - 1;
+    uint64_t tile = k / SCAN_TILE;
+    E6 pre;
+    for (int w = 0; w < 6; w++) pre.c[w] = tile_pre[tile * 6 + w];
+    v = e6_mul(pre, ld6(s, n, k));
+  }
+  st6(out, n, i, v);
+}
+
+// ---------------------------------------------------------------- claimed values
+// zp[k] = z^k, k < n.
+__global__ void k_e6_powers(E6 z, uint32_t n, uint32_t* zp) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  E6 v = e6_pow(z, k);
+  st6(zp, n, k, v);
+}
+
+// One block per (lane, point): out = sum_k coef[k] z^k (E6).
+struct DotJob { const uint32_t* coef; const uint32_t* zp; uint32_t n; uint32_t out_idx; };
+__global__ void k_dot(const DotJob* jobs, uint32_t* out) {
+  __shared__ E6 part[256];
+  DotJob jb = jobs[blockIdx.x];
+  E6 acc = e6_zero();
+  for (uint32_t k = threadIdx.x; k < jb.n; k += blockDim.x) {
+    uint32_t c = jb.coef[k];
+    for (int w = 0; w < 6; w++) acc.c[w] = add(acc.c[w], mul(jb.zp[(uint64_t)w * jb.n + k], c));
+  }
+  part[threadIdx.x] = acc;
+  __syncthreads();
+  for (int off = blockDim.x / 2; off > 0; off >>= 1) {
+    if (threadIdx.x < (unsigned)off) part[threadIdx.x] = e6_add(part[threadIdx.x], part[threadIdx.x + off]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int w = 0; w < 6; w++) out[jb.out_idx * 6 + w] = part[0].c[w];
+}
+
+// ---------------------------------------------------------------- DEEP
+// DQ(x) = sum_s (A_s - sum_{b in s} alpha^i_b P_b(x)) / (z_s - x) on the LDE
+// rows r of one class, x = w_4n^bitrev(r) (internal/fri/deep.go:205-266,
+// evaluated on the 4n LDE rows instead of the n trace rows and re-encoded:
+// DQ has degree < n, so both give the same codeword).
+constexpr int DEEP_MAX_POINTS = 4;
+struct DeepBundle { const uint32_t* lane0; uint64_t lane_stride; uint32_t ext; uint32_t mask; E6 scale; };
+struct DeepJob {
+  const DeepBundle* bundles;
+  uint32_t n_bundles;
+  uint32_t n_points;
+  E6 z[DEEP_MAX_POINTS];
+  E6 a[DEEP_MAX_POINTS];
+  int logn4;            // log2 of the LDE size
+  const uint32_t* tw;   // w_4n^j table
+  uint32_t* out;        // 6 lanes, lane stride 4n
+};
+__global__ void k_deep(DeepJob jb) {
+  const uint32_t big = 1u << jb.logn4;
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= big) return;
+  E6 acc[DEEP_MAX_POINTS];
+  for (uint32_t s = 0; s < jb.n_points; s++) acc[s] = jb.a[s];
+  for (uint32_t b = 0; b < jb.n_bundles; b++) {
+    DeepBundle bu = jb.bundles[b];
+    E6 v;
+    if (bu.ext) {
+      E6 px;
+      for (int w = 0; w < 6; w++) px.c[w] = bu.lane0[w * bu.lane_stride + r];
+      v = e6_mul(bu.scale, px);
+    } else {
+      v = e6_mul_base(bu.scale, bu.lane0[r]);
+    }
+    for (uint32_t s = 0; s < jb.n_points; s++)
+      if (bu.mask >> s & 1) acc[s] = e6_sub(acc[s], v);
+  }
+  uint32_t x = __ldg(jb.tw + bitrev32(r, jb.logn4));
+  E6 dq = e6_zero();
+  for (uint32_t s = 0; s < jb.n_points; s++) {
+    E6 d = jb.z[s];
+    d.c[0] = sub(d.c[0], x);
+    dq = e6_add(dq, e6_mul(acc[s], e6_inv(d)));
+  }
+  for (int w = 0; w < 6; w++) jb.out[(uint64_t)w * big + r] = dq.c[w];
+}
+
+// ---------------------------------------------------------------- FRI
+// running += gamma * level (6 lanes each, lane stride n)
+__global__ void k_axpy_e6(uint32_t* run, const uint32_t* lvl, uint64_t n, E6 gamma) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  E6 a = ld6(run, n, i), b = ld6(lvl, n, i);
+  st6(run, n, i, e6_add(a, e6_mul(b, gamma)));
+}
+
+// next[i] = (p+q)/2 + alpha (p-q)/(2 x_i), x_i^-1 = w_n^-bitrev(i, n/2)
+// (internal/fri/fri.go:1113-1118,1177-1198).  tw: w_n^j table.
+__global__ void k_fold(const uint32_t* layer, uint64_t n, E6 alpha, const uint32_t* tw, uint32_t inv2, uint32_t* next) {
+  const uint64_t half = n / 2;
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= half) return;
+  int lg = 0;
+  while ((1ull << lg) < half) lg++;
+  uint32_t e = bitrev32((uint32_t)i, lg);
+  uint32_t xinv = __ldg(tw + ((n - e) & (n - 1)));
+  E6 p = ld6(layer, n, 2 * i), q = ld6(layer, n, 2 * i + 1);
+  E6 s = e6_mul_base(e6_add(p, q), inv2);
+  E6 d = e6_mul(e6_mul_base(e6_mul_base(e6_sub(p, q), inv2), xinv), alpha);
+  st6(next, half, i, e6_add(s, d));
+}
+
+// ---------------------------------------------------------------- openings
+// Row pairs: for every query q and source, the rows (lo, lo+1) of each lane,
+// lo = (s_q >> shift) & ~1, written at out[q * per_q + off + 2 lane + h].
+struct RowSrc { const uint32_t* lane0; uint64_t lane_stride; uint32_t n_lanes; uint32_t shift; uint64_t off; };
+__global__ void k_gather_rows(const RowSrc* srcs, uint32_t n_src, const uint32_t* pos, uint32_t nq, uint64_t per_q,
+                              uint32_t* out) {
+  const uint32_t q = blockIdx.y;
+  const RowSrc s = srcs[blockIdx.z];
+  const uint32_t l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nq || l >= s.n_lanes) return;
+  uint32_t lo = (pos[q] >> s.shift) & ~1u;
+  const uint32_t* p = s.lane0 + l * s.lane_stride;
+  out[q * per_q + s.off + 2 * l] = p[lo];
+  out[q * per_q + s.off + 2 * l + 1] = p[lo + 1];
+}
+
+// Merkle paths: siblings of leaf idx = ((s_q >> shift) >> 1), leaf level
+// first, then the injection leaves inj_t[idx >> d_t].
+struct PathSrc {
+  const uint32_t* nodes;
+  const uint32_t* const* inj;
+  const uint32_t* inj_shift;  // d_t = log2(n_leaves / width_t)
+  uint32_t log_leaves;
+  uint32_t n_inj;
+  uint32_t shift;
+  uint64_t off;
+};
+__global__ void k_gather_paths(const PathSrc* srcs, const uint32_t* pos, uint32_t nq, uint64_t per_q, uint32_t* out) {
+  const uint32_t q = blockIdx.y;
+  const PathSrc s = srcs[blockIdx.z];
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nq || t >= s.log_leaves + s.n_inj) return;
+  uint32_t idx = (pos[q] >> s.shift) >> 1;
+  uint32_t* o = out + q * per_q + s.off + (uint64_t)t * 8;
+  const uint32_t* src;
+  if (t < s.log_leaves) {
+    uint64_t node = (((uint64_t)1 << s.log_leaves) + idx) >> t;
+    src = s.nodes + (node ^ 1) * 8;
+  } else {
+    uint32_t k = t - s.log_leaves;
+    src = s.inj[k] + (uint64_t)(idx >> s.inj_shift[k]) * 8;
+  }
+  for (int w = 0; w < 8; w++) o[w] = src[w];
+}
+
+}  // namespace lg

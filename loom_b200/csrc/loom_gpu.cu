@@ -1,0 +1,237 @@
+// C ABI of the library (declared in include/loom_gpu.h).  One translation
+// unit: every kernel and host component is included here.
+#include "../../include/loom_gpu.h"
+#include "prove_flow.cuh"
+
+using namespace lg;
+
+struct lg_ctx {
+  Ctx c;
+  std::vector<uint8_t> last_proof;
+};
+
+namespace {
+
+__global__ void k_aos_to_soa(const uint32_t* in, uint64_t n, uint32_t lanes, uint32_t* out) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n * lanes) return;
+  uint64_t row = i / lanes, w = i % lanes;
+  out[w * n + row] = in[i];
+}
+__global__ void k_soa_to_aos(const uint32_t* in, uint64_t n, uint32_t lanes, uint32_t* out) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n * lanes) return;
+  uint64_t row = i / lanes, w = i % lanes;
+  out[i] = in[w * n + row];
+}
+
+template <class F> int guarded(lg_ctx* ctx, F f) {
+  if (!ctx) return LG_ERR_INVALID;
+  try {
+    LG_CK(cudaSetDevice(ctx->c.device));
+    f();
+    return LG_OK;
+  } catch (Error& e) {
+    ctx->c.err = e.what();
+    return e.code;
+  } catch (std::exception& e) {
+    ctx->c.err = e.what();
+    return LG_ERR_INVALID;
+  }
+}
+
+// Copies `words` words from host or device memory into a fresh device buffer.
+DBufP to_device(Ctx& c, const uint32_t* src, size_t words, int on_device) {
+  auto b = std::make_shared<DBuf>(std::max<size_t>(words, 1), c.stream);
+  if (words)
+    LG_CK(cudaMemcpyAsync(b->p, src, words * 4, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c.stream));
+  return b;
+}
+void from_device(Ctx& c, uint32_t* dst, const uint32_t* src, size_t words, int on_device) {
+  LG_CK(cudaMemcpyAsync(dst, src, words * 4, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c.stream));
+  LG_CK(cudaStreamSynchronize(c.stream));
+}
+
+}  // namespace
+
+extern "C" {
+
+int lg_ctx_create(int device, lg_ctx** out) {
+  if (!out) return LG_ERR_INVALID;
+  *out = nullptr;
+  lg_ctx* ctx = new lg_ctx();
+  ctx->c.device = device;
+  int rc = guarded(ctx, [&] {
+    LG_CK(cudaStreamCreateWithFlags(&ctx->c.stream, cudaStreamNonBlocking));
+    cudaMemPool_t pool;
+    LG_CK(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t keep = UINT64_MAX;  // keep freed blocks for the next prove
+    LG_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    LG_CK(cudaDeviceGetAttribute(&ctx->c.sm_count, cudaDevAttrMultiProcessorCount, device));
+  });
+  if (rc != LG_OK) {
+    delete ctx;
+    return rc;
+  }
+  *out = ctx;
+  return LG_OK;
+}
+
+void lg_ctx_destroy(lg_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->c.device);
+  if (ctx->c.stream) cudaStreamSynchronize(ctx->c.stream);
+  ctx->c.tw.clear();
+  ctx->c.gpow.clear();
+  ctx->c.ginvpow.clear();
+  if (ctx->c.stream) {
+    cudaStreamSynchronize(ctx->c.stream);
+    cudaStreamDestroy(ctx->c.stream);
+  }
+  if (ctx->c.pinned) cudaFreeHost(ctx->c.pinned);
+  delete ctx;
+}
+
+const char* lg_last_error(lg_ctx* ctx) { return ctx ? ctx->c.err.c_str() : "null context"; }
+
+int lg_prove(lg_ctx* ctx, const char* hash_backend, const uint32_t* program, size_t program_words,
+             const uint32_t* const* witness, int witness_on_device, uint32_t num_queries, uint8_t* proof,
+             size_t* proof_len) {
+  return guarded(ctx, [&] {
+    std::string hb = hash_backend ? hash_backend : "";
+    if (hb != "" && hb != "poseidon2")
+      throw Error(LG_ERR_UNSUPPORTED, "hash backend \"" + hb + "\" is not available on the GPU path (poseidon2 only)");
+    if (!program || !proof_len) throw Error(LG_ERR_INVALID, "null argument");
+    Prover pr(ctx->c, program, program_words, num_queries);
+    ctx->last_proof = pr.prove(witness, witness_on_device != 0);
+    size_t need = ctx->last_proof.size();
+    if (!proof || *proof_len < need) {
+      *proof_len = need;
+      throw Error(LG_ERR_BUFFER, "proof buffer too small");
+    }
+    memcpy(proof, ctx->last_proof.data(), need);
+    *proof_len = need;
+  });
+}
+
+int lg_last_proof(lg_ctx* ctx, uint8_t* proof, size_t* proof_len) {
+  if (!ctx || !proof_len) return LG_ERR_INVALID;
+  size_t need = ctx->last_proof.size();
+  if (!proof || *proof_len < need) { *proof_len = need; return LG_ERR_BUFFER; }
+  memcpy(proof, ctx->last_proof.data(), need);
+  *proof_len = need;
+  return LG_OK;
+}
+
+int lg_commit_root(lg_ctx* ctx, uint32_t n_groups, const uint64_t* rows, const uint32_t* n_base,
+                   const uint32_t* n_ext, const uint32_t* const* cols, int on_device, uint32_t root[8]) {
+  return guarded(ctx, [&] {
+    Ctx& c = ctx->c;
+    if (!n_groups || !rows || !n_base || !n_ext || !cols || !root) throw Error(LG_ERR_INVALID, "null argument");
+    std::vector<DBufP> keep;
+    std::vector<GroupSpec> gs;
+    size_t ci = 0;
+    for (uint32_t g = 0; g < n_groups; g++) {
+      uint64_t n = rows[g];
+      if (n < 2 || (n & (n - 1))) throw Error(LG_ERR_INVALID, "group rows must be a power of two >= 2");
+      GroupSpec s;
+      s.log_n = 0;
+      while ((1ull << s.log_n) < n) s.log_n++;
+      s.nb = n_base[g];
+      s.ne = n_ext[g];
+      s.from_coeffs = false;
+      for (uint32_t i = 0; i < s.nb; i++) {
+        auto b = to_device(c, cols[ci++], n, on_device);
+        s.lanes.push_back(b->p);
+        keep.push_back(b);
+      }
+      for (uint32_t i = 0; i < s.ne; i++) {
+        auto a = to_device(c, cols[ci++], 6 * n, on_device);
+        auto b = std::make_shared<DBuf>(6 * n, c.stream);
+        k_aos_to_soa<<<(unsigned)((6 * n + 255) / 256), 256, 0, c.stream>>>(a->p, n, 6, b->p);
+        LG_LAUNCH();
+        for (int w = 0; w < 6; w++) s.lanes.push_back(b->p + (size_t)w * n);
+        keep.push_back(a);
+        keep.push_back(b);
+      }
+      gs.push_back(s);
+    }
+    Committed cm = commit(c, gs, false);
+    memcpy(root, cm.tree.root.v, 32);
+  });
+}
+
+int lg_rs_encode(lg_ctx* ctx, const uint32_t* in, uint64_t n_rows, uint32_t n_cols, uint32_t* out, int on_device) {
+  return guarded(ctx, [&] {
+    Ctx& c = ctx->c;
+    if (!in || !out || n_rows < 2 || (n_rows & (n_rows - 1))) throw Error(LG_ERR_INVALID, "bad arguments");
+    uint32_t logn = 0;
+    while ((1ull << logn) < n_rows) logn++;
+    auto src = to_device(c, in, n_rows * n_cols, on_device);
+    std::vector<const uint32_t*> lanes;
+    for (uint32_t i = 0; i < n_cols; i++) lanes.push_back(src->p + (size_t)i * n_rows);
+    LdeOut l = lde_lanes(c, lanes, logn, false, false);
+    from_device(c, out, l.lde->p, (size_t)n_cols * (n_rows << RATE_LOG), on_device);
+  });
+}
+
+int lg_poseidon2_permute(lg_ctx* ctx, uint32_t* states, uint64_t n_states, int on_device) {
+  return guarded(ctx, [&] {
+    Ctx& c = ctx->c;
+    if (!states) throw Error(LG_ERR_INVALID, "null argument");
+    if (!n_states) return;
+    auto b = to_device(c, states, 24 * n_states, on_device);
+    k_p2_permute<<<(unsigned)((n_states + 127) / 128), 128, 0, c.stream>>>(b->p, n_states);
+    LG_LAUNCH();
+    from_device(c, states, b->p, 24 * n_states, on_device);
+  });
+}
+
+int lg_merkle_root(lg_ctx* ctx, const uint32_t* leaves, uint64_t n_leaves, uint32_t n_inj, const uint64_t* inj_widths,
+                   const uint32_t* inj, int on_device, uint32_t root[8]) {
+  return guarded(ctx, [&] {
+    Ctx& c = ctx->c;
+    if (!leaves || !root || n_leaves == 0 || (n_leaves & (n_leaves - 1))) throw Error(LG_ERR_INVALID, "bad leaves");
+    TreeDev t;
+    while ((1ull << t.log_leaves) < n_leaves) t.log_leaves++;
+    t.nodes = std::make_shared<DBuf>(16 * n_leaves, c.stream);
+    LG_CK(cudaMemcpyAsync(t.nodes->p + 8 * n_leaves, leaves, 32 * n_leaves,
+                          on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c.stream));
+    size_t off = 0;
+    for (uint32_t k = 0; k < n_inj; k++) {
+      uint64_t w = inj_widths[k];
+      if (w == 0 || (w & (w - 1)) || w > n_leaves) throw Error(LG_ERR_INVALID, "bad injection width");
+      t.inj.push_back(to_device(c, inj + off, 8 * w, on_device));
+      uint32_t lw = 0;
+      while ((1ull << lw) < w) lw++;
+      t.inj_log_w.push_back(lw);
+      off += 8 * w;
+    }
+    build_tree(c, t);
+    memcpy(root, t.root.v, 32);
+  });
+}
+
+int lg_fri_fold(lg_ctx* ctx, const uint32_t* layer, uint64_t n, const uint32_t alpha[6], uint32_t* out, int on_device) {
+  return guarded(ctx, [&] {
+    Ctx& c = ctx->c;
+    if (!layer || !out || !alpha || n < 2 || (n & (n - 1)) || n > (1ull << 24)) throw Error(LG_ERR_INVALID, "bad arguments");
+    int logn = 0;
+    while ((1ull << logn) < n) logn++;
+    auto a = to_device(c, layer, 6 * n, on_device);
+    auto soa = std::make_shared<DBuf>(6 * n, c.stream);
+    k_aos_to_soa<<<(unsigned)((6 * n + 255) / 256), 256, 0, c.stream>>>(a->p, n, 6, soa->p);
+    LG_LAUNCH();
+    auto nx = std::make_shared<DBuf>(3 * n, c.stream);
+    E6 al;
+    for (int w = 0; w < 6; w++) al.c[w] = alpha[w];
+    k_fold<<<(unsigned)((n / 2 + 255) / 256), 256, 0, c.stream>>>(soa->p, n, al, c.twiddles(logn), inv(to_mont(2)), nx->p);
+    LG_LAUNCH();
+    auto aos = std::make_shared<DBuf>(3 * n, c.stream);
+    k_soa_to_aos<<<(unsigned)((3 * n + 255) / 256), 256, 0, c.stream>>>(nx->p, n / 2, 6, aos->p);
+    LG_LAUNCH();
+    from_device(c, out, aos->p, 3 * n, on_device);
+  });
+}
+
+}  // extern "C"

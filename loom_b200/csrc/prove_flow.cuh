@@ -1,0 +1,437 @@
+// Prover::prove: the ordered sequence of device phases and transcript steps.
+// Order of transcript operations follows prover/prover.go:142-719,
+// internal/fri/open.go:98-285 and internal/fri/fri.go:606-736.
+#pragma once
+#include "prover.cuh"
+
+namespace lg {
+
+inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool on_device) {
+  setup(witness, on_device);
+  const uint32_t R = pg.n_rounds;
+  for (uint32_t r = 0; r < R; r++) fs.add(coin_name(r));
+  fs.add("__zeta");
+  {
+    const std::string first = coin_name(0);
+    auto hb = string_to_elements(0x48415348u, "poseidon2");
+    fs.bind(first, hb.data(), hb.size());
+    std::vector<uint32_t> sz = {to_mont(0x53495a45u), to_mont((uint32_t)mod_order.size())};
+    for (uint32_t m : mod_order) sz.push_back(to_mont((uint32_t)mod_n(m)));
+    fs.bind(first, sz.data(), sz.size());
+  }
+  // ---- rounds: steps, commit, bind root, sample coin (prover/prover.go:360-411)
+  coins.assign(R, e6_zero());
+  size_t ti = 0;
+  for (uint32_t r = 0; r < R; r++) {
+    for (const Step& st : pg.steps) if (st.round == r) run_step(st);
+    if (ti < trees.size() && !trees[ti].air && trees[ti].round == (int)r) {
+      committed.push_back(commit_tree(trees[ti]));
+      Digest root = committed.back().tree.root;
+      commitments.push_back(root);
+      fs.bind(coin_name(r), root.v, 8);
+      ti++;
+    }
+    coins[r] = digest_e6(fs.compute(coin_name(r)));
+  }
+  // ---- AIR quotients and their commitment (prover/prover.go:461-561)
+  for (uint32_t m : mod_order) if (chunk_count(m)) quotient(m);
+  if (ti < trees.size() && trees[ti].air) {
+    committed.push_back(commit_tree(trees[ti]));
+    Digest root = committed.back().tree.root;
+    commitments.push_back(root);
+    fs.bind("__zeta", root.v, 8);
+    ti++;
+  }
+  zeta = digest_e6(fs.compute("__zeta"));
+
+  // ---- claimed values P(zeta w^s) from coefficients (internal/fri/values.go:46-110)
+  struct Poly { size_t t, g; bool ext; const uint32_t* coef; uint32_t logn; std::vector<int> shifts; };
+  std::vector<std::vector<std::vector<Poly>>> polys(trees.size());  // [tree][group] base polys then ext polys
+  for (size_t t = 0; t < trees.size(); t++) {
+    polys[t].resize(trees[t].groups.size());
+    for (size_t g = 0; g < trees[t].groups.size(); g++) {
+      const Group& G = trees[t].groups[g];
+      size_t n = mod_n(G.module);
+      uint32_t lw = root_ext[G.module] ? 6 : 1;
+      auto add_poly = [&](uint32_t idx, bool ext) {
+        Poly p{t, g, ext, nullptr, pg.modules[G.module].log_n, {}};
+        if (trees[t].air) { p.coef = chunk_coef.at(G.module)->p + (size_t)idx * lw * n; p.shifts = {0}; }
+        else {
+          p.coef = col_coef.at(idx);
+          auto it = col_shifts.find(idx);
+          if (it != col_shifts.end()) p.shifts = it->second;
+        }
+        polys[t][g].push_back(p);
+      };
+      for (uint32_t x : G.bcols) add_poly(x, false);
+      for (uint32_t x : G.ecols) add_poly(x, true);
+    }
+  }
+  std::map<std::pair<uint32_t, int>, DBufP> zp;  // (log n, shift) -> powers of zeta w^shift
+  std::map<std::pair<uint32_t, int>, E6> zpoint;
+  std::vector<DotJob> jobs;
+  for (auto& pt : polys)
+    for (auto& pgp : pt)
+      for (auto& p : pgp)
+        for (int s : p.shifts) {
+          auto key = std::make_pair(p.logn, s);
+          if (!zp.count(key)) {
+            uint32_t n = 1u << p.logn;
+            E6 z = e6_mul_base(zeta, mont_pow(root_of_unity_mont((int)p.logn), (uint64_t)s));
+            zpoint[key] = z;
+            auto b = std::make_shared<DBuf>(6 * (size_t)n, c.stream);
+            k_e6_powers<<<(n + 127) / 128, 128, 0, c.stream>>>(z, n, b->p);
+            LG_LAUNCH();
+            zp[key] = b;
+          }
+          uint32_t n = 1u << p.logn;
+          for (uint32_t w = 0; w < (p.ext ? 6u : 1u); w++)
+            jobs.push_back(DotJob{p.coef + (size_t)w * n, zp[key]->p, n, (uint32_t)jobs.size()});
+        }
+  std::vector<uint32_t> dots(6 * jobs.size());
+  if (!jobs.empty()) {
+    auto jd = upload_words(c, jobs.data(), jobs.size() * sizeof(DotJob));
+    auto od = std::make_shared<DBuf>(6 * jobs.size(), c.stream);
+    k_dot<<<(unsigned)jobs.size(), 256, 0, c.stream>>>((const DotJob*)jd->p, od->p);
+    LG_LAUNCH();
+    uint32_t* h = c.host_staging(dots.size());
+    c.d2h(h, od->p, dots.size());
+    memcpy(dots.data(), h, dots.size() * 4);
+  }
+  // values[t][g][poly][shift]
+  std::vector<std::vector<std::vector<std::vector<E6>>>> cv(trees.size());
+  {
+    size_t j = 0;
+    for (size_t t = 0; t < trees.size(); t++) {
+      cv[t].resize(polys[t].size());
+      for (size_t g = 0; g < polys[t].size(); g++)
+        for (auto& p : polys[t][g]) {
+          std::vector<E6> vals;
+          for (size_t si = 0; si < p.shifts.size(); si++) {
+            E6 v = e6_zero();
+            for (uint32_t w = 0; w < (p.ext ? 6u : 1u); w++, j++) {
+              E6 d;
+              for (int q = 0; q < 6; q++) d.c[q] = dots[6 * j + q];
+              E6 basis = e6_zero();
+              basis.c[w] = MONT_ONE;
+              v = e6_add(v, p.ext ? e6_mul(d, basis) : d);
+            }
+            vals.push_back(v);
+          }
+          cv[t][g].push_back(vals);
+        }
+    }
+  }
+  // DEEP classes = modules with committed groups, in sorted order
+  std::vector<uint32_t> classes;
+  for (uint32_t m : mod_order) {
+    bool has = false;
+    for (auto& t : trees) for (auto& g : t.groups) if (g.module == m) has = true;
+    if (has) classes.push_back(m);
+  }
+  fs.add("alpha_DEEP");
+  for (uint32_t m : classes)
+    for (size_t t = 0; t < trees.size(); t++)
+      for (size_t g = 0; g < trees[t].groups.size(); g++) {
+        if (trees[t].groups[g].module != m) continue;
+        for (auto& vals : cv[t][g]) for (auto& v : vals) fs.bind("alpha_DEEP", v.c, 6);
+      }
+  E6 alpha = digest_e6(fs.compute("alpha_DEEP"));
+
+  // ---- DEEP codewords on the LDE rows (internal/fri/deep.go:71-266)
+  std::vector<DBufP> deep(classes.size());
+  for (size_t ci = 0; ci < classes.size(); ci++) {
+    uint32_t m = classes[ci];
+    uint32_t logn = pg.modules[m].log_n;
+    size_t big = mod_n(m) << RATE_LOG;
+    uint32_t w_n = root_of_unity_mont((int)logn);
+    DeepJob jb{};
+    std::vector<DeepBundle> bundles;
+    std::vector<E6> pts;
+    E6 run = e6_one();
+    for (size_t t = 0; t < trees.size(); t++)
+      for (size_t g = 0; g < trees[t].groups.size(); g++) {
+        if (trees[t].groups[g].module != m) continue;
+        const LdeOut& l = committed[t].groups[g];
+        uint32_t lane = 0;
+        for (size_t i = 0; i < polys[t][g].size(); i++) {
+          const Poly& p = polys[t][g][i];
+          DeepBundle bu{};
+          bu.lane0 = l.lde->p + (size_t)lane * big;
+          bu.lane_stride = big;
+          bu.ext = p.ext;
+          bu.scale = run;
+          lane += p.ext ? 6 : 1;
+          for (size_t si = 0; si < p.shifts.size(); si++) {
+            E6 z = e6_mul_base(zeta, mont_pow(w_n, (uint64_t)p.shifts[si]));
+            size_t k = 0;
+            while (k < pts.size() && !e6_eq(pts[k], z)) k++;
+            if (k == pts.size()) {
+              if (pts.size() == DEEP_MAX_POINTS) throw Error(LG_ERR_UNSUPPORTED, "too many distinct opening points");
+              pts.push_back(z);
+              jb.a[k] = e6_zero();
+            }
+            jb.a[k] = e6_add(jb.a[k], e6_mul(run, cv[t][g][i][si]));
+            bu.mask |= 1u << k;
+          }
+          bundles.push_back(bu);
+          run = e6_mul(run, alpha);
+        }
+      }
+    for (size_t k = 0; k < pts.size(); k++) jb.z[k] = pts[k];
+    jb.n_points = (uint32_t)pts.size();
+    auto bd = upload_words(c, bundles.data(), bundles.size() * sizeof(DeepBundle));
+    jb.bundles = (const DeepBundle*)bd->p;
+    jb.n_bundles = (uint32_t)bundles.size();
+    jb.logn4 = (int)logn + RATE_LOG;
+    jb.tw = c.twiddles(jb.logn4);
+    deep[ci] = std::make_shared<DBuf>(6 * big, c.stream);
+    jb.out = deep[ci]->p;
+    k_deep<<<(unsigned)((big + 127) / 128), 128, 0, c.stream>>>(jb);
+    LG_LAUNCH();
+  }
+
+  // ---- FRI (internal/fri/fri.go:352-365,606-736)
+  std::vector<size_t> class_at(classes.size());
+  for (size_t i = 0; i < class_at.size(); i++) class_at[i] = i;
+  std::stable_sort(class_at.begin(), class_at.end(), [&](size_t a, size_t b) { return mod_n(classes[a]) > mod_n(classes[b]); });
+  const size_t L = class_at.size();
+  if (L == 0) throw Error(LG_ERR_INVALID, "nothing to open");
+  std::vector<uint32_t> lvl_log(L);
+  std::vector<DBufP> lvl(L);
+  for (size_t l = 0; l < L; l++) { lvl_log[l] = pg.modules[classes[class_at[l]]].log_n; lvl[l] = deep[class_at[l]]; }
+  const int NR = MAX_LOG_MODULE;
+  const int r0 = MAX_LOG_MODULE - (int)lvl_log[0];
+  auto jl = [&](size_t l) { return MAX_LOG_MODULE - (int)lvl_log[l]; };
+  for (size_t l = 1; l < L; l++) fs.add("fri_level_" + std::to_string(l) + "_gamma");
+  for (int j = 0; j < NR; j++) fs.add("fri_fold_" + std::to_string(j));
+  for (uint32_t k = 0; k < num_queries; k++) fs.add("fri_query_" + std::to_string(k));
+  TreeDev levels_tree;
+  levels_tree.log_leaves = lvl_log[0] + RATE_LOG - 1;
+  levels_tree.nodes = std::make_shared<DBuf>((size_t)16 << levels_tree.log_leaves, c.stream);
+  hash_leaves(c, lvl[0]->p, 0, 1, lvl_log[0] + RATE_LOG, levels_tree.nodes->p + ((size_t)8 << levels_tree.log_leaves));
+  for (size_t l = 1; l < L; l++) {
+    uint32_t lr = lvl_log[l] + RATE_LOG;
+    auto lv = std::make_shared<DBuf>((size_t)8 << (lr - 1), c.stream);
+    hash_leaves(c, lvl[l]->p, 0, 1, lr, lv->p);
+    levels_tree.inj.push_back(lv);
+    levels_tree.inj_log_w.push_back(lr - 1);
+  }
+  build_tree(c, levels_tree);
+  std::vector<E6> gam(L);
+  for (size_t l = 1; l < L; l++) {
+    std::string nm = "fri_level_" + std::to_string(l) + "_gamma";
+    if (l == 1) fs.bind(nm, levels_tree.root.v, 8);
+    gam[l] = digest_e6(fs.compute(nm));
+  }
+  Digest zero{};
+  for (int j = 0; j < r0; j++) {
+    fs.bind("fri_fold_" + std::to_string(j), zero.v, 8);
+    fs.compute("fri_fold_" + std::to_string(j));
+  }
+  std::vector<DBufP> layers(NR + 1);
+  std::vector<TreeDev> ftrees(NR);
+  std::vector<Digest> fri_roots;
+  size_t nj = (size_t)1 << (LOG_N_FRI - r0);
+  auto running = std::make_shared<DBuf>(6 * nj, c.stream);
+  LG_CK(cudaMemcpyAsync(running->p, lvl[0]->p, 6 * nj * 4, cudaMemcpyDeviceToDevice, c.stream));
+  const uint32_t inv2 = inv(to_mont(2));
+  for (int j = r0; j < NR; j++) {
+    if (j == r0) layers[j] = lvl[0];
+    for (size_t l = 1; l < L; l++) {
+      if (jl(l) != j) continue;
+      k_axpy_e6<<<(unsigned)((nj + 255) / 256), 256, 0, c.stream>>>(running->p, lvl[l]->p, nj, gam[l]);
+      LG_LAUNCH();
+    }
+    if (j > r0) layers[j] = running;
+    if (j == r0) ftrees[j] = levels_tree;
+    else {
+      TreeDev& t = ftrees[j];
+      t.log_leaves = (uint32_t)(LOG_N_FRI - j - 1);
+      t.nodes = std::make_shared<DBuf>((size_t)16 << t.log_leaves, c.stream);
+      hash_leaves(c, running->p, 0, 1, (uint32_t)(LOG_N_FRI - j), t.nodes->p + ((size_t)8 << t.log_leaves));
+      build_tree(c, t);
+    }
+    Digest root = ftrees[j].root;
+    std::string nm = "fri_fold_" + std::to_string(j);
+    fs.bind(nm, root.v, 8);
+    E6 a = digest_e6(fs.compute(nm));
+    if (j > r0) fri_roots.push_back(root);
+    auto next = std::make_shared<DBuf>(3 * nj, c.stream);
+    k_fold<<<(unsigned)((nj / 2 + 255) / 256), 256, 0, c.stream>>>(running->p, nj, a, c.twiddles(LOG_N_FRI - j), inv2, next->p);
+    LG_LAUNCH();
+    running = next;
+    nj /= 2;
+  }
+  std::vector<uint32_t> final_poly(6 * nj);
+  {
+    uint32_t* h = c.host_staging(6 * nj);
+    c.d2h(h, running->p, 6 * nj);
+    memcpy(final_poly.data(), h, 6 * nj * 4);
+    std::vector<uint32_t> fin = {to_mont(0x45585450u), to_mont((uint32_t)nj)};
+    for (size_t i = 0; i < nj; i++) for (int w = 0; w < 6; w++) fin.push_back(final_poly[w * nj + i]);
+    fs.bind("fri_query_0", fin.data(), fin.size());
+  }
+  std::vector<uint32_t> pos(num_queries);
+  for (uint32_t k = 0; k < num_queries; k++) {
+    Digest ch = fs.compute("fri_query_" + std::to_string(k));
+    uint64_t s = (((uint64_t)from_mont(ch.v[0]) << 31) ^ (uint64_t)from_mont(ch.v[1])) % (1ull << LOG_N_FRI);
+    pos[k] = (uint32_t)s;
+    if (k + 1 < num_queries) fs.bind("fri_query_" + std::to_string(k + 1), ch.v, 8);
+  }
+
+  // ---- openings: one gather into a staging buffer, one read-back
+  std::vector<RowSrc> rows;
+  std::vector<PathSrc> paths;
+  uint64_t per_q = 0;
+  auto add_rows = [&](const uint32_t* lane0, uint64_t stride, uint32_t nl, uint32_t shift) {
+    rows.push_back(RowSrc{lane0, stride, nl, shift, per_q});
+    uint64_t o = per_q;
+    per_q += 2ull * nl;
+    return o;
+  };
+  auto add_path = [&](const TreeDev& t, uint32_t shift, bool with_inj) {
+    PathSrc p{};
+    p.nodes = t.nodes->p;
+    p.inj = with_inj ? (const uint32_t* const*)t.inj_ptrs->p : nullptr;
+    p.inj_shift = with_inj ? t.inj_shift->p : nullptr;
+    p.log_leaves = t.log_leaves;
+    p.n_inj = with_inj ? (uint32_t)t.inj.size() : 0;
+    p.shift = shift;
+    p.off = per_q;
+    paths.push_back(p);
+    uint64_t o = per_q;
+    per_q += 8ull * (p.log_leaves + p.n_inj);
+    return o;
+  };
+  std::vector<uint64_t> fri_row_off(NR), fri_path_off(NR), lvl_row_off(L);
+  for (int j = r0; j < NR; j++) {
+    size_t n_j = (size_t)1 << (LOG_N_FRI - j);
+    fri_row_off[j] = add_rows(layers[j]->p, n_j, 6, (uint32_t)j);
+    fri_path_off[j] = add_path(ftrees[j], (uint32_t)j, false);
+  }
+  for (size_t l = 1; l < L; l++) lvl_row_off[l] = add_rows(lvl[l]->p, (size_t)1 << (lvl_log[l] + RATE_LOG), 6, (uint32_t)jl(l));
+  struct BatchOff { std::vector<uint64_t> rows; uint64_t path; };
+  std::vector<BatchOff> boff(committed.size());
+  for (size_t b = 0; b < committed.size(); b++) {
+    const Committed& cm = committed[b];
+    for (int gi : cm.order) {
+      const LdeOut& l = cm.groups[gi];
+      uint32_t log_rows = l.log_n + RATE_LOG;
+      boff[b].rows.push_back(add_rows(l.lde->p, (size_t)1 << log_rows, l.lanes, (uint32_t)(LOG_N_FRI - log_rows)));
+    }
+    const LdeOut& top = cm.groups[cm.order[0]];
+    boff[b].path = add_path(cm.tree, (uint32_t)(LOG_N_FRI - (top.log_n + RATE_LOG)), true);
+  }
+  auto pos_d = upload_words(c, pos.data(), pos.size() * 4);
+  auto out_d = std::make_shared<DBuf>(per_q * num_queries, c.stream);
+  {
+    auto rd = upload_words(c, rows.data(), rows.size() * sizeof(RowSrc));
+    uint32_t max_l = 1;
+    for (auto& r : rows) max_l = std::max(max_l, r.n_lanes);
+    k_gather_rows<<<dim3((max_l + 63) / 64, num_queries, (unsigned)rows.size()), 64, 0, c.stream>>>(
+        (const RowSrc*)rd->p, (uint32_t)rows.size(), pos_d->p, num_queries, per_q, out_d->p);
+    LG_LAUNCH();
+    auto pd = upload_words(c, paths.data(), paths.size() * sizeof(PathSrc));
+    uint32_t max_t = 1;
+    for (auto& p : paths) max_t = std::max(max_t, p.log_leaves + p.n_inj);
+    k_gather_paths<<<dim3((max_t + 31) / 32, num_queries, (unsigned)paths.size()), 32, 0, c.stream>>>(
+        (const PathSrc*)pd->p, pos_d->p, num_queries, per_q, out_d->p);
+    LG_LAUNCH();
+  }
+  uint32_t* G = c.host_staging(per_q * num_queries);
+  c.d2h(G, out_d->p, per_q * num_queries);
+
+  // ---- canonical encoding (same order as the proof structs)
+  Writer W;
+  W.str("poseidon2");
+  W.u32(0);
+  W.u32((uint32_t)commitments.size());
+  for (auto& d : commitments) W.dg(d);
+  W.u32((uint32_t)trees.size());
+  for (size_t t = 0; t < trees.size(); t++) {
+    W.u32((uint32_t)trees[t].groups.size());
+    for (size_t g = 0; g < trees[t].groups.size(); g++) {
+      const Group& G2 = trees[t].groups[g];
+      size_t nbp = G2.bcols.size();
+      W.u32((uint32_t)nbp);
+      for (size_t i = 0; i < nbp; i++) { W.u32((uint32_t)cv[t][g][i].size()); for (auto& v : cv[t][g][i]) W.e6(v); }
+      W.u32((uint32_t)G2.ecols.size());
+      for (size_t i = nbp; i < cv[t][g].size(); i++) { W.u32((uint32_t)cv[t][g][i].size()); for (auto& v : cv[t][g][i]) W.e6(v); }
+    }
+  }
+  auto wpair_e6 = [&](const uint32_t* q, uint64_t off) {  // lane-major (lo, hi) pairs of 6 lanes
+    uint32_t lo[6], hi[6];
+    for (int w = 0; w < 6; w++) { lo[w] = q[off + 2 * w]; hi[w] = q[off + 2 * w + 1]; }
+    W.e6w(lo);
+    W.e6w(hi);
+  };
+  auto wpath = [&](const uint32_t* q, uint64_t off, uint32_t leaf, uint32_t depth, uint32_t ninj) {
+    W.u32(leaf);
+    W.u32(depth);
+    for (uint32_t k = 0; k < depth; k++) W.dgw(q + off + 8 * k);
+    W.u32(ninj);
+    for (uint32_t k = 0; k < ninj; k++) W.dgw(q + off + 8 * (depth + k));
+  };
+  W.dg(levels_tree.root);
+  W.u32((uint32_t)(L - 1));
+  for (size_t l = 1; l < L; l++) {
+    W.u32(num_queries);
+    for (uint32_t k = 0; k < num_queries; k++) {
+      const uint32_t* q = G + (uint64_t)k * per_q;
+      W.u32(1);
+      W.u32(pos[k] >> jl(l));
+      wpair_e6(q, lvl_row_off[l]);
+      W.u32(0); W.u32(0); W.u32(0);
+    }
+  }
+  W.u32((uint32_t)fri_roots.size());
+  for (auto& d : fri_roots) W.dg(d);
+  W.u32(1);
+  W.u32((uint32_t)nj);
+  for (size_t i = 0; i < nj; i++) { uint32_t e[6]; for (int w = 0; w < 6; w++) e[w] = final_poly[w * nj + i]; W.e6w(e); }
+  W.u32(num_queries);
+  for (uint32_t k = 0; k < num_queries; k++) {
+    const uint32_t* q = G + (uint64_t)k * per_q;
+    W.u32((uint32_t)(NR - r0));
+    for (int j = r0; j < NR; j++) {
+      uint32_t row = pos[k] >> j;
+      W.u32(1);
+      W.u32(row);
+      wpair_e6(q, fri_row_off[j]);
+      wpath(q, fri_path_off[j], (row & ~1u) / 2, ftrees[j].log_leaves, 0);
+    }
+  }
+  W.u32(0);
+  W.u32(num_queries);
+  for (uint32_t k = 0; k < num_queries; k++) {
+    const uint32_t* q = G + (uint64_t)k * per_q;
+    W.u32((uint32_t)committed.size());
+    for (size_t b = 0; b < committed.size(); b++) {
+      const Committed& cm = committed[b];
+      auto wrowpair = [&](int gi, uint64_t off) {
+        const LdeOut& l = cm.groups[gi];
+        const Group& G2 = trees[b].groups[gi];
+        uint32_t nb = (uint32_t)G2.bcols.size(), ne = (uint32_t)G2.ecols.size();
+        (void)l;
+        for (int h = 0; h < 2; h++) {
+          W.u32(nb);
+          for (uint32_t i = 0; i < nb; i++) W.el(q[off + 2 * i + h]);
+          W.u32(ne);
+          for (uint32_t e = 0; e < ne; e++)
+            for (int w = 0; w < 6; w++) W.el(q[off + 2 * (nb + 6 * e + w) + h]);
+        }
+      };
+      const LdeOut& top = cm.groups[cm.order[0]];
+      uint32_t top_row = pos[k] >> (LOG_N_FRI - (top.log_n + RATE_LOG));
+      wrowpair(cm.order[0], boff[b].rows[0]);
+      wpath(q, boff[b].path, (top_row & ~1u) / 2, cm.tree.log_leaves, (uint32_t)cm.tree.inj.size());
+      W.u32((uint32_t)(cm.order.size() - 1));
+      for (size_t s = 1; s < cm.order.size(); s++) wrowpair(cm.order[s], boff[b].rows[s]);
+    }
+  }
+  LG_CK(cudaStreamSynchronize(c.stream));
+  return W.b;
+}
+
+}  // namespace lg

@@ -1,0 +1,425 @@
+// The prove flow on one device (prover/prover.go:142-719): rounds with
+// grand-product steps and commits, AIR quotients, claimed values, DEEP
+// codewords, multi-degree FRI and query openings.  The transcript runs on the
+// host; roots and openings are read back from the device.
+#pragma once
+#include <set>
+
+#include "commit.cuh"
+
+namespace lg {
+
+constexpr int MAX_LOG_MODULE = 22;  // internal/constants/const.go:27-32
+constexpr int LOG_N_FRI = MAX_LOG_MODULE + RATE_LOG;
+const int NEG_INF = -1000000;
+
+inline std::string coin_name(uint32_t r) { return "challenge@loom_" + std::to_string(r); }
+
+struct ProveStats { double ms_total = 0; };
+
+struct Prover {
+  Ctx& c;
+  Program pg;
+  uint32_t num_queries;
+  Transcript fs;
+  std::vector<E6> coins;
+  DBufP coins_dev;
+  std::vector<uint32_t> mod_order;
+  std::vector<int> fold_root, degree;
+  std::vector<bool> root_ext;
+  std::map<uint32_t, std::vector<int>> col_shifts;
+
+  // column data on the device: lane pointer = buf + w * n
+  std::map<uint32_t, DBufP> col_buf;
+  std::map<uint32_t, const uint32_t*> col_coef;  // committed columns: coefficient lane 0
+
+  struct Group { uint32_t module; std::vector<uint32_t> bcols, ecols; };
+  struct TreeL { bool air; int round; std::vector<Group> groups; };
+  std::vector<TreeL> trees;
+  std::vector<Committed> committed;
+  std::vector<Digest> commitments;
+  std::map<uint32_t, DBufP> chunk_coef;  // module -> chunks (d * lanes + w) * n
+  E6 zeta;
+
+  Prover(Ctx& ctx, const uint32_t* words, size_t nwords, uint32_t q) : c(ctx), num_queries(q) {
+    pg = parse_program(words, nwords);
+    if (q == 0) throw Error(LG_ERR_INVALID, "num_queries must be positive");
+  }
+
+  size_t mod_n(uint32_t m) const { return (size_t)1 << pg.modules[m].log_n; }
+  uint32_t lanes_of(uint32_t col) const { return pg.columns[col].field ? 6 : 1; }
+  const uint32_t* lane_ptr(uint32_t col, uint32_t w) const {
+    return col_buf.at(col)->p + (size_t)w * mod_n(pg.columns[col].module);
+  }
+
+  // ------------------------------------------------------------ DAG helpers
+  uint32_t push(uint32_t op, uint32_t a, uint32_t b) { pg.nodes.push_back({op, a, b}); return (uint32_t)pg.nodes.size() - 1; }
+  int node_degree(uint32_t id, std::vector<int>& memo) {
+    if (memo[id] != INT32_MIN) return memo[id];
+    const Node& x = pg.nodes[id];
+    int d = 0;
+    switch (x.op) {
+      case OP_COL: d = 1; break;
+      case OP_COIN: d = 0; break;
+      case OP_CONST: d = x.a % P == 0 ? NEG_INF : 0; break;
+      case OP_ADD: case OP_SUB: d = std::max(node_degree(x.a, memo), node_degree(x.b, memo)); break;
+      default: {
+        int l = node_degree(x.a, memo), r = node_degree(x.b, memo);
+        d = (l == NEG_INF || r == NEG_INF) ? NEG_INF : l + r;
+      }
+    }
+    return memo[id] = d;
+  }
+  bool node_ext(uint32_t id) const {
+    const Node& x = pg.nodes[id];
+    if (x.op == OP_COL) return pg.columns[x.a].field == 1;
+    if (x.op == OP_COIN) return true;
+    if (x.op == OP_CONST) return false;
+    return false;  // combined by the caller through ext_of
+  }
+  std::vector<char> ext_of;  // per node
+  void compute_ext() {
+    ext_of.assign(pg.nodes.size(), 0);
+    for (size_t i = 0; i < pg.nodes.size(); i++) {
+      const Node& x = pg.nodes[i];
+      if (x.op >= OP_ADD) ext_of[i] = ext_of[x.a] || ext_of[x.b];
+      else ext_of[i] = node_ext((uint32_t)i);
+    }
+  }
+  void collect(uint32_t id, std::vector<char>& seen) {
+    std::vector<uint32_t> st = {id};
+    while (!st.empty()) {
+      uint32_t x = st.back();
+      st.pop_back();
+      if (seen[x]) continue;
+      seen[x] = 1;
+      if (pg.nodes[x].op >= OP_ADD) { st.push_back(pg.nodes[x].a); st.push_back(pg.nodes[x].b); }
+    }
+  }
+
+  // Compiles the sub-DAG under `root` into register bytecode.  lane_of(col)
+  // gives the first lane index the kernel reads for that column.
+  struct XCode { std::vector<XInst> code; uint32_t n_regs = 0, result = 0, result_ext = 0; };
+  template <class LaneOf> XCode compile_expr(uint32_t root, LaneOf lane_of) {
+    std::vector<char> seen(pg.nodes.size(), 0);
+    collect(root, seen);
+    std::vector<uint32_t> order;
+    for (uint32_t i = 0; i < pg.nodes.size(); i++) if (seen[i]) order.push_back(i);
+    std::vector<int> last(pg.nodes.size(), -1);
+    for (size_t k = 0; k < order.size(); k++) {
+      const Node& x = pg.nodes[order[k]];
+      if (x.op >= OP_ADD) { last[x.a] = (int)k; last[x.b] = (int)k; }
+    }
+    last[root] = (int)order.size();
+    std::vector<int> reg(pg.nodes.size(), -1);
+    std::vector<uint32_t> free_regs;
+    XCode xc;
+    for (size_t k = 0; k < order.size(); k++) {
+      uint32_t id = order[k];
+      const Node& x = pg.nodes[id];
+      XInst in{};
+      // free operand registers whose last use is here (after reading them)
+      std::vector<uint32_t> to_free;
+      if (x.op >= OP_ADD) {
+        if (last[x.a] == (int)k) to_free.push_back((uint32_t)reg[x.a]);
+        if (last[x.b] == (int)k && x.b != x.a) to_free.push_back((uint32_t)reg[x.b]);
+      }
+      uint32_t d;
+      if (!free_regs.empty()) { d = free_regs.back(); free_regs.pop_back(); }
+      else d = xc.n_regs++;
+      in.d = (uint8_t)d;
+      bool ea = x.op >= OP_ADD && ext_of[x.a], eb = x.op >= OP_ADD && ext_of[x.b];
+      uint32_t ra = x.op >= OP_ADD ? (uint32_t)reg[x.a] : 0, rb = x.op >= OP_ADD ? (uint32_t)reg[x.b] : 0;
+      switch (x.op) {
+        case OP_COL:
+          in.op = pg.columns[x.a].field ? X_LOAD_E : X_LOAD_B;
+          in.imm = lane_of(x.a);
+          in.shift = (int32_t)x.b;
+          break;
+        case OP_COIN: in.op = X_COIN; in.imm = x.a; break;
+        case OP_CONST: in.op = X_CONST; in.imm = to_mont(x.a % P); break;
+        case OP_ADD:
+          if (!ea && !eb) in.op = X_ADD_BB;
+          else if (ea && eb) in.op = X_ADD_EE;
+          else { in.op = X_ADD_EB; if (!ea) std::swap(ra, rb); }
+          break;
+        case OP_SUB:
+          in.op = (!ea && !eb) ? X_SUB_BB : (ea && eb) ? X_SUB_EE : ea ? X_SUB_EB : X_SUB_BE;
+          break;
+        default:
+          if (!ea && !eb) in.op = X_MUL_BB;
+          else if (ea && eb) in.op = X_MUL_EE;
+          else { in.op = X_MUL_EB; if (!ea) std::swap(ra, rb); }
+      }
+      in.a = (uint8_t)ra;
+      in.b = (uint8_t)rb;
+      reg[id] = (int)d;
+      xc.code.push_back(in);
+      for (uint32_t r : to_free) free_regs.push_back(r);
+    }
+    xc.result = (uint32_t)reg[root];
+    xc.result_ext = ext_of[root];
+    if (xc.n_regs > X_MAX_REGS || xc.code.size() > X_MAX_INST)
+      throw Error(LG_ERR_UNSUPPORTED, "constraint expression too large for the device evaluator");
+    return xc;
+  }
+
+  // ------------------------------------------------------------ setup
+  void setup(const uint32_t* const* witness, bool on_device) {
+    for (uint32_t m = 0; m < pg.modules.size(); m++) mod_order.push_back(m);
+    std::sort(mod_order.begin(), mod_order.end(), [&](uint32_t a, uint32_t b) { return pg.modules[a].name < pg.modules[b].name; });
+    size_t wi = 0;
+    for (uint32_t col = 0; col < pg.columns.size(); col++) {
+      const Column& cl = pg.columns[col];
+      size_t n = mod_n(cl.module);
+      if (cl.kind == KIND_WITNESS) {
+        if (cl.field != 0) throw Error(LG_ERR_UNSUPPORTED, "extension-field witness columns are not supported");
+        auto b = std::make_shared<DBuf>(n, c.stream);
+        LG_CK(cudaMemcpyAsync(b->p, witness[wi++], n * 4, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                              c.stream));
+        col_buf[col] = b;
+      } else if (cl.kind == KIND_LAGRANGE) {
+        int64_t row = cl.param >= 0 ? cl.param : (int64_t)n - 1 - (-(int64_t)cl.param - 1);
+        if (row < 0 || row >= (int64_t)n) throw Error(LG_ERR_INVALID, "Lagrange column row out of range");
+        auto b = std::make_shared<DBuf>(n, c.stream);
+        LG_CK(cudaMemsetAsync(b->p, 0, n * 4, c.stream));
+        uint32_t one = MONT_ONE;
+        c.h2d(b->p + row, &one, 4);
+        col_buf[col] = b;
+      }
+    }
+    // fold relations with coin(last round) (board/program.go:62-80)
+    fold_root.assign(pg.modules.size(), -1);
+    degree.assign(pg.modules.size(), NEG_INF);
+    root_ext.assign(pg.modules.size(), false);
+    for (uint32_t m = 0; m < pg.modules.size(); m++) {
+      const auto& rels = pg.modules[m].rels;
+      if (rels.empty()) continue;
+      uint32_t res = rels.back();
+      for (int i = (int)rels.size() - 2; i >= 0; i--) {
+        uint32_t cn = push(OP_COIN, pg.n_rounds - 1, 0);
+        uint32_t t = push(OP_MUL, cn, res);
+        res = push(OP_ADD, rels[i], t);
+      }
+      fold_root[m] = (int)res;
+    }
+    compute_ext();
+    for (uint32_t m = 0; m < pg.modules.size(); m++) {
+      if (fold_root[m] < 0) continue;
+      std::vector<int> memo(pg.nodes.size(), INT32_MIN);
+      degree[m] = node_degree((uint32_t)fold_root[m], memo);
+      root_ext[m] = ext_of[fold_root[m]];
+    }
+    // shift schedule (internal/protocol/schedule.go:92-157)
+    for (uint32_t m : mod_order) {
+      if (fold_root[m] < 0) continue;
+      std::vector<char> seen(pg.nodes.size(), 0);
+      collect((uint32_t)fold_root[m], seen);
+      int64_t n = (int64_t)mod_n(m);
+      for (uint32_t id = 0; id < pg.nodes.size(); id++) {
+        if (!seen[id] || pg.nodes[id].op != OP_COL) continue;
+        const Column& cl = pg.columns[pg.nodes[id].a];
+        if (cl.kind == KIND_LAGRANGE) continue;
+        int64_t sh = (int32_t)pg.nodes[id].b;
+        int s = (int)(((sh % n) + n) % n);
+        auto& v = col_shifts[pg.nodes[id].a];
+        if (std::find(v.begin(), v.end(), s) == v.end()) v.push_back(s);
+      }
+    }
+    for (auto& kv : col_shifts) std::sort(kv.second.begin(), kv.second.end());
+    // layout (internal/protocol/layout.go:165-241)
+    for (uint32_t r = 0; r < pg.n_rounds; r++) {
+      TreeL t{false, (int)r, {}};
+      for (uint32_t m : mod_order) {
+        Group g{m, {}, {}};
+        for (uint32_t col : pg.staged[r]) {
+          if (pg.columns[col].module != m) continue;
+          if (pg.columns[col].kind == KIND_LAGRANGE) throw Error(LG_ERR_INVALID, "verifier column staged for commitment");
+          (pg.columns[col].field == 0 ? g.bcols : g.ecols).push_back(col);
+        }
+        if (!g.bcols.empty() || !g.ecols.empty()) t.groups.push_back(g);
+      }
+      if (!t.groups.empty()) trees.push_back(t);
+    }
+    TreeL air{true, -1, {}};
+    for (uint32_t m : mod_order) {
+      uint32_t nch = chunk_count(m);
+      if (!nch) continue;
+      Group g{m, {}, {}};
+      for (uint32_t k = 0; k < nch; k++) (root_ext[m] ? g.ecols : g.bcols).push_back(k);
+      air.groups.push_back(g);
+    }
+    if (!air.groups.empty()) trees.push_back(air);
+    for (uint32_t m = 0; m < pg.modules.size(); m++)
+      if (pg.modules[m].log_n > MAX_LOG_MODULE) throw Error(LG_ERR_INVALID, "module above 2^22 rows");
+  }
+
+  uint32_t chunk_count(uint32_t m) const {
+    if (fold_root[m] < 0 || degree[m] <= 0) return 0;
+    size_t n = mod_n(m), want = (size_t)std::max(degree[m] - 1, 1) * n, big = 1;
+    while (big < want) big <<= 1;
+    return (uint32_t)(big / n);
+  }
+
+  DBufP coins_on_device() {
+    std::vector<uint32_t> w;
+    for (auto& e : coins) for (int i = 0; i < 6; i++) w.push_back(e.c[i]);
+    return upload_words(c, w.data(), w.size() * 4);
+  }
+
+  // ------------------------------------------------------------ steps
+  // Grand product (internal/poly/iop_utils.go:170-192,316-323).
+  void run_step(const Step& st) {
+    uint32_t logn = pg.modules[st.module].log_n;
+    size_t n = (size_t)1 << logn;
+    std::vector<const uint32_t*> lanes;
+    std::map<uint32_t, uint32_t> first_lane;
+    auto lane_of = [&](uint32_t col) -> uint32_t {
+      auto it = first_lane.find(col);
+      if (it != first_lane.end()) return it->second;
+      if (!col_buf.count(col)) throw Error(LG_ERR_INVALID, "step reads a column that is not available yet");
+      uint32_t f = (uint32_t)lanes.size();
+      for (uint32_t w = 0; w < lanes_of(col); w++) lanes.push_back(lane_ptr(col, w));
+      first_lane[col] = f;
+      return f;
+    };
+    XCode xn = compile_expr(st.num, lane_of), xd = compile_expr(st.den, lane_of);
+    auto tab = upload_ptrs(c, lanes);
+    auto cn = upload_words(c, xn.code.data(), xn.code.size() * sizeof(XInst));
+    auto cd = upload_words(c, xd.code.data(), xd.code.size() * sizeof(XInst));
+    auto coins_d = coins_on_device();
+    auto out = std::make_shared<DBuf>(6 * n, c.stream);
+    XProgram pn{(const XInst*)cn->p, (uint32_t)xn.code.size(), xn.n_regs, xn.result, xn.result_ext};
+    XProgram pd{(const XInst*)cd->p, (uint32_t)xd.code.size(), xd.n_regs, xd.result, xd.result_ext};
+    const int T = 128;
+    size_t smem = (size_t)std::max(std::max(xn.n_regs, xd.n_regs), 1u) * 6 * T * 4;
+    LG_CK(cudaFuncSetAttribute(k_gp_ratio, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_gp_ratio<<<(unsigned)((n + T - 1) / T), T, smem, c.stream>>>(pn, pd, (const E6*)coins_d->p,
+                                                                     LaneTable{(const uint32_t* const*)tab->p}, (int)logn, out->p);
+    LG_LAUNCH();
+    uint32_t nt = (uint32_t)((n + SCAN_TILE - 1) / SCAN_TILE);
+    auto totals = std::make_shared<DBuf>(6 * (size_t)nt, c.stream);
+    k_scan_tiles<<<nt, SCAN_BLOCK, 0, c.stream>>>(out->p, n, totals->p);
+    LG_LAUNCH();
+    auto pre = std::make_shared<DBuf>(6 * (size_t)nt, c.stream);
+    k_tile_prefix<<<1, 1, 0, c.stream>>>(totals->p, nt, pre->p);
+    LG_LAUNCH();
+    auto res = std::make_shared<DBuf>(6 * n, c.stream);
+    k_gp_finish<<<(unsigned)((n + 255) / 256), 256, 0, c.stream>>>(out->p, n, pre->p, res->p);
+    LG_LAUNCH();
+    col_buf[st.out] = res;
+  }
+
+  // ------------------------------------------------------------ commits
+  Committed commit_tree(const TreeL& t) {
+    std::vector<GroupSpec> gs;
+    for (const Group& g : t.groups) {
+      GroupSpec s;
+      s.log_n = pg.modules[g.module].log_n;
+      s.nb = (uint32_t)g.bcols.size();
+      s.ne = (uint32_t)g.ecols.size();
+      size_t n = mod_n(g.module);
+      if (t.air) {
+        s.from_coeffs = true;
+        uint32_t lw = root_ext[g.module] ? 6 : 1;
+        const uint32_t* base = chunk_coef.at(g.module)->p;
+        for (uint32_t k : g.bcols) s.lanes.push_back(base + (size_t)k * n);
+        for (uint32_t k : g.ecols) for (uint32_t w = 0; w < 6; w++) s.lanes.push_back(base + ((size_t)k * lw + w) * n);
+      } else {
+        s.from_coeffs = false;
+        for (uint32_t col : g.bcols) s.lanes.push_back(lane_ptr(col, 0));
+        for (uint32_t col : g.ecols) for (uint32_t w = 0; w < 6; w++) s.lanes.push_back(lane_ptr(col, w));
+      }
+      gs.push_back(s);
+    }
+    Committed cm = commit(c, gs, !t.air);
+    if (!t.air) {
+      for (size_t gi = 0; gi < t.groups.size(); gi++) {
+        const Group& g = t.groups[gi];
+        size_t n = mod_n(g.module);
+        uint32_t lane = 0;
+        for (uint32_t col : g.bcols) col_coef[col] = cm.groups[gi].coef->p + (size_t)(lane++) * n;
+        for (uint32_t col : g.ecols) { col_coef[col] = cm.groups[gi].coef->p + (size_t)lane * n; lane += 6; }
+      }
+    }
+    return cm;
+  }
+
+  // ------------------------------------------------------------ quotient
+  void quotient(uint32_t m) {
+    uint32_t logn = pg.modules[m].log_n;
+    size_t n = mod_n(m), big = n << RATE_LOG;
+    uint32_t rho = chunk_count(m);
+    if (rho != 4) throw Error(LG_ERR_UNSUPPORTED, "quotient domains other than 4N are not supported by this build");
+    check_ntt_size((int)logn);
+    // coefficient lanes of every column the relation reads
+    std::vector<const uint32_t*> coef_lanes;
+    std::map<uint32_t, uint32_t> first_lane;
+    std::vector<DBufP> keep;
+    auto lane_of = [&](uint32_t col) -> uint32_t {
+      auto it = first_lane.find(col);
+      if (it != first_lane.end()) return it->second;
+      uint32_t f = (uint32_t)coef_lanes.size();
+      auto cc = col_coef.find(col);
+      if (cc != col_coef.end()) {
+        for (uint32_t w = 0; w < lanes_of(col); w++) coef_lanes.push_back(cc->second + (size_t)w * n);
+      } else {
+        // verifier columns: coefficients from a copy of the Lagrange values
+        auto b = std::make_shared<DBuf>(lanes_of(col) * n, c.stream);
+        LG_CK(cudaMemcpyAsync(b->p, col_buf.at(col)->p, lanes_of(col) * n * 4, cudaMemcpyDeviceToDevice, c.stream));
+        allow_smem(k_intt_inplace, n * 4);
+        k_intt_inplace<<<lanes_of(col), ntt_threads((int)logn), n * 4, c.stream>>>(b->p, n, (int)logn, c.twiddles((int)logn),
+                                                                                   inv(to_mont((uint32_t)n)));
+        LG_LAUNCH();
+        keep.push_back(b);
+        for (uint32_t w = 0; w < lanes_of(col); w++) coef_lanes.push_back(b->p + (size_t)w * n);
+      }
+      first_lane[col] = f;
+      return f;
+    };
+    XCode xc = compile_expr((uint32_t)fold_root[m], lane_of);
+    const uint32_t* twn = c.twiddles((int)logn);
+    const uint32_t* tw4 = c.twiddles((int)logn + RATE_LOG);
+    auto tab = upload_ptrs(c, coef_lanes);
+    auto cv = std::make_shared<DBuf>(coef_lanes.size() * big, c.stream);
+    dim3 grid((unsigned)coef_lanes.size(), 4);
+    allow_smem(k_coset_eval_ptrs, n * 4);
+    k_coset_eval_ptrs<<<grid, ntt_threads((int)logn), n * 4, c.stream>>>((const uint32_t* const*)tab->p, (int)logn, twn, tw4,
+                                                                         c.gpowers((int)logn, false), cv->p);
+    LG_LAUNCH();
+    // 1 / (s_c^n - 1), s_c = g w_4n^c (internal/poly/compute_quotient.go:400-421)
+    uint32_t zinv[4];
+    uint32_t g = to_mont(3), w4n = root_of_unity_mont((int)logn + RATE_LOG);
+    for (int cc = 0; cc < 4; cc++) {
+      uint32_t s = mul(g, mont_pow(w4n, cc));
+      zinv[cc] = inv(sub(mont_pow(s, n), MONT_ONE));
+    }
+    auto zinv_d = upload_words(c, zinv, sizeof zinv);
+    auto code = upload_words(c, xc.code.data(), xc.code.size() * sizeof(XInst));
+    auto coins_d = coins_on_device();
+    uint32_t lw = root_ext[m] ? 6 : 1;
+    auto qv = std::make_shared<DBuf>(6 * big, c.stream);
+    XProgram xp{(const XInst*)code->p, (uint32_t)xc.code.size(), xc.n_regs, xc.result, xc.result_ext};
+    const int T = 128;
+    size_t smem = (size_t)std::max(xc.n_regs, 1u) * 6 * T * 4;
+    LG_CK(cudaFuncSetAttribute(k_quotient_eval, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_quotient_eval<<<dim3((unsigned)((n + T - 1) / T), 4), T, smem, c.stream>>>(xp, (const E6*)coins_d->p, cv->p,
+                                                                                 (int)logn, zinv_d->p, qv->p);
+    LG_LAUNCH();
+    // coset values -> per-coset coefficients -> chunk coefficients
+    allow_smem(k_intt_inplace, n * 4);
+    k_intt_inplace<<<(unsigned)(lw * 4), ntt_threads((int)logn), n * 4, c.stream>>>(qv->p, n, (int)logn, twn,
+                                                                                    inv(to_mont((uint32_t)n)));
+    LG_LAUNCH();
+    auto chunks = std::make_shared<DBuf>(4 * lw * n, c.stream);
+    uint32_t gn_inv = inv(mont_pow(g, n));
+    k_quotient_chunks<<<dim3((unsigned)((n + 127) / 128), lw), 128, 0, c.stream>>>(
+        qv->p, (int)logn, c.gpowers((int)logn, true), tw4, chunks->p, inv(to_mont(4)), gn_inv, (int)lw);
+    LG_LAUNCH();
+    chunk_coef[m] = chunks;
+  }
+
+  std::vector<uint8_t> prove(const uint32_t* const* witness, bool on_device);
+};
+
+}  // namespace lg

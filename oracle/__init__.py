@@ -167,3 +167,13 @@ def merkle_root(leaves_mont: np.ndarray, injections: Sequence[np.ndarray] = ()) 
     root = np.zeros(8, dtype=np.uint32)
     lib().oracle_merkle_root(_p(lv), lv.size // 8, len(injections), widths.ctypes.data_as(u64p), _p(inj), _p(root))
     return root
+
+
+def fri_fold(layer_mont, alpha_mont) -> np.ndarray:
+    L = lib()
+    L.oracle_fri_fold.argtypes = [u32p, ctypes.c_size_t, u32p, u32p]
+    x = _u32(layer_mont).reshape(-1)
+    a = _u32(alpha_mont)
+    out = np.zeros(x.size // 2, dtype=np.uint32)
+    L.oracle_fri_fold(_p(x), x.size // 6, _p(a), _p(out))
+    return out.reshape(-1, 6)

@@ -175,3 +175,25 @@ void oracle_merkle_root(const uint32_t* leaves, size_t n, uint32_t n_inj, const 
 }
 
 }  // extern "C"
+
+extern "C" {
+// One FRI fold of n E6 values in bit-reversed order, Montgomery in/out
+// (internal/fri/fri.go:1177-1198).
+void oracle_fri_fold(const uint32_t* layer, size_t n, const uint32_t* alpha, uint32_t* out) {
+  E6 a;
+  for (int k = 0; k < 6; k++) a.c[k] = from_mont(alpha[k]);
+  size_t half = n / 2;
+  int lg = 0;
+  while ((1ull << lg) < half) lg++;
+  uint32_t winv = inv(root_of_unity(n)), inv2 = inv(2);
+  for (size_t i = 0; i < half; i++) {
+    E6 p, q;
+    for (int k = 0; k < 6; k++) { p.c[k] = from_mont(layer[6 * (2 * i) + k]); q.c[k] = from_mont(layer[6 * (2 * i + 1) + k]); }
+    uint32_t xi = pow(winv, bitrev((uint32_t)i, lg));
+    E6 s = e6_mul_base(e6_add(p, q), inv2);
+    E6 d = e6_mul(e6_mul_base(e6_mul_base(e6_sub(p, q), inv2), xi), a);
+    E6 r = e6_add(s, d);
+    for (int k = 0; k < 6; k++) out[6 * i + k] = to_mont(r.c[k]);
+  }
+}
+}

@@ -1,0 +1,140 @@
+"""GPU parity: every CUDA entry point against the CPU oracle, through the C ABI.
+
+Integer/field work, so the bar is bit-exact equality.  Sizes are ones the
+oracle finishes in seconds; the full 40 x 2^14 workload is covered by
+size-independent properties in test_gpu_full.py.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from loom_b200 import LoomError, field as F, plonk, proof
+
+pytestmark = pytest.mark.gpu
+
+
+def rnd(shape, seed):
+    return np.random.Generator(np.random.PCG64(seed)).integers(0, F.P, shape, dtype=np.uint64).astype(np.uint32)
+
+
+def test_poseidon2_permutation(ctx):
+    canon = rnd((257, 24), 1)
+    canon[0] = 0
+    got = F.from_mont(ctx.poseidon2_permute(F.to_mont(canon)))
+    for i in range(canon.shape[0]):
+        assert np.array_equal(got[i], oracle.p2_permute(canon[i], 24)), i
+
+
+@pytest.mark.parametrize("logn", [1, 2, 5, 8, 10, 12, 13, 14])
+def test_rs_encode(ctx, logn):
+    cols = F.to_mont(rnd((3, 1 << logn), logn))
+    got = ctx.rs_encode(cols)
+    for i in range(3):
+        assert np.array_equal(got[i], oracle.rs_encode(cols[i], 4 << logn)), (logn, i)
+
+
+def test_rs_encode_edge_values(ctx):
+    n = 1 << 9
+    cols = np.stack([np.zeros(n), np.full(n, F.P - 1), np.arange(n) % 2]).astype(np.uint32)
+    cols = F.to_mont(cols)
+    got = ctx.rs_encode(cols)
+    for i in range(cols.shape[0]):
+        assert np.array_equal(got[i], oracle.rs_encode(cols[i], 4 * n))
+
+
+@pytest.mark.parametrize("shape", [
+    [(1 << 10, 3, 0)],
+    [(1 << 8, 0, 1)],
+    [(1 << 10, 2, 1), (1 << 10, 1, 0), (1 << 8, 4, 2), (1 << 10, 0, 1), (1 << 6, 1, 0), (1 << 9, 2, 0)],
+    [(2, 1, 0), (2, 0, 1)],
+])
+def test_commit_root(ctx, shape):
+    groups = []
+    for gi, (n, nb, ne) in enumerate(shape):
+        groups.append({"rows": n,
+                       "base": [F.to_mont(rnd(n, 100 * gi + k)) for k in range(nb)],
+                       "ext": [F.to_mont(rnd((n, 6), 100 * gi + 50 + k)) for k in range(ne)]})
+    assert np.array_equal(ctx.commit_root(groups), oracle.commit(groups))
+
+
+def test_merkle_injections(ctx):
+    leaves = F.to_mont(rnd((64, 8), 7))
+    inj = [F.to_mont(rnd((64, 8), 8)), F.to_mont(rnd((64, 8), 9)), F.to_mont(rnd((16, 8), 10)),
+           F.to_mont(rnd((2, 8), 11)), F.to_mont(rnd((1, 8), 12)), F.to_mont(rnd((1, 8), 13))]
+    assert np.array_equal(ctx.merkle_root(leaves, inj), oracle.merkle_root(leaves, inj))
+    assert np.array_equal(ctx.merkle_root(leaves[:1]), oracle.merkle_root(leaves[:1]))
+
+
+@pytest.mark.parametrize("logn", [1, 4, 11, 16])
+def test_fri_fold(ctx, logn):
+    layer = F.to_mont(rnd((1 << logn, 6), logn))
+    alpha = F.to_mont(rnd(6, 99))
+    assert np.array_equal(ctx.fri_fold(layer, alpha), oracle.fri_fold(layer, alpha))
+
+
+def _prove_both(ctx, n_inst, n, q, seed):
+    compiled, wit = plonk.build(n_inst, n, seed=seed)
+    mont = [F.to_mont(w) for w in wit]
+    return ctx.prove(compiled.words, mont, q), oracle.prove(compiled.words, mont, q)
+
+
+@pytest.mark.parametrize("n_inst,logn,q", [(1, 4, 1), (2, 10, 16), (4, 12, 200), (3, 13, 7)])
+def test_prove_bytes_equal_oracle(ctx, n_inst, logn, q):
+    got, want = _prove_both(ctx, n_inst, 1 << logn, q, seed=0x10AD + logn)
+    assert len(got) == len(want)
+    assert got == want
+    p = proof.decode(got)
+    assert all(v == p.final_poly[0] for v in p.final_poly)
+
+
+def test_prove_uneven_modules(ctx):
+    from loom_b200.program import Builder, Module, col, copy_constraint
+    # modules of 2^8, 2^10 and 2^11 rows in one program
+    b = Builder()
+    trace = {}
+    for i, logn in enumerate([10, 8, 11, 8]):
+        n = 1 << logn
+        m = Module(f"plonk_{i}", n)
+        L, R, O = col(f"L_{i}"), col(f"R_{i}"), col(f"O_{i}")
+        QL, QR, QM, QO, QK = (col(f"{s}_{i}") for s in ("QL", "QR", "QM", "QO", "QK"))
+        m.assert_zero(QL * L + QR * R + QM * L * R + QO * O + QK)
+        b.add_module(m)
+        w, S = plonk.instance_witness(n, 5, i)
+        trace.update(w)
+        copy_constraint(b, m.name, [L, R, O], S, f"plonk.S_{i}")
+    trace.update(b.generated)
+    compiled = b.compile()
+    mont = [F.to_mont(trace[name]) for (name, _, _) in compiled.witness_columns]
+    got = ctx.prove(compiled.words, mont, 20)
+    assert got == oracle.prove(compiled.words, mont, 20)
+
+
+def test_repeated_proves_identical(ctx):
+    compiled, wit = plonk.build(2, 1 << 9, seed=3)
+    mont = [F.to_mont(w) for w in wit]
+    a = ctx.prove(compiled.words, mont, 8)
+    b = ctx.prove(compiled.words, mont, 8)
+    assert a == b
+
+
+def test_unsupported_hash_backend(ctx):
+    compiled, wit = plonk.build(1, 1 << 4, seed=1)
+    mont = [F.to_mont(w) for w in wit]
+    for hb in ("sha256", "blake3"):
+        with pytest.raises(LoomError) as e:
+            ctx.prove(compiled.words, mont, 4, hash_backend=hb)
+        assert e.value.code == 4
+
+
+def test_malformed_program(ctx):
+    compiled, wit = plonk.build(1, 1 << 4, seed=1)
+    mont = [F.to_mont(w) for w in wit]
+    bad = compiled.words.copy()
+    bad[0] ^= 1
+    with pytest.raises(LoomError) as e:
+        ctx.prove(bad, mont, 4)
+    assert e.value.code == 1
+    with pytest.raises(LoomError):
+        ctx.prove(compiled.words[:10], mont, 4)
+    # the context stays usable after errors
+    assert ctx.prove(compiled.words, mont, 4) == oracle.prove(compiled.words, mont, 4)
