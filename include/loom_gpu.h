@@ -113,6 +113,22 @@ int lg_merkle_root(lg_ctx* ctx, const uint32_t* leaves, uint64_t n_leaves, uint3
 int lg_fri_fold(lg_ctx* ctx, const uint32_t* layer, uint64_t n, const uint32_t alpha[6], uint32_t* out,
                 int on_device);
 
+/* Measurement hooks (no counterpart in the reference, which times phases
+ * with wall-clock callbacks, prover/prover.go:99-108): CUDA events recorded
+ * on the context's stream.  lg_timer_mark records event `slot` (< 16);
+ * lg_timer_elapsed waits for `to` and returns the milliseconds between the
+ * two marks. */
+int lg_timer_mark(lg_ctx* ctx, uint32_t slot);
+int lg_timer_elapsed(lg_ctx* ctx, uint32_t from, uint32_t to, float* ms);
+/* Number of kernels this library has launched since it was loaded. */
+uint64_t lg_kernel_launches(void);
+/* Per-kernel event profiler: enable (1) clears and starts recording events
+ * around the main kernels; lg_profile_report writes a JSON object
+ * {kernel: {launches, ms, bytes, perms}} with algorithmic bytes and Poseidon2
+ * permutations per kernel. */
+int lg_profile(lg_ctx* ctx, int enable);
+int lg_profile_report(lg_ctx* ctx, char* buf, size_t* len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -17,7 +17,8 @@ LIB_PATH = os.path.join(HERE, "libloom_gpu.so")
 
 LG_OK, LG_ERR_INVALID, LG_ERR_CUDA, LG_ERR_OOM, LG_ERR_UNSUPPORTED, LG_ERR_BUFFER = range(6)
 EXPORTS = ["lg_ctx_create", "lg_ctx_destroy", "lg_last_error", "lg_prove", "lg_last_proof", "lg_commit_root",
-           "lg_rs_encode", "lg_poseidon2_permute", "lg_merkle_root", "lg_fri_fold"]
+           "lg_rs_encode", "lg_poseidon2_permute", "lg_merkle_root", "lg_fri_fold", "lg_timer_mark",
+           "lg_timer_elapsed", "lg_kernel_launches", "lg_profile", "lg_profile_report"]
 
 u32p = ctypes.POINTER(ctypes.c_uint32)
 u64p = ctypes.POINTER(ctypes.c_uint64)
@@ -54,6 +55,12 @@ def load():
         L.lg_merkle_root.argtypes = [vp, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, u64p, ctypes.c_void_p,
                                      ctypes.c_int, u32p]
         L.lg_fri_fold.argtypes = [vp, ctypes.c_void_p, ctypes.c_uint64, u32p, ctypes.c_void_p, ctypes.c_int]
+        L.lg_timer_mark.argtypes = [vp, ctypes.c_uint32]
+        L.lg_timer_elapsed.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(ctypes.c_float)]
+        L.lg_kernel_launches.argtypes = []
+        L.lg_kernel_launches.restype = ctypes.c_uint64
+        L.lg_profile.argtypes = [vp, ctypes.c_int]
+        L.lg_profile_report.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_size_t)]
         _lib = L
         return L
 
@@ -115,6 +122,32 @@ class Context:
             rc = self.L.lg_last_proof(self.h, self._proof_buf, ctypes.byref(n))
         self._check(rc)
         return bytes(memoryview(self._proof_buf)[:n.value])
+
+    # ------------------------------------------------------------------ measurement
+    def mark(self, slot: int):
+        self._check(self.L.lg_timer_mark(self.h, slot))
+
+    def elapsed_ms(self, a: int, b: int) -> float:
+        ms = ctypes.c_float()
+        self._check(self.L.lg_timer_elapsed(self.h, a, b, ctypes.byref(ms)))
+        return float(ms.value)
+
+    def kernel_launches(self) -> int:
+        return int(self.L.lg_kernel_launches())
+
+    def profile(self, enable: bool):
+        self._check(self.L.lg_profile(self.h, int(enable)))
+
+    def profile_report(self) -> dict:
+        import json
+        n = ctypes.c_size_t(1 << 16)
+        buf = ctypes.create_string_buffer(n.value)
+        rc = self.L.lg_profile_report(self.h, buf, ctypes.byref(n))
+        if rc == LG_ERR_BUFFER:
+            buf = ctypes.create_string_buffer(n.value)
+            rc = self.L.lg_profile_report(self.h, buf, ctypes.byref(n))
+        self._check(rc)
+        return json.loads(buf.value.decode())
 
     # ------------------------------------------------------------------ phase entry points
     def commit_root(self, groups: List[dict]) -> np.ndarray:

@@ -98,10 +98,12 @@ inline LdeOut lde_lanes(Ctx& c, const std::vector<const uint32_t*>& src, uint32_
   const uint32_t* tw4 = c.twiddles((int)log_n + RATE_LOG);
   size_t smem = 2 * n * 4;
   allow_smem(k_lde_ptrs, smem);
-  k_lde_ptrs<<<(unsigned)src.size(), ntt_threads((int)log_n), smem, c.stream>>>(
-      (const uint32_t* const*)ptrs->p, (int)log_n, from_coeffs ? 1 : 0, twn, tw4, inv(to_mont((uint32_t)n)),
-      r.lde->p, keep_coef ? r.coef->p : nullptr);
-  LG_LAUNCH();
+  c.timed("lde", 20.0 * n * src.size(), 0, [&] {
+    k_lde_ptrs<<<(unsigned)src.size(), ntt_threads((int)log_n), smem, c.stream>>>(
+        (const uint32_t* const*)ptrs->p, (int)log_n, from_coeffs ? 1 : 0, twn, tw4, inv(to_mont((uint32_t)n)),
+        r.lde->p, keep_coef ? r.coef->p : nullptr);
+    LG_LAUNCH();
+  });
   return r;
 }
 
@@ -124,17 +126,21 @@ inline void build_tree(Ctx& c, TreeDev& t) {
     while (next < t.inj.size() && (1u << t.inj_log_w[next]) == start) ptrs.push_back(t.inj[next++]->p);
     if (ptrs.empty()) return;
     auto tab = upload_ptrs(c, ptrs);
-    k_merkle_inject<<<(start + 127) / 128, 128, 0, c.stream>>>(t.nodes->p, start, (const uint32_t* const*)tab->p,
-                                                                (uint32_t)ptrs.size());
-    LG_LAUNCH();
+    c.timed("merkle_inject", 96.0 * start * ptrs.size(), (double)start * ptrs.size(), [&] {
+      k_merkle_inject<<<(start + 127) / 128, 128, 0, c.stream>>>(t.nodes->p, start, (const uint32_t* const*)tab->p,
+                                                                  (uint32_t)ptrs.size());
+      LG_LAUNCH();
+    });
   };
   for (size_t k = 0; k < t.inj.size(); k++)
     if (t.inj_log_w[k] > t.log_leaves || (k && t.inj_log_w[k] > t.inj_log_w[k - 1]))
       throw Error(LG_ERR_INVALID, "injection widths must not increase");
   fold(nl);
   for (uint32_t start = nl >> 1; start >= 1; start >>= 1) {
-    k_merkle_level<<<(start + 127) / 128, 128, 0, c.stream>>>(t.nodes->p, start);
-    LG_LAUNCH();
+    c.timed("merkle_level", 96.0 * start, (double)start, [&] {
+      k_merkle_level<<<(start + 127) / 128, 128, 0, c.stream>>>(t.nodes->p, start);
+      LG_LAUNCH();
+    });
     fold(start);
   }
   std::vector<const uint32_t*> ip;
@@ -157,8 +163,11 @@ inline void hash_leaves(Ctx& c, const uint32_t* lde, uint32_t nb, uint32_t ne, u
   g.ne = ne;
   g.n_leaves = (uint32_t)(rows / 2);
   g.out = out;
-  k_hash_leaves<<<(g.n_leaves + 127) / 128, 128, 0, c.stream>>>(g);
-  LG_LAUNCH();
+  uint32_t total = 3 + 2 * nb + 12 * ne;
+  c.timed("hash_leaves", 4.0 * rows * (nb + 6 * ne) + 32.0 * g.n_leaves, (double)g.n_leaves * ((total + 15) / 16), [&] {
+    k_hash_leaves<<<(g.n_leaves + 127) / 128, 128, 0, c.stream>>>(g);
+    LG_LAUNCH();
+  });
 }
 
 struct GroupSpec {

@@ -6,6 +6,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -30,7 +32,14 @@ struct Error : std::runtime_error {
       throw ::lg::Error(e_ == cudaErrorMemoryAllocation ? LG_ERR_OOM : LG_ERR_CUDA,     \
                         std::string(#x) + ": " + cudaGetErrorString(e_));                             \
   } while (0)
-#define LG_LAUNCH() LG_CK(cudaGetLastError())
+// Every kernel launch is followed by LG_LAUNCH(): it checks the launch and
+// counts it (lg_kernel_launches).
+inline std::atomic<uint64_t> g_launches{0};
+#define LG_LAUNCH()                 \
+  do {                              \
+    LG_CK(cudaGetLastError());      \
+    ::lg::g_launches.fetch_add(1);  \
+  } while (0)
 
 // Device buffer of u32 words, stream-ordered allocation.
 struct DBuf {
@@ -67,6 +76,32 @@ struct Ctx {
   uint32_t* pinned = nullptr;    // host staging
   size_t pinned_words = 0;
   int sm_count = 148;
+
+  // Timer marks (lg_timer_mark) and the optional per-kernel event profiler:
+  // events recorded on this context's stream around selected launches, with
+  // the algorithmic bytes and Poseidon2 permutations of each launch.
+  cudaEvent_t marks[16] = {};
+  struct KRec { const char* name; cudaEvent_t a, b; double bytes, perms; };
+  bool profiling = false;
+  std::vector<KRec> recs;
+  std::vector<cudaEvent_t> event_pool;
+  size_t event_next = 0;
+  cudaEvent_t pooled_event() {
+    if (event_next == event_pool.size()) {
+      cudaEvent_t e;
+      LG_CK(cudaEventCreate(&e));
+      event_pool.push_back(e);
+    }
+    return event_pool[event_next++];
+  }
+  template <class F> void timed(const char* name, double bytes, double perms, F launch) {
+    if (!profiling) { launch(); return; }
+    KRec r{name, pooled_event(), pooled_event(), bytes, perms};
+    LG_CK(cudaEventRecord(r.a, stream));
+    launch();
+    LG_CK(cudaEventRecord(r.b, stream));
+    recs.push_back(r);
+  }
 
   const uint32_t* twiddles(int logn) {
     auto it = tw.find(logn);

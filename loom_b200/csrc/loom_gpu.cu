@@ -234,4 +234,65 @@ int lg_fri_fold(lg_ctx* ctx, const uint32_t* layer, uint64_t n, const uint32_t a
   });
 }
 
+int lg_timer_mark(lg_ctx* ctx, uint32_t slot) {
+  return guarded(ctx, [&] {
+    if (slot >= 16) throw Error(LG_ERR_INVALID, "timer slot must be < 16");
+    if (!ctx->c.marks[slot]) LG_CK(cudaEventCreate(&ctx->c.marks[slot]));
+    LG_CK(cudaEventRecord(ctx->c.marks[slot], ctx->c.stream));
+  });
+}
+
+int lg_timer_elapsed(lg_ctx* ctx, uint32_t from, uint32_t to, float* ms) {
+  return guarded(ctx, [&] {
+    if (from >= 16 || to >= 16 || !ctx->c.marks[from] || !ctx->c.marks[to] || !ms)
+      throw Error(LG_ERR_INVALID, "timer slots not recorded");
+    LG_CK(cudaEventSynchronize(ctx->c.marks[to]));
+    LG_CK(cudaEventElapsedTime(ms, ctx->c.marks[from], ctx->c.marks[to]));
+  });
+}
+
+uint64_t lg_kernel_launches(void) { return g_launches.load(); }
+
+int lg_profile(lg_ctx* ctx, int enable) {
+  return guarded(ctx, [&] {
+    LG_CK(cudaStreamSynchronize(ctx->c.stream));
+    ctx->c.profiling = enable != 0;
+    ctx->c.recs.clear();
+    ctx->c.event_next = 0;
+  });
+}
+
+int lg_profile_report(lg_ctx* ctx, char* buf, size_t* len) {
+  return guarded(ctx, [&] {
+    if (!len) throw Error(LG_ERR_INVALID, "null length");
+    LG_CK(cudaStreamSynchronize(ctx->c.stream));
+    struct Acc { uint64_t n = 0; double ms = 0, bytes = 0, perms = 0; };
+    std::map<std::string, Acc> acc;
+    for (auto& r : ctx->c.recs) {
+      float ms = 0;
+      LG_CK(cudaEventElapsedTime(&ms, r.a, r.b));
+      Acc& a = acc[r.name];
+      a.n++;
+      a.ms += ms;
+      a.bytes += r.bytes;
+      a.perms += r.perms;
+    }
+    std::string js = "{";
+    for (auto& kv : acc) {
+      char tmp[256];
+      snprintf(tmp, sizeof tmp, "%s\"%s\": {\"launches\": %llu, \"ms\": %.6f, \"bytes\": %.0f, \"perms\": %.0f}",
+               js.size() > 1 ? ", " : "", kv.first.c_str(), (unsigned long long)kv.second.n, kv.second.ms,
+               kv.second.bytes, kv.second.perms);
+      js += tmp;
+    }
+    js += "}";
+    if (!buf || *len < js.size() + 1) {
+      *len = js.size() + 1;
+      throw Error(LG_ERR_BUFFER, "report buffer too small");
+    }
+    memcpy(buf, js.c_str(), js.size() + 1);
+    *len = js.size() + 1;
+  });
+}
+
 }  // extern "C"

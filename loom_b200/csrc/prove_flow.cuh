@@ -187,8 +187,12 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
     jb.tw = c.twiddles(jb.logn4);
     deep[ci] = std::make_shared<DBuf>(6 * big, c.stream);
     jb.out = deep[ci]->p;
-    k_deep<<<(unsigned)((big + 127) / 128), 128, 0, c.stream>>>(jb);
-    LG_LAUNCH();
+    double row_bytes = 24.0;
+    for (auto& bu : bundles) row_bytes += bu.ext ? 24.0 : 4.0;
+    c.timed("deep", row_bytes * big, 0, [&] {
+      k_deep<<<(unsigned)((big + 127) / 128), 128, 0, c.stream>>>(jb);
+      LG_LAUNCH();
+    });
   }
 
   // ---- FRI (internal/fri/fri.go:352-365,606-736)
@@ -258,8 +262,11 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
     E6 a = digest_e6(fs.compute(nm));
     if (j > r0) fri_roots.push_back(root);
     auto next = std::make_shared<DBuf>(3 * nj, c.stream);
-    k_fold<<<(unsigned)((nj / 2 + 255) / 256), 256, 0, c.stream>>>(running->p, nj, a, c.twiddles(LOG_N_FRI - j), inv2, next->p);
-    LG_LAUNCH();
+    const uint32_t* twj = c.twiddles(LOG_N_FRI - j);
+    c.timed("fri_fold", 36.0 * nj, 0, [&] {
+      k_fold<<<(unsigned)((nj / 2 + 255) / 256), 256, 0, c.stream>>>(running->p, nj, a, twj, inv2, next->p);
+      LG_LAUNCH();
+    });
     running = next;
     nj /= 2;
   }

@@ -384,9 +384,12 @@ struct Prover {
     auto cv = std::make_shared<DBuf>(coef_lanes.size() * big, c.stream);
     dim3 grid((unsigned)coef_lanes.size(), 4);
     allow_smem(k_coset_eval_ptrs, n * 4);
-    k_coset_eval_ptrs<<<grid, ntt_threads((int)logn), n * 4, c.stream>>>((const uint32_t* const*)tab->p, (int)logn, twn, tw4,
-                                                                         c.gpowers((int)logn, false), cv->p);
-    LG_LAUNCH();
+    const uint32_t* gp = c.gpowers((int)logn, false);
+    c.timed("coset_eval", 20.0 * n * coef_lanes.size(), 0, [&] {
+      k_coset_eval_ptrs<<<grid, ntt_threads((int)logn), n * 4, c.stream>>>((const uint32_t* const*)tab->p, (int)logn, twn,
+                                                                           tw4, gp, cv->p);
+      LG_LAUNCH();
+    });
     // 1 / (s_c^n - 1), s_c = g w_4n^c (internal/poly/compute_quotient.go:400-421)
     uint32_t zinv[4];
     uint32_t g = to_mont(3), w4n = root_of_unity_mont((int)logn + RATE_LOG);
@@ -403,9 +406,11 @@ struct Prover {
     const int T = 128;
     size_t smem = (size_t)std::max(xc.n_regs, 1u) * 6 * T * 4;
     LG_CK(cudaFuncSetAttribute(k_quotient_eval, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_quotient_eval<<<dim3((unsigned)((n + T - 1) / T), 4), T, smem, c.stream>>>(xp, (const E6*)coins_d->p, cv->p,
-                                                                                 (int)logn, zinv_d->p, qv->p);
-    LG_LAUNCH();
+    c.timed("quotient_eval", 4.0 * big * coef_lanes.size() + 24.0 * big, 0, [&] {
+      k_quotient_eval<<<dim3((unsigned)((n + T - 1) / T), 4), T, smem, c.stream>>>(xp, (const E6*)coins_d->p, cv->p,
+                                                                                   (int)logn, zinv_d->p, qv->p);
+      LG_LAUNCH();
+    });
     // coset values -> per-coset coefficients -> chunk coefficients
     allow_smem(k_intt_inplace, n * 4);
     k_intt_inplace<<<(unsigned)(lw * 4), ntt_threads((int)logn), n * 4, c.stream>>>(qv->p, n, (int)logn, twn,
