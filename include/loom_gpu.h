@@ -113,6 +113,12 @@ int lg_merkle_root(lg_ctx* ctx, const uint32_t* leaves, uint64_t n_leaves, uint3
 int lg_fri_fold(lg_ctx* ctx, const uint32_t* layer, uint64_t n, const uint32_t alpha[6], uint32_t* out,
                 int on_device);
 
+/* Grand product of a prover step: out[0] = 1, out[i] = prod_{k<i} num[k]/den[k]
+ * over n E6 rows (6 words each, ext.E6 layout) — the accumulation of
+ * poly.BuildGrandProductMixed (internal/poly/iop_utils.go:170-192,316-323)
+ * after its numerator and denominator expressions are evaluated. */
+int lg_grand_product(lg_ctx* ctx, const uint32_t* num, const uint32_t* den, uint64_t n, uint32_t* out, int on_device);
+
 /* Measurement hooks (no counterpart in the reference, which times phases
  * with wall-clock callbacks, prover/prover.go:99-108): CUDA events recorded
  * on the context's stream.  lg_timer_mark records event `slot` (< 16);

@@ -18,7 +18,7 @@ LIB_PATH = os.path.join(HERE, "libloom_gpu.so")
 LG_OK, LG_ERR_INVALID, LG_ERR_CUDA, LG_ERR_OOM, LG_ERR_UNSUPPORTED, LG_ERR_BUFFER = range(6)
 EXPORTS = ["lg_ctx_create", "lg_ctx_destroy", "lg_last_error", "lg_prove", "lg_last_proof", "lg_commit_root",
            "lg_rs_encode", "lg_poseidon2_permute", "lg_merkle_root", "lg_fri_fold", "lg_timer_mark",
-           "lg_timer_elapsed", "lg_kernel_launches", "lg_profile", "lg_profile_report"]
+           "lg_timer_elapsed", "lg_kernel_launches", "lg_profile", "lg_profile_report", "lg_grand_product"]
 
 u32p = ctypes.POINTER(ctypes.c_uint32)
 u64p = ctypes.POINTER(ctypes.c_uint64)
@@ -55,6 +55,7 @@ def load():
         L.lg_merkle_root.argtypes = [vp, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, u64p, ctypes.c_void_p,
                                      ctypes.c_int, u32p]
         L.lg_fri_fold.argtypes = [vp, ctypes.c_void_p, ctypes.c_uint64, u32p, ctypes.c_void_p, ctypes.c_int]
+        L.lg_grand_product.argtypes = [vp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_int]
         L.lg_timer_mark.argtypes = [vp, ctypes.c_uint32]
         L.lg_timer_elapsed.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(ctypes.c_float)]
         L.lg_kernel_launches.argtypes = []
@@ -184,6 +185,12 @@ class Context:
         self._check(self.L.lg_merkle_root(self.h, _ptr(lv), lv.shape[0], len(injections), widths.ctypes.data_as(u64p),
                                           _ptr(inj), 0, root.ctypes.data_as(u32p)))
         return root
+
+    def grand_product(self, num: np.ndarray, den: np.ndarray) -> np.ndarray:
+        a, b = _u32(num).reshape(-1, 6), _u32(den).reshape(-1, 6)
+        out = np.zeros_like(a)
+        self._check(self.L.lg_grand_product(self.h, _ptr(a), _ptr(b), a.shape[0], _ptr(out), 0))
+        return out
 
     def fri_fold(self, layer: np.ndarray, alpha) -> np.ndarray:
         x = _u32(layer).reshape(-1, 6)

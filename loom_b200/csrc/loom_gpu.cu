@@ -25,6 +25,13 @@ __global__ void k_soa_to_aos(const uint32_t* in, uint64_t n, uint32_t lanes, uin
   out[i] = in[w * n + row];
 }
 
+__global__ void k_e6_div_soa(const uint32_t* num, const uint32_t* den, uint64_t n, uint32_t* out) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  E6 a = ld6(num, n, i), b = ld6(den, n, i);
+  st6(out, n, i, e6_mul(a, e6_inv(b)));
+}
+
 template <class F> int guarded(lg_ctx* ctx, F f) {
   if (!ctx) return LG_ERR_INVALID;
   try {
@@ -231,6 +238,36 @@ int lg_fri_fold(lg_ctx* ctx, const uint32_t* layer, uint64_t n, const uint32_t a
     k_soa_to_aos<<<(unsigned)((3 * n + 255) / 256), 256, 0, c.stream>>>(nx->p, n / 2, 6, aos->p);
     LG_LAUNCH();
     from_device(c, out, aos->p, 3 * n, on_device);
+  });
+}
+
+int lg_grand_product(lg_ctx* ctx, const uint32_t* num, const uint32_t* den, uint64_t n, uint32_t* out, int on_device) {
+  return guarded(ctx, [&] {
+    Ctx& c = ctx->c;
+    if (!num || !den || !out || n == 0) throw Error(LG_ERR_INVALID, "bad arguments");
+    auto na = to_device(c, num, 6 * n, on_device), da = to_device(c, den, 6 * n, on_device);
+    auto ns = std::make_shared<DBuf>(6 * n, c.stream), ds = std::make_shared<DBuf>(6 * n, c.stream);
+    unsigned g6 = (unsigned)((6 * n + 255) / 256), g1 = (unsigned)((n + 255) / 256);
+    k_aos_to_soa<<<g6, 256, 0, c.stream>>>(na->p, n, 6, ns->p);
+    LG_LAUNCH();
+    k_aos_to_soa<<<g6, 256, 0, c.stream>>>(da->p, n, 6, ds->p);
+    LG_LAUNCH();
+    auto ratio = std::make_shared<DBuf>(6 * n, c.stream);
+    k_e6_div_soa<<<g1, 256, 0, c.stream>>>(ns->p, ds->p, n, ratio->p);
+    LG_LAUNCH();
+    uint32_t nt = (uint32_t)((n + SCAN_TILE - 1) / SCAN_TILE);
+    auto totals = std::make_shared<DBuf>(6 * (size_t)nt, c.stream), pre = std::make_shared<DBuf>(6 * (size_t)nt, c.stream);
+    k_scan_tiles<<<nt, SCAN_BLOCK, 0, c.stream>>>(ratio->p, n, totals->p);
+    LG_LAUNCH();
+    k_tile_prefix<<<1, 1, 0, c.stream>>>(totals->p, nt, pre->p);
+    LG_LAUNCH();
+    auto res = std::make_shared<DBuf>(6 * n, c.stream);
+    k_gp_finish<<<g1, 256, 0, c.stream>>>(ratio->p, n, pre->p, res->p);
+    LG_LAUNCH();
+    auto aos = std::make_shared<DBuf>(6 * n, c.stream);
+    k_soa_to_aos<<<g6, 256, 0, c.stream>>>(res->p, n, 6, aos->p);
+    LG_LAUNCH();
+    from_device(c, out, aos->p, 6 * n, on_device);
   });
 }
 

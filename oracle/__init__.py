@@ -177,3 +177,12 @@ def fri_fold(layer_mont, alpha_mont) -> np.ndarray:
     out = np.zeros(x.size // 2, dtype=np.uint32)
     L.oracle_fri_fold(_p(x), x.size // 6, _p(a), _p(out))
     return out.reshape(-1, 6)
+
+
+def grand_product(num_mont, den_mont) -> np.ndarray:
+    L = lib()
+    L.oracle_grand_product.argtypes = [u32p, u32p, ctypes.c_size_t, u32p]
+    a, b = _u32(num_mont).reshape(-1), _u32(den_mont).reshape(-1)
+    out = np.zeros_like(a)
+    L.oracle_grand_product(_p(a), _p(b), a.size // 6, _p(out))
+    return out.reshape(-1, 6)

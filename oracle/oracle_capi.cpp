@@ -197,3 +197,17 @@ void oracle_fri_fold(const uint32_t* layer, size_t n, const uint32_t* alpha, uin
   }
 }
 }
+
+extern "C" {
+// R[0] = 1, R[i] = prod_{k<i} num[k]/den[k] over E6 rows, Montgomery in/out
+// (internal/poly/iop_utils.go:170-192,316-323).
+void oracle_grand_product(const uint32_t* num, const uint32_t* den, size_t n, uint32_t* out) {
+  E6 acc = e6_one();
+  for (size_t i = 0; i < n; i++) {
+    for (int k = 0; k < 6; k++) out[6 * i + k] = to_mont(acc.c[k]);
+    E6 a, b;
+    for (int k = 0; k < 6; k++) { a.c[k] = from_mont(num[6 * i + k]); b.c[k] = from_mont(den[6 * i + k]); }
+    acc = e6_mul(acc, e6_mul(a, e6_inv(b)));
+  }
+}
+}

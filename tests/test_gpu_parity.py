@@ -138,3 +138,10 @@ def test_malformed_program(ctx):
         ctx.prove(compiled.words[:10], mont, 4)
     # the context stays usable after errors
     assert ctx.prove(compiled.words, mont, 4) == oracle.prove(compiled.words, mont, 4)
+
+
+@pytest.mark.parametrize("n", [1, 2, 7, 2048, 2049, 5000, 1 << 14])
+def test_grand_product(ctx, n):
+    num = F.to_mont(rnd((n, 6), n))
+    den = F.to_mont(rnd((n, 6), n + 1))
+    assert np.array_equal(ctx.grand_product(num, den), oracle.grand_product(num, den))
