@@ -119,6 +119,20 @@ int lg_fri_fold(lg_ctx* ctx, const uint32_t* layer, uint64_t n, const uint32_t a
  * after its numerator and denominator expressions are evaluated. */
 int lg_grand_product(lg_ctx* ctx, const uint32_t* num, const uint32_t* den, uint64_t n, uint32_t* out, int on_device);
 
+/* Allocation-free grand product.  No counterpart in the reference: it is for
+ * callers that cannot call cudaMalloc (a framework's caching allocator owns
+ * the device memory, a memory-capped sandbox, a request path that must not
+ * allocate).  Same result as lg_grand_product; num, den and out are DEVICE
+ * pointers on the current device (n E6 rows, 6 words each), launched on
+ * `cuda_stream` (a cudaStream_t; NULL = default stream) and not waited for.
+ * Its only scratch is a fixed 96 KiB device array inside this library, held
+ * by every GPU that loads it until the process exits: n above 2^22 rows
+ * returns LG_ERR_UNSUPPORTED.  The first call on a device looks up that
+ * array's address (make it before any stream capture); calls whose work
+ * overlaps on the GPU share the array and race, so serialize them.  It calls
+ * no cudaMalloc, cudaFree or other allocating routine. */
+int lg_grand_product_noalloc(const uint32_t* num, const uint32_t* den, uint64_t n, uint32_t* out, void* cuda_stream);
+
 /* Measurement hooks (no counterpart in the reference, which times phases
  * with wall-clock callbacks, prover/prover.go:99-108): CUDA events recorded
  * on the context's stream.  lg_timer_mark records event `slot` (< 16);

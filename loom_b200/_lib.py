@@ -18,7 +18,7 @@ LIB_PATH = os.path.join(HERE, "libloom_gpu.so")
 LG_OK, LG_ERR_INVALID, LG_ERR_CUDA, LG_ERR_OOM, LG_ERR_UNSUPPORTED, LG_ERR_BUFFER = range(6)
 EXPORTS = ["lg_ctx_create", "lg_ctx_destroy", "lg_last_error", "lg_prove", "lg_last_proof", "lg_commit_root",
            "lg_rs_encode", "lg_poseidon2_permute", "lg_merkle_root", "lg_fri_fold", "lg_timer_mark",
-           "lg_timer_elapsed", "lg_kernel_launches", "lg_profile", "lg_profile_report", "lg_grand_product"]
+           "lg_timer_elapsed", "lg_kernel_launches", "lg_profile", "lg_profile_report", "lg_grand_product", "lg_grand_product_noalloc"]
 
 u32p = ctypes.POINTER(ctypes.c_uint32)
 u64p = ctypes.POINTER(ctypes.c_uint64)
@@ -56,6 +56,8 @@ def load():
                                      ctypes.c_int, u32p]
         L.lg_fri_fold.argtypes = [vp, ctypes.c_void_p, ctypes.c_uint64, u32p, ctypes.c_void_p, ctypes.c_int]
         L.lg_grand_product.argtypes = [vp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_int]
+        L.lg_grand_product_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                               ctypes.c_void_p]
         L.lg_timer_mark.argtypes = [vp, ctypes.c_uint32]
         L.lg_timer_elapsed.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(ctypes.c_float)]
         L.lg_kernel_launches.argtypes = []

@@ -6,7 +6,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = os.path.join(HERE, "csrc", "loom_gpu.cu")
+SRC = [os.path.join(HERE, "csrc", "loom_gpu.cu"), os.path.join(HERE, "csrc", "gp_noalloc.cu")]
 OUT = os.path.join(HERE, "libloom_gpu.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
@@ -29,7 +29,7 @@ def up_to_date() -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return OUT
-    cmd = [NVCC] + FLAGS + ["-o", OUT, SRC]
+    cmd = [NVCC] + FLAGS + ["-o", OUT] + SRC
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     subprocess.run(cmd, check=True)
