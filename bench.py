@@ -213,9 +213,22 @@ def main():
         pbh = ctx.prove(comp.words, host_cols, a.queries, on_device=False)
         ctx.mark(3)
         e2e_times.append(ctx.elapsed_ms(2, 3))
+    # ---- timed: the plain per-kernel prover (one launch per group / module)
+    ctx.set_batched(False)
+    ctx.prove(comp.words, dev_ptrs, a.queries, on_device=True)
+    plain_times = []
+    for _ in range(a.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        ctx.mark(4)
+        pbp = ctx.prove(comp.words, dev_ptrs, a.queries, on_device=True)
+        ctx.mark(5)
+        plain_times.append(ctx.elapsed_ms(4, 5))
+    ctx.set_batched(True)
     clk = clocks.stop()
     barrier()
     assert pbh == pb, "host-buffer and device-buffer proofs differ"
+    assert pbp == pb, "plain and batched proofs differ"
 
     # ---- per-kernel events over a profiled step (roofline of the dominant kernel)
     flush.fill_(1)
@@ -227,10 +240,11 @@ def main():
 
     ms = statistics.mean(times)
     e2e_ms = statistics.mean(e2e_times)
+    plain_ms = statistics.mean(plain_times)
     if dist is not None:
-        t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device=f"cuda:{device}")
+        t = torch.tensor([ms, e2e_ms, plain_ms], dtype=torch.float64, device=f"cuda:{device}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_ms = float(t[0]), float(t[1])
+        ms, e2e_ms, plain_ms = float(t[0]), float(t[1]), float(t[2])
 
     if rank == 0:
         peaks = {}
@@ -289,9 +303,12 @@ def main():
             "warmup": max(a.warmup, 3), "ms_per_step": round(ms, 3), "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded plonk-like witnesses)",
             "config": {"workload": workload_name(a), "instances": a.instances, "log_rows": a.log_n,
-                       "queries": a.queries, "mode": "plain", "parallelism": f"replicas x{world}",
+                       "queries": a.queries, "mode": "batched", "parallelism": f"replicas x{world}",
                        "l2": "flushed between steps (256 MB write)"},
             "proofs_per_s": round(world * 1e3 / ms, 3),
+            "plain": {"value": round(plain_ms, 3), "unit": "ms",
+                      "note": "same kernels, one launch per group / module (the plain per-kernel prover)"},
+            "batched_speedup_vs_plain": round(plain_ms / ms, 3),
             "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": h2d_bytes,
                     "d2h_bytes_per_step": len(pbh)},
             "gpu_launches": int(launches),

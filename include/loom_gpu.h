@@ -67,6 +67,11 @@ typedef struct lg_ctx lg_ctx;
  * state; the cgo shim creates one context per GPU. */
 int lg_ctx_create(int device, lg_ctx** out);
 void lg_ctx_destroy(lg_ctx* ctx);
+/* Launch partitioning of every phase: batched (1, the default) launches each
+ * kernel once over all groups / modules of a size class; plain (0) launches
+ * it once per group / module, like a per-column prover.  Both produce the
+ * same proof bytes. */
+int lg_ctx_set_batched(lg_ctx* ctx, int batched);
 /* NUL-terminated description of the last failure on `ctx` (never NULL). */
 const char* lg_last_error(lg_ctx* ctx);
 

@@ -140,9 +140,33 @@ struct Ctx {
     LG_CK(cudaMemcpyAsync(host, dev, words * 4, cudaMemcpyDeviceToHost, stream));
     LG_CK(cudaStreamSynchronize(stream));
   }
+  // Small uploads (pointer tables, job descriptors, bytecode) go through a
+  // pinned arena so the copy is asynchronous and the host can run ahead of
+  // the device.  The arena restarts when the stream is idle (arena_reset at
+  // the start of every call) or, when full, after a stream synchronize.
+  uint8_t* arena = nullptr;
+  size_t arena_cap = 0, arena_off = 0;
+  void arena_reset() { arena_off = 0; }
   void h2d(uint32_t* dev, const void* host, size_t bytes) {
-    LG_CK(cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, stream));
+    size_t need = (bytes + 255) & ~(size_t)255;
+    if (arena_off + need > arena_cap) {
+      LG_CK(cudaStreamSynchronize(stream));
+      if (need > arena_cap) {
+        if (arena) cudaFreeHost(arena);
+        arena = nullptr;
+        arena_cap = std::max(need, (size_t)64 << 20);
+        LG_CK(cudaMallocHost((void**)&arena, arena_cap));
+      }
+      arena_off = 0;
+    }
+    uint8_t* p = arena + arena_off;
+    memcpy(p, host, bytes);
+    arena_off += need;
+    LG_CK(cudaMemcpyAsync(dev, p, bytes, cudaMemcpyHostToDevice, stream));
   }
+  // One launch per phase over all groups / modules of a size (true), or one
+  // launch per group / module (false, the plain per-kernel prover).
+  bool batched = true;
 };
 
 // ---------------------------------------------------------------- program

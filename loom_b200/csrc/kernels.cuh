@@ -62,15 +62,68 @@ __device__ void smem_dif(uint32_t* A, int logn, const uint32_t* tw, bool inverse
 }
 
 // Inverse transform of natural-order values to natural-order coefficients
-// (scaled by 1/n), in place per lane.
-__global__ void k_intt_inplace(uint32_t* data, uint64_t lane_stride, int logn, const uint32_t* tw_n, uint32_t n_inv) {
+// (scaled by 1/n), in place; one block per lane, lanes[blockIdx.x].
+__global__ void k_intt(uint32_t* const* lanes, int logn, const uint32_t* tw_n, uint32_t n_inv) {
   extern __shared__ uint32_t sm[];
   const uint32_t n = 1u << logn;
-  uint32_t* d = data + blockIdx.x * lane_stride;
+  uint32_t* d = lanes[blockIdx.x];
   for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) sm[bitrev32(k, logn)] = d[k];
   __syncthreads();
   smem_dit(sm, logn, tw_n, true);
   for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) d[k] = mul(sm[k], n_inv);
+}
+
+// LDE of one lane per block: Lagrange values in natural order (or canonical
+// coefficients when from_coeffs) -> for coset a < 4,
+// out[a n + b] = P(w_4n^bitrev2(a) w_n^bitrev(b)), the bit-reversed
+// evaluations on <w_4n> of reedsolomon.Encode (internal/reedsolomon/rs.go:52-70).
+// Optionally writes the coefficients.
+struct LdeLane { const uint32_t* src; uint32_t* out; uint32_t* coef; };
+__global__ void k_lde(const LdeLane* lanes, int logn, int from_coeffs, const uint32_t* tw_n, const uint32_t* tw_4n,
+                      uint32_t n_inv) {
+  extern __shared__ uint32_t sm[];
+  const uint32_t n = 1u << logn;
+  uint32_t* A = sm;
+  uint32_t* B = sm + n;
+  const LdeLane L = lanes[blockIdx.x];
+  if (from_coeffs) {
+    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) A[k] = L.src[k];
+    __syncthreads();
+  } else {
+    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) A[bitrev32(k, logn)] = L.src[k];
+    __syncthreads();
+    smem_dit(A, logn, tw_n, true);
+    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) A[k] = mul(A[k], n_inv);
+    __syncthreads();
+  }
+  if (L.coef)
+    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) L.coef[k] = A[k];
+  const uint32_t big = n << RATE_LOG;
+  for (int a = 0; a < (1 << RATE_LOG); a++) {
+    const uint32_t e = bitrev32((uint32_t)a, RATE_LOG);
+    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) B[k] = mul(A[k], __ldg(tw_4n + ((e * k) & (big - 1))));
+    __syncthreads();
+    smem_dif(B, logn, tw_n, false);
+    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) L.out[(uint64_t)a * n + k] = B[k];
+    __syncthreads();
+  }
+}
+
+// Evaluations of a coefficient lane on the cosets s_c <w_n>, s_c = g w_4n^c,
+// c = blockIdx.y < 4, in natural order: out[c n + j] = P(s_c w_n^j).
+struct CosetLane { const uint32_t* src; uint32_t* out; };
+__global__ void k_coset_eval(const CosetLane* lanes, int logn, const uint32_t* tw_n, const uint32_t* tw_4n,
+                             const uint32_t* gpow) {
+  extern __shared__ uint32_t sm[];
+  const uint32_t n = 1u << logn, c = blockIdx.y;
+  const CosetLane L = lanes[blockIdx.x];
+  const uint32_t big = n << RATE_LOG;
+  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x)
+    sm[k] = mul(mul(L.src[k], __ldg(gpow + k)), __ldg(tw_4n + ((c * k) & (big - 1))));
+  __syncthreads();
+  smem_dif(sm, logn, tw_n, false);
+  uint32_t* o = L.out + (uint64_t)c * n;
+  for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) o[j] = sm[bitrev32(j, logn)];
 }
 
 // ---------------------------------------------------------------- leaves
@@ -103,7 +156,8 @@ __device__ __forceinline__ uint32_t leaf_elem(const LeafGroup& g, uint32_t idx, 
   return g.ext[e * g.stride + 2 * k + h];
 }
 
-__global__ void k_hash_leaves(LeafGroup g) {
+__global__ void k_hash_leaves(const LeafGroup* groups) {
+  const LeafGroup g = groups[blockIdx.y];
   uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= g.n_leaves) return;
   const uint32_t total = 3 + 2 * g.nb + 12 * g.ne;
@@ -155,6 +209,44 @@ __global__ void k_merkle_inject(uint32_t* nodes, uint32_t start, const uint32_t*
   }
 #pragma unroll
   for (int q = 0; q < 8; q++) nodes[id * 8 + q] = cur[q];
+}
+
+// Upper tree levels in one block: for start, start/2, ..., 1: the 2-to-1
+// step, then the injections of that width in schedule order.  When
+// fold_first, the injections of width `start` fold first (a tree whose leaf
+// level fits in one block).
+struct InjRef { const uint32_t* leaves; uint32_t width; };
+__global__ void k_merkle_tail(uint32_t* nodes, uint32_t start, int fold_first, const InjRef* inj, uint32_t n_inj) {
+  const uint32_t tag = to_mont(NODE_TAG);
+  auto fold = [&](uint32_t w) {
+    for (uint32_t j = threadIdx.x; j < w; j += blockDim.x) {
+      uint64_t id = w + j;
+      uint32_t cur[8], r[8];
+      for (int q = 0; q < 8; q++) cur[q] = nodes[id * 8 + q];
+      bool any = false;
+      for (uint32_t t = 0; t < n_inj; t++) {
+        if (inj[t].width != w) continue;
+        for (int q = 0; q < 8; q++) r[q] = inj[t].leaves[(uint64_t)j * 8 + q];
+        p2_compress(tag, cur, r, cur);
+        any = true;
+      }
+      if (any)
+        for (int q = 0; q < 8; q++) nodes[id * 8 + q] = cur[q];
+    }
+    __syncthreads();
+  };
+  if (fold_first) fold(start);
+  for (uint32_t w = start >> 1; w >= 1; w >>= 1) {
+    for (uint32_t i = threadIdx.x; i < w; i += blockDim.x) {
+      uint64_t id = w + i;
+      uint32_t l[8], r[8], o[8];
+      for (int q = 0; q < 8; q++) { l[q] = nodes[2 * id * 8 + q]; r[q] = nodes[(2 * id + 1) * 8 + q]; }
+      p2_compress(tag, l, r, o);
+      for (int q = 0; q < 8; q++) nodes[id * 8 + q] = o[q];
+    }
+    __syncthreads();
+    fold(w);
+  }
 }
 
 // Permutation test hook: one state of 24 words per thread.
@@ -260,69 +352,73 @@ __device__ __forceinline__ E6 x_eval(const XProgram& p, const E6* coins, uint32_
   return r;
 }
 
-// Quotient numerator on coset c, row j: V(...) / (s_c^n - 1), written as 6
-// lanes qv[w][c n + j] (lane stride 4n).  cv: coset values, lane l coset c at
-// cv[l * 4n + c n + j].
-__global__ void k_quotient_eval(XProgram p, const E6* coins, const uint32_t* cv, int logn, const uint32_t* zinv,
-                                uint32_t* qv) {
+// Quotient numerator of one module on coset c = blockIdx.y, row j:
+// V(...) / (s_c^n - 1), written as qv[w * 4n + c n + j].  cv: coset values,
+// lane l coset c at cv[l * 4n + c n + j].  One job per module (blockIdx.z).
+struct QJob { XProgram p; const uint32_t* cv; uint32_t* qv; int logn; uint32_t zinv[4]; };
+__global__ void k_quotient_eval(const QJob* jobs, const E6* coins) {
   extern __shared__ uint32_t regs[];
-  const uint32_t n = 1u << logn;
+  const QJob& J = jobs[blockIdx.z];
+  const uint32_t n = 1u << J.logn;
   const uint32_t c = blockIdx.y;
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
   const uint64_t big = (uint64_t)n << RATE_LOG;
+  const uint32_t* cv = J.cv;
   auto lane = [&](uint32_t l, uint32_t row) -> uint32_t { return cv[l * big + (uint64_t)c * n + row]; };
-  E6 v = x_eval(p, coins, regs + threadIdx.x, blockDim.x, j, n, lane);
-  v = e6_mul_base(v, zinv[c]);
-  for (int w = 0; w < 6; w++) qv[w * big + (uint64_t)c * n + j] = v.c[w];
+  E6 v = x_eval(J.p, coins, regs + threadIdx.x, blockDim.x, j, n, lane);
+  v = e6_mul_base(v, J.zinv[c]);
+  uint32_t lw = J.p.result_ext ? 6 : 1;
+  for (uint32_t w = 0; w < lw; w++) J.qv[w * big + (uint64_t)c * n + j] = v.c[w];
 }
 
 // Quotient chunk coefficients from the inverse-transformed coset values.
-// After k_intt_inplace, r[w][c n + k] holds [Y^k] R_c(Y) where
-// R_c(Y) = sum_d s_c^(dn) q_d(s_c Y).  With t_c = r_c[k] s_c^-k,
-// u_d = g^(dn) q_(d,k) = 1/4 sum_c t_c w_4^(-cd).
-// out: chunk d, lane w at out[(d * 6 + w) * n + k].
-__global__ void k_quotient_chunks(const uint32_t* r, int logn, const uint32_t* ginv_pow, const uint32_t* tw_4n,
-                                  uint32_t* out, uint32_t quarter, uint32_t gn_inv, int lanes) {
-  const uint32_t n = 1u << logn;
+// r[w][c n + k] holds [Y^k] R_c(Y), R_c(Y) = sum_d s_c^(dn) q_d(s_c Y).
+// With t_c = r_c[k] s_c^-k, u_d = g^(dn) q_(d,k) = 1/4 sum_c t_c w_4^(-cd).
+// out: chunk d, lane w at out[(d * lanes + w) * n + k].  One job per module.
+struct QcJob { const uint32_t* r; uint32_t* out; int logn; uint32_t lanes; const uint32_t* ginv_pow; const uint32_t* tw_4n; uint32_t gn_inv; };
+__global__ void k_quotient_chunks(const QcJob* jobs, uint32_t quarter) {
+  const QcJob& J = jobs[blockIdx.z];
+  const uint32_t n = 1u << J.logn;
   const uint64_t big = (uint64_t)n << RATE_LOG;
   uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t w = blockIdx.y;
-  if (k >= n || (int)w >= lanes) return;
+  if (k >= n || w >= J.lanes) return;
   uint32_t t[4];
-  const uint32_t gk = ginv_pow[k];
+  const uint32_t gk = J.ginv_pow[k];
   for (int c = 0; c < 4; c++) {
-    // s_c^-k = g^-k w_4n^-(c k)
-    uint32_t e = (uint32_t)((big - ((uint64_t)c * k) % big) % big);
-    t[c] = mul(mul(r[w * big + (uint64_t)c * n + k], gk), __ldg(tw_4n + e));
+    uint32_t e = (uint32_t)((big - ((uint64_t)c * k) % big) % big);  // s_c^-k = g^-k w_4n^-(c k)
+    t[c] = mul(mul(J.r[w * big + (uint64_t)c * n + k], gk), __ldg(J.tw_4n + e));
   }
-  // inverse 4-point DFT: u_d = 1/4 sum_c t_c w4^(-c d); w4^-1 = tw_4n[3n]
-  const uint32_t w4i = __ldg(tw_4n + 3 * n), w4i2 = mul(w4i, w4i), w4i3 = mul(w4i2, w4i);
+  const uint32_t w4i = __ldg(J.tw_4n + 3 * n), w4i2 = mul(w4i, w4i), w4i3 = mul(w4i2, w4i);
   uint32_t u[4];
   u[0] = add(add(t[0], t[1]), add(t[2], t[3]));
   u[1] = add(add(t[0], mul(t[1], w4i)), add(mul(t[2], w4i2), mul(t[3], w4i3)));
   u[2] = add(add(t[0], mul(t[1], w4i2)), add(t[2], mul(t[3], w4i2)));
   u[3] = add(add(t[0], mul(t[1], w4i3)), add(mul(t[2], w4i2), mul(t[3], w4i)));
-  uint32_t scale = quarter;  // 1/4, then times g^-(d n) per chunk
+  uint32_t scale = quarter;
   for (int d = 0; d < 4; d++) {
-    out[((uint64_t)d * lanes + w) * n + k] = mul(u[d], scale);
-    scale = mul(scale, gn_inv);
+    J.out[((uint64_t)d * J.lanes + w) * n + k] = mul(u[d], scale);
+    scale = mul(scale, J.gn_inv);
   }
 }
 
 // ---------------------------------------------------------------- grand product
 // ratio[j] = num(j) / den(j) on Lagrange rows (internal/poly/iop_utils.go:170-192).
-struct LaneTable { const uint32_t* const* lanes; };
-__global__ void k_gp_ratio(XProgram pn, XProgram pd, const E6* coins, LaneTable t, int logn, uint32_t* ratio) {
+// One job per step (blockIdx.y); lanes[l] is lane l of the step's inputs.
+struct GpJob { XProgram pn, pd; const uint32_t* const* lanes; uint32_t* ratio; int logn; };
+__global__ void k_gp_ratio(const GpJob* jobs, const E6* coins) {
   extern __shared__ uint32_t regs[];
-  const uint32_t n = 1u << logn;
+  const GpJob& J = jobs[blockIdx.y];
+  const uint32_t n = 1u << J.logn;
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
-  auto lane = [&](uint32_t l, uint32_t row) -> uint32_t { return t.lanes[l][row]; };
-  E6 a = x_eval(pn, coins, regs + threadIdx.x, blockDim.x, j, n, lane);
-  E6 b = x_eval(pd, coins, regs + threadIdx.x, blockDim.x, j, n, lane);
+  const uint32_t* const* lanes = J.lanes;
+  auto lane = [&](uint32_t l, uint32_t row) -> uint32_t { return lanes[l][row]; };
+  E6 a = x_eval(J.pn, coins, regs + threadIdx.x, blockDim.x, j, n, lane);
+  E6 b = x_eval(J.pd, coins, regs + threadIdx.x, blockDim.x, j, n, lane);
   E6 q = e6_mul(a, e6_inv(b));
-  for (int w = 0; w < 6; w++) ratio[(uint64_t)w * n + j] = q.c[w];
+  for (int w = 0; w < 6; w++) J.ratio[(uint64_t)w * n + j] = q.c[w];
 }
 
 constexpr int SCAN_BLOCK = 256, SCAN_PER_THREAD = 8, SCAN_TILE = SCAN_BLOCK * SCAN_PER_THREAD;
@@ -336,21 +432,27 @@ __device__ __forceinline__ void st6(uint32_t* p, uint64_t stride, uint64_t i, co
   for (int w = 0; w < 6; w++) p[w * stride + i] = v.c[w];
 }
 
-// Per-tile inclusive product scan of ratio (in place); tile totals out.
-__global__ void k_scan_tiles(uint32_t* x, uint64_t n, uint32_t* totals) {
+// Product scans over E6 vectors stored as 6 lanes of n words: per-tile
+// inclusive scan in place, tile totals, their exclusive prefix, and the
+// shifted result out[0] = 1, out[i] = prod_{k<i} x[k].  One job per vector.
+struct ScanJob { uint32_t* x; uint64_t n; uint32_t* totals; uint32_t* pre; uint32_t* out; uint32_t nt; };
+
+__global__ void k_scan_tiles(const ScanJob* jobs) {
   __shared__ E6 part[SCAN_BLOCK];
+  const ScanJob& J = jobs[blockIdx.y];
+  if (blockIdx.x >= J.nt) return;
+  const uint64_t n = J.n;
   const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_PER_THREAD;
   E6 acc = e6_one();
   E6 v[SCAN_PER_THREAD];
   for (int i = 0; i < SCAN_PER_THREAD; i++) {
     uint64_t idx = base + i;
-    v[i] = idx < n ? ld6(x, n, idx) : e6_one();
+    v[i] = idx < n ? ld6(J.x, n, idx) : e6_one();
     acc = e6_mul(acc, v[i]);
     v[i] = acc;
   }
   part[threadIdx.x] = acc;
   __syncthreads();
-  // exclusive product of the thread partials (Hillis-Steele on smem)
   for (int off = 1; off < SCAN_BLOCK; off <<= 1) {
     E6 t = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : e6_one();
     __syncthreads();
@@ -360,41 +462,40 @@ __global__ void k_scan_tiles(uint32_t* x, uint64_t n, uint32_t* totals) {
   E6 pre = threadIdx.x ? part[threadIdx.x - 1] : e6_one();
   for (int i = 0; i < SCAN_PER_THREAD; i++) {
     uint64_t idx = base + i;
-    if (idx < n) st6(x, n, idx, e6_mul(pre, v[i]));
+    if (idx < n) st6(J.x, n, idx, e6_mul(pre, v[i]));
   }
-  if (threadIdx.x == SCAN_BLOCK - 1) {
-    uint32_t nt = gridDim.x;
-    for (int w = 0; w < 6; w++) totals[w * nt + blockIdx.x] = part[SCAN_BLOCK - 1].c[w];
-  }
+  if (threadIdx.x == SCAN_BLOCK - 1)
+    for (int w = 0; w < 6; w++) J.totals[w * J.nt + blockIdx.x] = part[SCAN_BLOCK - 1].c[w];
 }
 
-// Exclusive prefix products of the tile totals (totals[w * nt + t]) into
-// pre[t * 6 + w]; nt is small (n / 2048), one thread walks it.
-__global__ void k_tile_prefix(const uint32_t* totals, uint32_t nt, uint32_t* pre) {
+// Exclusive prefix products of the tile totals (one thread per job; nt is
+// n / 2048).
+__global__ void k_tile_prefix(const ScanJob* jobs, uint32_t n_jobs) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_jobs) return;
+  const ScanJob& J = jobs[i];
   E6 acc = e6_one();
-  for (uint32_t t = 0; t < nt; t++) {
-    for (int w = 0; w < 6; w++) pre[t * 6 + w] = acc.c[w];
+  for (uint32_t t = 0; t < J.nt; t++) {
+    for (int w = 0; w < 6; w++) J.pre[t * 6 + w] = acc.c[w];
     E6 v;
-    for (int w = 0; w < 6; w++) v.c[w] = totals[w * nt + t];
+    for (int w = 0; w < 6; w++) v.c[w] = J.totals[w * J.nt + t];
     acc = e6_mul(acc, v);
   }
 }
 
-// Grand product from the tile-local inclusive scan s: out[0] = 1,
-// out[i] = s[i-1] times the product of the earlier tiles' totals.
-__global__ void k_gp_finish(const uint32_t* s, uint64_t n, const uint32_t* tile_pre, uint32_t* out) {
+__global__ void k_gp_finish(const ScanJob* jobs) {
+  const ScanJob& J = jobs[blockIdx.y];
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  if (i >= J.n) return;
   E6 v;
   if (i == 0) v = e6_one();
   else {
-    uint64_t k = i - 1;
-    uint64_t tile = k / SCAN_TILE;
+    uint64_t k = i - 1, tile = k / SCAN_TILE;
     E6 pre;
-    for (int w = 0; w < 6; w++) pre.c[w] = tile_pre[tile * 6 + w];
-    v = e6_mul(pre, ld6(s, n, k));
+    for (int w = 0; w < 6; w++) pre.c[w] = J.pre[tile * 6 + w];
+    v = e6_mul(pre, ld6(J.x, J.n, k));
   }
-  st6(out, n, i, v);
+  st6(J.out, J.n, i, v);
 }
 
 // ---------------------------------------------------------------- claimed values
@@ -443,7 +544,8 @@ struct DeepJob {
   const uint32_t* tw;   // w_4n^j table
   uint32_t* out;        // 6 lanes, lane stride 4n
 };
-__global__ void k_deep(DeepJob jb) {
+__global__ void k_deep(const DeepJob* jobs) {
+  const DeepJob& jb = jobs[blockIdx.y];
   const uint32_t big = 1u << jb.logn4;
   const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= big) return;
@@ -473,12 +575,15 @@ __global__ void k_deep(DeepJob jb) {
 }
 
 // ---------------------------------------------------------------- FRI
-// running += gamma * level (6 lanes each, lane stride n)
-__global__ void k_axpy_e6(uint32_t* run, const uint32_t* lvl, uint64_t n, E6 gamma) {
+// running += sum_t gamma_t * level_t (6 lanes each, lane stride n), the
+// levels entering FRI at this round in level order.
+struct AxpyTerm { const uint32_t* lvl; E6 gamma; };
+__global__ void k_axpy_e6(uint32_t* run, uint64_t n, const AxpyTerm* terms, uint32_t n_terms) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
-  E6 a = ld6(run, n, i), b = ld6(lvl, n, i);
-  st6(run, n, i, e6_add(a, e6_mul(b, gamma)));
+  E6 a = ld6(run, n, i);
+  for (uint32_t t = 0; t < n_terms; t++) a = e6_add(a, e6_mul(ld6(terms[t].lvl, n, i), terms[t].gamma));
+  st6(run, n, i, a);
 }
 
 // next[i] = (p+q)/2 + alpha (p-q)/(2 x_i), x_i^-1 = w_n^-bitrev(i, n/2)

@@ -36,6 +36,10 @@ template <class F> int guarded(lg_ctx* ctx, F f) {
   if (!ctx) return LG_ERR_INVALID;
   try {
     LG_CK(cudaSetDevice(ctx->c.device));
+    if (ctx->c.stream) {
+      LG_CK(cudaStreamSynchronize(ctx->c.stream));
+      ctx->c.arena_reset();
+    }
     f();
     return LG_OK;
   } catch (Error& e) {
@@ -97,6 +101,10 @@ void lg_ctx_destroy(lg_ctx* ctx) {
   }
   if (ctx->c.pinned) cudaFreeHost(ctx->c.pinned);
   delete ctx;
+}
+
+int lg_ctx_set_batched(lg_ctx* ctx, int batched) {
+  return guarded(ctx, [&] { ctx->c.batched = batched != 0; });
 }
 
 const char* lg_last_error(lg_ctx* ctx) { return ctx ? ctx->c.err.c_str() : "null context"; }
@@ -257,12 +265,14 @@ int lg_grand_product(lg_ctx* ctx, const uint32_t* num, const uint32_t* den, uint
     LG_LAUNCH();
     uint32_t nt = (uint32_t)((n + SCAN_TILE - 1) / SCAN_TILE);
     auto totals = std::make_shared<DBuf>(6 * (size_t)nt, c.stream), pre = std::make_shared<DBuf>(6 * (size_t)nt, c.stream);
-    k_scan_tiles<<<nt, SCAN_BLOCK, 0, c.stream>>>(ratio->p, n, totals->p);
-    LG_LAUNCH();
-    k_tile_prefix<<<1, 1, 0, c.stream>>>(totals->p, nt, pre->p);
-    LG_LAUNCH();
     auto res = std::make_shared<DBuf>(6 * n, c.stream);
-    k_gp_finish<<<g1, 256, 0, c.stream>>>(ratio->p, n, pre->p, res->p);
+    std::vector<ScanJob> sj = {ScanJob{ratio->p, n, totals->p, pre->p, res->p, nt}};
+    auto sd = upload_vec(c, sj);
+    k_scan_tiles<<<dim3(nt, 1), SCAN_BLOCK, 0, c.stream>>>((const ScanJob*)sd->p);
+    LG_LAUNCH();
+    k_tile_prefix<<<1, 64, 0, c.stream>>>((const ScanJob*)sd->p, 1);
+    LG_LAUNCH();
+    k_gp_finish<<<dim3(g1, 1), 256, 0, c.stream>>>((const ScanJob*)sd->p);
     LG_LAUNCH();
     auto aos = std::make_shared<DBuf>(6 * n, c.stream);
     k_soa_to_aos<<<g6, 256, 0, c.stream>>>(res->p, n, 6, aos->p);

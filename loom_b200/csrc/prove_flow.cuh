@@ -23,7 +23,7 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
   coins.assign(R, e6_zero());
   size_t ti = 0;
   for (uint32_t r = 0; r < R; r++) {
-    for (const Step& st : pg.steps) if (st.round == r) run_step(st);
+    run_steps(r);
     if (ti < trees.size() && !trees[ti].air && trees[ti].round == (int)r) {
       committed.push_back(commit_tree(trees[ti]));
       Digest root = committed.back().tree.root;
@@ -34,7 +34,7 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
     coins[r] = digest_e6(fs.compute(coin_name(r)));
   }
   // ---- AIR quotients and their commitment (prover/prover.go:461-561)
-  for (uint32_t m : mod_order) if (chunk_count(m)) quotient(m);
+  quotient_all();
   if (ti < trees.size() && trees[ti].air) {
     committed.push_back(commit_tree(trees[ti]));
     Digest root = committed.back().tree.root;
@@ -90,7 +90,7 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
         }
   std::vector<uint32_t> dots(6 * jobs.size());
   if (!jobs.empty()) {
-    auto jd = upload_words(c, jobs.data(), jobs.size() * sizeof(DotJob));
+    auto jd = upload_vec(c, jobs);
     auto od = std::make_shared<DBuf>(6 * jobs.size(), c.stream);
     k_dot<<<(unsigned)jobs.size(), 256, 0, c.stream>>>((const DotJob*)jd->p, od->p);
     LG_LAUNCH();
@@ -140,6 +140,9 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
 
   // ---- DEEP codewords on the LDE rows (internal/fri/deep.go:71-266)
   std::vector<DBufP> deep(classes.size());
+  std::vector<DeepJob> djobs;
+  std::vector<DBufP> dkeep;
+  std::vector<double> dbytes;
   for (size_t ci = 0; ci < classes.size(); ci++) {
     uint32_t m = classes[ci];
     uint32_t logn = pg.modules[m].log_n;
@@ -180,20 +183,32 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
       }
     for (size_t k = 0; k < pts.size(); k++) jb.z[k] = pts[k];
     jb.n_points = (uint32_t)pts.size();
-    auto bd = upload_words(c, bundles.data(), bundles.size() * sizeof(DeepBundle));
+    auto bd = upload_vec(c, bundles);
+    dkeep.push_back(bd);
     jb.bundles = (const DeepBundle*)bd->p;
     jb.n_bundles = (uint32_t)bundles.size();
     jb.logn4 = (int)logn + RATE_LOG;
     jb.tw = c.twiddles(jb.logn4);
     deep[ci] = std::make_shared<DBuf>(6 * big, c.stream);
     jb.out = deep[ci]->p;
+    djobs.push_back(jb);
     double row_bytes = 24.0;
     for (auto& bu : bundles) row_bytes += bu.ext ? 24.0 : 4.0;
-    c.timed("deep", row_bytes * big, 0, [&] {
-      k_deep<<<(unsigned)((big + 127) / 128), 128, 0, c.stream>>>(jb);
+    dbytes.push_back(row_bytes * big);
+  }
+  auto launch_deep = [&](size_t first, size_t count) {
+    std::vector<DeepJob> v(djobs.begin() + first, djobs.begin() + first + count);
+    uint32_t max_big = 0;
+    double bytes = 0;
+    for (size_t i = first; i < first + count; i++) { max_big = std::max(max_big, 1u << djobs[i].logn4); bytes += dbytes[i]; }
+    auto jd = upload_vec(c, v);
+    c.timed("deep", bytes, 0, [&] {
+      k_deep<<<dim3((max_big + 127) / 128, (unsigned)count), 128, 0, c.stream>>>((const DeepJob*)jd->p);
       LG_LAUNCH();
     });
-  }
+  };
+  if (c.batched) launch_deep(0, djobs.size());
+  else for (size_t i = 0; i < djobs.size(); i++) launch_deep(i, 1);
 
   // ---- FRI (internal/fri/fri.go:352-365,606-736)
   std::vector<size_t> class_at(classes.size());
@@ -213,13 +228,18 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
   TreeDev levels_tree;
   levels_tree.log_leaves = lvl_log[0] + RATE_LOG - 1;
   levels_tree.nodes = std::make_shared<DBuf>((size_t)16 << levels_tree.log_leaves, c.stream);
-  hash_leaves(c, lvl[0]->p, 0, 1, lvl_log[0] + RATE_LOG, levels_tree.nodes->p + ((size_t)8 << levels_tree.log_leaves));
-  for (size_t l = 1; l < L; l++) {
-    uint32_t lr = lvl_log[l] + RATE_LOG;
-    auto lv = std::make_shared<DBuf>((size_t)8 << (lr - 1), c.stream);
-    hash_leaves(c, lvl[l]->p, 0, 1, lr, lv->p);
-    levels_tree.inj.push_back(lv);
-    levels_tree.inj_log_w.push_back(lr - 1);
+  {
+    std::vector<LeafGroup> lgs;
+    lgs.push_back(leaf_group(lvl[0]->p, 0, 1, lvl_log[0] + RATE_LOG, levels_tree.nodes->p + ((size_t)8 << levels_tree.log_leaves)));
+    for (size_t l = 1; l < L; l++) {
+      uint32_t lr = lvl_log[l] + RATE_LOG;
+      auto lv = std::make_shared<DBuf>((size_t)8 << (lr - 1), c.stream);
+      lgs.push_back(leaf_group(lvl[l]->p, 0, 1, lr, lv->p));
+      levels_tree.inj.push_back(lv);
+      levels_tree.inj_log_w.push_back(lr - 1);
+    }
+    if (c.batched) launch_leaves(c, lgs);
+    else for (auto& g : lgs) launch_leaves(c, {g});
   }
   build_tree(c, levels_tree);
   std::vector<E6> gam(L);
@@ -242,10 +262,20 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
   const uint32_t inv2 = inv(to_mont(2));
   for (int j = r0; j < NR; j++) {
     if (j == r0) layers[j] = lvl[0];
-    for (size_t l = 1; l < L; l++) {
-      if (jl(l) != j) continue;
-      k_axpy_e6<<<(unsigned)((nj + 255) / 256), 256, 0, c.stream>>>(running->p, lvl[l]->p, nj, gam[l]);
-      LG_LAUNCH();
+    {
+      std::vector<AxpyTerm> terms;
+      for (size_t l = 1; l < L; l++)
+        if (jl(l) == j) terms.push_back(AxpyTerm{lvl[l]->p, gam[l]});
+      auto axpy = [&](const std::vector<AxpyTerm>& tv) {
+        auto td = upload_vec(c, tv);
+        k_axpy_e6<<<(unsigned)((nj + 255) / 256), 256, 0, c.stream>>>(running->p, nj, (const AxpyTerm*)td->p,
+                                                                       (uint32_t)tv.size());
+        LG_LAUNCH();
+      };
+      if (!terms.empty()) {
+        if (c.batched) axpy(terms);
+        else for (auto& tm : terms) axpy({tm});
+      }
     }
     if (j > r0) layers[j] = running;
     if (j == r0) ftrees[j] = levels_tree;
@@ -253,7 +283,7 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
       TreeDev& t = ftrees[j];
       t.log_leaves = (uint32_t)(LOG_N_FRI - j - 1);
       t.nodes = std::make_shared<DBuf>((size_t)16 << t.log_leaves, c.stream);
-      hash_leaves(c, running->p, 0, 1, (uint32_t)(LOG_N_FRI - j), t.nodes->p + ((size_t)8 << t.log_leaves));
+      launch_leaves(c, {leaf_group(running->p, 0, 1, (uint32_t)(LOG_N_FRI - j), t.nodes->p + ((size_t)8 << t.log_leaves))});
       build_tree(c, t);
     }
     Digest root = ftrees[j].root;
@@ -330,16 +360,16 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
     const LdeOut& top = cm.groups[cm.order[0]];
     boff[b].path = add_path(cm.tree, (uint32_t)(LOG_N_FRI - (top.log_n + RATE_LOG)), true);
   }
-  auto pos_d = upload_words(c, pos.data(), pos.size() * 4);
+  auto pos_d = upload_vec(c, pos);
   auto out_d = std::make_shared<DBuf>(per_q * num_queries, c.stream);
   {
-    auto rd = upload_words(c, rows.data(), rows.size() * sizeof(RowSrc));
+    auto rd = upload_vec(c, rows);
     uint32_t max_l = 1;
     for (auto& r : rows) max_l = std::max(max_l, r.n_lanes);
     k_gather_rows<<<dim3((max_l + 63) / 64, num_queries, (unsigned)rows.size()), 64, 0, c.stream>>>(
         (const RowSrc*)rd->p, (uint32_t)rows.size(), pos_d->p, num_queries, per_q, out_d->p);
     LG_LAUNCH();
-    auto pd = upload_words(c, paths.data(), paths.size() * sizeof(PathSrc));
+    auto pd = upload_vec(c, paths);
     uint32_t max_t = 1;
     for (auto& p : paths) max_t = std::max(max_t, p.log_leaves + p.n_inj);
     k_gather_paths<<<dim3((max_t + 31) / 32, num_queries, (unsigned)paths.size()), 32, 0, c.stream>>>(

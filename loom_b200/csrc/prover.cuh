@@ -264,50 +264,74 @@ struct Prover {
   DBufP coins_on_device() {
     std::vector<uint32_t> w;
     for (auto& e : coins) for (int i = 0; i < 6; i++) w.push_back(e.c[i]);
-    return upload_words(c, w.data(), w.size() * 4);
+    return upload_vec(c, w);
   }
 
   // ------------------------------------------------------------ steps
-  // Grand product (internal/poly/iop_utils.go:170-192,316-323).
-  void run_step(const Step& st) {
-    uint32_t logn = pg.modules[st.module].log_n;
-    size_t n = (size_t)1 << logn;
-    std::vector<const uint32_t*> lanes;
-    std::map<uint32_t, uint32_t> first_lane;
-    auto lane_of = [&](uint32_t col) -> uint32_t {
-      auto it = first_lane.find(col);
-      if (it != first_lane.end()) return it->second;
-      if (!col_buf.count(col)) throw Error(LG_ERR_INVALID, "step reads a column that is not available yet");
-      uint32_t f = (uint32_t)lanes.size();
-      for (uint32_t w = 0; w < lanes_of(col); w++) lanes.push_back(lane_ptr(col, w));
-      first_lane[col] = f;
-      return f;
-    };
-    XCode xn = compile_expr(st.num, lane_of), xd = compile_expr(st.den, lane_of);
-    auto tab = upload_ptrs(c, lanes);
-    auto cn = upload_words(c, xn.code.data(), xn.code.size() * sizeof(XInst));
-    auto cd = upload_words(c, xd.code.data(), xd.code.size() * sizeof(XInst));
+  // Grand products of round r (internal/poly/iop_utils.go:170-192,316-323):
+  // ratio num/den per row, then a product scan.  Batched: one launch per
+  // kernel for all steps of the round; plain: one set of launches per step.
+  void run_steps(uint32_t r) {
+    std::vector<const Step*> steps;
+    for (const Step& st : pg.steps) if (st.round == r) steps.push_back(&st);
+    if (steps.empty()) return;
     auto coins_d = coins_on_device();
-    auto out = std::make_shared<DBuf>(6 * n, c.stream);
-    XProgram pn{(const XInst*)cn->p, (uint32_t)xn.code.size(), xn.n_regs, xn.result, xn.result_ext};
-    XProgram pd{(const XInst*)cd->p, (uint32_t)xd.code.size(), xd.n_regs, xd.result, xd.result_ext};
+    std::vector<GpJob> jobs;
+    std::vector<ScanJob> scans;
+    std::vector<DBufP> keep;
+    uint32_t max_regs = 1;
+    for (const Step* st : steps) {
+      uint32_t logn = pg.modules[st->module].log_n;
+      size_t n = (size_t)1 << logn;
+      std::vector<const uint32_t*> lanes;
+      std::map<uint32_t, uint32_t> first_lane;
+      auto lane_of = [&](uint32_t col) -> uint32_t {
+        auto it = first_lane.find(col);
+        if (it != first_lane.end()) return it->second;
+        if (!col_buf.count(col)) throw Error(LG_ERR_INVALID, "step reads a column that is not available yet");
+        uint32_t f = (uint32_t)lanes.size();
+        for (uint32_t w = 0; w < lanes_of(col); w++) lanes.push_back(lane_ptr(col, w));
+        first_lane[col] = f;
+        return f;
+      };
+      XCode xn = compile_expr(st->num, lane_of), xd = compile_expr(st->den, lane_of);
+      max_regs = std::max(max_regs, std::max(xn.n_regs, xd.n_regs));
+      auto tab = upload_vec(c, lanes), cn = upload_vec(c, xn.code), cd = upload_vec(c, xd.code);
+      auto ratio = std::make_shared<DBuf>(6 * n, c.stream);
+      uint32_t nt = (uint32_t)((n + SCAN_TILE - 1) / SCAN_TILE);
+      auto totals = std::make_shared<DBuf>(6 * (size_t)nt, c.stream), pre = std::make_shared<DBuf>(6 * (size_t)nt, c.stream);
+      auto res = std::make_shared<DBuf>(6 * n, c.stream);
+      keep.insert(keep.end(), {tab, cn, cd, ratio, totals, pre});
+      jobs.push_back(GpJob{XProgram{(const XInst*)cn->p, (uint32_t)xn.code.size(), xn.n_regs, xn.result, xn.result_ext},
+                           XProgram{(const XInst*)cd->p, (uint32_t)xd.code.size(), xd.n_regs, xd.result, xd.result_ext},
+                           (const uint32_t* const*)tab->p, ratio->p, (int)logn});
+      scans.push_back(ScanJob{ratio->p, n, totals->p, pre->p, res->p, nt});
+      col_buf[st->out] = res;
+    }
     const int T = 128;
-    size_t smem = (size_t)std::max(std::max(xn.n_regs, xd.n_regs), 1u) * 6 * T * 4;
-    LG_CK(cudaFuncSetAttribute(k_gp_ratio, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_gp_ratio<<<(unsigned)((n + T - 1) / T), T, smem, c.stream>>>(pn, pd, (const E6*)coins_d->p,
-                                                                     LaneTable{(const uint32_t* const*)tab->p}, (int)logn, out->p);
-    LG_LAUNCH();
-    uint32_t nt = (uint32_t)((n + SCAN_TILE - 1) / SCAN_TILE);
-    auto totals = std::make_shared<DBuf>(6 * (size_t)nt, c.stream);
-    k_scan_tiles<<<nt, SCAN_BLOCK, 0, c.stream>>>(out->p, n, totals->p);
-    LG_LAUNCH();
-    auto pre = std::make_shared<DBuf>(6 * (size_t)nt, c.stream);
-    k_tile_prefix<<<1, 1, 0, c.stream>>>(totals->p, nt, pre->p);
-    LG_LAUNCH();
-    auto res = std::make_shared<DBuf>(6 * n, c.stream);
-    k_gp_finish<<<(unsigned)((n + 255) / 256), 256, 0, c.stream>>>(out->p, n, pre->p, res->p);
-    LG_LAUNCH();
-    col_buf[st.out] = res;
+    size_t smem = (size_t)max_regs * 6 * T * 4;
+    allow_smem(k_gp_ratio, smem);
+    auto launch = [&](size_t first, size_t count) {
+      uint32_t max_n = 0, max_nt = 0;
+      for (size_t i = first; i < first + count; i++) {
+        max_n = std::max<uint32_t>(max_n, (uint32_t)scans[i].n);
+        max_nt = std::max(max_nt, scans[i].nt);
+      }
+      std::vector<GpJob> jv(jobs.begin() + first, jobs.begin() + first + count);
+      std::vector<ScanJob> sv(scans.begin() + first, scans.begin() + first + count);
+      auto jd = upload_vec(c, jv), sd = upload_vec(c, sv);
+      k_gp_ratio<<<dim3((max_n + T - 1) / T, (unsigned)count), T, smem, c.stream>>>((const GpJob*)jd->p,
+                                                                                    (const E6*)coins_d->p);
+      LG_LAUNCH();
+      k_scan_tiles<<<dim3(max_nt, (unsigned)count), SCAN_BLOCK, 0, c.stream>>>((const ScanJob*)sd->p);
+      LG_LAUNCH();
+      k_tile_prefix<<<(unsigned)((count + 63) / 64), 64, 0, c.stream>>>((const ScanJob*)sd->p, (uint32_t)count);
+      LG_LAUNCH();
+      k_gp_finish<<<dim3((max_n + 255) / 256, (unsigned)count), 256, 0, c.stream>>>((const ScanJob*)sd->p);
+      LG_LAUNCH();
+    };
+    if (c.batched) launch(0, jobs.size());
+    else for (size_t i = 0; i < jobs.size(); i++) launch(i, 1);
   }
 
   // ------------------------------------------------------------ commits
@@ -346,82 +370,151 @@ struct Prover {
   }
 
   // ------------------------------------------------------------ quotient
-  void quotient(uint32_t m) {
-    uint32_t logn = pg.modules[m].log_n;
-    size_t n = mod_n(m), big = n << RATE_LOG;
-    uint32_t rho = chunk_count(m);
-    if (rho != 4) throw Error(LG_ERR_UNSUPPORTED, "quotient domains other than 4N are not supported by this build");
-    check_ntt_size((int)logn);
-    // coefficient lanes of every column the relation reads
-    std::vector<const uint32_t*> coef_lanes;
-    std::map<uint32_t, uint32_t> first_lane;
-    std::vector<DBufP> keep;
-    auto lane_of = [&](uint32_t col) -> uint32_t {
-      auto it = first_lane.find(col);
-      if (it != first_lane.end()) return it->second;
-      uint32_t f = (uint32_t)coef_lanes.size();
-      auto cc = col_coef.find(col);
-      if (cc != col_coef.end()) {
-        for (uint32_t w = 0; w < lanes_of(col); w++) coef_lanes.push_back(cc->second + (size_t)w * n);
-      } else {
-        // verifier columns: coefficients from a copy of the Lagrange values
-        auto b = std::make_shared<DBuf>(lanes_of(col) * n, c.stream);
-        LG_CK(cudaMemcpyAsync(b->p, col_buf.at(col)->p, lanes_of(col) * n * 4, cudaMemcpyDeviceToDevice, c.stream));
-        allow_smem(k_intt_inplace, n * 4);
-        k_intt_inplace<<<lanes_of(col), ntt_threads((int)logn), n * 4, c.stream>>>(b->p, n, (int)logn, c.twiddles((int)logn),
-                                                                                   inv(to_mont((uint32_t)n)));
-        LG_LAUNCH();
-        keep.push_back(b);
-        for (uint32_t w = 0; w < lanes_of(col); w++) coef_lanes.push_back(b->p + (size_t)w * n);
-      }
-      first_lane[col] = f;
-      return f;
+  // Q = V / (X^N - 1) of every module (internal/poly/compute_quotient.go:223-424),
+  // as chunk coefficients: coefficient lanes -> values on the four cosets
+  // g w_4n^c <w_n> -> bytecode evaluation and division -> per-coset inverse
+  // transforms -> a 4-point inverse DFT across cosets (k_quotient_chunks).
+  void quotient_all() {
+    struct ModQ {
+      uint32_t m, logn;
+      std::vector<CosetLane> lanes;
+      DBufP cv, qv, code, chunks;
+      XCode xc;
+      uint32_t zinv[4];
     };
-    XCode xc = compile_expr((uint32_t)fold_root[m], lane_of);
-    const uint32_t* twn = c.twiddles((int)logn);
-    const uint32_t* tw4 = c.twiddles((int)logn + RATE_LOG);
-    auto tab = upload_ptrs(c, coef_lanes);
-    auto cv = std::make_shared<DBuf>(coef_lanes.size() * big, c.stream);
-    dim3 grid((unsigned)coef_lanes.size(), 4);
-    allow_smem(k_coset_eval_ptrs, n * 4);
-    const uint32_t* gp = c.gpowers((int)logn, false);
-    c.timed("coset_eval", 20.0 * n * coef_lanes.size(), 0, [&] {
-      k_coset_eval_ptrs<<<grid, ntt_threads((int)logn), n * 4, c.stream>>>((const uint32_t* const*)tab->p, (int)logn, twn,
-                                                                           tw4, gp, cv->p);
-      LG_LAUNCH();
-    });
-    // 1 / (s_c^n - 1), s_c = g w_4n^c (internal/poly/compute_quotient.go:400-421)
-    uint32_t zinv[4];
-    uint32_t g = to_mont(3), w4n = root_of_unity_mont((int)logn + RATE_LOG);
-    for (int cc = 0; cc < 4; cc++) {
-      uint32_t s = mul(g, mont_pow(w4n, cc));
-      zinv[cc] = inv(sub(mont_pow(s, n), MONT_ONE));
+    std::vector<ModQ> mods;
+    std::vector<DBufP> keep;
+    for (uint32_t m : mod_order) {
+      if (!chunk_count(m)) continue;
+      if (chunk_count(m) != 4) throw Error(LG_ERR_UNSUPPORTED, "quotient domains other than 4N are not supported by this build");
+      uint32_t logn = pg.modules[m].log_n;
+      check_ntt_size((int)logn);
+      size_t n = (size_t)1 << logn, big = n << RATE_LOG;
+      ModQ q;
+      q.m = m;
+      q.logn = logn;
+      std::vector<const uint32_t*> coef_lanes;
+      std::map<uint32_t, uint32_t> first_lane;
+      auto lane_of = [&](uint32_t col) -> uint32_t {
+        auto it = first_lane.find(col);
+        if (it != first_lane.end()) return it->second;
+        uint32_t f = (uint32_t)coef_lanes.size();
+        auto cc = col_coef.find(col);
+        if (cc != col_coef.end()) {
+          for (uint32_t w = 0; w < lanes_of(col); w++) coef_lanes.push_back(cc->second + (size_t)w * n);
+        } else {
+          // verifier columns: coefficients of the Lagrange values
+          auto b = std::make_shared<DBuf>(lanes_of(col) * n, c.stream);
+          LG_CK(cudaMemcpyAsync(b->p, col_buf.at(col)->p, lanes_of(col) * n * 4, cudaMemcpyDeviceToDevice, c.stream));
+          std::vector<uint32_t*> ls;
+          for (uint32_t w = 0; w < lanes_of(col); w++) ls.push_back(b->p + (size_t)w * n);
+          auto tab = upload_vec(c, ls);
+          allow_smem(k_intt, n * 4);
+          k_intt<<<lanes_of(col), ntt_threads((int)logn), n * 4, c.stream>>>((uint32_t* const*)tab->p, (int)logn,
+                                                                             c.twiddles((int)logn), inv(to_mont((uint32_t)n)));
+          LG_LAUNCH();
+          keep.push_back(b);
+          keep.push_back(tab);
+          for (uint32_t w = 0; w < lanes_of(col); w++) coef_lanes.push_back(b->p + (size_t)w * n);
+        }
+        first_lane[col] = f;
+        return f;
+      };
+      q.xc = compile_expr((uint32_t)fold_root[m], lane_of);
+      q.cv = std::make_shared<DBuf>(coef_lanes.size() * big, c.stream);
+      for (size_t l = 0; l < coef_lanes.size(); l++) q.lanes.push_back(CosetLane{coef_lanes[l], q.cv->p + l * big});
+      uint32_t g = to_mont(3), w4n = root_of_unity_mont((int)logn + RATE_LOG);
+      for (int cc = 0; cc < 4; cc++) q.zinv[cc] = inv(sub(mont_pow(mul(g, mont_pow(w4n, cc)), n), MONT_ONE));
+      q.code = upload_vec(c, q.xc.code);
+      q.qv = std::make_shared<DBuf>((root_ext[m] ? 6 : 1) * big, c.stream);
+      q.chunks = std::make_shared<DBuf>(4 * (root_ext[m] ? 6 : 1) * n, c.stream);
+      chunk_coef[m] = q.chunks;
+      mods.push_back(std::move(q));
     }
-    auto zinv_d = upload_words(c, zinv, sizeof zinv);
-    auto code = upload_words(c, xc.code.data(), xc.code.size() * sizeof(XInst));
+    if (mods.empty()) return;
     auto coins_d = coins_on_device();
-    uint32_t lw = root_ext[m] ? 6 : 1;
-    auto qv = std::make_shared<DBuf>(6 * big, c.stream);
-    XProgram xp{(const XInst*)code->p, (uint32_t)xc.code.size(), xc.n_regs, xc.result, xc.result_ext};
     const int T = 128;
-    size_t smem = (size_t)std::max(xc.n_regs, 1u) * 6 * T * 4;
-    LG_CK(cudaFuncSetAttribute(k_quotient_eval, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    c.timed("quotient_eval", 4.0 * big * coef_lanes.size() + 24.0 * big, 0, [&] {
-      k_quotient_eval<<<dim3((unsigned)((n + T - 1) / T), 4), T, smem, c.stream>>>(xp, (const E6*)coins_d->p, cv->p,
-                                                                                   (int)logn, zinv_d->p, qv->p);
+    auto run = [&](const std::vector<ModQ*>& ms) {
+      // 1. coset evaluations, one launch per size
+      std::map<uint32_t, std::vector<CosetLane>> by_size;
+      for (ModQ* q : ms) by_size[q->logn].insert(by_size[q->logn].end(), q->lanes.begin(), q->lanes.end());
+      for (auto& kv : by_size) {
+        uint32_t logn = kv.first;
+        size_t n = (size_t)1 << logn;
+        auto tab = upload_vec(c, kv.second);
+        allow_smem(k_coset_eval, n * 4);
+        const uint32_t* twn = c.twiddles((int)logn);
+        const uint32_t* tw4 = c.twiddles((int)logn + RATE_LOG);
+        const uint32_t* gp = c.gpowers((int)logn, false);
+        c.timed("coset_eval", 20.0 * n * kv.second.size(), 0, [&] {
+          k_coset_eval<<<dim3((unsigned)kv.second.size(), 4), ntt_threads((int)logn), n * 4, c.stream>>>(
+              (const CosetLane*)tab->p, (int)logn, twn, tw4, gp);
+          LG_LAUNCH();
+        });
+      }
+      // 2. bytecode evaluation on the 4n coset points of every module
+      std::vector<QJob> qj;
+      uint32_t max_regs = 1, max_n = 0;
+      double qbytes = 0;
+      for (ModQ* q : ms) {
+        QJob j{};
+        j.p = XProgram{(const XInst*)q->code->p, (uint32_t)q->xc.code.size(), q->xc.n_regs, q->xc.result, q->xc.result_ext};
+        j.cv = q->cv->p;
+        j.qv = q->qv->p;
+        j.logn = (int)q->logn;
+        for (int k = 0; k < 4; k++) j.zinv[k] = q->zinv[k];
+        qj.push_back(j);
+        max_regs = std::max(max_regs, q->xc.n_regs);
+        max_n = std::max(max_n, 1u << q->logn);
+        qbytes += (4.0 * q->lanes.size() + 24.0) * (4.0 * (1u << q->logn));
+      }
+      auto qd = upload_vec(c, qj);
+      size_t smem = (size_t)max_regs * 6 * T * 4;
+      allow_smem(k_quotient_eval, smem);
+      c.timed("quotient_eval", qbytes, 0, [&] {
+        k_quotient_eval<<<dim3((max_n + T - 1) / T, 4, (unsigned)qj.size()), T, smem, c.stream>>>((const QJob*)qd->p,
+                                                                                                  (const E6*)coins_d->p);
+        LG_LAUNCH();
+      });
+      // 3. per-coset inverse transforms, one launch per size
+      std::map<uint32_t, std::vector<uint32_t*>> intt;
+      for (ModQ* q : ms) {
+        size_t n = (size_t)1 << q->logn;
+        uint32_t lw = root_ext[q->m] ? 6 : 1;
+        for (uint32_t w = 0; w < lw; w++)
+          for (int cc = 0; cc < 4; cc++) intt[q->logn].push_back(q->qv->p + (size_t)w * 4 * n + cc * n);
+      }
+      for (auto& kv : intt) {
+        size_t n = (size_t)1 << kv.first;
+        auto tab = upload_vec(c, kv.second);
+        allow_smem(k_intt, n * 4);
+        const uint32_t* twn = c.twiddles((int)kv.first);
+        c.timed("quotient_intt", 8.0 * n * kv.second.size(), 0, [&] {
+          k_intt<<<(unsigned)kv.second.size(), ntt_threads((int)kv.first), n * 4, c.stream>>>(
+              (uint32_t* const*)tab->p, (int)kv.first, twn, inv(to_mont((uint32_t)n)));
+          LG_LAUNCH();
+        });
+      }
+      // 4. chunk coefficients
+      std::vector<QcJob> cj;
+      for (ModQ* q : ms) {
+        size_t n = (size_t)1 << q->logn;
+        cj.push_back(QcJob{q->qv->p, q->chunks->p, (int)q->logn, root_ext[q->m] ? 6u : 1u,
+                           c.gpowers((int)q->logn, true), c.twiddles((int)q->logn + RATE_LOG),
+                           inv(mont_pow(to_mont(3), n))});
+      }
+      auto cd = upload_vec(c, cj);
+      k_quotient_chunks<<<dim3((max_n + 127) / 128, 6, (unsigned)cj.size()), 128, 0, c.stream>>>((const QcJob*)cd->p,
+                                                                                                inv(to_mont(4)));
       LG_LAUNCH();
-    });
-    // coset values -> per-coset coefficients -> chunk coefficients
-    allow_smem(k_intt_inplace, n * 4);
-    k_intt_inplace<<<(unsigned)(lw * 4), ntt_threads((int)logn), n * 4, c.stream>>>(qv->p, n, (int)logn, twn,
-                                                                                    inv(to_mont((uint32_t)n)));
-    LG_LAUNCH();
-    auto chunks = std::make_shared<DBuf>(4 * lw * n, c.stream);
-    uint32_t gn_inv = inv(mont_pow(g, n));
-    k_quotient_chunks<<<dim3((unsigned)((n + 127) / 128), lw), 128, 0, c.stream>>>(
-        qv->p, (int)logn, c.gpowers((int)logn, true), tw4, chunks->p, inv(to_mont(4)), gn_inv, (int)lw);
-    LG_LAUNCH();
-    chunk_coef[m] = chunks;
+    };
+    if (c.batched) {
+      std::vector<ModQ*> all;
+      for (auto& q : mods) all.push_back(&q);
+      run(all);
+    } else {
+      for (auto& q : mods) run({&q});
+    }
   }
 
   std::vector<uint8_t> prove(const uint32_t* const* witness, bool on_device);

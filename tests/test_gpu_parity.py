@@ -78,16 +78,22 @@ def _prove_both(ctx, n_inst, n, q, seed):
     return ctx.prove(compiled.words, mont, q), oracle.prove(compiled.words, mont, q)
 
 
-@pytest.mark.parametrize("n_inst,logn,q", [(1, 4, 1), (2, 10, 16), (4, 12, 200), (3, 13, 7)])
-def test_prove_bytes_equal_oracle(ctx, n_inst, logn, q):
-    got, want = _prove_both(ctx, n_inst, 1 << logn, q, seed=0x10AD + logn)
+@pytest.mark.parametrize("batched", [True, False])
+@pytest.mark.parametrize("n_inst,logn,q", [(1, 4, 1), (2, 10, 16), (4, 12, 200), (3, 13, 7), (5, 9, 3)])
+def test_prove_bytes_equal_oracle(ctx, n_inst, logn, q, batched):
+    ctx.set_batched(batched)
+    try:
+        got, want = _prove_both(ctx, n_inst, 1 << logn, q, seed=0x10AD + logn)
+    finally:
+        ctx.set_batched(True)
     assert len(got) == len(want)
     assert got == want
     p = proof.decode(got)
     assert all(v == p.final_poly[0] for v in p.final_poly)
 
 
-def test_prove_uneven_modules(ctx):
+@pytest.mark.parametrize("batched", [True, False])
+def test_prove_uneven_modules(ctx, batched):
     from loom_b200.program import Builder, Module, col, copy_constraint
     # modules of 2^8, 2^10 and 2^11 rows in one program
     b = Builder()
@@ -105,7 +111,11 @@ def test_prove_uneven_modules(ctx):
     trace.update(b.generated)
     compiled = b.compile()
     mont = [F.to_mont(trace[name]) for (name, _, _) in compiled.witness_columns]
-    got = ctx.prove(compiled.words, mont, 20)
+    ctx.set_batched(batched)
+    try:
+        got = ctx.prove(compiled.words, mont, 20)
+    finally:
+        ctx.set_batched(True)
     assert got == oracle.prove(compiled.words, mont, 20)
 
 
