@@ -237,6 +237,7 @@ def main():
     ctx.prove(comp.words, dev_ptrs, a.queries, on_device=True)
     rep = ctx.profile_report()
     ctx.profile(False)
+    phases = rep.pop("phases", {})
 
     ms = statistics.mean(times)
     e2e_ms = statistics.mean(e2e_times)
@@ -315,6 +316,8 @@ def main():
             "roofline": roof,
             "roofline_poseidon2": p2_roof,
             "kernel_shares": shares,
+            "kernel_ms_profiled_step": round(total_k, 3),
+            "host_phases_ms": {k: round(v, 3) for k, v in phases.items()},
             "dominant_kernel": dom,
             "cpu_baseline": base,
             "clocks": clk,

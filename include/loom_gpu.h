@@ -72,6 +72,10 @@ void lg_ctx_destroy(lg_ctx* ctx);
  * it once per group / module, like a per-column prover.  Both produce the
  * same proof bytes. */
 int lg_ctx_set_batched(lg_ctx* ctx, int batched);
+/* Thread mapping of Poseidon2 leaf hashing: 1 = one thread per permutation,
+ * 6 = six lanes of a warp per permutation, 0 = choose from the number of
+ * leaves (default).  Results do not depend on it. */
+int lg_ctx_set_leaf_mapping(lg_ctx* ctx, int lanes_per_permutation);
 /* NUL-terminated description of the last failure on `ctx` (never NULL). */
 const char* lg_last_error(lg_ctx* ctx);
 

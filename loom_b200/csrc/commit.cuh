@@ -55,8 +55,16 @@ inline void launch_leaves(Ctx& c, const std::vector<LeafGroup>& gs) {
     perms += (double)g.n_leaves * ((total + 15) / 16);
   }
   auto tab = upload_vec(c, gs);
+  uint64_t all_leaves = 0;
+  for (auto& g : gs) all_leaves += g.n_leaves;
+  // Enough independent leaves to fill every SM: one thread per permutation;
+  // otherwise six lanes per permutation for a shorter dependent chain.
+  bool per_thread = c.leaf_mapping == 1 || (c.leaf_mapping == 0 && all_leaves >= (uint64_t)c.sm_count * 1024);
   c.timed("hash_leaves", bytes, perms, [&] {
-    k_hash_leaves<<<dim3((max_leaves + 127) / 128, (unsigned)gs.size()), 128, 0, c.stream>>>((const LeafGroup*)tab->p);
+    if (per_thread)
+      k_hash_leaves1<<<dim3((max_leaves + 127) / 128, (unsigned)gs.size()), 128, 0, c.stream>>>((const LeafGroup*)tab->p);
+    else
+      k_hash_leaves<<<dim3((max_leaves + 19) / 20, (unsigned)gs.size()), 128, 0, c.stream>>>((const LeafGroup*)tab->p);
     LG_LAUNCH();
   });
 }
@@ -135,13 +143,13 @@ inline void build_tree(Ctx& c, TreeDev& t) {
     const uint32_t* const* tab = (const uint32_t* const*)t.inj_ptrs->p + first;
     uint32_t cnt = (uint32_t)(next - first);
     c.timed("merkle_inject", 96.0 * start * cnt, (double)start * cnt, [&] {
-      k_merkle_inject<<<(start + 127) / 128, 128, 0, c.stream>>>(t.nodes->p, start, tab, cnt);
+      k_merkle_inject<<<(start + 19) / 20, 128, 0, c.stream>>>(t.nodes->p, start, tab, cnt);
       LG_LAUNCH();
     });
   };
   auto level = [&](uint32_t start) {
     c.timed("merkle_level", 96.0 * start, (double)start, [&] {
-      k_merkle_level<<<(start + 127) / 128, 128, 0, c.stream>>>(t.nodes->p, start);
+      k_merkle_level<<<(start + 19) / 20, 128, 0, c.stream>>>(t.nodes->p, start);
       LG_LAUNCH();
     });
   };
@@ -150,12 +158,19 @@ inline void build_tree(Ctx& c, TreeDev& t) {
     for (size_t k = 0; k < t.inj.size(); k++)
       if ((1u << t.inj_log_w[k]) < top || (fold_first && (1u << t.inj_log_w[k]) == top)) perms += 1u << t.inj_log_w[k];
     c.timed("merkle_tail", 96.0 * perms, perms, [&] {
-      k_merkle_tail<<<1, 512, 0, c.stream>>>(t.nodes->p, top, fold_first, (const InjRef*)ref_tab->p,
+      k_merkle_tail<<<1, 1024, 0, c.stream>>>(t.nodes->p, top, fold_first, (const InjRef*)ref_tab->p,
                                              (uint32_t)refs.size());
       LG_LAUNCH();
     });
   };
-  if (!c.batched) {
+  // the tail block chains at most 64 injections of one width
+  bool tail_ok = true;
+  for (size_t k = 0; k < t.inj.size(); k++) {
+    size_t same = 0;
+    for (size_t q = 0; q < t.inj.size(); q++) same += t.inj_log_w[q] == t.inj_log_w[k];
+    if ((1u << t.inj_log_w[k]) <= MERKLE_TAIL && same > 64) tail_ok = false;
+  }
+  if (!c.batched || !tail_ok) {
     fold(nl);
     for (uint32_t start = nl >> 1; start >= 1; start >>= 1) { level(start); fold(start); }
   } else if (nl <= MERKLE_TAIL) {

@@ -25,8 +25,18 @@ constexpr uint32_t P_INV_NEG = 0x7effffffu;  // -p^-1 mod 2^32
 constexpr uint32_t MONT_ONE = 0x01fffffeu;   // 2^32 mod p
 constexpr uint32_t R2 = 0x17f7efe4u;         // 2^64 mod p (to_mont helper)
 
-LG_HD uint32_t add(uint32_t a, uint32_t b) { uint32_t s = a + b; return s >= P ? s - P : s; }
-LG_HD uint32_t sub(uint32_t a, uint32_t b) { uint32_t d = a - b; return a < b ? d + P : d; }
+// Reductions use min(x, x - p) on unsigned words: when x < p the
+// subtraction wraps above x, so the minimum is the reduced value without a
+// branch or predicate.
+LG_HD uint32_t umin(uint32_t a, uint32_t b) {
+#ifdef __CUDA_ARCH__
+  return ::min(a, b);
+#else
+  return a < b ? a : b;
+#endif
+}
+LG_HD uint32_t add(uint32_t a, uint32_t b) { uint32_t s = a + b; return umin(s, s - P); }
+LG_HD uint32_t sub(uint32_t a, uint32_t b) { uint32_t d = a - b; return umin(d, d + P); }
 LG_HD uint32_t neg(uint32_t a) { return a ? P - a : 0; }
 LG_HD uint32_t dbl(uint32_t a) { return add(a, a); }
 
@@ -36,7 +46,7 @@ LG_HD uint32_t mul(uint32_t a, uint32_t b) {
   uint32_t m = (uint32_t)t * P_INV_NEG;
   uint64_t u = t + (uint64_t)m * P;
   uint32_t r = (uint32_t)(u >> 32);
-  return r >= P ? r - P : r;
+  return umin(r, r - P);
 }
 LG_HD uint32_t sqr(uint32_t a) { return mul(a, a); }
 LG_HD uint32_t to_mont(uint32_t canonical) { return mul(canonical % P, R2); }

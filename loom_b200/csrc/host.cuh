@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -46,6 +47,7 @@ struct DBuf {
   uint32_t* p = nullptr;
   size_t words = 0;
   cudaStream_t st = nullptr;
+  bool borrowed = false;  // caller-owned memory: never freed here
   DBuf() = default;
   DBuf(size_t w, cudaStream_t s) : words(w), st(s) {
     if (w) LG_CK(cudaMallocAsync((void**)&p, w * 4, s));
@@ -54,12 +56,16 @@ struct DBuf {
   DBuf& operator=(const DBuf&) = delete;
   DBuf(DBuf&& o) noexcept { *this = std::move(o); }
   DBuf& operator=(DBuf&& o) noexcept {
-    if (this != &o) { release(); p = o.p; words = o.words; st = o.st; o.p = nullptr; o.words = 0; }
+    if (this != &o) {
+      release();
+      p = o.p; words = o.words; st = o.st; borrowed = o.borrowed;
+      o.p = nullptr; o.words = 0;
+    }
     return *this;
   }
   ~DBuf() { release(); }
   void release() {
-    if (p) cudaFreeAsync(p, st);
+    if (p && !borrowed) cudaFreeAsync(p, st);
     p = nullptr;
     words = 0;
   }
@@ -93,6 +99,16 @@ struct Ctx {
       event_pool.push_back(e);
     }
     return event_pool[event_next++];
+  }
+  // Host wall time per prove phase (milliseconds), recorded when profiling.
+  std::vector<std::pair<std::string, double>> phases;
+  std::chrono::steady_clock::time_point phase_t0;
+  void phase_start() { phase_t0 = std::chrono::steady_clock::now(); phases.clear(); }
+  void phase(const char* name) {
+    if (!profiling) return;
+    auto now = std::chrono::steady_clock::now();
+    phases.emplace_back(name, std::chrono::duration<double, std::milli>(now - phase_t0).count());
+    phase_t0 = now;
   }
   template <class F> void timed(const char* name, double bytes, double perms, F launch) {
     if (!profiling) { launch(); return; }
@@ -167,6 +183,9 @@ struct Ctx {
   // One launch per phase over all groups / modules of a size (true), or one
   // launch per group / module (false, the plain per-kernel prover).
   bool batched = true;
+  // Leaf hashing: 0 = choose by the amount of parallelism, 1 = one thread per
+  // permutation, 6 = six lanes per permutation.
+  int leaf_mapping = 0;
 };
 
 // ---------------------------------------------------------------- program
@@ -302,15 +321,40 @@ inline E6 digest_e6(const Digest& d) { E6 r; for (int i = 0; i < 6; i++) r.c[i] 
 
 // ---------------------------------------------------------------- proof writer
 // Canonical encoding: 4-byte big-endian words, field elements canonical.
+// `el*` take Montgomery words; `raw*` take words already canonical.
 struct Writer {
   std::vector<uint8_t> b;
-  void u32(uint32_t x) { for (int i = 3; i >= 0; i--) b.push_back((uint8_t)(x >> (8 * i))); }
-  void el(uint32_t m) { u32(from_mont(m)); }
+  size_t off = 0;
+  void reserve(size_t bytes) { if (b.size() < off + bytes) b.resize(std::max(b.size() * 2, off + bytes)); }
+  void put(uint32_t x) {
+    reserve(4);
+    uint32_t be = __builtin_bswap32(x);
+    memcpy(b.data() + off, &be, 4);
+    off += 4;
+  }
+  void u32(uint32_t x) { put(x); }
+  void el(uint32_t m) { put(from_mont(m)); }
   void e6(const E6& x) { for (int i = 0; i < 6; i++) el(x.c[i]); }
   void e6w(const uint32_t* w) { for (int i = 0; i < 6; i++) el(w[i]); }
   void dg(const Digest& d) { for (int i = 0; i < 8; i++) el(d.v[i]); }
   void dgw(const uint32_t* w) { for (int i = 0; i < 8; i++) el(w[i]); }
-  void str(const std::string& s) { u32((uint32_t)s.size()); b.insert(b.end(), s.begin(), s.end()); }
+  void raw(uint32_t canonical) { put(canonical); }
+  void raww(const uint32_t* w, size_t n) {
+    reserve(4 * n);
+    uint8_t* p = b.data() + off;
+    for (size_t i = 0; i < n; i++) {
+      uint32_t be = __builtin_bswap32(w[i]);
+      memcpy(p + 4 * i, &be, 4);
+    }
+    off += 4 * n;
+  }
+  void str(const std::string& s) {
+    put((uint32_t)s.size());
+    reserve(s.size());
+    memcpy(b.data() + off, s.data(), s.size());
+    off += s.size();
+  }
+  std::vector<uint8_t> take() { b.resize(off); return std::move(b); }
 };
 
 }  // namespace lg

@@ -5,7 +5,7 @@
 #include <cuda_runtime.h>
 
 #include "field.cuh"
-#include "poseidon2.cuh"
+#include "p2_coop.cuh"
 
 namespace lg {
 
@@ -156,7 +156,9 @@ __device__ __forceinline__ uint32_t leaf_elem(const LeafGroup& g, uint32_t idx, 
   return g.ext[e * g.stride + 2 * k + h];
 }
 
-__global__ void k_hash_leaves(const LeafGroup* groups) {
+// One thread per leaf: the fewest instructions per permutation, for launches
+// with enough leaves to fill the GPU.
+__global__ void k_hash_leaves1(const LeafGroup* groups) {
   const LeafGroup g = groups[blockIdx.y];
   uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= g.n_leaves) return;
@@ -176,89 +178,159 @@ __global__ void k_hash_leaves(const LeafGroup* groups) {
   for (int i = 0; i < 8; i++) o[i] = s[i];
 }
 
+// Cooperative form: six lanes per leaf (p2_coop.cuh), five leaves per warp.
+constexpr uint32_t P2_GROUPS_PER_WARP = 5;
+
+__global__ void k_hash_leaves(const LeafGroup* groups) {
+  __shared__ uint32_t keys[144];
+  p2_load_full_keys(keys);
+  P2Lane L;
+  L.init();
+  const LeafGroup g = groups[blockIdx.y];
+  const uint32_t warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  const uint32_t k = (blockIdx.x * warps + warp) * P2_GROUPS_PER_WARP + (uint32_t)L.base / 6;
+  const bool active = L.lane < 30 && k < g.n_leaves;
+  const uint32_t total = 3 + 2 * g.nb + 12 * g.ne;
+  const uint32_t h0 = to_mont(LEAF_TAG), h1 = to_mont(2 * g.nb), h2 = to_mont(2 * g.ne);
+  uint32_t x[4] = {0, 0, 0, 0};
+  for (uint32_t b = 0; b < total; b += 16) {
+    if (active && L.idx < 4) {
+#pragma unroll
+      for (uint32_t i = 0; i < 4; i++) {
+        uint32_t e = b + 4 * L.idx + i;
+        if (e < total) x[i] = leaf_elem(g, e, k, h0, h1, h2);
+      }
+    }
+    p2c_permute(x, L, keys);
+  }
+  if (active && L.idx < 2) {
+    uint32_t* o = g.out + (uint64_t)k * 8 + 4 * L.idx;
+#pragma unroll
+    for (int i = 0; i < 4; i++) o[i] = x[i];
+  }
+}
+
 // ---------------------------------------------------------------- Merkle
 // nodes: 1-indexed, 8 words per node.  Level step: node i = H(2i, 2i+1) for
 // i in [start, 2 start); injection fold: node start+j = H(node, inj[j]),
 // several injections of the same width chained in schedule order
-// (internal/merkle/tree.go:210-327).
+// (internal/merkle/tree.go:210-327).  Six lanes per node.
+
+// Loads digest words into the left (idx 2, 3) or right (idx 4, 5) slot.
+__device__ __forceinline__ void p2c_load_slot(uint32_t x[4], const P2Lane& L, int slot, const uint32_t* digest,
+                                              bool active) {
+  if (active && (L.idx >> 1) == slot) {
+    const uint32_t* d = digest + 4 * (L.idx & 1);
+#pragma unroll
+    for (int i = 0; i < 4; i++) x[i] = d[i];
+  }
+}
+__device__ __forceinline__ void p2c_store_digest(const uint32_t x[4], const P2Lane& L, uint32_t* digest, bool active) {
+  if (active && L.idx < 2) {
+    uint32_t* d = digest + 4 * L.idx;
+#pragma unroll
+    for (int i = 0; i < 4; i++) d[i] = x[i];
+  }
+}
+
+__device__ __forceinline__ void merkle_node(uint32_t* nodes, uint64_t id, const P2Lane& L, const uint32_t* keys,
+                                            bool active) {
+  uint32_t x[4] = {0, 0, 0, 0};
+  p2c_load_slot(x, L, 1, nodes + 2 * id * 8, active);
+  p2c_load_slot(x, L, 2, nodes + (2 * id + 1) * 8, active);
+  p2c_compress(x, L, keys);
+  p2c_store_digest(x, L, nodes + id * 8, active);
+}
+
+// node = H(... H(H(node, inj_0[j]), inj_1[j]) ..., inj_{n-1}[j])
+__device__ __forceinline__ void merkle_chain(uint32_t* nodes, uint64_t id, uint32_t j, const uint32_t* const* inj,
+                                             uint32_t n_inj, const P2Lane& L, const uint32_t* keys, bool active) {
+  if (n_inj == 0) return;
+  uint32_t x[4] = {0, 0, 0, 0};
+  p2c_load_slot(x, L, 1, nodes + id * 8, active);
+  for (uint32_t t = 0; t < n_inj; t++) {
+    p2c_load_slot(x, L, 2, inj[t] + (uint64_t)j * 8, active);
+    p2c_compress(x, L, keys);
+    if (t + 1 < n_inj) p2c_digest_to_left(x, L);
+  }
+  p2c_store_digest(x, L, nodes + id * 8, active);
+}
+
 __global__ void k_merkle_level(uint32_t* nodes, uint32_t start) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= start) return;
-  uint64_t id = start + i;
-  uint32_t l[8], r[8], o[8];
-#pragma unroll
-  for (int q = 0; q < 8; q++) { l[q] = nodes[2 * id * 8 + q]; r[q] = nodes[(2 * id + 1) * 8 + q]; }
-  p2_compress(to_mont(NODE_TAG), l, r, o);
-#pragma unroll
-  for (int q = 0; q < 8; q++) nodes[id * 8 + q] = o[q];
+  __shared__ uint32_t keys[144];
+  p2_load_full_keys(keys);
+  P2Lane L;
+  L.init();
+  const uint32_t warps = blockDim.x >> 5;
+  const uint32_t i = (blockIdx.x * warps + (threadIdx.x >> 5)) * P2_GROUPS_PER_WARP + (uint32_t)L.base / 6;
+  merkle_node(nodes, (uint64_t)start + i, L, keys, L.lane < 30 && i < start);
 }
 
 __global__ void k_merkle_inject(uint32_t* nodes, uint32_t start, const uint32_t* const* inj, uint32_t n_inj) {
-  uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= start) return;
-  uint64_t id = start + j;
-  uint32_t cur[8], r[8];
-#pragma unroll
-  for (int q = 0; q < 8; q++) cur[q] = nodes[id * 8 + q];
-  const uint32_t tag = to_mont(NODE_TAG);
-  for (uint32_t t = 0; t < n_inj; t++) {
-    const uint32_t* leaf = inj[t] + (uint64_t)j * 8;
-#pragma unroll
-    for (int q = 0; q < 8; q++) r[q] = leaf[q];
-    p2_compress(tag, cur, r, cur);
-  }
-#pragma unroll
-  for (int q = 0; q < 8; q++) nodes[id * 8 + q] = cur[q];
+  __shared__ uint32_t keys[144];
+  p2_load_full_keys(keys);
+  P2Lane L;
+  L.init();
+  const uint32_t warps = blockDim.x >> 5;
+  const uint32_t j = (blockIdx.x * warps + (threadIdx.x >> 5)) * P2_GROUPS_PER_WARP + (uint32_t)L.base / 6;
+  merkle_chain(nodes, (uint64_t)start + j, j, inj, n_inj, L, keys, L.lane < 30 && j < start);
 }
 
-// Upper tree levels in one block: for start, start/2, ..., 1: the 2-to-1
+// Upper tree levels in one block: for each width below `top`: the 2-to-1
 // step, then the injections of that width in schedule order.  When
-// fold_first, the injections of width `start` fold first (a tree whose leaf
+// fold_first, the injections of width `top` fold first (a tree whose leaf
 // level fits in one block).
 struct InjRef { const uint32_t* leaves; uint32_t width; };
-__global__ void k_merkle_tail(uint32_t* nodes, uint32_t start, int fold_first, const InjRef* inj, uint32_t n_inj) {
-  const uint32_t tag = to_mont(NODE_TAG);
+__global__ void k_merkle_tail(uint32_t* nodes, uint32_t top, int fold_first, const InjRef* inj, uint32_t n_inj) {
+  __shared__ uint32_t keys[144];
+  __shared__ const uint32_t* chain[64];
+  p2_load_full_keys(keys);
+  P2Lane L;
+  L.init();
+  const uint32_t warp = threadIdx.x >> 5, warps = blockDim.x >> 5, per = warps * P2_GROUPS_PER_WARP;
+  const uint32_t grp = warp * P2_GROUPS_PER_WARP + (uint32_t)L.base / 6;
   auto fold = [&](uint32_t w) {
-    for (uint32_t j = threadIdx.x; j < w; j += blockDim.x) {
-      uint64_t id = w + j;
-      uint32_t cur[8], r[8];
-      for (int q = 0; q < 8; q++) cur[q] = nodes[id * 8 + q];
-      bool any = false;
-      for (uint32_t t = 0; t < n_inj; t++) {
-        if (inj[t].width != w) continue;
-        for (int q = 0; q < 8; q++) r[q] = inj[t].leaves[(uint64_t)j * 8 + q];
-        p2_compress(tag, cur, r, cur);
-        any = true;
+    uint32_t cnt = 0;
+    for (uint32_t t = 0; t < n_inj && cnt < 64; t++)
+      if (inj[t].width == w) {
+        if (threadIdx.x == 0) chain[cnt] = inj[t].leaves;
+        cnt++;
       }
-      if (any)
-        for (int q = 0; q < 8; q++) nodes[id * 8 + q] = cur[q];
-    }
+    __syncthreads();
+    if (cnt)
+      for (uint32_t j0 = warp * P2_GROUPS_PER_WARP; j0 < w; j0 += per) {
+        uint32_t j = j0 + (uint32_t)L.base / 6;
+        merkle_chain(nodes, (uint64_t)w + j, j, chain, cnt, L, keys, L.lane < 30 && j < w);
+      }
     __syncthreads();
   };
-  if (fold_first) fold(start);
-  for (uint32_t w = start >> 1; w >= 1; w >>= 1) {
-    for (uint32_t i = threadIdx.x; i < w; i += blockDim.x) {
-      uint64_t id = w + i;
-      uint32_t l[8], r[8], o[8];
-      for (int q = 0; q < 8; q++) { l[q] = nodes[2 * id * 8 + q]; r[q] = nodes[(2 * id + 1) * 8 + q]; }
-      p2_compress(tag, l, r, o);
-      for (int q = 0; q < 8; q++) nodes[id * 8 + q] = o[q];
+  if (fold_first) fold(top);
+  for (uint32_t w = top >> 1; w >= 1; w >>= 1) {
+    for (uint32_t i0 = warp * P2_GROUPS_PER_WARP; i0 < w; i0 += per) {
+      uint32_t i = i0 + (uint32_t)L.base / 6;
+      merkle_node(nodes, (uint64_t)w + i, L, keys, L.lane < 30 && i < w);
     }
     __syncthreads();
     fold(w);
   }
+  (void)grp;
 }
 
-// Permutation test hook: one state of 24 words per thread.
+// Permutation test hook: one state of 24 words per group of six lanes.
 __global__ void k_p2_permute(uint32_t* states, uint64_t n) {
-  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  uint32_t s[24];
-#pragma unroll
-  for (int q = 0; q < 24; q++) s[q] = states[i * 24 + q];
-  p2_permute(s);
-#pragma unroll
-  for (int q = 0; q < 24; q++) states[i * 24 + q] = s[q];
+  __shared__ uint32_t keys[144];
+  p2_load_full_keys(keys);
+  P2Lane L;
+  L.init();
+  const uint64_t warps = blockDim.x >> 5;
+  const uint64_t i = (blockIdx.x * warps + (threadIdx.x >> 5)) * P2_GROUPS_PER_WARP + (uint64_t)L.base / 6;
+  const bool active = L.lane < 30 && i < n;
+  uint32_t x[4] = {0, 0, 0, 0};
+  if (active)
+    for (int q = 0; q < 4; q++) x[q] = states[i * 24 + 4 * L.idx + q];
+  p2c_permute(x, L, keys);
+  if (active)
+    for (int q = 0; q < 4; q++) states[i * 24 + 4 * L.idx + q] = x[q];
 }
 
 // ---------------------------------------------------------------- expressions
@@ -603,6 +675,12 @@ __global__ void k_fold(const uint32_t* layer, uint64_t n, E6 alpha, const uint32
 }
 
 // ---------------------------------------------------------------- openings
+// Montgomery -> canonical, in place (proof encoding of gathered openings).
+__global__ void k_from_mont(uint32_t* x, uint64_t n) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i < n) x[i] = from_mont(x[i]);
+}
+
 // Row pairs: for every query q and source, the rows (lo, lo+1) of each lane,
 // lo = (s_q >> shift) & ~1, written at out[q * per_q + off + 2 lane + h].
 struct RowSrc { const uint32_t* lane0; uint64_t lane_stride; uint32_t n_lanes; uint32_t shift; uint64_t off; };

@@ -107,6 +107,14 @@ int lg_ctx_set_batched(lg_ctx* ctx, int batched) {
   return guarded(ctx, [&] { ctx->c.batched = batched != 0; });
 }
 
+int lg_ctx_set_leaf_mapping(lg_ctx* ctx, int lanes_per_permutation) {
+  return guarded(ctx, [&] {
+    if (lanes_per_permutation != 0 && lanes_per_permutation != 1 && lanes_per_permutation != 6)
+      throw Error(LG_ERR_INVALID, "leaf mapping must be 0 (auto), 1 or 6 lanes per permutation");
+    ctx->c.leaf_mapping = lanes_per_permutation;
+  });
+}
+
 const char* lg_last_error(lg_ctx* ctx) { return ctx ? ctx->c.err.c_str() : "null context"; }
 
 int lg_prove(lg_ctx* ctx, const char* hash_backend, const uint32_t* program, size_t program_words,
@@ -196,7 +204,7 @@ int lg_poseidon2_permute(lg_ctx* ctx, uint32_t* states, uint64_t n_states, int o
     if (!states) throw Error(LG_ERR_INVALID, "null argument");
     if (!n_states) return;
     auto b = to_device(c, states, 24 * n_states, on_device);
-    k_p2_permute<<<(unsigned)((n_states + 127) / 128), 128, 0, c.stream>>>(b->p, n_states);
+    k_p2_permute<<<(unsigned)((n_states + 19) / 20), 128, 0, c.stream>>>(b->p, n_states);
     LG_LAUNCH();
     from_device(c, states, b->p, 24 * n_states, on_device);
   });
@@ -332,7 +340,14 @@ int lg_profile_report(lg_ctx* ctx, char* buf, size_t* len) {
                kv.second.bytes, kv.second.perms);
       js += tmp;
     }
-    js += "}";
+    js += js.size() > 1 ? ", " : "";
+    js += "\"phases\": {";
+    for (size_t i = 0; i < ctx->c.phases.size(); i++) {
+      char tmp[160];
+      snprintf(tmp, sizeof tmp, "%s\"%s\": %.4f", i ? ", " : "", ctx->c.phases[i].first.c_str(), ctx->c.phases[i].second);
+      js += tmp;
+    }
+    js += "}}";
     if (!buf || *len < js.size() + 1) {
       *len = js.size() + 1;
       throw Error(LG_ERR_BUFFER, "report buffer too small");

@@ -7,7 +7,9 @@
 namespace lg {
 
 inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool on_device) {
+  c.phase_start();
   setup(witness, on_device);
+  c.phase("setup+upload");
   const uint32_t R = pg.n_rounds;
   for (uint32_t r = 0; r < R; r++) fs.add(coin_name(r));
   fs.add("__zeta");
@@ -32,6 +34,7 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
       ti++;
     }
     coins[r] = digest_e6(fs.compute(coin_name(r)));
+    c.phase(("round " + std::to_string(r)).c_str());
   }
   // ---- AIR quotients and their commitment (prover/prover.go:461-561)
   quotient_all();
@@ -43,6 +46,7 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
     ti++;
   }
   zeta = digest_e6(fs.compute("__zeta"));
+  c.phase("quotient+air commit");
 
   // ---- claimed values P(zeta w^s) from coefficients (internal/fri/values.go:46-110)
   struct Poly { size_t t, g; bool ext; const uint32_t* coef; uint32_t logn; std::vector<int> shifts; };
@@ -137,6 +141,7 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
         for (auto& vals : cv[t][g]) for (auto& v : vals) fs.bind("alpha_DEEP", v.c, 6);
       }
   E6 alpha = digest_e6(fs.compute("alpha_DEEP"));
+  c.phase("claimed values+bind");
 
   // ---- DEEP codewords on the LDE rows (internal/fri/deep.go:71-266)
   std::vector<DBufP> deep(classes.size());
@@ -210,6 +215,7 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
   if (c.batched) launch_deep(0, djobs.size());
   else for (size_t i = 0; i < djobs.size(); i++) launch_deep(i, 1);
 
+  c.phase("deep");
   // ---- FRI (internal/fri/fri.go:352-365,606-736)
   std::vector<size_t> class_at(classes.size());
   for (size_t i = 0; i < class_at.size(); i++) class_at[i] = i;
@@ -242,6 +248,7 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
     else for (auto& g : lgs) launch_leaves(c, {g});
   }
   build_tree(c, levels_tree);
+  c.phase("levels tree");
   std::vector<E6> gam(L);
   for (size_t l = 1; l < L; l++) {
     std::string nm = "fri_level_" + std::to_string(l) + "_gamma";
@@ -309,6 +316,7 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
     for (size_t i = 0; i < nj; i++) for (int w = 0; w < 6; w++) fin.push_back(final_poly[w * nj + i]);
     fs.bind("fri_query_0", fin.data(), fin.size());
   }
+  c.phase("fri rounds");
   std::vector<uint32_t> pos(num_queries);
   for (uint32_t k = 0; k < num_queries; k++) {
     Digest ch = fs.compute("fri_query_" + std::to_string(k));
@@ -317,6 +325,7 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
     if (k + 1 < num_queries) fs.bind("fri_query_" + std::to_string(k + 1), ch.v, 8);
   }
 
+  c.phase("query challenges");
   // ---- openings: one gather into a staging buffer, one read-back
   std::vector<RowSrc> rows;
   std::vector<PathSrc> paths;
@@ -376,11 +385,15 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
         (const PathSrc*)pd->p, pos_d->p, num_queries, per_q, out_d->p);
     LG_LAUNCH();
   }
+  k_from_mont<<<(unsigned)((per_q * num_queries + 255) / 256), 256, 0, c.stream>>>(out_d->p, per_q * num_queries);
+  LG_LAUNCH();
   uint32_t* G = c.host_staging(per_q * num_queries);
   c.d2h(G, out_d->p, per_q * num_queries);
 
+  c.phase("openings gather");
   // ---- canonical encoding (same order as the proof structs)
   Writer W;
+  W.reserve((size_t)4 * per_q * num_queries + (1 << 20));
   W.str("poseidon2");
   W.u32(0);
   W.u32((uint32_t)commitments.size());
@@ -397,18 +410,19 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
       for (size_t i = nbp; i < cv[t][g].size(); i++) { W.u32((uint32_t)cv[t][g][i].size()); for (auto& v : cv[t][g][i]) W.e6(v); }
     }
   }
+  // gathered words are already canonical (k_from_mont)
   auto wpair_e6 = [&](const uint32_t* q, uint64_t off) {  // lane-major (lo, hi) pairs of 6 lanes
     uint32_t lo[6], hi[6];
     for (int w = 0; w < 6; w++) { lo[w] = q[off + 2 * w]; hi[w] = q[off + 2 * w + 1]; }
-    W.e6w(lo);
-    W.e6w(hi);
+    W.raww(lo, 6);
+    W.raww(hi, 6);
   };
   auto wpath = [&](const uint32_t* q, uint64_t off, uint32_t leaf, uint32_t depth, uint32_t ninj) {
     W.u32(leaf);
     W.u32(depth);
-    for (uint32_t k = 0; k < depth; k++) W.dgw(q + off + 8 * k);
+    W.raww(q + off, 8 * (size_t)depth);
     W.u32(ninj);
-    for (uint32_t k = 0; k < ninj; k++) W.dgw(q + off + 8 * (depth + k));
+    W.raww(q + off + 8 * (size_t)depth, 8 * (size_t)ninj);
   };
   W.dg(levels_tree.root);
   W.u32((uint32_t)(L - 1));
@@ -451,12 +465,19 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
         const Group& G2 = trees[b].groups[gi];
         uint32_t nb = (uint32_t)G2.bcols.size(), ne = (uint32_t)G2.ecols.size();
         (void)l;
+        uint32_t tmp[512];
         for (int h = 0; h < 2; h++) {
           W.u32(nb);
-          for (uint32_t i = 0; i < nb; i++) W.el(q[off + 2 * i + h]);
+          for (uint32_t i0 = 0; i0 < nb; i0 += 512) {
+            uint32_t k = std::min<uint32_t>(512, nb - i0);
+            for (uint32_t i = 0; i < k; i++) tmp[i] = q[off + 2 * (i0 + i) + h];
+            W.raww(tmp, k);
+          }
           W.u32(ne);
-          for (uint32_t e = 0; e < ne; e++)
-            for (int w = 0; w < 6; w++) W.el(q[off + 2 * (nb + 6 * e + w) + h]);
+          for (uint32_t e = 0; e < ne; e++) {
+            for (int w = 0; w < 6; w++) tmp[w] = q[off + 2 * (nb + 6 * e + w) + h];
+            W.raww(tmp, 6);
+          }
         }
       };
       const LdeOut& top = cm.groups[cm.order[0]];
@@ -468,7 +489,8 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
     }
   }
   LG_CK(cudaStreamSynchronize(c.stream));
-  return W.b;
+  c.phase("serialize");
+  return W.take();
 }
 
 }  // namespace lg

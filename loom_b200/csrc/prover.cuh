@@ -174,10 +174,18 @@ struct Prover {
       size_t n = mod_n(cl.module);
       if (cl.kind == KIND_WITNESS) {
         if (cl.field != 0) throw Error(LG_ERR_UNSUPPORTED, "extension-field witness columns are not supported");
-        auto b = std::make_shared<DBuf>(n, c.stream);
-        LG_CK(cudaMemcpyAsync(b->p, witness[wi++], n * 4, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-                              c.stream));
-        col_buf[col] = b;
+        if (on_device) {
+          // read-only input: use the caller's device buffer as it is
+          auto b = std::make_shared<DBuf>();
+          b->p = const_cast<uint32_t*>(witness[wi++]);
+          b->words = n;
+          b->borrowed = true;
+          col_buf[col] = b;
+        } else {
+          auto b = std::make_shared<DBuf>(n, c.stream);
+          LG_CK(cudaMemcpyAsync(b->p, witness[wi++], n * 4, cudaMemcpyHostToDevice, c.stream));
+          col_buf[col] = b;
+        }
       } else if (cl.kind == KIND_LAGRANGE) {
         int64_t row = cl.param >= 0 ? cl.param : (int64_t)n - 1 - (-(int64_t)cl.param - 1);
         if (row < 0 || row >= (int64_t)n) throw Error(LG_ERR_INVALID, "Lagrange column row out of range");

@@ -119,6 +119,18 @@ def test_prove_uneven_modules(ctx, batched):
     assert got == oracle.prove(compiled.words, mont, 20)
 
 
+@pytest.mark.parametrize("mapping", [1, 6])
+def test_leaf_mappings_agree(ctx, mapping):
+    compiled, wit = plonk.build(3, 1 << 11, seed=21)
+    mont = [F.to_mont(w) for w in wit]
+    ctx.set_leaf_mapping(mapping)
+    try:
+        got = ctx.prove(compiled.words, mont, 9)
+    finally:
+        ctx.set_leaf_mapping(0)
+    assert got == oracle.prove(compiled.words, mont, 9)
+
+
 def test_repeated_proves_identical(ctx):
     compiled, wit = plonk.build(2, 1 << 9, seed=3)
     mont = [F.to_mont(w) for w in wit]
