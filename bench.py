@@ -42,6 +42,8 @@ def parse():
     ap.add_argument("--queries", type=int, default=200)
     ap.add_argument("--cpu-sample", type=int, default=4, help="instances in the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--streams", type=str, default="2,4",
+                    help="concurrent proof streams for the throughput measurement")
     return ap.parse_args()
 
 
@@ -230,6 +232,26 @@ def main():
     assert pbh == pb, "host-buffer and device-buffer proofs differ"
     assert pbp == pb, "plain and batched proofs differ"
 
+    # ---- throughput: several proofs in flight, one context + stream each
+    from loom_b200.pool import ProverPool
+    thr = []
+    for S in [int(x) for x in a.streams.split(",") if x]:
+        with ProverPool(S, device) as pool:
+            for f in [pool.submit(comp.words, dev_ptrs, a.queries, on_device=True) for _ in range(S)]:
+                f.result()  # warm every context
+            jobs = S * max(2, a.steps)
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            futs = [pool.submit(comp.words, dev_ptrs, a.queries, on_device=True) for _ in range(jobs)]
+            outs = [f.result() for f in futs]
+            e1.record()
+            torch.cuda.synchronize()
+            assert all(o == pb for o in outs), "concurrent proofs differ from the single-stream proof"
+            wall = e0.elapsed_time(e1)
+            thr.append({"streams": S, "proofs": jobs, "ms": round(wall, 3), "proofs_per_s": round(jobs * 1e3 / wall, 3)})
+
     # ---- per-kernel events over a profiled step (roofline of the dominant kernel)
     flush.fill_(1)
     torch.cuda.synchronize()
@@ -310,6 +332,8 @@ def main():
             "plain": {"value": round(plain_ms, 3), "unit": "ms",
                       "note": "same kernels, one launch per group / module (the plain per-kernel prover)"},
             "batched_speedup_vs_plain": round(plain_ms / ms, 3),
+            "throughput": thr,
+            "best_throughput_vs_plain": round(max([t["proofs_per_s"] for t in thr] + [1e3 / ms]) * plain_ms / 1e3, 3),
             "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": h2d_bytes,
                     "d2h_bytes_per_step": len(pbh)},
             "gpu_launches": int(launches),
