@@ -2,6 +2,7 @@
 // every lane, pair-leaf Poseidon2 hashing, Merkle tree with level injections.
 #pragma once
 #include "host.cuh"
+#include "ntt_large.cuh"
 
 namespace lg {
 
@@ -20,17 +21,86 @@ template <class K> inline void allow_smem(K kernel, size_t bytes) {
 
 inline int ntt_threads(int logn) { return std::max(32, std::min(512, 1 << std::max(0, logn - 1))); }
 
+constexpr int MAX_NTT_LOG = 22;  // the largest loom module, 2^22 rows
 inline void check_ntt_size(int logn) {
-  if (logn > SMEM_NTT_MAX_LOG)
-    throw Error(LG_ERR_UNSUPPORTED, "module sizes above 2^" + std::to_string(SMEM_NTT_MAX_LOG) +
-                                        " rows are not supported by this build");
+  if (logn > MAX_NTT_LOG) throw Error(LG_ERR_UNSUPPORTED, "transforms above 2^22 points are not supported");
 }
 
-// One k_lde launch over lanes that share a size.
+// Runs four-step transforms of 2^logn points (logn > SMEM_NTT_MAX_LOG), all
+// jobs of one direction, in chunks whose scratch stays below 256 MiB.
+inline void big_ntt(Ctx& c, std::vector<BigNtt> jobs, int logn, bool inverse, const char* tag, double bytes_per_job) {
+  if (jobs.empty()) return;
+  const int logr = logn / 2, logc = logn - logr;
+  const size_t n = (size_t)1 << logn;
+  const uint32_t* tw_n = c.twiddles(logn);
+  const uint32_t* tw_c = c.twiddles(logc);
+  const uint32_t* tw_r = c.twiddles(logr);
+  const size_t per = std::max<size_t>(1, ((size_t)1 << 26) / n);
+  allow_smem(k_big_pass_a, ((size_t)BIG_TILE << logc) * 4);
+  allow_smem(k_big_pass_b, ((size_t)BIG_TILE << logr) * 4);
+  for (size_t first = 0; first < jobs.size(); first += per) {
+    size_t cnt = std::min(per, jobs.size() - first);
+    auto scratch = std::make_shared<DBuf>(cnt * n, c.stream);
+    std::vector<BigNtt> v(jobs.begin() + first, jobs.begin() + first + cnt);
+    for (size_t i = 0; i < cnt; i++) v[i].scratch = scratch->p + i * n;
+    auto jd = upload_vec(c, v);
+    c.timed(tag, bytes_per_job * cnt, 0, [&] {
+      k_big_pass_a<<<dim3((1u << logr) / BIG_TILE, (unsigned)cnt), 512, ((size_t)BIG_TILE << logc) * 4, c.stream>>>(
+          (const BigNtt*)jd->p, logn, logr, logc, inverse ? 1 : 0, tw_n, tw_c);
+      LG_LAUNCH();
+      k_big_pass_b<<<dim3((1u << logc) / BIG_TILE, (unsigned)cnt), 512, ((size_t)BIG_TILE << logr) * 4, c.stream>>>(
+          (const BigNtt*)jd->p, logr, logc, inverse ? 1 : 0, tw_r);
+      LG_LAUNCH();
+    });
+  }
+}
+
+inline BigNtt big_job(const uint32_t* in, uint32_t* out, uint32_t c0, bool bitrev_out) {
+  BigNtt j{};
+  j.in = in;
+  j.out = out;
+  j.c0 = c0;
+  j.out_bitrev = bitrev_out ? 1 : 0;
+  return j;
+}
+
+// One k_lde launch over lanes that share a size (four-step transforms above
+// 2^14 points).
 inline void launch_lde(Ctx& c, const std::vector<LdeLane>& lanes, uint32_t log_n, bool from_coeffs) {
   if (lanes.empty()) return;
   check_ntt_size((int)log_n);
   size_t n = (size_t)1 << log_n;
+  if ((int)log_n > SMEM_NTT_MAX_LOG) {
+    DBufP tmp;
+    std::vector<const uint32_t*> coef(lanes.size());
+    std::vector<BigNtt> inv_jobs, fwd_jobs;
+    bool need_tmp = false;
+    for (auto& L : lanes) need_tmp |= !from_coeffs && !L.coef;
+    if (need_tmp) tmp = std::make_shared<DBuf>(lanes.size() * n, c.stream);
+    for (size_t i = 0; i < lanes.size(); i++) {
+      if (from_coeffs) {
+        coef[i] = lanes[i].src;
+        if (lanes[i].coef)
+          LG_CK(cudaMemcpyAsync(lanes[i].coef, lanes[i].src, n * 4, cudaMemcpyDeviceToDevice, c.stream));
+      } else {
+        uint32_t* dst = lanes[i].coef ? lanes[i].coef : tmp->p + i * n;
+        inv_jobs.push_back(big_job(lanes[i].src, dst, inv(to_mont((uint32_t)n)), false));
+        coef[i] = dst;
+      }
+    }
+    big_ntt(c, inv_jobs, (int)log_n, true, "lde", 8.0 * n);
+    const uint32_t* tw4 = c.twiddles((int)log_n + RATE_LOG);
+    for (size_t i = 0; i < lanes.size(); i++)
+      for (int a = 0; a < (1 << RATE_LOG); a++) {
+        BigNtt j = big_job(coef[i], lanes[i].out + (size_t)a * n, MONT_ONE, true);
+        j.t2 = tw4;
+        j.m2_mask = (uint32_t)((n << RATE_LOG) - 1);
+        j.e2 = bitrev32((uint32_t)a, RATE_LOG);
+        fwd_jobs.push_back(j);
+      }
+    big_ntt(c, fwd_jobs, (int)log_n, false, "lde", 20.0 * n / (1 << RATE_LOG));
+    return;
+  }
   auto tab = upload_vec(c, lanes);
   const uint32_t* twn = c.twiddles((int)log_n);
   const uint32_t* tw4 = c.twiddles((int)log_n + RATE_LOG);

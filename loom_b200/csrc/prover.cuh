@@ -416,13 +416,19 @@ struct Prover {
           LG_CK(cudaMemcpyAsync(b->p, col_buf.at(col)->p, lanes_of(col) * n * 4, cudaMemcpyDeviceToDevice, c.stream));
           std::vector<uint32_t*> ls;
           for (uint32_t w = 0; w < lanes_of(col); w++) ls.push_back(b->p + (size_t)w * n);
-          auto tab = upload_vec(c, ls);
-          allow_smem(k_intt, n * 4);
-          k_intt<<<lanes_of(col), ntt_threads((int)logn), n * 4, c.stream>>>((uint32_t* const*)tab->p, (int)logn,
-                                                                             c.twiddles((int)logn), inv(to_mont((uint32_t)n)));
-          LG_LAUNCH();
+          if ((int)logn > SMEM_NTT_MAX_LOG) {
+            std::vector<BigNtt> jobs;
+            for (uint32_t* l : ls) jobs.push_back(big_job(l, l, inv(to_mont((uint32_t)n)), false));
+            big_ntt(c, jobs, (int)logn, true, "quotient_intt", 8.0 * n);
+          } else {
+            auto tab = upload_vec(c, ls);
+            allow_smem(k_intt, n * 4);
+            k_intt<<<lanes_of(col), ntt_threads((int)logn), n * 4, c.stream>>>((uint32_t* const*)tab->p, (int)logn,
+                                                                               c.twiddles((int)logn), inv(to_mont((uint32_t)n)));
+            LG_LAUNCH();
+            keep.push_back(tab);
+          }
           keep.push_back(b);
-          keep.push_back(tab);
           for (uint32_t w = 0; w < lanes_of(col); w++) coef_lanes.push_back(b->p + (size_t)w * n);
         }
         first_lane[col] = f;
@@ -449,6 +455,22 @@ struct Prover {
       for (auto& kv : by_size) {
         uint32_t logn = kv.first;
         size_t n = (size_t)1 << logn;
+        if ((int)logn > SMEM_NTT_MAX_LOG) {
+          std::vector<BigNtt> jobs;
+          const uint32_t* tw4 = c.twiddles((int)logn + RATE_LOG);
+          const uint32_t* gp = c.gpowers((int)logn, false);
+          for (auto& L : kv.second)
+            for (int cc = 0; cc < 4; cc++) {
+              BigNtt j = big_job(L.src, L.out + (size_t)cc * n, MONT_ONE, false);
+              j.t1 = gp;
+              j.t2 = tw4;
+              j.m2_mask = (uint32_t)((n << RATE_LOG) - 1);
+              j.e2 = (uint32_t)cc;
+              jobs.push_back(j);
+            }
+          big_ntt(c, jobs, (int)logn, false, "coset_eval", 5.0 * n);
+          continue;
+        }
         auto tab = upload_vec(c, kv.second);
         allow_smem(k_coset_eval, n * 4);
         const uint32_t* twn = c.twiddles((int)logn);
@@ -494,6 +516,12 @@ struct Prover {
       }
       for (auto& kv : intt) {
         size_t n = (size_t)1 << kv.first;
+        if ((int)kv.first > SMEM_NTT_MAX_LOG) {
+          std::vector<BigNtt> jobs;
+          for (uint32_t* l : kv.second) jobs.push_back(big_job(l, l, inv(to_mont((uint32_t)n)), false));
+          big_ntt(c, jobs, (int)kv.first, true, "quotient_intt", 8.0 * n);
+          continue;
+        }
         auto tab = upload_vec(c, kv.second);
         allow_smem(k_intt, n * 4);
         const uint32_t* twn = c.twiddles((int)kv.first);

@@ -167,3 +167,40 @@ def test_grand_product(ctx, n):
     num = F.to_mont(rnd((n, 6), n))
     den = F.to_mont(rnd((n, 6), n + 1))
     assert np.array_equal(ctx.grand_product(num, den), oracle.grand_product(num, den))
+
+
+@pytest.mark.parametrize("logn,cols", [(15, 3), (16, 2), (17, 1), (20, 1)])
+def test_rs_encode_large(ctx, logn, cols):
+    c = F.to_mont(rnd((cols, 1 << logn), 300 + logn))
+    got = ctx.rs_encode(c)
+    for i in range(cols):
+        assert np.array_equal(got[i], oracle.rs_encode(c[i], 4 << logn)), (logn, i)
+
+
+def test_commit_root_large_and_small(ctx):
+    groups = [{"rows": 1 << 10, "base": [F.to_mont(rnd(1 << 10, 5))]},
+              {"rows": 1 << 16, "base": [F.to_mont(rnd(1 << 16, 6)), F.to_mont(rnd(1 << 16, 7))],
+               "ext": [F.to_mont(rnd((1 << 16, 6), 8))]},
+              {"rows": 1 << 15, "ext": [F.to_mont(rnd((1 << 15, 6), 9))]}]
+    assert np.array_equal(ctx.commit_root(groups), oracle.commit(groups))
+
+
+def test_prove_large_module(ctx):
+    from loom_b200.program import Builder, Module, col, copy_constraint
+    b = Builder()
+    trace = {}
+    for i, logn in enumerate([15, 10]):
+        n = 1 << logn
+        m = Module(f"plonk_{i}", n)
+        L, R, O = col(f"L_{i}"), col(f"R_{i}"), col(f"O_{i}")
+        QL, QR, QM, QO, QK = (col(f"{s}_{i}") for s in ("QL", "QR", "QM", "QO", "QK"))
+        m.assert_zero(QL * L + QR * R + QM * L * R + QO * O + QK)
+        b.add_module(m)
+        w, S = plonk.instance_witness(n, 17, i)
+        trace.update(w)
+        copy_constraint(b, m.name, [L, R, O], S, f"plonk.S_{i}")
+    trace.update(b.generated)
+    compiled = b.compile()
+    mont = [F.to_mont(trace[name]) for (name, _, _) in compiled.witness_columns]
+    got = ctx.prove(compiled.words, mont, 4)
+    assert got == oracle.prove(compiled.words, mont, 4)
