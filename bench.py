@@ -42,6 +42,10 @@ def parse():
     ap.add_argument("--queries", type=int, default=200)
     ap.add_argument("--cpu-sample", type=int, default=4, help="instances in the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=48, help="requests in the serving measurement (0 = skip)")
+    ap.add_argument("--serve-shapes", type=int, default=8, help="distinct request shapes, replayed in turn")
+    ap.add_argument("--serve-rate", type=str, default="8,16", help="Poisson arrival rates (requests/s) to sweep")
+    ap.add_argument("--serve-streams", type=int, default=4)
     ap.add_argument("--streams", type=str, default="2,4",
                     help="concurrent proof streams for the throughput measurement")
     return ap.parse_args()
@@ -252,6 +256,46 @@ def main():
             wall = e0.elapsed_time(e1)
             thr.append({"streams": S, "proofs": jobs, "ms": round(wall, 3), "proofs_per_s": round(jobs * 1e3 / wall, 3)})
 
+    # ---- serving: requests of mixed sizes (log2 rows 12-20, 1-8 instances) with
+    # Poisson arrivals, admitted by HBM budget, overlapping on the GPU
+    serve_res = None
+    if a.serve_requests > 0 and rank == 0:
+        from loom_b200 import serve as SV
+        rng = np.random.Generator(np.random.PCG64(0x5E4E))
+        shapes = [(int(rng.integers(12, 21)), int(rng.integers(1, 9))) for _ in range(a.serve_shapes)]
+        pool_reqs = [SV.make_request(i, lg, inst, a.queries, seed=0x77 + i) for i, (lg, inst) in enumerate(shapes)]
+        # sequential plain-GPU proving of each shape once (the comparison baseline)
+        pctx = Context(device)
+        pctx.set_batched(False)
+        plain_one = []
+        ref_proof = {}
+        for r in pool_reqs:
+            pctx.prove(r.words, r.witness, r.num_queries)  # warm
+            pctx.mark(6)
+            ref_proof[r.rid] = pctx.prove(r.words, r.witness, r.num_queries)
+            pctx.mark(7)
+            plain_one.append(pctx.elapsed_ms(6, 7))
+        pctx.close()
+        sweeps = []
+        for rate in [float(x) for x in a.serve_rate.split(",") if x]:
+            reqs = []
+            for i in range(a.serve_requests):
+                t = pool_reqs[i % len(pool_reqs)]
+                reqs.append(SV.Request(i, t.words, t.witness, t.num_queries, t.rows))
+            shape_of = {i: i % len(pool_reqs) for i in range(a.serve_requests)}
+            res = SV.serve(reqs, SV.poisson_arrivals(len(reqs), rate, 11), streams=a.serve_streams, device=device)
+            same = all(r.proof == ref_proof[shape_of[r.rid]] for r in res["finished"])
+            seq_ms = sum(plain_one[shape_of[i]] for i in range(a.serve_requests))
+            sweeps.append({"rate_per_s": rate, "requests": res["requests"], "p50_ms": round(res["p50_ms"], 2),
+                           "p99_ms": round(res["p99_ms"], 2), "proofs_per_s": round(res["proofs_per_s"], 2),
+                           "errors": res["errors"], "first_error": res["first_error"],
+                           "proofs_identical_to_alone": same})
+        serve_res = {"shapes": [{"log_rows": lg, "instances": ins} for lg, ins in shapes],
+                     "streams": a.serve_streams, "queries": a.queries,
+                     "sequential_plain_proofs_per_s": round(len(plain_one) * 1e3 / sum(plain_one), 2),
+                     "plain_ms_per_shape": [round(x, 2) for x in plain_one],
+                     "sweep": sweeps}
+
     # ---- per-kernel events over a profiled step (roofline of the dominant kernel)
     flush.fill_(1)
     torch.cuda.synchronize()
@@ -333,6 +377,7 @@ def main():
                       "note": "same kernels, one launch per group / module (the plain per-kernel prover)"},
             "batched_speedup_vs_plain": round(plain_ms / ms, 3),
             "throughput": thr,
+            "serve": serve_res,
             "best_throughput_vs_plain": round(max([t["proofs_per_s"] for t in thr] + [1e3 / ms]) * plain_ms / 1e3, 3),
             "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": h2d_bytes,
                     "d2h_bytes_per_step": len(pbh)},

@@ -76,6 +76,8 @@ int lg_ctx_set_batched(lg_ctx* ctx, int batched);
  * 6 = six lanes of a warp per permutation, 0 = choose from the number of
  * leaves (default).  Results do not depend on it. */
 int lg_ctx_set_leaf_mapping(lg_ctx* ctx, int lanes_per_permutation);
+/* Free and total device memory of the context's GPU (serving admission). */
+int lg_mem_info(lg_ctx* ctx, uint64_t* free_bytes, uint64_t* total_bytes);
 /* NUL-terminated description of the last failure on `ctx` (never NULL). */
 const char* lg_last_error(lg_ctx* ctx);
 

@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libloom_gpu.so")
 
 LG_OK, LG_ERR_INVALID, LG_ERR_CUDA, LG_ERR_OOM, LG_ERR_UNSUPPORTED, LG_ERR_BUFFER = range(6)
-EXPORTS = ["lg_ctx_create", "lg_ctx_destroy", "lg_ctx_set_batched", "lg_ctx_set_leaf_mapping", "lg_last_error", "lg_prove", "lg_last_proof", "lg_commit_root",
+EXPORTS = ["lg_ctx_create", "lg_ctx_destroy", "lg_ctx_set_batched", "lg_ctx_set_leaf_mapping", "lg_mem_info", "lg_last_error", "lg_prove", "lg_last_proof", "lg_commit_root",
            "lg_rs_encode", "lg_poseidon2_permute", "lg_merkle_root", "lg_fri_fold", "lg_timer_mark",
            "lg_timer_elapsed", "lg_kernel_launches", "lg_profile", "lg_profile_report", "lg_grand_product", "lg_grand_product_noalloc"]
 
@@ -46,6 +46,7 @@ def load():
         L.lg_ctx_destroy.restype = None
         L.lg_ctx_set_batched.argtypes = [vp, ctypes.c_int]
         L.lg_ctx_set_leaf_mapping.argtypes = [vp, ctypes.c_int]
+        L.lg_mem_info.argtypes = [vp, u64p, u64p]
         L.lg_last_error.argtypes = [vp]
         L.lg_last_error.restype = ctypes.c_char_p
         L.lg_prove.argtypes = [vp, ctypes.c_char_p, u32p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
@@ -109,6 +110,12 @@ class Context:
         """Batched (default): one launch per phase over all groups/modules;
         plain: one launch per group/module."""
         self._check(self.L.lg_ctx_set_batched(self.h, int(batched)))
+
+    def mem_info(self):
+        """(free, total) device bytes."""
+        f, t = ctypes.c_uint64(), ctypes.c_uint64()
+        self._check(self.L.lg_mem_info(self.h, ctypes.byref(f), ctypes.byref(t)))
+        return int(f.value), int(t.value)
 
     def set_leaf_mapping(self, lanes: int):
         """Poseidon2 leaf hashing: 1 or 6 lanes per permutation, 0 = auto."""

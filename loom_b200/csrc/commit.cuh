@@ -1,6 +1,8 @@
 // PCS commit on the device (internal/fri/commitment.go:259-386): RS/LDE of
 // every lane, pair-leaf Poseidon2 hashing, Merkle tree with level injections.
 #pragma once
+#include <mutex>
+
 #include "host.cuh"
 #include "ntt_large.cuh"
 
@@ -15,8 +17,17 @@ template <class T> inline DBufP upload_vec(Ctx& c, const std::vector<T>& v) {
   return upload_words(c, v.data(), v.size() * sizeof(T));
 }
 
+// The dynamic shared-memory limit is a property of the kernel function, shared
+// by every context and thread in the process: it is only ever raised, so a
+// launch of one context never finds it lowered by another.
+inline std::mutex g_smem_mu;
+inline std::map<const void*, size_t> g_smem_set;
 template <class K> inline void allow_smem(K kernel, size_t bytes) {
+  std::lock_guard<std::mutex> lk(g_smem_mu);
+  size_t& cur = g_smem_set[(const void*)kernel];
+  if (bytes <= cur) return;
   LG_CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  cur = bytes;
 }
 
 inline int ntt_threads(int logn) { return std::max(32, std::min(512, 1 << std::max(0, logn - 1))); }

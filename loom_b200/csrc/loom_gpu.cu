@@ -107,6 +107,15 @@ int lg_ctx_set_batched(lg_ctx* ctx, int batched) {
   return guarded(ctx, [&] { ctx->c.batched = batched != 0; });
 }
 
+int lg_mem_info(lg_ctx* ctx, uint64_t* free_bytes, uint64_t* total_bytes) {
+  return guarded(ctx, [&] {
+    size_t f = 0, t = 0;
+    LG_CK(cudaMemGetInfo(&f, &t));
+    if (free_bytes) *free_bytes = f;
+    if (total_bytes) *total_bytes = t;
+  });
+}
+
 int lg_ctx_set_leaf_mapping(lg_ctx* ctx, int lanes_per_permutation) {
   return guarded(ctx, [&] {
     if (lanes_per_permutation != 0 && lanes_per_permutation != 1 && lanes_per_permutation != 6)

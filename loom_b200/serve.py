@@ -1,0 +1,156 @@
+"""Serving loop: proving requests of mixed sizes arriving over time.
+
+Requests wait in arrival order.  A request starts as soon as a stream slot is
+free and its device-memory estimate fits the HBM budget next to the requests
+already running (continuous batching: no request waits for a batch to drain;
+proofs of different requests overlap on the GPU, one CUDA stream each).  The
+witness of a running request and all its LDEs and trees stay on the device
+until its proof is read back.  Every proof is a pure function of its request,
+so a request's bytes are the same alone and in the mix.
+
+Latency = completion time - arrival time.  Reports p50/p99 and proofs/s.
+"""
+from __future__ import annotations
+
+import heapq
+import threading
+import time
+from dataclasses import dataclass, field
+from typing import Callable, Dict, List, Optional, Sequence
+
+import numpy as np
+
+from . import field as F, plonk
+from ._lib import Context
+
+
+@dataclass
+class Request:
+    rid: int
+    words: np.ndarray
+    witness: List[np.ndarray]     # Montgomery columns, descriptor order
+    num_queries: int
+    rows: int                     # total trace rows (sum over modules)
+    arrival: float = 0.0
+    start: float = 0.0
+    done: float = 0.0
+    proof: Optional[bytes] = None
+    error: Optional[str] = None
+
+
+def device_bytes_estimate(rows: int) -> int:
+    """Peak device bytes of one prove of plonk-like modules totalling `rows`
+    rows: LDEs and coefficients of the committed columns (about 44 lanes per
+    module row group at blowup 4), quotient scratch, DEEP codewords and trees;
+    2.2 KiB per row with headroom."""
+    return int(2304 * rows) + (64 << 20)
+
+
+def make_request(rid: int, log_rows: int, instances: int, num_queries: int, seed: int) -> Request:
+    compiled, wit = plonk.build(instances, 1 << log_rows, seed=seed)
+    mont = [np.ascontiguousarray(F.to_mont(w)) for w in wit]
+    return Request(rid, compiled.words, mont, num_queries, instances << log_rows)
+
+
+class Server:
+    def __init__(self, streams: int = 4, device: int = 0, hbm_budget: Optional[int] = None,
+                 batched: bool = True, context_factory: Optional[Callable[[int], object]] = None):
+        make = context_factory or Context
+        self.contexts = [make(device) for _ in range(streams)]
+        for c in self.contexts:
+            c.set_batched(batched)
+        free, total = self.contexts[0].mem_info()
+        self.budget = hbm_budget if hbm_budget is not None else int(0.8 * free)
+        self.in_use = 0
+        self.cv = threading.Condition()
+        self.queue: List[Request] = []     # arrival order
+        self.idle = list(self.contexts)
+        self.finished: List[Request] = []
+        self.peak_in_use = 0
+        self.t0 = time.perf_counter()
+
+    def now(self) -> float:
+        return time.perf_counter() - self.t0
+
+    def _admit(self) -> List[tuple]:
+        """Head-of-line admission: the oldest request starts when a slot and
+        its memory are free (no reordering, so no request starves)."""
+        started = []
+        while self.queue and self.idle:
+            r = self.queue[0]
+            need = device_bytes_estimate(r.rows)
+            if self.in_use + need > self.budget and self.in_use > 0:
+                break
+            self.queue.pop(0)
+            self.in_use += need
+            self.peak_in_use = max(self.peak_in_use, self.in_use)
+            started.append((r, self.idle.pop(), need))
+        return started
+
+    def _run(self, r: Request, ctx: Context, need: int):
+        r.start = self.now()
+        try:
+            r.proof = ctx.prove(r.words, r.witness, r.num_queries)
+        except Exception as e:  # reported per request
+            r.error = str(e)
+        r.done = self.now()
+        with self.cv:
+            self.in_use -= need
+            self.idle.append(ctx)
+            self.finished.append(r)
+            for item in self._admit():
+                threading.Thread(target=self._run, args=item, daemon=True).start()
+            self.cv.notify_all()
+
+    def submit(self, r: Request):
+        with self.cv:
+            r.arrival = self.now()
+            self.queue.append(r)
+            for item in self._admit():
+                threading.Thread(target=self._run, args=item, daemon=True).start()
+
+    def wait(self, n: int, timeout: float = 3600.0):
+        with self.cv:
+            self.cv.wait_for(lambda: len(self.finished) >= n, timeout=timeout)
+
+    def close(self):
+        for c in self.contexts:
+            c.close()
+
+
+def poisson_arrivals(n: int, rate_per_s: float, seed: int) -> np.ndarray:
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return np.cumsum(rng.exponential(1.0 / rate_per_s, n))
+
+
+def serve(requests: Sequence[Request], arrivals: Sequence[float], streams: int = 4, device: int = 0,
+          hbm_budget: Optional[int] = None, batched: bool = True,
+          context_factory: Optional[Callable[[int], object]] = None) -> Dict:
+    """Replays `requests` at the given arrival offsets (seconds); returns
+    latency percentiles, throughput and the finished requests."""
+    srv = Server(streams, device, hbm_budget, batched, context_factory)
+    try:
+        t_start = srv.now()
+        for r, at in zip(requests, arrivals):
+            delay = t_start + at - srv.now()
+            if delay > 0:
+                time.sleep(delay)
+            srv.submit(r)
+        srv.wait(len(requests))
+        t_end = srv.now()
+        lat = np.array([(r.done - r.arrival) * 1e3 for r in srv.finished])
+        return {
+            "requests": len(requests),
+            "streams": streams,
+            "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)),
+            "mean_ms": float(lat.mean()),
+            "proofs_per_s": len(requests) / (t_end - t_start),
+            "errors": sum(r.error is not None for r in srv.finished),
+            "first_error": next((r.error for r in srv.finished if r.error), None),
+            "peak_budget_in_use": srv.peak_in_use,
+            "budget": srv.budget,
+            "finished": srv.finished,
+        }
+    finally:
+        srv.close()
