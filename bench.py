@@ -42,6 +42,8 @@ def parse():
     ap.add_argument("--queries", type=int, default=200)
     ap.add_argument("--cpu-sample", type=int, default=4, help="instances in the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sweep", action="store_true",
+                    help="kernel roofline sweep (LDE, Merkle commit, FRI fold, DEEP) instead of the prove bench")
     ap.add_argument("--serve-requests", type=int, default=48, help="requests in the serving measurement (0 = skip)")
     ap.add_argument("--serve-shapes", type=int, default=8, help="distinct request shapes, replayed in turn")
     ap.add_argument("--serve-rate", type=str, default="8,16", help="Poisson arrival rates (requests/s) to sweep")
@@ -148,9 +150,109 @@ def reference_arm(a, rank):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------- kernel sweep
+def sweep(a):
+    """Kernel roofline sweep on seeded uniform data resident in HBM: batched
+    coset LDE (2^16..2^24 output rows), Poseidon2 Merkle commit over LDEs,
+    FRI fold of E6 vectors (2^18..2^24), DEEP over 256 columns at one point.
+    One JSON line per measurement; per-kernel times are CUDA events on the
+    library's stream."""
+    import ctypes
+    import faulthandler
+    import torch
+    from loom_b200 import Context, _lib
+    faulthandler.enable()
+    L = _lib.load()
+    dev = torch.device("cuda:0")
+    ctx = Context(0)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    g = torch.Generator(device=dev)
+    g.manual_seed(0x5EED)
+
+    def field(n):
+        return torch.randint(0, 0x7F000001, (n,), dtype=torch.int64, device=dev, generator=g).to(torch.int32)
+
+    def vp(t):
+        return ctypes.c_void_p(t.data_ptr())
+
+    def run(fn, what=""):
+        print("sweep:", what, file=sys.stderr, flush=True)
+        fn()  # warm (tables, pool)
+        torch.cuda.synchronize()
+        ctx.profile(True)
+        fn()
+        rep = ctx.profile_report()
+        ctx.profile(False)
+        rep.pop("phases", None)
+        return rep
+
+    def emit(kind, kernel, rep, **kw):
+        v = rep.get(kernel)
+        if not v:
+            return
+        ms = v["ms"]
+        line = {"sweep": kind, "kernel": kernel, "launches": v["launches"], "ms": round(ms, 4), **kw}
+        if v["bytes"]:
+            gbs = v["bytes"] / (ms * 1e-3) / 1e9
+            line.update({"GB/s": round(gbs, 1), "hbm_frac": round(gbs / hbm, 4)})
+        if v["perms"]:
+            line["Gperm/s"] = round(v["perms"] / (ms * 1e-3) / 1e9, 3)
+        print(json.dumps(line), flush=True)
+
+    def check(rc):
+        if rc != 0:
+            raise RuntimeError(L.lg_last_error(ctx.h).decode())
+
+    for log_out, cols in [(16, 1024), (18, 512), (20, 256), (22, 128), (24, 64)]:
+        n = 1 << (log_out - 2)
+        x = field(n * cols)
+        y = torch.empty(4 * n * cols, dtype=torch.int32, device=dev)
+        rep = run(lambda: check(L.lg_rs_encode(ctx.h, vp(x), n, cols, vp(y), 1)), f"lde {log_out} {cols}")
+        emit("lde", "lde", rep, rows_out=1 << log_out, cols=cols)
+        del x, y
+    for log_out, cols in [(16, 256), (20, 64), (22, 16)]:
+        n = 1 << (log_out - 2)
+        x = field(n * cols)
+        ptrs = (ctypes.c_void_p * cols)(*[x.data_ptr() + 4 * n * i for i in range(cols)])
+        rows = (ctypes.c_uint64 * 1)(n)
+        nb, ne = (ctypes.c_uint32 * 1)(cols), (ctypes.c_uint32 * 1)(0)
+        root = (ctypes.c_uint32 * 8)()
+        rep = run(lambda: check(L.lg_commit_root(ctx.h, 1, rows, nb, ne, ptrs, 1, root)), f"commit {log_out} {cols}")
+        for k in ("lde", "hash_leaves", "merkle_level", "merkle_tail", "merkle_inject"):
+            emit("merkle_commit", k, rep, rows_out=1 << log_out, cols=cols)
+        del x
+    alpha = (ctypes.c_uint32 * 6)(*[12345 + i for i in range(6)])
+    for logn in (18, 20, 22, 24):
+        n = 1 << logn
+        x = field(6 * n)
+        y = torch.empty(3 * n, dtype=torch.int32, device=dev)
+        rep = run(lambda: check(L.lg_fri_fold(ctx.h, vp(x), n, alpha, vp(y), 1)), f"fold {logn}")
+        emit("fri_fold", "fri_fold", rep, n_e6=n)
+        del x, y
+    for logr, cols in [(20, 256), (22, 64)]:
+        rows = 1 << logr
+        x = field(rows * cols)
+        vals = field(6 * cols)
+        out = torch.empty(6 * rows, dtype=torch.int32, device=dev)
+        z = (ctypes.c_uint32 * 6)(*[777 + i for i in range(6)])
+        rep = run(lambda: check(L.lg_deep_quotient(ctx.h, vp(x), cols, rows, alpha, z, vp(vals), vp(out), 1)),
+                  f"deep {logr} {cols}")
+        emit("deep", "deep", rep, rows=rows, cols=cols)
+        del x, out
+    ctx.close()
+
+
 # ---------------------------------------------------------------------- GPU arm
 def main():
     a = parse()
+    if a.sweep:
+        return sweep(a)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -174,12 +276,14 @@ def main():
     mont = [np.ascontiguousarray(F.to_mont(w)) for w in wit]
     dev_cols = [torch.from_numpy(m.view(np.int32)).to(f"cuda:{device}") for m in mont]
     dev_ptrs = [t.data_ptr() for t in dev_cols]
-    pinned = []
+    # pinned host witness, columns back to back in descriptor order (one copy)
+    pinned_all = torch.empty(sum(m.size for m in mont), dtype=torch.int32, pin_memory=True)
+    host_all = pinned_all.numpy().view(np.uint32)
+    host_cols, off = [], 0
     for m in mont:
-        t = torch.empty(m.size, dtype=torch.int32, pin_memory=True)
-        t.numpy()[:] = m.view(np.int32)
-        pinned.append(t)
-    host_cols = [t.numpy().view(np.uint32) for t in pinned]
+        host_all[off:off + m.size] = m
+        host_cols.append(host_all[off:off + m.size])
+        off += m.size
     h2d_bytes = int(sum(m.nbytes for m in mont))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{device}")  # > 126 MB L2
     torch.cuda.synchronize()
@@ -283,7 +387,8 @@ def main():
                 t = pool_reqs[i % len(pool_reqs)]
                 reqs.append(SV.Request(i, t.words, t.witness, t.num_queries, t.rows))
             shape_of = {i: i % len(pool_reqs) for i in range(a.serve_requests)}
-            res = SV.serve(reqs, SV.poisson_arrivals(len(reqs), rate, 11), streams=a.serve_streams, device=device)
+            res = SV.serve(reqs, SV.poisson_arrivals(len(reqs), rate, 11), streams=a.serve_streams, device=device,
+                           warm=pool_reqs)
             same = all(r.proof == ref_proof[shape_of[r.rid]] for r in res["finished"])
             seq_ms = sum(plain_one[shape_of[i]] for i in range(a.serve_requests))
             sweeps.append({"rate_per_s": rate, "requests": res["requests"], "p50_ms": round(res["p50_ms"], 2),

@@ -13,8 +13,12 @@
  * 6 such words [B0.A0, B0.A1, B1.A0, B1.A1, B2.A0, B2.A1] (ext.E6).  A
  * digest is 8 words (hash.Digest).
  *
- * Buffers flagged `on_device` are device pointers on the context's GPU;
- * otherwise host pointers.  Input pointers are only read during the call.
+ * Data buffers flagged `on_device` are device pointers on the context's GPU;
+ * otherwise host pointers.  Small parameter arrays (challenges such as
+ * alpha and z, row counts, widths, and the arrays of column pointers
+ * themselves) are always host memory.  Input pointers are only read during
+ * the call; device witness columns given to lg_prove are used in place and
+ * must not change until it returns.
  *
  * Program descriptor (lg_prove): little-endian u32 words —
  *   magic 0x3150474C, n_rounds, n_modules, n_columns, n_nodes, n_steps
@@ -123,6 +127,17 @@ int lg_merkle_root(lg_ctx* ctx, const uint32_t* leaves, uint64_t n_leaves, uint3
  * (foldLayerExt, internal/fri/fri.go:1177-1198); writes n/2 E6 values. */
 int lg_fri_fold(lg_ctx* ctx, const uint32_t* layer, uint64_t n, const uint32_t alpha[6], uint32_t* out,
                 int on_device);
+
+/* DEEP quotient at one point over base columns in LDE form: for each row r
+ * (x = w^bitrev(r) on the subgroup of order `rows`),
+ * out[r] = sum_i alpha^i (values[i] - P_i(x)) / (z - x), where `lde` holds
+ * n_cols columns of `rows` bit-reversed evaluations one after another and
+ * values[i] = P_i(z) (E6; with on_device, all of lde, values and out are
+ * device pointers).  The single-point form of
+ * accumulateDeepQuotientByPolynomialOnTrace (internal/fri/deep.go:205-266),
+ * evaluated on the LDE rows.  Writes `rows` E6 values. */
+int lg_deep_quotient(lg_ctx* ctx, const uint32_t* lde, uint32_t n_cols, uint64_t rows, const uint32_t alpha[6],
+                     const uint32_t z[6], const uint32_t* values, uint32_t* out, int on_device);
 
 /* Grand product of a prover step: out[0] = 1, out[i] = prod_{k<i} num[k]/den[k]
  * over n E6 rows (6 words each, ext.E6 layout) — the accumulation of

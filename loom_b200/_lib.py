@@ -18,7 +18,7 @@ LIB_PATH = os.path.join(HERE, "libloom_gpu.so")
 LG_OK, LG_ERR_INVALID, LG_ERR_CUDA, LG_ERR_OOM, LG_ERR_UNSUPPORTED, LG_ERR_BUFFER = range(6)
 EXPORTS = ["lg_ctx_create", "lg_ctx_destroy", "lg_ctx_set_batched", "lg_ctx_set_leaf_mapping", "lg_mem_info", "lg_last_error", "lg_prove", "lg_last_proof", "lg_commit_root",
            "lg_rs_encode", "lg_poseidon2_permute", "lg_merkle_root", "lg_fri_fold", "lg_timer_mark",
-           "lg_timer_elapsed", "lg_kernel_launches", "lg_profile", "lg_profile_report", "lg_grand_product", "lg_grand_product_noalloc"]
+           "lg_timer_elapsed", "lg_kernel_launches", "lg_profile", "lg_profile_report", "lg_grand_product", "lg_grand_product_noalloc", "lg_deep_quotient"]
 
 u32p = ctypes.POINTER(ctypes.c_uint32)
 u64p = ctypes.POINTER(ctypes.c_uint64)
@@ -58,6 +58,8 @@ def load():
         L.lg_merkle_root.argtypes = [vp, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, u64p, ctypes.c_void_p,
                                      ctypes.c_int, u32p]
         L.lg_fri_fold.argtypes = [vp, ctypes.c_void_p, ctypes.c_uint64, u32p, ctypes.c_void_p, ctypes.c_int]
+        L.lg_deep_quotient.argtypes = [vp, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, u32p, u32p, ctypes.c_void_p,
+                                       ctypes.c_void_p, ctypes.c_int]
         L.lg_grand_product.argtypes = [vp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_int]
         L.lg_grand_product_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
                                                ctypes.c_void_p]
@@ -205,6 +207,15 @@ class Context:
         self._check(self.L.lg_merkle_root(self.h, _ptr(lv), lv.shape[0], len(injections), widths.ctypes.data_as(u64p),
                                           _ptr(inj), 0, root.ctypes.data_as(u32p)))
         return root
+
+    def deep_quotient(self, lde: np.ndarray, alpha, z, values) -> np.ndarray:
+        """Single-point DEEP quotient over base LDE columns (rows bit-reversed)."""
+        x = _u32(lde)
+        a, zz, v = _u32(alpha), _u32(z), _u32(values).reshape(-1)
+        out = np.zeros((x.shape[1], 6), dtype=np.uint32)
+        self._check(self.L.lg_deep_quotient(self.h, _ptr(x), x.shape[0], x.shape[1], a.ctypes.data_as(u32p),
+                                            zz.ctypes.data_as(u32p), _ptr(v), _ptr(out), 0))
+        return out
 
     def grand_product(self, num: np.ndarray, den: np.ndarray) -> np.ndarray:
         a, b = _u32(num).reshape(-1, 6), _u32(den).reshape(-1, 6)

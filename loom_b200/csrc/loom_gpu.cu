@@ -257,8 +257,11 @@ int lg_fri_fold(lg_ctx* ctx, const uint32_t* layer, uint64_t n, const uint32_t a
     auto nx = std::make_shared<DBuf>(3 * n, c.stream);
     E6 al;
     for (int w = 0; w < 6; w++) al.c[w] = alpha[w];
-    k_fold<<<(unsigned)((n / 2 + 255) / 256), 256, 0, c.stream>>>(soa->p, n, al, c.twiddles(logn), inv(to_mont(2)), nx->p);
-    LG_LAUNCH();
+    const uint32_t* tw = c.twiddles(logn);
+    c.timed("fri_fold", 36.0 * n, 0, [&] {
+      k_fold<<<(unsigned)((n / 2 + 255) / 256), 256, 0, c.stream>>>(soa->p, n, al, tw, inv(to_mont(2)), nx->p);
+      LG_LAUNCH();
+    });
     auto aos = std::make_shared<DBuf>(3 * n, c.stream);
     k_soa_to_aos<<<(unsigned)((3 * n + 255) / 256), 256, 0, c.stream>>>(nx->p, n / 2, 6, aos->p);
     LG_LAUNCH();
@@ -295,6 +298,71 @@ int lg_grand_product(lg_ctx* ctx, const uint32_t* num, const uint32_t* den, uint
     k_soa_to_aos<<<g6, 256, 0, c.stream>>>(res->p, n, 6, aos->p);
     LG_LAUNCH();
     from_device(c, out, aos->p, 6 * n, on_device);
+  });
+}
+
+int lg_deep_quotient(lg_ctx* ctx, const uint32_t* lde, uint32_t n_cols, uint64_t rows, const uint32_t alpha[6],
+                     const uint32_t z[6], const uint32_t* values, uint32_t* out, int on_device) {
+  return guarded(ctx, [&] {
+    Ctx& c = ctx->c;
+    if (!lde || !alpha || !z || !values || !out || !n_cols || rows < 2 || (rows & (rows - 1)) || rows > (1ull << 24))
+      throw Error(LG_ERR_INVALID, "bad arguments");
+    int logr = 0;
+    while ((1ull << logr) < rows) logr++;
+    DBufP src;
+    const uint32_t* lanes = lde;
+    if (!on_device) {
+      src = to_device(c, lde, (size_t)n_cols * rows, 0);
+      lanes = src->p;
+    }
+    E6 a, zz;
+    for (int w = 0; w < 6; w++) { a.c[w] = alpha[w]; zz.c[w] = z[w]; }
+    // the claimed values are read on the host: bring them back when they live on the device
+    std::vector<uint32_t> vals_host;
+    if (on_device) {
+      vals_host.resize(6 * (size_t)n_cols);
+      LG_CK(cudaMemcpyAsync(vals_host.data(), values, vals_host.size() * 4, cudaMemcpyDeviceToHost, c.stream));
+      LG_CK(cudaStreamSynchronize(c.stream));
+      values = vals_host.data();
+    }
+    DeepJob jb{};
+    std::vector<DeepBundle> bundles;
+    E6 run = e6_one(), acc = e6_zero();
+    for (uint32_t i = 0; i < n_cols; i++) {
+      DeepBundle bu{};
+      bu.lane0 = lanes + (size_t)i * rows;
+      bu.lane_stride = rows;
+      bu.ext = 0;
+      bu.mask = 1;
+      bu.scale = run;
+      E6 v;
+      for (int w = 0; w < 6; w++) v.c[w] = values[6 * i + w];
+      acc = e6_add(acc, e6_mul(run, v));
+      bundles.push_back(bu);
+      run = e6_mul(run, a);
+    }
+    jb.n_points = 1;
+    jb.z[0] = zz;
+    jb.a[0] = acc;
+    auto bd = upload_vec(c, bundles);
+    jb.bundles = (const DeepBundle*)bd->p;
+    jb.n_bundles = n_cols;
+    jb.logn4 = logr;
+    jb.tw = c.twiddles(logr);
+    auto soa = std::make_shared<DBuf>(6 * rows, c.stream);
+    jb.out = soa->p;
+    std::vector<DeepJob> jv = {jb};
+    auto jd = upload_vec(c, jv);
+    c.timed("deep", (4.0 * n_cols + 24.0) * rows, 0, [&] {
+      k_deep<<<dim3((unsigned)((rows + 127) / 128), 1), 128, 0, c.stream>>>((const DeepJob*)jd->p);
+      LG_LAUNCH();
+    });
+    auto aos = on_device ? DBufP() : std::make_shared<DBuf>(6 * rows, c.stream);
+    uint32_t* dst = on_device ? out : aos->p;
+    k_soa_to_aos<<<(unsigned)((6 * rows + 255) / 256), 256, 0, c.stream>>>(soa->p, rows, 6, dst);
+    LG_LAUNCH();
+    if (!on_device) from_device(c, out, aos->p, 6 * rows, 0);
+    else LG_CK(cudaStreamSynchronize(c.stream));
   });
 }
 

@@ -31,6 +31,7 @@ struct Prover {
 
   // column data on the device: lane pointer = buf + w * n
   std::map<uint32_t, DBufP> col_buf;
+  DBufP witness_dev;  // host witness columns, uploaded into one buffer
   std::map<uint32_t, const uint32_t*> col_coef;  // committed columns: coefficient lane 0
 
   struct Group { uint32_t module; std::vector<uint32_t> bcols, ecols; };
@@ -168,24 +169,39 @@ struct Prover {
   void setup(const uint32_t* const* witness, bool on_device) {
     for (uint32_t m = 0; m < pg.modules.size(); m++) mod_order.push_back(m);
     std::sort(mod_order.begin(), mod_order.end(), [&](uint32_t a, uint32_t b) { return pg.modules[a].name < pg.modules[b].name; });
-    size_t wi = 0;
+    // Host witness: one device buffer for all columns; columns that follow
+    // one another in host memory go up in a single copy.
+    size_t total_words = 0;
+    for (const Column& cl : pg.columns)
+      if (cl.kind == KIND_WITNESS) total_words += mod_n(cl.module);
+    if (!on_device && total_words) witness_dev = std::make_shared<DBuf>(total_words, c.stream);
+    size_t wi = 0, woff = 0;
+    const uint32_t* run_src = nullptr;
+    uint32_t* run_dst = nullptr;
+    size_t run_words = 0;
+    auto flush = [&]() {
+      if (run_words) LG_CK(cudaMemcpyAsync(run_dst, run_src, run_words * 4, cudaMemcpyHostToDevice, c.stream));
+      run_words = 0;
+    };
     for (uint32_t col = 0; col < pg.columns.size(); col++) {
       const Column& cl = pg.columns[col];
       size_t n = mod_n(cl.module);
       if (cl.kind == KIND_WITNESS) {
         if (cl.field != 0) throw Error(LG_ERR_UNSUPPORTED, "extension-field witness columns are not supported");
+        auto b = std::make_shared<DBuf>();
+        b->words = n;
+        b->borrowed = true;
+        const uint32_t* src = witness[wi++];
         if (on_device) {
           // read-only input: use the caller's device buffer as it is
-          auto b = std::make_shared<DBuf>();
-          b->p = const_cast<uint32_t*>(witness[wi++]);
-          b->words = n;
-          b->borrowed = true;
-          col_buf[col] = b;
+          b->p = const_cast<uint32_t*>(src);
         } else {
-          auto b = std::make_shared<DBuf>(n, c.stream);
-          LG_CK(cudaMemcpyAsync(b->p, witness[wi++], n * 4, cudaMemcpyHostToDevice, c.stream));
-          col_buf[col] = b;
+          b->p = witness_dev->p + woff;
+          if (run_words && src == run_src + run_words) run_words += n;
+          else { flush(); run_src = src; run_dst = b->p; run_words = n; }
+          woff += n;
         }
+        col_buf[col] = b;
       } else if (cl.kind == KIND_LAGRANGE) {
         int64_t row = cl.param >= 0 ? cl.param : (int64_t)n - 1 - (-(int64_t)cl.param - 1);
         if (row < 0 || row >= (int64_t)n) throw Error(LG_ERR_INVALID, "Lagrange column row out of range");
@@ -196,6 +212,7 @@ struct Prover {
         col_buf[col] = b;
       }
     }
+    flush();
     // fold relations with coin(last round) (board/program.go:62-80)
     fold_root.assign(pg.modules.size(), -1);
     degree.assign(pg.modules.size(), NEG_INF);

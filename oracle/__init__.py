@@ -186,3 +186,13 @@ def grand_product(num_mont, den_mont) -> np.ndarray:
     out = np.zeros_like(a)
     L.oracle_grand_product(_p(a), _p(b), a.size // 6, _p(out))
     return out.reshape(-1, 6)
+
+
+def deep_quotient(lde_mont, alpha_m, z_m, values_m) -> np.ndarray:
+    L = lib()
+    L.oracle_deep_quotient.argtypes = [u32p, ctypes.c_uint32, ctypes.c_size_t, u32p, u32p, u32p, u32p]
+    x = _u32(lde_mont)
+    a, z, v = _u32(alpha_m), _u32(z_m), _u32(values_m).reshape(-1)
+    out = np.zeros(6 * x.shape[1], dtype=np.uint32)
+    L.oracle_deep_quotient(_p(x), x.shape[0], x.shape[1], _p(a), _p(z), _p(v), _p(out))
+    return out.reshape(-1, 6)

@@ -211,3 +211,29 @@ void oracle_grand_product(const uint32_t* num, const uint32_t* den, size_t n, ui
   }
 }
 }
+
+extern "C" {
+// Single-point DEEP quotient over base LDE columns of `rows` bit-reversed
+// evaluations (internal/fri/deep.go:205-266), Montgomery in/out.
+void oracle_deep_quotient(const uint32_t* lde, uint32_t n_cols, size_t rows, const uint32_t* alpha_m,
+                          const uint32_t* z_m, const uint32_t* values_m, uint32_t* out) {
+  E6 a, z;
+  for (int k = 0; k < 6; k++) { a.c[k] = from_mont(alpha_m[k]); z.c[k] = from_mont(z_m[k]); }
+  int lg = 0;
+  while ((1ull << lg) < rows) lg++;
+  uint32_t w = root_of_unity(rows);
+  for (size_t r = 0; r < rows; r++) {
+    uint32_t x = pow(w, bitrev((uint32_t)r, lg));
+    E6 num = e6_zero(), run = e6_one();
+    for (uint32_t i = 0; i < n_cols; i++) {
+      E6 v;
+      for (int k = 0; k < 6; k++) v.c[k] = from_mont(values_m[6 * i + k]);
+      uint32_t p = from_mont(lde[(size_t)i * rows + r]);
+      num = e6_add(num, e6_sub(e6_mul(run, v), e6_mul_base(run, p)));
+      run = e6_mul(run, a);
+    }
+    E6 q = e6_mul(num, e6_inv(e6_sub(z, e6_from_base(x))));
+    for (int k = 0; k < 6; k++) out[6 * r + k] = to_mont(q.c[k]);
+  }
+}
+}

@@ -204,3 +204,11 @@ def test_prove_large_module(ctx):
     mont = [F.to_mont(trace[name]) for (name, _, _) in compiled.witness_columns]
     got = ctx.prove(compiled.words, mont, 4)
     assert got == oracle.prove(compiled.words, mont, 4)
+
+
+@pytest.mark.parametrize("cols,logr", [(1, 3), (5, 10), (37, 12)])
+def test_deep_quotient(ctx, cols, logr):
+    lde = F.to_mont(rnd((cols, 1 << logr), cols))
+    alpha, z = F.to_mont(rnd(6, 1)), F.to_mont(rnd(6, 2))
+    values = F.to_mont(rnd((cols, 6), 3))
+    assert np.array_equal(ctx.deep_quotient(lde, alpha, z, values), oracle.deep_quotient(lde, alpha, z, values))
