@@ -30,7 +30,10 @@ template <class K> inline void allow_smem(K kernel, size_t bytes) {
   cur = bytes;
 }
 
-inline int ntt_threads(int logn) { return std::max(32, std::min(512, 1 << std::max(0, logn - 1))); }
+// 16 elements per thread for n >= 16 (radix-16 passes), up to 1024 threads.
+inline int ntt_threads(int logn) { return logn < 4 ? 32 : std::max(32, std::min(1024, 1 << (logn - 4))); }
+// shared words of one pad16 array of n = 2^logn points
+inline size_t pad16_words(int logn) { return ((size_t)1 << logn) + ((size_t)1 << logn) / 16 + 1; }
 
 constexpr int MAX_NTT_LOG = 22;  // the largest loom module, 2^22 rows
 inline void check_ntt_size(int logn) {
@@ -115,7 +118,7 @@ inline void launch_lde(Ctx& c, const std::vector<LdeLane>& lanes, uint32_t log_n
   auto tab = upload_vec(c, lanes);
   const uint32_t* twn = c.twiddles((int)log_n);
   const uint32_t* tw4 = c.twiddles((int)log_n + RATE_LOG);
-  size_t smem = 2 * n * 4;
+  size_t smem = 2 * pad16_words((int)log_n) * 4;
   allow_smem(k_lde, smem);
   c.timed("lde", 20.0 * n * lanes.size(), 0, [&] {
     k_lde<<<(unsigned)lanes.size(), ntt_threads((int)log_n), smem, c.stream>>>((const LdeLane*)tab->p, (int)log_n,

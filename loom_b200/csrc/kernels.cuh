@@ -6,6 +6,7 @@
 
 #include "field.cuh"
 #include "p2_coop.cuh"
+#include "ntt16.cuh"
 
 namespace lg {
 
@@ -63,54 +64,109 @@ __device__ void smem_dif(uint32_t* A, int logn, const uint32_t* tw, bool inverse
 
 // Inverse transform of natural-order values to natural-order coefficients
 // (scaled by 1/n), in place; one block per lane, lanes[blockIdx.x].
+// n >= 16: DIT whose first pass gathers the bit-reversed input from global
+// memory; smaller n: radix-2 stages in shared memory.
 __global__ void k_intt(uint32_t* const* lanes, int logn, const uint32_t* tw_n, uint32_t n_inv) {
   extern __shared__ uint32_t sm[];
   const uint32_t n = 1u << logn;
   uint32_t* d = lanes[blockIdx.x];
-  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) sm[bitrev32(k, logn)] = d[k];
-  __syncthreads();
-  smem_dit(sm, logn, tw_n, true);
-  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) d[k] = mul(sm[k], n_inv);
+  if (logn < 4) {
+    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) sm[bitrev32(k, logn)] = d[k];
+    __syncthreads();
+    smem_dit(sm, logn, tw_n, true);
+    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) d[k] = mul(sm[k], n_inv);
+    return;
+  }
+  auto first = [&](uint32_t t, uint32_t r, int lo) { return d[bitrev32(grp_index(t, r, lo), logn)]; };
+  auto store = [&](uint32_t t, int lo, const uint32_t* v) {
+#pragma unroll
+    for (uint32_t r = 0; r < 16; r++) d[grp_index(t, r, lo)] = mul(v[r], n_inv);
+  };
+  ntt16<false>(sm, logn, tw_n, true, first, store);
 }
 
 // LDE of one lane per block: Lagrange values in natural order (or canonical
 // coefficients when from_coeffs) -> for coset a < 4,
 // out[a n + b] = P(w_4n^bitrev2(a) w_n^bitrev(b)), the bit-reversed
 // evaluations on <w_4n> of reedsolomon.Encode (internal/reedsolomon/rs.go:52-70).
-// Optionally writes the coefficients.
+// Optionally writes the coefficients.  Shared memory: A (coefficients) and B
+// (work), pad16 layout.
 struct LdeLane { const uint32_t* src; uint32_t* out; uint32_t* coef; };
 __global__ void k_lde(const LdeLane* lanes, int logn, int from_coeffs, const uint32_t* tw_n, const uint32_t* tw_4n,
                       uint32_t n_inv) {
   extern __shared__ uint32_t sm[];
   const uint32_t n = 1u << logn;
-  uint32_t* A = sm;
-  uint32_t* B = sm + n;
   const LdeLane L = lanes[blockIdx.x];
+  const uint32_t big = n << RATE_LOG;
+  if (logn < 4) {  // tiny columns: radix-2 stages
+    uint32_t* A = sm;
+    uint32_t* B = sm + n;
+    if (from_coeffs) {
+      for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) A[k] = L.src[k];
+      __syncthreads();
+    } else {
+      for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) A[bitrev32(k, logn)] = L.src[k];
+      __syncthreads();
+      smem_dit(A, logn, tw_n, true);
+      for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) A[k] = mul(A[k], n_inv);
+      __syncthreads();
+    }
+    if (L.coef)
+      for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) L.coef[k] = A[k];
+    for (int a = 0; a < (1 << RATE_LOG); a++) {
+      const uint32_t e = bitrev32((uint32_t)a, RATE_LOG);
+      for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) B[k] = mul(A[k], __ldg(tw_4n + ((e * k) & (big - 1))));
+      __syncthreads();
+      smem_dif(B, logn, tw_n, false);
+      for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) L.out[(uint64_t)a * n + k] = B[k];
+      __syncthreads();
+    }
+    return;
+  }
+  uint32_t* A = sm;
+  uint32_t* B = sm + pad16(n);
   if (from_coeffs) {
-    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) A[k] = L.src[k];
+    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) {
+      uint32_t v = L.src[k];
+      A[pad16(k)] = v;
+      if (L.coef) L.coef[k] = v;
+    }
     __syncthreads();
   } else {
-    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) A[bitrev32(k, logn)] = L.src[k];
-    __syncthreads();
-    smem_dit(A, logn, tw_n, true);
-    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) A[k] = mul(A[k], n_inv);
-    __syncthreads();
+    auto first = [&](uint32_t t, uint32_t r, int lo) { return L.src[bitrev32(grp_index(t, r, lo), logn)]; };
+    auto store = [&](uint32_t t, int lo, const uint32_t* v) {
+#pragma unroll
+      for (uint32_t r = 0; r < 16; r++) {
+        uint32_t i = grp_index(t, r, lo), c = mul(v[r], n_inv);
+        A[pad16(i)] = c;
+        if (L.coef) L.coef[i] = c;
+      }
+    };
+    ntt16<false>(A, logn, tw_n, true, first, store);  // A is both work and result
   }
-  if (L.coef)
-    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) L.coef[k] = A[k];
-  const uint32_t big = n << RATE_LOG;
   for (int a = 0; a < (1 << RATE_LOG); a++) {
     const uint32_t e = bitrev32((uint32_t)a, RATE_LOG);
-    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) B[k] = mul(A[k], __ldg(tw_4n + ((e * k) & (big - 1))));
-    __syncthreads();
-    smem_dif(B, logn, tw_n, false);
-    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) L.out[(uint64_t)a * n + k] = B[k];
-    __syncthreads();
+    uint32_t* o = L.out + (uint64_t)a * n;
+    auto first = [&](uint32_t t, uint32_t r, int lo) {
+      uint32_t i = grp_index(t, r, lo);
+      return mul(A[pad16(i)], __ldg(tw_4n + ((e * i) & (big - 1))));
+    };
+    auto store = [&](uint32_t t, int lo, const uint32_t* v) {
+      // DIF's last pass has lo = 0: the group is 16 consecutive outputs
+      uint4* q = reinterpret_cast<uint4*>(o + ((uint64_t)t << 4));
+      q[0] = make_uint4(v[0], v[1], v[2], v[3]);
+      q[1] = make_uint4(v[4], v[5], v[6], v[7]);
+      q[2] = make_uint4(v[8], v[9], v[10], v[11]);
+      q[3] = make_uint4(v[12], v[13], v[14], v[15]);
+    };
+    ntt16<true>(B, logn, tw_n, false, first, store);
   }
 }
 
 // Evaluations of a coefficient lane on the cosets s_c <w_n>, s_c = g w_4n^c,
 // c = blockIdx.y < 4, in natural order: out[c n + j] = P(s_c w_n^j).
+// n >= 16: DIT whose first pass gathers the scaled coefficients in
+// bit-reversed order from global memory.
 struct CosetLane { const uint32_t* src; uint32_t* out; };
 __global__ void k_coset_eval(const CosetLane* lanes, int logn, const uint32_t* tw_n, const uint32_t* tw_4n,
                              const uint32_t* gpow) {
@@ -118,12 +174,24 @@ __global__ void k_coset_eval(const CosetLane* lanes, int logn, const uint32_t* t
   const uint32_t n = 1u << logn, c = blockIdx.y;
   const CosetLane L = lanes[blockIdx.x];
   const uint32_t big = n << RATE_LOG;
-  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x)
-    sm[k] = mul(mul(L.src[k], __ldg(gpow + k)), __ldg(tw_4n + ((c * k) & (big - 1))));
-  __syncthreads();
-  smem_dif(sm, logn, tw_n, false);
   uint32_t* o = L.out + (uint64_t)c * n;
-  for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) o[j] = sm[bitrev32(j, logn)];
+  if (logn < 4) {
+    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x)
+      sm[k] = mul(mul(L.src[k], __ldg(gpow + k)), __ldg(tw_4n + ((c * k) & (big - 1))));
+    __syncthreads();
+    smem_dif(sm, logn, tw_n, false);
+    for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) o[j] = sm[bitrev32(j, logn)];
+    return;
+  }
+  auto first = [&](uint32_t t, uint32_t r, int lo) {
+    uint32_t k = bitrev32(grp_index(t, r, lo), logn);
+    return mul(mul(L.src[k], __ldg(gpow + k)), __ldg(tw_4n + ((c * k) & (big - 1))));
+  };
+  auto store = [&](uint32_t t, int lo, const uint32_t* v) {
+#pragma unroll
+    for (uint32_t r = 0; r < 16; r++) o[grp_index(t, r, lo)] = v[r];
+  };
+  ntt16<false>(sm, logn, tw_n, false, first, store);
 }
 
 // ---------------------------------------------------------------- leaves

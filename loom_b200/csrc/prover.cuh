@@ -439,8 +439,8 @@ struct Prover {
             big_ntt(c, jobs, (int)logn, true, "quotient_intt", 8.0 * n);
           } else {
             auto tab = upload_vec(c, ls);
-            allow_smem(k_intt, n * 4);
-            k_intt<<<lanes_of(col), ntt_threads((int)logn), n * 4, c.stream>>>((uint32_t* const*)tab->p, (int)logn,
+            allow_smem(k_intt, pad16_words((int)logn) * 4);
+            k_intt<<<lanes_of(col), ntt_threads((int)logn), pad16_words((int)logn) * 4, c.stream>>>((uint32_t* const*)tab->p, (int)logn,
                                                                                c.twiddles((int)logn), inv(to_mont((uint32_t)n)));
             LG_LAUNCH();
             keep.push_back(tab);
@@ -489,12 +489,12 @@ struct Prover {
           continue;
         }
         auto tab = upload_vec(c, kv.second);
-        allow_smem(k_coset_eval, n * 4);
+        allow_smem(k_coset_eval, pad16_words((int)logn) * 4);
         const uint32_t* twn = c.twiddles((int)logn);
         const uint32_t* tw4 = c.twiddles((int)logn + RATE_LOG);
         const uint32_t* gp = c.gpowers((int)logn, false);
         c.timed("coset_eval", 20.0 * n * kv.second.size(), 0, [&] {
-          k_coset_eval<<<dim3((unsigned)kv.second.size(), 4), ntt_threads((int)logn), n * 4, c.stream>>>(
+          k_coset_eval<<<dim3((unsigned)kv.second.size(), 4), ntt_threads((int)logn), pad16_words((int)logn) * 4, c.stream>>>(
               (const CosetLane*)tab->p, (int)logn, twn, tw4, gp);
           LG_LAUNCH();
         });
@@ -540,10 +540,10 @@ struct Prover {
           continue;
         }
         auto tab = upload_vec(c, kv.second);
-        allow_smem(k_intt, n * 4);
+        allow_smem(k_intt, pad16_words((int)kv.first) * 4);
         const uint32_t* twn = c.twiddles((int)kv.first);
         c.timed("quotient_intt", 8.0 * n * kv.second.size(), 0, [&] {
-          k_intt<<<(unsigned)kv.second.size(), ntt_threads((int)kv.first), n * 4, c.stream>>>(
+          k_intt<<<(unsigned)kv.second.size(), ntt_threads((int)kv.first), pad16_words((int)kv.first) * 4, c.stream>>>(
               (uint32_t* const*)tab->p, (int)kv.first, twn, inv(to_mont((uint32_t)n)));
           LG_LAUNCH();
         });
