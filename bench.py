@@ -190,6 +190,7 @@ def sweep(a):
         rep = ctx.profile_report()
         ctx.profile(False)
         rep.pop("phases", None)
+        rep.pop("kernels_by_phase", None)
         return rep
 
     def emit(kind, kernel, rep, **kw):
@@ -409,6 +410,7 @@ def main():
     rep = ctx.profile_report()
     ctx.profile(False)
     phases = rep.pop("phases", {})
+    by_phase = rep.pop("kernels_by_phase", {})
 
     ms = statistics.mean(times)
     e2e_ms = statistics.mean(e2e_times)
@@ -492,6 +494,7 @@ def main():
             "kernel_shares": shares,
             "kernel_ms_profiled_step": round(total_k, 3),
             "host_phases_ms": {k: round(v, 3) for k, v in phases.items()},
+            "kernel_ms_by_phase": {ph: {k: round(v["ms"], 3) for k, v in ks.items()} for ph, ks in by_phase.items()},
             "dominant_kernel": dom,
             "cpu_baseline": base,
             "clocks": clk,

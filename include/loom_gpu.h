@@ -76,9 +76,11 @@ void lg_ctx_destroy(lg_ctx* ctx);
  * it once per group / module, like a per-column prover.  Both produce the
  * same proof bytes. */
 int lg_ctx_set_batched(lg_ctx* ctx, int batched);
-/* Thread mapping of Poseidon2 leaf hashing: 1 = one thread per permutation,
- * 6 = six lanes of a warp per permutation, 0 = choose from the number of
- * leaves (default).  Results do not depend on it. */
+/* Thread mapping of Poseidon2 leaf hashing and of the Merkle levels and
+ * injection chains outside the one-block tree top: 1 = one thread per
+ * permutation chain, 6 = six lanes of a warp per permutation, 0 = choose from
+ * the number of independent chains per launch (default).  Results do not
+ * depend on it. */
 int lg_ctx_set_leaf_mapping(lg_ctx* ctx, int lanes_per_permutation);
 /* Free and total device memory of the context's GPU (serving admission). */
 int lg_mem_info(lg_ctx* ctx, uint64_t* free_bytes, uint64_t* total_bytes);

@@ -128,6 +128,17 @@ inline void launch_lde(Ctx& c, const std::vector<LdeLane>& lanes, uint32_t log_n
   });
 }
 
+// Poseidon2 lane mapping for a launch of `parallel` independent permutation
+// chains (leaves, nodes of one level): with at least `per_sm` of them per SM,
+// one thread per chain (fewest instructions per permutation); otherwise six
+// lanes per chain for a dependent chain six times shorter.  Measured on B200:
+// one thread per chain wins for leaf hashing and injection chains from 128
+// chains per SM, for one-permutation Merkle levels from 512.
+constexpr uint32_t P2_THREAD_MIN_LEAVES = 128, P2_THREAD_MIN_NODES = 512;
+inline bool p2_per_thread(const Ctx& c, uint64_t parallel, uint32_t per_sm = P2_THREAD_MIN_LEAVES) {
+  return c.leaf_mapping == 1 || (c.leaf_mapping == 0 && parallel >= (uint64_t)c.sm_count * per_sm);
+}
+
 inline void launch_leaves(Ctx& c, const std::vector<LeafGroup>& gs) {
   if (gs.empty()) return;
   uint32_t max_leaves = 0;
@@ -141,9 +152,7 @@ inline void launch_leaves(Ctx& c, const std::vector<LeafGroup>& gs) {
   auto tab = upload_vec(c, gs);
   uint64_t all_leaves = 0;
   for (auto& g : gs) all_leaves += g.n_leaves;
-  // Enough independent leaves to fill every SM: one thread per permutation;
-  // otherwise six lanes per permutation for a shorter dependent chain.
-  bool per_thread = c.leaf_mapping == 1 || (c.leaf_mapping == 0 && all_leaves >= (uint64_t)c.sm_count * 1024);
+  bool per_thread = p2_per_thread(c, all_leaves);
   c.timed("hash_leaves", bytes, perms, [&] {
     if (per_thread)
       k_hash_leaves1<<<dim3((max_leaves + 127) / 128, (unsigned)gs.size()), 128, 0, c.stream>>>((const LeafGroup*)tab->p);
@@ -199,7 +208,19 @@ struct TreeDev {
   Digest root;
 };
 
-constexpr uint32_t MERKLE_TAIL = 1024;  // levels at or below this width run in one block
+// Levels below this width run in one block (k_merkle_tail); wider levels are
+// grid launches.  The block is throughput bound on its one SM at wide levels
+// and latency bound at narrow ones.
+#ifndef LG_MERKLE_TAIL
+#define LG_MERKLE_TAIL 64
+#endif
+constexpr uint32_t MERKLE_TAIL = LG_MERKLE_TAIL;
+static_assert(MERKLE_TAIL >= 2 && MERKLE_TAIL <= 1024 && (MERKLE_TAIL & (MERKLE_TAIL - 1)) == 0, "tail width");
+// six lanes per permutation, five permutations per warp
+inline unsigned tail_threads(uint32_t top, int fold_first) {
+  uint32_t perms = std::max(1u, fold_first ? top : top / 2);
+  return std::min(1024u, (perms + 4) / 5 * 32);
+}
 
 // nodes must already hold the leaves at [n_leaves, 2 n_leaves).  Reads the
 // root back (the transcript needs it).
@@ -227,13 +248,19 @@ inline void build_tree(Ctx& c, TreeDev& t) {
     const uint32_t* const* tab = (const uint32_t* const*)t.inj_ptrs->p + first;
     uint32_t cnt = (uint32_t)(next - first);
     c.timed("merkle_inject", 96.0 * start * cnt, (double)start * cnt, [&] {
-      k_merkle_inject<<<(start + 19) / 20, 128, 0, c.stream>>>(t.nodes->p, start, tab, cnt);
+      if (p2_per_thread(c, start))
+        k_merkle_inject1<<<(start + 127) / 128, 128, 0, c.stream>>>(t.nodes->p, start, tab, cnt);
+      else
+        k_merkle_inject<<<(start + 19) / 20, 128, 0, c.stream>>>(t.nodes->p, start, tab, cnt);
       LG_LAUNCH();
     });
   };
   auto level = [&](uint32_t start) {
     c.timed("merkle_level", 96.0 * start, (double)start, [&] {
-      k_merkle_level<<<(start + 19) / 20, 128, 0, c.stream>>>(t.nodes->p, start);
+      if (p2_per_thread(c, start, P2_THREAD_MIN_NODES))
+        k_merkle_level1<<<(start + 127) / 128, 128, 0, c.stream>>>(t.nodes->p, start);
+      else
+        k_merkle_level<<<(start + 19) / 20, 128, 0, c.stream>>>(t.nodes->p, start);
       LG_LAUNCH();
     });
   };
@@ -242,7 +269,7 @@ inline void build_tree(Ctx& c, TreeDev& t) {
     for (size_t k = 0; k < t.inj.size(); k++)
       if ((1u << t.inj_log_w[k]) < top || (fold_first && (1u << t.inj_log_w[k]) == top)) perms += 1u << t.inj_log_w[k];
     c.timed("merkle_tail", 96.0 * perms, perms, [&] {
-      k_merkle_tail<<<1, 1024, 0, c.stream>>>(t.nodes->p, top, fold_first, (const InjRef*)ref_tab->p,
+      k_merkle_tail<<<1, tail_threads(top, fold_first), 0, c.stream>>>(t.nodes->p, top, fold_first, (const InjRef*)ref_tab->p,
                                              (uint32_t)refs.size());
       LG_LAUNCH();
     });

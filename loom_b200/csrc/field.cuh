@@ -38,9 +38,13 @@ LG_HD uint32_t umin(uint32_t a, uint32_t b) {
 LG_HD uint32_t add(uint32_t a, uint32_t b) { uint32_t s = a + b; return umin(s, s - P); }
 LG_HD uint32_t sub(uint32_t a, uint32_t b) { uint32_t d = a - b; return umin(d, d + P); }
 LG_HD uint32_t neg(uint32_t a) { return a ? P - a : 0; }
+// x in [0, 2p) -> [0, p)
+LG_HD uint32_t red(uint32_t x) { return umin(x, x - P); }
 LG_HD uint32_t dbl(uint32_t a) { return add(a, a); }
 
-// Montgomery product a*b*2^-32 mod p, inputs and output in [0, p).
+// Montgomery product a*b*2^-32 mod p, output in [0, p).  Inputs: b in
+// [0, p) and a in [0, p) or, unreduced, anywhere in [0, 2^32): then
+// t + m p < 2^33 p < 2^64 and the quotient stays below 2p.
 LG_HD uint32_t mul(uint32_t a, uint32_t b) {
   uint64_t t = (uint64_t)a * b;
   uint32_t m = (uint32_t)t * P_INV_NEG;

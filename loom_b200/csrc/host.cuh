@@ -87,7 +87,7 @@ struct Ctx {
   // events recorded on this context's stream around selected launches, with
   // the algorithmic bytes and Poseidon2 permutations of each launch.
   cudaEvent_t marks[16] = {};
-  struct KRec { const char* name; cudaEvent_t a, b; double bytes, perms; };
+  struct KRec { const char* name; cudaEvent_t a, b; double bytes, perms; size_t phase; };  // phase: index of the prove phase it ran in
   bool profiling = false;
   std::vector<KRec> recs;
   std::vector<cudaEvent_t> event_pool;
@@ -112,7 +112,7 @@ struct Ctx {
   }
   template <class F> void timed(const char* name, double bytes, double perms, F launch) {
     if (!profiling) { launch(); return; }
-    KRec r{name, pooled_event(), pooled_event(), bytes, perms};
+    KRec r{name, pooled_event(), pooled_event(), bytes, perms, phases.size()};
     LG_CK(cudaEventRecord(r.a, stream));
     launch();
     LG_CK(cudaEventRecord(r.b, stream));

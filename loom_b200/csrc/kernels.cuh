@@ -344,6 +344,40 @@ __global__ void k_merkle_inject(uint32_t* nodes, uint32_t start, const uint32_t*
   merkle_chain(nodes, (uint64_t)start + j, j, inj, n_inj, L, keys, L.lane < 30 && j < start);
 }
 
+// One thread per node (levels and injection chains wide enough to fill the
+// GPU): the fewest instructions per permutation.  Digests are 32-byte
+// aligned, so they move as two 16-byte words.
+__device__ __forceinline__ void ld_digest(const uint32_t* p, uint32_t d[8]) {
+  const uint4 a = reinterpret_cast<const uint4*>(p)[0], b = reinterpret_cast<const uint4*>(p)[1];
+  d[0] = a.x; d[1] = a.y; d[2] = a.z; d[3] = a.w; d[4] = b.x; d[5] = b.y; d[6] = b.z; d[7] = b.w;
+}
+__device__ __forceinline__ void st_digest(uint32_t* p, const uint32_t d[8]) {
+  reinterpret_cast<uint4*>(p)[0] = make_uint4(d[0], d[1], d[2], d[3]);
+  reinterpret_cast<uint4*>(p)[1] = make_uint4(d[4], d[5], d[6], d[7]);
+}
+__global__ void k_merkle_level1(uint32_t* nodes, uint32_t start) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= start) return;
+  const uint64_t id = (uint64_t)start + i;
+  uint32_t l[8], r[8];
+  ld_digest(nodes + 2 * id * 8, l);
+  ld_digest(nodes + (2 * id + 1) * 8, r);
+  p2_compress(to_mont(NODE_TAG), l, r, l);
+  st_digest(nodes + id * 8, l);
+}
+__global__ void k_merkle_inject1(uint32_t* nodes, uint32_t start, const uint32_t* const* inj, uint32_t n_inj) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= start) return;
+  uint32_t* nd = nodes + ((uint64_t)start + j) * 8;
+  uint32_t l[8], r[8];
+  ld_digest(nd, l);
+  for (uint32_t t = 0; t < n_inj; t++) {
+    ld_digest(inj[t] + (uint64_t)j * 8, r);
+    p2_compress(to_mont(NODE_TAG), l, r, l);
+  }
+  st_digest(nd, l);
+}
+
 // Upper tree levels in one block: for each width below `top`: the 2-to-1
 // step, then the injections of that width in schedule order.  When
 // fold_first, the injections of width `top` fold first (a tree whose leaf

@@ -400,14 +400,16 @@ int lg_profile_report(lg_ctx* ctx, char* buf, size_t* len) {
     LG_CK(cudaStreamSynchronize(ctx->c.stream));
     struct Acc { uint64_t n = 0; double ms = 0, bytes = 0, perms = 0; };
     std::map<std::string, Acc> acc;
+    std::vector<std::map<std::string, Acc>> by_phase(ctx->c.phases.size() + 1);
     for (auto& r : ctx->c.recs) {
       float ms = 0;
       LG_CK(cudaEventElapsedTime(&ms, r.a, r.b));
-      Acc& a = acc[r.name];
-      a.n++;
-      a.ms += ms;
-      a.bytes += r.bytes;
-      a.perms += r.perms;
+      for (Acc* a : {&acc[r.name], &by_phase[std::min(r.phase, ctx->c.phases.size())][r.name]}) {
+        a->n++;
+        a->ms += ms;
+        a->bytes += r.bytes;
+        a->perms += r.perms;
+      }
     }
     std::string js = "{";
     for (auto& kv : acc) {
@@ -423,6 +425,23 @@ int lg_profile_report(lg_ctx* ctx, char* buf, size_t* len) {
       char tmp[160];
       snprintf(tmp, sizeof tmp, "%s\"%s\": %.4f", i ? ", " : "", ctx->c.phases[i].first.c_str(), ctx->c.phases[i].second);
       js += tmp;
+    }
+    js += "}, \"kernels_by_phase\": {";
+    bool first = true;
+    for (size_t i = 0; i < ctx->c.phases.size(); i++) {
+      if (by_phase[i].empty()) continue;
+      js += first ? "\"" : ", \"";
+      first = false;
+      js += ctx->c.phases[i].first + "\": {";
+      bool f2 = true;
+      for (auto& kv : by_phase[i]) {
+        char tmp[256];
+        snprintf(tmp, sizeof tmp, "%s\"%s\": {\"launches\": %llu, \"ms\": %.6f, \"perms\": %.0f}", f2 ? "" : ", ",
+                 kv.first.c_str(), (unsigned long long)kv.second.n, kv.second.ms, kv.second.perms);
+        f2 = false;
+        js += tmp;
+      }
+      js += "}";
     }
     js += "}}";
     if (!buf || *len < js.size() + 1) {

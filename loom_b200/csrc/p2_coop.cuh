@@ -58,14 +58,26 @@ __device__ __forceinline__ void p2c_permute(uint32_t x[4], const P2Lane& L, cons
   p2c_external(x, L);
 #pragma unroll
   for (int r = 0; r < 3; r++) p2c_full(x, L, smem_keys + 24 * r);
+  // Partial rounds as p2_partial_rounds: R = s_1 + ... + s_23 is carried,
+  // the group sum of d_i s_i runs while lane idx 0 computes the S-box, and
+  // only the S-box output crosses lanes on the dependent chain.
+  uint32_t R = L.allreduce(add(add(L.idx ? x[0] : 0u, x[1]), add(x[2], x[3])));
 #pragma unroll 3
   for (int r = 0; r < 21; r++) {
-    if (L.idx == 0) x[0] = p2_cube(add(x[0], P2_PARTIAL_RK_D[r]));
-    uint32_t local = add(add(x[0], x[1]), add(x[2], x[3]));
-    uint32_t tot = L.allreduce(local);
+    uint32_t p[4];
 #pragma unroll
-    for (int i = 0; i < 4; i++) x[i] = add(tot, mul(x[i], L.diag[i]));
+    for (int i = 0; i < 4; i++) p[i] = mul(x[i], L.diag[i]);
+    const uint32_t D = L.allreduce(add(add(L.idx ? p[0] : 0u, p[1]), add(p[2], p[3])));
+    const uint32_t u = p2_cube(add(x[0], P2_PARTIAL_RK_D[r]));  // meaningful in lane idx 0
+    const uint32_t sum = add(__shfl_sync(0xffffffffu, u, L.base & 31), R);
+    const uint32_t pu = mul(u, L.diag[0]);
+    x[0] = add(sum, L.idx ? p[0] : pu);
+#pragma unroll
+    for (int i = 1; i < 4; i++) x[i] = sum + p[i];  // unreduced in [0, 2p) until the next product
+    R = add(mul(sum, MONT_23), D);
   }
+#pragma unroll
+  for (int i = 1; i < 4; i++) x[i] = red(x[i]);
 #pragma unroll
   for (int r = 3; r < 6; r++) p2c_full(x, L, smem_keys + 24 * r);
 }

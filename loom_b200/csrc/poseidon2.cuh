@@ -59,34 +59,85 @@ LG_HD void p2_external(uint32_t s[24]) {
 }
 
 LG_HD void p2_internal(uint32_t s[24]) {
-  uint32_t sum = s[0];
+  // pairwise sum: 5 dependent additions instead of 23
+  uint32_t t[12];
 #pragma unroll
-  for (int i = 1; i < 24; i++) sum = add(sum, s[i]);
+  for (int i = 0; i < 12; i++) t[i] = add(s[2 * i], s[2 * i + 1]);
+#pragma unroll
+  for (int i = 0; i < 6; i++) t[i] = add(t[2 * i], t[2 * i + 1]);
+#pragma unroll
+  for (int i = 0; i < 3; i++) t[i] = add(t[2 * i], t[2 * i + 1]);
+  const uint32_t sum = add(add(t[0], t[1]), t[2]);
 #pragma unroll
   for (int i = 0; i < 24; i++) s[i] = add(sum, mul(s[i], LG_P2_DIAG[i]));
 }
 
 LG_HD uint32_t p2_cube(uint32_t x) { return mul(sqr(x), x); }
 
+// Unrolling of the round loops.  A fully unrolled permutation is ~9K
+// instructions, more than the SM's instruction caches hold when warps drift
+// apart; rolled round loops keep the hot code small.
+#ifndef LG_P2_FULL_UNROLL
+#define LG_P2_FULL_UNROLL 1
+#endif
+#ifndef LG_P2_PARTIAL_UNROLL
+#define LG_P2_PARTIAL_UNROLL 3
+#endif
+#define LG_PRAGMA(x) _Pragma(#x)
+#define LG_UNROLL(n) LG_PRAGMA(unroll n)
+
+LG_HD void p2_full_round(uint32_t s[24], const uint32_t* rk) {
+#pragma unroll
+  for (int i = 0; i < 24; i++) s[i] = p2_cube(add(s[i], rk[i]));
+  p2_external(s);
+}
+
+// Pairwise sum of v[0..N): depth log2(N) instead of N - 1.
+template <int N> LG_HD uint32_t tree_sum(const uint32_t* v) {
+  if constexpr (N == 1) return v[0];
+  else return add(tree_sum<N / 2>(v), tree_sum<N - N / 2>(v + N / 2));
+}
+
+constexpr uint32_t P2_DIAG_C[24] = LG_P2_DIAG_INIT;
+static_assert(P2_DIAG_C[1] == MONT_ONE, "internal diagonal entry 1 is 1");
+constexpr uint32_t MONT_23 = 0x2dffffd2u;  // 23 * 2^32 mod p
+
+// Partial rounds (S-box on lane 0, internal layer 1.1^T + diag).  With
+// R = s_1 + ... + s_23 carried from round to round, one round is
+//   u = S(s_0 + c),  sum = u + R,  s_0 <- sum + d_0 u,  s_i <- sum + d_i s_i,
+//   R <- 23 sum + sum_{i>=1} d_i s_i   (s_i before the update),
+// which is the same linear map; the products d_i s_i and their sum no longer
+// wait for the S-box, so a round's dependent chain is the S-box and two
+// additions.  s_1 .. s_23 stay unreduced in [0, 2p) between rounds (their
+// only consumer is the next product d_i s_i, which accepts them), saving two
+// of the three instructions of each of their additions.
+LG_HD void p2_partial_rounds(uint32_t s[24]) {
+  uint32_t R = tree_sum<23>(s + 1);
+  LG_UNROLL(LG_P2_PARTIAL_UNROLL)
+  for (int r = 0; r < 21; r++) {
+    const uint32_t u = p2_cube(add(s[0], LG_P2_PARTIAL_RK[r]));
+    uint32_t p[24];
+    p[1] = red(s[1]);  // d_1 = 1
+#pragma unroll
+    for (int i = 2; i < 24; i++) p[i] = mul(s[i], LG_P2_DIAG[i]);
+    const uint32_t D = tree_sum<23>(p + 1);
+    const uint32_t sum = add(u, R);
+    s[0] = add(sum, mul(u, LG_P2_DIAG[0]));
+#pragma unroll
+    for (int i = 1; i < 24; i++) s[i] = sum + p[i];
+    R = add(mul(sum, MONT_23), D);
+  }
+#pragma unroll
+  for (int i = 1; i < 24; i++) s[i] = red(s[i]);
+}
+
 LG_HD void p2_permute(uint32_t s[24]) {
   p2_external(s);
-#pragma unroll
-  for (int r = 0; r < 3; r++) {
-#pragma unroll
-    for (int i = 0; i < 24; i++) s[i] = p2_cube(add(s[i], LG_P2_FULL_RK[r][i]));
-    p2_external(s);
-  }
-#pragma unroll 3
-  for (int r = 0; r < 21; r++) {
-    s[0] = p2_cube(add(s[0], LG_P2_PARTIAL_RK[r]));
-    p2_internal(s);
-  }
-#pragma unroll
-  for (int r = 3; r < 6; r++) {
-#pragma unroll
-    for (int i = 0; i < 24; i++) s[i] = p2_cube(add(s[i], LG_P2_FULL_RK[r][i]));
-    p2_external(s);
-  }
+  LG_UNROLL(LG_P2_FULL_UNROLL)
+  for (int r = 0; r < 3; r++) p2_full_round(s, LG_P2_FULL_RK[r]);
+  p2_partial_rounds(s);
+  LG_UNROLL(LG_P2_FULL_UNROLL)
+  for (int r = 3; r < 6; r++) p2_full_round(s, LG_P2_FULL_RK[r]);
 }
 
 // node = first 8 lanes of Perm([tag, 0 x7, left, right])
