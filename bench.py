@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--serve-shapes", type=int, default=8, help="distinct request shapes, replayed in turn")
     ap.add_argument("--serve-rate", type=str, default="8,16", help="Poisson arrival rates (requests/s) to sweep")
     ap.add_argument("--serve-streams", type=int, default=4)
-    ap.add_argument("--streams", type=str, default="2,4",
+    ap.add_argument("--streams", type=str, default="2,4,8",
                     help="concurrent proof streams for the throughput measurement")
     return ap.parse_args()
 

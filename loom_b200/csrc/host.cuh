@@ -101,6 +101,7 @@ struct Ctx {
     return event_pool[event_next++];
   }
   // Host wall time per prove phase (milliseconds), recorded when profiling.
+  std::vector<uint8_t> proof_buf;  // encoding of the last proof (Writer target)
   std::vector<std::pair<std::string, double>> phases;
   std::chrono::steady_clock::time_point phase_t0;
   void phase_start() { phase_t0 = std::chrono::steady_clock::now(); phases.clear(); }
@@ -322,9 +323,12 @@ inline E6 digest_e6(const Digest& d) { E6 r; for (int i = 0; i < 6; i++) r.c[i] 
 // ---------------------------------------------------------------- proof writer
 // Canonical encoding: 4-byte big-endian words, field elements canonical.
 // `el*` take Montgomery words; `raw*` take words already canonical.
+// Appends the proof encoding to a caller-owned buffer that is reused from
+// proof to proof (it only grows), so its pages are touched once.
 struct Writer {
-  std::vector<uint8_t> b;
+  std::vector<uint8_t>& b;
   size_t off = 0;
+  explicit Writer(std::vector<uint8_t>& buf) : b(buf) {}
   void reserve(size_t bytes) { if (b.size() < off + bytes) b.resize(std::max(b.size() * 2, off + bytes)); }
   void put(uint32_t x) {
     reserve(4);
@@ -348,13 +352,19 @@ struct Writer {
     }
     off += 4 * n;
   }
+  // words already in proof encoding (big-endian canonical bytes)
+  void bytes(const uint32_t* be, size_t n) {
+    reserve(4 * n);
+    memcpy(b.data() + off, be, 4 * n);
+    off += 4 * n;
+  }
   void str(const std::string& s) {
     put((uint32_t)s.size());
     reserve(s.size());
     memcpy(b.data() + off, s.data(), s.size());
     off += s.size();
   }
-  std::vector<uint8_t> take() { b.resize(off); return std::move(b); }
+  size_t length() const { return off; }
 };
 
 }  // namespace lg

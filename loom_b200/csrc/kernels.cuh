@@ -778,13 +778,16 @@ __global__ void k_fold(const uint32_t* layer, uint64_t n, E6 alpha, const uint32
 
 // ---------------------------------------------------------------- openings
 // Montgomery -> canonical, in place (proof encoding of gathered openings).
-__global__ void k_from_mont(uint32_t* x, uint64_t n) {
+// Montgomery words -> canonical values as big-endian bytes (the proof
+// encoding), in place.
+__global__ void k_proof_words(uint32_t* x, uint64_t n) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (i < n) x[i] = from_mont(x[i]);
+  if (i < n) x[i] = __byte_perm(from_mont(x[i]), 0, 0x0123);
 }
 
-// Row pairs: for every query q and source, the rows (lo, lo+1) of each lane,
-// lo = (s_q >> shift) & ~1, written at out[q * per_q + off + 2 lane + h].
+// Row pairs: for every query q and source, the rows lo and lo + 1 of each
+// lane, lo = (s_q >> shift) & ~1: row lo of every lane, then row lo + 1, at
+// out[q * per_q + off + h * n_lanes + lane] (the order the proof lists them).
 struct RowSrc { const uint32_t* lane0; uint64_t lane_stride; uint32_t n_lanes; uint32_t shift; uint64_t off; };
 __global__ void k_gather_rows(const RowSrc* srcs, uint32_t n_src, const uint32_t* pos, uint32_t nq, uint64_t per_q,
                               uint32_t* out) {
@@ -794,8 +797,8 @@ __global__ void k_gather_rows(const RowSrc* srcs, uint32_t n_src, const uint32_t
   if (q >= nq || l >= s.n_lanes) return;
   uint32_t lo = (pos[q] >> s.shift) & ~1u;
   const uint32_t* p = s.lane0 + l * s.lane_stride;
-  out[q * per_q + s.off + 2 * l] = p[lo];
-  out[q * per_q + s.off + 2 * l + 1] = p[lo + 1];
+  out[q * per_q + s.off + l] = p[lo];
+  out[q * per_q + s.off + s.n_lanes + l] = p[lo + 1];
 }
 
 // Merkle paths: siblings of leaf idx = ((s_q >> shift) >> 1), leaf level

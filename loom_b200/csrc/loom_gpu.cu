@@ -7,7 +7,7 @@ using namespace lg;
 
 struct lg_ctx {
   Ctx c;
-  std::vector<uint8_t> last_proof;
+  size_t last_proof_len = 0;  // bytes of the last proof in c.proof_buf
 };
 
 namespace {
@@ -135,22 +135,23 @@ int lg_prove(lg_ctx* ctx, const char* hash_backend, const uint32_t* program, siz
       throw Error(LG_ERR_UNSUPPORTED, "hash backend \"" + hb + "\" is not available on the GPU path (poseidon2 only)");
     if (!program || !proof_len) throw Error(LG_ERR_INVALID, "null argument");
     Prover pr(ctx->c, program, program_words, num_queries);
-    ctx->last_proof = pr.prove(witness, witness_on_device != 0);
-    size_t need = ctx->last_proof.size();
+    ctx->last_proof_len = 0;
+    ctx->last_proof_len = pr.prove(witness, witness_on_device != 0);
+    size_t need = ctx->last_proof_len;
     if (!proof || *proof_len < need) {
       *proof_len = need;
       throw Error(LG_ERR_BUFFER, "proof buffer too small");
     }
-    memcpy(proof, ctx->last_proof.data(), need);
+    memcpy(proof, ctx->c.proof_buf.data(), need);
     *proof_len = need;
   });
 }
 
 int lg_last_proof(lg_ctx* ctx, uint8_t* proof, size_t* proof_len) {
   if (!ctx || !proof_len) return LG_ERR_INVALID;
-  size_t need = ctx->last_proof.size();
+  size_t need = ctx->last_proof_len;
   if (!proof || *proof_len < need) { *proof_len = need; return LG_ERR_BUFFER; }
-  memcpy(proof, ctx->last_proof.data(), need);
+  memcpy(proof, ctx->c.proof_buf.data(), need);
   *proof_len = need;
   return LG_OK;
 }

@@ -6,7 +6,7 @@
 
 namespace lg {
 
-inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool on_device) {
+inline size_t Prover::prove(const uint32_t* const* witness, bool on_device) {
   c.phase_start();
   setup(witness, on_device);
   c.phase("setup+upload");
@@ -84,8 +84,10 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
             E6 z = e6_mul_base(zeta, mont_pow(root_of_unity_mont((int)p.logn), (uint64_t)s));
             zpoint[key] = z;
             auto b = std::make_shared<DBuf>(6 * (size_t)n, c.stream);
-            k_e6_powers<<<(n + 127) / 128, 128, 0, c.stream>>>(z, n, b->p);
-            LG_LAUNCH();
+            c.timed("claimed_values", 0, 0, [&] {
+              k_e6_powers<<<(n + 127) / 128, 128, 0, c.stream>>>(z, n, b->p);
+              LG_LAUNCH();
+            });
             zp[key] = b;
           }
           uint32_t n = 1u << p.logn;
@@ -96,8 +98,10 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
   if (!jobs.empty()) {
     auto jd = upload_vec(c, jobs);
     auto od = std::make_shared<DBuf>(6 * jobs.size(), c.stream);
-    k_dot<<<(unsigned)jobs.size(), 256, 0, c.stream>>>((const DotJob*)jd->p, od->p);
-    LG_LAUNCH();
+    c.timed("claimed_values", 0, 0, [&] {
+      k_dot<<<(unsigned)jobs.size(), 256, 0, c.stream>>>((const DotJob*)jd->p, od->p);
+      LG_LAUNCH();
+    });
     uint32_t* h = c.host_staging(dots.size());
     c.d2h(h, od->p, dots.size());
     memcpy(dots.data(), h, dots.size() * 4);
@@ -275,9 +279,11 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
         if (jl(l) == j) terms.push_back(AxpyTerm{lvl[l]->p, gam[l]});
       auto axpy = [&](const std::vector<AxpyTerm>& tv) {
         auto td = upload_vec(c, tv);
-        k_axpy_e6<<<(unsigned)((nj + 255) / 256), 256, 0, c.stream>>>(running->p, nj, (const AxpyTerm*)td->p,
-                                                                       (uint32_t)tv.size());
-        LG_LAUNCH();
+        c.timed("fri_axpy", 0, 0, [&] {
+          k_axpy_e6<<<(unsigned)((nj + 255) / 256), 256, 0, c.stream>>>(running->p, nj, (const AxpyTerm*)td->p,
+                                                                         (uint32_t)tv.size());
+          LG_LAUNCH();
+        });
       };
       if (!terms.empty()) {
         if (c.batched) axpy(terms);
@@ -375,24 +381,27 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
     auto rd = upload_vec(c, rows);
     uint32_t max_l = 1;
     for (auto& r : rows) max_l = std::max(max_l, r.n_lanes);
-    k_gather_rows<<<dim3((max_l + 63) / 64, num_queries, (unsigned)rows.size()), 64, 0, c.stream>>>(
-        (const RowSrc*)rd->p, (uint32_t)rows.size(), pos_d->p, num_queries, per_q, out_d->p);
-    LG_LAUNCH();
     auto pd = upload_vec(c, paths);
     uint32_t max_t = 1;
     for (auto& p : paths) max_t = std::max(max_t, p.log_leaves + p.n_inj);
-    k_gather_paths<<<dim3((max_t + 31) / 32, num_queries, (unsigned)paths.size()), 32, 0, c.stream>>>(
-        (const PathSrc*)pd->p, pos_d->p, num_queries, per_q, out_d->p);
-    LG_LAUNCH();
+    c.timed("openings", 8.0 * per_q * num_queries, 0, [&] {
+      k_gather_rows<<<dim3((max_l + 63) / 64, num_queries, (unsigned)rows.size()), 64, 0, c.stream>>>(
+          (const RowSrc*)rd->p, (uint32_t)rows.size(), pos_d->p, num_queries, per_q, out_d->p);
+      LG_LAUNCH();
+      k_gather_paths<<<dim3((max_t + 31) / 32, num_queries, (unsigned)paths.size()), 32, 0, c.stream>>>(
+          (const PathSrc*)pd->p, pos_d->p, num_queries, per_q, out_d->p);
+      LG_LAUNCH();
+      k_proof_words<<<(unsigned)((per_q * num_queries + 255) / 256), 256, 0, c.stream>>>(out_d->p,
+                                                                                         per_q * num_queries);
+      LG_LAUNCH();
+    });
   }
-  k_from_mont<<<(unsigned)((per_q * num_queries + 255) / 256), 256, 0, c.stream>>>(out_d->p, per_q * num_queries);
-  LG_LAUNCH();
   uint32_t* G = c.host_staging(per_q * num_queries);
   c.d2h(G, out_d->p, per_q * num_queries);
 
   c.phase("openings gather");
   // ---- canonical encoding (same order as the proof structs)
-  Writer W;
+  Writer W(c.proof_buf);
   W.reserve((size_t)4 * per_q * num_queries + (1 << 20));
   W.str("poseidon2");
   W.u32(0);
@@ -410,19 +419,17 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
       for (size_t i = nbp; i < cv[t][g].size(); i++) { W.u32((uint32_t)cv[t][g][i].size()); for (auto& v : cv[t][g][i]) W.e6(v); }
     }
   }
-  // gathered words are already canonical (k_from_mont)
-  auto wpair_e6 = [&](const uint32_t* q, uint64_t off) {  // lane-major (lo, hi) pairs of 6 lanes
-    uint32_t lo[6], hi[6];
-    for (int w = 0; w < 6; w++) { lo[w] = q[off + 2 * w]; hi[w] = q[off + 2 * w + 1]; }
-    W.raww(lo, 6);
-    W.raww(hi, 6);
+  // gathered words are already in proof encoding (k_proof_words), rows lo
+  // and lo + 1 each lane-contiguous
+  auto wpair_e6 = [&](const uint32_t* q, uint64_t off) {  // rows lo, hi of 6 lanes
+    W.bytes(q + off, 12);
   };
   auto wpath = [&](const uint32_t* q, uint64_t off, uint32_t leaf, uint32_t depth, uint32_t ninj) {
     W.u32(leaf);
     W.u32(depth);
-    W.raww(q + off, 8 * (size_t)depth);
+    W.bytes(q + off, 8 * (size_t)depth);
     W.u32(ninj);
-    W.raww(q + off + 8 * (size_t)depth, 8 * (size_t)ninj);
+    W.bytes(q + off + 8 * (size_t)depth, 8 * (size_t)ninj);
   };
   W.dg(levels_tree.root);
   W.u32((uint32_t)(L - 1));
@@ -464,20 +471,13 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
         const LdeOut& l = cm.groups[gi];
         const Group& G2 = trees[b].groups[gi];
         uint32_t nb = (uint32_t)G2.bcols.size(), ne = (uint32_t)G2.ecols.size();
-        (void)l;
-        uint32_t tmp[512];
+        if (l.lanes != nb + 6 * ne) throw Error(LG_ERR_INVALID, "opening row width");
         for (int h = 0; h < 2; h++) {
+          const uint32_t* row = q + off + (uint64_t)h * l.lanes;
           W.u32(nb);
-          for (uint32_t i0 = 0; i0 < nb; i0 += 512) {
-            uint32_t k = std::min<uint32_t>(512, nb - i0);
-            for (uint32_t i = 0; i < k; i++) tmp[i] = q[off + 2 * (i0 + i) + h];
-            W.raww(tmp, k);
-          }
+          W.bytes(row, nb);
           W.u32(ne);
-          for (uint32_t e = 0; e < ne; e++) {
-            for (int w = 0; w < 6; w++) tmp[w] = q[off + 2 * (nb + 6 * e + w) + h];
-            W.raww(tmp, 6);
-          }
+          W.bytes(row + nb, 6 * (size_t)ne);
         }
       };
       const LdeOut& top = cm.groups[cm.order[0]];
@@ -490,7 +490,7 @@ inline std::vector<uint8_t> Prover::prove(const uint32_t* const* witness, bool o
   }
   LG_CK(cudaStreamSynchronize(c.stream));
   c.phase("serialize");
-  return W.take();
+  return W.length();
 }
 
 }  // namespace lg

@@ -345,15 +345,17 @@ struct Prover {
       std::vector<GpJob> jv(jobs.begin() + first, jobs.begin() + first + count);
       std::vector<ScanJob> sv(scans.begin() + first, scans.begin() + first + count);
       auto jd = upload_vec(c, jv), sd = upload_vec(c, sv);
-      k_gp_ratio<<<dim3((max_n + T - 1) / T, (unsigned)count), T, smem, c.stream>>>((const GpJob*)jd->p,
-                                                                                    (const E6*)coins_d->p);
-      LG_LAUNCH();
-      k_scan_tiles<<<dim3(max_nt, (unsigned)count), SCAN_BLOCK, 0, c.stream>>>((const ScanJob*)sd->p);
-      LG_LAUNCH();
-      k_tile_prefix<<<(unsigned)((count + 63) / 64), 64, 0, c.stream>>>((const ScanJob*)sd->p, (uint32_t)count);
-      LG_LAUNCH();
-      k_gp_finish<<<dim3((max_n + 255) / 256, (unsigned)count), 256, 0, c.stream>>>((const ScanJob*)sd->p);
-      LG_LAUNCH();
+      c.timed("grand_product", 0, 0, [&] {
+        k_gp_ratio<<<dim3((max_n + T - 1) / T, (unsigned)count), T, smem, c.stream>>>((const GpJob*)jd->p,
+                                                                                      (const E6*)coins_d->p);
+        LG_LAUNCH();
+        k_scan_tiles<<<dim3(max_nt, (unsigned)count), SCAN_BLOCK, 0, c.stream>>>((const ScanJob*)sd->p);
+        LG_LAUNCH();
+        k_tile_prefix<<<(unsigned)((count + 63) / 64), 64, 0, c.stream>>>((const ScanJob*)sd->p, (uint32_t)count);
+        LG_LAUNCH();
+        k_gp_finish<<<dim3((max_n + 255) / 256, (unsigned)count), 256, 0, c.stream>>>((const ScanJob*)sd->p);
+        LG_LAUNCH();
+      });
     };
     if (c.batched) launch(0, jobs.size());
     else for (size_t i = 0; i < jobs.size(); i++) launch(i, 1);
@@ -557,9 +559,11 @@ struct Prover {
                            inv(mont_pow(to_mont(3), n))});
       }
       auto cd = upload_vec(c, cj);
-      k_quotient_chunks<<<dim3((max_n + 127) / 128, 6, (unsigned)cj.size()), 128, 0, c.stream>>>((const QcJob*)cd->p,
-                                                                                                inv(to_mont(4)));
-      LG_LAUNCH();
+      c.timed("quotient_chunks", 0, 0, [&] {
+        k_quotient_chunks<<<dim3((max_n + 127) / 128, 6, (unsigned)cj.size()), 128, 0, c.stream>>>(
+            (const QcJob*)cd->p, inv(to_mont(4)));
+        LG_LAUNCH();
+      });
     };
     if (c.batched) {
       std::vector<ModQ*> all;
@@ -570,7 +574,8 @@ struct Prover {
     }
   }
 
-  std::vector<uint8_t> prove(const uint32_t* const* witness, bool on_device);
+  // returns the proof length; the bytes are in c.proof_buf
+  size_t prove(const uint32_t* const* witness, bool on_device);
 };
 
 }  // namespace lg
