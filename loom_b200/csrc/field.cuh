@@ -53,6 +53,13 @@ LG_HD uint32_t mul(uint32_t a, uint32_t b) {
   return umin(r, r - P);
 }
 LG_HD uint32_t sqr(uint32_t a) { return mul(a, a); }
+// Montgomery product without the final reduction: result in [0, 2p) for
+// inputs in [0, p); fit to feed mul() as its unreduced operand.
+LG_HD uint32_t mul_lazy(uint32_t a, uint32_t b) {
+  uint64_t t = (uint64_t)a * b;
+  uint32_t m = (uint32_t)t * P_INV_NEG;
+  return (uint32_t)((t + (uint64_t)m * P) >> 32);
+}
 LG_HD uint32_t to_mont(uint32_t canonical) { return mul(canonical % P, R2); }
 LG_HD uint32_t from_mont(uint32_t m) { return mul(m, 1u); }
 LG_HD uint32_t mont_pow(uint32_t a, uint64_t e) {

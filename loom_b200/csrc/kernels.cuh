@@ -142,9 +142,19 @@ __global__ void k_lde(const LdeLane* lanes, int logn, int from_coeffs, const uin
         if (L.coef) L.coef[i] = c;
       }
     };
-    ntt16<false>(A, logn, tw_n, true, first, store);  // A is both work and result
+    // Coset 0 is <w_n> itself: its bit-reversed evaluations are the input
+    // values in bit-reversed order, which the DIT's first pass (local bits
+    // [0, 4): 16 consecutive positions) has just gathered.
+    auto coset0 = [&](uint32_t t, const uint32_t* v) {
+      uint4* q = reinterpret_cast<uint4*>(L.out + ((uint64_t)t << 4));
+      q[0] = make_uint4(v[0], v[1], v[2], v[3]);
+      q[1] = make_uint4(v[4], v[5], v[6], v[7]);
+      q[2] = make_uint4(v[8], v[9], v[10], v[11]);
+      q[3] = make_uint4(v[12], v[13], v[14], v[15]);
+    };
+    ntt16<false>(A, logn, tw_n, true, first, store, coset0);  // A is both work and result
   }
-  for (int a = 0; a < (1 << RATE_LOG); a++) {
+  for (int a = from_coeffs ? 0 : 1; a < (1 << RATE_LOG); a++) {
     const uint32_t e = bitrev32((uint32_t)a, RATE_LOG);
     uint32_t* o = L.out + (uint64_t)a * n;
     auto first = [&](uint32_t t, uint32_t r, int lo) {

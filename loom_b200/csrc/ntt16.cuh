@@ -82,12 +82,18 @@ __device__ __forceinline__ void pass_plan(int p, int logn, int& lo, int& s_lo, i
   }
 }
 
+struct NoHook {
+  __device__ void operator()(uint32_t, const uint32_t*) const {}
+};
+
 // Full transform of n = 2^logn >= 16 points.  Pass 0 takes its inputs from
-// `first(t, r, lo)` (a global gather, or a shared-memory read with a scale);
-// every pass but the last writes back to S (pad16 layout); the last pass
-// hands its 16 registers to `store(t, lo, v)`.
-template <bool DIF, class First, class Store>
-__device__ void ntt16(uint32_t* S, int logn, const uint32_t* tw, bool inverse, First first, Store store) {
+// `first(t, r, lo)` (a global gather, or a shared-memory read with a scale)
+// and shows them to `loaded(t, v)` before its butterflies; every pass but the
+// last writes back to S (pad16 layout); the last pass hands its 16 registers
+// to `store(t, lo, v)`.
+template <bool DIF, class First, class Store, class Loaded = NoHook>
+__device__ void ntt16(uint32_t* S, int logn, const uint32_t* tw, bool inverse, First first, Store store,
+                      Loaded loaded = Loaded()) {
   const uint32_t groups = (1u << logn) >> 4;
   const int np = pass_count(logn);
   for (int p = 0; p < np; p++) {
@@ -98,6 +104,7 @@ __device__ void ntt16(uint32_t* S, int logn, const uint32_t* tw, bool inverse, F
       if (p == 0) {
 #pragma unroll
         for (uint32_t r = 0; r < 16; r++) v[r] = first(t, r, lo);
+        loaded(t, v);
       } else {
 #pragma unroll
         for (uint32_t r = 0; r < 16; r++) v[r] = S[pad16(grp_index(t, r, lo))];

@@ -72,7 +72,7 @@ LG_HD void p2_internal(uint32_t s[24]) {
   for (int i = 0; i < 24; i++) s[i] = add(sum, mul(s[i], LG_P2_DIAG[i]));
 }
 
-LG_HD uint32_t p2_cube(uint32_t x) { return mul(sqr(x), x); }
+LG_HD uint32_t p2_cube(uint32_t x) { return mul(mul_lazy(x, x), x); }
 
 // Unrolling of the round loops.  A fully unrolled permutation is ~9K
 // instructions, more than the SM's instruction caches hold when warps drift
