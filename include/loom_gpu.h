@@ -92,8 +92,10 @@ const char* lg_last_error(lg_ctx* ctx);
  * (internal/fri/hash_backend.go:21-40) and WithNumFriQueries(num_queries)
  * (prover/prover.go:74-80), no setup columns, no public inputs.
  * `hash_backend` must be "poseidon2" (or "" = default); "sha256" and
- * "blake3" return LG_ERR_UNSUPPORTED.  On LG_ERR_BUFFER the proof is kept
- * in the context and lg_last_proof() copies it. */
+ * "blake3" return LG_ERR_UNSUPPORTED.  The proof is written straight into
+ * `proof` (capacity *proof_len; its length comes back in *proof_len).  On
+ * LG_ERR_BUFFER it is kept in the context instead and lg_last_proof()
+ * copies it out. */
 int lg_prove(lg_ctx* ctx, const char* hash_backend, const uint32_t* program, size_t program_words,
              const uint32_t* const* witness, int witness_on_device, uint32_t num_queries, uint8_t* proof,
              size_t* proof_len);

@@ -146,6 +146,30 @@ class Context:
         self._check(rc)
         return bytes(memoryview(self._proof_buf)[:n.value])
 
+    def prove_into(self, out, program_words: np.ndarray, witness: Sequence, num_queries: int,
+                   on_device: bool = False, hash_backend: str = "poseidon2") -> int:
+        """prove() writing the proof straight into `out` (a writable buffer:
+        bytearray, numpy uint8 array, ...), without the copy into a new bytes
+        object.  Returns the proof length; raises LoomError (LG_ERR_BUFFER,
+        needed size in the message) when `out` is too small."""
+        prog = _u32(program_words)
+        if on_device:
+            arr = (ctypes.c_void_p * max(1, len(witness)))(*[int(p) for p in witness])
+        else:
+            cols = [_u32(c) for c in witness]
+            arr = (ctypes.c_void_p * max(1, len(cols)))(*[c.ctypes.data for c in cols])
+        mv = memoryview(out).cast("B")
+        if mv.readonly:
+            raise TypeError("out must be writable")
+        buf = (ctypes.c_uint8 * len(mv)).from_buffer(mv)
+        n = ctypes.c_size_t(len(mv))
+        rc = self.L.lg_prove(self.h, hash_backend.encode(), prog.ctypes.data_as(u32p), prog.size, arr, int(on_device),
+                             num_queries, buf, ctypes.byref(n))
+        if rc == LG_ERR_BUFFER:
+            raise LoomError(rc, f"output buffer of {len(mv)} bytes is too small: the proof needs {n.value}")
+        self._check(rc)
+        return int(n.value)
+
     # ------------------------------------------------------------------ measurement
     def mark(self, slot: int):
         self._check(self.L.lg_timer_mark(self.h, slot))

@@ -249,7 +249,9 @@ inline void build_tree(Ctx& c, TreeDev& t) {
     uint32_t cnt = (uint32_t)(next - first);
     c.timed("merkle_inject", 96.0 * start * cnt, (double)start * cnt, [&] {
       if (p2_per_thread(c, start))
-        k_merkle_inject1<<<(start + 127) / 128, 128, 0, c.stream>>>(t.nodes->p, start, tab, cnt);
+        // one warp per block: chains are few (down to ~200 per SM) and long,
+        // so small blocks spread them evenly over the SMs
+        k_merkle_inject1<<<(start + 31) / 32, 32, 0, c.stream>>>(t.nodes->p, start, tab, cnt);
       else
         k_merkle_inject<<<(start + 19) / 20, 128, 0, c.stream>>>(t.nodes->p, start, tab, cnt);
       LG_LAUNCH();

@@ -323,17 +323,35 @@ inline E6 digest_e6(const Digest& d) { E6 r; for (int i = 0; i < 6; i++) r.c[i] 
 // ---------------------------------------------------------------- proof writer
 // Canonical encoding: 4-byte big-endian words, field elements canonical.
 // `el*` take Montgomery words; `raw*` take words already canonical.
-// Appends the proof encoding to a caller-owned buffer that is reused from
-// proof to proof (it only grows), so its pages are touched once.
+// Appends the proof encoding straight into the caller's output buffer while
+// it fits; past its end, moves what it has to `spill` (a context-owned buffer
+// reused from proof to proof, so its pages are touched once) and goes on
+// there.
 struct Writer {
-  std::vector<uint8_t>& b;
-  size_t off = 0;
-  explicit Writer(std::vector<uint8_t>& buf) : b(buf) {}
-  void reserve(size_t bytes) { if (b.size() < off + bytes) b.resize(std::max(b.size() * 2, off + bytes)); }
+  std::vector<uint8_t>& spill;
+  uint8_t* p;
+  size_t cap, off = 0;
+  bool external;
+  Writer(std::vector<uint8_t>& spill_buf, uint8_t* out, size_t out_cap) : spill(spill_buf) {
+    external = out && out_cap;
+    p = external ? out : spill.data();
+    cap = external ? out_cap : spill.size();
+  }
+  void reserve(size_t bytes) {
+    if (off + bytes <= cap) return;
+    size_t want = std::max(off + bytes, 2 * off + ((size_t)1 << 20));
+    if (spill.size() < want) spill.resize(want);
+    if (external) memcpy(spill.data(), p, off);
+    external = false;
+    p = spill.data();
+    cap = spill.size();
+  }
+  // size hint for the spill buffer (no effect while writing to the caller's)
+  void expect(size_t bytes) { if (!external) reserve(bytes); }
   void put(uint32_t x) {
     reserve(4);
     uint32_t be = __builtin_bswap32(x);
-    memcpy(b.data() + off, &be, 4);
+    memcpy(p + off, &be, 4);
     off += 4;
   }
   void u32(uint32_t x) { put(x); }
@@ -345,26 +363,27 @@ struct Writer {
   void raw(uint32_t canonical) { put(canonical); }
   void raww(const uint32_t* w, size_t n) {
     reserve(4 * n);
-    uint8_t* p = b.data() + off;
+    uint8_t* q = p + off;
     for (size_t i = 0; i < n; i++) {
       uint32_t be = __builtin_bswap32(w[i]);
-      memcpy(p + 4 * i, &be, 4);
+      memcpy(q + 4 * i, &be, 4);
     }
     off += 4 * n;
   }
   // words already in proof encoding (big-endian canonical bytes)
   void bytes(const uint32_t* be, size_t n) {
     reserve(4 * n);
-    memcpy(b.data() + off, be, 4 * n);
+    memcpy(p + off, be, 4 * n);
     off += 4 * n;
   }
   void str(const std::string& s) {
     put((uint32_t)s.size());
     reserve(s.size());
-    memcpy(b.data() + off, s.data(), s.size());
+    memcpy(p + off, s.data(), s.size());
     off += s.size();
   }
   size_t length() const { return off; }
+  bool in_caller_buffer() const { return external; }
 };
 
 }  // namespace lg

@@ -840,4 +840,36 @@ __global__ void k_gather_paths(const PathSrc* srcs, const uint32_t* pos, uint32_
   for (int w = 0; w < 8; w++) o[w] = src[w];
 }
 
+// Per-query proof sections.  Every query's part of a section has the same
+// layout, described once per section by a word map: code >> 30 = 0 copies
+// gathered word (code & 0x3fffffff) of the query, 1 is constant word
+// consts[code & ..], 2 is a position word of pos_ops[code & ..] (the query's
+// row or leaf index at some layer).  Output: big-endian words, query k of
+// section s at out + s.out_off + k * s.q_words.
+struct PosOp { uint32_t shift, leaf; };
+struct SectionSrc { uint64_t map_off, out_off; uint32_t q_words; };
+constexpr uint32_t SEC_COPY = 0u, SEC_CONST = 1u, SEC_POS = 2u;
+__global__ void k_assemble(const SectionSrc* secs, const uint32_t* map, const uint32_t* consts, const PosOp* pops,
+                           const uint32_t* pos, const uint32_t* gathered, uint64_t per_q, uint32_t nq, uint32_t* out) {
+  const SectionSrc sc = secs[blockIdx.z];
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
+  if (j >= sc.q_words || k >= nq) return;
+  const uint32_t code = map[sc.map_off + j], kind = code >> 30, idx = code & 0x3fffffffu;
+  uint32_t w;
+  if (kind == SEC_COPY) {
+    w = gathered[(uint64_t)k * per_q + idx];  // already big-endian (k_proof_words)
+  } else {
+    uint32_t v;
+    if (kind == SEC_CONST) {
+      v = consts[idx];
+    } else {
+      const PosOp op = pops[idx];
+      v = pos[k] >> op.shift;
+      if (op.leaf) v = (v & ~1u) >> 1;
+    }
+    w = __byte_perm(v, 0, 0x0123);
+  }
+  out[sc.out_off + (uint64_t)k * sc.q_words + j] = w;
+}
+
 }  // namespace lg

@@ -78,6 +78,12 @@ int lg_ctx_create(int device, lg_ctx** out) {
     LG_CK(cudaDeviceGetDefaultMemPool(&pool, device));
     uint64_t keep = UINT64_MAX;  // keep freed blocks for the next prove
     LG_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    // Concurrent contexts (one stream each) must not hand each other blocks
+    // whose frees are still queued on the other stream: the pool would make
+    // the allocating stream wait for the freeing one and serialise proofs.
+    int no = 0;
+    LG_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no));
+    LG_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowOpportunistic, &no));
     LG_CK(cudaDeviceGetAttribute(&ctx->c.sm_count, cudaDevAttrMultiProcessorCount, device));
   });
   if (rc != LG_OK) {
@@ -136,14 +142,13 @@ int lg_prove(lg_ctx* ctx, const char* hash_backend, const uint32_t* program, siz
     if (!program || !proof_len) throw Error(LG_ERR_INVALID, "null argument");
     Prover pr(ctx->c, program, program_words, num_queries);
     ctx->last_proof_len = 0;
-    ctx->last_proof_len = pr.prove(witness, witness_on_device != 0);
-    size_t need = ctx->last_proof_len;
-    if (!proof || *proof_len < need) {
-      *proof_len = need;
+    bool direct = false;
+    size_t need = pr.prove(witness, witness_on_device != 0, proof, proof ? *proof_len : 0, &direct);
+    *proof_len = need;
+    if (!direct) {  // did not fit: kept for lg_last_proof
+      ctx->last_proof_len = need;
       throw Error(LG_ERR_BUFFER, "proof buffer too small");
     }
-    memcpy(proof, ctx->c.proof_buf.data(), need);
-    *proof_len = need;
   });
 }
 

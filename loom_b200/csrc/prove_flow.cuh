@@ -6,7 +6,8 @@
 
 namespace lg {
 
-inline size_t Prover::prove(const uint32_t* const* witness, bool on_device) {
+inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint8_t* out, size_t out_cap,
+                            bool* in_out) {
   c.phase_start();
   setup(witness, on_device);
   c.phase("setup+upload");
@@ -396,13 +397,101 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device) {
       LG_LAUNCH();
     });
   }
-  uint32_t* G = c.host_staging(per_q * num_queries);
-  c.d2h(G, out_d->p, per_q * num_queries);
+  // ---- per-query sections, laid out on the GPU in proof order and encoding
+  struct SecBuild {
+    std::vector<uint32_t> map, consts;
+    std::vector<PosOp> pops;
+    std::vector<SectionSrc> secs;
+    uint64_t total = 0;
+    size_t start = 0;
+    void begin() { start = map.size(); }
+    void konst(uint32_t v) {
+      map.push_back((SEC_CONST << 30) | (uint32_t)consts.size());
+      consts.push_back(v);
+    }
+    void posw(uint32_t shift, bool leaf) {
+      map.push_back((SEC_POS << 30) | (uint32_t)pops.size());
+      pops.push_back(PosOp{shift, leaf ? 1u : 0u});
+    }
+    void copy(uint64_t off, size_t n) {
+      if (off + n > 0x3fffffffu) throw Error(LG_ERR_UNSUPPORTED, "opening block too large");
+      for (size_t i = 0; i < n; i++) map.push_back((uint32_t)(off + i));
+    }
+    SectionSrc end(uint32_t nq) {
+      SectionSrc sc{start, total, (uint32_t)(map.size() - start)};
+      secs.push_back(sc);
+      total += (uint64_t)nq * sc.q_words;
+      return sc;
+    }
+  } SB;
+  std::vector<SectionSrc> lvl_sec(L);
+  for (size_t l = 1; l < L; l++) {  // FRI level openings (one section per level)
+    SB.begin();
+    SB.konst(1);
+    SB.posw((uint32_t)jl(l), false);
+    SB.copy(lvl_row_off[l], 12);
+    SB.konst(0); SB.konst(0); SB.konst(0);
+    lvl_sec[l] = SB.end(num_queries);
+  }
+  SB.begin();  // FRI fold openings
+  SB.konst((uint32_t)(NR - r0));
+  for (int j = r0; j < NR; j++) {
+    SB.konst(1);
+    SB.posw((uint32_t)j, false);
+    SB.copy(fri_row_off[j], 12);
+    SB.posw((uint32_t)j, true);
+    SB.konst(ftrees[j].log_leaves);
+    SB.copy(fri_path_off[j], 8 * (size_t)ftrees[j].log_leaves);
+    SB.konst(0);
+  }
+  const SectionSrc fri_sec = SB.end(num_queries);
+  SB.begin();  // batch openings: rows of every group, the batch tree's path
+  SB.konst((uint32_t)committed.size());
+  for (size_t b = 0; b < committed.size(); b++) {
+    const Committed& cm = committed[b];
+    auto rowpair = [&](int gi, uint64_t off) {
+      const LdeOut& l = cm.groups[gi];
+      const Group& G2 = trees[b].groups[gi];
+      uint32_t nb = (uint32_t)G2.bcols.size(), ne = (uint32_t)G2.ecols.size();
+      if (l.lanes != nb + 6 * ne) throw Error(LG_ERR_INVALID, "opening row width");
+      for (int h = 0; h < 2; h++) {
+        SB.konst(nb);
+        SB.copy(off + (uint64_t)h * l.lanes, nb);
+        SB.konst(ne);
+        SB.copy(off + (uint64_t)h * l.lanes + nb, 6 * (size_t)ne);
+      }
+    };
+    const LdeOut& top = cm.groups[cm.order[0]];
+    rowpair(cm.order[0], boff[b].rows[0]);
+    SB.posw((uint32_t)(LOG_N_FRI - (top.log_n + RATE_LOG)), true);
+    SB.konst(cm.tree.log_leaves);
+    SB.copy(boff[b].path, 8 * (size_t)cm.tree.log_leaves);
+    SB.konst((uint32_t)cm.tree.inj.size());
+    SB.copy(boff[b].path + 8 * (size_t)cm.tree.log_leaves, 8 * cm.tree.inj.size());
+    SB.konst((uint32_t)(cm.order.size() - 1));
+    for (size_t s = 1; s < cm.order.size(); s++) rowpair(cm.order[s], boff[b].rows[s]);
+  }
+  const SectionSrc batch_sec = SB.end(num_queries);
+  auto asm_d = std::make_shared<DBuf>(SB.total, c.stream);
+  {
+    auto map_d = upload_vec(c, SB.map), consts_d = upload_vec(c, SB.consts);
+    auto pops_d = upload_vec(c, SB.pops), secs_d = upload_vec(c, SB.secs);
+    uint32_t max_q = 1;
+    for (auto& sc : SB.secs) max_q = std::max(max_q, sc.q_words);
+    c.timed("openings", 8.0 * SB.total, 0, [&] {
+      k_assemble<<<dim3((max_q + 255) / 256, num_queries, (unsigned)SB.secs.size()), 256, 0, c.stream>>>(
+          (const SectionSrc*)secs_d->p, map_d->p, consts_d->p, (const PosOp*)pops_d->p, pos_d->p, out_d->p, per_q,
+          num_queries, asm_d->p);
+      LG_LAUNCH();
+    });
+  }
+  uint32_t* A = c.host_staging(SB.total);
+  c.d2h(A, asm_d->p, SB.total);
 
   c.phase("openings gather");
   // ---- canonical encoding (same order as the proof structs)
-  Writer W(c.proof_buf);
-  W.reserve((size_t)4 * per_q * num_queries + (1 << 20));
+  Writer W(c.proof_buf, out, out_cap);
+  W.expect((size_t)4 * SB.total + (1 << 20));
   W.str("poseidon2");
   W.u32(0);
   W.u32((uint32_t)commitments.size());
@@ -419,29 +508,12 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device) {
       for (size_t i = nbp; i < cv[t][g].size(); i++) { W.u32((uint32_t)cv[t][g][i].size()); for (auto& v : cv[t][g][i]) W.e6(v); }
     }
   }
-  // gathered words are already in proof encoding (k_proof_words), rows lo
-  // and lo + 1 each lane-contiguous
-  auto wpair_e6 = [&](const uint32_t* q, uint64_t off) {  // rows lo, hi of 6 lanes
-    W.bytes(q + off, 12);
-  };
-  auto wpath = [&](const uint32_t* q, uint64_t off, uint32_t leaf, uint32_t depth, uint32_t ninj) {
-    W.u32(leaf);
-    W.u32(depth);
-    W.bytes(q + off, 8 * (size_t)depth);
-    W.u32(ninj);
-    W.bytes(q + off + 8 * (size_t)depth, 8 * (size_t)ninj);
-  };
+  auto section = [&](const SectionSrc& sc) { W.bytes(A + sc.out_off, (size_t)num_queries * sc.q_words); };
   W.dg(levels_tree.root);
   W.u32((uint32_t)(L - 1));
   for (size_t l = 1; l < L; l++) {
     W.u32(num_queries);
-    for (uint32_t k = 0; k < num_queries; k++) {
-      const uint32_t* q = G + (uint64_t)k * per_q;
-      W.u32(1);
-      W.u32(pos[k] >> jl(l));
-      wpair_e6(q, lvl_row_off[l]);
-      W.u32(0); W.u32(0); W.u32(0);
-    }
+    section(lvl_sec[l]);
   }
   W.u32((uint32_t)fri_roots.size());
   for (auto& d : fri_roots) W.dg(d);
@@ -449,47 +521,13 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device) {
   W.u32((uint32_t)nj);
   for (size_t i = 0; i < nj; i++) { uint32_t e[6]; for (int w = 0; w < 6; w++) e[w] = final_poly[w * nj + i]; W.e6w(e); }
   W.u32(num_queries);
-  for (uint32_t k = 0; k < num_queries; k++) {
-    const uint32_t* q = G + (uint64_t)k * per_q;
-    W.u32((uint32_t)(NR - r0));
-    for (int j = r0; j < NR; j++) {
-      uint32_t row = pos[k] >> j;
-      W.u32(1);
-      W.u32(row);
-      wpair_e6(q, fri_row_off[j]);
-      wpath(q, fri_path_off[j], (row & ~1u) / 2, ftrees[j].log_leaves, 0);
-    }
-  }
+  section(fri_sec);
   W.u32(0);
   W.u32(num_queries);
-  for (uint32_t k = 0; k < num_queries; k++) {
-    const uint32_t* q = G + (uint64_t)k * per_q;
-    W.u32((uint32_t)committed.size());
-    for (size_t b = 0; b < committed.size(); b++) {
-      const Committed& cm = committed[b];
-      auto wrowpair = [&](int gi, uint64_t off) {
-        const LdeOut& l = cm.groups[gi];
-        const Group& G2 = trees[b].groups[gi];
-        uint32_t nb = (uint32_t)G2.bcols.size(), ne = (uint32_t)G2.ecols.size();
-        if (l.lanes != nb + 6 * ne) throw Error(LG_ERR_INVALID, "opening row width");
-        for (int h = 0; h < 2; h++) {
-          const uint32_t* row = q + off + (uint64_t)h * l.lanes;
-          W.u32(nb);
-          W.bytes(row, nb);
-          W.u32(ne);
-          W.bytes(row + nb, 6 * (size_t)ne);
-        }
-      };
-      const LdeOut& top = cm.groups[cm.order[0]];
-      uint32_t top_row = pos[k] >> (LOG_N_FRI - (top.log_n + RATE_LOG));
-      wrowpair(cm.order[0], boff[b].rows[0]);
-      wpath(q, boff[b].path, (top_row & ~1u) / 2, cm.tree.log_leaves, (uint32_t)cm.tree.inj.size());
-      W.u32((uint32_t)(cm.order.size() - 1));
-      for (size_t s = 1; s < cm.order.size(); s++) wrowpair(cm.order[s], boff[b].rows[s]);
-    }
-  }
+  section(batch_sec);
   LG_CK(cudaStreamSynchronize(c.stream));
   c.phase("serialize");
+  *in_out = W.in_caller_buffer();
   return W.length();
 }
 

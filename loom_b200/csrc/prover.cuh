@@ -45,6 +45,7 @@ struct Prover {
   Prover(Ctx& ctx, const uint32_t* words, size_t nwords, uint32_t q) : c(ctx), num_queries(q) {
     pg = parse_program(words, nwords);
     if (q == 0) throw Error(LG_ERR_INVALID, "num_queries must be positive");
+    if (q > 65535) throw Error(LG_ERR_UNSUPPORTED, "num_queries above 65535 is not supported by this build");
   }
 
   size_t mod_n(uint32_t m) const { return (size_t)1 << pg.modules[m].log_n; }
@@ -411,6 +412,8 @@ struct Prover {
     };
     std::vector<ModQ> mods;
     std::vector<DBufP> keep;
+    // log n -> columns -> lanes (Lagrange values -> coefficients)
+    std::map<uint32_t, std::vector<std::vector<uint32_t*>>> verifier_intt;
     for (uint32_t m : mod_order) {
       if (!chunk_count(m)) continue;
       if (chunk_count(m) != 4) throw Error(LG_ERR_UNSUPPORTED, "quotient domains other than 4N are not supported by this build");
@@ -433,20 +436,11 @@ struct Prover {
           // verifier columns: coefficients of the Lagrange values
           auto b = std::make_shared<DBuf>(lanes_of(col) * n, c.stream);
           LG_CK(cudaMemcpyAsync(b->p, col_buf.at(col)->p, lanes_of(col) * n * 4, cudaMemcpyDeviceToDevice, c.stream));
+          // transformed in place below: batched, one launch per size over all
+          // modules; plain, one launch per column
           std::vector<uint32_t*> ls;
           for (uint32_t w = 0; w < lanes_of(col); w++) ls.push_back(b->p + (size_t)w * n);
-          if ((int)logn > SMEM_NTT_MAX_LOG) {
-            std::vector<BigNtt> jobs;
-            for (uint32_t* l : ls) jobs.push_back(big_job(l, l, inv(to_mont((uint32_t)n)), false));
-            big_ntt(c, jobs, (int)logn, true, "quotient_intt", 8.0 * n);
-          } else {
-            auto tab = upload_vec(c, ls);
-            allow_smem(k_intt, pad16_words((int)logn) * 4);
-            k_intt<<<lanes_of(col), ntt_threads((int)logn), pad16_words((int)logn) * 4, c.stream>>>((uint32_t* const*)tab->p, (int)logn,
-                                                                               c.twiddles((int)logn), inv(to_mont((uint32_t)n)));
-            LG_LAUNCH();
-            keep.push_back(tab);
-          }
+          verifier_intt[logn].push_back(ls);
           keep.push_back(b);
           for (uint32_t w = 0; w < lanes_of(col); w++) coef_lanes.push_back(b->p + (size_t)w * n);
         }
@@ -463,6 +457,33 @@ struct Prover {
       q.chunks = std::make_shared<DBuf>(4 * (root_ext[m] ? 6 : 1) * n, c.stream);
       chunk_coef[m] = q.chunks;
       mods.push_back(std::move(q));
+    }
+    auto intt_lanes = [&](uint32_t logn, const std::vector<uint32_t*>& lanes) {
+      const size_t n = (size_t)1 << logn;
+      if ((int)logn > SMEM_NTT_MAX_LOG) {
+        std::vector<BigNtt> jobs;
+        for (uint32_t* l : lanes) jobs.push_back(big_job(l, l, inv(to_mont((uint32_t)n)), false));
+        big_ntt(c, jobs, (int)logn, true, "quotient_intt", 8.0 * n);
+        return;
+      }
+      auto tab = upload_vec(c, lanes);
+      keep.push_back(tab);
+      allow_smem(k_intt, pad16_words((int)logn) * 4);
+      const uint32_t* twn = c.twiddles((int)logn);
+      c.timed("quotient_intt", 8.0 * n * lanes.size(), 0, [&] {
+        k_intt<<<(unsigned)lanes.size(), ntt_threads((int)logn), pad16_words((int)logn) * 4, c.stream>>>(
+            (uint32_t* const*)tab->p, (int)logn, twn, inv(to_mont((uint32_t)n)));
+        LG_LAUNCH();
+      });
+    };
+    for (auto& kv : verifier_intt) {
+      if (c.batched) {
+        std::vector<uint32_t*> all;
+        for (auto& col : kv.second) all.insert(all.end(), col.begin(), col.end());
+        intt_lanes(kv.first, all);
+      } else {
+        for (auto& col : kv.second) intt_lanes(kv.first, col);
+      }
     }
     if (mods.empty()) return;
     auto coins_d = coins_on_device();
@@ -574,8 +595,9 @@ struct Prover {
     }
   }
 
-  // returns the proof length; the bytes are in c.proof_buf
-  size_t prove(const uint32_t* const* witness, bool on_device);
+  // Returns the proof length.  The bytes go to out[0, out_cap) when they fit
+  // (*in_out = true), else to c.proof_buf.
+  size_t prove(const uint32_t* const* witness, bool on_device, uint8_t* out, size_t out_cap, bool* in_out);
 };
 
 }  // namespace lg

@@ -139,6 +139,26 @@ def test_repeated_proves_identical(ctx):
     assert a == b
 
 
+def test_prove_into_caller_buffer(ctx):
+    """The proof lands in the caller's buffer (exact size, and larger); a
+    buffer one byte short is refused with LG_ERR_BUFFER and the needed size,
+    and the context keeps that proof for lg_last_proof (prove() re-reads it)."""
+    compiled, wit = plonk.build(2, 1 << 9, seed=5)
+    mont = [F.to_mont(w) for w in wit]
+    ref = ctx.prove(compiled.words, mont, 8)
+    exact = bytearray(len(ref))
+    assert ctx.prove_into(exact, compiled.words, mont, 8) == len(ref)
+    assert bytes(exact) == ref
+    big = np.zeros(len(ref) + 4096, dtype=np.uint8)
+    n = ctx.prove_into(big, compiled.words, mont, 8)
+    assert n == len(ref) and big[:n].tobytes() == ref and not big[n:].any()
+    with pytest.raises(LoomError) as e:
+        ctx.prove_into(bytearray(len(ref) - 1), compiled.words, mont, 8)
+    assert e.value.code == 5 and str(len(ref)) in str(e.value)
+    ctx._proof_cap = 16  # force prove() through LG_ERR_BUFFER + lg_last_proof
+    assert ctx.prove(compiled.words, mont, 8) == ref
+
+
 def test_unsupported_hash_backend(ctx):
     compiled, wit = plonk.build(1, 1 << 4, seed=1)
     mont = [F.to_mont(w) for w in wit]
