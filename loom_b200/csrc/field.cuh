@@ -53,6 +53,39 @@ LG_HD uint32_t mul(uint32_t a, uint32_t b) {
   return umin(r, r - P);
 }
 LG_HD uint32_t sqr(uint32_t a) { return mul(a, a); }
+
+// Product by a fixed constant w (canonical, < p) with its precomputed
+// companion ws = floor(w 2^32 / p) (Shoup's precomputed-quotient method):
+// q = hi(x ws) under-estimates floor(x w / p) by at most one, so
+// r = x w - q p (mod 2^32) lies in [0, 2p) for every x < 2^32, unreduced
+// inputs included.  Three 32-bit multiplies, no 64-bit product.  Montgomery
+// words need no conversion: (x R) w = (x w) R.
+constexpr uint32_t shoup(uint32_t w) { return (uint32_t)(((uint64_t)w << 32) / P); }
+LG_HD uint32_t umulhi32(uint32_t a, uint32_t b) {
+#ifdef __CUDA_ARCH__
+  return __umulhi(a, b);
+#else
+  return (uint32_t)(((uint64_t)a * b) >> 32);
+#endif
+}
+LG_HD uint32_t mulc_lazy(uint32_t x, uint32_t w, uint32_t ws) { return x * w - umulhi32(x, ws) * P; }
+LG_HD uint32_t mulc(uint32_t x, uint32_t w, uint32_t ws) {
+  const uint32_t r = mulc_lazy(x, w, ws);
+  return umin(r, r - P);
+}
+
+// Compile-time field arithmetic on canonical values (constant tables).
+constexpr uint32_t cx_mulmod(uint32_t a, uint32_t b) { return (uint32_t)((uint64_t)a * b % P); }
+constexpr uint32_t cx_pow(uint32_t a, uint64_t e) {
+  uint32_t r = 1;
+  while (e) {
+    if (e & 1) r = cx_mulmod(r, a);
+    a = cx_mulmod(a, a);
+    e >>= 1;
+  }
+  return r;
+}
+constexpr uint32_t cx_from_mont(uint32_t m) { return cx_mulmod(m, cx_pow(MONT_ONE, P - 2)); }
 // Montgomery product without the final reduction: result in [0, 2p) for
 // inputs in [0, p); fit to feed mul() as its unreduced operand.
 LG_HD uint32_t mul_lazy(uint32_t a, uint32_t b) {

@@ -17,12 +17,15 @@ namespace lg {
 
 struct P2Lane {
   int lane, base, idx;    // warp lane, first lane of the group, index in the group (0..5)
-  uint32_t diag[4];       // internal diagonal for this lane's four elements
+  uint32_t dw[4], dws[4];  // internal diagonal (canonical, Shoup companion) of this lane's four elements
   __device__ __forceinline__ void init() {
     lane = threadIdx.x & 31;
     idx = lane % 6;
     base = lane - idx;
-    for (int i = 0; i < 4; i++) diag[i] = P2_DIAG_D[(4 * idx + i) % 24];
+    for (int i = 0; i < 4; i++) {
+      dw[i] = P2_DSH_D.w[(4 * idx + i) % 24];
+      dws[i] = P2_DSH_D.ws[(4 * idx + i) % 24];
+    }
   }
   __device__ __forceinline__ int at(int k) const { return (base + ((idx + k) % 6)) & 31; }
   // sum over the group's six lanes, in every lane
@@ -66,15 +69,15 @@ __device__ __forceinline__ void p2c_permute(uint32_t x[4], const P2Lane& L, cons
   for (int r = 0; r < 21; r++) {
     uint32_t p[4];
 #pragma unroll
-    for (int i = 0; i < 4; i++) p[i] = mul(x[i], L.diag[i]);
+    for (int i = 0; i < 4; i++) p[i] = mulc(x[i], L.dw[i], L.dws[i]);
     const uint32_t D = L.allreduce(add(add(L.idx ? p[0] : 0u, p[1]), add(p[2], p[3])));
     const uint32_t u = p2_cube(add(x[0], P2_PARTIAL_RK_D[r]));  // meaningful in lane idx 0
     const uint32_t sum = add(__shfl_sync(0xffffffffu, u, L.base & 31), R);
-    const uint32_t pu = mul(u, L.diag[0]);
+    const uint32_t pu = mulc(u, L.dw[0], L.dws[0]);
     x[0] = add(sum, L.idx ? p[0] : pu);
 #pragma unroll
     for (int i = 1; i < 4; i++) x[i] = sum + p[i];  // unreduced in [0, 2p) until the next product
-    R = add(mul(sum, MONT_23), D);
+    R = add(mulc(sum, C23, C23_SH), D);
   }
 #pragma unroll
   for (int i = 1; i < 4; i++) x[i] = red(x[i]);

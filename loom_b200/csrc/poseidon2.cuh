@@ -100,7 +100,29 @@ template <int N> LG_HD uint32_t tree_sum(const uint32_t* v) {
 
 constexpr uint32_t P2_DIAG_C[24] = LG_P2_DIAG_INIT;
 static_assert(P2_DIAG_C[1] == MONT_ONE, "internal diagonal entry 1 is 1");
-constexpr uint32_t MONT_23 = 0x2dffffd2u;  // 23 * 2^32 mod p
+
+// The internal diagonal as canonical constants with their Shoup companions
+// (products by d_i need no 64-bit multiply), and 23 for the carried sum.
+struct P2DiagShoup { uint32_t w[24], ws[24]; };
+constexpr P2DiagShoup make_p2_diag_shoup() {
+  P2DiagShoup d{};
+  for (int i = 0; i < 24; i++) {
+    d.w[i] = cx_from_mont(P2_DIAG_C[i]);
+    d.ws[i] = shoup(d.w[i]);
+  }
+  return d;
+}
+constexpr P2DiagShoup P2_DSH_H = make_p2_diag_shoup();
+static_assert(P2_DSH_H.w[1] == 1, "internal diagonal entry 1 is 1");
+#ifdef __CUDACC__
+__constant__ P2DiagShoup P2_DSH_D = make_p2_diag_shoup();
+#endif
+#ifdef __CUDA_ARCH__
+#define LG_P2_DSH P2_DSH_D
+#else
+#define LG_P2_DSH P2_DSH_H
+#endif
+constexpr uint32_t C23 = 23, C23_SH = shoup(23);
 
 // Partial rounds (S-box on lane 0, internal layer 1.1^T + diag).  With
 // R = s_1 + ... + s_23 carried from round to round, one round is
@@ -119,13 +141,13 @@ LG_HD void p2_partial_rounds(uint32_t s[24]) {
     uint32_t p[24];
     p[1] = red(s[1]);  // d_1 = 1
 #pragma unroll
-    for (int i = 2; i < 24; i++) p[i] = mul(s[i], LG_P2_DIAG[i]);
+    for (int i = 2; i < 24; i++) p[i] = mulc(s[i], LG_P2_DSH.w[i], LG_P2_DSH.ws[i]);
     const uint32_t D = tree_sum<23>(p + 1);
     const uint32_t sum = add(u, R);
-    s[0] = add(sum, mul(u, LG_P2_DIAG[0]));
+    s[0] = add(sum, mulc(u, LG_P2_DSH.w[0], LG_P2_DSH.ws[0]));
 #pragma unroll
     for (int i = 1; i < 24; i++) s[i] = sum + p[i];
-    R = add(mul(sum, MONT_23), D);
+    R = add(mulc(sum, C23, C23_SH), D);
   }
 #pragma unroll
   for (int i = 1; i < 24; i++) s[i] = red(s[i]);
