@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--serve-shapes", type=int, default=8, help="distinct request shapes, replayed in turn")
     ap.add_argument("--serve-rate", type=str, default="8,16", help="Poisson arrival rates (requests/s) to sweep")
     ap.add_argument("--serve-streams", type=int, default=4)
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (library defaults)")
+    ap.add_argument("--retune", action="store_true", help="re-measure even if the tuning cache has this GPU")
     ap.add_argument("--streams", type=str, default="2,4,8",
                     help="concurrent proof streams for the throughput measurement")
     return ap.parse_args()
@@ -290,6 +292,11 @@ def main():
     torch.cuda.synchronize()
 
     ctx = Context(device)
+    tune = None
+    if not a.no_tune:
+        from loom_b200 import autotune as AT
+        tune = AT.autotune(ctx, force=a.retune)
+    tparams = tune["params"] if tune else None
 
     def barrier():
         if dist is not None:
@@ -349,7 +356,7 @@ def main():
     from loom_b200.pool import ProverPool
     thr = []
     for S in [int(x) for x in a.streams.split(",") if x]:
-        with ProverPool(S, device) as pool:
+        with ProverPool(S, device, tparams) as pool:
             for f in [pool.submit(comp.words, dev_ptrs, a.queries, on_device=True) for _ in range(S)]:
                 f.result()  # warm every context
             jobs = S * max(2, a.steps)
@@ -374,7 +381,7 @@ def main():
         shapes = [(int(rng.integers(12, 21)), int(rng.integers(1, 9))) for _ in range(a.serve_shapes)]
         pool_reqs = [SV.make_request(i, lg, inst, a.queries, seed=0x77 + i) for i, (lg, inst) in enumerate(shapes)]
         # sequential plain-GPU proving of each shape once (the comparison baseline)
-        pctx = Context(device)
+        pctx = Context(device, tparams)
         pctx.set_batched(False)
         plain_one = []
         ref_proof = {}
@@ -393,7 +400,7 @@ def main():
                 reqs.append(SV.Request(i, t.words, t.witness, t.num_queries, t.rows))
             shape_of = {i: i % len(pool_reqs) for i in range(a.serve_requests)}
             res = SV.serve(reqs, SV.poisson_arrivals(len(reqs), rate, 11), streams=a.serve_streams, device=device,
-                           warm=pool_reqs)
+                           warm=pool_reqs, tuning=tparams)
             same = all(r.proof == ref_proof[shape_of[r.rid]] for r in res["finished"])
             seq_ms = sum(plain_one[shape_of[i]] for i in range(a.serve_requests))
             sweeps.append({"rate_per_s": rate, "requests": res["requests"], "p50_ms": round(res["p50_ms"], 2),
@@ -506,6 +513,7 @@ def main():
             "kernel_shares": shares,
             "kernel_ms_profiled_step": round(total_k, 3),
             "host_phases_ms": {k: round(v, 3) for k, v in phases.items()},
+            "tuning": tune,
             "kernel_ms_by_phase": {ph: {k: round(v["ms"], 3) for k, v in ks.items()} for ph, ks in by_phase.items()},
             "dominant_kernel": dom,
             "cpu_baseline": base,

@@ -82,6 +82,18 @@ int lg_ctx_set_batched(lg_ctx* ctx, int batched);
  * the number of independent chains per launch (default).  Results do not
  * depend on it. */
 int lg_ctx_set_leaf_mapping(lg_ctx* ctx, int lanes_per_permutation);
+/* Launch-shape choices (no counterpart in the reference: the autotuner in
+ * loom_b200/autotune.py sets them from measurements).  Proof bytes never
+ * depend on them.  Names and ranges:
+ *   "p2_leaf_min_per_sm"  one thread per leaf / injection chain when a launch
+ *                         has at least this many per SM (else six lanes)
+ *   "p2_node_min_per_sm"  the same for one-permutation Merkle levels
+ *   "merkle_tail"         levels narrower than this (power of two, 2..1024)
+ *                         run in one block
+ *   "inject_block", "leaf_block"  threads per block (power of two, 32..1024)
+ * Unknown names or values out of range return LG_ERR_INVALID. */
+int lg_ctx_set_tuning(lg_ctx* ctx, const char* name, int64_t value);
+int lg_ctx_get_tuning(lg_ctx* ctx, const char* name, int64_t* value);
 /* Free and total device memory of the context's GPU (serving admission). */
 int lg_mem_info(lg_ctx* ctx, uint64_t* free_bytes, uint64_t* total_bytes);
 /* NUL-terminated description of the last failure on `ctx` (never NULL). */

@@ -16,7 +16,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libloom_gpu.so")
 
 LG_OK, LG_ERR_INVALID, LG_ERR_CUDA, LG_ERR_OOM, LG_ERR_UNSUPPORTED, LG_ERR_BUFFER = range(6)
-EXPORTS = ["lg_ctx_create", "lg_ctx_destroy", "lg_ctx_set_batched", "lg_ctx_set_leaf_mapping", "lg_mem_info", "lg_last_error", "lg_prove", "lg_last_proof", "lg_commit_root",
+EXPORTS = ["lg_ctx_create", "lg_ctx_destroy", "lg_ctx_set_batched", "lg_ctx_set_leaf_mapping", "lg_ctx_set_tuning",
+           "lg_ctx_get_tuning", "lg_mem_info", "lg_last_error", "lg_prove", "lg_last_proof", "lg_commit_root",
            "lg_rs_encode", "lg_poseidon2_permute", "lg_merkle_root", "lg_fri_fold", "lg_timer_mark",
            "lg_timer_elapsed", "lg_kernel_launches", "lg_profile", "lg_profile_report", "lg_grand_product", "lg_grand_product_noalloc", "lg_deep_quotient"]
 
@@ -46,6 +47,8 @@ def load():
         L.lg_ctx_destroy.restype = None
         L.lg_ctx_set_batched.argtypes = [vp, ctypes.c_int]
         L.lg_ctx_set_leaf_mapping.argtypes = [vp, ctypes.c_int]
+        L.lg_ctx_set_tuning.argtypes = [vp, ctypes.c_char_p, ctypes.c_int64]
+        L.lg_ctx_get_tuning.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]
         L.lg_mem_info.argtypes = [vp, u64p, u64p]
         L.lg_last_error.argtypes = [vp]
         L.lg_last_error.restype = ctypes.c_char_p
@@ -84,14 +87,19 @@ def _ptr(a: np.ndarray):
 class Context:
     """A device context (lg_ctx): one CUDA stream, caches and memory pool."""
 
-    def __init__(self, device: int = 0):
+    def __init__(self, device: int = 0, tuning: Optional[dict] = None):
+        """`tuning`: launch-shape values to apply (see set_tuning), e.g. the
+        "params" of loom_b200.autotune.autotune()."""
         self.L = load()
+        self.device = device
         self.h = ctypes.c_void_p()
         rc = self.L.lg_ctx_create(device, ctypes.byref(self.h))
         if rc != LG_OK:
             raise LoomError(rc, f"lg_ctx_create failed on device {device}")
         self._proof_cap = 1 << 22
         self._proof_buf = (ctypes.c_uint8 * self._proof_cap)()
+        if tuning:
+            self.apply_tuning(tuning)
 
     def close(self):
         if self.h:
@@ -118,6 +126,24 @@ class Context:
         f, t = ctypes.c_uint64(), ctypes.c_uint64()
         self._check(self.L.lg_mem_info(self.h, ctypes.byref(f), ctypes.byref(t)))
         return int(f.value), int(t.value)
+
+    TUNING_NAMES = ("p2_leaf_min_per_sm", "p2_node_min_per_sm", "merkle_tail", "inject_block", "leaf_block")
+
+    def set_tuning(self, name: str, value: int):
+        """Launch-shape choice (see include/loom_gpu.h); proofs do not depend on it."""
+        self._check(self.L.lg_ctx_set_tuning(self.h, name.encode(), int(value)))
+
+    def get_tuning(self, name: str) -> int:
+        v = ctypes.c_int64()
+        self._check(self.L.lg_ctx_get_tuning(self.h, name.encode(), ctypes.byref(v)))
+        return int(v.value)
+
+    def tuning(self) -> dict:
+        return {n: self.get_tuning(n) for n in self.TUNING_NAMES}
+
+    def apply_tuning(self, params: dict):
+        for n, v in params.items():
+            self.set_tuning(n, v)
 
     def set_leaf_mapping(self, lanes: int):
         """Poseidon2 leaf hashing: 1 or 6 lanes per permutation, 0 = auto."""

@@ -133,9 +133,8 @@ inline void launch_lde(Ctx& c, const std::vector<LdeLane>& lanes, uint32_t log_n
 // one thread per chain (fewest instructions per permutation); otherwise six
 // lanes per chain for a dependent chain six times shorter.  Measured on B200:
 // one thread per chain wins for leaf hashing and injection chains from 128
-// chains per SM, for one-permutation Merkle levels from 512.
-constexpr uint32_t P2_THREAD_MIN_LEAVES = 128, P2_THREAD_MIN_NODES = 512;
-inline bool p2_per_thread(const Ctx& c, uint64_t parallel, uint32_t per_sm = P2_THREAD_MIN_LEAVES) {
+// chains per SM, for one-permutation Merkle levels from 512 (Ctx::tune).
+inline bool p2_per_thread(const Ctx& c, uint64_t parallel, uint32_t per_sm) {
   return c.leaf_mapping == 1 || (c.leaf_mapping == 0 && parallel >= (uint64_t)c.sm_count * per_sm);
 }
 
@@ -152,10 +151,11 @@ inline void launch_leaves(Ctx& c, const std::vector<LeafGroup>& gs) {
   auto tab = upload_vec(c, gs);
   uint64_t all_leaves = 0;
   for (auto& g : gs) all_leaves += g.n_leaves;
-  bool per_thread = p2_per_thread(c, all_leaves);
+  bool per_thread = p2_per_thread(c, all_leaves, c.tune.p2_leaf_min_per_sm);
+  const unsigned lb = c.tune.leaf_block;
   c.timed("hash_leaves", bytes, perms, [&] {
     if (per_thread)
-      k_hash_leaves1<<<dim3((max_leaves + 127) / 128, (unsigned)gs.size()), 128, 0, c.stream>>>((const LeafGroup*)tab->p);
+      k_hash_leaves1<<<dim3((max_leaves + lb - 1) / lb, (unsigned)gs.size()), lb, 0, c.stream>>>((const LeafGroup*)tab->p);
     else
       k_hash_leaves<<<dim3((max_leaves + 19) / 20, (unsigned)gs.size()), 128, 0, c.stream>>>((const LeafGroup*)tab->p);
     LG_LAUNCH();
@@ -211,11 +211,6 @@ struct TreeDev {
 // Levels below this width run in one block (k_merkle_tail); wider levels are
 // grid launches.  The block is throughput bound on its one SM at wide levels
 // and latency bound at narrow ones.
-#ifndef LG_MERKLE_TAIL
-#define LG_MERKLE_TAIL 64
-#endif
-constexpr uint32_t MERKLE_TAIL = LG_MERKLE_TAIL;
-static_assert(MERKLE_TAIL >= 2 && MERKLE_TAIL <= 1024 && (MERKLE_TAIL & (MERKLE_TAIL - 1)) == 0, "tail width");
 // six lanes per permutation, five permutations per warp
 inline unsigned tail_threads(uint32_t top, int fold_first) {
   uint32_t perms = std::max(1u, fold_first ? top : top / 2);
@@ -248,18 +243,19 @@ inline void build_tree(Ctx& c, TreeDev& t) {
     const uint32_t* const* tab = (const uint32_t* const*)t.inj_ptrs->p + first;
     uint32_t cnt = (uint32_t)(next - first);
     c.timed("merkle_inject", 96.0 * start * cnt, (double)start * cnt, [&] {
-      if (p2_per_thread(c, start))
-        // one warp per block: chains are few (down to ~200 per SM) and long,
-        // so small blocks spread them evenly over the SMs
-        k_merkle_inject1<<<(start + 31) / 32, 32, 0, c.stream>>>(t.nodes->p, start, tab, cnt);
-      else
+      if (p2_per_thread(c, start, c.tune.p2_leaf_min_per_sm)) {
+        // small blocks (one warp by default): chains are few (down to ~200
+        // per SM) and long, so small blocks spread them evenly over the SMs
+        const unsigned ib = c.tune.inject_block;
+        k_merkle_inject1<<<(start + ib - 1) / ib, ib, 0, c.stream>>>(t.nodes->p, start, tab, cnt);
+      } else
         k_merkle_inject<<<(start + 19) / 20, 128, 0, c.stream>>>(t.nodes->p, start, tab, cnt);
       LG_LAUNCH();
     });
   };
   auto level = [&](uint32_t start) {
     c.timed("merkle_level", 96.0 * start, (double)start, [&] {
-      if (p2_per_thread(c, start, P2_THREAD_MIN_NODES))
+      if (p2_per_thread(c, start, c.tune.p2_node_min_per_sm))
         k_merkle_level1<<<(start + 127) / 128, 128, 0, c.stream>>>(t.nodes->p, start);
       else
         k_merkle_level<<<(start + 19) / 20, 128, 0, c.stream>>>(t.nodes->p, start);
@@ -276,22 +272,23 @@ inline void build_tree(Ctx& c, TreeDev& t) {
       LG_LAUNCH();
     });
   };
+  const uint32_t tail_w = c.tune.merkle_tail;
   // the tail block chains at most 64 injections of one width
   bool tail_ok = true;
   for (size_t k = 0; k < t.inj.size(); k++) {
     size_t same = 0;
     for (size_t q = 0; q < t.inj.size(); q++) same += t.inj_log_w[q] == t.inj_log_w[k];
-    if ((1u << t.inj_log_w[k]) <= MERKLE_TAIL && same > 64) tail_ok = false;
+    if ((1u << t.inj_log_w[k]) <= tail_w && same > 64) tail_ok = false;
   }
   if (!c.batched || !tail_ok) {
     fold(nl);
     for (uint32_t start = nl >> 1; start >= 1; start >>= 1) { level(start); fold(start); }
-  } else if (nl <= MERKLE_TAIL) {
+  } else if (nl <= tail_w) {
     tail(nl, 1);
   } else {
     fold(nl);
-    for (uint32_t start = nl >> 1; start >= MERKLE_TAIL; start >>= 1) { level(start); fold(start); }
-    tail(MERKLE_TAIL, 0);
+    for (uint32_t start = nl >> 1; start >= tail_w; start >>= 1) { level(start); fold(start); }
+    tail(tail_w, 0);
   }
   uint32_t* h = c.host_staging(8);
   c.d2h(h, t.nodes->p + 8, 8);

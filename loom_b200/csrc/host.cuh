@@ -187,6 +187,15 @@ struct Ctx {
   // Leaf hashing: 0 = choose by the amount of parallelism, 1 = one thread per
   // permutation, 6 = six lanes per permutation.
   int leaf_mapping = 0;
+  // Launch-shape choices (lg_ctx_set_tuning, set by the autotuner); proofs do
+  // not depend on them.  Defaults measured on B200.
+  struct Tuning {
+    uint32_t p2_leaf_min_per_sm = 128;  // one thread per leaf / injection chain from this many per SM
+    uint32_t p2_node_min_per_sm = 512;  // one thread per node of a Merkle level from this many per SM
+    uint32_t merkle_tail = 64;          // levels narrower than this run in one block
+    uint32_t inject_block = 32;         // threads per block, one-thread injection chains
+    uint32_t leaf_block = 128;          // threads per block, one-thread leaf hashing
+  } tune;
 };
 
 // ---------------------------------------------------------------- program

@@ -130,6 +130,40 @@ int lg_ctx_set_leaf_mapping(lg_ctx* ctx, int lanes_per_permutation) {
   });
 }
 
+int lg_ctx_set_tuning(lg_ctx* ctx, const char* name, int64_t value) {
+  return guarded(ctx, [&] {
+    if (!name) throw Error(LG_ERR_INVALID, "null tuning name");
+    std::string n = name;
+    auto in = [&](int64_t lo, int64_t hi) {
+      if (value < lo || value > hi) throw Error(LG_ERR_INVALID, "tuning " + n + " out of range");
+    };
+    auto pow2 = [&] {
+      if (value & (value - 1)) throw Error(LG_ERR_INVALID, "tuning " + n + " must be a power of two");
+    };
+    Ctx::Tuning& t = ctx->c.tune;
+    if (n == "p2_leaf_min_per_sm") { in(0, 1 << 20); t.p2_leaf_min_per_sm = (uint32_t)value; }
+    else if (n == "p2_node_min_per_sm") { in(0, 1 << 20); t.p2_node_min_per_sm = (uint32_t)value; }
+    else if (n == "merkle_tail") { in(2, 1024); pow2(); t.merkle_tail = (uint32_t)value; }
+    else if (n == "inject_block") { in(32, 1024); pow2(); t.inject_block = (uint32_t)value; }
+    else if (n == "leaf_block") { in(32, 1024); pow2(); t.leaf_block = (uint32_t)value; }
+    else throw Error(LG_ERR_INVALID, "unknown tuning " + n);
+  });
+}
+
+int lg_ctx_get_tuning(lg_ctx* ctx, const char* name, int64_t* value) {
+  return guarded(ctx, [&] {
+    if (!name || !value) throw Error(LG_ERR_INVALID, "null argument");
+    std::string n = name;
+    const Ctx::Tuning& t = ctx->c.tune;
+    if (n == "p2_leaf_min_per_sm") *value = t.p2_leaf_min_per_sm;
+    else if (n == "p2_node_min_per_sm") *value = t.p2_node_min_per_sm;
+    else if (n == "merkle_tail") *value = t.merkle_tail;
+    else if (n == "inject_block") *value = t.inject_block;
+    else if (n == "leaf_block") *value = t.leaf_block;
+    else throw Error(LG_ERR_INVALID, "unknown tuning " + n);
+  });
+}
+
 const char* lg_last_error(lg_ctx* ctx) { return ctx ? ctx->c.err.c_str() : "null context"; }
 
 int lg_prove(lg_ctx* ctx, const char* hash_backend, const uint32_t* program, size_t program_words,

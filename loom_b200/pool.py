@@ -18,8 +18,8 @@ from ._lib import Context
 
 
 class ProverPool:
-    def __init__(self, streams: int, device: int = 0):
-        self.contexts: List[Context] = [Context(device) for _ in range(streams)]
+    def __init__(self, streams: int, device: int = 0, tuning: Optional[dict] = None):
+        self.contexts: List[Context] = [Context(device, tuning) for _ in range(streams)]
         self._q: "queue.Queue[Optional[tuple]]" = queue.Queue()
         self._threads = [threading.Thread(target=self._worker, args=(c,), daemon=True) for c in self.contexts]
         for t in self._threads:

@@ -54,11 +54,14 @@ def make_request(rid: int, log_rows: int, instances: int, num_queries: int, seed
 
 class Server:
     def __init__(self, streams: int = 4, device: int = 0, hbm_budget: Optional[int] = None,
-                 batched: bool = True, context_factory: Optional[Callable[[int], object]] = None):
+                 batched: bool = True, context_factory: Optional[Callable[[int], object]] = None,
+                 tuning: Optional[dict] = None):
         make = context_factory or Context
         self.contexts = [make(device) for _ in range(streams)]
         for c in self.contexts:
             c.set_batched(batched)
+            if tuning:
+                c.apply_tuning(tuning)
         free, total = self.contexts[0].mem_info()
         self.budget = hbm_budget if hbm_budget is not None else int(0.8 * free)
         self.in_use = 0
@@ -133,11 +136,11 @@ def poisson_arrivals(n: int, rate_per_s: float, seed: int) -> np.ndarray:
 def serve(requests: Sequence[Request], arrivals: Sequence[float], streams: int = 4, device: int = 0,
           hbm_budget: Optional[int] = None, batched: bool = True,
           context_factory: Optional[Callable[[int], object]] = None,
-          warm: Sequence[Request] = ()) -> Dict:
+          warm: Sequence[Request] = (), tuning: Optional[dict] = None) -> Dict:
     """Replays `requests` at the given arrival offsets (seconds); returns
     latency percentiles, throughput and the finished requests.  `warm`
     requests run once per context before the clock starts."""
-    srv = Server(streams, device, hbm_budget, batched, context_factory)
+    srv = Server(streams, device, hbm_budget, batched, context_factory, tuning)
     try:
         srv.warm(warm)
         srv.t0 = time.perf_counter()

@@ -159,6 +159,30 @@ def test_prove_into_caller_buffer(ctx):
     assert ctx.prove(compiled.words, mont, 8) == ref
 
 
+def test_tuning_never_changes_proofs(ctx):
+    """Launch-shape values at the ends of their ranges give the same proof
+    bytes; invalid names and values are refused."""
+    compiled, wit = plonk.build(3, 1 << 10, seed=9)
+    mont = [F.to_mont(w) for w in wit]
+    defaults = ctx.tuning()
+    ref = ctx.prove(compiled.words, mont, 16)
+    try:
+        for params in ({"merkle_tail": 2, "p2_leaf_min_per_sm": 0, "p2_node_min_per_sm": 0, "inject_block": 1024,
+                        "leaf_block": 32},
+                       {"merkle_tail": 1024, "p2_leaf_min_per_sm": 1 << 20, "p2_node_min_per_sm": 1 << 20,
+                        "inject_block": 32, "leaf_block": 1024}):
+            ctx.apply_tuning(params)
+            assert ctx.tuning() == params
+            assert ctx.prove(compiled.words, mont, 16) == ref
+    finally:
+        ctx.apply_tuning(defaults)
+    for name, value in (("merkle_tail", 48), ("merkle_tail", 2048), ("leaf_block", 16), ("no_such", 1)):
+        with pytest.raises(LoomError) as e:
+            ctx.set_tuning(name, value)
+        assert e.value.code == 1
+    assert ctx.tuning() == defaults
+
+
 def test_unsupported_hash_backend(ctx):
     compiled, wit = plonk.build(1, 1 << 4, seed=1)
     mont = [F.to_mont(w) for w in wit]
