@@ -6,7 +6,8 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = [os.path.join(HERE, "csrc", "loom_gpu.cu"), os.path.join(HERE, "csrc", "gp_noalloc.cu")]
+SRC = [os.path.join(HERE, "csrc", "loom_gpu.cu"), os.path.join(HERE, "csrc", "gp_noalloc.cu"),
+       os.path.join(HERE, "csrc", "p2_host.cpp")]
 OUT = os.path.join(HERE, "libloom_gpu.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
@@ -15,7 +16,7 @@ FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std
 
 def sources():
     d = os.path.join(HERE, "csrc")
-    return [os.path.join(d, f) for f in sorted(os.listdir(d)) if f.endswith((".cu", ".cuh", ".h"))] + \
+    return [os.path.join(d, f) for f in sorted(os.listdir(d)) if f.endswith((".cu", ".cuh", ".h", ".cpp"))] + \
         [os.path.join(HERE, "..", "include", "loom_gpu.h")]
 
 

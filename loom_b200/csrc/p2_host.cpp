@@ -1,0 +1,123 @@
+// Host Poseidon2 (width 24) for the Fiat-Shamir transcript: the transcript is
+// a chain of sponge absorptions the host computes between device phases
+// (challenges, claimed-value binding, query positions), so its latency adds to
+// every proof.  With AVX2 (checked at run time) the 24-word state lives in
+// three 8-lane vectors: Montgomery products as even/odd 32x32->64 multiplies,
+// the M4 blocks of the external layer as in-lane shuffles, the partial rounds
+// in the carried-sum form of p2_partial_rounds (poseidon2.cuh) with one
+// horizontal sum per round.  Same permutation, same words as p2_permute.
+#include "poseidon2.cuh"
+
+#if defined(__x86_64__)
+#include <immintrin.h>
+#define LG_AVX2 __attribute__((target("avx2")))
+
+namespace lg {
+namespace {
+
+LG_AVX2 inline __m256i vp() { return _mm256_set1_epi32((int)P); }
+
+// a + b mod p for a, b in [0, p)
+LG_AVX2 inline __m256i vadd(__m256i a, __m256i b) {
+  const __m256i s = _mm256_add_epi32(a, b);
+  return _mm256_min_epu32(s, _mm256_sub_epi32(s, vp()));
+}
+// x in [0, 2p) -> [0, p)
+LG_AVX2 inline __m256i vred(__m256i x) { return _mm256_min_epu32(x, _mm256_sub_epi32(x, vp())); }
+
+// Montgomery product, b in [0, p), a in [0, 2^32): as mul() in field.cuh.
+LG_AVX2 inline __m256i vmul(__m256i a, __m256i b) {
+  const __m256i p = vp(), pinv = _mm256_set1_epi32((int)P_INV_NEG);
+  const __m256i te = _mm256_mul_epu32(a, b);
+  const __m256i to = _mm256_mul_epu32(_mm256_srli_epi64(a, 32), _mm256_srli_epi64(b, 32));
+  const __m256i me = _mm256_mul_epu32(te, pinv), mo = _mm256_mul_epu32(to, pinv);
+  const __m256i ue = _mm256_add_epi64(te, _mm256_mul_epu32(me, p));
+  const __m256i uo = _mm256_add_epi64(to, _mm256_mul_epu32(mo, p));
+  return vred(_mm256_blend_epi32(_mm256_srli_epi64(ue, 32), uo, 0xAA));
+}
+
+LG_AVX2 inline __m256i vcube(__m256i x) { return vmul(vmul(x, x), x); }
+
+// M4 on the two 4-word blocks of v: y_i = x_i + 2 x_{i+1} + (x_0 + x_1 + x_2 + x_3),
+// indices mod 4 -- the matrix of p2_m4's addition chain.
+LG_AVX2 inline __m256i vm4(__m256i v) {
+  const __m256i r = _mm256_shuffle_epi32(v, _MM_SHUFFLE(0, 3, 2, 1));
+  const __m256i e = vadd(v, vadd(r, r));
+  const __m256i s1 = vadd(v, _mm256_shuffle_epi32(v, _MM_SHUFFLE(2, 3, 0, 1)));
+  const __m256i t = vadd(s1, _mm256_shuffle_epi32(s1, _MM_SHUFFLE(1, 0, 3, 2)));
+  return vadd(e, t);
+}
+
+LG_AVX2 inline void vexternal(__m256i v[3]) {
+  for (int k = 0; k < 3; k++) v[k] = vm4(v[k]);
+  const __m256i s = vadd(vadd(v[0], v[1]), v[2]);  // column sums of blocks (0,2,4) | (1,3,5)
+  const __m256i tot = vadd(s, _mm256_permute2x128_si256(s, s, 0x01));
+  for (int k = 0; k < 3; k++) v[k] = vadd(v[k], tot);
+}
+
+// sum of the 8 lanes of x (each in [0, p))
+LG_AVX2 inline uint32_t vhsum(__m256i x) {
+  x = vadd(x, _mm256_permute2x128_si256(x, x, 0x01));
+  x = vadd(x, _mm256_shuffle_epi32(x, _MM_SHUFFLE(1, 0, 3, 2)));
+  x = vadd(x, _mm256_shuffle_epi32(x, _MM_SHUFFLE(2, 3, 0, 1)));
+  return (uint32_t)_mm256_cvtsi256_si32(x);
+}
+
+LG_AVX2 inline void vfull_round(__m256i v[3], const uint32_t* rk) {
+  for (int k = 0; k < 3; k++)
+    v[k] = vcube(vadd(v[k], _mm256_loadu_si256(reinterpret_cast<const __m256i*>(rk + 8 * k))));
+  vexternal(v);
+}
+
+constexpr uint32_t MONT_23 = 0x2dffffd2u;  // 23 * 2^32 mod p
+
+LG_AVX2 void p2_permute_avx2(uint32_t s[24]) {
+  __m256i v[3];
+  for (int k = 0; k < 3; k++) v[k] = _mm256_loadu_si256(reinterpret_cast<const __m256i*>(s + 8 * k));
+  __m256i dg[3];
+  for (int k = 0; k < 3; k++) dg[k] = _mm256_loadu_si256(reinterpret_cast<const __m256i*>(P2_DIAG_H + 8 * k));
+  const __m256i zero = _mm256_setzero_si256();
+  vexternal(v);
+  for (int r = 0; r < 3; r++) vfull_round(v, P2_FULL_RK_H[r]);
+  // partial rounds, carried R = s_1 + ... + s_23 (as p2_partial_rounds)
+  uint32_t R = vhsum(vadd(_mm256_blend_epi32(v[0], zero, 0x01), vadd(v[1], v[2])));
+  for (int r = 0; r < 21; r++) {
+    const uint32_t s0 = (uint32_t)_mm256_cvtsi256_si32(v[0]);
+    const uint32_t u = p2_cube(add(s0, P2_PARTIAL_RK_H[r]));
+    const __m256i p0 = vmul(v[0], dg[0]), p1 = vmul(v[1], dg[1]), p2 = vmul(v[2], dg[2]);
+    const uint32_t D = vhsum(vadd(_mm256_blend_epi32(p0, zero, 0x01), vadd(p1, p2)));
+    const uint32_t sum = add(u, R);
+    const __m256i sv = _mm256_set1_epi32((int)sum);
+    const uint32_t s0n = add(sum, mul(u, P2_DIAG_H[0]));
+    v[0] = _mm256_blend_epi32(_mm256_add_epi32(sv, p0), _mm256_set1_epi32((int)s0n), 0x01);
+    v[1] = _mm256_add_epi32(sv, p1);  // unreduced in [0, 2p) until the next product
+    v[2] = _mm256_add_epi32(sv, p2);
+    R = add(mul(sum, MONT_23), D);
+  }
+  for (int k = 0; k < 3; k++) v[k] = vred(v[k]);
+  for (int r = 3; r < 6; r++) vfull_round(v, P2_FULL_RK_H[r]);
+  for (int k = 0; k < 3; k++) _mm256_storeu_si256(reinterpret_cast<__m256i*>(s + 8 * k), v[k]);
+}
+
+bool cpu_has_avx2() {
+  __builtin_cpu_init();
+  return __builtin_cpu_supports("avx2");
+}
+
+}  // namespace
+
+void p2_permute_host(uint32_t s[24]) {
+  static const bool simd = cpu_has_avx2();
+  if (simd)
+    p2_permute_avx2(s);
+  else
+    p2_permute(s);
+}
+
+}  // namespace lg
+
+#else
+namespace lg {
+void p2_permute_host(uint32_t s[24]) { p2_permute(s); }
+}  // namespace lg
+#endif

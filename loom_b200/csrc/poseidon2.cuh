@@ -176,6 +176,10 @@ LG_HD void p2_compress(uint32_t tag_m, const uint32_t l[8], const uint32_t r[8],
   for (int i = 0; i < 8; i++) out[i] = s[i];
 }
 
+// The host's permutation for the transcript (p2_host.cpp): the same map as
+// p2_permute, vectorised when the CPU has AVX2.
+void p2_permute_host(uint32_t s[24]);
+
 // Host sponge: width 24, rate 16, overwrite mode, no padding
 // (internal/hash/poseidon2.go:165-255).
 struct HostSponge {
@@ -194,7 +198,7 @@ struct HostSponge {
     block[len++] = x_mont;
     if (len == 16) {
       for (int i = 0; i < 16; i++) state[i] = block[i];
-      p2_permute(state);
+      p2_permute_host(state);
       for (int i = 0; i < 16; i++) block[i] = 0;
       len = 0;
       wrote = true;
@@ -204,7 +208,7 @@ struct HostSponge {
     if (!wrote && len == 0) { for (int i = 0; i < 8; i++) out[i] = 0; return; }
     if (len > 0) {
       for (int i = 0; i < len; i++) state[i] = block[i];
-      p2_permute(state);
+      p2_permute_host(state);
       for (int i = 0; i < 16; i++) block[i] = 0;
       len = 0;
       wrote = true;
