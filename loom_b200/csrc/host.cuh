@@ -42,7 +42,51 @@ inline std::atomic<uint64_t> g_launches{0};
     ::lg::g_launches.fetch_add(1);  \
   } while (0)
 
-// Device buffer of u32 words, stream-ordered allocation.
+// Prove-scoped device memory: the small buffers of one prove (upload tables,
+// per-group scratch; about a thousand per prove) come from a bump arena of
+// retained chunks instead of one stream-ordered pool allocation and free
+// each.  The arena is rewound when the next call on the context starts, after
+// its stream is idle; chunks are used on that context's stream only.
+struct DevArena {
+  static constexpr size_t MAX_OBJ = (size_t)1 << 20, CHUNK = (size_t)32 << 20, ALIGN = 256;
+  std::vector<std::pair<uint8_t*, size_t>> chunks;
+  size_t cur = 0, off = 0;
+  void* take(size_t bytes, cudaStream_t s) {
+    bytes = (bytes + ALIGN - 1) & ~(ALIGN - 1);
+    while (cur < chunks.size() && off + bytes > chunks[cur].second) {
+      cur++;
+      off = 0;
+    }
+    if (cur == chunks.size()) {
+      uint8_t* p = nullptr;
+      size_t sz = std::max(CHUNK, bytes);
+      LG_CK(cudaMallocAsync((void**)&p, sz, s));
+      chunks.push_back({p, sz});
+      off = 0;
+    }
+    void* r = chunks[cur].first + off;
+    off += bytes;
+    return r;
+  }
+  void rewind() { cur = 0; off = 0; }
+  void release(cudaStream_t s) {
+    for (auto& c : chunks) cudaFreeAsync(c.first, s);
+    chunks.clear();
+    rewind();
+  }
+};
+// The arena that this thread's small DBufs come from (null: pool allocations).
+inline thread_local DevArena* g_dev_arena = nullptr;
+struct ArenaScope {
+  DevArena* prev;
+  explicit ArenaScope(DevArena* a) : prev(g_dev_arena) { g_dev_arena = a; }
+  ~ArenaScope() { g_dev_arena = prev; }
+  ArenaScope(const ArenaScope&) = delete;
+  ArenaScope& operator=(const ArenaScope&) = delete;
+};
+
+// Device buffer of u32 words, stream-ordered allocation (or a slice of the
+// current prove's arena).
 struct DBuf {
   uint32_t* p = nullptr;
   size_t words = 0;
@@ -50,7 +94,13 @@ struct DBuf {
   bool borrowed = false;  // caller-owned memory: never freed here
   DBuf() = default;
   DBuf(size_t w, cudaStream_t s) : words(w), st(s) {
-    if (w) LG_CK(cudaMallocAsync((void**)&p, w * 4, s));
+    if (!w) return;
+    if (g_dev_arena && w * 4 <= DevArena::MAX_OBJ) {
+      p = (uint32_t*)g_dev_arena->take(w * 4, s);
+      borrowed = true;  // the arena owns it
+    } else {
+      LG_CK(cudaMallocAsync((void**)&p, w * 4, s));
+    }
   }
   DBuf(const DBuf&) = delete;
   DBuf& operator=(const DBuf&) = delete;
@@ -75,6 +125,7 @@ using DBufP = std::shared_ptr<DBuf>;
 struct Ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  DevArena dev_arena;            // prove-scoped small device buffers
   std::map<int, DBufP> tw;       // log n -> w_n^j, j < n
   std::map<int, DBufP> gpow;     // log n -> g^k, k < n
   std::map<int, DBufP> ginvpow;  // log n -> g^-k, k < n
@@ -124,6 +175,7 @@ struct Ctx {
     auto it = tw.find(logn);
     if (it != tw.end()) return it->second->p;
     size_t n = (size_t)1 << logn;
+    ArenaScope cached(nullptr);  // kept across proves: never from the arena
     auto b = std::make_shared<DBuf>(n, stream);
     k_fill_powers<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(b->p, n, root_of_unity_mont(logn), MONT_ONE);
     LG_LAUNCH();
@@ -135,6 +187,7 @@ struct Ctx {
     auto it = m.find(logn);
     if (it != m.end()) return it->second->p;
     size_t n = (size_t)1 << logn;
+    ArenaScope cached(nullptr);  // kept across proves: never from the arena
     auto b = std::make_shared<DBuf>(n, stream);
     uint32_t g = to_mont(3);
     if (inverse) g = inv(g);

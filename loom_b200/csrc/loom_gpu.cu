@@ -39,6 +39,7 @@ template <class F> int guarded(lg_ctx* ctx, F f) {
     if (ctx->c.stream) {
       LG_CK(cudaStreamSynchronize(ctx->c.stream));
       ctx->c.arena_reset();
+      ctx->c.dev_arena.rewind();
     }
     f();
     return LG_OK;
@@ -102,6 +103,8 @@ void lg_ctx_destroy(lg_ctx* ctx) {
   ctx->c.gpow.clear();
   ctx->c.ginvpow.clear();
   if (ctx->c.stream) {
+    cudaStreamSynchronize(ctx->c.stream);
+    ctx->c.dev_arena.release(ctx->c.stream);
     cudaStreamSynchronize(ctx->c.stream);
     cudaStreamDestroy(ctx->c.stream);
   }

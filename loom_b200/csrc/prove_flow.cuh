@@ -8,6 +8,7 @@ namespace lg {
 
 inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint8_t* out, size_t out_cap,
                             bool* in_out) {
+  ArenaScope arena(&c.dev_arena);  // rewound by the next call on the context
   c.phase_start();
   setup(witness, on_device);
   c.phase("setup+upload");
