@@ -513,6 +513,8 @@ def main():
             "kernel_shares": shares,
             "kernel_ms_profiled_step": round(total_k, 3),
             "host_phases_ms": {k: round(v, 3) for k, v in phases.items()},
+            "step_ms": {"prove": [round(x, 3) for x in times], "e2e": [round(x, 3) for x in e2e_times],
+                        "plain": [round(x, 3) for x in plain_times]},
             "tuning": tune,
             "kernel_ms_by_phase": {ph: {k: round(v["ms"], 3) for k, v in ks.items()} for ph, ks in by_phase.items()},
             "dominant_kernel": dom,

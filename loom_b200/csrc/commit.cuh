@@ -319,16 +319,28 @@ inline Committed commit(Ctx& c, const std::vector<GroupSpec>& gs, bool keep_coef
     cm.order.push_back((int)i);
   }
   std::stable_sort(cm.order.begin(), cm.order.end(), [&](int a, int b) { return gs[a].log_n > gs[b].log_n; });
-  // LDE buffers, one per group
+  // LDE buffers, one per group, slices of one allocation
   std::map<uint32_t, std::vector<LdeLane>> by_size;
   std::vector<std::vector<LdeLane>> per_group(gs.size());
+  size_t lde_words = 0, coef_words = 0;
+  for (auto& g : gs) {
+    lde_words += g.lanes.size() * ((size_t)1 << (g.log_n + RATE_LOG));
+    coef_words += g.lanes.size() * ((size_t)1 << g.log_n);
+  }
+  auto lde_all = std::make_shared<DBuf>(lde_words, c.stream);
+  auto coef_all = keep_coef ? std::make_shared<DBuf>(coef_words, c.stream) : DBufP();
+  size_t lde_off = 0, coef_off = 0;
   for (size_t i = 0; i < gs.size(); i++) {
     LdeOut o;
     o.lanes = (uint32_t)gs[i].lanes.size();
     o.log_n = gs[i].log_n;
     size_t n = (size_t)1 << o.log_n;
-    o.lde = std::make_shared<DBuf>(o.lanes * (n << RATE_LOG), c.stream);
-    if (keep_coef) o.coef = std::make_shared<DBuf>(o.lanes * n, c.stream);
+    o.lde = dbuf_slice(lde_all, lde_off, o.lanes * (n << RATE_LOG));
+    lde_off += o.lanes * (n << RATE_LOG);
+    if (keep_coef) {
+      o.coef = dbuf_slice(coef_all, coef_off, o.lanes * n);
+      coef_off += o.lanes * n;
+    }
     for (uint32_t l = 0; l < o.lanes; l++) {
       LdeLane L{gs[i].lanes[l], o.lde->p + l * (n << RATE_LOG), keep_coef ? o.coef->p + l * n : nullptr};
       (c.batched ? by_size[o.log_n] : per_group[i]).push_back(L);

@@ -122,6 +122,22 @@ struct DBuf {
 };
 using DBufP = std::shared_ptr<DBuf>;
 
+// words [off, off + words) of `backing` as a buffer of its own; it keeps the
+// backing alive.  Lets one allocation serve many groups or modules.
+inline DBufP dbuf_slice(const DBufP& backing, size_t off, size_t words) {
+  struct View {
+    DBufP backing;
+    DBuf v;
+  };
+  auto h = std::make_shared<View>();
+  h->backing = backing;
+  h->v.p = backing->p + off;
+  h->v.words = words;
+  h->v.st = backing->st;
+  h->v.borrowed = true;
+  return DBufP(h, &h->v);
+}
+
 struct Ctx {
   int device = 0;
   cudaStream_t stream = nullptr;

@@ -79,12 +79,6 @@ int lg_ctx_create(int device, lg_ctx** out) {
     LG_CK(cudaDeviceGetDefaultMemPool(&pool, device));
     uint64_t keep = UINT64_MAX;  // keep freed blocks for the next prove
     LG_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
-    // Concurrent contexts (one stream each) must not hand each other blocks
-    // whose frees are still queued on the other stream: the pool would make
-    // the allocating stream wait for the freeing one and serialise proofs.
-    int no = 0;
-    LG_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no));
-    LG_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowOpportunistic, &no));
     LG_CK(cudaDeviceGetAttribute(&ctx->c.sm_count, cudaDevAttrMultiProcessorCount, device));
   });
   if (rc != LG_OK) {

@@ -151,6 +151,13 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
 
   // ---- DEEP codewords on the LDE rows (internal/fri/deep.go:71-266)
   std::vector<DBufP> deep(classes.size());
+  DBufP deep_all;  // one allocation for every class's codeword
+  {
+    size_t words = 0;
+    for (uint32_t m : classes) words += 6 * (mod_n(m) << RATE_LOG);
+    deep_all = std::make_shared<DBuf>(words, c.stream);
+  }
+  size_t deep_off = 0;
   std::vector<DeepJob> djobs;
   std::vector<DBufP> dkeep;
   std::vector<double> dbytes;
@@ -200,7 +207,8 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
     jb.n_bundles = (uint32_t)bundles.size();
     jb.logn4 = (int)logn + RATE_LOG;
     jb.tw = c.twiddles(jb.logn4);
-    deep[ci] = std::make_shared<DBuf>(6 * big, c.stream);
+    deep[ci] = dbuf_slice(deep_all, deep_off, 6 * big);
+    deep_off += 6 * big;
     jb.out = deep[ci]->p;
     djobs.push_back(jb);
     double row_bytes = 24.0;

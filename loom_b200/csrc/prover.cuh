@@ -405,6 +405,7 @@ struct Prover {
   void quotient_all() {
     struct ModQ {
       uint32_t m, logn;
+      std::vector<const uint32_t*> coef_lanes;
       std::vector<CosetLane> lanes;
       DBufP cv, qv, code, chunks;
       XCode xc;
@@ -419,7 +420,7 @@ struct Prover {
       if (chunk_count(m) != 4) throw Error(LG_ERR_UNSUPPORTED, "quotient domains other than 4N are not supported by this build");
       uint32_t logn = pg.modules[m].log_n;
       check_ntt_size((int)logn);
-      size_t n = (size_t)1 << logn, big = n << RATE_LOG;
+      size_t n = (size_t)1 << logn;
       ModQ q;
       q.m = m;
       q.logn = logn;
@@ -448,15 +449,35 @@ struct Prover {
         return f;
       };
       q.xc = compile_expr((uint32_t)fold_root[m], lane_of);
-      q.cv = std::make_shared<DBuf>(coef_lanes.size() * big, c.stream);
-      for (size_t l = 0; l < coef_lanes.size(); l++) q.lanes.push_back(CosetLane{coef_lanes[l], q.cv->p + l * big});
+      q.coef_lanes = coef_lanes;
       uint32_t g = to_mont(3), w4n = root_of_unity_mont((int)logn + RATE_LOG);
       for (int cc = 0; cc < 4; cc++) q.zinv[cc] = inv(sub(mont_pow(mul(g, mont_pow(w4n, cc)), n), MONT_ONE));
       q.code = upload_vec(c, q.xc.code);
-      q.qv = std::make_shared<DBuf>((root_ext[m] ? 6 : 1) * big, c.stream);
-      q.chunks = std::make_shared<DBuf>(4 * (root_ext[m] ? 6 : 1) * n, c.stream);
-      chunk_coef[m] = q.chunks;
       mods.push_back(std::move(q));
+    }
+    {  // coset values, quotient values and chunks of all modules: one allocation each
+      size_t cv_words = 0, qv_words = 0, ch_words = 0;
+      for (auto& q : mods) {
+        const size_t n = (size_t)1 << q.logn, big = n << RATE_LOG, w = root_ext[q.m] ? 6 : 1;
+        cv_words += q.coef_lanes.size() * big;
+        qv_words += w * big;
+        ch_words += 4 * w * n;
+      }
+      auto cv_all = std::make_shared<DBuf>(cv_words, c.stream);
+      auto qv_all = std::make_shared<DBuf>(qv_words, c.stream);
+      auto ch_all = std::make_shared<DBuf>(ch_words, c.stream);
+      size_t cv_off = 0, qv_off = 0, ch_off = 0;
+      for (auto& q : mods) {
+        const size_t n = (size_t)1 << q.logn, big = n << RATE_LOG, w = root_ext[q.m] ? 6 : 1;
+        q.cv = dbuf_slice(cv_all, cv_off, q.coef_lanes.size() * big);
+        cv_off += q.coef_lanes.size() * big;
+        for (size_t l = 0; l < q.coef_lanes.size(); l++) q.lanes.push_back(CosetLane{q.coef_lanes[l], q.cv->p + l * big});
+        q.qv = dbuf_slice(qv_all, qv_off, w * big);
+        qv_off += w * big;
+        q.chunks = dbuf_slice(ch_all, ch_off, 4 * w * n);
+        ch_off += 4 * w * n;
+        chunk_coef[q.m] = q.chunks;
+      }
     }
     auto intt_lanes = [&](uint32_t logn, const std::vector<uint32_t*>& lanes) {
       const size_t n = (size_t)1 << logn;
