@@ -218,8 +218,8 @@ inline unsigned tail_threads(uint32_t top, int fold_first) {
 }
 
 // nodes must already hold the leaves at [n_leaves, 2 n_leaves).  Reads the
-// root back (the transcript needs it).
-inline void build_tree(Ctx& c, TreeDev& t) {
+// root back (the transcript needs it) unless read_root is false.
+inline void build_tree(Ctx& c, TreeDev& t, bool read_root = true) {
   const uint32_t nl = 1u << t.log_leaves;
   for (size_t k = 0; k < t.inj.size(); k++)
     if (t.inj_log_w[k] > t.log_leaves || (k && t.inj_log_w[k] > t.inj_log_w[k - 1]))
@@ -290,6 +290,7 @@ inline void build_tree(Ctx& c, TreeDev& t) {
     for (uint32_t start = nl >> 1; start >= tail_w; start >>= 1) { level(start); fold(start); }
     tail(tail_w, 0);
   }
+  if (!read_root) return;  // the root stays on the device (nodes[1])
   uint32_t* h = c.host_staging(8);
   c.d2h(h, t.nodes->p + 8, 8);
   memcpy(t.root.v, h, 32);

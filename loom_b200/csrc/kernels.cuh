@@ -772,10 +772,15 @@ __global__ void k_axpy_e6(uint32_t* run, uint64_t n, const AxpyTerm* terms, uint
 
 // next[i] = (p+q)/2 + alpha (p-q)/(2 x_i), x_i^-1 = w_n^-bitrev(i, n/2)
 // (internal/fri/fri.go:1113-1118,1177-1198).  tw: w_n^j table.
-__global__ void k_fold(const uint32_t* layer, uint64_t n, E6 alpha, const uint32_t* tw, uint32_t inv2, uint32_t* next) {
+// alpha: device words (the first six words of a challenge digest).
+__global__ void k_fold(const uint32_t* layer, uint64_t n, const uint32_t* alpha_w, const uint32_t* tw, uint32_t inv2,
+                       uint32_t* next) {
   const uint64_t half = n / 2;
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= half) return;
+  E6 alpha;
+#pragma unroll
+  for (int w = 0; w < 6; w++) alpha.c[w] = __ldg(alpha_w + w);
   int lg = 0;
   while ((1ull << lg) < half) lg++;
   uint32_t e = bitrev32((uint32_t)i, lg);
@@ -786,8 +791,37 @@ __global__ void k_fold(const uint32_t* layer, uint64_t n, E6 alpha, const uint32
   st6(next, half, i, e6_add(s, d));
 }
 
+// One Fiat-Shamir challenge on the device, for challenges whose bindings are
+// already in device memory (the FRI layer roots): digest = state[0..8) of
+// the width-24 sponge (rate 16, overwrite, no padding) over
+// pre[0..n_pre) || prev[0..8) || bind[0..8), as Transcript::compute on the
+// host (internal/fiat-shamir/transcript.go:221-315).  One warp, six lanes
+// per permutation; `out` gets 8 words.
+__global__ void k_fs_challenge(const uint32_t* pre, uint32_t n_pre, const uint32_t* prev, const uint32_t* bind,
+                               uint32_t* out) {
+  __shared__ uint32_t keys[144];
+  __shared__ uint32_t msg[64];
+  const uint32_t total = n_pre + 16;  // n_pre <= 48, checked by the host
+  for (uint32_t i = threadIdx.x; i < total; i += blockDim.x)
+    msg[i] = i < n_pre ? pre[i] : (i < n_pre + 8 ? prev[i - n_pre] : bind[i - n_pre - 8]);
+  p2_load_full_keys(keys);  // ends with a barrier
+  P2Lane L;
+  L.init();
+  uint32_t x[4] = {0, 0, 0, 0};
+  for (uint32_t b = 0; b < total; b += 16) {
+    const uint32_t len = min(16u, total - b);  // words 0..len of the state are overwritten
+    if (L.idx < 4)
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+        if (4 * (uint32_t)L.idx + k < len) x[k] = msg[b + 4 * L.idx + k];
+    p2c_permute(x, L, keys);
+  }
+  if (L.lane < 2)
+#pragma unroll
+    for (int k = 0; k < 4; k++) out[4 * L.lane + k] = x[k];
+}
+
 // ---------------------------------------------------------------- openings
-// Montgomery -> canonical, in place (proof encoding of gathered openings).
 // Montgomery words -> canonical values as big-endian bytes (the proof
 // encoding), in place.
 __global__ void k_proof_words(uint32_t* x, uint64_t n) {

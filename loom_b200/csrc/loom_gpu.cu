@@ -292,11 +292,10 @@ int lg_fri_fold(lg_ctx* ctx, const uint32_t* layer, uint64_t n, const uint32_t a
     k_aos_to_soa<<<(unsigned)((6 * n + 255) / 256), 256, 0, c.stream>>>(a->p, n, 6, soa->p);
     LG_LAUNCH();
     auto nx = std::make_shared<DBuf>(3 * n, c.stream);
-    E6 al;
-    for (int w = 0; w < 6; w++) al.c[w] = alpha[w];
+    auto al = upload_vec(c, std::vector<uint32_t>(alpha, alpha + 6));
     const uint32_t* tw = c.twiddles(logn);
     c.timed("fri_fold", 36.0 * n, 0, [&] {
-      k_fold<<<(unsigned)((n / 2 + 255) / 256), 256, 0, c.stream>>>(soa->p, n, al, tw, inv(to_mont(2)), nx->p);
+      k_fold<<<(unsigned)((n / 2 + 255) / 256), 256, 0, c.stream>>>(soa->p, n, al->p, tw, inv(to_mont(2)), nx->p);
       LG_LAUNCH();
     });
     auto aos = std::make_shared<DBuf>(3 * n, c.stream);

@@ -277,6 +277,20 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
   std::vector<DBufP> layers(NR + 1);
   std::vector<TreeDev> ftrees(NR);
   std::vector<Digest> fri_roots;
+  // Fold challenges after the first are computed on the device from the
+  // layer roots (k_fs_challenge), so the rounds run without a host round
+  // trip; the host replays them after the loop and checks every digest.
+  auto chal = std::make_shared<DBuf>((size_t)8 * NR, c.stream);
+  std::vector<uint32_t> pre_all;
+  std::vector<uint32_t> pre_off(NR), pre_len(NR);
+  for (int j = r0 + 1; j < NR; j++) {
+    auto pe = string_to_elements(0x46534944u, "fri_fold_" + std::to_string(j));
+    if (pe.size() > 48) throw Error(LG_ERR_UNSUPPORTED, "challenge name too long");
+    pre_off[j] = (uint32_t)pre_all.size();
+    pre_len[j] = (uint32_t)pe.size();
+    pre_all.insert(pre_all.end(), pe.begin(), pe.end());
+  }
+  auto pre_d = upload_vec(c, pre_all.empty() ? std::vector<uint32_t>{0} : pre_all);
   size_t nj = (size_t)1 << (LOG_N_FRI - r0);
   auto running = std::make_shared<DBuf>(6 * nj, c.stream);
   LG_CK(cudaMemcpyAsync(running->p, lvl[0]->p, 6 * nj * 4, cudaMemcpyDeviceToDevice, c.stream));
@@ -301,23 +315,29 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
       }
     }
     if (j > r0) layers[j] = running;
-    if (j == r0) ftrees[j] = levels_tree;
-    else {
+    if (j == r0) {
+      ftrees[j] = levels_tree;
+      const std::string nm = "fri_fold_" + std::to_string(j);
+      fs.bind(nm, levels_tree.root.v, 8);
+      Digest d = fs.compute(nm);
+      c.h2d(chal->p + 8 * (size_t)j, d.v, 32);
+    } else {
       TreeDev& t = ftrees[j];
       t.log_leaves = (uint32_t)(LOG_N_FRI - j - 1);
       t.nodes = std::make_shared<DBuf>((size_t)16 << t.log_leaves, c.stream);
       launch_leaves(c, {leaf_group(running->p, 0, 1, (uint32_t)(LOG_N_FRI - j), t.nodes->p + ((size_t)8 << t.log_leaves))});
-      build_tree(c, t);
+      build_tree(c, t, false);
+      c.timed("fri_challenge", 0, 0, [&] {
+        k_fs_challenge<<<1, 32, 0, c.stream>>>(pre_d->p + pre_off[j], pre_len[j], chal->p + 8 * (size_t)(j - 1),
+                                               t.nodes->p + 8, chal->p + 8 * (size_t)j);
+        LG_LAUNCH();
+      });
     }
-    Digest root = ftrees[j].root;
-    std::string nm = "fri_fold_" + std::to_string(j);
-    fs.bind(nm, root.v, 8);
-    E6 a = digest_e6(fs.compute(nm));
-    if (j > r0) fri_roots.push_back(root);
     auto next = std::make_shared<DBuf>(3 * nj, c.stream);
     const uint32_t* twj = c.twiddles(LOG_N_FRI - j);
     c.timed("fri_fold", 36.0 * nj, 0, [&] {
-      k_fold<<<(unsigned)((nj / 2 + 255) / 256), 256, 0, c.stream>>>(running->p, nj, a, twj, inv2, next->p);
+      k_fold<<<(unsigned)((nj / 2 + 255) / 256), 256, 0, c.stream>>>(running->p, nj, chal->p + 8 * (size_t)j, twj, inv2,
+                                                                     next->p);
       LG_LAUNCH();
     });
     running = next;
@@ -325,9 +345,27 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
   }
   std::vector<uint32_t> final_poly(6 * nj);
   {
-    uint32_t* h = c.host_staging(6 * nj);
-    c.d2h(h, running->p, 6 * nj);
+    // one read-back: final polynomial, device challenges, layer roots
+    const size_t nroot = (size_t)(NR > r0 + 1 ? NR - r0 - 1 : 0);
+    uint32_t* h = c.host_staging(6 * nj + 8 * (size_t)NR + 8 * nroot);
+    LG_CK(cudaMemcpyAsync(h, running->p, 6 * nj * 4, cudaMemcpyDeviceToHost, c.stream));
+    LG_CK(cudaMemcpyAsync(h + 6 * nj, chal->p, 8 * (size_t)NR * 4, cudaMemcpyDeviceToHost, c.stream));
+    for (int j = r0 + 1; j < NR; j++)
+      LG_CK(cudaMemcpyAsync(h + 6 * nj + 8 * (size_t)NR + 8 * (size_t)(j - r0 - 1), ftrees[j].nodes->p + 8, 32,
+                            cudaMemcpyDeviceToHost, c.stream));
+    LG_CK(cudaStreamSynchronize(c.stream));
     memcpy(final_poly.data(), h, 6 * nj * 4);
+    for (int j = r0 + 1; j < NR; j++) {
+      Digest root;
+      memcpy(root.v, h + 6 * nj + 8 * (size_t)NR + 8 * (size_t)(j - r0 - 1), 32);
+      ftrees[j].root = root;
+      fri_roots.push_back(root);
+      const std::string nm = "fri_fold_" + std::to_string(j);
+      fs.bind(nm, root.v, 8);
+      Digest d = fs.compute(nm);
+      if (memcmp(d.v, h + 6 * nj + 8 * (size_t)j, 32) != 0)
+        throw Error(LG_ERR_CUDA, "device and host transcripts disagree at " + nm);
+    }
     std::vector<uint32_t> fin = {to_mont(0x45585450u), to_mont((uint32_t)nj)};
     for (size_t i = 0; i < nj; i++) for (int w = 0; w < 6; w++) fin.push_back(final_poly[w * nj + i]);
     fs.bind("fri_query_0", fin.data(), fin.size());
