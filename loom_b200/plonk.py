@@ -20,7 +20,7 @@ from typing import Dict, List, Tuple
 import numpy as np
 
 from . import field as F
-from .program import Builder, Compiled, Module, col, copy_constraint
+from .program import Builder, Compiled, Module, col, copy_constraint, range_check
 
 
 def _ith(s: str, i: int) -> str:
@@ -79,6 +79,38 @@ def build(n_instances: int, n: int, seed: int = 0x10AD) -> Tuple[Compiled, List[
     compiled = b.compile()
     witness = [np.ascontiguousarray(trace[name], dtype=np.uint32) for (name, fld, rows) in compiled.witness_columns]
     return compiled, witness
+
+
+def build_mixed(log_sizes: List[int], seed: int = 0x10AD, range_bound: int = 256) -> Tuple[Compiled, List[np.ndarray]]:
+    """Modules of uneven sizes 2^log_sizes[i], each a plonk-like module as in
+    build() plus a column RC_i of values in [0, range_bound) range-checked by a
+    logup lookup into the shared range table (arguments.Range): the batched
+    form of the prove benchmark (gates, a permutation argument and a lookup)."""
+    b = Builder()
+    trace: Dict[str, np.ndarray] = {}
+    for i, lg in enumerate(log_sizes):
+        n = 1 << lg
+        m = Module(_ith("plonk", i), n)
+        L, R, O = col(_ith("L", i)), col(_ith("R", i)), col(_ith("O", i))
+        QL, QR, QM, QO, QK = (col(_ith(s, i)) for s in ("QL", "QR", "QM", "QO", "QK"))
+        m.assert_zero(QL * L + QR * R + QM * L * R + QO * O + QK)
+        b.add_module(m)
+        w, S = instance_witness(n, seed, i)
+        trace.update(w)
+        copy_constraint(b, m.name, [L, R, O], S, _ith("plonk.S", i))
+        rng = np.random.Generator(np.random.PCG64([seed, i, 0x5243]))
+        trace[_ith("RC", i)] = rng.integers(0, range_bound, n, dtype=np.uint32)
+        range_check(b, col(_ith("RC", i)), m.name, range_bound)
+    trace.update(b.generated)
+    compiled = b.compile()
+    witness = [np.ascontiguousarray(trace[name], dtype=np.uint32) for (name, fld, rows) in compiled.witness_columns]
+    return compiled, witness
+
+
+def mixed_sizes(n_modules: int, lo: int, hi: int, seed: int) -> List[int]:
+    """log2 module sizes drawn uniformly from [lo, hi] (seeded)."""
+    rng = np.random.Generator(np.random.PCG64([seed, 0x5A5E]))
+    return [int(x) for x in rng.integers(lo, hi + 1, n_modules)]
 
 
 def check_gates(witness_by_name: Dict[str, np.ndarray], i: int) -> bool:

@@ -12,6 +12,10 @@ the program the Go prover would build:
     board/rounds.go:108-135, board/board.go:66-69,251-267.
   * ``copy_constraint`` — arguments/permutation.go:37-127 (ID support and
     permutation columns generated as in board/module.go:229-293).
+  * ``range_check`` / ``lookup`` — arguments/lookup.go:31-230: the range module
+    and its column (board/module.go:56-71), lookup multiplicities
+    (board/board.go:235-249) and cyclic logup columns with their exposed
+    totals (board/logup.go:70-149).
   * ``Builder.compile`` — board/program.go:45-89 and the last-round sweep of
     board/rounds.go:219-292.
 """
@@ -27,8 +31,11 @@ from . import field as F
 ROUND_FOLD, ROUND_LOG_DERIVATIVE, ROUND_RUNNING_SUMS = 0, 1, 2
 BASE, EXT = 0, 1
 KIND_WITNESS, KIND_STEP, KIND_LAGRANGE = 0, 1, 2
-OP_COL, OP_COIN, OP_CONST, OP_ADD, OP_SUB, OP_MUL = range(6)
+OP_COL, OP_COIN, OP_CONST, OP_ADD, OP_SUB, OP_MUL, OP_EXPAVG = range(7)
+STEP_GP, STEP_MULT, STEP_LOGUP = 0, 1, 2
 MAGIC = 0x3150474C
+RANGE_MODULE, LOGUP = "range", "logup"  # internal/constants/const.go:34,41
+MAX_LOGUP_DEGREE, MAX_LOGUP_BATCH = 5, 4  # board/logup.go:37, arguments/lookup.go:156
 
 
 class Expr:
@@ -59,7 +66,20 @@ class Expr:
             return ("k", self.a)
         if self.op == OP_CONST:
             return ("v", self.a)
+        if self.op == OP_EXPAVG:
+            return ("x", self.a)
         return (self.op, self.a.key(), self.b.key())
+
+    def degree(self) -> int:
+        """expr Degree: columns (committed or verifier, exposed averages
+        included) count 1, coins and constants 0."""
+        if self.op in (OP_COL, OP_EXPAVG):
+            return 1
+        if self.op in (OP_COIN, OP_CONST):
+            return 0
+        if self.op == OP_MUL:
+            return self.a.degree() + self.b.degree()
+        return max(self.a.degree(), self.b.degree())
 
 
 def _lift(o):
@@ -77,6 +97,12 @@ def coin(r: int) -> Expr:
 
 def const(v: int) -> Expr:
     return Expr(OP_CONST, int(v) % F.P)
+
+
+def exposed_average(total: str) -> Expr:
+    """The constant extension column T/N of an exposed total T, N the size of
+    the module using it (expr/ast.go:223-227)."""
+    return Expr(OP_EXPAVG, total)
 
 
 def fold(v: Expr, cs: Sequence[Expr]) -> Expr:
@@ -130,6 +156,25 @@ class GrandProductStep:
 
 
 @dataclass
+class MultiplicityStep:
+    """board/board.go:235-249: one multiplicity column per target table."""
+    round: int
+    sources: List[Expr]
+    targets: List[Expr]
+    outs: List[str]
+
+
+@dataclass
+class LogupStep:
+    """board/logup.go:80-127: a cyclic logup column and its exposed total."""
+    round: int
+    module: str
+    terms: List[Tuple[Expr, Expr]]  # (E, M): fraction M / E
+    out: str
+    total: str
+
+
+@dataclass
 class Compiled:
     words: np.ndarray              # descriptor, uint32
     witness_columns: List[Tuple[str, int, int]]  # (name, field, rows), in descriptor order
@@ -170,6 +215,39 @@ class Builder:
     def _is_verifier(self, name: str) -> bool:
         return any(name in m.lagrange for m in self.modules.values())
 
+    def add_lookup_multiplicity_step(self, r: int, S: Sequence[Expr], T: Sequence[Expr], output: str) -> List[str]:
+        """Width-1 tables (board/board.go:235-249); outs "<output>_<i>"."""
+        self._grow(r)
+        outs = [f"{output}_{i}" for i in range(len(T))]
+        self.rounds[r]["steps"].append(MultiplicityStep(r, list(S), list(T), outs))
+        return outs
+
+    def add_cyclic_logup_step(self, r: int, module: str, terms: Sequence[Tuple[Expr, Expr]], output: str) -> str:
+        """board/logup.go:80-127: L - L_{-1} + T/N = sum_j M_j / E_j on every
+        row (row 0 reads L_{N-1}); returns the exposed total's name."""
+        if not terms:
+            raise ValueError(f"logup {output}: no terms")
+        if logup_constraint_degree(terms) > MAX_LOGUP_DEGREE:
+            raise ValueError(f"logup {output}: constraint degree above {MAX_LOGUP_DEGREE}")
+        total = output + "_total"
+        self._grow(r)
+        self.rounds[r]["steps"].append(LogupStep(r, module, list(terms), output, total))
+
+        def prod_e(skip: int) -> Optional[Expr]:
+            res = None
+            for i, (e, _) in enumerate(terms):
+                if i != skip:
+                    res = e if res is None else res * e
+            return res
+
+        increment = col(output) - col(output, -1) + exposed_average(total)
+        relation = increment * prod_e(-1)
+        for j, (_, m) in enumerate(terms):
+            num = m * prod_e(j) if len(terms) > 1 else m
+            relation = relation - num
+        self.modules[module].assert_zero(relation)
+        return total
+
     def add_grand_product_step(self, r: int, module: str, num: Expr, den: Expr, out: str):
         self._grow(r)
         self.rounds[r]["steps"].append(GrandProductStep(r, module, num, den, out))
@@ -190,7 +268,13 @@ class Builder:
                 for lf in rel.leaves():
                     if lf.op == OP_COL and lf.a not in verifier:
                         owner[lf.a] = mname
-        step_out = {s.out: s for rd in self.rounds for s in rd["steps"]}
+        step_out = {}
+        for rd in self.rounds:
+            for s_ in rd["steps"]:
+                for o in (s_.outs if isinstance(s_, MultiplicityStep) else [s_.out]):
+                    step_out[o] = s_
+        exposed = [s_.total for rd in self.rounds for s_ in rd["steps"] if isinstance(s_, LogupStep)]
+        exposed_idx = {nm: i for i, nm in enumerate(exposed)}
         staged: List[List[str]] = []
         seen = {}
         for r, rd in enumerate(self.rounds):
@@ -213,15 +297,22 @@ class Builder:
         def field_of(e: Expr, fields) -> int:
             if e.op == OP_COL:
                 return fields.get(e.a, BASE)
-            if e.op == OP_COIN:
+            if e.op in (OP_COIN, OP_EXPAVG):
                 return EXT
             if e.op == OP_CONST:
                 return BASE
             return max(field_of(e.a, fields), field_of(e.b, fields))
 
         fields: Dict[str, int] = {}
-        for s in step_out.values():
-            fields[s.out] = max(field_of(s.num, fields), field_of(s.den, fields))
+        for rd in self.rounds:
+            for s_ in rd["steps"]:
+                if isinstance(s_, GrandProductStep):
+                    fields[s_.out] = max(field_of(s_.num, fields), field_of(s_.den, fields))
+                elif isinstance(s_, LogupStep):
+                    fields[s_.out] = EXT
+                else:
+                    for o in s_.outs:
+                        fields[o] = BASE
         columns: List[Tuple[str, int, int, int, int]] = []  # name, module idx, field, kind, param
         mod_names = list(self.modules)
         mod_idx = {n: i for i, n in enumerate(mod_names)}
@@ -251,6 +342,10 @@ class Builder:
                 t = (OP_COIN, e.a, 0)
             elif e.op == OP_CONST:
                 t = (OP_CONST, e.a, 0)
+            elif e.op == OP_EXPAVG:
+                if e.a not in exposed_idx:
+                    raise ValueError(f"exposed value {e.a} is not produced by any step")
+                t = (OP_EXPAVG, exposed_idx[e.a], 0)
             else:
                 a, b = emit(e.a), emit(e.b)
                 t = (e.op, a, b)
@@ -261,8 +356,18 @@ class Builder:
         mod_rels = [[emit(r) for r in self.modules[n].relations] for n in mod_names]
         steps = []
         for rd in self.rounds:
-            for s in rd["steps"]:
-                steps.append((0, s.round, mod_idx[s.module], emit(s.num), emit(s.den), col_idx[s.out]))
+            for s_ in rd["steps"]:
+                if isinstance(s_, GrandProductStep):
+                    steps.append((STEP_GP, s_.round, mod_idx[s_.module], emit(s_.num), emit(s_.den), col_idx[s_.out]))
+                elif isinstance(s_, MultiplicityStep):
+                    steps.append((STEP_MULT, s_.round, len(s_.sources), len(s_.targets),
+                                  *[emit(x) for x in s_.sources], *[emit(x) for x in s_.targets],
+                                  *[col_idx[o] for o in s_.outs]))
+                else:
+                    w_ = [STEP_LOGUP, s_.round, mod_idx[s_.module], col_idx[s_.out], len(s_.terms)]
+                    for e_, m_ in s_.terms:
+                        w_ += [emit(e_), emit(m_)]
+                    steps.append(tuple(w_))
 
         w: List[int] = [MAGIC, n_rounds, len(mod_names), len(columns), len(nodes), len(steps)]
 
@@ -309,6 +414,75 @@ def permutation_within_module(b: Builder, module: str, A: Sequence[Expr], B: Seq
     gp = b.fresh_name("gp_")
     b.add_grand_product_step(ROUND_RUNNING_SUMS, module, amul, bmul, gp)
     b.modules[module].assert_equal_at(const(1), col(gp), 0)
+
+
+def logup_constraint_degree(terms: Sequence[Tuple[Expr, Expr]]) -> int:
+    """board/logup.go:41-51."""
+    sum_e = sum(e.degree() for e, _ in terms)
+    deg = 1 + sum_e
+    for e, m in terms:
+        deg = max(deg, m.degree() + sum_e - e.degree())
+    return deg
+
+
+def range_module_name(bound: int) -> str:
+    return f"{RANGE_MODULE}_{bound}"
+
+
+def range_col_name(bound: int) -> str:
+    return f"{RANGE_MODULE}.bound_{bound}"
+
+
+def range_check(b: "Builder", S: Expr, s_module: str, bound: int):
+    """arguments/lookup.go:31-47 Range: S ⊂ {0, .., bound-1} (bound rounded up
+    to a power of two); the range module and its column are created on first
+    use (board/module.go:56-71: values 0..bound-1 on its `bound` rows)."""
+    bound = 1 << max(0, (bound - 1).bit_length())
+    rm = range_module_name(bound)
+    if rm not in b.modules:
+        b.add_module(Module(rm, bound))
+        b.generated[range_col_name(bound)] = np.arange(bound, dtype=np.uint32)
+    lookup(b, [(S, s_module)], [(col(range_col_name(bound)), rm)])
+
+
+def lookup(b: "Builder", S: Sequence[Tuple[Expr, str]], T: Sequence[Tuple[Expr, str]]):
+    """arguments/lookup.go:53-80 LookupUnion of width-1 tables (expression,
+    module): stage the tables and their multiplicities at RoundFold, then one
+    cyclic logup column per module at RoundRunningSums with fractions
+    1/(s - gamma) and -m/(t - gamma)."""
+    mult = b.fresh_name("Mult_")
+    for e, _ in list(S) + list(T):
+        b.stage_leaves(ROUND_FOLD, e)
+    outs = b.add_lookup_multiplicity_step(ROUND_FOLD, [e for e, _ in S], [e for e, _ in T], mult)
+    b.stage_columns(ROUND_FOLD, *outs)
+    gamma = coin(ROUND_LOG_DERIVATIVE)
+    minus_one = const(F.P - 1)
+    terms = [(mod, e - gamma, const(1)) for e, mod in S]
+    terms += [(mod, e - gamma, minus_one * col(outs[i])) for i, (e, mod) in enumerate(T)]
+    return add_logup_columns(b, f"{LOGUP}_", terms)
+
+
+def add_logup_columns(b: "Builder", prefix: str, terms: Sequence[Tuple[str, Expr, Expr]]) -> List[str]:
+    """arguments/lookup.go:176-214: terms grouped by module (first-appearance
+    order), batched up to MAX_LOGUP_BATCH per column within the degree bound."""
+    order: List[str] = []
+    by_mod: Dict[str, List[Tuple[Expr, Expr]]] = {}
+    for mod, e, m in terms:
+        if mod not in by_mod:
+            order.append(mod)
+            by_mod[mod] = []
+        by_mod[mod].append((e, m))
+    totals = []
+    for mod in order:
+        ts = by_mod[mod]
+        while ts:
+            n = 1
+            while n < min(MAX_LOGUP_BATCH, len(ts)) and logup_constraint_degree(ts[:n + 1]) <= MAX_LOGUP_DEGREE:
+                n += 1
+            name = b.fresh_name(f"{mod}.{prefix}") + "_0"
+            totals.append(b.add_cyclic_logup_step(ROUND_RUNNING_SUMS, mod, ts[:n], name))
+            ts = ts[n:]
+    return totals
 
 
 def id_support(n_chunks: int, n: int) -> List[np.ndarray]:

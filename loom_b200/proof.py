@@ -9,7 +9,9 @@ checked against the CPU oracle: every integer and every field element is a
 4-byte big-endian word, field elements in canonical (non-Montgomery) form,
 E6 values as 6 words [B0.A0, B0.A1, B1.A0, B1.A1, B2.A0, B2.A1], digests as
 8 words, strings as a length word then the bytes, lists as a count word then
-the items, in struct field order.
+the items, in struct field order.  The exposed values (a Go map) are listed by
+name: name, entry count, then per entry its index, its field kind (0 base,
+1 extension) and six words (the value as an extension element).
 """
 from __future__ import annotations
 
@@ -77,6 +79,7 @@ class WMerkleProof:
 @dataclass
 class Proof:
     hash_backend: str
+    exposed: dict              # name -> [(index, field kind, e6)]
     commitments: list
     claimed_values: list       # [batch][group] -> {"base": [[e6]], "ext": [[e6]]}
     levels_root: tuple
@@ -115,8 +118,10 @@ def _row(r: _R) -> RawRow:
 def decode(b: bytes) -> Proof:
     r = _R(b)
     hb = r.str()
-    if r.u32() != 0:
-        raise ValueError("exposed values are not supported by this decoder")
+    exposed = {}
+    for _ in range(r.u32()):
+        name = r.str()
+        exposed[name] = [(r.u32(), r.u32(), r.e6()) for _ in range(r.u32())]
     commits = [r.digest() for _ in range(r.u32())]
     cvs = []
     for _ in range(r.u32()):
@@ -146,4 +151,4 @@ def decode(b: bytes) -> Proof:
         ps.append(per)
     if r.o != len(b):
         raise ValueError(f"trailing bytes: {len(b) - r.o}")
-    return Proof(hb, commits, cvs, levels_root, lq, roots, ff, final, fq, ps, b)
+    return Proof(hb, exposed, commits, cvs, levels_root, lq, roots, ff, final, fq, ps, b)

@@ -53,14 +53,41 @@ Program parse_program(const uint32_t* w, size_t n) {
   }
   for (uint32_t i = 0; i < nn; i++) {
     PNode x; x.op = rd(); x.a = rd(); x.b = rd();
-    if (x.op >= OP_ADD && (x.a >= i || x.b >= i)) throw std::runtime_error("program: node children must precede parents");
+    if (x.op > OP_EXPAVG) throw std::runtime_error("program: unknown node op");
+    if (x.op >= OP_ADD && x.op <= OP_MUL && (x.a >= i || x.b >= i))
+      throw std::runtime_error("program: node children must precede parents");
     if (x.op == OP_COL && x.a >= nc) throw std::runtime_error("program: node column out of range");
     p.nodes.push_back(x);
   }
+  uint32_t n_exposed = 0;
+  auto node = [&]() { uint32_t v = rd(); if (v >= nn) throw std::runtime_error("program: step node out of range"); return v; };
+  auto column = [&]() { uint32_t v = rd(); if (v >= nc) throw std::runtime_error("program: step column out of range"); return v; };
   for (uint32_t i = 0; i < ns; i++) {
-    PStep s; s.type = rd(); s.round = rd(); s.module = rd(); s.num = rd(); s.den = rd(); s.out = rd();
+    PStep s;
+    s.type = rd();
+    s.round = rd();
+    if (s.type == STEP_GP) {
+      s.module = rd(); s.num = node(); s.den = node(); s.out = column();
+    } else if (s.type == STEP_MULT) {
+      uint32_t a = rd(), b = rd();
+      if (!a || !b || a > 4096 || b > 4096) throw std::runtime_error("program: bad multiplicity step");
+      for (uint32_t k = 0; k < a; k++) s.src.push_back(node());
+      for (uint32_t k = 0; k < b; k++) s.tgt.push_back(node());
+      for (uint32_t k = 0; k < b; k++) s.outs.push_back(column());
+    } else if (s.type == STEP_LOGUP) {
+      s.module = rd(); s.out = column();
+      uint32_t t = rd();
+      if (!t || t > 16) throw std::runtime_error("program: bad logup step");
+      for (uint32_t k = 0; k < t; k++) { s.e.push_back(node()); s.m.push_back(node()); }
+      s.exposed = n_exposed++;
+    } else {
+      throw std::runtime_error("program: unknown step type");
+    }
+    if (s.module >= nm) throw std::runtime_error("program: step module out of range");
     p.steps.push_back(s);
   }
+  for (const PNode& x : p.nodes)
+    if (x.op == OP_EXPAVG && x.a >= n_exposed) throw std::runtime_error("program: exposed value out of range");
   for (uint32_t r = 0; r < p.n_rounds; r++) {
     uint32_t k = rd();
     std::vector<uint32_t> v;
@@ -103,12 +130,15 @@ Val vmul(const Val& x, const Val& y) {
 }
 
 const int NEG_INF = -1000000;
+inline bool is_binary(uint32_t op) { return op == OP_ADD || op == OP_SUB || op == OP_MUL; }
 
 struct Prover {
   const Program& pg;
   uint32_t num_queries;
   Transcript fs;
   std::vector<E6> coins;              // per round
+  std::vector<E6> exposed;            // logup totals, in step order
+  std::vector<std::string> exposed_names;
   std::map<uint32_t, std::vector<uint32_t>> base;  // column id -> Lagrange-normal values
   std::map<uint32_t, std::vector<E6>> ext;
   std::vector<uint32_t> mod_order;    // module ids sorted by name
@@ -146,6 +176,7 @@ struct Prover {
     int d = 0;
     switch (x.op) {
       case OP_COL: d = 1; break;
+      case OP_EXPAVG: d = 1; break;  // a verifier column (internal/dag/dag.go:1536)
       case OP_COIN: d = 0; break;
       case OP_CONST: d = x.a == 0 ? NEG_INF : 0; break;
       case OP_ADD: case OP_SUB: d = std::max(node_degree(x.a, memo), node_degree(x.b, memo)); break;
@@ -162,8 +193,8 @@ struct Prover {
     const PNode& x = nodes[id];
     bool e = false;
     if (x.op == OP_COL) e = pg.columns[x.a].field == 1;
-    else if (x.op == OP_COIN) e = true;
-    else if (x.op >= OP_ADD) e = node_ext(x.a, memo) || node_ext(x.b, memo);
+    else if (x.op == OP_COIN || x.op == OP_EXPAVG) e = true;
+    else if (is_binary(x.op)) e = node_ext(x.a, memo) || node_ext(x.b, memo);
     memo[id] = e;
     return e;
   }
@@ -171,7 +202,7 @@ struct Prover {
     if (seen[id]) return;
     seen[id] = 1;
     const PNode& x = nodes[id];
-    if (x.op >= OP_ADD) { collect(x.a, seen, order); collect(x.b, seen, order); }
+    if (is_binary(x.op)) { collect(x.a, seen, order); collect(x.b, seen, order); }
     order.push_back(id);
   }
 
@@ -190,6 +221,7 @@ struct Prover {
         }
         case OP_COIN: v = ve(coins.at(x.a)); break;
         case OP_CONST: v = vb(x.a); break;
+        case OP_EXPAVG: v = ve(e6_mul_base(exposed.at(x.a), inv((uint32_t)n))); break;
         case OP_ADD: v = vadd(scratch[x.a], scratch[x.b]); break;
         case OP_SUB: v = vsub(scratch[x.a], scratch[x.b]); break;
         default: v = vmul(scratch[x.a], scratch[x.b]); break;
@@ -365,8 +397,107 @@ struct Prover {
   // ---------------------------------------------------------- steps
   // Grand product R[0] = 1, R[i+1] = R[i] num(i)/den(i)
   // (internal/poly/iop_utils.go:170-192,316-323)
+  // module whose rows an expression ranges over: that of its first column
+  uint32_t expr_module(uint32_t root) {
+    std::vector<char> seen(nodes.size(), 0);
+    std::vector<uint32_t> order;
+    collect(root, seen, order);
+    for (uint32_t id : order)
+      if (nodes[id].op == OP_COL) return pg.columns[nodes[id].a].module;
+    throw std::runtime_error("lookup table without a column");
+  }
+  std::vector<uint32_t> eval_base_rows(uint32_t root, uint32_t module) {
+    size_t n = mod_n(module);
+    std::vector<char> seen(nodes.size(), 0);
+    std::vector<uint32_t> order;
+    collect(root, seen, order);
+    auto colval = [&](uint32_t c, size_t r) -> Val {
+      if (pg.columns[c].field == 0) return vb(base.at(c)[r]);
+      return ve(ext.at(c)[r]);
+    };
+    std::vector<uint32_t> out(n);
+    std::vector<Val> sc(nodes.size());
+    for (size_t j = 0; j < n; j++) {
+      Val v = eval(order, root, j, n, colval, sc);
+      if (v.ext) throw std::runtime_error("lookup table values must be base-field");
+      out[j] = v.b;
+    }
+    return out;
+  }
+
+  // Lookup multiplicities of width-1 tables (internal/poly/lookup_multiplicity.go:37-100):
+  // the weight of every source value goes to its first target row (T[0]
+  // rows, then T[1] rows, ...); a source value found in no target is an error.
+  void run_multiplicities(const PStep& st) {
+    std::map<uint32_t, uint32_t> weight;
+    for (uint32_t s : st.src)
+      for (uint32_t v : eval_base_rows(s, expr_module(s))) weight[v] = add(weight[v], 1);
+    std::set<uint32_t> assigned;
+    for (size_t k = 0; k < st.tgt.size(); k++) {
+      uint32_t mod = expr_module(st.tgt[k]);
+      std::vector<uint32_t> tv = eval_base_rows(st.tgt[k], mod), res(tv.size(), 0);
+      for (size_t i = 0; i < tv.size(); i++) {
+        auto it = weight.find(tv[i]);
+        if (it == weight.end() || assigned.count(tv[i])) continue;
+        res[i] = it->second;
+        assigned.insert(tv[i]);
+      }
+      if (pg.columns[st.outs[k]].module != mod) throw std::runtime_error("multiplicity column module");
+      base[st.outs[k]] = res;
+    }
+    for (auto& kv : weight)
+      if (!assigned.count(kv.first) && kv.second) throw std::runtime_error("lookup: source value not in the table");
+  }
+
+  // Cyclic logup column (board/logup.go:129-180, internal/poly/iop_utils.go:110-131):
+  // v_i = sum_j M_j(i) / E_j(i); S_i = v_0 + ... + v_i; T = S_{n-1};
+  // L_i = S_i - (i + 1) T / n.  T is exposed.
+  void run_logup(const PStep& st) {
+    size_t n = mod_n(st.module);
+    auto colval = [&](uint32_t c, size_t r) -> Val {
+      if (pg.columns[c].field == 0) return vb(base.at(c)[r]);
+      return ve(ext.at(c)[r]);
+    };
+    std::vector<std::vector<uint32_t>> oe(st.e.size()), om(st.e.size());
+    for (size_t k = 0; k < st.e.size(); k++) {
+      std::vector<char> s1(nodes.size(), 0), s2(nodes.size(), 0);
+      collect(st.e[k], s1, oe[k]);
+      collect(st.m[k], s2, om[k]);
+    }
+    std::vector<E6> col(n);
+    std::vector<Val> sc(nodes.size());
+    E6 run = e6_zero();
+    std::vector<E6> sums(n);
+    for (size_t j = 0; j < n; j++) {
+      E6 v = e6_zero();
+      for (size_t k = 0; k < st.e.size(); k++) {
+        E6 e = as_e6(eval(oe[k], st.e[k], j, n, colval, sc));
+        E6 m = as_e6(eval(om[k], st.m[k], j, n, colval, sc));
+        if (e6_is_zero(e)) throw std::runtime_error("logup: zero denominator");
+        v = e6_add(v, e6_mul(m, e6_inv(e)));
+      }
+      run = e6_add(run, v);
+      sums[j] = run;
+    }
+    E6 total = sums[n - 1];
+    E6 avg = e6_mul_base(total, inv((uint32_t)n));
+    E6 shift = e6_zero();
+    for (size_t i = 0; i < n; i++) {
+      shift = e6_add(shift, avg);
+      col[i] = e6_sub(sums[i], shift);
+    }
+    if (pg.columns[st.out].module != st.module || pg.columns[st.out].field != 1)
+      throw std::runtime_error("logup column must be an extension column of its module");
+    ext[st.out] = col;
+    if (exposed.size() <= st.exposed) { exposed.resize(st.exposed + 1); exposed_names.resize(st.exposed + 1); }
+    exposed[st.exposed] = total;
+    exposed_names[st.exposed] = pg.columns[st.out].name + "_total";
+  }
+
   void run_step(const PStep& st) {
-    if (st.type != 0) throw std::runtime_error("unsupported step type");
+    if (st.type == STEP_MULT) return run_multiplicities(st);
+    if (st.type == STEP_LOGUP) return run_logup(st);
+    if (st.type != STEP_GP) throw std::runtime_error("unsupported step type");
     size_t n = mod_n(st.module);
     std::vector<uint32_t> order_n, order_d;
     { std::vector<char> seen(nodes.size(), 0); collect(st.num, seen, order_n); }
@@ -544,6 +675,14 @@ struct Prover {
         commitments.push_back(root);
         fs.bind(coin_name(r), root.v, 8);
         tree_idx++;
+      }
+      // BindExposedValues (prover/prover.go:386-396): in step order, entry
+      // index then the value as six elements (board/logup.go:218-225)
+      for (const PStep& st : pg.steps) {
+        if (st.round != r || st.type != STEP_LOGUP) continue;
+        uint32_t w[7] = {0};
+        for (int k = 0; k < 6; k++) w[1 + k] = exposed[st.exposed].c[k];
+        fs.bind(coin_name(r), w, 7);
       }
       coins[r] = digest_to_e6(fs.compute(coin_name(r)));
     }
@@ -734,7 +873,19 @@ struct Prover {
 
     // ---- serialize (canonical encoding; see loom_gpu.h)
     W.str("poseidon2");
-    W.u32(0);  // exposed values
+    {  // exposed values, by name: name, entries (index, field kind 1 = ext, six words)
+      std::vector<size_t> ord(exposed.size());
+      for (size_t i = 0; i < ord.size(); i++) ord[i] = i;
+      std::sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return exposed_names[a] < exposed_names[b]; });
+      W.u32((uint32_t)ord.size());
+      for (size_t i : ord) {
+        W.str(exposed_names[i]);
+        W.u32(1);
+        W.u32(0);
+        W.u32(1);
+        for (int k = 0; k < 6; k++) W.u32(exposed[i].c[k]);
+      }
+    }
     W.u32((uint32_t)commitments.size());
     for (auto& d : commitments) W.dg(d);
     W.u32((uint32_t)trees.size());

@@ -12,11 +12,17 @@
 //   column  : str name, module, field(0 base|1 ext), kind(0 witness|1 step
 //             output|2 Lagrange verifier column), param(int32 row; <0 means
 //             relative from the end, -(i+1))
-//   node    : op(0 col|1 coin|2 const|3 add|4 sub|5 mul), a, b
-//             col: a = column, b = shift (int32); coin: a = round;
+//   node    : op(0 col|1 coin|2 const|3 add|4 sub|5 mul|6 exposed average),
+//             a, b.  col: a = column, b = shift (int32); coin: a = round;
 //             const: a = canonical value; add/sub/mul: a, b = child nodes
-//             (children precede parents)
-//   step    : type(0 grand product), round, module, num_node, den_node, out_col
+//             (children precede parents); exposed average: a = exposed value
+//             (the a-th logup step's total), value total / N of the module
+//             evaluating it (expr/ast.go:223-227)
+//   step    : type 0 grand product: 0, round, module, num_node, den_node, out_col
+//             type 1 lookup multiplicities (width-1 tables): 1, round, n_src,
+//               n_tgt, src_node[n_src], tgt_node[n_tgt], out_col[n_tgt]
+//             type 2 cyclic logup: 2, round, module, out_col, n_terms,
+//               (E_node, M_node)[n_terms]; its total is exposed
 //   round   : n_staged, col[n_staged]
 //   str     : byte length, then the bytes packed 4 per word
 #pragma once
@@ -26,13 +32,19 @@
 
 namespace orc {
 
-enum { OP_COL = 0, OP_COIN = 1, OP_CONST = 2, OP_ADD = 3, OP_SUB = 4, OP_MUL = 5 };
+enum { OP_COL = 0, OP_COIN = 1, OP_CONST = 2, OP_ADD = 3, OP_SUB = 4, OP_MUL = 5, OP_EXPAVG = 6 };
+enum { STEP_GP = 0, STEP_MULT = 1, STEP_LOGUP = 2 };
 enum { KIND_WITNESS = 0, KIND_STEP = 1, KIND_LAGRANGE = 2 };
 
 struct PModule { uint32_t log_n; std::string name; std::vector<uint32_t> rels; };
 struct PColumn { std::string name; uint32_t module, field, kind; int32_t param; };
 struct PNode { uint32_t op, a, b; };
-struct PStep { uint32_t type, round, module, num, den, out; };
+struct PStep {
+  uint32_t type, round, module = 0, num = 0, den = 0, out = 0;
+  std::vector<uint32_t> src, tgt, outs;   // multiplicities
+  std::vector<uint32_t> e, m;             // logup terms M/E
+  uint32_t exposed = 0;                   // logup: index of its exposed total
+};
 struct Program {
   uint32_t n_rounds = 0;
   std::vector<PModule> modules;
