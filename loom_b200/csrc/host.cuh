@@ -269,12 +269,19 @@ struct Ctx {
 
 // ---------------------------------------------------------------- program
 // Flat descriptor; the format is documented in include/loom_gpu.h.
-enum { OP_COL = 0, OP_COIN = 1, OP_CONST = 2, OP_ADD = 3, OP_SUB = 4, OP_MUL = 5 };
+enum { OP_COL = 0, OP_COIN = 1, OP_CONST = 2, OP_ADD = 3, OP_SUB = 4, OP_MUL = 5, OP_EXPAVG = 6 };
 enum { KIND_WITNESS = 0, KIND_STEP = 1, KIND_LAGRANGE = 2 };
+enum { STEP_GP = 0, STEP_MULT = 1, STEP_LOGUP = 2 };
+inline bool is_binary(uint32_t op) { return op == OP_ADD || op == OP_SUB || op == OP_MUL; }
 struct Module { uint32_t log_n; std::string name; std::vector<uint32_t> rels; };
 struct Column { std::string name; uint32_t module, field, kind; int32_t param; };
 struct Node { uint32_t op, a, b; };
-struct Step { uint32_t type, round, module, num, den, out; };
+struct Step {
+  uint32_t type, round, module = 0, num = 0, den = 0, out = 0;
+  std::vector<uint32_t> src, tgt, outs;  // lookup multiplicities (width-1 tables)
+  std::vector<uint32_t> e, m;            // cyclic logup: fractions m[k] / e[k]
+  uint32_t exposed = 0;                  // cyclic logup: index of its exposed total
+};
 struct Program {
   uint32_t n_rounds = 0;
   std::vector<Module> modules;
@@ -323,18 +330,56 @@ inline Program parse_program(const uint32_t* w, size_t n) {
   }
   for (uint32_t i = 0; i < nn; i++) {
     Node x{rd(), rd(), rd()};
-    if (x.op > OP_MUL) throw Error(LG_ERR_INVALID, "bad node op");
-    if (x.op >= OP_ADD && (x.a >= i || x.b >= i)) throw Error(LG_ERR_INVALID, "node children must precede parents");
+    if (x.op > OP_EXPAVG) throw Error(LG_ERR_INVALID, "bad node op");
+    if (is_binary(x.op) && (x.a >= i || x.b >= i)) throw Error(LG_ERR_INVALID, "node children must precede parents");
     if (x.op == OP_COL && x.a >= nc) throw Error(LG_ERR_INVALID, "node column out of range");
     if (x.op == OP_COIN && x.a >= p.n_rounds) throw Error(LG_ERR_INVALID, "node coin out of range");
     p.nodes.push_back(x);
   }
+  uint32_t n_exposed = 0;
+  auto node = [&]() {
+    uint32_t v = rd();
+    if (v >= nn) throw Error(LG_ERR_INVALID, "step node out of range");
+    return v;
+  };
+  auto column = [&]() {
+    uint32_t v = rd();
+    if (v >= nc) throw Error(LG_ERR_INVALID, "step column out of range");
+    return v;
+  };
   for (uint32_t i = 0; i < ns; i++) {
-    Step s{rd(), rd(), rd(), rd(), rd(), rd()};
-    if (s.type != 0 || s.round >= p.n_rounds || s.module >= nm || s.num >= nn || s.den >= nn || s.out >= nc)
-      throw Error(LG_ERR_INVALID, "bad step");
+    Step s;
+    s.type = rd();
+    s.round = rd();
+    if (s.type == STEP_GP) {
+      s.module = rd();
+      s.num = node();
+      s.den = node();
+      s.out = column();
+    } else if (s.type == STEP_MULT) {
+      uint32_t a = rd(), b = rd();
+      if (!a || !b || a > 4096 || b > 4096) throw Error(LG_ERR_INVALID, "bad multiplicity step");
+      for (uint32_t k = 0; k < a; k++) s.src.push_back(node());
+      for (uint32_t k = 0; k < b; k++) s.tgt.push_back(node());
+      for (uint32_t k = 0; k < b; k++) s.outs.push_back(column());
+    } else if (s.type == STEP_LOGUP) {
+      s.module = rd();
+      s.out = column();
+      uint32_t t = rd();
+      if (!t || t > 16) throw Error(LG_ERR_INVALID, "bad logup step");
+      for (uint32_t k = 0; k < t; k++) {
+        s.e.push_back(node());
+        s.m.push_back(node());
+      }
+      s.exposed = n_exposed++;
+    } else {
+      throw Error(LG_ERR_INVALID, "unknown step type");
+    }
+    if (s.round >= p.n_rounds || s.module >= nm) throw Error(LG_ERR_INVALID, "bad step");
     p.steps.push_back(s);
   }
+  for (const Node& x : p.nodes)
+    if (x.op == OP_EXPAVG && x.a >= n_exposed) throw Error(LG_ERR_INVALID, "exposed value out of range");
   for (uint32_t r = 0; r < p.n_rounds; r++) {
     uint32_t k = rd();
     std::vector<uint32_t> v;

@@ -621,49 +621,57 @@ __device__ __forceinline__ void st6(uint32_t* p, uint64_t stride, uint64_t i, co
 // shifted result out[0] = 1, out[i] = prod_{k<i} x[k].  One job per vector.
 struct ScanJob { uint32_t* x; uint64_t n; uint32_t* totals; uint32_t* pre; uint32_t* out; uint32_t nt; };
 
+// The scans run over products (grand products) or sums (logup running sums).
+template <bool SUM> __device__ __forceinline__ E6 scan_id() { return SUM ? e6_zero() : e6_one(); }
+template <bool SUM> __device__ __forceinline__ E6 scan_op(const E6& a, const E6& b) {
+  return SUM ? e6_add(a, b) : e6_mul(a, b);
+}
+
+template <bool SUM = false>
 __global__ void k_scan_tiles(const ScanJob* jobs) {
   __shared__ E6 part[SCAN_BLOCK];
   const ScanJob& J = jobs[blockIdx.y];
   if (blockIdx.x >= J.nt) return;
   const uint64_t n = J.n;
   const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_PER_THREAD;
-  E6 acc = e6_one();
+  E6 acc = scan_id<SUM>();
   E6 v[SCAN_PER_THREAD];
   for (int i = 0; i < SCAN_PER_THREAD; i++) {
     uint64_t idx = base + i;
-    v[i] = idx < n ? ld6(J.x, n, idx) : e6_one();
-    acc = e6_mul(acc, v[i]);
+    v[i] = idx < n ? ld6(J.x, n, idx) : scan_id<SUM>();
+    acc = scan_op<SUM>(acc, v[i]);
     v[i] = acc;
   }
   part[threadIdx.x] = acc;
   __syncthreads();
   for (int off = 1; off < SCAN_BLOCK; off <<= 1) {
-    E6 t = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : e6_one();
+    E6 t = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : scan_id<SUM>();
     __syncthreads();
-    if (threadIdx.x >= (unsigned)off) part[threadIdx.x] = e6_mul(part[threadIdx.x], t);
+    if (threadIdx.x >= (unsigned)off) part[threadIdx.x] = scan_op<SUM>(part[threadIdx.x], t);
     __syncthreads();
   }
-  E6 pre = threadIdx.x ? part[threadIdx.x - 1] : e6_one();
+  E6 pre = threadIdx.x ? part[threadIdx.x - 1] : scan_id<SUM>();
   for (int i = 0; i < SCAN_PER_THREAD; i++) {
     uint64_t idx = base + i;
-    if (idx < n) st6(J.x, n, idx, e6_mul(pre, v[i]));
+    if (idx < n) st6(J.x, n, idx, scan_op<SUM>(pre, v[i]));
   }
   if (threadIdx.x == SCAN_BLOCK - 1)
     for (int w = 0; w < 6; w++) J.totals[w * J.nt + blockIdx.x] = part[SCAN_BLOCK - 1].c[w];
 }
 
-// Exclusive prefix products of the tile totals (one thread per job; nt is
-// n / 2048).
+// Exclusive prefix (products or sums) of the tile totals (one thread per
+// job; nt is n / 2048).
+template <bool SUM = false>
 __global__ void k_tile_prefix(const ScanJob* jobs, uint32_t n_jobs) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_jobs) return;
   const ScanJob& J = jobs[i];
-  E6 acc = e6_one();
+  E6 acc = scan_id<SUM>();
   for (uint32_t t = 0; t < J.nt; t++) {
     for (int w = 0; w < 6; w++) J.pre[t * 6 + w] = acc.c[w];
     E6 v;
     for (int w = 0; w < 6; w++) v.c[w] = J.totals[w * J.nt + t];
-    acc = e6_mul(acc, v);
+    acc = scan_op<SUM>(acc, v);
   }
 }
 
@@ -680,6 +688,124 @@ __global__ void k_gp_finish(const ScanJob* jobs) {
     v = e6_mul(pre, ld6(J.x, J.n, k));
   }
   st6(J.out, J.n, i, v);
+}
+
+// ---------------------------------------------------------------- lookups
+// Cyclic logup fractions (internal/poly/iop_utils.go:110-131): per row,
+// frac = sum_k M_k / E_k over the step's terms.  One job per step.
+constexpr int LOGUP_MAX_TERMS = 4;
+struct LogupJob {
+  XProgram e[LOGUP_MAX_TERMS], m[LOGUP_MAX_TERMS];
+  uint32_t n_terms;
+  const uint32_t* const* lanes;
+  uint32_t* frac;
+  int logn;
+};
+__global__ void k_logup_frac(const LogupJob* jobs, const E6* coins) {
+  extern __shared__ uint32_t regs[];
+  const LogupJob& J = jobs[blockIdx.y];
+  const uint32_t n = 1u << J.logn;
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const uint32_t* const* lanes = J.lanes;
+  auto lane = [&](uint32_t l, uint32_t row) -> uint32_t { return lanes[l][row]; };
+  E6 v = e6_zero();
+  for (uint32_t k = 0; k < J.n_terms; k++) {
+    E6 e = x_eval(J.e[k], coins, regs + threadIdx.x, blockDim.x, j, n, lane);
+    E6 m = x_eval(J.m[k], coins, regs + threadIdx.x, blockDim.x, j, n, lane);
+    v = e6_add(v, e6_mul(m, e6_inv(e)));
+  }
+  for (int w = 0; w < 6; w++) J.frac[(uint64_t)w * n + j] = v.c[w];
+}
+
+// L_i = S_i - (i + 1) T / n with S the inclusive running sums (tile scans in
+// x plus the tile prefixes) and T = S_{n-1}; thread 0 writes T to `total`
+// (board/logup.go:150-170).
+struct LogupFinish { uint32_t* total; uint32_t n_inv; };
+__global__ void k_logup_finish(const ScanJob* jobs, const LogupFinish* fin) {
+  const ScanJob& J = jobs[blockIdx.y];
+  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= J.n) return;
+  auto prefix = [&](uint64_t k) {
+    E6 pre;
+    for (int w = 0; w < 6; w++) pre.c[w] = J.pre[(k / SCAN_TILE) * 6 + w];
+    return e6_add(pre, ld6(J.x, J.n, k));
+  };
+  const E6 T = prefix(J.n - 1);
+  const E6 avg = e6_mul_base(T, fin[blockIdx.y].n_inv);
+  const E6 L = e6_sub(prefix(i), e6_mul_base(avg, to_mont((uint32_t)(i + 1))));
+  st6(J.out, J.n, i, L);
+  if (i == 0)
+    for (int w = 0; w < 6; w++) fin[blockIdx.y].total[w] = T.c[w];
+}
+
+// Lookup multiplicities of width-1 tables (internal/poly/lookup_multiplicity.go:37-100)
+// with an open-addressing table per step: target values are inserted with
+// the smallest combined row index (T_0 rows, then T_1 rows, ...) holding them,
+// sources add one to the count of their value's first row, and the counts
+// become the multiplicity columns.  A source value absent from every target
+// sets `missing`.  All probe loops stop after `cap` slots.
+constexpr uint32_t MULT_EMPTY = 0xffffffffu;
+struct MultTab { uint32_t* keys; uint32_t* first; uint32_t* count; uint32_t cap; };
+struct MultVec { const uint32_t* vals; uint32_t n, comb_off, tab; uint32_t* out; };
+__device__ __forceinline__ uint32_t mult_hash(uint32_t v, uint32_t mask) {
+  v ^= v >> 16;
+  v *= 0x7feb352du;
+  v ^= v >> 15;
+  v *= 0x846ca68bu;
+  v ^= v >> 16;
+  return v & mask;
+}
+__global__ void k_mult_insert(const MultVec* tv, const MultTab* tabs) {
+  const MultVec V = tv[blockIdx.y];
+  const MultTab T = tabs[V.tab];
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V.n) return;
+  const uint32_t key = V.vals[i], mask = T.cap - 1;
+  uint32_t h = mult_hash(key, mask);
+  for (uint32_t probe = 0; probe < T.cap; probe++, h = (h + 1) & mask) {
+    const uint32_t prev = atomicCAS(T.keys + h, MULT_EMPTY, key);
+    if (prev == MULT_EMPTY || prev == key) {
+      atomicMin(T.first + h, V.comb_off + i);
+      return;
+    }
+  }
+}
+__global__ void k_mult_count(const MultVec* sv, const MultTab* tabs, uint32_t* missing) {
+  const MultVec V = sv[blockIdx.y];
+  const MultTab T = tabs[V.tab];
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V.n) return;
+  const uint32_t key = V.vals[i], mask = T.cap - 1;
+  uint32_t h = mult_hash(key, mask);
+  for (uint32_t probe = 0; probe < T.cap; probe++, h = (h + 1) & mask) {
+    const uint32_t k = T.keys[h];
+    if (k == key) {
+      atomicAdd(T.count + T.first[h], 1u);
+      return;
+    }
+    if (k == MULT_EMPTY) break;
+  }
+  atomicOr(missing, 1u);
+}
+__global__ void k_mult_write(const MultVec* tv, const MultTab* tabs) {
+  const MultVec V = tv[blockIdx.y];
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V.n) return;
+  V.out[i] = to_mont(tabs[V.tab].count[V.comb_off + i]);
+}
+// Values of a base-field expression on every row (for lookup tables that are
+// not plain columns).
+struct EvalJob { XProgram p; const uint32_t* const* lanes; uint32_t* out; int logn; };
+__global__ void k_eval_base(const EvalJob* jobs, const E6* coins) {
+  extern __shared__ uint32_t regs[];
+  const EvalJob& J = jobs[blockIdx.y];
+  const uint32_t n = 1u << J.logn;
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const uint32_t* const* lanes = J.lanes;
+  auto lane = [&](uint32_t l, uint32_t row) -> uint32_t { return lanes[l][row]; };
+  J.out[j] = x_eval(J.p, coins, regs + threadIdx.x, blockDim.x, j, n, lane).c[0];
 }
 
 // ---------------------------------------------------------------- claimed values

@@ -35,6 +35,16 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
       fs.bind(coin_name(r), root.v, 8);
       ti++;
     }
+    // BindExposedValues (prover/prover.go:386-396): the round's logup totals
+    // in step order, each as its entry index then six elements
+    // (board/logup.go:218-225)
+    read_exposed(r);
+    for (const Step& st : pg.steps) {
+      if (st.round != r || st.type != STEP_LOGUP) continue;
+      uint32_t w[7] = {0};
+      for (int k = 0; k < 6; k++) w[1 + k] = exposed[st.exposed].c[k];
+      fs.bind(coin_name(r), w, 7);
+    }
     coins[r] = digest_e6(fs.compute(coin_name(r)));
     c.phase(("round " + std::to_string(r)).c_str());
   }
@@ -540,7 +550,20 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
   Writer W(c.proof_buf, out, out_cap);
   W.expect((size_t)4 * SB.total + (1 << 20));
   W.str("poseidon2");
-  W.u32(0);
+  {  // exposed values by name: name, one entry (index 0, extension kind 1, value)
+    std::vector<std::pair<std::string, size_t>> ev;
+    for (const Step& st : pg.steps)
+      if (st.type == STEP_LOGUP) ev.push_back({pg.columns[st.out].name + "_total", st.exposed});
+    std::sort(ev.begin(), ev.end());
+    W.u32((uint32_t)ev.size());
+    for (auto& e : ev) {
+      W.str(e.first);
+      W.u32(1);
+      W.u32(0);
+      W.u32(1);
+      W.e6(exposed[e.second]);
+    }
+  }
   W.u32((uint32_t)commitments.size());
   for (auto& d : commitments) W.dg(d);
   W.u32((uint32_t)trees.size());

@@ -23,6 +23,10 @@ struct Prover {
   uint32_t num_queries;
   Transcript fs;
   std::vector<E6> coins;
+  // Exposed values (logup totals, in step order): Montgomery E6 once read back.
+  std::vector<E6> exposed;
+  std::vector<char> exposed_ready;
+  DBufP exposed_d;  // 6 words per exposed value, written by k_logup_finish
   DBufP coins_dev;
   std::vector<uint32_t> mod_order;
   std::vector<int> fold_root, degree;
@@ -62,6 +66,7 @@ struct Prover {
     int d = 0;
     switch (x.op) {
       case OP_COL: d = 1; break;
+      case OP_EXPAVG: d = 1; break;  // a verifier column (internal/dag/dag.go:1536)
       case OP_COIN: d = 0; break;
       case OP_CONST: d = x.a % P == 0 ? NEG_INF : 0; break;
       case OP_ADD: case OP_SUB: d = std::max(node_degree(x.a, memo), node_degree(x.b, memo)); break;
@@ -75,7 +80,7 @@ struct Prover {
   bool node_ext(uint32_t id) const {
     const Node& x = pg.nodes[id];
     if (x.op == OP_COL) return pg.columns[x.a].field == 1;
-    if (x.op == OP_COIN) return true;
+    if (x.op == OP_COIN || x.op == OP_EXPAVG) return true;
     if (x.op == OP_CONST) return false;
     return false;  // combined by the caller through ext_of
   }
@@ -84,7 +89,7 @@ struct Prover {
     ext_of.assign(pg.nodes.size(), 0);
     for (size_t i = 0; i < pg.nodes.size(); i++) {
       const Node& x = pg.nodes[i];
-      if (x.op >= OP_ADD) ext_of[i] = ext_of[x.a] || ext_of[x.b];
+      if (is_binary(x.op)) ext_of[i] = ext_of[x.a] || ext_of[x.b];
       else ext_of[i] = node_ext((uint32_t)i);
     }
   }
@@ -95,7 +100,7 @@ struct Prover {
       st.pop_back();
       if (seen[x]) continue;
       seen[x] = 1;
-      if (pg.nodes[x].op >= OP_ADD) { st.push_back(pg.nodes[x].a); st.push_back(pg.nodes[x].b); }
+      if (is_binary(pg.nodes[x].op)) { st.push_back(pg.nodes[x].a); st.push_back(pg.nodes[x].b); }
     }
   }
 
@@ -110,7 +115,7 @@ struct Prover {
     std::vector<int> last(pg.nodes.size(), -1);
     for (size_t k = 0; k < order.size(); k++) {
       const Node& x = pg.nodes[order[k]];
-      if (x.op >= OP_ADD) { last[x.a] = (int)k; last[x.b] = (int)k; }
+      if (is_binary(x.op)) { last[x.a] = (int)k; last[x.b] = (int)k; }
     }
     last[root] = (int)order.size();
     std::vector<int> reg(pg.nodes.size(), -1);
@@ -122,7 +127,7 @@ struct Prover {
       XInst in{};
       // free operand registers whose last use is here (after reading them)
       std::vector<uint32_t> to_free;
-      if (x.op >= OP_ADD) {
+      if (is_binary(x.op)) {
         if (last[x.a] == (int)k) to_free.push_back((uint32_t)reg[x.a]);
         if (last[x.b] == (int)k && x.b != x.a) to_free.push_back((uint32_t)reg[x.b]);
       }
@@ -130,8 +135,8 @@ struct Prover {
       if (!free_regs.empty()) { d = free_regs.back(); free_regs.pop_back(); }
       else d = xc.n_regs++;
       in.d = (uint8_t)d;
-      bool ea = x.op >= OP_ADD && ext_of[x.a], eb = x.op >= OP_ADD && ext_of[x.b];
-      uint32_t ra = x.op >= OP_ADD ? (uint32_t)reg[x.a] : 0, rb = x.op >= OP_ADD ? (uint32_t)reg[x.b] : 0;
+      bool ea = is_binary(x.op) && ext_of[x.a], eb = is_binary(x.op) && ext_of[x.b];
+      uint32_t ra = is_binary(x.op) ? (uint32_t)reg[x.a] : 0, rb = is_binary(x.op) ? (uint32_t)reg[x.b] : 0;
       switch (x.op) {
         case OP_COL:
           in.op = pg.columns[x.a].field ? X_LOAD_E : X_LOAD_B;
@@ -139,6 +144,8 @@ struct Prover {
           in.shift = (int32_t)x.b;
           break;
         case OP_COIN: in.op = X_COIN; in.imm = x.a; break;
+        // exposed averages follow the round coins in the kernels' coin table
+        case OP_EXPAVG: in.op = X_COIN; in.imm = pg.n_rounds + x.a; break;
         case OP_CONST: in.op = X_CONST; in.imm = to_mont(x.a % P); break;
         case OP_ADD:
           if (!ea && !eb) in.op = X_ADD_BB;
@@ -168,6 +175,8 @@ struct Prover {
 
   // ------------------------------------------------------------ setup
   void setup(const uint32_t* const* witness, bool on_device) {
+    exposed.assign(n_exposed(), e6_zero());
+    exposed_ready.assign(n_exposed(), 0);
     for (uint32_t m = 0; m < pg.modules.size(); m++) mod_order.push_back(m);
     std::sort(mod_order.begin(), mod_order.end(), [&](uint32_t a, uint32_t b) { return pg.modules[a].name < pg.modules[b].name; });
     // Host witness: one device buffer for all columns; columns that follow
@@ -287,9 +296,17 @@ struct Prover {
     return (uint32_t)(big / n);
   }
 
+  // Round coins, then the exposed averages total / N (N: the size of the
+  // logup column's module), as E6 Montgomery words.
   DBufP coins_on_device() {
     std::vector<uint32_t> w;
     for (auto& e : coins) for (int i = 0; i < 6; i++) w.push_back(e.c[i]);
+    for (const Step& st : pg.steps) {
+      if (st.type != STEP_LOGUP) continue;
+      E6 avg = exposed_ready[st.exposed] ? e6_mul_base(exposed[st.exposed], inv(to_mont((uint32_t)mod_n(st.module))))
+                                         : e6_zero();
+      for (int i = 0; i < 6; i++) w.push_back(avg.c[i]);
+    }
     return upload_vec(c, w);
   }
 
@@ -297,11 +314,223 @@ struct Prover {
   // Grand products of round r (internal/poly/iop_utils.go:170-192,316-323):
   // ratio num/den per row, then a product scan.  Batched: one launch per
   // kernel for all steps of the round; plain: one set of launches per step.
+  size_t n_exposed() const {
+    size_t k = 0;
+    for (const Step& st : pg.steps) k += st.type == STEP_LOGUP;
+    return k;
+  }
+
+  // Lanes of the columns an expression reads, in first-use order (lane_of
+  // for compile_expr).
+  struct LaneTable {
+    Prover* pr;
+    std::vector<const uint32_t*> lanes;
+    std::map<uint32_t, uint32_t> first;
+    uint32_t operator()(uint32_t col) {
+      auto it = first.find(col);
+      if (it != first.end()) return it->second;
+      if (!pr->col_buf.count(col)) throw Error(LG_ERR_INVALID, "step reads a column that is not available yet");
+      uint32_t f = (uint32_t)lanes.size();
+      for (uint32_t w = 0; w < pr->lanes_of(col); w++) lanes.push_back(pr->lane_ptr(col, w));
+      first[col] = f;
+      return f;
+    }
+  };
+  // module whose rows an expression ranges over: that of its first column
+  uint32_t expr_module(uint32_t root) {
+    std::vector<char> seen(pg.nodes.size(), 0);
+    collect(root, seen);
+    for (uint32_t i = 0; i < pg.nodes.size(); i++)
+      if (seen[i] && pg.nodes[i].op == OP_COL) return pg.columns[pg.nodes[i].a].module;
+    throw Error(LG_ERR_INVALID, "lookup table without a column");
+  }
+  XProgram upload_program(const XCode& xc, std::vector<DBufP>& keep) {
+    auto code = upload_vec(c, xc.code);
+    keep.push_back(code);
+    return XProgram{(const XInst*)code->p, (uint32_t)xc.code.size(), xc.n_regs, xc.result, xc.result_ext};
+  }
+
+  // Lookup multiplicities of width-1 tables, all steps of a round in one set
+  // of launches (k_mult_insert / k_mult_count / k_mult_write).
+  void run_multiplicities(const std::vector<const Step*>& steps, const DBufP& coins_d) {
+    std::vector<DBufP> keep;
+    std::vector<EvalJob> evals;
+    uint32_t eval_regs = 1, eval_n = 0;
+    // device values of one table: the column itself when the expression is
+    // a plain unshifted base column, else an evaluation
+    auto values = [&](uint32_t root, uint32_t& n) -> const uint32_t* {
+      const Node& x = pg.nodes[root];
+      uint32_t mod = expr_module(root);
+      n = (uint32_t)mod_n(mod);
+      if (x.op == OP_COL && x.b == 0 && pg.columns[x.a].field == 0 && col_buf.count(x.a)) return lane_ptr(x.a, 0);
+      if (ext_of[root]) throw Error(LG_ERR_INVALID, "lookup table values must be base-field");
+      LaneTable lt{this, {}, {}};
+      XCode xc = compile_expr(root, std::ref(lt));
+      auto tab = upload_vec(c, lt.lanes);
+      auto out = std::make_shared<DBuf>(n, c.stream);
+      keep.insert(keep.end(), {tab, out});
+      evals.push_back(EvalJob{upload_program(xc, keep), (const uint32_t* const*)tab->p, out->p, (int)pg.modules[mod].log_n});
+      eval_regs = std::max(eval_regs, xc.n_regs);
+      eval_n = std::max(eval_n, n);
+      return out->p;
+    };
+    std::vector<MultTab> tabs;
+    std::vector<MultVec> tv, sv;
+    uint32_t max_t = 1, max_s = 1;
+    for (const Step* st : steps) {
+      uint32_t tab = (uint32_t)tabs.size(), comb = 0;
+      for (size_t k = 0; k < st->tgt.size(); k++) {
+        uint32_t n = 0;
+        const uint32_t* v = values(st->tgt[k], n);
+        uint32_t out = st->outs[k];
+        if (pg.columns[out].field != 0 || mod_n(pg.columns[out].module) != n)
+          throw Error(LG_ERR_INVALID, "multiplicity column must be a base column of its table's module");
+        auto b = std::make_shared<DBuf>(n, c.stream);
+        col_buf[out] = b;
+        tv.push_back(MultVec{v, n, comb, tab, b->p});
+        comb += n;
+        max_t = std::max(max_t, n);
+      }
+      for (uint32_t src : st->src) {
+        uint32_t n = 0;
+        const uint32_t* v = values(src, n);
+        sv.push_back(MultVec{v, n, 0, tab, nullptr});
+        max_s = std::max(max_s, n);
+      }
+      uint32_t cap = 64;
+      while (cap < 2 * comb) cap <<= 1;
+      auto mem = std::make_shared<DBuf>((size_t)2 * cap + comb, c.stream);
+      keep.push_back(mem);
+      LG_CK(cudaMemsetAsync(mem->p, 0xff, (size_t)2 * cap * 4, c.stream));
+      LG_CK(cudaMemsetAsync(mem->p + 2 * (size_t)cap, 0, (size_t)comb * 4, c.stream));
+      tabs.push_back(MultTab{mem->p, mem->p + cap, mem->p + 2 * (size_t)cap, cap});
+    }
+    auto missing = std::make_shared<DBuf>(1, c.stream);
+    LG_CK(cudaMemsetAsync(missing->p, 0, 4, c.stream));
+    auto tabs_d = upload_vec(c, tabs), tv_d = upload_vec(c, tv), sv_d = upload_vec(c, sv);
+    c.timed("lookup_multiplicities", 0, 0, [&] {
+      if (!evals.empty()) {
+        auto ed = upload_vec(c, evals);
+        keep.push_back(ed);
+        const int T = 128;
+        size_t smem = (size_t)eval_regs * 6 * T * 4;
+        allow_smem(k_eval_base, smem);
+        k_eval_base<<<dim3((eval_n + T - 1) / T, (unsigned)evals.size()), T, smem, c.stream>>>(
+            (const EvalJob*)ed->p, (const E6*)coins_d->p);
+        LG_LAUNCH();
+      }
+      k_mult_insert<<<dim3((max_t + 255) / 256, (unsigned)tv.size()), 256, 0, c.stream>>>((const MultVec*)tv_d->p,
+                                                                                         (const MultTab*)tabs_d->p);
+      LG_LAUNCH();
+      k_mult_count<<<dim3((max_s + 255) / 256, (unsigned)sv.size()), 256, 0, c.stream>>>(
+          (const MultVec*)sv_d->p, (const MultTab*)tabs_d->p, missing->p);
+      LG_LAUNCH();
+      k_mult_write<<<dim3((max_t + 255) / 256, (unsigned)tv.size()), 256, 0, c.stream>>>((const MultVec*)tv_d->p,
+                                                                                        (const MultTab*)tabs_d->p);
+      LG_LAUNCH();
+    });
+    uint32_t* h = c.host_staging(1);
+    c.d2h(h, missing->p, 1);
+    if (*h) throw Error(LG_ERR_INVALID, "lookup: a source value is not in its table");
+  }
+
+  // Cyclic logup columns and their totals (board/logup.go:129-180): one set of
+  // launches over all logup steps of a round (batched) or one per step.
+  void run_logups(const std::vector<const Step*>& steps, const DBufP& coins_d) {
+    if (!exposed_d) exposed_d = std::make_shared<DBuf>(6 * std::max<size_t>(n_exposed(), 1), c.stream);
+    std::vector<DBufP> keep;
+    std::vector<LogupJob> jobs;
+    std::vector<ScanJob> scans;
+    std::vector<LogupFinish> fins;
+    uint32_t max_regs = 1;
+    for (const Step* st : steps) {
+      if (st->e.size() > (size_t)LOGUP_MAX_TERMS)
+        throw Error(LG_ERR_UNSUPPORTED, "logup columns of more than 4 fractions are not supported by this build");
+      if (pg.columns[st->out].field != 1 || pg.columns[st->out].module != st->module)
+        throw Error(LG_ERR_INVALID, "logup column must be an extension column of its module");
+      uint32_t logn = pg.modules[st->module].log_n;
+      size_t n = (size_t)1 << logn;
+      LaneTable lt{this, {}, {}};
+      LogupJob J{};
+      J.n_terms = (uint32_t)st->e.size();
+      for (size_t k = 0; k < st->e.size(); k++) {
+        XCode xe = compile_expr(st->e[k], std::ref(lt)), xm = compile_expr(st->m[k], std::ref(lt));
+        J.e[k] = upload_program(xe, keep);
+        J.m[k] = upload_program(xm, keep);
+        max_regs = std::max(max_regs, std::max(xe.n_regs, xm.n_regs));
+      }
+      auto tab = upload_vec(c, lt.lanes);
+      auto frac = std::make_shared<DBuf>(6 * n, c.stream);
+      uint32_t nt = (uint32_t)((n + SCAN_TILE - 1) / SCAN_TILE);
+      auto totals = std::make_shared<DBuf>(6 * (size_t)nt, c.stream), pre = std::make_shared<DBuf>(6 * (size_t)nt, c.stream);
+      auto res = std::make_shared<DBuf>(6 * n, c.stream);
+      keep.insert(keep.end(), {tab, frac, totals, pre});
+      J.lanes = (const uint32_t* const*)tab->p;
+      J.frac = frac->p;
+      J.logn = (int)logn;
+      jobs.push_back(J);
+      scans.push_back(ScanJob{frac->p, n, totals->p, pre->p, res->p, nt});
+      fins.push_back(LogupFinish{exposed_d->p + 6 * (size_t)st->exposed, inv(to_mont((uint32_t)n))});
+      col_buf[st->out] = res;
+    }
+    const int T = 128;
+    size_t smem = (size_t)max_regs * 6 * T * 4;
+    allow_smem(k_logup_frac, smem);
+    auto launch = [&](size_t first, size_t count) {
+      uint32_t max_n = 0, max_nt = 0;
+      for (size_t i = first; i < first + count; i++) {
+        max_n = std::max<uint32_t>(max_n, (uint32_t)scans[i].n);
+        max_nt = std::max(max_nt, scans[i].nt);
+      }
+      std::vector<LogupJob> jv(jobs.begin() + first, jobs.begin() + first + count);
+      std::vector<ScanJob> sv(scans.begin() + first, scans.begin() + first + count);
+      std::vector<LogupFinish> fv(fins.begin() + first, fins.begin() + first + count);
+      auto jd = upload_vec(c, jv), sd = upload_vec(c, sv), fd = upload_vec(c, fv);
+      c.timed("logup", 0, 0, [&] {
+        k_logup_frac<<<dim3((max_n + T - 1) / T, (unsigned)count), T, smem, c.stream>>>((const LogupJob*)jd->p,
+                                                                                        (const E6*)coins_d->p);
+        LG_LAUNCH();
+        k_scan_tiles<true><<<dim3(max_nt, (unsigned)count), SCAN_BLOCK, 0, c.stream>>>((const ScanJob*)sd->p);
+        LG_LAUNCH();
+        k_tile_prefix<true><<<(unsigned)((count + 63) / 64), 64, 0, c.stream>>>((const ScanJob*)sd->p, (uint32_t)count);
+        LG_LAUNCH();
+        k_logup_finish<<<dim3((max_n + 255) / 256, (unsigned)count), 256, 0, c.stream>>>((const ScanJob*)sd->p,
+                                                                                         (const LogupFinish*)fd->p);
+        LG_LAUNCH();
+      });
+    };
+    if (c.batched) launch(0, jobs.size());
+    else for (size_t i = 0; i < jobs.size(); i++) launch(i, 1);
+  }
+
+  // Exposed totals of round r's logup steps: read back (Montgomery E6).
+  void read_exposed(uint32_t r) {
+    std::vector<const Step*> lg;
+    for (const Step& st : pg.steps) if (st.round == r && st.type == STEP_LOGUP) lg.push_back(&st);
+    if (lg.empty()) return;
+    uint32_t* h = c.host_staging(6 * exposed.size());
+    c.d2h(h, exposed_d->p, 6 * exposed.size());
+    for (const Step* st : lg) {
+      for (int w = 0; w < 6; w++) exposed[st->exposed].c[w] = h[6 * st->exposed + w];
+      exposed_ready[st->exposed] = 1;
+    }
+  }
+
   void run_steps(uint32_t r) {
-    std::vector<const Step*> steps;
-    for (const Step& st : pg.steps) if (st.round == r) steps.push_back(&st);
+    std::vector<const Step*> steps, gps, mults, logups;
+    for (const Step& st : pg.steps) {
+      if (st.round != r) continue;
+      steps.push_back(&st);
+      (st.type == STEP_GP ? gps : st.type == STEP_MULT ? mults : logups).push_back(&st);
+    }
     if (steps.empty()) return;
     auto coins_d = coins_on_device();
+    // steps of one round read only earlier rounds' columns; multiplicities,
+    // grand products and logups are independent of each other
+    if (!mults.empty()) run_multiplicities(mults, coins_d);
+    if (!logups.empty()) run_logups(logups, coins_d);
+    steps = gps;
+    if (steps.empty()) return;
     std::vector<GpJob> jobs;
     std::vector<ScanJob> scans;
     std::vector<DBufP> keep;
@@ -417,7 +646,10 @@ struct Prover {
     std::map<uint32_t, std::vector<std::vector<uint32_t*>>> verifier_intt;
     for (uint32_t m : mod_order) {
       if (!chunk_count(m)) continue;
-      if (chunk_count(m) != 4) throw Error(LG_ERR_UNSUPPORTED, "quotient domains other than 4N are not supported by this build");
+      // Four cosets give all four chunks of Q; a module of lower degree commits
+      // the first chunk_count of them (the others vanish for a valid witness).
+      if (chunk_count(m) != 1 && chunk_count(m) != 2 && chunk_count(m) != 4)
+        throw Error(LG_ERR_UNSUPPORTED, "quotients of more than four chunks are not supported by this build");
       uint32_t logn = pg.modules[m].log_n;
       check_ntt_size((int)logn);
       size_t n = (size_t)1 << logn;

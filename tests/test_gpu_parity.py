@@ -159,6 +159,33 @@ def test_prove_into_caller_buffer(ctx):
     assert ctx.prove(compiled.words, mont, 8) == ref
 
 
+@pytest.mark.parametrize("batched", [True, False])
+@pytest.mark.parametrize("sizes,q", [([6, 5, 7, 4], 8), ([10, 12, 9, 11, 10], 24)])
+def test_prove_lookup_equals_oracle(ctx, sizes, q, batched):
+    """Uneven modules with a range lookup (logup into a shared 2^8 table):
+    multiplicities, cyclic logup columns, exposed totals and their binding."""
+    compiled, wit = plonk.build_mixed(sizes, seed=sum(sizes))
+    mont = [F.to_mont(w) for w in wit]
+    ctx.set_batched(batched)
+    try:
+        got = ctx.prove(compiled.words, mont, q)
+    finally:
+        ctx.set_batched(True)
+    assert got == oracle.prove(compiled.words, mont, q)
+    assert proof.decode(got).exposed
+
+
+def test_prove_lookup_value_outside_table_is_refused(ctx):
+    compiled, wit = plonk.build_mixed([6, 5], seed=4)
+    mont = [F.to_mont(w) for w in wit]
+    i = [c[0] for c in compiled.witness_columns].index("RC_1")
+    mont[i] = mont[i].copy()
+    mont[i][7] = F.to_mont(np.array([1000], dtype=np.uint32))[0]
+    with pytest.raises(LoomError) as e:
+        ctx.prove(compiled.words, mont, 4)
+    assert e.value.code == 1 and "not in its table" in str(e.value)
+
+
 def test_tuning_never_changes_proofs(ctx):
     """Launch-shape values at the ends of their ranges give the same proof
     bytes; invalid names and values are refused."""

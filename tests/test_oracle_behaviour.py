@@ -173,3 +173,50 @@ def test_broken_copy_constraint_breaks_quotient():
     sig[[1, 2]] = sig[[2, 1]]
     p = proof.decode(oracle.prove(compiled.words, [F.to_mont(w) for w in wit], 4))
     assert any(g["ext"][3][0] != (0,) * 6 for g in p.claimed_values[-1])
+
+
+# ---- logup lookups (arguments.Range into a shared 2^8 range table)
+@pytest.fixture(scope="module")
+def mixed():
+    comp, wit = plonk.build_mixed([6, 5, 7, 4], seed=21)
+    mont = [F.to_mont(w) for w in wit]
+    return comp, wit, mont, oracle.prove(comp.words, mont, 8)
+
+
+def test_lookup_proof_low_degree_and_balanced_bus(mixed):
+    """The FRI final polynomial is constant only if every constraint holds,
+    the logup ones included; the exposed totals of a lookup balance to 0
+    (the LogupBus the verifier checks, proof/public_inputs.go:55-62)."""
+    comp, wit, mont, pb = mixed
+    p = proof.decode(pb)
+    assert all(v == p.final_poly[0] for v in p.final_poly)
+    assert len(p.exposed) == 8  # one logup column per source module and one per lookup in the range module
+    tot = [0] * 6
+    for ents in p.exposed.values():
+        (idx, kind, e), = ents
+        assert idx == 0 and kind == 1
+        tot = [(a + b) % F.P for a, b in zip(tot, e)]
+    assert tot == [0] * 6
+    names = sorted(p.exposed)
+    assert names[0].startswith("plonk_0.logup_") and names[-1].startswith("range_256.logup_")
+
+
+def test_lookup_value_outside_table_is_refused(mixed):
+    comp, wit, mont, _ = mixed
+    i = [c[0] for c in comp.witness_columns].index("RC_2")
+    bad = [m.copy() for m in mont]
+    bad[i][5] = F.to_mont(np.array([256], dtype=np.uint32))[0]
+    with pytest.raises(Exception, match="not in the table"):
+        oracle.prove(comp.words, bad, 8)
+
+
+def test_lookup_proofs_bind_exposed_totals(mixed):
+    """A different witness (same range) gives different totals and a
+    different transcript."""
+    comp, wit, mont, pb = mixed
+    i = [c[0] for c in comp.witness_columns].index("RC_0")
+    other = [m.copy() for m in mont]
+    other[i] = F.to_mont((wit[i].astype(np.uint64) + 1) % 256).astype(np.uint32)
+    pb2 = oracle.prove(comp.words, other, 8)
+    assert proof.decode(pb2).exposed != proof.decode(pb).exposed
+    assert proof.decode(pb2).commitments[1:] != proof.decode(pb).commitments[1:]
