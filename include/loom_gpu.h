@@ -28,11 +28,20 @@
  *             column), param (int32 row for kind 2; negative -(i+1) counts
  *             from the last row)
  *   node    : op (0 column | 1 round coin | 2 constant | 3 add | 4 sub |
- *             5 mul), a, b — column: a = column, b = int32 shift; coin:
- *             a = round; constant: a = canonical value; add/sub/mul: a, b =
- *             earlier nodes
- *   step    : type (0 grand product), round, module, numerator node,
- *             denominator node, output column
+ *             5 mul | 6 exposed average), a, b — column: a = column,
+ *             b = int32 shift; coin: a = round; constant: a = canonical
+ *             value; add/sub/mul: a, b = earlier nodes; exposed average:
+ *             a = exposed value index (the a-th logup step), the constant
+ *             total / N of its module (expr/ast.go:223-227)
+ *   step    : type 0 grand product (board/step.go:301-327): 0, round,
+ *             module, numerator node, denominator node, output column
+ *             type 1 lookup multiplicities of width-1 tables
+ *             (board/board.go:235-249): 1, round, n_src, n_tgt,
+ *             source nodes, target nodes, output column per target
+ *             type 2 cyclic logup column (board/logup.go:80-180): 2, round,
+ *             module, output column, n_terms (<= 4 on the GPU), then
+ *             (denominator node, numerator node) per term; its total is
+ *             exposed in the proof and bound after the round's commitment
  *   round   : n_staged, staged column indices (board.Compile's order,
  *             including the sweep of unstaged columns into the last round)
  *   str     : byte length, then the bytes packed 4 per word
