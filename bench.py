@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--serve-shapes", type=int, default=8, help="distinct request shapes, replayed in turn")
     ap.add_argument("--serve-rate", type=str, default="8,16", help="Poisson arrival rates (requests/s) to sweep")
     ap.add_argument("--serve-streams", type=int, default=4)
+    ap.add_argument("--no-c4", action="store_true",
+                    help="skip the mixed-size lookup workload (40 modules, log2 rows 10-20, range lookup)")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (library defaults)")
     ap.add_argument("--retune", action="store_true", help="re-measure even if the tuning cache has this GPU")
     ap.add_argument("--streams", type=str, default="2,4,8",
@@ -373,6 +375,46 @@ def main():
             wall = e0.elapsed_time(e1)
             thr.append({"streams": S, "proofs": jobs, "ms": round(wall, 3), "proofs_per_s": round(jobs * 1e3 / wall, 3)})
 
+    # ---- batched form: 40 modules of uneven sizes (log2 rows 10-20, seeded)
+    # with plonk gates, a copy constraint and a range lookup into a shared 2^8
+    # table; batched against plain on the same inputs, byte-identical proofs
+    c4 = None
+    if not a.no_c4 and rank == 0:
+        sizes = plonk.mixed_sizes(40, 10, 20, 0xC4)
+        c4comp, c4wit = plonk.build_mixed(sizes, seed=0xC4)
+        c4dev = [torch.from_numpy(F.to_mont(w).astype(np.int64)).to(torch.int32).to(f"cuda:{device}") for w in c4wit]
+        c4ptrs = [t.data_ptr() for t in c4dev]
+        c4out = bytearray(64 << 20)
+        res4 = {}
+        for mode in ("batched", "plain"):
+            ctx.set_batched(mode == "batched")
+            for _ in range(2):
+                n4 = ctx.prove_into(c4out, c4comp.words, c4ptrs, a.queries, on_device=True)
+            ts = []
+            for _ in range(max(2, min(a.steps, 3))):
+                flush.fill_(1)
+                torch.cuda.synchronize()
+                ctx.mark(8)
+                n4 = ctx.prove_into(c4out, c4comp.words, c4ptrs, a.queries, on_device=True)
+                ctx.mark(9)
+                ts.append(ctx.elapsed_ms(8, 9))
+            res4[mode] = (statistics.mean(ts), bytes(c4out[:n4]))
+        ctx.set_batched(True)
+        p4 = proof.decode(res4["batched"][1])
+        bus = [0] * 6
+        for ents in p4.exposed.values():
+            for (_, _, e) in ents:
+                bus = [(x + y) % F.P for x, y in zip(bus, e)]
+        c4 = {"workload": "40 modules, log2 rows 10-20 (seeded), plonk gates + copy constraint + range lookup "
+                          "into a 2^8 table, Poseidon2, %d queries" % a.queries,
+              "rows": int(sum(1 << x for x in sizes)), "log2_rows": sizes,
+              "batched_ms": round(res4["batched"][0], 3), "plain_ms": round(res4["plain"][0], 3),
+              "batched_speedup_vs_plain": round(res4["plain"][0] / res4["batched"][0], 3),
+              "proofs_identical": res4["batched"][1] == res4["plain"][1],
+              "final_poly_constant": all(v == p4.final_poly[0] for v in p4.final_poly),
+              "logup_bus_balanced": bus == [0] * 6}
+        del c4dev
+
     # ---- serving: requests of mixed sizes (log2 rows 12-20, 1-8 instances) with
     # Poisson arrivals, admitted by HBM budget, overlapping on the GPU
     serve_res = None
@@ -516,6 +558,7 @@ def main():
             "host_phases_ms": {k: round(v, 3) for k, v in phases.items()},
             "step_ms": {"prove": [round(x, 3) for x in times], "e2e": [round(x, 3) for x in e2e_times],
                         "plain": [round(x, 3) for x in plain_times]},
+            "c4_mixed_lookup": c4,
             "tuning": tune,
             "kernel_ms_by_phase": {ph: {k: round(v["ms"], 3) for k, v in ks.items()} for ph, ks in by_phase.items()},
             "dominant_kernel": dom,

@@ -460,7 +460,7 @@ enum : uint8_t {
 };
 struct XInst { uint8_t op, d, a, b; uint32_t imm; int32_t shift; };
 constexpr int X_MAX_REGS = 24;
-constexpr int X_MAX_INST = 512;
+constexpr int X_MAX_INST = 16384;  // instructions are read from global memory; no fixed array
 
 struct XProgram {
   const XInst* code;

@@ -110,8 +110,37 @@ struct Prover {
   template <class LaneOf> XCode compile_expr(uint32_t root, LaneOf lane_of) {
     std::vector<char> seen(pg.nodes.size(), 0);
     collect(root, seen);
+    // Evaluation order: post-order from the root, the child that needs more
+    // registers first (Sethi-Ullman), so a long sum of relations folded by
+    // Horner keeps one accumulator live instead of every relation's value.
+    std::vector<int> need(pg.nodes.size(), 0);
+    for (uint32_t i = 0; i < pg.nodes.size(); i++) {
+      if (!seen[i]) continue;
+      const Node& x = pg.nodes[i];
+      if (!is_binary(x.op)) { need[i] = 1; continue; }
+      int na = need[x.a], nb = need[x.b];
+      need[i] = na == nb ? na + 1 : std::max(na, nb);
+    }
     std::vector<uint32_t> order;
-    for (uint32_t i = 0; i < pg.nodes.size(); i++) if (seen[i]) order.push_back(i);
+    {
+      std::vector<char> done(pg.nodes.size(), 0);
+      std::vector<std::pair<uint32_t, int>> st = {{root, 0}};
+      while (!st.empty()) {
+        auto [x, state] = st.back();
+        st.pop_back();
+        if (done[x]) continue;
+        const Node& nd = pg.nodes[x];
+        if (state == 1 || !is_binary(nd.op)) {
+          done[x] = 1;
+          order.push_back(x);
+          continue;
+        }
+        st.push_back({x, 1});
+        uint32_t first = need[nd.a] >= need[nd.b] ? nd.a : nd.b, second = first == nd.a ? nd.b : nd.a;
+        st.push_back({second, 0});
+        st.push_back({first, 0});
+      }
+    }
     std::vector<int> last(pg.nodes.size(), -1);
     for (size_t k = 0; k < order.size(); k++) {
       const Node& x = pg.nodes[order[k]];
