@@ -1,8 +1,10 @@
 """GPU parity: every CUDA entry point against the CPU oracle, through the C ABI.
 
 Integer/field work, so the bar is bit-exact equality.  Sizes are ones the
-oracle finishes in seconds; the full 40 x 2^14 workload is covered by
-size-independent properties in test_gpu_full.py.
+oracle finishes in seconds; workloads too large for the oracle (the mixed
+40-module lookup program, 2^20-row modules) are covered by size-independent
+properties: batched == plain bytes, a constant FRI final polynomial, balanced
+logup totals.
 """
 import numpy as np
 import pytest
