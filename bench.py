@@ -253,6 +253,17 @@ def sweep(a):
     ctx.close()
 
 
+def max_over_ranks(values, dist, device):
+    """Element-wise maximum of per-rank values: a job of N replicas takes as
+    long as its slowest rank.  Identity with one process."""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
 # ---------------------------------------------------------------------- GPU arm
 def main():
     a = parse()
@@ -354,6 +365,10 @@ def main():
     barrier()
     assert pbh == pb, "host-buffer and device-buffer proofs differ"
     assert pbp == pb, "plain and batched proofs differ"
+    # max over ranks now, before the sections only rank 0 runs (every rank
+    # takes the same collective steps in the same order)
+    ms, e2e_ms, plain_ms = max_over_ranks(
+        [statistics.mean(times), statistics.mean(e2e_times), statistics.mean(plain_times)], dist, f"cuda:{device}")
 
     # ---- throughput: several proofs in flight, one context + stream each
     from loom_b200.pool import ProverPool
@@ -379,7 +394,7 @@ def main():
     # with plonk gates, a copy constraint and a range lookup into a shared 2^8
     # table; batched against plain on the same inputs, byte-identical proofs
     c4 = None
-    if not a.no_c4 and rank == 0:
+    if not a.no_c4 and world == 1:
         sizes = plonk.mixed_sizes(40, 10, 20, 0xC4)
         c4comp, c4wit = plonk.build_mixed(sizes, seed=0xC4)
         c4dev = [torch.from_numpy(F.to_mont(w).astype(np.int64)).to(torch.int32).to(f"cuda:{device}") for w in c4wit]
@@ -418,7 +433,7 @@ def main():
     # ---- serving: requests of mixed sizes (log2 rows 12-20, 1-8 instances) with
     # Poisson arrivals, admitted by HBM budget, overlapping on the GPU
     serve_res = None
-    if a.serve_requests > 0 and rank == 0:
+    if a.serve_requests > 0 and world == 1:
         from loom_b200 import serve as SV
         rng = np.random.Generator(np.random.PCG64(0x5E4E))
         shapes = [(int(rng.integers(12, 21)), int(rng.integers(1, 9))) for _ in range(a.serve_shapes)]
@@ -465,14 +480,6 @@ def main():
     ctx.profile(False)
     phases = rep.pop("phases", {})
     by_phase = rep.pop("kernels_by_phase", {})
-
-    ms = statistics.mean(times)
-    e2e_ms = statistics.mean(e2e_times)
-    plain_ms = statistics.mean(plain_times)
-    if dist is not None:
-        t = torch.tensor([ms, e2e_ms, plain_ms], dtype=torch.float64, device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_ms, plain_ms = float(t[0]), float(t[1]), float(t[2])
 
     if rank == 0:
         peaks = {}
