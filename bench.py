@@ -375,9 +375,10 @@ def main():
     thr = []
     for S in [int(x) for x in a.streams.split(",") if x]:
         with ProverPool(S, device, tparams) as pool:
-            for f in [pool.submit(comp.words, dev_ptrs, a.queries, on_device=True) for _ in range(S)]:
-                f.result()  # warm every context
-            jobs = S * max(2, a.steps)
+            for _ in range(2):  # warm every context (buffers, pools, tables), twice
+                for f in [pool.submit(comp.words, dev_ptrs, a.queries, on_device=True) for _ in range(S)]:
+                    f.result()
+            jobs = S * max(4, a.steps)
             flush.fill_(1)
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
