@@ -14,6 +14,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/loom_gpu.h"
@@ -493,11 +494,25 @@ struct Writer {
     }
     off += 4 * n;
   }
-  // words already in proof encoding (big-endian canonical bytes)
+  // words already in proof encoding (big-endian canonical bytes); large
+  // blocks (the per-query sections, megabytes) are copied by four threads
   void bytes(const uint32_t* be, size_t n) {
     reserve(4 * n);
-    memcpy(p + off, be, 4 * n);
-    off += 4 * n;
+    const size_t len = 4 * n;
+    if (len < ((size_t)2 << 20)) {
+      memcpy(p + off, be, len);
+    } else {
+      const size_t parts = 4, step = (len / parts + 63) & ~(size_t)63;
+      std::vector<std::thread> th;
+      const uint8_t* src = reinterpret_cast<const uint8_t*>(be);
+      for (size_t k = 1; k < parts; k++) {
+        const size_t a = std::min(len, k * step), b = std::min(len, (k + 1) * step);
+        if (a < b) th.emplace_back([=] { memcpy(p + off + a, src + a, b - a); });
+      }
+      memcpy(p + off, src, std::min(len, step));
+      for (auto& t : th) t.join();
+    }
+    off += len;
   }
   void str(const std::string& s) {
     put((uint32_t)s.size());
