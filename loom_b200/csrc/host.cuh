@@ -270,9 +270,10 @@ struct Ctx {
 
 // ---------------------------------------------------------------- program
 // Flat descriptor; the format is documented in include/loom_gpu.h.
-enum { OP_COL = 0, OP_COIN = 1, OP_CONST = 2, OP_ADD = 3, OP_SUB = 4, OP_MUL = 5, OP_EXPAVG = 6 };
+enum { OP_COL = 0, OP_COIN = 1, OP_CONST = 2, OP_ADD = 3, OP_SUB = 4, OP_MUL = 5, OP_EXPAVG = 6, OP_EXPVAL = 7 };
 enum { KIND_WITNESS = 0, KIND_STEP = 1, KIND_LAGRANGE = 2 };
-enum { STEP_GP = 0, STEP_MULT = 1, STEP_LOGUP = 2 };
+enum { STEP_GP = 0, STEP_MULT = 1, STEP_LOGUP = 2, STEP_RATIO = 3 };
+inline bool exposes(uint32_t step_type) { return step_type == STEP_LOGUP || step_type == STEP_RATIO; }
 inline bool is_binary(uint32_t op) { return op == OP_ADD || op == OP_SUB || op == OP_MUL; }
 struct Module { uint32_t log_n; std::string name; std::vector<uint32_t> rels; };
 struct Column { std::string name; uint32_t module, field, kind; int32_t param; };
@@ -281,7 +282,7 @@ struct Step {
   uint32_t type, round, module = 0, num = 0, den = 0, out = 0;
   std::vector<uint32_t> src, tgt, outs;  // lookup multiplicities (width-1 tables)
   std::vector<uint32_t> e, m;            // cyclic logup: fractions m[k] / e[k]
-  uint32_t exposed = 0;                  // cyclic logup: index of its exposed total
+  uint32_t exposed = 0;                  // cyclic logup / running ratio: index of its exposed value
 };
 struct Program {
   uint32_t n_rounds = 0;
@@ -331,7 +332,7 @@ inline Program parse_program(const uint32_t* w, size_t n) {
   }
   for (uint32_t i = 0; i < nn; i++) {
     Node x{rd(), rd(), rd()};
-    if (x.op > OP_EXPAVG) throw Error(LG_ERR_INVALID, "bad node op");
+    if (x.op > OP_EXPVAL) throw Error(LG_ERR_INVALID, "bad node op");
     if (is_binary(x.op) && (x.a >= i || x.b >= i)) throw Error(LG_ERR_INVALID, "node children must precede parents");
     if (x.op == OP_COL && x.a >= nc) throw Error(LG_ERR_INVALID, "node column out of range");
     if (x.op == OP_COIN && x.a >= p.n_rounds) throw Error(LG_ERR_INVALID, "node coin out of range");
@@ -352,11 +353,12 @@ inline Program parse_program(const uint32_t* w, size_t n) {
     Step s;
     s.type = rd();
     s.round = rd();
-    if (s.type == STEP_GP) {
+    if (s.type == STEP_GP || s.type == STEP_RATIO) {
       s.module = rd();
       s.num = node();
       s.den = node();
       s.out = column();
+      if (s.type == STEP_RATIO) s.exposed = n_exposed++;
     } else if (s.type == STEP_MULT) {
       uint32_t a = rd(), b = rd();
       if (!a || !b || a > 4096 || b > 4096) throw Error(LG_ERR_INVALID, "bad multiplicity step");
@@ -380,7 +382,8 @@ inline Program parse_program(const uint32_t* w, size_t n) {
     p.steps.push_back(s);
   }
   for (const Node& x : p.nodes)
-    if (x.op == OP_EXPAVG && x.a >= n_exposed) throw Error(LG_ERR_INVALID, "exposed value out of range");
+    if ((x.op == OP_EXPAVG || x.op == OP_EXPVAL) && x.a >= n_exposed)
+      throw Error(LG_ERR_INVALID, "exposed value out of range");
   for (uint32_t r = 0; r < p.n_rounds; r++) {
     uint32_t k = rd();
     std::vector<uint32_t> v;

@@ -619,7 +619,16 @@ __device__ __forceinline__ void st6(uint32_t* p, uint64_t stride, uint64_t i, co
 // Product scans over E6 vectors stored as 6 lanes of n words: per-tile
 // inclusive scan in place, tile totals, their exclusive prefix, and the
 // shifted result out[0] = 1, out[i] = prod_{k<i} x[k].  One job per vector.
-struct ScanJob { uint32_t* x; uint64_t n; uint32_t* totals; uint32_t* pre; uint32_t* out; uint32_t nt; };
+struct ScanJob {
+  uint32_t* x;
+  uint64_t n;
+  uint32_t* totals;
+  uint32_t* pre;
+  uint32_t* out;
+  uint32_t nt;
+  uint32_t inclusive = 0;  // running ratio: out[i] = prod_{k<=i} x[k] ...
+  uint32_t* end = nullptr; // ... and its last value written here (6 words)
+};
 
 // The scans run over products (grand products) or sums (logup running sums).
 template <bool SUM> __device__ __forceinline__ E6 scan_id() { return SUM ? e6_zero() : e6_one(); }
@@ -680,14 +689,16 @@ __global__ void k_gp_finish(const ScanJob* jobs) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= J.n) return;
   E6 v;
-  if (i == 0) v = e6_one();
+  if (!J.inclusive && i == 0) v = e6_one();
   else {
-    uint64_t k = i - 1, tile = k / SCAN_TILE;
+    uint64_t k = J.inclusive ? i : i - 1, tile = k / SCAN_TILE;
     E6 pre;
     for (int w = 0; w < 6; w++) pre.c[w] = J.pre[tile * 6 + w];
     v = e6_mul(pre, ld6(J.x, J.n, k));
   }
   st6(J.out, J.n, i, v);
+  if (J.end && i == J.n - 1)
+    for (int w = 0; w < 6; w++) J.end[w] = v.c[w];
 }
 
 // ---------------------------------------------------------------- lookups

@@ -40,7 +40,7 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
     // (board/logup.go:218-225)
     read_exposed(r);
     for (const Step& st : pg.steps) {
-      if (st.round != r || st.type != STEP_LOGUP) continue;
+      if (st.round != r || !exposes(st.type)) continue;
       uint32_t w[7] = {0};
       for (int k = 0; k < 6; k++) w[1 + k] = exposed[st.exposed].c[k];
       fs.bind(coin_name(r), w, 7);
@@ -553,7 +553,8 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
   {  // exposed values by name: name, one entry (index 0, extension kind 1, value)
     std::vector<std::pair<std::string, size_t>> ev;
     for (const Step& st : pg.steps)
-      if (st.type == STEP_LOGUP) ev.push_back({pg.columns[st.out].name + "_total", st.exposed});
+      if (exposes(st.type))
+        ev.push_back({pg.columns[st.out].name + (st.type == STEP_LOGUP ? "_total" : "_end"), st.exposed});
     std::sort(ev.begin(), ev.end());
     W.u32((uint32_t)ev.size());
     for (auto& e : ev) {

@@ -67,6 +67,7 @@ struct Prover {
     switch (x.op) {
       case OP_COL: d = 1; break;
       case OP_EXPAVG: d = 1; break;  // a verifier column (internal/dag/dag.go:1536)
+      case OP_EXPVAL: d = 0; break;  // a constant (times L_0 it is the sparse column)
       case OP_COIN: d = 0; break;
       case OP_CONST: d = x.a % P == 0 ? NEG_INF : 0; break;
       case OP_ADD: case OP_SUB: d = std::max(node_degree(x.a, memo), node_degree(x.b, memo)); break;
@@ -80,7 +81,7 @@ struct Prover {
   bool node_ext(uint32_t id) const {
     const Node& x = pg.nodes[id];
     if (x.op == OP_COL) return pg.columns[x.a].field == 1;
-    if (x.op == OP_COIN || x.op == OP_EXPAVG) return true;
+    if (x.op == OP_COIN || x.op == OP_EXPAVG || x.op == OP_EXPVAL) return true;
     if (x.op == OP_CONST) return false;
     return false;  // combined by the caller through ext_of
   }
@@ -173,8 +174,9 @@ struct Prover {
           in.shift = (int32_t)x.b;
           break;
         case OP_COIN: in.op = X_COIN; in.imm = x.a; break;
-        // exposed averages follow the round coins in the kernels' coin table
+        // the kernels' coin table: round coins, exposed averages, exposed values
         case OP_EXPAVG: in.op = X_COIN; in.imm = pg.n_rounds + x.a; break;
+        case OP_EXPVAL: in.op = X_COIN; in.imm = pg.n_rounds + (uint32_t)n_exposed() + x.a; break;
         case OP_CONST: in.op = X_CONST; in.imm = to_mont(x.a % P); break;
         case OP_ADD:
           if (!ea && !eb) in.op = X_ADD_BB;
@@ -325,17 +327,20 @@ struct Prover {
     return (uint32_t)(big / n);
   }
 
-  // Round coins, then the exposed averages total / N (N: the size of the
-  // logup column's module), as E6 Montgomery words.
+  // Round coins, then per exposed value its average value / N (N: the size of
+  // the exposing step's module), then the exposed values themselves, as E6
+  // Montgomery words.
   DBufP coins_on_device() {
     std::vector<uint32_t> w;
     for (auto& e : coins) for (int i = 0; i < 6; i++) w.push_back(e.c[i]);
+    std::vector<E6> avg(n_exposed(), e6_zero()), val(n_exposed(), e6_zero());
     for (const Step& st : pg.steps) {
-      if (st.type != STEP_LOGUP) continue;
-      E6 avg = exposed_ready[st.exposed] ? e6_mul_base(exposed[st.exposed], inv(to_mont((uint32_t)mod_n(st.module))))
-                                         : e6_zero();
-      for (int i = 0; i < 6; i++) w.push_back(avg.c[i]);
+      if (!exposes(st.type) || !exposed_ready[st.exposed]) continue;
+      val[st.exposed] = exposed[st.exposed];
+      avg[st.exposed] = e6_mul_base(exposed[st.exposed], inv(to_mont((uint32_t)mod_n(st.module))));
     }
+    for (auto& e : avg) for (int i = 0; i < 6; i++) w.push_back(e.c[i]);
+    for (auto& e : val) for (int i = 0; i < 6; i++) w.push_back(e.c[i]);
     return upload_vec(c, w);
   }
 
@@ -345,7 +350,7 @@ struct Prover {
   // kernel for all steps of the round; plain: one set of launches per step.
   size_t n_exposed() const {
     size_t k = 0;
-    for (const Step& st : pg.steps) k += st.type == STEP_LOGUP;
+    for (const Step& st : pg.steps) k += exposes(st.type);
     return k;
   }
 
@@ -466,7 +471,6 @@ struct Prover {
   // Cyclic logup columns and their totals (board/logup.go:129-180): one set of
   // launches over all logup steps of a round (batched) or one per step.
   void run_logups(const std::vector<const Step*>& steps, const DBufP& coins_d) {
-    if (!exposed_d) exposed_d = std::make_shared<DBuf>(6 * std::max<size_t>(n_exposed(), 1), c.stream);
     std::vector<DBufP> keep;
     std::vector<LogupJob> jobs;
     std::vector<ScanJob> scans;
@@ -532,10 +536,10 @@ struct Prover {
     else for (size_t i = 0; i < jobs.size(); i++) launch(i, 1);
   }
 
-  // Exposed totals of round r's logup steps: read back (Montgomery E6).
+  // Exposed values of round r's steps: read back (Montgomery E6).
   void read_exposed(uint32_t r) {
     std::vector<const Step*> lg;
-    for (const Step& st : pg.steps) if (st.round == r && st.type == STEP_LOGUP) lg.push_back(&st);
+    for (const Step& st : pg.steps) if (st.round == r && exposes(st.type)) lg.push_back(&st);
     if (lg.empty()) return;
     uint32_t* h = c.host_staging(6 * exposed.size());
     c.d2h(h, exposed_d->p, 6 * exposed.size());
@@ -550,8 +554,9 @@ struct Prover {
     for (const Step& st : pg.steps) {
       if (st.round != r) continue;
       steps.push_back(&st);
-      (st.type == STEP_GP ? gps : st.type == STEP_MULT ? mults : logups).push_back(&st);
+      (st.type == STEP_GP || st.type == STEP_RATIO ? gps : st.type == STEP_MULT ? mults : logups).push_back(&st);
     }
+    if (!exposed_d && n_exposed()) exposed_d = std::make_shared<DBuf>(6 * n_exposed(), c.stream);
     if (steps.empty()) return;
     auto coins_d = coins_on_device();
     // steps of one round read only earlier rounds' columns; multiplicities,
@@ -589,7 +594,14 @@ struct Prover {
       jobs.push_back(GpJob{XProgram{(const XInst*)cn->p, (uint32_t)xn.code.size(), xn.n_regs, xn.result, xn.result_ext},
                            XProgram{(const XInst*)cd->p, (uint32_t)xd.code.size(), xd.n_regs, xd.result, xd.result_ext},
                            (const uint32_t* const*)tab->p, ratio->p, (int)logn});
-      scans.push_back(ScanJob{ratio->p, n, totals->p, pre->p, res->p, nt});
+      ScanJob sj{ratio->p, n, totals->p, pre->p, res->p, nt};
+      if (st->type == STEP_RATIO) {  // inclusive products; the end is exposed
+        if (pg.columns[st->out].field != 1 || pg.columns[st->out].module != st->module)
+          throw Error(LG_ERR_INVALID, "running ratio column must be an extension column of its module");
+        sj.inclusive = 1;
+        sj.end = exposed_d->p + 6 * (size_t)st->exposed;
+      }
+      scans.push_back(sj);
       col_buf[st->out] = res;
     }
     const int T = 128;

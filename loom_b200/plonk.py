@@ -107,6 +107,37 @@ def build_mixed(log_sizes: List[int], seed: int = 0x10AD, range_bound: int = 256
     return compiled, witness
 
 
+def build_with_ratio(n: int, seed: int = 5, permuted: bool = True):
+    """A plonk module next to a module with columns A and B (staged at
+    RoundFold) and the running ratio of (A - gamma) / (B - gamma) at
+    RoundRunningSums (board/product.go:72-198).  With B a permutation of A the
+    exposed end is 1.  Returns (program, witness, name of the exposed end)."""
+    from .program import ROUND_FOLD, ROUND_LOG_DERIVATIVE, ROUND_RUNNING_SUMS, coin
+    rng = np.random.Generator(np.random.PCG64([seed, 0x5252]))
+    b = Builder()
+    trace: Dict[str, np.ndarray] = {}
+    m0 = Module("plonk_0", n)
+    L, R, O = col("L_0"), col("R_0"), col("O_0")
+    QL, QR, QM, QO, QK = (col(f"{s}_0") for s in ("QL", "QR", "QM", "QO", "QK"))
+    m0.assert_zero(QL * L + QR * R + QM * L * R + QO * O + QK)
+    b.add_module(m0)
+    w, S = instance_witness(n, seed, 0)
+    trace.update(w)
+    copy_constraint(b, "plonk_0", [L, R, O], S, "plonk.S_0")
+    b.add_module(Module("ratio_0", n))
+    a = rng.integers(0, F.P, n, dtype=np.uint64).astype(np.uint32)
+    trace["A_0"] = a
+    trace["B_0"] = rng.permutation(a) if permuted else rng.integers(0, F.P, n, dtype=np.uint64).astype(np.uint32)
+    b.stage_leaves(ROUND_FOLD, col("A_0"), col("B_0"))
+    gamma = coin(ROUND_LOG_DERIVATIVE)
+    end = b.add_running_ratio_step(ROUND_RUNNING_SUMS, "ratio_0", [col("A_0") - gamma], [col("B_0") - gamma],
+                                   b.fresh_name("rr_"))
+    trace.update(b.generated)
+    comp = b.compile()
+    wit = [np.ascontiguousarray(trace[nm], dtype=np.uint32) for (nm, f, r) in comp.witness_columns]
+    return comp, wit, end
+
+
 def mixed_sizes(n_modules: int, lo: int, hi: int, seed: int) -> List[int]:
     """log2 module sizes drawn uniformly from [lo, hi] (seeded)."""
     rng = np.random.Generator(np.random.PCG64([seed, 0x5A5E]))

@@ -31,8 +31,8 @@ from . import field as F
 ROUND_FOLD, ROUND_LOG_DERIVATIVE, ROUND_RUNNING_SUMS = 0, 1, 2
 BASE, EXT = 0, 1
 KIND_WITNESS, KIND_STEP, KIND_LAGRANGE = 0, 1, 2
-OP_COL, OP_COIN, OP_CONST, OP_ADD, OP_SUB, OP_MUL, OP_EXPAVG = range(7)
-STEP_GP, STEP_MULT, STEP_LOGUP = 0, 1, 2
+OP_COL, OP_COIN, OP_CONST, OP_ADD, OP_SUB, OP_MUL, OP_EXPAVG, OP_EXPVAL = range(8)
+STEP_GP, STEP_MULT, STEP_LOGUP, STEP_RATIO = 0, 1, 2, 3
 MAGIC = 0x3150474C
 RANGE_MODULE, LOGUP = "range", "logup"  # internal/constants/const.go:34,41
 MAX_LOGUP_DEGREE, MAX_LOGUP_BATCH = 5, 4  # board/logup.go:37, arguments/lookup.go:156
@@ -68,6 +68,8 @@ class Expr:
             return ("v", self.a)
         if self.op == OP_EXPAVG:
             return ("x", self.a)
+        if self.op == OP_EXPVAL:
+            return ("e", self.a)
         return (self.op, self.a.key(), self.b.key())
 
     def degree(self) -> int:
@@ -75,7 +77,7 @@ class Expr:
         included) count 1, coins and constants 0."""
         if self.op in (OP_COL, OP_EXPAVG):
             return 1
-        if self.op in (OP_COIN, OP_CONST):
+        if self.op in (OP_COIN, OP_CONST, OP_EXPVAL):
             return 0
         if self.op == OP_MUL:
             return self.a.degree() + self.b.degree()
@@ -103,6 +105,12 @@ def exposed_average(total: str) -> Expr:
     """The constant extension column T/N of an exposed total T, N the size of
     the module using it (expr/ast.go:223-227)."""
     return Expr(OP_EXPAVG, total)
+
+
+def exposed_value(name: str) -> Expr:
+    """An exposed value as a constant; times L_0 it is the sparse verifier
+    column expr.Exposed (board/product.go:109, the end P at row 0)."""
+    return Expr(OP_EXPVAL, name)
 
 
 def fold(v: Expr, cs: Sequence[Expr]) -> Expr:
@@ -172,6 +180,17 @@ class LogupStep:
     terms: List[Tuple[Expr, Expr]]  # (E, M): fraction M / E
     out: str
     total: str
+
+
+@dataclass
+class RunningRatioStep:
+    """board/product.go:72-198: Z_i = prod_{k<=i} num_k / den_k, end P = Z_{N-1} exposed."""
+    round: int
+    module: str
+    num: Expr
+    den: Expr
+    out: str
+    end: str
 
 
 @dataclass
@@ -248,6 +267,38 @@ class Builder:
         self.modules[module].assert_zero(relation)
         return total
 
+    def add_running_ratio_step(self, r: int, module: str, num: Sequence[Expr], den: Sequence[Expr], output: str) -> str:
+        """board/product.go:72-121: Z·d·(1 - L_0 + E) - Z_{-1}·n = 0 and
+        L_0·Z_{-1} - E = 0 with E = P·L_0, P the exposed end; returns P's name."""
+        if not num and not den:
+            raise ValueError(f"running ratio {output}: no factors")
+        deg = max(1 + sum(f.degree() for f in num), 2 + sum(f.degree() for f in den))
+        if deg > MAX_LOGUP_DEGREE:
+            raise ValueError(f"running ratio {output}: constraint degree {deg} above {MAX_LOGUP_DEGREE}")
+
+        def product(fs):
+            res = None
+            for f in fs:
+                res = f if res is None else res * f
+            return res
+
+        end = output + "_end"
+        pn, pd = product(num), product(den)
+        self._grow(r)
+        self.rounds[r]["steps"].append(RunningRatioStep(r, module, pn if pn is not None else const(1),
+                                                        pd if pd is not None else const(1), output, end))
+        m = self.modules[module]
+        z, zprev = col(output), col(output, -1)
+        l0 = m.lagrange_col(0)
+        e = exposed_value(end) * l0
+        lhs = z * (const(1) - l0 + e)
+        if pd is not None:
+            lhs = lhs * pd
+        rhs = zprev if pn is None else zprev * pn
+        m.assert_zero(lhs - rhs)
+        m.assert_zero(l0 * zprev - e)
+        return end
+
     def add_grand_product_step(self, r: int, module: str, num: Expr, den: Expr, out: str):
         self._grow(r)
         self.rounds[r]["steps"].append(GrandProductStep(r, module, num, den, out))
@@ -273,7 +324,13 @@ class Builder:
             for s_ in rd["steps"]:
                 for o in (s_.outs if isinstance(s_, MultiplicityStep) else [s_.out]):
                     step_out[o] = s_
-        exposed = [s_.total for rd in self.rounds for s_ in rd["steps"] if isinstance(s_, LogupStep)]
+        exposed = []  # exposed values in step order (board/logup.go:183-191)
+        for rd in self.rounds:
+            for s_ in rd["steps"]:
+                if isinstance(s_, LogupStep):
+                    exposed.append(s_.total)
+                elif isinstance(s_, RunningRatioStep):
+                    exposed.append(s_.end)
         exposed_idx = {nm: i for i, nm in enumerate(exposed)}
         staged: List[List[str]] = []
         seen = {}
@@ -297,7 +354,7 @@ class Builder:
         def field_of(e: Expr, fields) -> int:
             if e.op == OP_COL:
                 return fields.get(e.a, BASE)
-            if e.op in (OP_COIN, OP_EXPAVG):
+            if e.op in (OP_COIN, OP_EXPAVG, OP_EXPVAL):
                 return EXT
             if e.op == OP_CONST:
                 return BASE
@@ -308,7 +365,7 @@ class Builder:
             for s_ in rd["steps"]:
                 if isinstance(s_, GrandProductStep):
                     fields[s_.out] = max(field_of(s_.num, fields), field_of(s_.den, fields))
-                elif isinstance(s_, LogupStep):
+                elif isinstance(s_, (LogupStep, RunningRatioStep)):
                     fields[s_.out] = EXT
                 else:
                     for o in s_.outs:
@@ -342,10 +399,10 @@ class Builder:
                 t = (OP_COIN, e.a, 0)
             elif e.op == OP_CONST:
                 t = (OP_CONST, e.a, 0)
-            elif e.op == OP_EXPAVG:
+            elif e.op in (OP_EXPAVG, OP_EXPVAL):
                 if e.a not in exposed_idx:
                     raise ValueError(f"exposed value {e.a} is not produced by any step")
-                t = (OP_EXPAVG, exposed_idx[e.a], 0)
+                t = (e.op, exposed_idx[e.a], 0)
             else:
                 a, b = emit(e.a), emit(e.b)
                 t = (e.op, a, b)
@@ -359,6 +416,9 @@ class Builder:
             for s_ in rd["steps"]:
                 if isinstance(s_, GrandProductStep):
                     steps.append((STEP_GP, s_.round, mod_idx[s_.module], emit(s_.num), emit(s_.den), col_idx[s_.out]))
+                elif isinstance(s_, RunningRatioStep):
+                    steps.append((STEP_RATIO, s_.round, mod_idx[s_.module], emit(s_.num), emit(s_.den),
+                                  col_idx[s_.out]))
                 elif isinstance(s_, MultiplicityStep):
                     steps.append((STEP_MULT, s_.round, len(s_.sources), len(s_.targets),
                                   *[emit(x) for x in s_.sources], *[emit(x) for x in s_.targets],

@@ -53,7 +53,7 @@ Program parse_program(const uint32_t* w, size_t n) {
   }
   for (uint32_t i = 0; i < nn; i++) {
     PNode x; x.op = rd(); x.a = rd(); x.b = rd();
-    if (x.op > OP_EXPAVG) throw std::runtime_error("program: unknown node op");
+    if (x.op > OP_EXPVAL) throw std::runtime_error("program: unknown node op");
     if (x.op >= OP_ADD && x.op <= OP_MUL && (x.a >= i || x.b >= i))
       throw std::runtime_error("program: node children must precede parents");
     if (x.op == OP_COL && x.a >= nc) throw std::runtime_error("program: node column out of range");
@@ -66,8 +66,9 @@ Program parse_program(const uint32_t* w, size_t n) {
     PStep s;
     s.type = rd();
     s.round = rd();
-    if (s.type == STEP_GP) {
+    if (s.type == STEP_GP || s.type == STEP_RATIO) {
       s.module = rd(); s.num = node(); s.den = node(); s.out = column();
+      if (s.type == STEP_RATIO) s.exposed = n_exposed++;
     } else if (s.type == STEP_MULT) {
       uint32_t a = rd(), b = rd();
       if (!a || !b || a > 4096 || b > 4096) throw std::runtime_error("program: bad multiplicity step");
@@ -87,7 +88,8 @@ Program parse_program(const uint32_t* w, size_t n) {
     p.steps.push_back(s);
   }
   for (const PNode& x : p.nodes)
-    if (x.op == OP_EXPAVG && x.a >= n_exposed) throw std::runtime_error("program: exposed value out of range");
+    if ((x.op == OP_EXPAVG || x.op == OP_EXPVAL) && x.a >= n_exposed)
+      throw std::runtime_error("program: exposed value out of range");
   for (uint32_t r = 0; r < p.n_rounds; r++) {
     uint32_t k = rd();
     std::vector<uint32_t> v;
@@ -177,6 +179,7 @@ struct Prover {
     switch (x.op) {
       case OP_COL: d = 1; break;
       case OP_EXPAVG: d = 1; break;  // a verifier column (internal/dag/dag.go:1536)
+      case OP_EXPVAL: d = 0; break;  // a constant (times L_0 it is the sparse column)
       case OP_COIN: d = 0; break;
       case OP_CONST: d = x.a == 0 ? NEG_INF : 0; break;
       case OP_ADD: case OP_SUB: d = std::max(node_degree(x.a, memo), node_degree(x.b, memo)); break;
@@ -193,7 +196,7 @@ struct Prover {
     const PNode& x = nodes[id];
     bool e = false;
     if (x.op == OP_COL) e = pg.columns[x.a].field == 1;
-    else if (x.op == OP_COIN || x.op == OP_EXPAVG) e = true;
+    else if (x.op == OP_COIN || x.op == OP_EXPAVG || x.op == OP_EXPVAL) e = true;
     else if (is_binary(x.op)) e = node_ext(x.a, memo) || node_ext(x.b, memo);
     memo[id] = e;
     return e;
@@ -222,6 +225,7 @@ struct Prover {
         case OP_COIN: v = ve(coins.at(x.a)); break;
         case OP_CONST: v = vb(x.a); break;
         case OP_EXPAVG: v = ve(e6_mul_base(exposed.at(x.a), inv((uint32_t)n))); break;
+        case OP_EXPVAL: v = ve(exposed.at(x.a)); break;
         case OP_ADD: v = vadd(scratch[x.a], scratch[x.b]); break;
         case OP_SUB: v = vsub(scratch[x.a], scratch[x.b]); break;
         default: v = vmul(scratch[x.a], scratch[x.b]); break;
@@ -494,9 +498,39 @@ struct Prover {
     exposed_names[st.exposed] = pg.columns[st.out].name + "_total";
   }
 
+  // Running ratio (board/product.go:123-198): Z_i = prod_{k<=i} num_k / den_k,
+  // end P = Z_{N-1} exposed.
+  void run_ratio(const PStep& st) {
+    size_t n = mod_n(st.module);
+    std::vector<uint32_t> order_n, order_d;
+    { std::vector<char> seen(nodes.size(), 0); collect(st.num, seen, order_n); }
+    { std::vector<char> seen(nodes.size(), 0); collect(st.den, seen, order_d); }
+    auto colval = [&](uint32_t c, size_t r) -> Val {
+      if (pg.columns[c].field == 0) return vb(base.at(c)[r]);
+      return ve(ext.at(c)[r]);
+    };
+    std::vector<Val> sc(nodes.size());
+    std::vector<E6> col(n);
+    E6 acc = e6_one();
+    for (size_t j = 0; j < n; j++) {
+      E6 a = as_e6(eval(order_n, st.num, j, n, colval, sc));
+      E6 b = as_e6(eval(order_d, st.den, j, n, colval, sc));
+      if (e6_is_zero(b)) throw std::runtime_error("running ratio: zero denominator");
+      acc = e6_mul(acc, e6_mul(a, e6_inv(b)));
+      col[j] = acc;
+    }
+    if (pg.columns[st.out].module != st.module || pg.columns[st.out].field != 1)
+      throw std::runtime_error("running ratio column must be an extension column of its module");
+    ext[st.out] = col;
+    if (exposed.size() <= st.exposed) { exposed.resize(st.exposed + 1); exposed_names.resize(st.exposed + 1); }
+    exposed[st.exposed] = col[n - 1];
+    exposed_names[st.exposed] = pg.columns[st.out].name + "_end";
+  }
+
   void run_step(const PStep& st) {
     if (st.type == STEP_MULT) return run_multiplicities(st);
     if (st.type == STEP_LOGUP) return run_logup(st);
+    if (st.type == STEP_RATIO) return run_ratio(st);
     if (st.type != STEP_GP) throw std::runtime_error("unsupported step type");
     size_t n = mod_n(st.module);
     std::vector<uint32_t> order_n, order_d;
@@ -679,7 +713,7 @@ struct Prover {
       // BindExposedValues (prover/prover.go:386-396): in step order, entry
       // index then the value as six elements (board/logup.go:218-225)
       for (const PStep& st : pg.steps) {
-        if (st.round != r || st.type != STEP_LOGUP) continue;
+        if (st.round != r || (st.type != STEP_LOGUP && st.type != STEP_RATIO)) continue;
         uint32_t w[7] = {0};
         for (int k = 0; k < 6; k++) w[1 + k] = exposed[st.exposed].c[k];
         fs.bind(coin_name(r), w, 7);

@@ -16,13 +16,17 @@
 //             a, b.  col: a = column, b = shift (int32); coin: a = round;
 //             const: a = canonical value; add/sub/mul: a, b = child nodes
 //             (children precede parents); exposed average: a = exposed value
-//             (the a-th logup step's total), value total / N of the module
-//             evaluating it (expr/ast.go:223-227)
+//             (the a-th exposing step's value), value total / N of the
+//             module evaluating it (expr/ast.go:223-227); 7 exposed value:
+//             a = exposed value index, the value itself (a constant)
 //   step    : type 0 grand product: 0, round, module, num_node, den_node, out_col
 //             type 1 lookup multiplicities (width-1 tables): 1, round, n_src,
 //               n_tgt, src_node[n_src], tgt_node[n_tgt], out_col[n_tgt]
 //             type 2 cyclic logup: 2, round, module, out_col, n_terms,
 //               (E_node, M_node)[n_terms]; its total is exposed
+//             type 3 running ratio: 3, round, module, num_node, den_node,
+//               out_col; its end is exposed (board/product.go:72-198)
+//             Exposed values are numbered in step order over types 2 and 3.
 //   round   : n_staged, col[n_staged]
 //   str     : byte length, then the bytes packed 4 per word
 #pragma once
@@ -32,8 +36,8 @@
 
 namespace orc {
 
-enum { OP_COL = 0, OP_COIN = 1, OP_CONST = 2, OP_ADD = 3, OP_SUB = 4, OP_MUL = 5, OP_EXPAVG = 6 };
-enum { STEP_GP = 0, STEP_MULT = 1, STEP_LOGUP = 2 };
+enum { OP_COL = 0, OP_COIN = 1, OP_CONST = 2, OP_ADD = 3, OP_SUB = 4, OP_MUL = 5, OP_EXPAVG = 6, OP_EXPVAL = 7 };
+enum { STEP_GP = 0, STEP_MULT = 1, STEP_LOGUP = 2, STEP_RATIO = 3 };
 enum { KIND_WITNESS = 0, KIND_STEP = 1, KIND_LAGRANGE = 2 };
 
 struct PModule { uint32_t log_n; std::string name; std::vector<uint32_t> rels; };

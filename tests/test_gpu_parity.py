@@ -202,6 +202,17 @@ def test_mixed_lookup_full_size_properties(ctx):
     assert bus == [0] * 6 and len(p.exposed) == 80
 
 
+@pytest.mark.parametrize("permuted", [True, False])
+@pytest.mark.parametrize("logn", [6, 12])
+def test_prove_running_ratio_equals_oracle(ctx, logn, permuted):
+    compiled, wit, end = plonk.build_with_ratio(1 << logn, seed=logn, permuted=permuted)
+    mont = [F.to_mont(w) for w in wit]
+    got = ctx.prove(compiled.words, mont, 12)
+    assert got == oracle.prove(compiled.words, mont, 12)
+    (idx, kind, e), = proof.decode(got).exposed[end]
+    assert (tuple(e) == (1, 0, 0, 0, 0, 0)) == permuted
+
+
 def test_prove_lookup_value_outside_table_is_refused(ctx):
     compiled, wit = plonk.build_mixed([6, 5], seed=4)
     mont = [F.to_mont(w) for w in wit]

@@ -220,3 +220,15 @@ def test_lookup_proofs_bind_exposed_totals(mixed):
     pb2 = oracle.prove(comp.words, other, 8)
     assert proof.decode(pb2).exposed != proof.decode(pb).exposed
     assert proof.decode(pb2).commitments[1:] != proof.decode(pb).commitments[1:]
+
+
+# ---- running ratio (board/product.go:72-198)
+@pytest.mark.parametrize("permuted", [True, False])
+def test_running_ratio_proof(permuted):
+    comp, wit, end = plonk.build_with_ratio(64, seed=5, permuted=permuted)
+    mont = [F.to_mont(w) for w in wit]
+    p = proof.decode(oracle.prove(comp.words, mont, 8))
+    assert all(v == p.final_poly[0] for v in p.final_poly)
+    (idx, kind, e), = p.exposed[end]
+    assert idx == 0 and kind == 1
+    assert (tuple(e) == (1, 0, 0, 0, 0, 0)) == permuted
