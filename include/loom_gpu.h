@@ -28,11 +28,13 @@
  *             column), param (int32 row for kind 2; negative -(i+1) counts
  *             from the last row)
  *   node    : op (0 column | 1 round coin | 2 constant | 3 add | 4 sub |
- *             5 mul | 6 exposed average), a, b — column: a = column,
- *             b = int32 shift; coin: a = round; constant: a = canonical
- *             value; add/sub/mul: a, b = earlier nodes; exposed average:
- *             a = exposed value index (the a-th logup step), the constant
- *             total / N of its module (expr/ast.go:223-227)
+ *             5 mul | 6 exposed average | 7 exposed value), a, b — column:
+ *             a = column, b = int32 shift; coin: a = round; constant: a =
+ *             canonical value; add/sub/mul: a, b = earlier nodes; exposed
+ *             average: a = exposed value index, the constant value / N of
+ *             the exposing step's module (expr/ast.go:223-227); exposed
+ *             value: a = exposed value index, the value as a constant
+ *             (times L_0 it is expr.Exposed, board/product.go:109)
  *   step    : type 0 grand product (board/step.go:301-327): 0, round,
  *             module, numerator node, denominator node, output column
  *             type 1 lookup multiplicities of width-1 tables
@@ -42,6 +44,10 @@
  *             module, output column, n_terms (<= 4 on the GPU), then
  *             (denominator node, numerator node) per term; its total is
  *             exposed in the proof and bound after the round's commitment
+ *             type 3 running ratio (board/product.go:72-198): 3, round,
+ *             module, numerator node, denominator node, output column; its
+ *             end is exposed.  Exposed values are numbered in step order
+ *             over types 2 and 3.
  *   round   : n_staged, staged column indices (board.Compile's order,
  *             including the sweep of unstaged columns into the last round)
  *   str     : byte length, then the bytes packed 4 per word
