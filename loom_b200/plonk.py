@@ -132,6 +132,7 @@ def build_with_ratio(n: int, seed: int = 5, permuted: bool = True):
     gamma = coin(ROUND_LOG_DERIVATIVE)
     end = b.add_running_ratio_step(ROUND_RUNNING_SUMS, "ratio_0", [col("A_0") - gamma], [col("B_0") - gamma],
                                    b.fresh_name("rr_"))
+    b.product_buses.append([end])  # B is claimed to be a permutation of A: the end is one
     trace.update(b.generated)
     comp = b.compile()
     wit = [np.ascontiguousarray(trace[nm], dtype=np.uint32) for (nm, f, r) in comp.witness_columns]

@@ -199,6 +199,8 @@ class Compiled:
     witness_columns: List[Tuple[str, int, int]]  # (name, field, rows), in descriptor order
     modules: Dict[str, int]        # name -> N
     n_rounds: int
+    logup_buses: List[List[str]] = dfield(default_factory=list)    # totals that sum to zero
+    product_buses: List[List[str]] = dfield(default_factory=list)  # running-ratio ends whose product is one
 
 
 class Builder:
@@ -207,6 +209,8 @@ class Builder:
         self.rounds: List[dict] = []
         self.names = 0
         self.generated: Dict[str, np.ndarray] = {}  # generated base columns (ID support, permutation)
+        self.logup_buses: List[List[str]] = []    # board.LogupBus (board/board.go:35-38)
+        self.product_buses: List[List[str]] = []  # board.ProductBus (board/board.go:28-29)
 
     def add_module(self, m: Module):
         self.modules[m.name] = m
@@ -457,7 +461,8 @@ class Builder:
             w.append(len(lst))
             w.extend(col_idx[nm] for nm in lst)
         witness = [(nm, fld, self.modules[mod_names[mi]].n) for (nm, mi, fld, kind, _) in columns if kind == KIND_WITNESS]
-        return Compiled(np.array(w, dtype=np.uint32), witness, {n: self.modules[n].n for n in mod_names}, n_rounds)
+        return Compiled(np.array(w, dtype=np.uint32), witness, {n: self.modules[n].n for n in mod_names}, n_rounds,
+                        [list(x) for x in self.logup_buses], [list(x) for x in self.product_buses])
 
 
 # ---------------------------------------------------------------------- arguments
@@ -519,7 +524,9 @@ def lookup(b: "Builder", S: Sequence[Tuple[Expr, str]], T: Sequence[Tuple[Expr, 
     minus_one = const(F.P - 1)
     terms = [(mod, e - gamma, const(1)) for e, mod in S]
     terms += [(mod, e - gamma, minus_one * col(outs[i])) for i, (e, mod) in enumerate(T)]
-    return add_logup_columns(b, f"{LOGUP}_", terms)
+    totals = add_logup_columns(b, f"{LOGUP}_", terms)
+    b.logup_buses.append(list(totals))  # arguments/lookup.go:177
+    return totals
 
 
 def add_logup_columns(b: "Builder", prefix: str, terms: Sequence[Tuple[str, Expr, Expr]]) -> List[str]:

@@ -35,6 +35,8 @@ def lib():
         L.oracle_last_error.restype = ctypes.c_char_p
         L.oracle_prove.argtypes = [u32p, ctypes.c_size_t, ctypes.POINTER(u32p), ctypes.c_uint32,
                                    ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_size_t)]
+        L.oracle_verify.argtypes = [u32p, ctypes.c_size_t, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_uint32,
+                                    ctypes.c_char_p]
         L.oracle_p2_permute.argtypes = [u32p, ctypes.c_int]
         L.oracle_p2_round_keys.argtypes = [ctypes.c_int, u32p]
         L.oracle_p2_diag.argtypes = [ctypes.c_int, u32p]
@@ -58,6 +60,23 @@ def _p(a: np.ndarray):
 
 def _u32(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+class VerifyError(Exception):
+    """The oracle's verifier rejected a proof."""
+
+
+def verify(program_words: np.ndarray, proof: bytes, num_queries: int, logup_buses: Sequence[Sequence[str]] = (),
+           product_buses: Sequence[Sequence[str]] = ()) -> None:
+    """Checks proof bytes against the program the way loom's verifier does
+    (transcript replay, buses, AIR relation at zeta, FRI, Merkle openings,
+    DEEP bridge); raises VerifyError with the reason when it rejects."""
+    L = lib()
+    prog = _u32(program_words)
+    spec = ";".join(["P:" + ",".join(b) for b in product_buses] + ["L:" + ",".join(b) for b in logup_buses])
+    rc = L.oracle_verify(_p(prog), prog.size, bytes(proof), len(proof), num_queries, spec.encode())
+    if rc != 0:
+        raise VerifyError(L.oracle_last_error().decode(errors="replace"))
 
 
 def prove(program_words: np.ndarray, witness_mont: Sequence[np.ndarray], num_queries: int) -> bytes:

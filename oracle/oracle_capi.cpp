@@ -16,6 +16,7 @@
 
 namespace orc {
 std::vector<uint8_t> oracle_prove_bytes(const Program& pg, const uint32_t* const* witness, uint32_t num_queries);
+void oracle_verify_bytes(const Program& pg, const uint8_t* proof, size_t len, uint32_t num_queries, const std::string& buses);
 }
 using namespace orc;
 
@@ -35,6 +36,22 @@ int oracle_prove(const uint32_t* program, size_t nwords, const uint32_t* const* 
     if (*out_len < b.size()) { *out_len = b.size(); return 1; }
     memcpy(out, b.data(), b.size());
     *out_len = b.size();
+    return 0;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return 2;
+  }
+}
+
+// Verifies proof bytes against the program (verifier/verifier.go:487-533).
+// `buses` (may be NULL) lists the program's product and logup buses as
+// "P:end,end;L:total,total,...".  Returns 0 when the proof is accepted, 2
+// when it is rejected or malformed (the reason in oracle_last_error()).
+int oracle_verify(const uint32_t* program, size_t nwords, const uint8_t* proof, size_t len, uint32_t num_queries,
+                  const char* buses) {
+  try {
+    Program pg = parse_program(program, nwords);
+    oracle_verify_bytes(pg, proof, len, num_queries, buses ? buses : "");
     return 0;
   } catch (std::exception& e) {
     g_err = e.what();

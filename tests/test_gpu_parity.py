@@ -200,6 +200,7 @@ def test_mixed_lookup_full_size_properties(ctx):
         for (_, _, e) in ents:
             bus = [(x + y) % F.P for x, y in zip(bus, e)]
     assert bus == [0] * 6 and len(p.exposed) == 80
+    oracle.verify(compiled.words, a, 32, compiled.logup_buses)
 
 
 @pytest.mark.parametrize("permuted", [True, False])
@@ -211,6 +212,11 @@ def test_prove_running_ratio_equals_oracle(ctx, logn, permuted):
     assert got == oracle.prove(compiled.words, mont, 12)
     (idx, kind, e), = proof.decode(got).exposed[end]
     assert (tuple(e) == (1, 0, 0, 0, 0, 0)) == permuted
+    if permuted:
+        oracle.verify(compiled.words, got, 12, product_buses=compiled.product_buses)
+    else:
+        with pytest.raises(oracle.VerifyError, match="do not multiply to one"):
+            oracle.verify(compiled.words, got, 12, product_buses=compiled.product_buses)
 
 
 def test_prove_lookup_value_outside_table_is_refused(ctx):
@@ -313,6 +319,23 @@ def test_prove_large_module(ctx):
     mont = [F.to_mont(trace[name]) for (name, _, _) in compiled.witness_columns]
     got = ctx.prove(compiled.words, mont, 4)
     assert got == oracle.prove(compiled.words, mont, 4)
+    oracle.verify(compiled.words, got, 4)
+
+
+def test_verifier_accepts_gpu_proofs_and_rejects_false_ones(ctx):
+    """GPU proofs too large for the oracle prover at these query counts go
+    through the oracle's verifier; a GPU proof of a violated gate does not
+    verify."""
+    compiled, wit = plonk.build(8, 1 << 13, seed=0x5EED)
+    mont = [F.to_mont(w) for w in wit]
+    got = ctx.prove(compiled.words, mont, 200)
+    oracle.verify(compiled.words, got, 200)
+    names = [n for (n, _, _) in compiled.witness_columns]
+    bad = [m.copy() for m in mont]
+    i = names.index("O_5")
+    bad[i][100] = F.to_mont(np.array([(int(F.from_mont(bad[i][100:101])[0]) + 1) % F.P], dtype=np.uint32))[0]
+    with pytest.raises(oracle.VerifyError, match="AIR relation"):
+        oracle.verify(compiled.words, ctx.prove(compiled.words, bad, 200), 200)
 
 
 @pytest.mark.parametrize("cols,logr", [(1, 3), (5, 10), (37, 12)])

@@ -1,0 +1,106 @@
+"""The oracle's verifier (a restatement of verifier/verifier.go and
+internal/fri/verify.go) on oracle proofs: valid proofs are accepted, proofs
+of false statements and tampered proofs are rejected.  The GPU proofs go
+through the same verifier in the `gpu` tests."""
+import numpy as np
+import pytest
+
+import oracle
+from loom_b200 import field as F, plonk
+
+
+def _prove(compiled, wit, q):
+    return oracle.prove(compiled.words, [F.to_mont(w) for w in wit], q)
+
+
+@pytest.fixture(scope="module")
+def small():
+    compiled, wit = plonk.build(2, 1 << 8, seed=11)
+    return compiled, wit, _prove(compiled, wit, 12)
+
+
+@pytest.fixture(scope="module")
+def mixed():
+    compiled, wit = plonk.build_mixed([6, 5, 7, 4], seed=21)
+    return compiled, wit, _prove(compiled, wit, 8)
+
+
+def test_accepts_plonk_proof(small):
+    compiled, _, pb = small
+    oracle.verify(compiled.words, pb, 12)
+
+
+def test_accepts_lookup_proof_with_its_buses(mixed):
+    compiled, _, pb = mixed
+    assert len(compiled.logup_buses) == 4 and all(len(b) == 2 for b in compiled.logup_buses)
+    oracle.verify(compiled.words, pb, 8, compiled.logup_buses)
+
+
+def test_unbalanced_logup_bus_is_rejected(mixed):
+    """Totals of two different lookups do not cancel each other."""
+    compiled, _, pb = mixed
+    bus = [compiled.logup_buses[0][0], compiled.logup_buses[1][1]]
+    with pytest.raises(oracle.VerifyError, match="do not sum to zero"):
+        oracle.verify(compiled.words, pb, 8, [bus])
+
+
+@pytest.mark.parametrize("permuted", [True, False])
+def test_running_ratio_product_bus(permuted):
+    compiled, wit, end = plonk.build_with_ratio(64, seed=5, permuted=permuted)
+    assert compiled.product_buses == [[end]]
+    pb = _prove(compiled, wit, 8)
+    oracle.verify(compiled.words, pb, 8)  # the constraints hold either way
+    if permuted:
+        oracle.verify(compiled.words, pb, 8, product_buses=compiled.product_buses)
+    else:
+        with pytest.raises(oracle.VerifyError, match="do not multiply to one"):
+            oracle.verify(compiled.words, pb, 8, product_buses=compiled.product_buses)
+
+
+def test_false_gate_is_rejected(small):
+    compiled, wit, _ = small
+    names = [n for (n, _, _) in compiled.witness_columns]
+    bad = [w.copy() for w in wit]
+    bad[names.index("O_0")][3] = (int(bad[names.index("O_0")][3]) + 1) % F.P
+    with pytest.raises(oracle.VerifyError, match="AIR relation"):
+        oracle.verify(compiled.words, _prove(compiled, bad, 12), 12)
+
+
+def test_broken_copy_constraint_is_rejected():
+    compiled, wit = plonk.build(1, 1 << 6, seed=13)
+    names = [n for (n, _, _) in compiled.witness_columns]
+    wit = [w.copy() for w in wit]
+    sig = wit[names.index("plonk.S_0_0")]
+    sig[[1, 2]] = sig[[2, 1]]
+    with pytest.raises(oracle.VerifyError, match="AIR relation"):
+        oracle.verify(compiled.words, _prove(compiled, wit, 4), 4)
+
+
+@pytest.mark.parametrize("case,flips", [("small", 500), ("mixed", 250)])
+def test_every_single_bit_flip_is_rejected(small, mixed, case, flips):
+    """Random single-bit flips anywhere in the proof (values, digests, paths,
+    rows, counts, names) never verify."""
+    compiled, _, pb = small if case == "small" else mixed
+    q = 12 if case == "small" else 8
+    rng = np.random.default_rng(7)
+    accepted = []
+    for _ in range(flips):
+        i, bit = int(rng.integers(0, len(pb))), int(rng.integers(0, 8))
+        b = bytearray(pb)
+        b[i] ^= 1 << bit
+        try:
+            oracle.verify(compiled.words, bytes(b), q, compiled.logup_buses)
+            accepted.append((i, bit))
+        except oracle.VerifyError:
+            pass
+    assert accepted == []
+
+
+def test_wrong_query_count_or_program_is_rejected(small, mixed):
+    compiled, _, pb = small
+    with pytest.raises(oracle.VerifyError):
+        oracle.verify(compiled.words, pb, 11)
+    with pytest.raises(oracle.VerifyError):
+        oracle.verify(mixed[0].words, pb, 12)
+    with pytest.raises(oracle.VerifyError, match="truncated"):
+        oracle.verify(compiled.words, pb[:-4], 12)
