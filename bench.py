@@ -195,6 +195,7 @@ def sweep(a):
         ctx.profile(False)
         rep.pop("phases", None)
         rep.pop("kernels_by_phase", None)
+        rep.pop("timeline", None)
         return rep
 
     def emit(kind, kernel, rep, **kw):
@@ -265,6 +266,26 @@ def max_over_ranks(values, dist, device):
 
 
 # ---------------------------------------------------------------------- GPU arm
+def device_idle(timeline, phase_names):
+    """Gaps between the recorded launches of one prove on its stream (device
+    time with no recorded kernel running), total and per prove phase (a gap
+    counts in the phase of the launch that ends it).  Small unrecorded
+    kernels and copies fall inside gaps."""
+    spans = sorted((t0, t0 + ms, ph) for (_, ph, t0, ms) in timeline)
+    if not spans:
+        return None
+    by, end, total = {}, spans[0][1], 0.0
+    for t0, t1, ph in spans[1:]:
+        if t0 > end:
+            gap = t0 - end
+            total += gap
+            name = phase_names[ph] if ph < len(phase_names) else "after last phase"
+            by[name] = by.get(name, 0.0) + gap
+        end = max(end, t1)
+    return {"total": round(total, 3), "span": round(end - spans[0][0], 3),
+            "by_phase": {k: round(v, 3) for k, v in by.items()}}
+
+
 def main():
     a = parse()
     if a.sweep:
@@ -481,6 +502,7 @@ def main():
     ctx.profile(False)
     phases = rep.pop("phases", {})
     by_phase = rep.pop("kernels_by_phase", {})
+    idle = device_idle(rep.pop("timeline", []), list(phases))
 
     if rank == 0:
         peaks = {}
@@ -569,6 +591,7 @@ def main():
             "c4_mixed_lookup": c4,
             "tuning": tune,
             "kernel_ms_by_phase": {ph: {k: round(v["ms"], 3) for k, v in ks.items()} for ph, ks in by_phase.items()},
+            "device_idle_ms": idle,
             "dominant_kernel": dom,
             "cpu_baseline": base,
             "clocks": clk,

@@ -202,7 +202,10 @@ uint64_t lg_kernel_launches(void);
 /* Per-kernel event profiler: enable (1) clears and starts recording events
  * around the main kernels; lg_profile_report writes a JSON object
  * {kernel: {launches, ms, bytes, perms}} with algorithmic bytes and Poseidon2
- * permutations per kernel. */
+ * permutations per kernel, plus "phases" (host milliseconds per prove
+ * phase), "kernels_by_phase" and "timeline": one [kernel, phase index,
+ * start ms, duration ms] per recorded launch, starts relative to the first
+ * recorded launch, so gaps between launches show where the device waited. */
 int lg_profile(lg_ctx* ctx, int enable);
 int lg_profile_report(lg_ctx* ctx, char* buf, size_t* len);
 

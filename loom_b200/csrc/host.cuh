@@ -10,6 +10,7 @@
 #include <chrono>
 #include <cstdio>
 #include <cstring>
+#include <list>
 #include <map>
 #include <memory>
 #include <stdexcept>
@@ -139,6 +140,8 @@ inline DBufP dbuf_slice(const DBufP& backing, size_t off, size_t words) {
   return DBufP(h, &h->v);
 }
 
+struct ProgCache;  // compiled bytecode of one program (prover.cuh)
+
 struct Ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -146,6 +149,12 @@ struct Ctx {
   std::map<int, DBufP> tw;       // log n -> w_n^j, j < n
   std::map<int, DBufP> gpow;     // log n -> g^k, k < n
   std::map<int, DBufP> ginvpow;  // log n -> g^-k, k < n
+  // Program-constant device data kept across proves: Lagrange columns
+  // (log n, row) -> values and coefficients, and the compiled bytecode of the
+  // most recently proven programs (most recent first).
+  std::map<std::pair<uint32_t, uint32_t>, DBufP> lagrange_vals, lagrange_coef;
+  std::list<std::shared_ptr<ProgCache>> programs;
+  static constexpr size_t MAX_PROGRAMS = 8;
   std::string err;
   uint32_t* pinned = nullptr;    // host staging
   size_t pinned_words = 0;

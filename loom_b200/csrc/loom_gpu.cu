@@ -93,9 +93,13 @@ void lg_ctx_destroy(lg_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->c.device);
   if (ctx->c.stream) cudaStreamSynchronize(ctx->c.stream);
+  // every cached device buffer frees on the stream: release them while it exists
   ctx->c.tw.clear();
   ctx->c.gpow.clear();
   ctx->c.ginvpow.clear();
+  ctx->c.lagrange_vals.clear();
+  ctx->c.lagrange_coef.clear();
+  ctx->c.programs.clear();
   if (ctx->c.stream) {
     cudaStreamSynchronize(ctx->c.stream);
     ctx->c.dev_arena.release(ctx->c.stream);
@@ -479,7 +483,19 @@ int lg_profile_report(lg_ctx* ctx, char* buf, size_t* len) {
       }
       js += "}";
     }
-    js += "}}";
+    // launch timeline on the context's stream: kernel, phase index, start
+    // (ms after the first recorded launch began) and duration
+    js += "}, \"timeline\": [";
+    for (size_t i = 0; i < ctx->c.recs.size(); i++) {
+      const auto& r = ctx->c.recs[i];
+      float t0 = 0, ms = 0;
+      LG_CK(cudaEventElapsedTime(&t0, ctx->c.recs[0].a, r.a));
+      LG_CK(cudaEventElapsedTime(&ms, r.a, r.b));
+      char tmp[192];
+      snprintf(tmp, sizeof tmp, "%s[\"%s\", %llu, %.4f, %.4f]", i ? ", " : "", r.name, (unsigned long long)r.phase, t0, ms);
+      js += tmp;
+    }
+    js += "]}";
     if (!buf || *len < js.size() + 1) {
       *len = js.size() + 1;
       throw Error(LG_ERR_BUFFER, "report buffer too small");

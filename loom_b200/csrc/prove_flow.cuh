@@ -169,7 +169,8 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
   }
   size_t deep_off = 0;
   std::vector<DeepJob> djobs;
-  std::vector<DBufP> dkeep;
+  std::vector<DeepBundle> all_bundles;  // every class's bundles, one upload
+  std::vector<size_t> bundle_off;
   std::vector<double> dbytes;
   for (size_t ci = 0; ci < classes.size(); ci++) {
     uint32_t m = classes[ci];
@@ -211,9 +212,8 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
       }
     for (size_t k = 0; k < pts.size(); k++) jb.z[k] = pts[k];
     jb.n_points = (uint32_t)pts.size();
-    auto bd = upload_vec(c, bundles);
-    dkeep.push_back(bd);
-    jb.bundles = (const DeepBundle*)bd->p;
+    bundle_off.push_back(all_bundles.size());
+    all_bundles.insert(all_bundles.end(), bundles.begin(), bundles.end());
     jb.n_bundles = (uint32_t)bundles.size();
     jb.logn4 = (int)logn + RATE_LOG;
     jb.tw = c.twiddles(jb.logn4);
@@ -225,6 +225,8 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
     for (auto& bu : bundles) row_bytes += bu.ext ? 24.0 : 4.0;
     dbytes.push_back(row_bytes * big);
   }
+  auto bundles_d = upload_vec(c, all_bundles);
+  for (size_t i = 0; i < djobs.size(); i++) djobs[i].bundles = (const DeepBundle*)bundles_d->p + bundle_off[i];
   auto launch_deep = [&](size_t first, size_t count) {
     std::vector<DeepJob> v(djobs.begin() + first, djobs.begin() + first + count);
     uint32_t max_big = 0;

@@ -17,6 +17,25 @@ inline std::string coin_name(uint32_t r) { return "challenge@loom_" + std::to_st
 
 struct ProveStats { double ms_total = 0; };
 
+// Register bytecode of one expression (compile_expr).
+struct XCode { std::vector<XInst> code; uint32_t n_regs = 0, result = 0, result_ext = 0; };
+
+// The bytecode of one compile site (a step's expressions, a module's folded
+// relation) depends only on the program and on the order in which the site's
+// columns first reach its lane table.  A later prove of the same program
+// feeds the recorded columns to a fresh table in that order, which rebuilds
+// the same lane indices, and reuses the code and its device copy.
+struct CodeSet {
+  std::vector<XCode> xc;
+  std::vector<XProgram> dev;   // device copies, in xc order
+  std::vector<uint32_t> cols;  // columns in first-use order
+  DBufP code;                  // every xc back to back (kept across proves)
+};
+struct ProgCache {
+  std::vector<uint32_t> words;  // the program descriptor, compared in full
+  std::map<std::string, std::shared_ptr<CodeSet>> sites;
+};
+
 struct Prover {
   Ctx& c;
   Program pg;
@@ -46,11 +65,57 @@ struct Prover {
   std::map<uint32_t, DBufP> chunk_coef;  // module -> chunks (d * lanes + w) * n
   E6 zeta;
 
+  ProgCache* prog = nullptr;  // compiled code of this program, kept on the context
+
   Prover(Ctx& ctx, const uint32_t* words, size_t nwords, uint32_t q) : c(ctx), num_queries(q) {
     pg = parse_program(words, nwords);
     if (q == 0) throw Error(LG_ERR_INVALID, "num_queries must be positive");
     if (q > 65535) throw Error(LG_ERR_UNSUPPORTED, "num_queries above 65535 is not supported by this build");
+    auto& L = c.programs;
+    auto it = std::find_if(L.begin(), L.end(), [&](const std::shared_ptr<ProgCache>& e) {
+      return e->words.size() == nwords && std::equal(e->words.begin(), e->words.end(), words);
+    });
+    if (it != L.end()) {
+      L.splice(L.begin(), L, it);
+    } else {
+      auto e = std::make_shared<ProgCache>();
+      e->words.assign(words, words + nwords);
+      L.push_front(e);
+      while (L.size() > Ctx::MAX_PROGRAMS) L.pop_back();
+    }
+    prog = L.front().get();
   }
+
+  // The bytecode of `roots` compiled in order against one lane table
+  // (lane_of), from the program's cache when this site was compiled before.
+  template <class LaneOf> const CodeSet& compiled(const std::string& site, LaneOf& lane_of, const std::vector<uint32_t>& roots) {
+    auto it = prog->sites.find(site);
+    if (it != prog->sites.end()) {
+      for (uint32_t col : it->second->cols) lane_of(col);
+      return *it->second;
+    }
+    auto cs = std::make_shared<CodeSet>();
+    std::vector<char> seen(pg.columns.size(), 0);
+    auto rec = [&](uint32_t col) -> uint32_t {
+      if (!seen[col]) { seen[col] = 1; cs->cols.push_back(col); }
+      return lane_of(col);
+    };
+    for (uint32_t r : roots) cs->xc.push_back(compile_expr(r, rec));
+    std::vector<XInst> all;
+    std::vector<size_t> off;
+    for (auto& x : cs->xc) { off.push_back(all.size()); all.insert(all.end(), x.code.begin(), x.code.end()); }
+    {
+      ArenaScope kept(nullptr);  // outlives this prove
+      cs->code = upload_vec(c, all);
+    }
+    for (size_t i = 0; i < cs->xc.size(); i++) {
+      const XCode& x = cs->xc[i];
+      cs->dev.push_back(XProgram{(const XInst*)cs->code->p + off[i], (uint32_t)x.code.size(), x.n_regs, x.result, x.result_ext});
+    }
+    prog->sites[site] = cs;
+    return *cs;
+  }
+  size_t step_index(const Step* st) const { return (size_t)(st - pg.steps.data()); }
 
   size_t mod_n(uint32_t m) const { return (size_t)1 << pg.modules[m].log_n; }
   uint32_t lanes_of(uint32_t col) const { return pg.columns[col].field ? 6 : 1; }
@@ -107,7 +172,6 @@ struct Prover {
 
   // Compiles the sub-DAG under `root` into register bytecode.  lane_of(col)
   // gives the first lane index the kernel reads for that column.
-  struct XCode { std::vector<XInst> code; uint32_t n_regs = 0, result = 0, result_ext = 0; };
   template <class LaneOf> XCode compile_expr(uint32_t root, LaneOf lane_of) {
     std::vector<char> seen(pg.nodes.size(), 0);
     collect(root, seen);
@@ -244,13 +308,18 @@ struct Prover {
         }
         col_buf[col] = b;
       } else if (cl.kind == KIND_LAGRANGE) {
-        int64_t row = cl.param >= 0 ? cl.param : (int64_t)n - 1 - (-(int64_t)cl.param - 1);
-        if (row < 0 || row >= (int64_t)n) throw Error(LG_ERR_INVALID, "Lagrange column row out of range");
-        auto b = std::make_shared<DBuf>(n, c.stream);
-        LG_CK(cudaMemsetAsync(b->p, 0, n * 4, c.stream));
-        uint32_t one = MONT_ONE;
-        c.h2d(b->p + row, &one, 4);
-        col_buf[col] = b;
+        // 1 at its row: a program constant, kept on the context
+        auto key = std::make_pair(pg.modules[cl.module].log_n, lagrange_row(col));
+        auto it = c.lagrange_vals.find(key);
+        if (it == c.lagrange_vals.end()) {
+          ArenaScope kept(nullptr);
+          auto b = std::make_shared<DBuf>(n, c.stream);
+          LG_CK(cudaMemsetAsync(b->p, 0, n * 4, c.stream));
+          uint32_t one = MONT_ONE;
+          c.h2d(b->p + key.second, &one, 4);
+          it = c.lagrange_vals.emplace(key, b).first;
+        }
+        col_buf[col] = it->second;
       }
     }
     flush();
@@ -320,6 +389,15 @@ struct Prover {
       if (pg.modules[m].log_n > MAX_LOG_MODULE) throw Error(LG_ERR_INVALID, "module above 2^22 rows");
   }
 
+  // row of a Lagrange column (board/module.go:56-82: i, or N-1-i for relative rows)
+  uint32_t lagrange_row(uint32_t col) const {
+    const Column& cl = pg.columns[col];
+    int64_t n = (int64_t)mod_n(cl.module);
+    int64_t row = cl.param >= 0 ? cl.param : n - 1 - (-(int64_t)cl.param - 1);
+    if (row < 0 || row >= n) throw Error(LG_ERR_INVALID, "Lagrange column row out of range");
+    return (uint32_t)row;
+  }
+
   uint32_t chunk_count(uint32_t m) const {
     if (fold_root[m] < 0 || degree[m] <= 0) return 0;
     size_t n = mod_n(m), want = (size_t)std::max(degree[m] - 1, 1) * n, big = 1;
@@ -378,11 +456,6 @@ struct Prover {
       if (seen[i] && pg.nodes[i].op == OP_COL) return pg.columns[pg.nodes[i].a].module;
     throw Error(LG_ERR_INVALID, "lookup table without a column");
   }
-  XProgram upload_program(const XCode& xc, std::vector<DBufP>& keep) {
-    auto code = upload_vec(c, xc.code);
-    keep.push_back(code);
-    return XProgram{(const XInst*)code->p, (uint32_t)xc.code.size(), xc.n_regs, xc.result, xc.result_ext};
-  }
 
   // Lookup multiplicities of width-1 tables, all steps of a round in one set
   // of launches (k_mult_insert / k_mult_count / k_mult_write).
@@ -399,12 +472,12 @@ struct Prover {
       if (x.op == OP_COL && x.b == 0 && pg.columns[x.a].field == 0 && col_buf.count(x.a)) return lane_ptr(x.a, 0);
       if (ext_of[root]) throw Error(LG_ERR_INVALID, "lookup table values must be base-field");
       LaneTable lt{this, {}, {}};
-      XCode xc = compile_expr(root, std::ref(lt));
+      const CodeSet& cs = compiled("e" + std::to_string(root), lt, {root});
       auto tab = upload_vec(c, lt.lanes);
       auto out = std::make_shared<DBuf>(n, c.stream);
       keep.insert(keep.end(), {tab, out});
-      evals.push_back(EvalJob{upload_program(xc, keep), (const uint32_t* const*)tab->p, out->p, (int)pg.modules[mod].log_n});
-      eval_regs = std::max(eval_regs, xc.n_regs);
+      evals.push_back(EvalJob{cs.dev[0], (const uint32_t* const*)tab->p, out->p, (int)pg.modules[mod].log_n});
+      eval_regs = std::max(eval_regs, cs.xc[0].n_regs);
       eval_n = std::max(eval_n, n);
       return out->p;
     };
@@ -486,11 +559,13 @@ struct Prover {
       LaneTable lt{this, {}, {}};
       LogupJob J{};
       J.n_terms = (uint32_t)st->e.size();
+      std::vector<uint32_t> roots;
+      for (size_t k = 0; k < st->e.size(); k++) { roots.push_back(st->e[k]); roots.push_back(st->m[k]); }
+      const CodeSet& cs = compiled("l" + std::to_string(step_index(st)), lt, roots);
       for (size_t k = 0; k < st->e.size(); k++) {
-        XCode xe = compile_expr(st->e[k], std::ref(lt)), xm = compile_expr(st->m[k], std::ref(lt));
-        J.e[k] = upload_program(xe, keep);
-        J.m[k] = upload_program(xm, keep);
-        max_regs = std::max(max_regs, std::max(xe.n_regs, xm.n_regs));
+        J.e[k] = cs.dev[2 * k];
+        J.m[k] = cs.dev[2 * k + 1];
+        max_regs = std::max(max_regs, std::max(cs.xc[2 * k].n_regs, cs.xc[2 * k + 1].n_regs));
       }
       auto tab = upload_vec(c, lt.lanes);
       auto frac = std::make_shared<DBuf>(6 * n, c.stream);
@@ -568,6 +643,8 @@ struct Prover {
     std::vector<GpJob> jobs;
     std::vector<ScanJob> scans;
     std::vector<DBufP> keep;
+    std::vector<const uint32_t*> all_lanes;  // every step's lane table, one upload
+    std::vector<size_t> lane_off;
     uint32_t max_regs = 1;
     for (const Step* st : steps) {
       uint32_t logn = pg.modules[st->module].log_n;
@@ -583,17 +660,16 @@ struct Prover {
         first_lane[col] = f;
         return f;
       };
-      XCode xn = compile_expr(st->num, lane_of), xd = compile_expr(st->den, lane_of);
-      max_regs = std::max(max_regs, std::max(xn.n_regs, xd.n_regs));
-      auto tab = upload_vec(c, lanes), cn = upload_vec(c, xn.code), cd = upload_vec(c, xd.code);
+      const CodeSet& cs = compiled("g" + std::to_string(step_index(st)), lane_of, {st->num, st->den});
+      max_regs = std::max(max_regs, std::max(cs.xc[0].n_regs, cs.xc[1].n_regs));
+      lane_off.push_back(all_lanes.size());
+      all_lanes.insert(all_lanes.end(), lanes.begin(), lanes.end());
       auto ratio = std::make_shared<DBuf>(6 * n, c.stream);
       uint32_t nt = (uint32_t)((n + SCAN_TILE - 1) / SCAN_TILE);
       auto totals = std::make_shared<DBuf>(6 * (size_t)nt, c.stream), pre = std::make_shared<DBuf>(6 * (size_t)nt, c.stream);
       auto res = std::make_shared<DBuf>(6 * n, c.stream);
-      keep.insert(keep.end(), {tab, cn, cd, ratio, totals, pre});
-      jobs.push_back(GpJob{XProgram{(const XInst*)cn->p, (uint32_t)xn.code.size(), xn.n_regs, xn.result, xn.result_ext},
-                           XProgram{(const XInst*)cd->p, (uint32_t)xd.code.size(), xd.n_regs, xd.result, xd.result_ext},
-                           (const uint32_t* const*)tab->p, ratio->p, (int)logn});
+      keep.insert(keep.end(), {ratio, totals, pre});
+      jobs.push_back(GpJob{cs.dev[0], cs.dev[1], nullptr, ratio->p, (int)logn});
       ScanJob sj{ratio->p, n, totals->p, pre->p, res->p, nt};
       if (st->type == STEP_RATIO) {  // inclusive products; the end is exposed
         if (pg.columns[st->out].field != 1 || pg.columns[st->out].module != st->module)
@@ -604,6 +680,9 @@ struct Prover {
       scans.push_back(sj);
       col_buf[st->out] = res;
     }
+    auto tab_all = upload_vec(c, all_lanes);
+    keep.push_back(tab_all);
+    for (size_t i = 0; i < jobs.size(); i++) jobs[i].lanes = (const uint32_t* const*)tab_all->p + lane_off[i];
     const int T = 128;
     size_t smem = (size_t)max_regs * 6 * T * 4;
     allow_smem(k_gp_ratio, smem);
@@ -677,14 +756,18 @@ struct Prover {
       uint32_t m, logn;
       std::vector<const uint32_t*> coef_lanes;
       std::vector<CosetLane> lanes;
-      DBufP cv, qv, code, chunks;
+      DBufP cv, qv, chunks;
       XCode xc;
+      XProgram prog;
       uint32_t zinv[4];
     };
     std::vector<ModQ> mods;
     std::vector<DBufP> keep;
     // log n -> columns -> lanes (Lagrange values -> coefficients)
     std::map<uint32_t, std::vector<std::vector<uint32_t*>>> verifier_intt;
+    // Lagrange coefficients first computed by this prove: kept on the context
+    // once their transforms are enqueued
+    std::map<std::pair<uint32_t, uint32_t>, DBufP> new_lagrange;
     for (uint32_t m : mod_order) {
       if (!chunk_count(m)) continue;
       // Four cosets give all four chunks of Q; a module of lower degree commits
@@ -706,6 +789,21 @@ struct Prover {
         auto cc = col_coef.find(col);
         if (cc != col_coef.end()) {
           for (uint32_t w = 0; w < lanes_of(col); w++) coef_lanes.push_back(cc->second + (size_t)w * n);
+        } else if (pg.columns[col].kind == KIND_LAGRANGE) {
+          // a program constant: coefficients kept from an earlier prove, or
+          // computed by this one (values copied, transformed below)
+          auto key = std::make_pair(logn, lagrange_row(col));
+          auto hit = c.lagrange_coef.find(key);
+          DBufP b = hit != c.lagrange_coef.end() ? hit->second : nullptr;
+          if (!b && new_lagrange.count(key)) b = new_lagrange.at(key);
+          if (!b) {
+            ArenaScope kept(nullptr);
+            b = std::make_shared<DBuf>(n, c.stream);
+            LG_CK(cudaMemcpyAsync(b->p, col_buf.at(col)->p, n * 4, cudaMemcpyDeviceToDevice, c.stream));
+            verifier_intt[logn].push_back({b->p});
+            new_lagrange[key] = b;
+          }
+          coef_lanes.push_back(b->p);
         } else {
           // verifier columns: coefficients of the Lagrange values
           auto b = std::make_shared<DBuf>(lanes_of(col) * n, c.stream);
@@ -721,11 +819,12 @@ struct Prover {
         first_lane[col] = f;
         return f;
       };
-      q.xc = compile_expr((uint32_t)fold_root[m], lane_of);
+      const CodeSet& cs = compiled("q" + std::to_string(m), lane_of, {(uint32_t)fold_root[m]});
+      q.xc = cs.xc[0];
+      q.prog = cs.dev[0];
       q.coef_lanes = coef_lanes;
       uint32_t g = to_mont(3), w4n = root_of_unity_mont((int)logn + RATE_LOG);
       for (int cc = 0; cc < 4; cc++) q.zinv[cc] = inv(sub(mont_pow(mul(g, mont_pow(w4n, cc)), n), MONT_ONE));
-      q.code = upload_vec(c, q.xc.code);
       mods.push_back(std::move(q));
     }
     {  // coset values, quotient values and chunks of all modules: one allocation each
@@ -779,6 +878,7 @@ struct Prover {
         for (auto& col : kv.second) intt_lanes(kv.first, col);
       }
     }
+    for (auto& kv : new_lagrange) c.lagrange_coef[kv.first] = kv.second;
     if (mods.empty()) return;
     auto coins_d = coins_on_device();
     const int T = 128;
@@ -822,7 +922,7 @@ struct Prover {
       double qbytes = 0;
       for (ModQ* q : ms) {
         QJob j{};
-        j.p = XProgram{(const XInst*)q->code->p, (uint32_t)q->xc.code.size(), q->xc.n_regs, q->xc.result, q->xc.result_ext};
+        j.p = q->prog;
         j.cv = q->cv->p;
         j.qv = q->qv->p;
         j.logn = (int)q->logn;
