@@ -139,6 +139,50 @@ def build_with_ratio(n: int, seed: int = 5, permuted: bool = True):
     return comp, wit, end
 
 
+def build_with_bus(n: int, seed: int = 9, balanced: bool = True):
+    """A plonk module next to two modules joined by a width-2 bus
+    (arguments.Bus, arguments/bus.go:42-67): "bussend_0" (n rows) sends the
+    tuples (A0, A1) on the rows where SA = 1, "busrecv_0" (n/2 rows) receives
+    (X0, X1) where SX = 1.  The received tuples are the sent ones in another
+    order (one of them altered unless `balanced`); the unselected rows hold
+    unrelated values.  Returns (program, witness, bus ends)."""
+    from .program import bus
+    rng = np.random.Generator(np.random.PCG64([seed, 0xB005]))
+    b = Builder()
+    trace: Dict[str, np.ndarray] = {}
+    m0 = Module("plonk_0", n)
+    L, R, O = col("L_0"), col("R_0"), col("O_0")
+    QL, QR, QM, QO, QK = (col(f"{s}_0") for s in ("QL", "QR", "QM", "QO", "QK"))
+    m0.assert_zero(QL * L + QR * R + QM * L * R + QO * O + QK)
+    b.add_module(m0)
+    w, S = instance_witness(n, seed, 0)
+    trace.update(w)
+    copy_constraint(b, "plonk_0", [L, R, O], S, "plonk.S_0")
+    h = n // 2
+    b.add_module(Module("bussend_0", n))
+    b.add_module(Module("busrecv_0", h))
+    rnd = lambda k: rng.integers(0, F.P, k, dtype=np.uint64).astype(np.uint32)
+    a0, a1, x0, x1 = rnd(n), rnd(n), rnd(h), rnd(h)
+    k = n // 4
+    sa = np.zeros(n, dtype=np.uint32)
+    sent = rng.choice(n, k, replace=False)
+    sa[sent] = 1
+    sx = np.zeros(h, dtype=np.uint32)
+    recv = rng.choice(h, k, replace=False)
+    sx[recv] = 1
+    order = rng.permutation(k)
+    x0[recv], x1[recv] = a0[sent][order], a1[sent][order]
+    if not balanced:
+        x1[recv[0]] = (int(x1[recv[0]]) + 1) % F.P
+    trace.update({"A0_0": a0, "A1_0": a1, "SA_0": sa, "X0_0": x0, "X1_0": x1, "SX_0": sx})
+    ends = bus(b, [col("SA_0")], [col("SX_0")], [([col("A0_0"), col("A1_0")], "bussend_0")],
+               [([col("X0_0"), col("X1_0")], "busrecv_0")])
+    trace.update(b.generated)
+    comp = b.compile()
+    wit = [np.ascontiguousarray(trace[nm], dtype=np.uint32) for (nm, f, r) in comp.witness_columns]
+    return comp, wit, ends
+
+
 def mixed_sizes(n_modules: int, lo: int, hi: int, seed: int) -> List[int]:
     """log2 module sizes drawn uniformly from [lo, hi] (seeded)."""
     rng = np.random.Generator(np.random.PCG64([seed, 0x5A5E]))

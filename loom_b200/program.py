@@ -276,7 +276,7 @@ class Builder:
         L_0·Z_{-1} - E = 0 with E = P·L_0, P the exposed end; returns P's name."""
         if not num and not den:
             raise ValueError(f"running ratio {output}: no factors")
-        deg = max(1 + sum(f.degree() for f in num), 2 + sum(f.degree() for f in den))
+        deg = running_ratio_constraint_degree(num, den)
         if deg > MAX_LOGUP_DEGREE:
             raise ValueError(f"running ratio {output}: constraint degree {deg} above {MAX_LOGUP_DEGREE}")
 
@@ -527,6 +527,83 @@ def lookup(b: "Builder", S: Sequence[Tuple[Expr, str]], T: Sequence[Tuple[Expr, 
     totals = add_logup_columns(b, f"{LOGUP}_", terms)
     b.logup_buses.append(list(totals))  # arguments/lookup.go:177
     return totals
+
+
+def running_ratio_constraint_degree(num: Sequence[Expr], den: Sequence[Expr]) -> int:
+    """board/product.go:43-52."""
+    return max(1 + sum(f.degree() for f in num), 2 + sum(f.degree() for f in den))
+
+
+def bus(b: "Builder", sel_s: Sequence[Expr], sel_r: Sequence[Expr], S: Sequence[Tuple[Sequence[Expr], str]],
+        R: Sequence[Tuple[Sequence[Expr], str]]) -> List[str]:
+    """arguments/bus.go:42-67 Bus: the tuples S[i] (sent on the rows where
+    sel_s[i] = 1) and R[i] (received where sel_r[i] = 1) balance as
+    multisets.  Tables are (expressions of the tuple, module).  Every selected
+    row contributes the factor beta + alpha^w + alpha^(w-1) c_(w-1) + ... + c_0
+    (sends as numerators, receives as denominators) and an unselected row 1,
+    as sel (factor - 1) + 1; the factors go into running-ratio columns whose
+    ends form a product bus.  Returns the ends."""
+    if len(sel_s) != len(S) or len(sel_r) != len(R):
+        raise ValueError("bus: one selector per table")
+    if not S and not R:
+        return []
+    tables = list(S) + list(R)
+    if len({len(t) for t, _ in tables}) != 1:
+        raise ValueError("bus: inconsistent width")
+    for t, _ in tables:
+        b.stage_leaves(ROUND_FOLD, *t)
+    b.stage_leaves(ROUND_FOLD, *sel_s)
+    b.stage_leaves(ROUND_FOLD, *sel_r)
+    ends = _add_running_ratios(b, _bus_factors(S, sel_s), _bus_factors(R, sel_r))
+    b.product_buses.append(list(ends))  # arguments/bus.go:66
+    return ends
+
+
+def _bus_factors(tables, sels) -> List[Tuple[str, Expr]]:
+    """arguments/bus.go:76-90: sel (beta + fold(row) - 1) + 1, fold by Horner
+    from the sentinel alpha^w."""
+    alpha, beta, one = coin(ROUND_FOLD), coin(ROUND_LOG_DERIVATIVE), const(1)
+    res = []
+    for (t, module), sel in zip(tables, sels):
+        f = alpha + t[-1]
+        for c in reversed(t[:-1]):
+            f = f * alpha + c
+        res.append((module, sel * (f + beta - one) + one))
+    return res
+
+
+def _add_running_ratios(b: "Builder", num, den) -> List[str]:
+    """arguments/bus.go:98-137: factors grouped by module (first-appearance
+    order) into running-ratio columns at RoundRunningSums, each taking in turn
+    the module's next denominator and next numerator while the constraint
+    degree stays within MAX_LOGUP_DEGREE."""
+    order: List[str] = []
+    by_mod: Dict[str, Tuple[List[Expr], List[Expr]]] = {}
+    for side, fs in ((0, num), (1, den)):
+        for module, f in fs:
+            if module not in by_mod:
+                order.append(module)
+                by_mod[module] = ([], [])
+            by_mod[module][side].append(f)
+    ends = []
+    for module in order:
+        nums, dens = list(by_mod[module][0]), list(by_mod[module][1])
+        while nums or dens:
+            cn: List[Expr] = []
+            cd: List[Expr] = []
+            grown = True
+            while grown:
+                grown = False
+                if dens and running_ratio_constraint_degree(cn, cd + [dens[0]]) <= MAX_LOGUP_DEGREE:
+                    cd.append(dens.pop(0))
+                    grown = True
+                if nums and running_ratio_constraint_degree(cn + [nums[0]], cd) <= MAX_LOGUP_DEGREE:
+                    cn.append(nums.pop(0))
+                    grown = True
+            if not cn and not cd:
+                raise ValueError(f"module {module}: a bus factor alone exceeds degree {MAX_LOGUP_DEGREE}")
+            ends.append(b.add_running_ratio_step(ROUND_RUNNING_SUMS, module, cn, cd, b.fresh_name(f"{module}.busratio_")))
+    return ends
 
 
 def add_logup_columns(b: "Builder", prefix: str, terms: Sequence[Tuple[str, Expr, Expr]]) -> List[str]:

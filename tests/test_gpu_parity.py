@@ -219,6 +219,22 @@ def test_prove_running_ratio_equals_oracle(ctx, logn, permuted):
             oracle.verify(compiled.words, got, 12, product_buses=compiled.product_buses)
 
 
+@pytest.mark.parametrize("balanced", [True, False])
+@pytest.mark.parametrize("logn", [6, 11])
+def test_prove_bus_equals_oracle(ctx, logn, balanced):
+    """arguments.Bus (width-2 tuples, selectors, two modules): running-ratio
+    columns packed by degree, product bus over their ends."""
+    compiled, wit, ends = plonk.build_with_bus(1 << logn, seed=logn, balanced=balanced)
+    mont = [F.to_mont(w) for w in wit]
+    got = ctx.prove(compiled.words, mont, 12)
+    assert got == oracle.prove(compiled.words, mont, 12)
+    if balanced:
+        oracle.verify(compiled.words, got, 12, product_buses=compiled.product_buses)
+    else:
+        with pytest.raises(oracle.VerifyError, match="do not multiply to one"):
+            oracle.verify(compiled.words, got, 12, product_buses=compiled.product_buses)
+
+
 def test_prove_lookup_value_outside_table_is_refused(ctx):
     compiled, wit = plonk.build_mixed([6, 5], seed=4)
     mont = [F.to_mont(w) for w in wit]

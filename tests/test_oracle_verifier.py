@@ -57,6 +57,21 @@ def test_running_ratio_product_bus(permuted):
             oracle.verify(compiled.words, pb, 8, product_buses=compiled.product_buses)
 
 
+@pytest.mark.parametrize("balanced", [True, False])
+def test_bus_argument(balanced):
+    """arguments.Bus between two modules: the ends of the two running-ratio
+    columns multiply to one exactly when the received tuples are the sent
+    ones."""
+    compiled, wit, ends = plonk.build_with_bus(64, seed=9, balanced=balanced)
+    pb = _prove(compiled, wit, 8)
+    oracle.verify(compiled.words, pb, 8)  # every constraint holds either way
+    if balanced:
+        oracle.verify(compiled.words, pb, 8, product_buses=compiled.product_buses)
+    else:
+        with pytest.raises(oracle.VerifyError, match="do not multiply to one"):
+            oracle.verify(compiled.words, pb, 8, product_buses=compiled.product_buses)
+
+
 def test_false_gate_is_rejected(small):
     compiled, wit, _ = small
     names = [n for (n, _, _) in compiled.witness_columns]

@@ -76,3 +76,22 @@ def test_id_support_values():
     w = F.root_of_unity(n)
     assert sup[0].tolist() == [pow(w, j, F.P) for j in range(n)]
     assert sup[2].tolist() == [9 * pow(w, j, F.P) % F.P for j in range(n)]
+
+
+def test_bus_packs_factors_by_degree():
+    """arguments/bus.go:98-137: per module, a running-ratio column takes the
+    next denominator and the next numerator in turn while the constraint
+    degree stays within 5; bus factors have degree 2, so a column holds one
+    receive and two sends (2 + 2 = 4, then 1 + 2 + 2 = 5)."""
+    from loom_b200.program import Builder, Module, bus, col
+    b = Builder()
+    b.add_module(Module("m", 16))
+    sends = [([col(f"a{i}"), col(f"b{i}")], "m") for i in range(3)]
+    recvs = [([col(f"x{i}"), col(f"y{i}")], "m") for i in range(2)]
+    ends = bus(b, [col(f"s{i}") for i in range(3)], [col(f"r{i}") for i in range(2)], sends, recvs)
+    steps = b.rounds[2]["steps"]
+    assert len(ends) == 2 and b.product_buses == [ends]
+    assert [s.end for s in steps] == ends
+    assert all(e.startswith("m.busratio_") and e.endswith("_end") for e in ends)
+    staged = b.rounds[0]["staged"]
+    assert {"a0", "b2", "x1", "y0", "s2", "r1"} <= set(staged)
