@@ -2,6 +2,7 @@
 // every lane, pair-leaf Poseidon2 hashing, Merkle tree with level injections.
 #pragma once
 #include <mutex>
+#include <type_traits>
 
 #include "host.cuh"
 #include "ntt_large.cuh"
@@ -31,6 +32,25 @@ template <class K> inline void allow_smem(K kernel, size_t bytes) {
 }
 
 // 16 elements per thread for n >= 16 (radix-16 passes), up to 1024 threads.
+// Calls f(std::integral_constant<int, L>{}) with L = logn for the
+// shared-memory transform sizes 2^4..2^14 (kernels instantiated per size),
+// L = 0 (size read at run time) for the others.
+template <class F> inline void with_ntt_size(int logn, F&& f) {
+  switch (logn) {
+    case 4: f(std::integral_constant<int, 4>{}); break;
+    case 5: f(std::integral_constant<int, 5>{}); break;
+    case 6: f(std::integral_constant<int, 6>{}); break;
+    case 7: f(std::integral_constant<int, 7>{}); break;
+    case 8: f(std::integral_constant<int, 8>{}); break;
+    case 9: f(std::integral_constant<int, 9>{}); break;
+    case 10: f(std::integral_constant<int, 10>{}); break;
+    case 11: f(std::integral_constant<int, 11>{}); break;
+    case 12: f(std::integral_constant<int, 12>{}); break;
+    case 13: f(std::integral_constant<int, 13>{}); break;
+    case 14: f(std::integral_constant<int, 14>{}); break;
+    default: f(std::integral_constant<int, 0>{}); break;
+  }
+}
 inline int ntt_threads(int logn) { return logn < 4 ? 32 : std::max(32, std::min(1024, 1 << (logn - 4))); }
 // shared words of one pad16 array of n = 2^logn points
 inline size_t pad16_words(int logn) { return ((size_t)1 << logn) + ((size_t)1 << logn) / 16 + 1; }
@@ -119,12 +139,13 @@ inline void launch_lde(Ctx& c, const std::vector<LdeLane>& lanes, uint32_t log_n
   const uint32_t* twn = c.twiddles((int)log_n);
   const uint32_t* tw4 = c.twiddles((int)log_n + RATE_LOG);
   size_t smem = 2 * pad16_words((int)log_n) * 4;
-  allow_smem(k_lde, smem);
-  c.timed("lde", 20.0 * n * lanes.size(), 0, [&] {
-    k_lde<<<(unsigned)lanes.size(), ntt_threads((int)log_n), smem, c.stream>>>((const LdeLane*)tab->p, (int)log_n,
-                                                                               from_coeffs ? 1 : 0, twn, tw4,
-                                                                               inv(to_mont((uint32_t)n)));
-    LG_LAUNCH();
+  with_ntt_size((int)log_n, [&](auto L) {
+    allow_smem(k_lde<decltype(L)::value>, smem);
+    c.timed("lde", 20.0 * n * lanes.size(), 0, [&] {
+      k_lde<decltype(L)::value><<<(unsigned)lanes.size(), ntt_threads((int)log_n), smem, c.stream>>>(
+          (const LdeLane*)tab->p, (int)log_n, from_coeffs ? 1 : 0, twn, tw4, inv(to_mont((uint32_t)n)));
+      LG_LAUNCH();
+    });
   });
 }
 

@@ -66,7 +66,10 @@ __device__ void smem_dif(uint32_t* A, int logn, const uint32_t* tw, bool inverse
 // (scaled by 1/n), in place; one block per lane, lanes[blockIdx.x].
 // n >= 16: DIT whose first pass gathers the bit-reversed input from global
 // memory; smaller n: radix-2 stages in shared memory.
-__global__ void k_intt(uint32_t* const* lanes, int logn, const uint32_t* tw_n, uint32_t n_inv) {
+// LOGN: the size when fixed at compile time (2^4..2^14), else 0 and logn_rt.
+template <int LOGN>
+__global__ void k_intt(uint32_t* const* lanes, int logn_rt, const uint32_t* tw_n, uint32_t n_inv) {
+  const int logn = LOGN ? LOGN : logn_rt;
   extern __shared__ uint32_t sm[];
   const uint32_t n = 1u << logn;
   uint32_t* d = lanes[blockIdx.x];
@@ -92,8 +95,10 @@ __global__ void k_intt(uint32_t* const* lanes, int logn, const uint32_t* tw_n, u
 // Optionally writes the coefficients.  Shared memory: A (coefficients) and B
 // (work), pad16 layout.
 struct LdeLane { const uint32_t* src; uint32_t* out; uint32_t* coef; };
-__global__ void k_lde(const LdeLane* lanes, int logn, int from_coeffs, const uint32_t* tw_n, const uint32_t* tw_4n,
+template <int LOGN>
+__global__ void k_lde(const LdeLane* lanes, int logn_rt, int from_coeffs, const uint32_t* tw_n, const uint32_t* tw_4n,
                       uint32_t n_inv) {
+  const int logn = LOGN ? LOGN : logn_rt;
   extern __shared__ uint32_t sm[];
   const uint32_t n = 1u << logn;
   const LdeLane L = lanes[blockIdx.x];
@@ -178,8 +183,10 @@ __global__ void k_lde(const LdeLane* lanes, int logn, int from_coeffs, const uin
 // n >= 16: DIT whose first pass gathers the scaled coefficients in
 // bit-reversed order from global memory.
 struct CosetLane { const uint32_t* src; uint32_t* out; };
-__global__ void k_coset_eval(const CosetLane* lanes, int logn, const uint32_t* tw_n, const uint32_t* tw_4n,
+template <int LOGN>
+__global__ void k_coset_eval(const CosetLane* lanes, int logn_rt, const uint32_t* tw_n, const uint32_t* tw_4n,
                              const uint32_t* gpow) {
+  const int logn = LOGN ? LOGN : logn_rt;
   extern __shared__ uint32_t sm[];
   const uint32_t n = 1u << logn, c = blockIdx.y;
   const CosetLane L = lanes[blockIdx.x];

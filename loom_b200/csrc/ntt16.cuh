@@ -91,11 +91,16 @@ struct NoHook {
 // and shows them to `loaded(t, v)` before its butterflies; every pass but the
 // last writes back to S (pad16 layout); the last pass hands its 16 registers
 // to `store(t, lo, v)`.
+//
+// Callers instantiate their kernels per size (logn a compile-time constant
+// after inlining), so the pass plan, the index arithmetic and the twiddle
+// offsets fold into constants and the pass loop unrolls.
 template <bool DIF, class First, class Store, class Loaded = NoHook>
-__device__ void ntt16(uint32_t* S, int logn, const uint32_t* tw, bool inverse, First first, Store store,
-                      Loaded loaded = Loaded()) {
+__device__ __forceinline__ void ntt16(uint32_t* S, int logn, const uint32_t* tw, bool inverse, First first,
+                                      Store store, Loaded loaded = Loaded()) {
   const uint32_t groups = (1u << logn) >> 4;
   const int np = pass_count(logn);
+#pragma unroll
   for (int p = 0; p < np; p++) {
     int lo, s_lo, s_hi;
     pass_plan<DIF>(p, logn, lo, s_lo, s_hi);

@@ -861,12 +861,14 @@ struct Prover {
       }
       auto tab = upload_vec(c, lanes);
       keep.push_back(tab);
-      allow_smem(k_intt, pad16_words((int)logn) * 4);
       const uint32_t* twn = c.twiddles((int)logn);
-      c.timed("quotient_intt", 8.0 * n * lanes.size(), 0, [&] {
-        k_intt<<<(unsigned)lanes.size(), ntt_threads((int)logn), pad16_words((int)logn) * 4, c.stream>>>(
-            (uint32_t* const*)tab->p, (int)logn, twn, inv(to_mont((uint32_t)n)));
-        LG_LAUNCH();
+      with_ntt_size((int)logn, [&](auto L) {
+        allow_smem(k_intt<decltype(L)::value>, pad16_words((int)logn) * 4);
+        c.timed("quotient_intt", 8.0 * n * lanes.size(), 0, [&] {
+          k_intt<decltype(L)::value><<<(unsigned)lanes.size(), ntt_threads((int)logn), pad16_words((int)logn) * 4,
+                                       c.stream>>>((uint32_t* const*)tab->p, (int)logn, twn, inv(to_mont((uint32_t)n)));
+          LG_LAUNCH();
+        });
       });
     };
     for (auto& kv : verifier_intt) {
@@ -906,14 +908,17 @@ struct Prover {
           continue;
         }
         auto tab = upload_vec(c, kv.second);
-        allow_smem(k_coset_eval, pad16_words((int)logn) * 4);
         const uint32_t* twn = c.twiddles((int)logn);
         const uint32_t* tw4 = c.twiddles((int)logn + RATE_LOG);
         const uint32_t* gp = c.gpowers((int)logn, false);
-        c.timed("coset_eval", 20.0 * n * kv.second.size(), 0, [&] {
-          k_coset_eval<<<dim3((unsigned)kv.second.size(), 4), ntt_threads((int)logn), pad16_words((int)logn) * 4, c.stream>>>(
-              (const CosetLane*)tab->p, (int)logn, twn, tw4, gp);
-          LG_LAUNCH();
+        with_ntt_size((int)logn, [&](auto L) {
+          allow_smem(k_coset_eval<decltype(L)::value>, pad16_words((int)logn) * 4);
+          c.timed("coset_eval", 20.0 * n * kv.second.size(), 0, [&] {
+            k_coset_eval<decltype(L)::value><<<dim3((unsigned)kv.second.size(), 4), ntt_threads((int)logn),
+                                               pad16_words((int)logn) * 4, c.stream>>>((const CosetLane*)tab->p,
+                                                                                       (int)logn, twn, tw4, gp);
+            LG_LAUNCH();
+          });
         });
       }
       // 2. bytecode evaluation on the 4n coset points of every module
@@ -957,12 +962,15 @@ struct Prover {
           continue;
         }
         auto tab = upload_vec(c, kv.second);
-        allow_smem(k_intt, pad16_words((int)kv.first) * 4);
         const uint32_t* twn = c.twiddles((int)kv.first);
-        c.timed("quotient_intt", 8.0 * n * kv.second.size(), 0, [&] {
-          k_intt<<<(unsigned)kv.second.size(), ntt_threads((int)kv.first), pad16_words((int)kv.first) * 4, c.stream>>>(
-              (uint32_t* const*)tab->p, (int)kv.first, twn, inv(to_mont((uint32_t)n)));
-          LG_LAUNCH();
+        with_ntt_size((int)kv.first, [&](auto L) {
+          allow_smem(k_intt<decltype(L)::value>, pad16_words((int)kv.first) * 4);
+          c.timed("quotient_intt", 8.0 * n * kv.second.size(), 0, [&] {
+            k_intt<decltype(L)::value><<<(unsigned)kv.second.size(), ntt_threads((int)kv.first),
+                                         pad16_words((int)kv.first) * 4, c.stream>>>(
+                (uint32_t* const*)tab->p, (int)kv.first, twn, inv(to_mont((uint32_t)n)));
+            LG_LAUNCH();
+          });
         });
       }
       // 4. chunk coefficients
