@@ -105,6 +105,9 @@ int lg_ctx_set_leaf_mapping(lg_ctx* ctx, int lanes_per_permutation);
  *   "p2_node_min_per_sm"  the same for one-permutation Merkle levels
  *   "merkle_tail"         levels narrower than this (power of two, 2..1024)
  *                         run in one block
+ *   "merkle_subtree"      above that, one launch builds the levels over
+ *                         this many nodes per block (power of two, 2..1024;
+ *                         0: a launch per level)
  *   "inject_block", "leaf_block"  threads per block (power of two, 32..1024)
  * Unknown names or values out of range return LG_ERR_INVALID. */
 int lg_ctx_set_tuning(lg_ctx* ctx, const char* name, int64_t value);

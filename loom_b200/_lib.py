@@ -127,7 +127,8 @@ class Context:
         self._check(self.L.lg_mem_info(self.h, ctypes.byref(f), ctypes.byref(t)))
         return int(f.value), int(t.value)
 
-    TUNING_NAMES = ("p2_leaf_min_per_sm", "p2_node_min_per_sm", "merkle_tail", "inject_block", "leaf_block")
+    TUNING_NAMES = ("p2_leaf_min_per_sm", "p2_node_min_per_sm", "merkle_tail", "merkle_subtree", "inject_block",
+                    "leaf_block")
 
     def set_tuning(self, name: str, value: int):
         """Launch-shape choice (see include/loom_gpu.h); proofs do not depend on it."""

@@ -29,7 +29,8 @@ from . import field as F
 CANDIDATES: Dict[str, Sequence[int]] = {
     "p2_leaf_min_per_sm": (32, 64, 128, 256, 512),
     "p2_node_min_per_sm": (128, 256, 512, 1024, 2048),
-    "merkle_tail": (16, 32, 64, 128, 256),
+    "merkle_tail": (16, 32, 64, 128),
+    "merkle_subtree": (0, 8, 16, 32, 64),
     "inject_block": (32, 64, 128),
     "leaf_block": (64, 128, 256),
 }

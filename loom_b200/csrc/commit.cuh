@@ -229,10 +229,10 @@ struct TreeDev {
   Digest root;
 };
 
-// Levels below this width run in one block (k_merkle_tail); wider levels are
-// grid launches.  The block is throughput bound on its one SM at wide levels
-// and latency bound at narrow ones.
-// six lanes per permutation, five permutations per warp
+// Levels below merkle_tail run in one block (k_merkle_tail); above it, a
+// launch per merkle_subtree input nodes builds one subtree per block (or a
+// launch per level).  Six lanes per permutation, five permutations per warp,
+// sized for the widest level of a block.
 inline unsigned tail_threads(uint32_t top, int fold_first) {
   uint32_t perms = std::max(1u, fold_first ? top : top / 2);
   return std::min(1024u, (perms + 4) / 5 * 32);
@@ -283,33 +283,56 @@ inline void build_tree(Ctx& c, TreeDev& t, bool read_root = true) {
       LG_LAUNCH();
     });
   };
-  auto tail = [&](uint32_t top, int fold_first) {
-    double perms = (double)top;  // top/2 + top/4 + ... + 1 levels plus injections below top
-    for (size_t k = 0; k < t.inj.size(); k++)
-      if ((1u << t.inj_log_w[k]) < top || (fold_first && (1u << t.inj_log_w[k]) == top)) perms += 1u << t.inj_log_w[k];
-    c.timed("merkle_tail", 96.0 * perms, perms, [&] {
-      k_merkle_tail<<<1, tail_threads(top, fold_first), 0, c.stream>>>(t.nodes->p, top, fold_first, (const InjRef*)ref_tab->p,
-                                             (uint32_t)refs.size());
+  // blocks = 1: the tree top from width `top` (k_merkle_tail); blocks > 1:
+  // the levels top/2 .. blocks, one subtree per block
+  auto subtrees = [&](uint32_t top, int fold_first, uint32_t blocks) {
+    double perms = (double)(top - blocks);  // nodes of the levels built, plus their injections
+    for (size_t k = 0; k < t.inj.size(); k++) {
+      const uint32_t w = 1u << t.inj_log_w[k];
+      if ((w < top && w >= blocks) || (fold_first && w == top)) perms += w;
+    }
+    c.timed(blocks == 1 ? "merkle_tail" : "merkle_level", 96.0 * perms, perms, [&] {
+      k_merkle_tail<<<blocks, tail_threads(top / blocks, fold_first), 0, c.stream>>>(
+          t.nodes->p, top, fold_first, (const InjRef*)ref_tab->p, (uint32_t)refs.size());
       LG_LAUNCH();
     });
   };
-  const uint32_t tail_w = c.tune.merkle_tail;
-  // the tail block chains at most 64 injections of one width
-  bool tail_ok = true;
+  const uint32_t tail_w = c.tune.merkle_tail, sub = c.tune.merkle_subtree;
+  // a block chains at most 64 injections of one width
+  bool chain_ok = true;
   for (size_t k = 0; k < t.inj.size(); k++) {
     size_t same = 0;
     for (size_t q = 0; q < t.inj.size(); q++) same += t.inj_log_w[q] == t.inj_log_w[k];
-    if ((1u << t.inj_log_w[k]) <= tail_w && same > 64) tail_ok = false;
+    if ((1u << t.inj_log_w[k]) < nl && same > 64) chain_ok = false;
   }
-  if (!c.batched || !tail_ok) {
+  if (!c.batched || !chain_ok) {
     fold(nl);
     for (uint32_t start = nl >> 1; start >= 1; start >>= 1) { level(start); fold(start); }
   } else if (nl <= tail_w) {
-    tail(nl, 1);
+    subtrees(nl, 1, 1);
   } else {
     fold(nl);
-    for (uint32_t start = nl >> 1; start >= tail_w; start >>= 1) { level(start); fold(start); }
-    tail(tail_w, 0);
+    uint32_t start = nl;
+    while (start > tail_w) {
+      // one launch reaches down to `stop`: start / sub at most, and not
+      // through a level with injections above the tail, whose chains run
+      // GPU-wide (fold) rather than on a block's few warps
+      const uint32_t lo = sub >= 2 ? std::max(tail_w, start / sub) : start;
+      uint32_t stop = lo;
+      for (size_t k = 0; k < t.inj.size(); k++) {
+        const uint32_t w = 1u << t.inj_log_w[k];
+        if (w >= lo && w < start) stop = std::max(stop, 2 * w);
+      }
+      if (stop < start) {
+        subtrees(start, 0, stop);
+        start = stop;
+      } else {
+        level(start >> 1);
+        fold(start >> 1);
+        start >>= 1;
+      }
+    }
+    subtrees(start, 0, 1);
   }
   if (!read_root) return;  // the root stays on the device (nodes[1])
   uint32_t* h = c.host_staging(8);

@@ -271,7 +271,8 @@ struct Ctx {
   struct Tuning {
     uint32_t p2_leaf_min_per_sm = 128;  // one thread per leaf / injection chain from this many per SM
     uint32_t p2_node_min_per_sm = 512;  // one thread per node of a Merkle level from this many per SM
-    uint32_t merkle_tail = 64;          // levels narrower than this run in one block
+    uint32_t merkle_tail = 32;          // levels narrower than this run in one block
+    uint32_t merkle_subtree = 16;       // nodes a block reduces to one in the levels above (0: a launch per level)
     uint32_t inject_block = 32;         // threads per block, one-thread injection chains
     uint32_t leaf_block = 128;          // threads per block, one-thread leaf hashing
   } tune;

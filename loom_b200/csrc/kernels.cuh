@@ -395,8 +395,12 @@ __global__ void k_merkle_inject1(uint32_t* nodes, uint32_t start, const uint32_t
   st_digest(nd, l);
 }
 
-// Upper tree levels in one block: for each width below `top`: the 2-to-1
-// step, then the injections of that width in schedule order.  When
+// Upper tree levels, one subtree per block: block b of B (gridDim.x) owns the
+// nodes [b top/B, (b+1) top/B) of width `top` and, for each width w from
+// top/2 down to B, runs the 2-to-1 step over its share of the level, then the
+// injections of width w in schedule order, with a block barrier between
+// levels.  One block (B = 1) builds a whole tree top; B > 1 replaces the
+// launches of the levels top/2 .. B, which are latency bound, by one.  When
 // fold_first, the injections of width `top` fold first (a tree whose leaf
 // level fits in one block).
 struct InjRef { const uint32_t* leaves; uint32_t width; };
@@ -407,7 +411,7 @@ __global__ void k_merkle_tail(uint32_t* nodes, uint32_t top, int fold_first, con
   P2Lane L;
   L.init();
   const uint32_t warp = threadIdx.x >> 5, warps = blockDim.x >> 5, per = warps * P2_GROUPS_PER_WARP;
-  const uint32_t grp = warp * P2_GROUPS_PER_WARP + (uint32_t)L.base / 6;
+  const uint32_t nb = gridDim.x, b = blockIdx.x, slot = warp * P2_GROUPS_PER_WARP + (uint32_t)L.base / 6;
   auto fold = [&](uint32_t w) {
     uint32_t cnt = 0;
     for (uint32_t t = 0; t < n_inj && cnt < 64; t++)
@@ -416,23 +420,24 @@ __global__ void k_merkle_tail(uint32_t* nodes, uint32_t top, int fold_first, con
         cnt++;
       }
     __syncthreads();
+    const uint32_t share = w / nb;
     if (cnt)
-      for (uint32_t j0 = warp * P2_GROUPS_PER_WARP; j0 < w; j0 += per) {
-        uint32_t j = j0 + (uint32_t)L.base / 6;
-        merkle_chain(nodes, (uint64_t)w + j, j, chain, cnt, L, keys, L.lane < 30 && j < w);
+      for (uint32_t j0 = 0; j0 < share; j0 += per) {
+        const uint32_t jl = j0 + slot, j = b * share + jl;
+        merkle_chain(nodes, (uint64_t)w + j, j, chain, cnt, L, keys, L.lane < 30 && jl < share);
       }
     __syncthreads();
   };
   if (fold_first) fold(top);
-  for (uint32_t w = top >> 1; w >= 1; w >>= 1) {
-    for (uint32_t i0 = warp * P2_GROUPS_PER_WARP; i0 < w; i0 += per) {
-      uint32_t i = i0 + (uint32_t)L.base / 6;
-      merkle_node(nodes, (uint64_t)w + i, L, keys, L.lane < 30 && i < w);
+  for (uint32_t w = top >> 1; w >= nb; w >>= 1) {
+    const uint32_t share = w / nb;
+    for (uint32_t i0 = 0; i0 < share; i0 += per) {
+      const uint32_t il = i0 + slot;
+      merkle_node(nodes, (uint64_t)w + b * share + il, L, keys, L.lane < 30 && il < share);
     }
     __syncthreads();
     fold(w);
   }
-  (void)grp;
 }
 
 // Permutation test hook: one state of 24 words per group of six lanes.

@@ -145,7 +145,10 @@ int lg_ctx_set_tuning(lg_ctx* ctx, const char* name, int64_t value) {
     if (n == "p2_leaf_min_per_sm") { in(0, 1 << 20); t.p2_leaf_min_per_sm = (uint32_t)value; }
     else if (n == "p2_node_min_per_sm") { in(0, 1 << 20); t.p2_node_min_per_sm = (uint32_t)value; }
     else if (n == "merkle_tail") { in(2, 1024); pow2(); t.merkle_tail = (uint32_t)value; }
-    else if (n == "inject_block") { in(32, 1024); pow2(); t.inject_block = (uint32_t)value; }
+    else if (n == "merkle_subtree") {
+      if (value != 0) { in(2, 1024); pow2(); }
+      t.merkle_subtree = (uint32_t)value;
+    } else if (n == "inject_block") { in(32, 1024); pow2(); t.inject_block = (uint32_t)value; }
     else if (n == "leaf_block") { in(32, 1024); pow2(); t.leaf_block = (uint32_t)value; }
     else throw Error(LG_ERR_INVALID, "unknown tuning " + n);
   });
@@ -159,6 +162,7 @@ int lg_ctx_get_tuning(lg_ctx* ctx, const char* name, int64_t* value) {
     if (n == "p2_leaf_min_per_sm") *value = t.p2_leaf_min_per_sm;
     else if (n == "p2_node_min_per_sm") *value = t.p2_node_min_per_sm;
     else if (n == "merkle_tail") *value = t.merkle_tail;
+    else if (n == "merkle_subtree") *value = t.merkle_subtree;
     else if (n == "inject_block") *value = t.inject_block;
     else if (n == "leaf_block") *value = t.leaf_block;
     else throw Error(LG_ERR_INVALID, "unknown tuning " + n);

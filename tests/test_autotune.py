@@ -10,8 +10,8 @@ from loom_b200 import autotune as AT
 class FakeContext:
     """Commit time is a fixed function of the tuning values; minimum at
     p2_leaf_min_per_sm=64, merkle_tail=128, everything else at its default."""
-    DEFAULTS = {"p2_leaf_min_per_sm": 128, "p2_node_min_per_sm": 512, "merkle_tail": 64, "inject_block": 32,
-                "leaf_block": 128}
+    DEFAULTS = {"p2_leaf_min_per_sm": 128, "p2_node_min_per_sm": 512, "merkle_tail": 32, "merkle_subtree": 16,
+                "inject_block": 32, "leaf_block": 128}
 
     def __init__(self):
         self.t = dict(self.DEFAULTS)
@@ -68,5 +68,7 @@ def test_candidates_are_valid_library_values():
                 assert v & (v - 1) == 0
             if name == "merkle_tail":
                 assert 2 <= v <= 1024
+            if name == "merkle_subtree":
+                assert v == 0 or (2 <= v <= 1024 and v & (v - 1) == 0)
             if name in ("inject_block", "leaf_block"):
                 assert 32 <= v <= 1024
