@@ -52,7 +52,7 @@ def parse():
                     help="skip the mixed-size lookup workload (40 modules, log2 rows 10-20, range lookup)")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (library defaults)")
     ap.add_argument("--retune", action="store_true", help="re-measure even if the tuning cache has this GPU")
-    ap.add_argument("--streams", type=str, default="2,4,8",
+    ap.add_argument("--streams", type=str, default="2,4,8,16",
                     help="concurrent proof streams for the throughput measurement")
     return ap.parse_args()
 
