@@ -81,6 +81,32 @@ def build(n_instances: int, n: int, seed: int = 0x10AD) -> Tuple[Compiled, List[
     return compiled, witness
 
 
+def build_with_setup(n_instances: int, n: int, seed: int = 0x10AD):
+    """The plonk program of build() with its circuit constants as setup columns
+    (expr.Setup): the selectors QL..QK, the copy permutation sigma_k and the
+    identity columns ID_k, precommitted once (setup/setup.go:68-124) instead of
+    committed in every proof.  Returns (program, witness, setup values), each
+    list in descriptor order."""
+    b = Builder()
+    trace: Dict[str, np.ndarray] = {}
+    for i in range(n_instances):
+        m = Module(_ith("plonk", i), n)
+        L, R, O = col(_ith("L", i)), col(_ith("R", i)), col(_ith("O", i))
+        QL, QR, QM, QO, QK = (col(_ith(s, i)) for s in ("QL", "QR", "QM", "QO", "QK"))
+        m.assert_zero(QL * L + QR * R + QM * L * R + QO * O + QK)
+        b.add_module(m)
+        w, S = instance_witness(n, seed, i)
+        trace.update(w)
+        copy_constraint(b, m.name, [L, R, O], S, _ith("plonk.S", i))
+        b.mark_setup(*(_ith(s, i) for s in ("QL", "QR", "QM", "QO", "QK")))
+        b.mark_setup(*(m.id_support_name(k) for k in range(3)), *(f"{_ith('plonk.S', i)}_{k}" for k in range(3)))
+    trace.update(b.generated)
+    compiled = b.compile()
+    witness = [np.ascontiguousarray(trace[name], dtype=np.uint32) for (name, fld, rows) in compiled.witness_columns]
+    setup = [np.ascontiguousarray(trace[name], dtype=np.uint32) for (name, fld, rows) in compiled.setup_columns]
+    return compiled, witness, setup
+
+
 def build_mixed(log_sizes: List[int], seed: int = 0x10AD, range_bound: int = 256) -> Tuple[Compiled, List[np.ndarray]]:
     """Modules of uneven sizes 2^log_sizes[i], each a plonk-like module as in
     build() plus a column RC_i of values in [0, range_bound) range-checked by a

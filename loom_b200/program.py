@@ -30,7 +30,7 @@ from . import field as F
 
 ROUND_FOLD, ROUND_LOG_DERIVATIVE, ROUND_RUNNING_SUMS = 0, 1, 2
 BASE, EXT = 0, 1
-KIND_WITNESS, KIND_STEP, KIND_LAGRANGE = 0, 1, 2
+KIND_WITNESS, KIND_STEP, KIND_LAGRANGE, KIND_SETUP = 0, 1, 2, 3
 OP_COL, OP_COIN, OP_CONST, OP_ADD, OP_SUB, OP_MUL, OP_EXPAVG, OP_EXPVAL = range(8)
 STEP_GP, STEP_MULT, STEP_LOGUP, STEP_RATIO = 0, 1, 2, 3
 MAGIC = 0x3150474C
@@ -201,6 +201,7 @@ class Compiled:
     n_rounds: int
     logup_buses: List[List[str]] = dfield(default_factory=list)    # totals that sum to zero
     product_buses: List[List[str]] = dfield(default_factory=list)  # running-ratio ends whose product is one
+    setup_columns: List[Tuple[str, int, int]] = dfield(default_factory=list)  # (name, field, rows), descriptor order
 
 
 class Builder:
@@ -210,10 +211,17 @@ class Builder:
         self.names = 0
         self.generated: Dict[str, np.ndarray] = {}  # generated base columns (ID support, permutation)
         self.logup_buses: List[List[str]] = []    # board.LogupBus (board/board.go:35-38)
+        self.setup_names: set = set()             # expr.Setup columns (expr/ast.go:211-217)
         self.product_buses: List[List[str]] = []  # board.ProductBus (board/board.go:28-29)
 
     def add_module(self, m: Module):
         self.modules[m.name] = m
+
+    def mark_setup(self, *names: str):
+        """Declares columns as setup columns (expr.Setup, expr/ast.go:211-217):
+        program constants precommitted once in the setup tree (setup/setup.go:68-124),
+        never staged in a round."""
+        self.setup_names.update(names)
 
     def fresh_name(self, prefix: str) -> str:
         self.names += 1
@@ -341,6 +349,8 @@ class Builder:
         for r, rd in enumerate(self.rounds):
             lst = []
             for nm in rd["staged"]:
+                if nm in self.setup_names:  # setup leaves are never staged (board/rounds.go:194)
+                    continue
                 if nm in seen:
                     raise ValueError(f"column {nm} staged twice")
                 if nm not in owner:
@@ -349,7 +359,7 @@ class Builder:
                 lst.append(nm)
             staged.append(lst)
         for nm in sorted(owner):  # sweep into the last round, sorted by name
-            if nm not in seen:
+            if nm not in seen and nm not in self.setup_names:
                 seen[nm] = n_rounds - 1
                 staged[-1].append(nm)
 
@@ -378,8 +388,11 @@ class Builder:
         mod_names = list(self.modules)
         mod_idx = {n: i for i, n in enumerate(mod_names)}
         col_idx: Dict[str, int] = {}
+        for nm in self.setup_names:
+            if nm in step_out or nm in verifier:
+                raise ValueError(f"setup column {nm} is a step output or a verifier column")
         for nm in sorted(owner):
-            kind = KIND_STEP if nm in step_out else KIND_WITNESS
+            kind = KIND_STEP if nm in step_out else KIND_SETUP if nm in self.setup_names else KIND_WITNESS
             col_idx[nm] = len(columns)
             columns.append((nm, mod_idx[owner[nm]], fields.get(nm, BASE), kind, 0))
         for nm, (mname, row) in sorted(verifier.items()):
@@ -461,8 +474,9 @@ class Builder:
             w.append(len(lst))
             w.extend(col_idx[nm] for nm in lst)
         witness = [(nm, fld, self.modules[mod_names[mi]].n) for (nm, mi, fld, kind, _) in columns if kind == KIND_WITNESS]
+        setup = [(nm, fld, self.modules[mod_names[mi]].n) for (nm, mi, fld, kind, _) in columns if kind == KIND_SETUP]
         return Compiled(np.array(w, dtype=np.uint32), witness, {n: self.modules[n].n for n in mod_names}, n_rounds,
-                        [list(x) for x in self.logup_buses], [list(x) for x in self.product_buses])
+                        [list(x) for x in self.logup_buses], [list(x) for x in self.product_buses], setup)
 
 
 # ---------------------------------------------------------------------- arguments

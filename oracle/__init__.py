@@ -36,7 +36,8 @@ def lib():
         L.oracle_prove.argtypes = [u32p, ctypes.c_size_t, ctypes.POINTER(u32p), ctypes.c_uint32,
                                    ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_size_t)]
         L.oracle_verify.argtypes = [u32p, ctypes.c_size_t, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_uint32,
-                                    ctypes.c_char_p]
+                                    ctypes.c_char_p, u32p, ctypes.c_uint32]
+        L.oracle_setup.argtypes = [u32p, ctypes.c_size_t, ctypes.POINTER(u32p), u32p]
         L.oracle_p2_permute.argtypes = [u32p, ctypes.c_int]
         L.oracle_p2_round_keys.argtypes = [ctypes.c_int, u32p]
         L.oracle_p2_diag.argtypes = [ctypes.c_int, u32p]
@@ -67,23 +68,42 @@ class VerifyError(Exception):
 
 
 def verify(program_words: np.ndarray, proof: bytes, num_queries: int, logup_buses: Sequence[Sequence[str]] = (),
-           product_buses: Sequence[Sequence[str]] = ()) -> None:
+           product_buses: Sequence[Sequence[str]] = (), setup_root=None) -> None:
     """Checks proof bytes against the program the way loom's verifier does
     (transcript replay, buses, AIR relation at zeta, FRI, Merkle openings,
-    DEEP bridge); raises VerifyError with the reason when it rejects."""
+    DEEP bridge); raises VerifyError with the reason when it rejects.
+    `setup_root` (8 canonical words) is the verification key of a program
+    with setup columns."""
     L = lib()
     prog = _u32(program_words)
     spec = ";".join(["P:" + ",".join(b) for b in product_buses] + ["L:" + ",".join(b) for b in logup_buses])
-    rc = L.oracle_verify(_p(prog), prog.size, bytes(proof), len(proof), num_queries, spec.encode())
+    vk = _u32(setup_root if setup_root is not None else np.zeros(8, np.uint32))
+    rc = L.oracle_verify(_p(prog), prog.size, bytes(proof), len(proof), num_queries, spec.encode(), _p(vk),
+                         0 if setup_root is None else 1)
     if rc != 0:
         raise VerifyError(L.oracle_last_error().decode(errors="replace"))
 
 
-def prove(program_words: np.ndarray, witness_mont: Sequence[np.ndarray], num_queries: int) -> bytes:
-    """Proof bytes (canonical encoding) for Montgomery-form witness columns."""
+def setup_root(program_words: np.ndarray, setup_mont: Sequence[np.ndarray]) -> np.ndarray:
+    """Root of the setup tree (the verification key, 8 canonical words) of a
+    program's setup columns (Montgomery words, descriptor order)."""
     L = lib()
     prog = _u32(program_words)
-    cols = [_u32(c) for c in witness_mont]
+    cols = [_u32(c) for c in setup_mont]
+    arr = (u32p * max(1, len(cols)))(*[_p(c) for c in cols])
+    out = np.zeros(8, np.uint32)
+    if L.oracle_setup(_p(prog), prog.size, arr, _p(out)) != 0:
+        raise RuntimeError("oracle_setup: " + L.oracle_last_error().decode())
+    return out
+
+
+def prove(program_words: np.ndarray, witness_mont: Sequence[np.ndarray], num_queries: int,
+          setup_mont: Sequence[np.ndarray] = ()) -> bytes:
+    """Proof bytes (canonical encoding) for Montgomery-form witness columns
+    (and setup columns, for a program that has them), descriptor order."""
+    L = lib()
+    prog = _u32(program_words)
+    cols = [_u32(c) for c in list(witness_mont) + list(setup_mont)]
     arr = (u32p * max(1, len(cols)))(*[_p(c) for c in cols])
     cap = ctypes.c_size_t(1 << 20)
     while True:

@@ -16,7 +16,9 @@
 
 namespace orc {
 std::vector<uint8_t> oracle_prove_bytes(const Program& pg, const uint32_t* const* witness, uint32_t num_queries);
-void oracle_verify_bytes(const Program& pg, const uint8_t* proof, size_t len, uint32_t num_queries, const std::string& buses);
+void oracle_verify_bytes(const Program& pg, const uint8_t* proof, size_t len, uint32_t num_queries, const std::string& buses,
+                         const std::vector<Digest>& setup_roots);
+Digest oracle_setup_root(const Program& pg, const uint32_t* const* setup);
 }
 using namespace orc;
 
@@ -45,13 +47,31 @@ int oracle_prove(const uint32_t* program, size_t nwords, const uint32_t* const* 
 
 // Verifies proof bytes against the program (verifier/verifier.go:487-533).
 // `buses` (may be NULL) lists the program's product and logup buses as
-// "P:end,end;L:total,total,...".  Returns 0 when the proof is accepted, 2
-// when it is rejected or malformed (the reason in oracle_last_error()).
+// "P:end,end;L:total,total,...".  `setup_roots` holds n_setup_roots digests
+// (8 canonical words each), the verification key of a program with setup
+// columns.  Returns 0 when the proof is accepted, 2 when it is rejected or
+// malformed (the reason in oracle_last_error()).
 int oracle_verify(const uint32_t* program, size_t nwords, const uint8_t* proof, size_t len, uint32_t num_queries,
-                  const char* buses) {
+                  const char* buses, const uint32_t* setup_roots, uint32_t n_setup_roots) {
   try {
     Program pg = parse_program(program, nwords);
-    oracle_verify_bytes(pg, proof, len, num_queries, buses ? buses : "");
+    std::vector<Digest> vk(n_setup_roots);
+    for (uint32_t i = 0; i < n_setup_roots; i++) memcpy(vk[i].v, setup_roots + 8 * i, 32);
+    oracle_verify_bytes(pg, proof, len, num_queries, buses ? buses : "", vk);
+    return 0;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return 2;
+  }
+}
+
+// Root of the setup tree (setup/setup.go:68-124) of a program's setup
+// columns (Montgomery words, descriptor order), as 8 canonical words.
+int oracle_setup(const uint32_t* program, size_t nwords, const uint32_t* const* setup, uint32_t* root_out) {
+  try {
+    Program pg = parse_program(program, nwords);
+    Digest d = oracle_setup_root(pg, setup);
+    memcpy(root_out, d.v, 32);
     return 0;
   } catch (std::exception& e) {
     g_err = e.what();

@@ -41,6 +41,7 @@ Program parse_program(const uint32_t* w, size_t n) {
     PColumn c;
     c.name = rds();
     c.module = rd(); c.field = rd(); c.kind = rd(); c.param = (int32_t)rd();
+    if (c.kind > KIND_SETUP) throw std::runtime_error("program: unknown column kind");
     if (c.module >= nm) throw std::runtime_error("program: column module out of range");
     p.columns.push_back(c);
   }
@@ -95,6 +96,11 @@ Program parse_program(const uint32_t* w, size_t n) {
 std::vector<uint8_t> oracle_prove_bytes(const Program& pg, const uint32_t* const* witness, uint32_t num_queries) {
   Prover p(pg, num_queries);
   return p.prove(witness);
+}
+
+Digest oracle_setup_root(const Program& pg, const uint32_t* const* setup) {
+  Prover p(pg, 1);
+  return p.setup_commit(setup);
 }
 
 }  // namespace orc

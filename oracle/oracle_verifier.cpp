@@ -240,6 +240,8 @@ struct Verifier {
   E6 zeta;
   std::map<std::pair<uint32_t, int>, E6> col_at;       // (column, normalized shift) -> value
   std::map<std::pair<uint32_t, uint32_t>, E6> chunk_at;  // (module, chunk) -> value
+  std::vector<Digest> vk;     // setup roots (the verification key)
+  std::vector<Digest> roots;  // per tree of the layout: setup roots, then the proof's commitments
 
   Verifier(const Program& p, uint32_t q) : pg(p), nq(q), lay(p, q) {}
 
@@ -260,11 +262,12 @@ struct Verifier {
     std::vector<uint32_t> sz = {0x53495a45, (uint32_t)lay.mod_order.size()};
     for (uint32_t m : lay.mod_order) sz.push_back((uint32_t)mod_n(m));
     fs.bind(first, sz);
+    for (const Digest& d : vk) fs.bind(first, d.v, 8);  // setup roots (verifier/verifier.go:191-197)
     coins.assign(R, e6_zero());
-    size_t ti = 0;
+    size_t ti = vk.size();
     for (uint32_t r = 0; r < R; r++) {
       if (ti < lay.trees.size() && !lay.trees[ti].air && lay.trees[ti].round == (int)r) {
-        fs.bind(coin_name(r), pf.commitments[ti].v, 8);
+        fs.bind(coin_name(r), roots[ti].v, 8);
         ti++;
       }
       for (const PStep& st : pg.steps) {  // BindExposedValues, board/logup.go:219-226
@@ -278,7 +281,7 @@ struct Verifier {
       coins[r] = digest_to_e6(fs.compute(coin_name(r)));
     }
     if (ti < lay.trees.size() && lay.trees[ti].air) {
-      fs.bind("__zeta", pf.commitments[ti].v, 8);
+      fs.bind("__zeta", roots[ti].v, 8);
       ti++;
     }
     if (ti != lay.trees.size()) fail("commitments out of layout order");
@@ -288,7 +291,11 @@ struct Verifier {
   // ---------------------------------------------------------- shapes
   void check_shapes() {
     if (pf.backend != "poseidon2") fail("proof hash backend \"" + pf.backend + "\" is not poseidon2");
-    if (pf.commitments.size() != lay.trees.size()) fail("commitment count differs from the layout");
+    const size_t n_setup = !lay.trees.empty() && lay.trees[0].setup ? 1 : 0;
+    if (vk.size() != n_setup) fail("the verification key has " + std::to_string(vk.size()) + " setup roots, the layout " + std::to_string(n_setup));
+    if (pf.commitments.size() + n_setup != lay.trees.size()) fail("commitment count differs from the layout");
+    roots = vk;
+    roots.insert(roots.end(), pf.commitments.begin(), pf.commitments.end());
     if (pf.cv.size() != lay.trees.size()) fail("claimed-value batches differ from the layout");
     for (size_t t = 0; t < lay.trees.size(); t++) {
       const auto& T = lay.trees[t];
@@ -592,7 +599,7 @@ struct Verifier {
           idx >>= 1;
           fold((size_t)1 << (depth - s - 1));
         }
-        if (next != widths.size() || !digest_eq(h, pf.commitments[t]))
+        if (next != widths.size() || !digest_eq(h, roots[t]))
           fail("point samplings: Merkle path does not authenticate under batch " + std::to_string(t) + "'s root");
       }
     }
@@ -692,8 +699,10 @@ struct Verifier {
 
 }  // namespace
 
-void oracle_verify_bytes(const Program& pg, const uint8_t* proof, size_t len, uint32_t num_queries, const std::string& buses) {
+void oracle_verify_bytes(const Program& pg, const uint8_t* proof, size_t len, uint32_t num_queries, const std::string& buses,
+                         const std::vector<Digest>& setup_roots) {
   Verifier v(pg, num_queries);
+  v.vk = setup_roots;
   v.verify(proof, len, buses);
 }
 

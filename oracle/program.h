@@ -10,8 +10,8 @@
 //   magic 0x3150474C, n_rounds, n_modules, n_columns, n_nodes, n_steps
 //   module  : log_n, str name, n_rel, rel_root[n_rel]
 //   column  : str name, module, field(0 base|1 ext), kind(0 witness|1 step
-//             output|2 Lagrange verifier column), param(int32 row; <0 means
-//             relative from the end, -(i+1))
+//             output|2 Lagrange verifier column|3 setup column), param(int32
+//             row; <0 means relative from the end, -(i+1))
 //   node    : op(0 col|1 coin|2 const|3 add|4 sub|5 mul|6 exposed average),
 //             a, b.  col: a = column, b = shift (int32); coin: a = round;
 //             const: a = canonical value; add/sub/mul: a, b = child nodes
@@ -38,7 +38,7 @@ namespace orc {
 
 enum { OP_COL = 0, OP_COIN = 1, OP_CONST = 2, OP_ADD = 3, OP_SUB = 4, OP_MUL = 5, OP_EXPAVG = 6, OP_EXPVAL = 7 };
 enum { STEP_GP = 0, STEP_MULT = 1, STEP_LOGUP = 2, STEP_RATIO = 3 };
-enum { KIND_WITNESS = 0, KIND_STEP = 1, KIND_LAGRANGE = 2 };
+enum { KIND_WITNESS = 0, KIND_STEP = 1, KIND_LAGRANGE = 2, KIND_SETUP = 3 };
 
 struct PModule { uint32_t log_n; std::string name; std::vector<uint32_t> rels; };
 struct PColumn { std::string name; uint32_t module, field, kind; int32_t param; };

@@ -70,7 +70,7 @@ struct Prover {
 
   // Layout: trees in canonical order (rounds with staged columns, then AIR).
   struct Group { uint32_t module; std::vector<uint32_t> bcols, ecols; };  // column ids, or chunk ids for AIR
-  struct TreeL { bool air; int round; std::vector<Group> groups; };
+  struct TreeL { bool air; int round; std::vector<Group> groups; bool setup = false; };
   std::vector<TreeL> trees;
   // AIR chunks: (module, chunk) -> Lagrange-normal polynomial.
   std::map<std::pair<uint32_t, uint32_t>, std::vector<uint32_t>> air_base;
@@ -80,7 +80,8 @@ struct Prover {
   struct Source { std::vector<std::vector<uint32_t>> b; std::vector<std::vector<E6>> e; size_t rows; };
   struct Committed { Tree tree; std::vector<Source> sources; };  // sources in sorted order
   std::vector<Committed> committed;
-  std::vector<Digest> commitments;
+  std::vector<Digest> commitments;   // trace and AIR roots (the proof's)
+  Digest setup_root{};               // the verification key when there is a setup tree
   E6 zeta;
 
   Prover(const Program& p, uint32_t q) : pg(p), num_queries(q) {}
@@ -157,23 +158,40 @@ struct Prover {
     setup_layout();
     load_columns(witness);
   }
-  // witness columns and the Lagrange columns' values
+  // values of column c from Montgomery words
+  void load_column(uint32_t c, const uint32_t* src) {
+    size_t n = mod_n(pg.columns[c].module);
+    if (pg.columns[c].field == 0) {
+      std::vector<uint32_t> v(n);
+      for (size_t i = 0; i < n; i++) v[i] = from_mont(src[i]);
+      base[c] = v;
+    } else {
+      std::vector<E6> v(n);
+      for (size_t i = 0; i < n; i++) for (int k = 0; k < 6; k++) v[i].c[k] = from_mont(src[6 * i + k]);
+      ext[c] = v;
+    }
+  }
+  // The setup tree's root (the verification key) from the setup columns
+  // alone, in descriptor order (setup/setup.go:68-124).
+  Digest setup_commit(const uint32_t* const* setup) {
+    setup_layout();
+    size_t si = 0;
+    for (uint32_t c = 0; c < pg.columns.size(); c++)
+      if (pg.columns[c].kind == KIND_SETUP) load_column(c, setup[si++]);
+    if (trees.empty() || !trees[0].setup) throw std::runtime_error("setup: the program has no setup columns");
+    return commit(tree_groups(trees[0])).tree.root();
+  }
+  // witness columns, then setup columns (each in descriptor order, as
+  // `witness` lists them), and the Lagrange columns' values
   void load_columns(const uint32_t* const* witness) {
-    size_t wi = 0;
+    size_t nw = 0;
+    for (const PColumn& col : pg.columns) nw += col.kind == KIND_WITNESS;
+    size_t wi = 0, si = nw;
     for (uint32_t c = 0; c < pg.columns.size(); c++) {
       const PColumn& col = pg.columns[c];
       size_t n = mod_n(col.module);
-      if (col.kind == KIND_WITNESS) {
-        const uint32_t* src = witness[wi++];
-        if (col.field == 0) {
-          std::vector<uint32_t> v(n);
-          for (size_t i = 0; i < n; i++) v[i] = from_mont(src[i]);
-          base[c] = v;
-        } else {
-          std::vector<E6> v(n);
-          for (size_t i = 0; i < n; i++) for (int k = 0; k < 6; k++) v[i].c[k] = from_mont(src[6 * i + k]);
-          ext[c] = v;
-        }
+      if (col.kind == KIND_WITNESS || col.kind == KIND_SETUP) {
+        load_column(c, witness[col.kind == KIND_WITNESS ? wi++ : si++]);
       } else if (col.kind == KIND_LAGRANGE) {
         // board/module.go:56-82: 1 at row i (or N-1-i for relative columns)
         std::vector<uint32_t> v(n, 0);
@@ -232,8 +250,23 @@ struct Prover {
       }
     }
     for (auto& kv : col_shifts) std::sort(kv.second.begin(), kv.second.end());
-    // layout (internal/protocol/layout.go:165-241): one tree per round with
-    // staged columns, then one AIR tree; groups in sorted module order.
+    // layout (internal/protocol/layout.go:165-241): the setup tree (setup
+    // columns by module, sorted by name within a module, base then ext;
+    // internal/protocol/layout.go:131-151), one tree per round with staged
+    // columns, then one AIR tree; groups in sorted module order.
+    {
+      TreeL t; t.air = false; t.round = -2; t.setup = true;
+      for (uint32_t m : mod_order) {
+        std::vector<uint32_t> cols;
+        for (uint32_t c = 0; c < pg.columns.size(); c++)
+          if (pg.columns[c].kind == KIND_SETUP && pg.columns[c].module == m) cols.push_back(c);
+        std::sort(cols.begin(), cols.end(), [&](uint32_t a, uint32_t b) { return pg.columns[a].name < pg.columns[b].name; });
+        Group g; g.module = m;
+        for (uint32_t c : cols) (pg.columns[c].field == 0 ? g.bcols : g.ecols).push_back(c);
+        if (!g.bcols.empty() || !g.ecols.empty()) t.groups.push_back(g);
+      }
+      if (!t.groups.empty()) trees.push_back(t);
+    }
     for (uint32_t r = 0; r < pg.n_rounds; r++) {
       TreeL t; t.air = false; t.round = (int)r;
       for (uint32_t m : mod_order) {
@@ -623,8 +656,16 @@ struct Prover {
       for (uint32_t m : mod_order) sz.push_back((uint32_t)mod_n(m));
       fs.bind(first, sz);
     }
-    // rounds: steps, commit, bind root, sample (prover/prover.go:360-411)
+    // setup tree: precommitted, its root bound to the first challenge and
+    // kept out of the proof's commitments (prover/prover.go:175-229)
     size_t tree_idx = 0;
+    if (!trees.empty() && trees[0].setup) {
+      committed.push_back(commit(tree_groups(trees[0])));
+      setup_root = committed.back().tree.root();
+      fs.bind(first, setup_root.v, 8);
+      tree_idx = 1;
+    }
+    // rounds: steps, commit, bind root, sample (prover/prover.go:360-411)
     coins.assign(R, e6_zero());
     for (uint32_t r = 0; r < R; r++) {
       for (const PStep& st : pg.steps) if (st.round == r) run_step(st);

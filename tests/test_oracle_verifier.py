@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import oracle
-from loom_b200 import field as F, plonk
+from loom_b200 import field as F, plonk, proof
 
 
 def _prove(compiled, wit, q):
@@ -119,3 +119,27 @@ def test_wrong_query_count_or_program_is_rejected(small, mixed):
         oracle.verify(mixed[0].words, pb, 12)
     with pytest.raises(oracle.VerifyError, match="truncated"):
         oracle.verify(compiled.words, pb[:-4], 12)
+
+
+def test_setup_precommit():
+    """setup.Setup (setup/setup.go:68-124): selectors, copy permutation and
+    identity columns as setup columns go into one precommitted tree whose root
+    is the verification key; the proof's commitments leave it out, its claimed
+    values and openings come first, and only the right key verifies."""
+    compiled, wit, setup = plonk.build_with_setup(2, 64)
+    sm = [F.to_mont(x) for x in setup]
+    pb = oracle.prove(compiled.words, [F.to_mont(w) for w in wit], 8, sm)
+    root = oracle.setup_root(compiled.words, sm)
+    oracle.verify(compiled.words, pb, 8, setup_root=root)
+    p = proof.decode(pb)
+    assert len(p.commitments) == 3 and len(p.claimed_values) == 4
+    assert [len(g["base"]) for g in p.claimed_values[0]] == [11, 11]  # 5 selectors, 3 sigma, 3 ID
+    assert [len(g["base"]) for g in p.claimed_values[1]] == [3, 3]    # L, R, O only
+    with pytest.raises(oracle.VerifyError, match="verification key"):
+        oracle.verify(compiled.words, pb, 8)
+    bad = root.copy()
+    bad[0] ^= 1
+    with pytest.raises(oracle.VerifyError):
+        oracle.verify(compiled.words, pb, 8, setup_root=bad)
+    other = plonk.build_with_setup(2, 64, seed=7)[2]
+    assert (oracle.setup_root(compiled.words, [F.to_mont(x) for x in other]) != root).any()
