@@ -25,8 +25,8 @@
  *   module  : log2(N), str name, n_rel, rel_root[n_rel]
  *   column  : str name, module, field (0 base | 1 ext),
  *             kind (0 witness | 1 prover-step output | 2 Lagrange verifier
- *             column), param (int32 row for kind 2; negative -(i+1) counts
- *             from the last row)
+ *             column | 3 setup column, precommitted by lg_setup), param
+ *             (int32 row for kind 2; negative -(i+1) counts from the last row)
  *   node    : op (0 column | 1 round coin | 2 constant | 3 add | 4 sub |
  *             5 mul | 6 exposed average | 7 exposed value), a, b — column:
  *             a = column, b = int32 shift; coin: a = round; constant: a =
@@ -120,7 +120,8 @@ const char* lg_last_error(lg_ctx* ctx);
 /* Whole prove phase for the Poseidon2 backend: replaces prover.Prove
  * (prover/prover.go:655-719) called with fri.Poseidon2HashBackend()
  * (internal/fri/hash_backend.go:21-40) and WithNumFriQueries(num_queries)
- * (prover/prover.go:74-80), no setup columns, no public inputs.
+ * (prover/prover.go:74-80), no public inputs; setup columns come from
+ * lg_setup.
  * `hash_backend` must be "poseidon2" (or "" = default); "sha256" and
  * "blake3" return LG_ERR_UNSUPPORTED.  The proof is written straight into
  * `proof` (capacity *proof_len; its length comes back in *proof_len).  On
@@ -130,6 +131,17 @@ int lg_prove(lg_ctx* ctx, const char* hash_backend, const uint32_t* program, siz
              const uint32_t* const* witness, int witness_on_device, uint32_t num_queries, uint8_t* proof,
              size_t* proof_len);
 int lg_last_proof(lg_ctx* ctx, uint8_t* proof, size_t* proof_len);
+/* setup.Setup (setup/setup.go:68-124) for a program with setup columns
+ * (column kind 3: circuit constants such as selectors and permutations):
+ * commits them, base field only, passed in descriptor order, into the setup
+ * tree and keeps tree, LDE and columns on the context with the program (the
+ * proving key); writes the root (the verification key, Montgomery words).
+ * lg_prove of that program then takes only the witness columns (kind 0),
+ * binds the root after the module sizes and leaves it out of the proof's
+ * commitments.  The context keeps the setups of its eight most recently
+ * proven programs; a program that dropped out needs lg_setup again. */
+int lg_setup(lg_ctx* ctx, const uint32_t* program, size_t program_words, const uint32_t* const* setup_cols,
+             int on_device, uint32_t root[8]);
 
 /* PCS.Commit of one batch (internal/fri/pcs.go:145-168 →
  * internal/fri/commitment.go:259-386): RS-encode every polynomial at rate 4,

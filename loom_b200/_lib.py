@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(HERE, "libloom_gpu.so")
 
 LG_OK, LG_ERR_INVALID, LG_ERR_CUDA, LG_ERR_OOM, LG_ERR_UNSUPPORTED, LG_ERR_BUFFER = range(6)
 EXPORTS = ["lg_ctx_create", "lg_ctx_destroy", "lg_ctx_set_batched", "lg_ctx_set_leaf_mapping", "lg_ctx_set_tuning",
-           "lg_ctx_get_tuning", "lg_mem_info", "lg_last_error", "lg_prove", "lg_last_proof", "lg_commit_root",
+           "lg_ctx_get_tuning", "lg_mem_info", "lg_last_error", "lg_prove", "lg_last_proof", "lg_setup", "lg_commit_root",
            "lg_rs_encode", "lg_poseidon2_permute", "lg_merkle_root", "lg_fri_fold", "lg_timer_mark",
            "lg_timer_elapsed", "lg_kernel_launches", "lg_profile", "lg_profile_report", "lg_grand_product", "lg_grand_product_noalloc", "lg_deep_quotient"]
 
@@ -55,6 +55,7 @@ def load():
         L.lg_prove.argtypes = [vp, ctypes.c_char_p, u32p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
                                ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_size_t)]
         L.lg_last_proof.argtypes = [vp, ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_size_t)]
+        L.lg_setup.argtypes = [vp, u32p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_int, u32p]
         L.lg_commit_root.argtypes = [vp, ctypes.c_uint32, u64p, u32p, u32p, ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, u32p]
         L.lg_rs_encode.argtypes = [vp, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_int]
         L.lg_poseidon2_permute.argtypes = [vp, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int]
@@ -151,6 +152,21 @@ class Context:
         self._check(self.L.lg_ctx_set_leaf_mapping(self.h, lanes))
 
     # ------------------------------------------------------------------ prove
+    def setup(self, program_words: np.ndarray, setup_cols: Sequence, on_device: bool = False) -> np.ndarray:
+        """setup.Setup: precommits the program's setup columns (Montgomery,
+        descriptor order; device addresses with on_device=True) on this
+        context; returns the root (the verification key, Montgomery words)."""
+        prog = _u32(program_words)
+        if on_device:
+            arr = (ctypes.c_void_p * max(1, len(setup_cols)))(*[int(p) for p in setup_cols])
+        else:
+            cols = [_u32(c) for c in setup_cols]
+            arr = (ctypes.c_void_p * max(1, len(cols)))(*[c.ctypes.data for c in cols])
+        root = np.zeros(8, dtype=np.uint32)
+        self._check(self.L.lg_setup(self.h, prog.ctypes.data_as(u32p), prog.size, ctypes.cast(arr, ctypes.c_void_p),
+                                    int(on_device), root.ctypes.data_as(u32p)))
+        return root
+
     def prove(self, program_words: np.ndarray, witness: Sequence, num_queries: int, on_device: bool = False,
               hash_backend: str = "poseidon2") -> bytes:
         """prover.Prove with the Poseidon2 backend.  `witness`: Montgomery

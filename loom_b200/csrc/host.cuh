@@ -281,7 +281,7 @@ struct Ctx {
 // ---------------------------------------------------------------- program
 // Flat descriptor; the format is documented in include/loom_gpu.h.
 enum { OP_COL = 0, OP_COIN = 1, OP_CONST = 2, OP_ADD = 3, OP_SUB = 4, OP_MUL = 5, OP_EXPAVG = 6, OP_EXPVAL = 7 };
-enum { KIND_WITNESS = 0, KIND_STEP = 1, KIND_LAGRANGE = 2 };
+enum { KIND_WITNESS = 0, KIND_STEP = 1, KIND_LAGRANGE = 2, KIND_SETUP = 3 };
 enum { STEP_GP = 0, STEP_MULT = 1, STEP_LOGUP = 2, STEP_RATIO = 3 };
 inline bool exposes(uint32_t step_type) { return step_type == STEP_LOGUP || step_type == STEP_RATIO; }
 inline bool is_binary(uint32_t op) { return op == OP_ADD || op == OP_SUB || op == OP_MUL; }
@@ -337,7 +337,7 @@ inline Program parse_program(const uint32_t* w, size_t n) {
     Column c;
     c.name = rds();
     c.module = rd(); c.field = rd(); c.kind = rd(); c.param = (int32_t)rd();
-    if (c.module >= nm || c.field > 1 || c.kind > 2) throw Error(LG_ERR_INVALID, "bad column " + c.name);
+    if (c.module >= nm || c.field > 1 || c.kind > KIND_SETUP) throw Error(LG_ERR_INVALID, "bad column " + c.name);
     p.columns.push_back(c);
   }
   for (uint32_t i = 0; i < nn; i++) {

@@ -191,6 +191,17 @@ int lg_prove(lg_ctx* ctx, const char* hash_backend, const uint32_t* program, siz
   });
 }
 
+int lg_setup(lg_ctx* ctx, const uint32_t* program, size_t program_words, const uint32_t* const* setup_cols,
+             int on_device, uint32_t root[8]) {
+  return guarded(ctx, [&] {
+    if (!program || !setup_cols || !root) throw Error(LG_ERR_INVALID, "null argument");
+    Prover pr(ctx->c, program, program_words, 1);
+    pr.precommit(setup_cols, on_device != 0);
+    LG_CK(cudaStreamSynchronize(ctx->c.stream));
+    memcpy(root, pr.prog->setup->root.v, 32);
+  });
+}
+
 int lg_last_proof(lg_ctx* ctx, uint8_t* proof, size_t* proof_len) {
   if (!ctx || !proof_len) return LG_ERR_INVALID;
   size_t need = ctx->last_proof_len;

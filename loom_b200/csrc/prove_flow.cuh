@@ -23,9 +23,16 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
     for (uint32_t m : mod_order) sz.push_back(to_mont((uint32_t)mod_n(m)));
     fs.bind(first, sz.data(), sz.size());
   }
+  // ---- the precommitted setup tree: its root binds to the first challenge
+  // and stays out of the proof's commitments (prover/prover.go:175-229)
+  size_t ti = 0;
+  if (!trees.empty() && trees[0].setup) {
+    committed.push_back(prog->setup->committed);
+    fs.bind(coin_name(0), prog->setup->root.v, 8);
+    ti = 1;
+  }
   // ---- rounds: steps, commit, bind root, sample coin (prover/prover.go:360-411)
   coins.assign(R, e6_zero());
-  size_t ti = 0;
   for (uint32_t r = 0; r < R; r++) {
     run_steps(r);
     if (ti < trees.size() && !trees[ti].air && trees[ti].round == (int)r) {

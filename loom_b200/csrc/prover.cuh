@@ -31,9 +31,19 @@ struct CodeSet {
   std::vector<uint32_t> cols;  // columns in first-use order
   DBufP code;                  // every xc back to back (kept across proves)
 };
+// A program's precommitted setup tree (lg_setup; setup/setup.go:68-124): the
+// committed LDE and tree, the setup columns' values and coefficients, and the
+// root the verifier holds as its key.  Kept on the context with the program.
+struct SetupData {
+  Committed committed;
+  Digest root;
+  std::map<uint32_t, DBufP> values;            // setup column -> Lagrange values
+  std::map<uint32_t, const uint32_t*> coef;    // setup column -> coefficient lane 0 (in committed)
+};
 struct ProgCache {
   std::vector<uint32_t> words;  // the program descriptor, compared in full
   std::map<std::string, std::shared_ptr<CodeSet>> sites;
+  std::shared_ptr<SetupData> setup;
 };
 
 struct Prover {
@@ -58,7 +68,7 @@ struct Prover {
   std::map<uint32_t, const uint32_t*> col_coef;  // committed columns: coefficient lane 0
 
   struct Group { uint32_t module; std::vector<uint32_t> bcols, ecols; };
-  struct TreeL { bool air; int round; std::vector<Group> groups; };
+  struct TreeL { bool air; int round; std::vector<Group> groups; bool setup = false; };
   std::vector<TreeL> trees;
   std::vector<Committed> committed;
   std::vector<Digest> commitments;
@@ -269,11 +279,53 @@ struct Prover {
   }
 
   // ------------------------------------------------------------ setup
-  void setup(const uint32_t* const* witness, bool on_device) {
+  void init_order() {
     exposed.assign(n_exposed(), e6_zero());
     exposed_ready.assign(n_exposed(), 0);
     for (uint32_t m = 0; m < pg.modules.size(); m++) mod_order.push_back(m);
     std::sort(mod_order.begin(), mod_order.end(), [&](uint32_t a, uint32_t b) { return pg.modules[a].name < pg.modules[b].name; });
+  }
+
+  // lg_setup (setup/setup.go:68-124): uploads the setup columns (base field,
+  // descriptor order), commits the setup tree and keeps tree, LDE, values
+  // and coefficients on the context with the program.  Everything allocated
+  // here outlives the call.
+  void precommit(const uint32_t* const* cols, bool on_device) {
+    ArenaScope kept(nullptr);
+    init_order();
+    size_t total = 0;
+    for (const Column& cl : pg.columns)
+      if (cl.kind == KIND_SETUP) {
+        if (cl.field != 0) throw Error(LG_ERR_UNSUPPORTED, "extension-field setup columns are not supported");
+        total += mod_n(cl.module);
+      }
+    if (!total) throw Error(LG_ERR_INVALID, "the program has no setup columns");
+    auto all = std::make_shared<DBuf>(total, c.stream);
+    size_t off = 0, si = 0;
+    for (uint32_t col = 0; col < pg.columns.size(); col++) {
+      const Column& cl = pg.columns[col];
+      if (cl.kind != KIND_SETUP) continue;
+      const size_t n = mod_n(cl.module);
+      if (!cols[si]) throw Error(LG_ERR_INVALID, "null setup column");
+      LG_CK(cudaMemcpyAsync(all->p + off, cols[si++], n * 4, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                            c.stream));
+      col_buf[col] = dbuf_slice(all, off, n);
+      off += n;
+    }
+    setup_layout();
+    auto sd = std::make_shared<SetupData>();
+    sd->committed = commit_tree(trees[0]);  // also records the setup columns' coefficients
+    sd->root = sd->committed.tree.root;
+    for (uint32_t col = 0; col < pg.columns.size(); col++)
+      if (pg.columns[col].kind == KIND_SETUP) {
+        sd->values[col] = col_buf.at(col);
+        sd->coef[col] = col_coef.at(col);
+      }
+    prog->setup = sd;
+  }
+
+  void setup(const uint32_t* const* witness, bool on_device) {
+    init_order();
     // Host witness: one device buffer for all columns; columns that follow
     // one another in host memory go up in a single copy.
     size_t total_words = 0;
@@ -320,9 +372,19 @@ struct Prover {
           it = c.lagrange_vals.emplace(key, b).first;
         }
         col_buf[col] = it->second;
+      } else if (cl.kind == KIND_SETUP) {  // precommitted by lg_setup
+        if (!prog->setup) throw Error(LG_ERR_INVALID, "the program has setup columns: precommit them with lg_setup first");
+        col_buf[col] = prog->setup->values.at(col);
+        col_coef[col] = prog->setup->coef.at(col);
       }
     }
     flush();
+    setup_layout();
+  }
+
+  // Module order is set; folded relations, degrees, shift schedule and the
+  // tree layout (no column data needed).
+  void setup_layout() {
     // fold relations with coin(last round) (board/program.go:62-80)
     fold_root.assign(pg.modules.size(), -1);
     degree.assign(pg.modules.size(), NEG_INF);
@@ -362,7 +424,22 @@ struct Prover {
       }
     }
     for (auto& kv : col_shifts) std::sort(kv.second.begin(), kv.second.end());
-    // layout (internal/protocol/layout.go:165-241)
+    // layout (internal/protocol/layout.go:165-241): the setup tree (setup
+    // columns by module, sorted by name within a module; layout.go:131-151),
+    // one tree per round, the AIR tree
+    {
+      TreeL t{false, -2, {}, true};
+      for (uint32_t m : mod_order) {
+        std::vector<uint32_t> cols;
+        for (uint32_t col = 0; col < pg.columns.size(); col++)
+          if (pg.columns[col].kind == KIND_SETUP && pg.columns[col].module == m) cols.push_back(col);
+        std::sort(cols.begin(), cols.end(), [&](uint32_t a, uint32_t b) { return pg.columns[a].name < pg.columns[b].name; });
+        Group g{m, {}, {}};
+        for (uint32_t col : cols) (pg.columns[col].field == 0 ? g.bcols : g.ecols).push_back(col);
+        if (!g.bcols.empty() || !g.ecols.empty()) t.groups.push_back(g);
+      }
+      if (!t.groups.empty()) trees.push_back(t);
+    }
     for (uint32_t r = 0; r < pg.n_rounds; r++) {
       TreeL t{false, (int)r, {}};
       for (uint32_t m : mod_order) {
@@ -370,6 +447,7 @@ struct Prover {
         for (uint32_t col : pg.staged[r]) {
           if (pg.columns[col].module != m) continue;
           if (pg.columns[col].kind == KIND_LAGRANGE) throw Error(LG_ERR_INVALID, "verifier column staged for commitment");
+          if (pg.columns[col].kind == KIND_SETUP) throw Error(LG_ERR_INVALID, "setup column staged in a round");
           (pg.columns[col].field == 0 ? g.bcols : g.ecols).push_back(col);
         }
         if (!g.bcols.empty() || !g.ecols.empty()) t.groups.push_back(g);

@@ -235,6 +235,36 @@ def test_prove_bus_equals_oracle(ctx, logn, balanced):
             oracle.verify(compiled.words, got, 12, product_buses=compiled.product_buses)
 
 
+@pytest.mark.parametrize("batched", [True, False])
+@pytest.mark.parametrize("n_inst,logn", [(2, 6), (3, 11)])
+def test_prove_with_setup_equals_oracle(ctx, n_inst, logn, batched):
+    """setup.Setup then Prove: the selectors, copy permutation and identity
+    columns precommitted once (lg_setup); the root equals the oracle's, the
+    proofs equal the oracle's byte for byte on every prove that reuses the
+    precommit, and the verifier accepts them under that key."""
+    compiled, wit, setup = plonk.build_with_setup(n_inst, 1 << logn, seed=logn)
+    wm = [F.to_mont(w) for w in wit]
+    sm = [F.to_mont(x) for x in setup]
+    root = ctx.setup(compiled.words, sm)
+    want_root = oracle.setup_root(compiled.words, sm)
+    assert F.from_mont(root).tolist() == want_root.tolist()
+    ctx.set_batched(batched)
+    try:
+        got = ctx.prove(compiled.words, wm, 12)
+        again = ctx.prove(compiled.words, wm, 12)
+    finally:
+        ctx.set_batched(True)
+    assert got == again == oracle.prove(compiled.words, wm, 12, sm)
+    oracle.verify(compiled.words, got, 12, setup_root=want_root)
+
+
+def test_prove_without_setup_is_refused(ctx):
+    compiled, wit, setup = plonk.build_with_setup(1, 1 << 5, seed=3)
+    with pytest.raises(LoomError) as e:
+        ctx.prove(compiled.words, [F.to_mont(w) for w in wit], 4)
+    assert e.value.code == 1 and "lg_setup" in str(e.value)
+
+
 def test_prove_lookup_value_outside_table_is_refused(ctx):
     compiled, wit = plonk.build_mixed([6, 5], seed=4)
     mont = [F.to_mont(w) for w in wit]
