@@ -209,6 +209,62 @@ def build_with_bus(n: int, seed: int = 9, balanced: bool = True):
     return comp, wit, ends
 
 
+def build_with_tuple_lookup(n: int, seed: int = 13, present: bool = True):
+    """A plonk module next to a conditional tuple lookup
+    (arguments.CLookupUnionTuple, arguments/lookup.go:86-110): the rows of
+    (SA, SB) in "lookA_0" (n rows, selector SS) and of (XA, XB) in "lookB_0"
+    (n/4 rows, selector SX) whose selector is non-zero lie among the rows of
+    (TA, TB) in "table_0" (n/2 rows) whose selector ST is non-zero.  Selector
+    values other than 1 weight the rows (a source row with SS = 2 counts twice;
+    a target row with ST = 3 carries a third of its tuple's weight in its
+    multiplicity); some target tuples repeat, one of them first on an
+    unselected row.  Unless `present`, one selected source tuple is missing
+    from the table.  Returns (program, witness)."""
+    from .program import lookup_tuple
+    rng = np.random.Generator(np.random.PCG64([seed, 0x7AB1]))
+    b = Builder()
+    trace: Dict[str, np.ndarray] = {}
+    m0 = Module("plonk_0", n)
+    L, R, O = col("L_0"), col("R_0"), col("O_0")
+    QL, QR, QM, QO, QK = (col(f"{s}_0") for s in ("QL", "QR", "QM", "QO", "QK"))
+    m0.assert_zero(QL * L + QR * R + QM * L * R + QO * O + QK)
+    b.add_module(m0)
+    w, S = instance_witness(n, seed, 0)
+    trace.update(w)
+    copy_constraint(b, "plonk_0", [L, R, O], S, "plonk.S_0")
+    h, q = n // 2, n // 4
+    for name, rows in (("table_0", h), ("lookA_0", n), ("lookB_0", q)):
+        b.add_module(Module(name, rows))
+    rnd = lambda k: rng.integers(0, F.P, k, dtype=np.uint64).astype(np.uint32)
+    ta, tb = rnd(h), rnd(h)
+    ta[5], tb[5] = ta[9], tb[9]        # a repeated tuple, both rows selected
+    ta[2], tb[2] = ta[11], tb[11]      # repeated, first occurrence unselected
+    st = (rng.integers(0, 4, h) > 0).astype(np.uint32)
+    st[[5, 9, 11]] = 1
+    st[2] = 0
+    st[7] = 3
+    live = np.flatnonzero(st)
+    pick = lambda k: rng.choice(live, k)
+    sa_idx, sx_idx = pick(n), pick(q)
+    sa, sb, xa, xb = ta[sa_idx], tb[sa_idx], ta[sx_idx], tb[sx_idx]
+    ss = (rng.integers(0, 3, n) > 0).astype(np.uint32)
+    ss[[3, 4]] = 2
+    sx = (rng.integers(0, 3, q) > 0).astype(np.uint32)
+    junk = ss == 0
+    sa[junk], sb[junk] = rnd(int(junk.sum())), rnd(int(junk.sum()))
+    sa[0], sb[0], ss[0] = ta[7], tb[7], 1  # weight on the row whose selector is 3
+    if not present:
+        sb[1], ss[1] = (int(sb[1]) + 1) % F.P, 1
+    trace.update({"TA_0": ta, "TB_0": tb, "ST_0": st, "SA_0": sa, "SB_0": sb, "SS_0": ss,
+                  "XA_0": xa, "XB_0": xb, "SX_0": sx})
+    lookup_tuple(b, [([col("SA_0"), col("SB_0")], "lookA_0"), ([col("XA_0"), col("XB_0")], "lookB_0")],
+                 [([col("TA_0"), col("TB_0")], "table_0")], sel_s=[col("SS_0"), col("SX_0")], sel_t=[col("ST_0")])
+    trace.update(b.generated)
+    comp = b.compile()
+    wit = [np.ascontiguousarray(trace[nm], dtype=np.uint32) for (nm, f, r) in comp.witness_columns]
+    return comp, wit
+
+
 def mixed_sizes(n_modules: int, lo: int, hi: int, seed: int) -> List[int]:
     """log2 module sizes drawn uniformly from [lo, hi] (seeded)."""
     rng = np.random.Generator(np.random.PCG64([seed, 0x5A5E]))

@@ -32,7 +32,7 @@ ROUND_FOLD, ROUND_LOG_DERIVATIVE, ROUND_RUNNING_SUMS = 0, 1, 2
 BASE, EXT = 0, 1
 KIND_WITNESS, KIND_STEP, KIND_LAGRANGE, KIND_SETUP = 0, 1, 2, 3
 OP_COL, OP_COIN, OP_CONST, OP_ADD, OP_SUB, OP_MUL, OP_EXPAVG, OP_EXPVAL = range(8)
-STEP_GP, STEP_MULT, STEP_LOGUP, STEP_RATIO = 0, 1, 2, 3
+STEP_GP, STEP_MULT, STEP_LOGUP, STEP_RATIO, STEP_MULTW = 0, 1, 2, 3, 4
 MAGIC = 0x3150474C
 RANGE_MODULE, LOGUP = "range", "logup"  # internal/constants/const.go:34,41
 MAX_LOGUP_DEGREE, MAX_LOGUP_BATCH = 5, 4  # board/logup.go:37, arguments/lookup.go:156
@@ -173,6 +173,20 @@ class MultiplicityStep:
 
 
 @dataclass
+class TupleMultiplicityStep:
+    """board/board.go:235-249 in general: tables of `width` expressions, with
+    optional selectors (None: every row counts); one multiplicity column per
+    target table."""
+    round: int
+    width: int
+    sources: List[List[Expr]]
+    targets: List[List[Expr]]
+    sel_s: Optional[List[Expr]]
+    sel_t: Optional[List[Expr]]
+    outs: List[str]
+
+
+@dataclass
 class LogupStep:
     """board/logup.go:80-127: a cyclic logup column and its exposed total."""
     round: int
@@ -251,6 +265,20 @@ class Builder:
         self._grow(r)
         outs = [f"{output}_{i}" for i in range(len(T))]
         self.rounds[r]["steps"].append(MultiplicityStep(r, list(S), list(T), outs))
+        return outs
+
+    def add_tuple_multiplicity_step(self, r: int, sel_s, sel_t, S: Sequence[Sequence[Expr]],
+                                    T: Sequence[Sequence[Expr]], output: str) -> List[str]:
+        """Tables of any width, with optional selectors (board/board.go:235-249,
+        internal/poly/lookup_multiplicity.go:37-100); outs "<output>_<i>"."""
+        widths = {len(t) for t in list(S) + list(T)}
+        if len(widths) != 1:
+            raise ValueError("lookup: inconsistent width")
+        self._grow(r)
+        outs = [f"{output}_{i}" for i in range(len(T))]
+        self.rounds[r]["steps"].append(TupleMultiplicityStep(
+            r, widths.pop(), [list(x) for x in S], [list(x) for x in T], None if sel_s is None else list(sel_s),
+            None if sel_t is None else list(sel_t), outs))
         return outs
 
     def add_cyclic_logup_step(self, r: int, module: str, terms: Sequence[Tuple[Expr, Expr]], output: str) -> str:
@@ -334,7 +362,7 @@ class Builder:
         step_out = {}
         for rd in self.rounds:
             for s_ in rd["steps"]:
-                for o in (s_.outs if isinstance(s_, MultiplicityStep) else [s_.out]):
+                for o in (s_.outs if isinstance(s_, (MultiplicityStep, TupleMultiplicityStep)) else [s_.out]):
                     step_out[o] = s_
         exposed = []  # exposed values in step order (board/logup.go:183-191)
         for rd in self.rounds:
@@ -381,7 +409,7 @@ class Builder:
                     fields[s_.out] = max(field_of(s_.num, fields), field_of(s_.den, fields))
                 elif isinstance(s_, (LogupStep, RunningRatioStep)):
                     fields[s_.out] = EXT
-                else:
+                else:  # multiplicity columns
                     for o in s_.outs:
                         fields[o] = BASE
         columns: List[Tuple[str, int, int, int, int]] = []  # name, module idx, field, kind, param
@@ -439,6 +467,12 @@ class Builder:
                 elif isinstance(s_, MultiplicityStep):
                     steps.append((STEP_MULT, s_.round, len(s_.sources), len(s_.targets),
                                   *[emit(x) for x in s_.sources], *[emit(x) for x in s_.targets],
+                                  *[col_idx[o] for o in s_.outs]))
+                elif isinstance(s_, TupleMultiplicityStep):
+                    flags = (s_.sel_s is not None) | ((s_.sel_t is not None) << 1)
+                    steps.append((STEP_MULTW, s_.round, s_.width, len(s_.sources), len(s_.targets), flags,
+                                  *[emit(x) for x in (s_.sel_s or [])], *[emit(x) for x in (s_.sel_t or [])],
+                                  *[emit(x) for t in s_.sources for x in t], *[emit(x) for t in s_.targets for x in t],
                                   *[col_idx[o] for o in s_.outs]))
                 else:
                     w_ = [STEP_LOGUP, s_.round, mod_idx[s_.module], col_idx[s_.out], len(s_.terms)]
@@ -540,6 +574,38 @@ def lookup(b: "Builder", S: Sequence[Tuple[Expr, str]], T: Sequence[Tuple[Expr, 
     terms += [(mod, e - gamma, minus_one * col(outs[i])) for i, (e, mod) in enumerate(T)]
     totals = add_logup_columns(b, f"{LOGUP}_", terms)
     b.logup_buses.append(list(totals))  # arguments/lookup.go:177
+    return totals
+
+
+def lookup_tuple(b: "Builder", S: Sequence[Tuple[Sequence[Expr], str]], T: Sequence[Tuple[Sequence[Expr], str]],
+                 sel_s: Optional[Sequence[Expr]] = None, sel_t: Optional[Sequence[Expr]] = None):
+    """arguments/lookup.go:60-110 LookupUnionTuple / CLookupUnionTuple: the
+    rows of the source tables (tuples of expressions, with their module)
+    whose selector is non-zero lie among the selected rows of the target
+    tables.  Multiplicities are counted on the raw tuples at RoundFold; the
+    logup folds each tuple with alpha = Coin(RoundFold), fractions
+    sel_s/(s - gamma) and -m sel_t/(t - gamma)."""
+    if sel_s is not None and len(sel_s) != len(S):
+        raise ValueError("lookup: one source selector per source table")
+    if sel_t is not None and len(sel_t) != len(T):
+        raise ValueError("lookup: one target selector per target table")
+    mult = b.fresh_name("Mult_")
+    for t, _ in list(S) + list(T):
+        b.stage_leaves(ROUND_FOLD, *t)
+    b.stage_leaves(ROUND_FOLD, *(sel_s or []))
+    b.stage_leaves(ROUND_FOLD, *(sel_t or []))
+    outs = b.add_tuple_multiplicity_step(ROUND_FOLD, sel_s, sel_t, [t for t, _ in S], [t for t, _ in T], mult)
+    b.stage_columns(ROUND_FOLD, *outs)
+    alpha, gamma, minus_one = coin(ROUND_FOLD), coin(ROUND_LOG_DERIVATIVE), const(F.P - 1)
+
+    def folded(t):  # arguments/lookup.go:232-244
+        return t[0] if len(t) == 1 else fold(alpha, list(t))
+
+    terms = [(mod, folded(t) - gamma, const(1) if sel_s is None else sel_s[i]) for i, (t, mod) in enumerate(S)]
+    terms += [(mod, folded(t) - gamma, minus_one * (col(outs[i]) if sel_t is None else col(outs[i]) * sel_t[i]))
+              for i, (t, mod) in enumerate(T)]
+    totals = add_logup_columns(b, f"{LOGUP}_", terms)
+    b.logup_buses.append(list(totals))
     return totals
 
 

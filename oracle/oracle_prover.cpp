@@ -69,6 +69,17 @@ Program parse_program(const uint32_t* w, size_t n) {
       for (uint32_t k = 0; k < a; k++) s.src.push_back(node());
       for (uint32_t k = 0; k < b; k++) s.tgt.push_back(node());
       for (uint32_t k = 0; k < b; k++) s.outs.push_back(column());
+    } else if (s.type == STEP_MULTW) {
+      s.width = rd();
+      uint32_t a = rd(), b = rd();
+      s.flags = rd();
+      if (!s.width || s.width > 8 || !a || !b || a > 4096 || b > 4096 || s.flags > 3)
+        throw std::runtime_error("program: bad tuple multiplicity step");
+      if (s.flags & 1) for (uint32_t k = 0; k < a; k++) s.sel_s.push_back(node());
+      if (s.flags & 2) for (uint32_t k = 0; k < b; k++) s.sel_t.push_back(node());
+      for (uint32_t k = 0; k < a * s.width; k++) s.src.push_back(node());
+      for (uint32_t k = 0; k < b * s.width; k++) s.tgt.push_back(node());
+      for (uint32_t k = 0; k < b; k++) s.outs.push_back(column());
     } else if (s.type == STEP_LOGUP) {
       s.module = rd(); s.out = column();
       uint32_t t = rd();

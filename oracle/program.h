@@ -26,6 +26,11 @@
 //               (E_node, M_node)[n_terms]; its total is exposed
 //             type 3 running ratio: 3, round, module, num_node, den_node,
 //               out_col; its end is exposed (board/product.go:72-198)
+//             type 4 lookup multiplicities of tuples with optional selectors:
+//               4, round, width, n_src, n_tgt, flags (bit 0: source
+//               selectors, bit 1: target selectors), src_sel[n_src],
+//               tgt_sel[n_tgt] (when flagged), src nodes [n_src x width],
+//               tgt nodes [n_tgt x width], out_col[n_tgt]
 //             Exposed values are numbered in step order over types 2 and 3.
 //   round   : n_staged, col[n_staged]
 //   str     : byte length, then the bytes packed 4 per word
@@ -37,7 +42,7 @@
 namespace orc {
 
 enum { OP_COL = 0, OP_COIN = 1, OP_CONST = 2, OP_ADD = 3, OP_SUB = 4, OP_MUL = 5, OP_EXPAVG = 6, OP_EXPVAL = 7 };
-enum { STEP_GP = 0, STEP_MULT = 1, STEP_LOGUP = 2, STEP_RATIO = 3 };
+enum { STEP_GP = 0, STEP_MULT = 1, STEP_LOGUP = 2, STEP_RATIO = 3, STEP_MULTW = 4 };
 enum { KIND_WITNESS = 0, KIND_STEP = 1, KIND_LAGRANGE = 2, KIND_SETUP = 3 };
 
 struct PModule { uint32_t log_n; std::string name; std::vector<uint32_t> rels; };
@@ -45,7 +50,9 @@ struct PColumn { std::string name; uint32_t module, field, kind; int32_t param; 
 struct PNode { uint32_t op, a, b; };
 struct PStep {
   uint32_t type, round, module = 0, num = 0, den = 0, out = 0;
-  std::vector<uint32_t> src, tgt, outs;   // multiplicities
+  std::vector<uint32_t> src, tgt, outs;   // multiplicities (type 4: width nodes per table, table-major)
+  uint32_t width = 1, flags = 0;          // type 4: tuple width; bit 0 source selectors, bit 1 target selectors
+  std::vector<uint32_t> sel_s, sel_t;     // type 4 selectors
   std::vector<uint32_t> e, m;             // logup terms M/E
   uint32_t exposed = 0;                   // logup: index of its exposed total
 };

@@ -411,6 +411,60 @@ struct Prover {
       if (!assigned.count(kv.first) && kv.second) throw std::runtime_error("lookup: source value not in the table");
   }
 
+  // Lookup multiplicities of tuples with selectors
+  // (internal/poly/lookup_multiplicity.go:37-100): the selected weight of
+  // every source tuple (compared on its base-field values) goes to its first
+  // target row with a non-zero selector, divided by that selector; a
+  // selected source tuple found in no target is an error.
+  void run_multiplicities_tuple(const PStep& st) {
+    const uint32_t W = st.width;
+    auto table = [&](const std::vector<uint32_t>& nodes_, size_t k, std::vector<std::vector<uint32_t>>& cols) {
+      uint32_t mod = expr_module(nodes_[k * W]);
+      cols.clear();
+      for (uint32_t w = 0; w < W; w++) {
+        if (expr_module(nodes_[k * W + w]) != mod) throw std::runtime_error("lookup: a tuple spans modules");
+        cols.push_back(eval_base_rows(nodes_[k * W + w], mod));
+      }
+      return mod;
+    };
+    auto selector = [&](const std::vector<uint32_t>& sels, size_t k, uint32_t mod) {
+      if (sels.empty()) return std::vector<uint32_t>(mod_n(mod), 1);
+      if (expr_module(sels[k]) != mod) throw std::runtime_error("lookup: selector of another module");
+      return eval_base_rows(sels[k], mod);
+    };
+    std::map<std::vector<uint32_t>, uint32_t> weight;
+    std::vector<std::vector<uint32_t>> cols;
+    for (size_t k = 0; k < st.src.size() / W; k++) {
+      uint32_t mod = table(st.src, k, cols);
+      std::vector<uint32_t> sel = selector(st.sel_s, k, mod);
+      for (size_t i = 0; i < sel.size(); i++) {
+        if (!sel[i]) continue;
+        std::vector<uint32_t> key(W);
+        for (uint32_t w = 0; w < W; w++) key[w] = cols[w][i];
+        weight[key] = add(weight[key], sel[i]);
+      }
+    }
+    std::set<std::vector<uint32_t>> assigned;
+    for (size_t k = 0; k < st.outs.size(); k++) {
+      uint32_t mod = table(st.tgt, k, cols);
+      std::vector<uint32_t> sel = selector(st.sel_t, k, mod), res(sel.size(), 0);
+      for (size_t i = 0; i < sel.size(); i++) {
+        if (!sel[i]) continue;
+        std::vector<uint32_t> key(W);
+        for (uint32_t w = 0; w < W; w++) key[w] = cols[w][i];
+        auto it = weight.find(key);
+        if (it == weight.end() || assigned.count(key)) continue;
+        res[i] = mul(it->second, inv(sel[i]));
+        assigned.insert(key);
+      }
+      if (pg.columns[st.outs[k]].module != mod || pg.columns[st.outs[k]].field != 0)
+        throw std::runtime_error("multiplicity column must be a base column of its table's module");
+      base[st.outs[k]] = res;
+    }
+    for (auto& kv : weight)
+      if (kv.second && !assigned.count(kv.first)) throw std::runtime_error("lookup: source value not in the table");
+  }
+
   // Cyclic logup column (board/logup.go:129-180, internal/poly/iop_utils.go:110-131):
   // v_i = sum_j M_j(i) / E_j(i); S_i = v_0 + ... + v_i; T = S_{n-1};
   // L_i = S_i - (i + 1) T / n.  T is exposed.
@@ -487,6 +541,7 @@ struct Prover {
 
   void run_step(const PStep& st) {
     if (st.type == STEP_MULT) return run_multiplicities(st);
+    if (st.type == STEP_MULTW) return run_multiplicities_tuple(st);
     if (st.type == STEP_LOGUP) return run_logup(st);
     if (st.type == STEP_RATIO) return run_ratio(st);
     if (st.type != STEP_GP) throw std::runtime_error("unsupported step type");

@@ -143,3 +143,18 @@ def test_setup_precommit():
         oracle.verify(compiled.words, pb, 8, setup_root=bad)
     other = plonk.build_with_setup(2, 64, seed=7)[2]
     assert (oracle.setup_root(compiled.words, [F.to_mont(x) for x in other]) != root).any()
+
+
+def test_conditional_tuple_lookup():
+    """arguments.CLookupUnionTuple: width-2 tuples from two modules with
+    selectors (weights 1 and 2) into a table with a selector (values 0, 1, 3)
+    and repeated tuples; the proof verifies with its logup bus, and a selected
+    source tuple missing from the table is refused by the prover."""
+    compiled, wit = plonk.build_with_tuple_lookup(64)
+    pb = _prove(compiled, wit, 8)
+    oracle.verify(compiled.words, pb, 8, compiled.logup_buses)
+    p = proof.decode(pb)
+    assert all(v == p.final_poly[0] for v in p.final_poly)
+    compiled, wit = plonk.build_with_tuple_lookup(64, present=False)
+    with pytest.raises(RuntimeError, match="not in the table"):
+        _prove(compiled, wit, 8)
