@@ -282,7 +282,7 @@ struct Ctx {
 // Flat descriptor; the format is documented in include/loom_gpu.h.
 enum { OP_COL = 0, OP_COIN = 1, OP_CONST = 2, OP_ADD = 3, OP_SUB = 4, OP_MUL = 5, OP_EXPAVG = 6, OP_EXPVAL = 7 };
 enum { KIND_WITNESS = 0, KIND_STEP = 1, KIND_LAGRANGE = 2, KIND_SETUP = 3 };
-enum { STEP_GP = 0, STEP_MULT = 1, STEP_LOGUP = 2, STEP_RATIO = 3 };
+enum { STEP_GP = 0, STEP_MULT = 1, STEP_LOGUP = 2, STEP_RATIO = 3, STEP_MULTW = 4 };
 inline bool exposes(uint32_t step_type) { return step_type == STEP_LOGUP || step_type == STEP_RATIO; }
 inline bool is_binary(uint32_t op) { return op == OP_ADD || op == OP_SUB || op == OP_MUL; }
 struct Module { uint32_t log_n; std::string name; std::vector<uint32_t> rels; };
@@ -290,7 +290,9 @@ struct Column { std::string name; uint32_t module, field, kind; int32_t param; }
 struct Node { uint32_t op, a, b; };
 struct Step {
   uint32_t type, round, module = 0, num = 0, den = 0, out = 0;
-  std::vector<uint32_t> src, tgt, outs;  // lookup multiplicities (width-1 tables)
+  std::vector<uint32_t> src, tgt, outs;  // lookup multiplicities (type 4: `width` nodes per table)
+  uint32_t width = 1, flags = 0;         // type 4: tuple width; bit 0 source selectors, bit 1 target selectors
+  std::vector<uint32_t> sel_s, sel_t;    // type 4 selectors
   std::vector<uint32_t> e, m;            // cyclic logup: fractions m[k] / e[k]
   uint32_t exposed = 0;                  // cyclic logup / running ratio: index of its exposed value
 };
@@ -374,6 +376,17 @@ inline Program parse_program(const uint32_t* w, size_t n) {
       if (!a || !b || a > 4096 || b > 4096) throw Error(LG_ERR_INVALID, "bad multiplicity step");
       for (uint32_t k = 0; k < a; k++) s.src.push_back(node());
       for (uint32_t k = 0; k < b; k++) s.tgt.push_back(node());
+      for (uint32_t k = 0; k < b; k++) s.outs.push_back(column());
+    } else if (s.type == STEP_MULTW) {
+      s.width = rd();
+      uint32_t a = rd(), b = rd();
+      s.flags = rd();
+      if (!s.width || s.width > 8 || !a || !b || a > 4096 || b > 4096 || s.flags > 3)
+        throw Error(LG_ERR_INVALID, "bad tuple multiplicity step");
+      if (s.flags & 1) for (uint32_t k = 0; k < a; k++) s.sel_s.push_back(node());
+      if (s.flags & 2) for (uint32_t k = 0; k < b; k++) s.sel_t.push_back(node());
+      for (uint32_t k = 0; k < a * s.width; k++) s.src.push_back(node());
+      for (uint32_t k = 0; k < b * s.width; k++) s.tgt.push_back(node());
       for (uint32_t k = 0; k < b; k++) s.outs.push_back(column());
     } else if (s.type == STEP_LOGUP) {
       s.module = rd();

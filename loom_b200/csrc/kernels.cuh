@@ -817,6 +817,89 @@ __global__ void k_mult_write(const MultVec* tv, const MultTab* tabs) {
   if (i >= V.n) return;
   V.out[i] = to_mont(tabs[V.tab].count[V.comb_off + i]);
 }
+// Tuple lookups with selectors (internal/poly/lookup_multiplicity.go:37-100).
+// A step's hash table keys tuples by a representative target row whose
+// tuple sits in `keys` (w words per combined target row); per slot, the
+// first selected target row holding the tuple and the selected source weight
+// (sum of canonical selector values, 64-bit).  Probes are bounded by the
+// table size, which is at least twice the target rows.
+constexpr uint32_t TUPLE_MAX_W = 8;
+struct TupleVec { const uint32_t* comp[TUPLE_MAX_W]; const uint32_t* sel; uint32_t n, comb_off, tab; uint32_t* out; };
+struct TupleTab { uint32_t* rep; uint32_t* first; unsigned long long* weight; uint32_t* keys; uint32_t cap, w; };
+__device__ __forceinline__ uint32_t tuple_hash(const TupleVec& V, uint32_t i, uint32_t w, uint32_t mask) {
+  uint32_t h = 0x9e3779b9u;
+  for (uint32_t k = 0; k < w; k++) h = mult_hash(h ^ V.comp[k][i], 0xffffffffu) + k;
+  return mult_hash(h, mask);
+}
+__device__ __forceinline__ bool tuple_eq(const TupleVec& V, uint32_t i, const uint32_t* key, uint32_t w) {
+  for (uint32_t k = 0; k < w; k++)
+    if (V.comp[k][i] != key[k]) return false;
+  return true;
+}
+__global__ void k_tuple_keys(const TupleVec* tv, const TupleTab* tabs) {
+  const TupleVec V = tv[blockIdx.y];
+  const TupleTab T = tabs[V.tab];
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V.n) return;
+  for (uint32_t k = 0; k < T.w; k++) T.keys[(uint64_t)(V.comb_off + i) * T.w + k] = V.comp[k][i];
+}
+__global__ void k_tuple_insert(const TupleVec* tv, const TupleTab* tabs, uint32_t* fail) {
+  const TupleVec V = tv[blockIdx.y];
+  const TupleTab T = tabs[V.tab];
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V.n || (V.sel && V.sel[i] == 0)) return;
+  const uint32_t g = V.comb_off + i, mask = T.cap - 1;
+  uint32_t h = tuple_hash(V, i, T.w, mask);
+  for (uint32_t probe = 0; probe < T.cap; probe++, h = (h + 1) & mask) {
+    const uint32_t prev = atomicCAS(T.rep + h, MULT_EMPTY, g);
+    if (prev == MULT_EMPTY || tuple_eq(V, i, T.keys + (uint64_t)prev * T.w, T.w)) {
+      atomicMin(T.first + h, g);
+      return;
+    }
+  }
+  atomicOr(fail, 2u);
+}
+__global__ void k_tuple_count(const TupleVec* sv, const TupleTab* tabs, uint32_t* missing) {
+  const TupleVec V = sv[blockIdx.y];
+  const TupleTab T = tabs[V.tab];
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V.n) return;
+  const uint32_t sel = V.sel ? V.sel[i] : MONT_ONE;
+  if (sel == 0) return;
+  const uint32_t mask = T.cap - 1;
+  uint32_t h = tuple_hash(V, i, T.w, mask);
+  for (uint32_t probe = 0; probe < T.cap; probe++, h = (h + 1) & mask) {
+    const uint32_t r = T.rep[h];
+    if (r == MULT_EMPTY) break;
+    if (tuple_eq(V, i, T.keys + (uint64_t)r * T.w, T.w)) {
+      atomicAdd(T.weight + h, (unsigned long long)from_mont(sel));
+      return;
+    }
+  }
+  atomicOr(missing, 1u);
+}
+__global__ void k_tuple_write(const TupleVec* tv, const TupleTab* tabs) {
+  const TupleVec V = tv[blockIdx.y];
+  const TupleTab T = tabs[V.tab];
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V.n) return;
+  uint32_t m = 0;
+  const uint32_t sel = V.sel ? V.sel[i] : MONT_ONE;
+  if (sel != 0) {
+    const uint32_t g = V.comb_off + i, mask = T.cap - 1;
+    uint32_t h = tuple_hash(V, i, T.w, mask);
+    for (uint32_t probe = 0; probe < T.cap; probe++, h = (h + 1) & mask) {
+      const uint32_t r = T.rep[h];
+      if (r == MULT_EMPTY) break;
+      if (tuple_eq(V, i, T.keys + (uint64_t)r * T.w, T.w)) {
+        if (T.first[h] == g) m = mul(to_mont((uint32_t)(T.weight[h] % P)), V.sel ? inv(sel) : MONT_ONE);
+        break;
+      }
+    }
+  }
+  V.out[i] = m;
+}
+
 // Values of a base-field expression on every row (for lookup tables that are
 // not plain columns).
 struct EvalJob { XProgram p; const uint32_t* const* lanes; uint32_t* out; int logn; };

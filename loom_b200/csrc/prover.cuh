@@ -619,6 +619,102 @@ struct Prover {
     if (*h) throw Error(LG_ERR_INVALID, "lookup: a source value is not in its table");
   }
 
+  // Lookup multiplicities of tuples with optional selectors, all type-4 steps
+  // of a round in one set of launches: target tuples into `keys`, insertion
+  // (first selected row per tuple), selected source weights, multiplicity
+  // columns (k_tuple_*).
+  void run_tuple_multiplicities(const std::vector<const Step*>& steps, const DBufP& coins_d) {
+    std::vector<DBufP> keep;
+    std::vector<EvalJob> evals;
+    uint32_t eval_regs = 1, eval_n = 0;
+    auto values = [&](uint32_t root, uint32_t mod) -> const uint32_t* {
+      const Node& x = pg.nodes[root];
+      const uint32_t n = (uint32_t)mod_n(mod);
+      if (expr_module(root) != mod) throw Error(LG_ERR_INVALID, "lookup: a table spans modules");
+      if (x.op == OP_COL && x.b == 0 && pg.columns[x.a].field == 0 && col_buf.count(x.a)) return lane_ptr(x.a, 0);
+      if (ext_of[root]) throw Error(LG_ERR_INVALID, "lookup tuples and selectors must be base-field");
+      LaneTable lt{this, {}, {}};
+      const CodeSet& cs = compiled("e" + std::to_string(root), lt, {root});
+      auto tab = upload_vec(c, lt.lanes);
+      auto out = std::make_shared<DBuf>(n, c.stream);
+      keep.insert(keep.end(), {tab, out});
+      evals.push_back(EvalJob{cs.dev[0], (const uint32_t* const*)tab->p, out->p, (int)pg.modules[mod].log_n});
+      eval_regs = std::max(eval_regs, cs.xc[0].n_regs);
+      eval_n = std::max(eval_n, n);
+      return out->p;
+    };
+    std::vector<TupleTab> tabs;
+    std::vector<TupleVec> tv, sv;
+    uint32_t max_t = 1, max_s = 1;
+    for (const Step* st : steps) {
+      const uint32_t W = st->width, tab = (uint32_t)tabs.size();
+      auto table = [&](const std::vector<uint32_t>& nodes_, size_t k, const std::vector<uint32_t>& sels) {
+        TupleVec V{};
+        const uint32_t mod = expr_module(nodes_[k * W]);
+        V.n = (uint32_t)mod_n(mod);
+        for (uint32_t w = 0; w < W; w++) V.comp[w] = values(nodes_[k * W + w], mod);
+        V.sel = sels.empty() ? nullptr : values(sels[k], mod);
+        V.tab = tab;
+        return V;
+      };
+      uint32_t comb = 0;
+      for (size_t k = 0; k < st->outs.size(); k++) {
+        TupleVec V = table(st->tgt, k, st->sel_t);
+        const uint32_t out = st->outs[k];
+        if (pg.columns[out].field != 0 || mod_n(pg.columns[out].module) != V.n)
+          throw Error(LG_ERR_INVALID, "multiplicity column must be a base column of its table's module");
+        auto b = std::make_shared<DBuf>(V.n, c.stream);
+        col_buf[out] = b;
+        V.out = b->p;
+        V.comb_off = comb;
+        comb += V.n;
+        max_t = std::max(max_t, V.n);
+        tv.push_back(V);
+      }
+      for (size_t k = 0; k < st->src.size() / W; k++) {
+        TupleVec V = table(st->src, k, st->sel_s);
+        max_s = std::max(max_s, V.n);
+        sv.push_back(V);
+      }
+      uint32_t cap = 64;
+      while (cap < 2 * comb) cap <<= 1;
+      auto mem = std::make_shared<DBuf>((size_t)4 * cap + (size_t)comb * W, c.stream);
+      keep.push_back(mem);
+      LG_CK(cudaMemsetAsync(mem->p, 0xff, (size_t)2 * cap * 4, c.stream));
+      LG_CK(cudaMemsetAsync(mem->p + 2 * (size_t)cap, 0, (size_t)2 * cap * 4, c.stream));
+      tabs.push_back(TupleTab{mem->p, mem->p + cap, (unsigned long long*)(mem->p + 2 * (size_t)cap),
+                              mem->p + 4 * (size_t)cap, cap, W});
+    }
+    auto flags = std::make_shared<DBuf>(1, c.stream);
+    LG_CK(cudaMemsetAsync(flags->p, 0, 4, c.stream));
+    auto tabs_d = upload_vec(c, tabs), tv_d = upload_vec(c, tv), sv_d = upload_vec(c, sv);
+    c.timed("lookup_multiplicities", 0, 0, [&] {
+      if (!evals.empty()) {
+        auto ed = upload_vec(c, evals);
+        keep.push_back(ed);
+        const int T = 128;
+        size_t smem = (size_t)eval_regs * 6 * T * 4;
+        allow_smem(k_eval_base, smem);
+        k_eval_base<<<dim3((eval_n + T - 1) / T, (unsigned)evals.size()), T, smem, c.stream>>>(
+            (const EvalJob*)ed->p, (const E6*)coins_d->p);
+        LG_LAUNCH();
+      }
+      const dim3 gt((max_t + 255) / 256, (unsigned)tv.size()), gs((max_s + 255) / 256, (unsigned)sv.size());
+      k_tuple_keys<<<gt, 256, 0, c.stream>>>((const TupleVec*)tv_d->p, (const TupleTab*)tabs_d->p);
+      LG_LAUNCH();
+      k_tuple_insert<<<gt, 256, 0, c.stream>>>((const TupleVec*)tv_d->p, (const TupleTab*)tabs_d->p, flags->p);
+      LG_LAUNCH();
+      k_tuple_count<<<gs, 256, 0, c.stream>>>((const TupleVec*)sv_d->p, (const TupleTab*)tabs_d->p, flags->p);
+      LG_LAUNCH();
+      k_tuple_write<<<gt, 256, 0, c.stream>>>((const TupleVec*)tv_d->p, (const TupleTab*)tabs_d->p);
+      LG_LAUNCH();
+    });
+    uint32_t* h = c.host_staging(1);
+    c.d2h(h, flags->p, 1);
+    if (*h & 2) throw Error(LG_ERR_INVALID, "lookup: hash table full");
+    if (*h & 1) throw Error(LG_ERR_INVALID, "lookup: a source value is not in its table");
+  }
+
   // Cyclic logup columns and their totals (board/logup.go:129-180): one set of
   // launches over all logup steps of a round (batched) or one per step.
   void run_logups(const std::vector<const Step*>& steps, const DBufP& coins_d) {
@@ -703,11 +799,14 @@ struct Prover {
   }
 
   void run_steps(uint32_t r) {
-    std::vector<const Step*> steps, gps, mults, logups;
+    std::vector<const Step*> steps, gps, mults, tmults, logups;
     for (const Step& st : pg.steps) {
       if (st.round != r) continue;
       steps.push_back(&st);
-      (st.type == STEP_GP || st.type == STEP_RATIO ? gps : st.type == STEP_MULT ? mults : logups).push_back(&st);
+      (st.type == STEP_GP || st.type == STEP_RATIO ? gps
+       : st.type == STEP_MULT                      ? mults
+       : st.type == STEP_MULTW                     ? tmults
+                                                   : logups).push_back(&st);
     }
     if (!exposed_d && n_exposed()) exposed_d = std::make_shared<DBuf>(6 * n_exposed(), c.stream);
     if (steps.empty()) return;
@@ -715,6 +814,7 @@ struct Prover {
     // steps of one round read only earlier rounds' columns; multiplicities,
     // grand products and logups are independent of each other
     if (!mults.empty()) run_multiplicities(mults, coins_d);
+    if (!tmults.empty()) run_tuple_multiplicities(tmults, coins_d);
     if (!logups.empty()) run_logups(logups, coins_d);
     steps = gps;
     if (steps.empty()) return;

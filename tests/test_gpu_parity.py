@@ -258,6 +258,30 @@ def test_prove_with_setup_equals_oracle(ctx, n_inst, logn, batched):
     oracle.verify(compiled.words, got, 12, setup_root=want_root)
 
 
+@pytest.mark.parametrize("batched", [True, False])
+@pytest.mark.parametrize("logn", [6, 12])
+def test_prove_tuple_lookup_equals_oracle(ctx, logn, batched):
+    """arguments.CLookupUnionTuple on the GPU: width-2 tuples from two modules
+    with selectors of weight 1 and 2 into a table with selectors 0, 1, 3 and
+    repeated tuples (device hash table on tuples, 64-bit weights)."""
+    compiled, wit = plonk.build_with_tuple_lookup(1 << logn, seed=logn)
+    mont = [F.to_mont(w) for w in wit]
+    ctx.set_batched(batched)
+    try:
+        got = ctx.prove(compiled.words, mont, 12)
+    finally:
+        ctx.set_batched(True)
+    assert got == oracle.prove(compiled.words, mont, 12)
+    oracle.verify(compiled.words, got, 12, compiled.logup_buses)
+
+
+def test_prove_tuple_lookup_missing_tuple_is_refused(ctx):
+    compiled, wit = plonk.build_with_tuple_lookup(1 << 6, present=False)
+    with pytest.raises(LoomError) as e:
+        ctx.prove(compiled.words, [F.to_mont(w) for w in wit], 4)
+    assert e.value.code == 1 and "not in its table" in str(e.value)
+
+
 def test_prove_without_setup_is_refused(ctx):
     compiled, wit, setup = plonk.build_with_setup(1, 1 << 5, seed=3)
     with pytest.raises(LoomError) as e:
