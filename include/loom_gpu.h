@@ -48,6 +48,12 @@
  *             module, numerator node, denominator node, output column; its
  *             end is exposed.  Exposed values are numbered in step order
  *             over types 2 and 3.
+ *             type 4 lookup multiplicities of tuples with optional selectors
+ *             (internal/poly/lookup_multiplicity.go:37-100): 4, round, width
+ *             (<= 8), n_src, n_tgt, flags (bit 0 source selectors, bit 1
+ *             target selectors), source selector nodes, target selector
+ *             nodes (when flagged), source nodes (width per table), target
+ *             nodes (width per table), output column per target
  *   round   : n_staged, staged column indices (board.Compile's order,
  *             including the sweep of unstaged columns into the last round)
  *   str     : byte length, then the bytes packed 4 per word
