@@ -137,6 +137,18 @@ int lg_prove(lg_ctx* ctx, const char* hash_backend, const uint32_t* program, siz
              const uint32_t* const* witness, int witness_on_device, uint32_t num_queries, uint8_t* proof,
              size_t* proof_len);
 int lg_last_proof(lg_ctx* ctx, uint8_t* proof, size_t* proof_len);
+/* verifier.Verify (verifier/verifier.go:487-533) of proof bytes in the
+ * canonical encoding against the program: transcript replay, buses, the AIR
+ * relation at zeta and the FRI fold chains on the host; every Merkle opening
+ * (committed batches with their injected groups, the levels tree, the FRI
+ * layers) and the DEEP bridge of every query on the GPU.  `setup_root` (8
+ * Montgomery words) is the verification key of a program with setup columns,
+ * NULL otherwise; `buses` (may be NULL) lists product and logup buses as
+ * "P:end,end;L:total,total,..." (board.Program's ProductBus and LogupBus).
+ * Returns LG_OK when the proof is accepted; LG_ERR_INVALID with the reason in
+ * lg_last_error() ("proof rejected: ...") when it is not. */
+int lg_verify(lg_ctx* ctx, const uint32_t* program, size_t program_words, const uint8_t* proof, size_t proof_len,
+              uint32_t num_queries, const uint32_t* setup_root, const char* buses);
 /* setup.Setup (setup/setup.go:68-124) for a program with setup columns
  * (column kind 3: circuit constants such as selectors and permutations):
  * commits them, base field only, passed in descriptor order, into the setup

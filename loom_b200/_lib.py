@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(HERE, "libloom_gpu.so")
 
 LG_OK, LG_ERR_INVALID, LG_ERR_CUDA, LG_ERR_OOM, LG_ERR_UNSUPPORTED, LG_ERR_BUFFER = range(6)
 EXPORTS = ["lg_ctx_create", "lg_ctx_destroy", "lg_ctx_set_batched", "lg_ctx_set_leaf_mapping", "lg_ctx_set_tuning",
-           "lg_ctx_get_tuning", "lg_mem_info", "lg_last_error", "lg_prove", "lg_last_proof", "lg_setup", "lg_commit_root",
+           "lg_ctx_get_tuning", "lg_mem_info", "lg_last_error", "lg_prove", "lg_last_proof", "lg_setup", "lg_verify", "lg_commit_root",
            "lg_rs_encode", "lg_poseidon2_permute", "lg_merkle_root", "lg_fri_fold", "lg_timer_mark",
            "lg_timer_elapsed", "lg_kernel_launches", "lg_profile", "lg_profile_report", "lg_grand_product", "lg_grand_product_noalloc", "lg_deep_quotient"]
 
@@ -56,6 +56,8 @@ def load():
                                ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_size_t)]
         L.lg_last_proof.argtypes = [vp, ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_size_t)]
         L.lg_setup.argtypes = [vp, u32p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_int, u32p]
+        L.lg_verify.argtypes = [vp, u32p, ctypes.c_size_t, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_uint32, u32p,
+                                ctypes.c_char_p]
         L.lg_commit_root.argtypes = [vp, ctypes.c_uint32, u64p, u32p, u32p, ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, u32p]
         L.lg_rs_encode.argtypes = [vp, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_int]
         L.lg_poseidon2_permute.argtypes = [vp, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int]
@@ -166,6 +168,17 @@ class Context:
         self._check(self.L.lg_setup(self.h, prog.ctypes.data_as(u32p), prog.size, ctypes.cast(arr, ctypes.c_void_p),
                                     int(on_device), root.ctypes.data_as(u32p)))
         return root
+
+    def verify(self, program_words: np.ndarray, proof_bytes: bytes, num_queries: int, logup_buses=(),
+               product_buses=(), setup_root=None) -> None:
+        """verifier.Verify on the GPU; raises LoomError (code 1, "proof
+        rejected: ...") when the proof does not verify.  `setup_root`: the
+        verification key (Montgomery words) of a program with setup columns."""
+        prog = _u32(program_words)
+        spec = ";".join(["P:" + ",".join(b) for b in product_buses] + ["L:" + ",".join(b) for b in logup_buses])
+        root = None if setup_root is None else _u32(setup_root)
+        self._check(self.L.lg_verify(self.h, prog.ctypes.data_as(u32p), prog.size, bytes(proof_bytes), len(proof_bytes),
+                                     num_queries, None if root is None else root.ctypes.data_as(u32p), spec.encode()))
 
     def prove(self, program_words: np.ndarray, witness: Sequence, num_queries: int, on_device: bool = False,
               hash_backend: str = "poseidon2") -> bytes:

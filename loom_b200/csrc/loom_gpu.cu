@@ -2,6 +2,7 @@
 // unit: every kernel and host component is included here.
 #include "../../include/loom_gpu.h"
 #include "prove_flow.cuh"
+#include "verify.cuh"
 
 using namespace lg;
 
@@ -199,6 +200,18 @@ int lg_setup(lg_ctx* ctx, const uint32_t* program, size_t program_words, const u
     pr.precommit(setup_cols, on_device != 0);
     LG_CK(cudaStreamSynchronize(ctx->c.stream));
     memcpy(root, pr.prog->setup->root.v, 32);
+  });
+}
+
+int lg_verify(lg_ctx* ctx, const uint32_t* program, size_t program_words, const uint8_t* proof, size_t proof_len,
+              uint32_t num_queries, const uint32_t* setup_root, const char* buses) {
+  return guarded(ctx, [&] {
+    if (!program || !proof) throw Error(LG_ERR_INVALID, "null argument");
+    ArenaScope arena(&ctx->c.dev_arena);
+    ProofVerifier v(ctx->c, program, program_words, num_queries);
+    Digest root{};
+    if (setup_root) memcpy(root.v, setup_root, 32);
+    v.verify(proof, proof_len, setup_root ? &root : nullptr, buses);
   });
 }
 
