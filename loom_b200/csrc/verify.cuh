@@ -498,16 +498,21 @@ struct ProofVerifier {
     return o;
   }
   // a Merkle job; groups: (lo words, hi words, nb, ne, log2 pair width)
-  struct JGroup { std::vector<uint32_t> lo, hi; uint32_t nb, ne, logw; };
-  static std::vector<uint32_t> words_of(const E6& e) { return std::vector<uint32_t>(e.c, e.c + 6); }
+  // (the rows stay where the decoder put them; they are copied once, here)
+  struct JGroup { const uint32_t* lo; const uint32_t* hi; uint32_t nb, ne, logw; };
+  std::vector<uint64_t> last_rows;  // word offset of each group's lo row in the last job
+  DBufP words_d;                    // `words` on the device (path jobs, then the bridge)
   void add_path_job(const std::vector<JGroup>& gs, const VPath& p, const std::vector<Digest>* inj, const Digest& root,
                     const std::string& what) {
     if (gs.size() > VJ_MAX_GROUPS) reject("too many injected groups");
     VerifyJob J{};
     J.rows_off = words.size();
+    last_rows.clear();
     for (auto& g : gs) {
-      words.insert(words.end(), g.lo.begin(), g.lo.end());
-      words.insert(words.end(), g.hi.begin(), g.hi.end());
+      const size_t w = g.nb + 6 * (size_t)g.ne;
+      last_rows.push_back(words.size());
+      words.insert(words.end(), g.lo, g.lo + w);
+      words.insert(words.end(), g.hi, g.hi + w);
     }
     J.sib_off = push_digests(p.sib);
     J.inj_off = inj && !inj->empty() ? push_digests(*inj) : ~0ull;
@@ -547,9 +552,13 @@ struct ProofVerifier {
       level_of[idx[l]] = l;
     }
     fri_verify();
+    c.phase("verify: FRI queries");
     point_samplings();
+    c.phase("verify: opening jobs");
     run_path_jobs();
+    c.phase("verify: Merkle openings (GPU)");
     bridge();
+    c.phase("verify: DEEP bridge");
   }
 
   void fri_verify() {
@@ -607,14 +616,14 @@ struct ProofVerifier {
         if (layer.field != 1) reject("FRI: query layer is not an extension layer");
         if (layer.row != row) reject("FRI: query row differs from the transcript's");
         if (layer.path.leaf_idx != lo / 2) reject("FRI: path opens the wrong pair");
-        std::vector<JGroup> gs = {{words_of(layer.p), words_of(layer.q), 0, 1, (uint32_t)(LOG_N_FRI - j - 1)}};
+        std::vector<JGroup> gs = {{layer.p.c, layer.q.c, 0, 1, (uint32_t)(LOG_N_FRI - j - 1)}};
         if (j == r0) {  // levels tree: every other level's pair is an injection
           for (size_t l = 1; l < L; l++) {
             const VLayer& ld = lq[l - 1][k];
             if (ld.field != 1) reject("FRI: level query is not an extension layer");
             if (ld.path.leaf_idx || !ld.path.sib.empty() || !ld.path.inj.empty()) reject("FRI: level query carries a path");
             if (ld.row != (s >> levels[l].intro)) reject("FRI: level query row differs from the transcript's");
-            gs.push_back({words_of(ld.p), words_of(ld.q), 0, 1, (uint32_t)lg2((levels[l].d << RATE_LOG) / 2)});
+            gs.push_back({ld.p.c, ld.q.c, 0, 1, (uint32_t)lg2((levels[l].d << RATE_LOG) / 2)});
           }
           if (!layer.path.inj.empty()) reject("FRI: levels path carries injection leaves");
           add_path_job(gs, layer.path, nullptr, fr[j], "FRI levels tree at query " + std::to_string(k));
@@ -650,22 +659,30 @@ struct ProofVerifier {
     }
   }
 
-  std::vector<size_t> injection_order(size_t t) const {
-    const auto& G = lay.trees[t].groups;
-    std::vector<size_t> o(G.size());
-    for (size_t i = 0; i < o.size(); i++) o[i] = i;
-    std::stable_sort(o.begin(), o.end(), [&](size_t a, size_t b) { return mod_n(G[a].module) > mod_n(G[b].module); });
-    return o;
+  // per tree: groups in decreasing row count, ties in declaration order
+  // (the leaf level first, then the injected groups), and each group's place
+  std::vector<std::vector<size_t>> inj_ord, inj_at;
+  void injection_orders() {
+    for (const auto& T : lay.trees) {
+      std::vector<size_t> o(T.groups.size()), at(T.groups.size());
+      for (size_t i = 0; i < o.size(); i++) o[i] = i;
+      std::stable_sort(o.begin(), o.end(), [&](size_t a, size_t b) { return mod_n(T.groups[a].module) > mod_n(T.groups[b].module); });
+      for (size_t i = 0; i < o.size(); i++) at[o[i]] = i;
+      inj_ord.push_back(o);
+      inj_at.push_back(at);
+    }
   }
 
+  std::vector<std::vector<std::vector<uint64_t>>> row_off;  // query, tree, place in injection order -> lo row
   void point_samplings() {
     if (ps.size() != nq) reject("point samplings: wrong number of queries");
+    row_off.assign(nq, std::vector<std::vector<uint64_t>>(lay.trees.size()));
     for (uint32_t k = 0; k < nq; k++) {
       if (ps[k].size() != lay.trees.size()) reject("point samplings: wrong number of batches");
       for (size_t t = 0; t < lay.trees.size(); t++) {
         const VSample& sp = ps[k][t];
         const auto& G = lay.trees[t].groups;
-        const std::vector<size_t> ord = injection_order(t);
+        const std::vector<size_t>& ord = inj_ord[t];
         if (sp.inj.size() != ord.size() - 1) reject("point samplings: wrong number of injected groups");
         auto width_ok = [&](const VRow& r, const Prover::Group& g) { return r.nb == g.bcols.size() && r.ne == g.ecols.size(); };
         if (!width_ok(sp.top_lo, G[ord[0]]) || !width_ok(sp.top_hi, G[ord[0]])) reject("point samplings: top row width");
@@ -674,7 +691,7 @@ struct ProofVerifier {
         if (sp.path.leaf_idx != tlo / 2) reject("point samplings: path opens the wrong pair");
         if (sp.path.sib.size() != (size_t)lg2(top_rows / 2)) reject("point samplings: path depth");
         if (!sp.path.inj.empty() && sp.path.inj.size() != ord.size() - 1) reject("point samplings: injection leaves count");
-        std::vector<JGroup> gs = {{sp.top_lo.w, sp.top_hi.w, sp.top_lo.nb, sp.top_lo.ne, (uint32_t)lg2(top_rows / 2)}};
+        std::vector<JGroup> gs = {{sp.top_lo.w.data(), sp.top_hi.w.data(), sp.top_lo.nb, sp.top_lo.ne, (uint32_t)lg2(top_rows / 2)}};
         for (size_t i = 1; i < ord.size(); i++) {
           const auto& rows = sp.inj[i - 1];
           if (!width_ok(rows.first, G[ord[i]]) || !width_ok(rows.second, G[ord[i]])) reject("point samplings: injected row width");
@@ -682,16 +699,19 @@ struct ProofVerifier {
           // the injected pair sits on the path: its index is the path index at its width
           const uint64_t lo = (pos[k] >> (LOG_N_FRI - lg2(rws))) & ~1ull;
           if ((sp.path.leaf_idx >> (lg2(top_rows / 2) - lg2(rws / 2))) != lo / 2) reject("point samplings: injected pair off the path");
-          gs.push_back({rows.first.w, rows.second.w, rows.first.nb, rows.first.ne, (uint32_t)lg2(rws / 2)});
+          gs.push_back({rows.first.w.data(), rows.second.w.data(), rows.first.nb, rows.first.ne, (uint32_t)lg2(rws / 2)});
         }
         add_path_job(gs, sp.path, &sp.path.inj, roots[t], "batch " + std::to_string(t) + " at query " + std::to_string(k));
+        row_off[k][t] = last_rows;
       }
     }
   }
 
   void run_path_jobs() {
     if (pjobs.empty()) return;
-    auto wd = upload_vec(c, words), sd = upload_vec(c, shapes), jd = upload_vec(c, pjobs);
+    words_d = upload_vec(c, words);
+    auto& wd = words_d;
+    auto sd = upload_vec(c, shapes), jd = upload_vec(c, pjobs);
     auto bad = std::make_shared<DBuf>(pjobs.size(), c.stream);
     c.timed("verify_paths", 0, 0, [&] {
       k_verify_paths<<<(unsigned)((pjobs.size() + 63) / 64), 64, 0, c.stream>>>((const VerifyJob*)jd->p, (uint32_t)pjobs.size(),
@@ -711,7 +731,6 @@ struct ProofVerifier {
     std::vector<E6> cvs, zss, scales;
     std::vector<BridgeTerm> terms;
     std::vector<BridgeJob> jobs;
-    words.clear();
     struct PolyRef { size_t t, g; bool ext; size_t i; uint32_t scale; std::vector<int> shifts; uint32_t cv0; };
     std::vector<std::vector<PolyRef>> per_class(classes.size());
     std::vector<std::map<int, uint32_t>> z_index(classes.size());
@@ -749,14 +768,11 @@ struct ProofVerifier {
         J.x = mont_pow(root_of_unity_mont(lg2(rat)), bitrev32((uint32_t)lo, lg2(rat)));
         J.t0 = (uint32_t)terms.size();
         for (const PolyRef& pr : per_class[ci]) {
-          const std::vector<size_t> ord = injection_order(pr.t);
-          const size_t at = (size_t)(std::find(ord.begin(), ord.end(), pr.g) - ord.begin());
+          const size_t at = inj_at[pr.t][pr.g];
           const VSample& sp = ps[k][pr.t];
           const VRow& rlo = at == 0 ? sp.top_lo : sp.inj[at - 1].first;
-          const VRow& rhi = at == 0 ? sp.top_hi : sp.inj[at - 1].second;
-          const size_t off = pr.ext ? rlo.nb + 6 * pr.i : pr.i;
-          const uint64_t lo_off = push_words(rlo.w.data() + off, pr.ext ? 6 : 1);
-          const uint64_t hi_off = push_words(rhi.w.data() + off, pr.ext ? 6 : 1);
+          const uint64_t width = rlo.nb + 6 * (uint64_t)rlo.ne;
+          const uint64_t lo_off = row_off[k][pr.t][at] + (pr.ext ? rlo.nb + 6 * pr.i : pr.i), hi_off = lo_off + width;
           for (size_t q = 0; q < pr.shifts.size(); q++)
             terms.push_back(BridgeTerm{lo_off, hi_off, pr.ext ? 1u : 0u, pr.cv0 + (uint32_t)q, z_index[ci][pr.shifts[q]], pr.scale});
         }
@@ -767,7 +783,9 @@ struct ProofVerifier {
         J.want_q = want.q;
         jobs.push_back(J);
       }
-    auto wd = upload_vec(c, words), td = upload_vec(c, terms), jd = upload_vec(c, jobs);
+    if (!words_d) words_d = upload_vec(c, words);
+    auto& wd = words_d;
+    auto td = upload_vec(c, terms), jd = upload_vec(c, jobs);
     auto cd = upload_vec(c, cvs), zd = upload_vec(c, zss), scd = upload_vec(c, scales);
     auto bad = std::make_shared<DBuf>(jobs.size(), c.stream);
     c.timed("verify_bridge", 0, 0, [&] {
@@ -785,13 +803,17 @@ struct ProofVerifier {
   }
 
   void verify(const uint8_t* proof, size_t len, const Digest* setup_root, const char* buses) {
+    c.phase_start();
     decode(proof, len);
+    c.phase("verify: decode");
     lay.init_order();
     lay.setup_layout();
+    injection_orders();
     check_shapes(setup_root);
     derive_challenges();
     check_buses(buses);
     check_air();
+    c.phase("verify: transcript and AIR");
     pcs_verify();
   }
 };
