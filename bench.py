@@ -455,6 +455,16 @@ def main():
     # ---- the same workload with the circuit constants (selectors, copy
     # permutation, identity columns) as setup columns precommitted once
     # (setup.Setup): each proof commits only the wires and the grand product
+    # ---- verification of the headline proof (lg_verify: host transcript and
+    # checks, Merkle openings and DEEP bridge on the GPU)
+    ctx.verify(comp.words, pb, a.queries)
+    vts = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        ctx.verify(comp.words, pb, a.queries)
+        vts.append((time.perf_counter() - t0) * 1e3)
+    verify_res = {"ms": round(statistics.median(vts), 3), "accepted": True, "proof_bytes": len(pb)}
+
     setup_res = None
     if world == 1:
         scomp, swit, sset = plonk.build_with_setup(a.instances, 1 << a.log_n, seed=0x10AD)
@@ -622,6 +632,7 @@ def main():
                         "plain": [round(x, 3) for x in plain_times]},
             "c4_mixed_lookup": c4,
             "setup_precommit": setup_res,
+            "verify": verify_res,
             "tuning": tune,
             "kernel_ms_by_phase": {ph: {k: round(v["ms"], 3) for k, v in ks.items()} for ph, ks in by_phase.items()},
             "device_idle_ms": idle,
