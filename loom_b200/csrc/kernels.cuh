@@ -138,7 +138,11 @@ __global__ void k_lde(const LdeLane* lanes, int logn_rt, int from_coeffs, const 
     }
     __syncthreads();
   } else {
-    auto first = [&](uint32_t t, uint32_t r, int lo) { return L.src[bitrev32(grp_index(t, r, lo), logn)]; };
+    // the input goes to B (free until the coset transforms) with coalesced
+    // loads; the first pass gathers it in bit-reversed order from there
+    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) B[pad16(k)] = L.src[k];
+    __syncthreads();
+    auto first = [&](uint32_t t, uint32_t r, int lo) { return B[pad16(bitrev32(grp_index(t, r, lo), logn))]; };
     auto store = [&](uint32_t t, int lo, const uint32_t* v) {
 #pragma unroll
       for (uint32_t r = 0; r < 16; r++) {
