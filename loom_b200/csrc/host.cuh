@@ -149,6 +149,7 @@ struct Ctx {
   std::map<int, DBufP> tw;       // log n -> w_n^j, j < n
   std::map<int, DBufP> gpow;     // log n -> g^k, k < n
   std::map<int, DBufP> ginvpow;  // log n -> g^-k, k < n
+  std::map<int, DBufP> cshift;   // log n -> (g w_4n^c)^k, k < n, for c = 0..3 (4 tables back to back)
   // Program-constant device data kept across proves: Lagrange columns
   // (log n, row) -> values and coefficients, and the compiled bytecode of the
   // most recently proven programs (most recent first).
@@ -220,6 +221,23 @@ struct Ctx {
     k_fill_powers<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(b->p, n, g, MONT_ONE);
     LG_LAUNCH();
     m[logn] = b;
+    return b->p;
+  }
+  // Coset shifts of the quotient cosets g w_4n^c <w_n>: (g w_4n^c)^k, k < n,
+  // c = 0..3, one table after another.
+  const uint32_t* coset_shifts(int logn) {
+    auto it = cshift.find(logn);
+    if (it != cshift.end()) return it->second->p;
+    size_t n = (size_t)1 << logn;
+    ArenaScope cached(nullptr);  // kept across proves: never from the arena
+    auto b = std::make_shared<DBuf>(4 * n, stream);
+    const uint32_t w4 = root_of_unity_mont(logn + 2);
+    for (uint32_t cc = 0; cc < 4; cc++) {
+      const uint32_t s = mul(to_mont(3), mont_pow(w4, cc));
+      k_fill_powers<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(b->p + cc * n, n, s, MONT_ONE);
+      LG_LAUNCH();
+    }
+    cshift[logn] = b;
     return b->p;
   }
   uint32_t* host_staging(size_t words) {

@@ -184,30 +184,30 @@ __global__ void k_lde(const LdeLane* lanes, int logn_rt, int from_coeffs, const 
 
 // Evaluations of a coefficient lane on the cosets s_c <w_n>, s_c = g w_4n^c,
 // c = blockIdx.y < 4, in natural order: out[c n + j] = P(s_c w_n^j).
-// n >= 16: DIT whose first pass gathers the scaled coefficients in
-// bit-reversed order from global memory.
+// n >= 16: the scaled coefficients coef[k] s_c^k (shift: the table of s_c^k,
+// coset_shifts) go to the second half of shared memory with coalesced loads;
+// a DIT whose first pass gathers them in bit-reversed order from there works
+// in the first half.
 struct CosetLane { const uint32_t* src; uint32_t* out; };
 template <int LOGN>
-__global__ void k_coset_eval(const CosetLane* lanes, int logn_rt, const uint32_t* tw_n, const uint32_t* tw_4n,
-                             const uint32_t* gpow) {
+__global__ void k_coset_eval(const CosetLane* lanes, int logn_rt, const uint32_t* tw_n, const uint32_t* shift) {
   const int logn = LOGN ? LOGN : logn_rt;
   extern __shared__ uint32_t sm[];
   const uint32_t n = 1u << logn, c = blockIdx.y;
   const CosetLane L = lanes[blockIdx.x];
-  const uint32_t big = n << RATE_LOG;
+  const uint32_t* sh = shift + (uint64_t)c * n;
   uint32_t* o = L.out + (uint64_t)c * n;
   if (logn < 4) {
-    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x)
-      sm[k] = mul(mul(L.src[k], __ldg(gpow + k)), __ldg(tw_4n + ((c * k) & (big - 1))));
+    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) sm[k] = mul(L.src[k], sh[k]);
     __syncthreads();
     smem_dif(sm, logn, tw_n, false);
     for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) o[j] = sm[bitrev32(j, logn)];
     return;
   }
-  auto first = [&](uint32_t t, uint32_t r, int lo) {
-    uint32_t k = bitrev32(grp_index(t, r, lo), logn);
-    return mul(mul(L.src[k], __ldg(gpow + k)), __ldg(tw_4n + ((c * k) & (big - 1))));
-  };
+  uint32_t* S2 = sm + pad16(n) + 1;
+  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) S2[pad16(k)] = mul(L.src[k], sh[k]);
+  __syncthreads();
+  auto first = [&](uint32_t t, uint32_t r, int lo) { return S2[pad16(bitrev32(grp_index(t, r, lo), logn))]; };
   auto store = [&](uint32_t t, int lo, const uint32_t* v) {
 #pragma unroll
     for (uint32_t r = 0; r < 16; r++) o[grp_index(t, r, lo)] = v[r];

@@ -98,6 +98,7 @@ void lg_ctx_destroy(lg_ctx* ctx) {
   ctx->c.tw.clear();
   ctx->c.gpow.clear();
   ctx->c.ginvpow.clear();
+  ctx->c.cshift.clear();
   ctx->c.lagrange_vals.clear();
   ctx->c.lagrange_coef.clear();
   ctx->c.programs.clear();

@@ -1087,14 +1087,13 @@ struct Prover {
         }
         auto tab = upload_vec(c, kv.second);
         const uint32_t* twn = c.twiddles((int)logn);
-        const uint32_t* tw4 = c.twiddles((int)logn + RATE_LOG);
-        const uint32_t* gp = c.gpowers((int)logn, false);
+        const uint32_t* shifts = c.coset_shifts((int)logn);
+        const size_t smem = 2 * pad16_words((int)logn) * 4;
         with_ntt_size((int)logn, [&](auto L) {
-          allow_smem(k_coset_eval<decltype(L)::value>, pad16_words((int)logn) * 4);
+          allow_smem(k_coset_eval<decltype(L)::value>, smem);
           c.timed("coset_eval", 20.0 * n * kv.second.size(), 0, [&] {
-            k_coset_eval<decltype(L)::value><<<dim3((unsigned)kv.second.size(), 4), ntt_threads((int)logn),
-                                               pad16_words((int)logn) * 4, c.stream>>>((const CosetLane*)tab->p,
-                                                                                       (int)logn, twn, tw4, gp);
+            k_coset_eval<decltype(L)::value><<<dim3((unsigned)kv.second.size(), 4), ntt_threads((int)logn), smem,
+                                               c.stream>>>((const CosetLane*)tab->p, (int)logn, twn, shifts);
             LG_LAUNCH();
           });
         });
