@@ -985,11 +985,23 @@ __global__ void k_deep(const DeepJob* jobs) {
       if (bu.mask >> s & 1) acc[s] = e6_sub(acc[s], v);
   }
   uint32_t x = __ldg(jb.tw + bitrev32(r, jb.logn4));
+  // sum_s acc_s / (z_s - x) with one inversion (Montgomery's trick over the
+  // points): pre_s = d_0 ... d_s, then 1/d_s = pre_(s-1) / pre_s from the top
+  E6 d[DEEP_MAX_POINTS], pre[DEEP_MAX_POINTS];
+  const uint32_t np = jb.n_points;
+  for (uint32_t s = 0; s < np; s++) {
+    d[s] = jb.z[s];
+    d[s].c[0] = sub(d[s].c[0], x);
+    pre[s] = s ? e6_mul(pre[s - 1], d[s]) : d[s];
+  }
   E6 dq = e6_zero();
-  for (uint32_t s = 0; s < jb.n_points; s++) {
-    E6 d = jb.z[s];
-    d.c[0] = sub(d.c[0], x);
-    dq = e6_add(dq, e6_mul(acc[s], e6_inv(d)));
+  if (np) {
+    E6 inv_run = e6_inv(pre[np - 1]);  // 1 / (d_0 ... d_(np-1))
+    for (uint32_t s = np - 1; s > 0; s--) {
+      dq = e6_add(dq, e6_mul(acc[s], e6_mul(inv_run, pre[s - 1])));
+      inv_run = e6_mul(inv_run, d[s]);
+    }
+    dq = e6_add(dq, e6_mul(acc[0], inv_run));
   }
   for (int w = 0; w < 6; w++) jb.out[(uint64_t)w * big + r] = dq.c[w];
 }
