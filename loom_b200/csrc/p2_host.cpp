@@ -1,8 +1,8 @@
 // Host Poseidon2 (width 24) for the Fiat-Shamir transcript: the transcript is
 // a chain of sponge absorptions the host computes between device phases
 // (challenges, claimed-value binding, query positions), so its latency adds to
-// every proof.  With AVX2 (checked at run time) the 24-word state lives in
-// three 8-lane vectors: Montgomery products as even/odd 32x32->64 multiplies,
+// every proof.  With AVX-512 (checked at run time) the 24-word state lives in
+// a 16-lane and an 8-lane vector; with AVX2 only, in three 8-lane vectors: Montgomery products as even/odd 32x32->64 multiplies,
 // the M4 blocks of the external layer as in-lane shuffles, the partial rounds
 // in the carried-sum form of p2_partial_rounds (poseidon2.cuh) with one
 // horizontal sum per round.  Same permutation, same words as p2_permute.
@@ -10,6 +10,8 @@
 
 #if defined(__x86_64__)
 #include <immintrin.h>
+
+#include <cstdlib>
 #define LG_AVX2 __attribute__((target("avx2")))
 
 namespace lg {
@@ -99,25 +101,113 @@ LG_AVX2 void p2_permute_avx2(uint32_t s[24]) {
   for (int k = 0; k < 3; k++) _mm256_storeu_si256(reinterpret_cast<__m256i*>(s + 8 * k), v[k]);
 }
 
-bool cpu_has_avx2() {
+// AVX-512: lanes 0..15 in one 16-lane vector (four M4 blocks), lanes 16..23
+// in an 8-lane one (two blocks); the same steps as p2_permute_avx2.
+#define LG_AVX512 __attribute__((target("avx512f,avx2")))
+
+LG_AVX512 inline __m512i zp() { return _mm512_set1_epi32((int)P); }
+LG_AVX512 inline __m512i zadd(__m512i a, __m512i b) {
+  const __m512i s = _mm512_add_epi32(a, b);
+  return _mm512_min_epu32(s, _mm512_sub_epi32(s, zp()));
+}
+LG_AVX512 inline __m512i zred(__m512i x) { return _mm512_min_epu32(x, _mm512_sub_epi32(x, zp())); }
+LG_AVX512 inline __m512i zmul(__m512i a, __m512i b) {
+  const __m512i p = zp(), pinv = _mm512_set1_epi32((int)P_INV_NEG);
+  const __m512i te = _mm512_mul_epu32(a, b);
+  const __m512i to = _mm512_mul_epu32(_mm512_srli_epi64(a, 32), _mm512_srli_epi64(b, 32));
+  const __m512i me = _mm512_mul_epu32(te, pinv), mo = _mm512_mul_epu32(to, pinv);
+  const __m512i ue = _mm512_add_epi64(te, _mm512_mul_epu32(me, p));
+  const __m512i uo = _mm512_add_epi64(to, _mm512_mul_epu32(mo, p));
+  return zred(_mm512_mask_blend_epi32((__mmask16)0xAAAA, _mm512_srli_epi64(ue, 32), uo));
+}
+LG_AVX512 inline __m512i zcube(__m512i x) { return zmul(zmul(x, x), x); }
+LG_AVX512 inline __m512i zm4(__m512i v) {  // p2_m4 on each 128-bit lane, as vm4
+  const __m512i r = _mm512_shuffle_epi32(v, (_MM_PERM_ENUM)_MM_SHUFFLE(0, 3, 2, 1));
+  const __m512i e = zadd(v, zadd(r, r));
+  const __m512i s1 = zadd(v, _mm512_shuffle_epi32(v, (_MM_PERM_ENUM)_MM_SHUFFLE(2, 3, 0, 1)));
+  const __m512i t = zadd(s1, _mm512_shuffle_epi32(s1, (_MM_PERM_ENUM)_MM_SHUFFLE(1, 0, 3, 2)));
+  return zadd(e, t);
+}
+LG_AVX512 inline void zexternal(__m512i& a, __m256i& b) {
+  a = zm4(a);
+  b = vm4(b);
+  __m512i t = zadd(a, _mm512_shuffle_i32x4(a, a, _MM_SHUFFLE(1, 0, 3, 2)));  // blocks 0+2, 1+3
+  t = zadd(t, _mm512_shuffle_i32x4(t, t, _MM_SHUFFLE(2, 3, 0, 1)));          // all four, in every lane
+  const __m256i u = vadd(b, _mm256_permute2x128_si256(b, b, 0x01));         // blocks 4+5
+  const __m512i tot = zadd(t, _mm512_broadcast_i32x4(_mm256_castsi256_si128(u)));
+  a = zadd(a, tot);
+  b = vadd(b, _mm512_castsi512_si256(tot));
+}
+LG_AVX512 inline void zfull_round(__m512i& a, __m256i& b, const uint32_t* rk) {
+  a = zcube(zadd(a, _mm512_loadu_si512(rk)));
+  b = vcube(vadd(b, _mm256_loadu_si256(reinterpret_cast<const __m256i*>(rk + 16))));
+  zexternal(a, b);
+}
+
+// lanes 1..23 of (x, y) summed (each in [0, p))
+LG_AVX512 inline uint32_t zsum_tail(__m512i x, __m256i y) {
+  x = _mm512_mask_blend_epi32((__mmask16)0x0001, x, _mm512_setzero_si512());
+  return vhsum(vadd(vadd(_mm512_castsi512_si256(x), _mm512_extracti64x4_epi64(x, 1)), y));
+}
+
+LG_AVX512 void p2_permute_avx512(uint32_t s[24]) {
+  __m512i a = _mm512_loadu_si512(s);
+  __m256i b = _mm256_loadu_si256(reinterpret_cast<const __m256i*>(s + 16));
+  const __m512i da = _mm512_loadu_si512(P2_DIAG_H);
+  const __m256i db = _mm256_loadu_si256(reinterpret_cast<const __m256i*>(P2_DIAG_H + 16));
+  zexternal(a, b);
+  for (int r = 0; r < 3; r++) zfull_round(a, b, P2_FULL_RK_H[r]);
+  // partial rounds, carried R = s_1 + ... + s_23 (as p2_partial_rounds)
+  uint32_t R = zsum_tail(a, b);
+  for (int r = 0; r < 21; r++) {
+    const uint32_t s0 = (uint32_t)_mm_cvtsi128_si32(_mm512_castsi512_si128(a));
+    const uint32_t u = p2_cube(add(s0, P2_PARTIAL_RK_H[r]));
+    const __m512i pa = zmul(a, da);
+    const __m256i pb = vmul(b, db);
+    const uint32_t D = zsum_tail(pa, pb);
+    const uint32_t sum = add(u, R);
+    const __m512i sv = _mm512_set1_epi32((int)sum);
+    const uint32_t s0n = add(sum, mul(u, P2_DIAG_H[0]));
+    a = _mm512_mask_blend_epi32((__mmask16)0x0001, _mm512_add_epi32(sv, pa), _mm512_set1_epi32((int)s0n));
+    b = _mm256_add_epi32(_mm512_castsi512_si256(sv), pb);  // unreduced in [0, 2p) until the next product
+    R = add(mul(sum, MONT_23), D);
+  }
+  a = zred(a);
+  b = vred(b);
+  for (int r = 3; r < 6; r++) zfull_round(a, b, P2_FULL_RK_H[r]);
+  _mm512_storeu_si512(s, a);
+  _mm256_storeu_si256(reinterpret_cast<__m256i*>(s + 16), b);
+}
+
+// 2: AVX-512, 1: AVX2, 0: neither
+int cpu_simd_level() {
   __builtin_cpu_init();
-  return __builtin_cpu_supports("avx2");
+  if (__builtin_cpu_supports("avx512f") && !getenv("LOOM_B200_NO_AVX512")) return 2;
+  return __builtin_cpu_supports("avx2") ? 1 : 0;
 }
 
 }  // namespace
 
-void p2_permute_host(uint32_t s[24]) {
-  static const bool simd = cpu_has_avx2();
-  if (simd)
+void p2_permute_host_at(uint32_t s[24], int level) {
+  if (level >= 2)
+    p2_permute_avx512(s);
+  else if (level == 1)
     p2_permute_avx2(s);
   else
     p2_permute(s);
 }
+int p2_host_simd_level() {
+  static const int simd = cpu_simd_level();
+  return simd;
+}
+void p2_permute_host(uint32_t s[24]) { p2_permute_host_at(s, p2_host_simd_level()); }
 
 }  // namespace lg
 
 #else
 namespace lg {
+void p2_permute_host_at(uint32_t s[24], int) { p2_permute(s); }
+int p2_host_simd_level() { return 0; }
 void p2_permute_host(uint32_t s[24]) { p2_permute(s); }
 }  // namespace lg
 #endif

@@ -192,6 +192,10 @@ LG_HD void p2_compress(uint32_t tag_m, const uint32_t l[8], const uint32_t r[8],
 // The host's permutation for the transcript (p2_host.cpp): the same map as
 // p2_permute, vectorised when the CPU has AVX2.
 void p2_permute_host(uint32_t s[24]);
+// The same with a given vector width (2: AVX-512, 1: AVX2, 0: scalar; the
+// caller checks the CPU has it) and the width p2_permute_host uses.
+void p2_permute_host_at(uint32_t s[24], int level);
+int p2_host_simd_level();
 
 // Host sponge: width 24, rate 16, overwrite mode, no padding
 // (internal/hash/poseidon2.go:165-255).

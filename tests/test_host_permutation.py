@@ -21,6 +21,10 @@ extern "C" void host_permute(uint32_t* states, unsigned long n) {
 extern "C" void scalar_permute(uint32_t* states, unsigned long n) {
   for (unsigned long i = 0; i < n; i++) lg::p2_permute(states + 24 * i);
 }
+extern "C" void level_permute(uint32_t* states, unsigned long n, int level) {
+  for (unsigned long i = 0; i < n; i++) lg::p2_permute_host_at(states + 24 * i, level);
+}
+extern "C" int simd_level() { return lg::p2_host_simd_level(); }
 '''
 
 
@@ -39,6 +43,7 @@ def lib(tmp_path_factory):
     L = ctypes.CDLL(str(out))
     for f in (L.host_permute, L.scalar_permute):
         f.argtypes = [ctypes.c_void_p, ctypes.c_ulong]
+    L.level_permute.argtypes = [ctypes.c_void_p, ctypes.c_ulong, ctypes.c_int]
     return L
 
 
@@ -54,3 +59,17 @@ def test_host_permutation_matches_oracle(lib):
         got = F.from_mont(st)
         for i in range(canon.shape[0]):
             assert np.array_equal(got[i], oracle.p2_permute(canon[i], 24)), (name, i)
+
+
+def test_every_vector_width_matches_oracle(lib):
+    """Each width this CPU has (AVX-512 and AVX2 where present, scalar always)
+    gives the oracle's permutation."""
+    rng = np.random.Generator(np.random.PCG64(25))
+    canon = rng.integers(0, F.P, (200, 24), dtype=np.uint64).astype(np.uint32)
+    canon[0] = F.P - 1
+    for level in range(lib.simd_level() + 1):
+        st = np.ascontiguousarray(F.to_mont(canon))
+        lib.level_permute(st.ctypes.data, st.shape[0], level)
+        got = F.from_mont(st)
+        for i in range(canon.shape[0]):
+            assert np.array_equal(got[i], oracle.p2_permute(canon[i], 24)), (level, i)
