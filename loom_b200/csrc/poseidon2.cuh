@@ -137,6 +137,72 @@ __constant__ P2DiagShoup P2_DSH_D = make_p2_diag_shoup();
 #endif
 constexpr uint32_t C23 = 23, C23_SH = shoup(23);
 
+// Products by the diagonal entries +-2^-k (17 of the 24).  With
+// x = hi 2^k + lo (lo < 2^k) and 2^k (p - 1)/2^k = p - 1 = -1 mod p,
+//   x 2^-k = hi + lo 2^-k = hi - lo (p - 1)/2^k  (mod p):
+// a shift, a mask and one multiply by a small constant in place of Shoup's
+// three multiplies.  For x < 2p both hi and lo (p - 1)/2^k are below p, so
+// t = +-(hi - lo c) lies in (-p, p) and min(t, t + p) on unsigned words is
+// its residue in [0, p).  Montgomery words need no conversion (linear map).
+template <int K, bool NEG> LG_HD uint32_t mul_pow2_inv(uint32_t x) {
+  static_assert(K >= 1 && K <= 24, "p - 1 = 127 2^24");
+  constexpr uint32_t c = (P - 1) >> K;
+  const uint32_t lo = x & ((1u << K) - 1), hi = x >> K;
+  const uint32_t t = NEG ? lo * c - hi : hi - lo * c;
+  return umin(t, t + P);
+}
+constexpr uint32_t cx_pow2_inv(int k, bool neg) {
+  const uint32_t v = cx_pow((P + 1) / 2, (uint64_t)k);
+  return neg ? (P - v) % P : v;
+}
+#define LG_P2_DIAG_POW2(i, k, neg) \
+  static_assert(P2_DSH_H.w[i] == cx_pow2_inv(k, neg), "internal diagonal entry " #i " is " #neg " 2^-" #k)
+LG_P2_DIAG_POW2(3, 1, false);
+LG_P2_DIAG_POW2(6, 1, true);
+LG_P2_DIAG_POW2(9, 8, false);
+LG_P2_DIAG_POW2(10, 2, false);
+LG_P2_DIAG_POW2(11, 3, false);
+LG_P2_DIAG_POW2(12, 4, false);
+LG_P2_DIAG_POW2(13, 5, false);
+LG_P2_DIAG_POW2(14, 6, false);
+LG_P2_DIAG_POW2(15, 24, false);
+LG_P2_DIAG_POW2(16, 8, true);
+LG_P2_DIAG_POW2(17, 3, true);
+LG_P2_DIAG_POW2(18, 4, true);
+LG_P2_DIAG_POW2(19, 5, true);
+LG_P2_DIAG_POW2(20, 6, true);
+LG_P2_DIAG_POW2(21, 7, true);
+LG_P2_DIAG_POW2(22, 9, true);
+LG_P2_DIAG_POW2(23, 24, true);
+#undef LG_P2_DIAG_POW2
+
+// d_i s_i for i = 2..23 into p[2..23], for s_i < 2p; outputs in [0, p).
+// Entries 2, 4, 5, 7, 8 (2, 3, 4, -3, -4) use Shoup's products.
+LG_HD void p2_diag_products(const uint32_t s[24], uint32_t p[24]) {
+  p[2] = mulc(s[2], LG_P2_DSH.w[2], LG_P2_DSH.ws[2]);
+  p[3] = mul_pow2_inv<1, false>(s[3]);
+  p[4] = mulc(s[4], LG_P2_DSH.w[4], LG_P2_DSH.ws[4]);
+  p[5] = mulc(s[5], LG_P2_DSH.w[5], LG_P2_DSH.ws[5]);
+  p[6] = mul_pow2_inv<1, true>(s[6]);
+  p[7] = mulc(s[7], LG_P2_DSH.w[7], LG_P2_DSH.ws[7]);
+  p[8] = mulc(s[8], LG_P2_DSH.w[8], LG_P2_DSH.ws[8]);
+  p[9] = mul_pow2_inv<8, false>(s[9]);
+  p[10] = mul_pow2_inv<2, false>(s[10]);
+  p[11] = mul_pow2_inv<3, false>(s[11]);
+  p[12] = mul_pow2_inv<4, false>(s[12]);
+  p[13] = mul_pow2_inv<5, false>(s[13]);
+  p[14] = mul_pow2_inv<6, false>(s[14]);
+  p[15] = mul_pow2_inv<24, false>(s[15]);
+  p[16] = mul_pow2_inv<8, true>(s[16]);
+  p[17] = mul_pow2_inv<3, true>(s[17]);
+  p[18] = mul_pow2_inv<4, true>(s[18]);
+  p[19] = mul_pow2_inv<5, true>(s[19]);
+  p[20] = mul_pow2_inv<6, true>(s[20]);
+  p[21] = mul_pow2_inv<7, true>(s[21]);
+  p[22] = mul_pow2_inv<9, true>(s[22]);
+  p[23] = mul_pow2_inv<24, true>(s[23]);
+}
+
 // Partial rounds (S-box on lane 0, internal layer 1.1^T + diag).  With
 // R = s_1 + ... + s_23 carried from round to round, one round is
 //   u = S(s_0 + c),  sum = u + R,  s_0 <- sum + d_0 u,  s_i <- sum + d_i s_i,
@@ -153,8 +219,7 @@ LG_HD void p2_partial_rounds(uint32_t s[24]) {
     const uint32_t u = p2_cube(add(s[0], LG_P2_PARTIAL_RK[r]));
     uint32_t p[24];
     p[1] = red(s[1]);  // d_1 = 1
-#pragma unroll
-    for (int i = 2; i < 24; i++) p[i] = mulc(s[i], LG_P2_DSH.w[i], LG_P2_DSH.ws[i]);
+    p2_diag_products(s, p);
     const uint32_t D = wide_sum<23>(p + 1);
     const uint32_t sum = add(u, R);
     s[0] = add(sum, mulc(u, LG_P2_DSH.w[0], LG_P2_DSH.ws[0]));
