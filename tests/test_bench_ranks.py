@@ -42,3 +42,43 @@ def test_single_process_is_identity():
     sys.path.insert(0, ROOT)
     import bench
     assert bench.max_over_ranks([1, 2.5], None, "cpu") == [1.0, 2.5]
+
+
+def _run_bench(args, env_extra=None):
+    import json
+    import subprocess
+    env = dict(os.environ, **(env_extra or {}))
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py")] + args, cwd=ROOT, env=env,
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(l) for l in r.stdout.splitlines() if l.startswith("{")]
+    return lines
+
+
+def test_reference_arm_line_contract():
+    """`bench.py --impl reference` times the CPU restatement on the host cores
+    and prints the same metric, unit and config as the GPU arm, with the
+    reference-arm keys (impl, cpu_baseline, e2e with no host<->device bytes)."""
+    args = ["--impl", "reference", "--steps", "1", "--warmup", "1", "--instances", "2", "--log-n", "8",
+            "--cpu-sample", "1", "--queries", "8"]
+    (line,) = _run_bench(args)
+    assert line["impl"] == "reference" and line["unit"] == "ms" and line["higher_is_better"] is False
+    assert line["value"] > 0 and line["value"] == line["ms_per_step"] == line["e2e"]["value"]
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+    base = line["cpu_baseline"]
+    assert base["kind"] == "port" and base["cores"] >= 1 and "1 of 2 instances" in base["sample"]
+    assert line["config"]["instances"] == 2 and line["config"]["log_rows"] == 8
+    # under torchrun only rank 0 runs and prints; the other ranks exit 0 without work
+    assert _run_bench(args, {"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"}) == []
+
+
+def test_device_idle_accounting():
+    """Gaps between recorded launches count in the phase of the launch that
+    ends them; overlapping launches leave no gap."""
+    sys.path.insert(0, ROOT)
+    import bench
+    timeline = [("k_a", 0, 0.0, 1.0), ("k_b", 0, 0.5, 1.0), ("k_c", 1, 2.0, 0.5), ("k_d", 2, 3.0, 1.0),
+                ("k_e", 5, 4.25, 0.25)]
+    got = bench.device_idle(timeline, ["round 0", "round 2", "deep"])
+    assert got == {"total": 1.25, "span": 4.5, "by_phase": {"round 2": 0.5, "deep": 0.5, "after last phase": 0.25}}
+    assert bench.device_idle([], ["round 0"]) is None
