@@ -70,6 +70,8 @@ class Server:
         self.idle = list(self.contexts)
         self.finished: List[Request] = []
         self.peak_in_use = 0
+        self.running = 0                   # requests in flight
+        self.closed = False
         self.t0 = time.perf_counter()
 
     def warm(self, requests: Sequence[Request]):
@@ -86,12 +88,13 @@ class Server:
         """Head-of-line admission: the oldest request starts when a slot and
         its memory are free (no reordering, so no request starves)."""
         started = []
-        while self.queue and self.idle:
+        while self.queue and self.idle and not self.closed:
             r = self.queue[0]
             need = device_bytes_estimate(r.rows)
             if self.in_use + need > self.budget and self.in_use > 0:
                 break
             self.queue.pop(0)
+            self.running += 1
             self.in_use += need
             self.peak_in_use = max(self.peak_in_use, self.in_use)
             started.append((r, self.idle.pop(), need))
@@ -105,6 +108,7 @@ class Server:
             r.error = str(e)
         r.done = self.now()
         with self.cv:
+            self.running -= 1
             self.in_use -= need
             self.idle.append(ctx)
             self.finished.append(r)
@@ -123,8 +127,17 @@ class Server:
         with self.cv:
             self.cv.wait_for(lambda: len(self.finished) >= n, timeout=timeout)
 
-    def close(self):
-        for c in self.contexts:
+    def close(self, timeout: Optional[float] = None):
+        """Admits nothing more, waits for the requests in flight (a context
+        must not be destroyed under a running prove), then destroys the
+        contexts.  A context still proving when `timeout` runs out is left
+        to the process exit rather than freed under its prove."""
+        with self.cv:
+            self.closed = True
+            self.cv.wait_for(lambda: self.running == 0, timeout=timeout)
+            idle = list(self.idle)
+            self.idle = []
+        for c in idle:
             c.close()
 
 

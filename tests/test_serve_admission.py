@@ -75,3 +75,29 @@ def test_poisson_arrivals_are_seeded_and_increasing():
     a = S.poisson_arrivals(100, 50.0, 3)
     assert np.all(np.diff(a) > 0) and np.array_equal(a, S.poisson_arrivals(100, 50.0, 3))
     assert 1.0 < a[-1] < 4.0
+
+
+def test_close_waits_for_requests_in_flight():
+    """A context is destroyed only after its running prove returns, and a
+    closed server admits nothing more."""
+    events = []
+
+    class SlowContext(FakeContext):
+        def prove(self, words, witness, q):
+            time.sleep(0.2)
+            events.append(("proved", id(self)))
+            return b"ok"
+
+        def close(self):
+            events.append(("closed", id(self)))
+
+    srv = S.Server(streams=2, hbm_budget=1 << 40, context_factory=SlowContext)
+    rs = reqs([1024] * 3, [1, 1, 1])
+    for r in rs:
+        srv.submit(r)
+    srv.close()
+    assert sorted(e for e, _ in events) == ["closed", "closed", "proved", "proved"]
+    for ctx_id in {i for _, i in events}:
+        mine = [e for e, i in events if i == ctx_id]
+        assert mine == ["proved", "closed"]
+    assert len(srv.finished) == 2 and srv.queue == [rs[2]]  # the third was never admitted
