@@ -183,7 +183,9 @@ int lg_poseidon2_permute(lg_ctx* ctx, uint32_t* states, uint64_t n_states, int o
 /* Merkle root over n_leaves digests with level injections
  * (merkle.NewWithInjections + Build, internal/merkle/tree.go:117-296):
  * n_inj injections of widths inj_widths[k] (non-increasing), their leaves
- * concatenated in `inj`. */
+ * concatenated in `inj`.  A schedule validateInjections rejects
+ * (internal/merkle/tree.go:140-160: a width that is not a power of two,
+ * exceeds n_leaves or grows) returns LG_ERR_INVALID. */
 int lg_merkle_root(lg_ctx* ctx, const uint32_t* leaves, uint64_t n_leaves, uint32_t n_inj,
                    const uint64_t* inj_widths, const uint32_t* inj, int on_device, uint32_t root[8]);
 

@@ -294,6 +294,15 @@ int lg_merkle_root(lg_ctx* ctx, const uint32_t* leaves, uint64_t n_leaves, uint3
   return guarded(ctx, [&] {
     Ctx& c = ctx->c;
     if (!leaves || !root || n_leaves == 0 || (n_leaves & (n_leaves - 1))) throw Error(LG_ERR_INVALID, "bad leaves");
+    if (n_inj && (!inj_widths || !inj)) throw Error(LG_ERR_INVALID, "null injections");
+    // the schedule merkle.NewWithInjections accepts (validateInjections,
+    // internal/merkle/tree.go:140-160):
+    // powers of two, none wider than the leaves, widths never increasing
+    for (uint32_t k = 0; k < n_inj; k++) {
+      const uint64_t w = inj_widths[k];
+      if (w == 0 || (w & (w - 1)) || w > n_leaves || (k && w > inj_widths[k - 1]))
+        throw Error(LG_ERR_INVALID, "bad injection schedule");
+    }
     TreeDev t;
     while ((1ull << t.log_leaves) < n_leaves) t.log_leaves++;
     t.nodes = std::make_shared<DBuf>(16 * n_leaves, c.stream);
@@ -301,8 +310,7 @@ int lg_merkle_root(lg_ctx* ctx, const uint32_t* leaves, uint64_t n_leaves, uint3
                           on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c.stream));
     size_t off = 0;
     for (uint32_t k = 0; k < n_inj; k++) {
-      uint64_t w = inj_widths[k];
-      if (w == 0 || (w & (w - 1)) || w > n_leaves) throw Error(LG_ERR_INVALID, "bad injection width");
+      const uint64_t w = inj_widths[k];
       t.inj.push_back(to_device(c, inj + off, 8 * w, on_device));
       uint32_t lw = 0;
       while ((1ull << lw) < w) lw++;

@@ -51,6 +51,7 @@ def lib():
         L.oracle_sponge.argtypes = [u32p, ctypes.c_size_t, u32p]
         L.oracle_commit.argtypes = [ctypes.c_uint32, u64p, u32p, u32p, ctypes.POINTER(u32p), u32p, u32p]
         L.oracle_merkle_root.argtypes = [u32p, ctypes.c_size_t, ctypes.c_uint32, u64p, u32p, u32p]
+        L.oracle_merkle_root.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -204,7 +205,9 @@ def merkle_root(leaves_mont: np.ndarray, injections: Sequence[np.ndarray] = ()) 
     widths = np.array([len(_u32(x).reshape(-1)) // 8 for x in injections], dtype=np.uint64)
     inj = np.concatenate([_u32(x).reshape(-1) for x in injections]) if injections else np.zeros(8, dtype=np.uint32)
     root = np.zeros(8, dtype=np.uint32)
-    lib().oracle_merkle_root(_p(lv), lv.size // 8, len(injections), widths.ctypes.data_as(u64p), _p(inj), _p(root))
+    L = lib()
+    if L.oracle_merkle_root(_p(lv), lv.size // 8, len(injections), widths.ctypes.data_as(u64p), _p(inj), _p(root)):
+        raise ValueError("oracle_merkle_root: " + L.oracle_last_error().decode())
     return root
 
 

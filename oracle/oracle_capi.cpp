@@ -194,21 +194,29 @@ int oracle_commit(uint32_t n_groups, const uint64_t* rows, const uint32_t* nb, c
 }
 
 // Merkle root over `n` leaves (Montgomery digests) with injections of
-// widths inj_w[k] whose leaves follow one another in `inj` .
-void oracle_merkle_root(const uint32_t* leaves, size_t n, uint32_t n_inj, const uint64_t* inj_w, const uint32_t* inj,
-                        uint32_t* root_out) {
-  auto rd = [](const uint32_t* p) { Digest d; for (int i = 0; i < 8; i++) d.v[i] = from_mont(p[i]); return d; };
-  std::vector<Digest> lv(n);
-  for (size_t i = 0; i < n; i++) lv[i] = rd(leaves + 8 * i);
-  std::vector<Injection> ij;
-  size_t o = 0;
-  for (uint32_t k = 0; k < n_inj; k++) {
-    Injection x;
-    for (uint64_t i = 0; i < inj_w[k]; i++) { x.leaves.push_back(rd(inj + o)); o += 8; }
-    ij.push_back(x);
+// widths inj_w[k] whose leaves follow one another in `inj`.  Returns 0, or 2
+// for a schedule merkle.NewWithInjections rejects (the reason in
+// oracle_last_error()).
+int oracle_merkle_root(const uint32_t* leaves, size_t n, uint32_t n_inj, const uint64_t* inj_w, const uint32_t* inj,
+                       uint32_t* root_out) {
+  try {
+    auto rd = [](const uint32_t* p) { Digest d; for (int i = 0; i < 8; i++) d.v[i] = from_mont(p[i]); return d; };
+    std::vector<Digest> lv(n);
+    for (size_t i = 0; i < n; i++) lv[i] = rd(leaves + 8 * i);
+    std::vector<Injection> ij;
+    size_t o = 0;
+    for (uint32_t k = 0; k < n_inj; k++) {
+      Injection x;
+      for (uint64_t i = 0; i < inj_w[k]; i++) { x.leaves.push_back(rd(inj + o)); o += 8; }
+      ij.push_back(x);
+    }
+    Tree t = build_tree(lv, ij);
+    for (int i = 0; i < 8; i++) root_out[i] = to_mont(t.root().v[i]);
+    return 0;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return 2;
   }
-  Tree t = build_tree(lv, ij);
-  for (int i = 0; i < 8; i++) root_out[i] = to_mont(t.root().v[i]);
 }
 
 }  // extern "C"

@@ -67,6 +67,21 @@ def test_merkle_injections(ctx):
     assert np.array_equal(ctx.merkle_root(leaves[:1]), oracle.merkle_root(leaves[:1]))
 
 
+def test_merkle_injection_order_and_schedule_checks(ctx):
+    """Same-width injections do not commute (the GPU agrees with the oracle
+    either way), and a schedule merkle.NewWithInjections rejects (a width
+    that grows, exceeds the leaves or is not a power of two) is refused."""
+    leaves = F.to_mont(rnd((8, 8), 10))
+    a, b = F.to_mont(rnd((4, 8), 11)), F.to_mont(rnd((4, 8), 12))
+    ab, ba = ctx.merkle_root(leaves, [a, b]), ctx.merkle_root(leaves, [b, a])
+    assert not np.array_equal(ab, ba)
+    assert np.array_equal(ab, oracle.merkle_root(leaves, [a, b]))
+    assert np.array_equal(ba, oracle.merkle_root(leaves, [b, a]))
+    for widths in ([4, 8], [16], [3], [0]):
+        with pytest.raises(LoomError, match="injection"):
+            ctx.merkle_root(leaves, [F.to_mont(rnd((w, 8), 20 + w)) for w in widths])
+
+
 @pytest.mark.parametrize("logn", [1, 4, 11, 16])
 def test_fri_fold(ctx, logn):
     layer = F.to_mont(rnd((1 << logn, 6), logn))

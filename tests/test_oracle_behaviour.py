@@ -59,6 +59,25 @@ def test_merkle_injections_match_naive_root():
     assert F.from_mont(got).tolist() == level[0]
 
 
+def test_same_width_injection_order_matters():
+    # injection_test.go TestSameWidthOrderMatters: the order of two injections
+    # of one width is part of the commitment
+    leaves = F.to_mont(rnd((8, 8), 10))
+    a, b = F.to_mont(rnd((4, 8), 11)), F.to_mont(rnd((4, 8), 12))
+    assert not np.array_equal(oracle.merkle_root(leaves, [a, b]), oracle.merkle_root(leaves, [b, a]))
+
+
+@pytest.mark.parametrize("widths", [[4, 8], [16], [3], [0]])
+def test_bad_injection_schedule_is_rejected(widths):
+    # injection_test.go TestInjectionScheduleValidation / validateInjections
+    # (internal/merkle/tree.go:140-160): widths must be powers of two, at most
+    # the leaves, and must not increase
+    leaves = F.to_mont(rnd((8, 8), 10))
+    inj = [F.to_mont(rnd((w, 8), 20 + w)) for w in widths]
+    with pytest.raises(ValueError, match="injection"):
+        oracle.merkle_root(leaves, inj)
+
+
 def _py_sponge(elems):
     state = [0] * 24
     block = []
