@@ -147,6 +147,14 @@ class Module:
             disj = disj + self.lagrange_col(r)
         self.assert_zero(rel * disj)
 
+    def assert_zero_except_at(self, rel: Expr, *rows: int):
+        """board/module.go:167-176 AssertZeroExceptAt: rel times the product
+        of (1 - L_i) over the excepted rows."""
+        conj = const(1) - self.lagrange_col(rows[0])
+        for r in rows[1:]:
+            conj = conj * (const(1) - self.lagrange_col(r))
+        self.assert_zero(rel * conj)
+
     def assert_equal_at(self, a: Expr, b: Expr, i: int):
         self.assert_zero((a - b) * self.lagrange_col(i))
 

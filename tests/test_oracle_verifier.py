@@ -2,6 +2,8 @@
 internal/fri/verify.go) on oracle proofs: valid proofs are accepted, proofs
 of false statements and tampered proofs are rejected.  The GPU proofs go
 through the same verifier in the `gpu` tests."""
+import struct
+
 import numpy as np
 import pytest
 
@@ -158,3 +160,47 @@ def test_conditional_tuple_lookup():
     compiled, wit = plonk.build_with_tuple_lookup(64, present=False)
     with pytest.raises(RuntimeError, match="not in the table"):
         _prove(compiled, wit, 8)
+
+
+def test_mixed_trace_round_trip_and_tampered_injection_row():
+    """verifier_test.go TestVerifyMixedTraceRoundTrip: a Fibonacci module of 4
+    rows (shifted columns, constraints except at the last row) looks up A, B
+    and C in a range module of 8 rows, so the trace tree injects the smaller
+    group; the proof verifies with its logup buses, and a tampered injection
+    row is rejected."""
+    from loom_b200.program import Builder, Module, col, lookup
+    n = 4
+    b = Builder()
+    fib = Module("fibonacci", n)
+    fib.assert_zero_except_at(col("A", 1) - col("B"), n - 1)
+    fib.assert_zero_except_at(col("B", 1) - col("C"), n - 1)
+    fib.assert_zero(col("C") - col("A") - col("B"))
+    b.add_module(fib)
+    b.add_module(Module("range", 2 * n))
+    for name in ("A", "B", "C"):
+        lookup(b, [(col(name), "fibonacci")], [(col("Lookup"), "range")])
+    compiled = b.compile()
+    # prover.TraceFibonacci(4, 0, 1) and prover.TraceRange(4) (prover/test_utils.go:58-92)
+    trace = {"A": [0, 1, 1, 2], "B": [1, 1, 2, 3], "C": [1, 2, 3, 5], "Lookup": list(range(2 * n))}
+    trace.update(b.generated)
+    wit = [np.array(trace[name], dtype=np.uint32) for (name, _, _) in compiled.witness_columns]
+    pb = _prove(compiled, wit, 8)
+    assert len(compiled.logup_buses) == 3
+    oracle.verify(compiled.words, pb, 8, compiled.logup_buses)
+
+    p = proof.decode(pb)
+    rows = [inj[0] for per in p.point_samplings for wp in per for inj in wp.injections]
+    assert rows, "the mixed-size trace tree opens injection rows"
+    words = rows[0].base
+    at = pb.find(struct.pack(">%dI" % len(words), *words))
+    assert at > 0
+    bad = bytearray(pb)
+    bad[at + 3] ^= 1
+    with pytest.raises(oracle.VerifyError):
+        oracle.verify(compiled.words, bytes(bad), 8, compiled.logup_buses)
+
+    # a wrong Fibonacci step is caught by the AIR relation
+    trace["C"] = [1, 2, 3, 6]
+    wit = [np.array(trace[name], dtype=np.uint32) for (name, _, _) in compiled.witness_columns]
+    with pytest.raises(oracle.VerifyError, match="AIR relation"):
+        oracle.verify(compiled.words, _prove(compiled, wit, 8), 8, compiled.logup_buses)
