@@ -204,3 +204,60 @@ def test_mixed_trace_round_trip_and_tampered_injection_row():
     wit = [np.array(trace[name], dtype=np.uint32) for (name, _, _) in compiled.witness_columns]
     with pytest.raises(oracle.VerifyError, match="AIR relation"):
         oracle.verify(compiled.words, _prove(compiled, wit, 8), 8, compiled.logup_buses)
+
+
+def _one_module(n):
+    from loom_b200.program import Builder, Module
+    b = Builder()
+    b.add_module(Module("m", n))
+    return b
+
+
+def _witness(b, compiled, trace):
+    trace = dict(trace)
+    trace.update(b.generated)
+    return [np.asarray(trace[name], dtype=np.uint32) for (name, _, _) in compiled.witness_columns]
+
+
+@pytest.mark.parametrize("bad", [False, True])
+def test_bus_within_one_module(bad):
+    """bus_test.go TestBusSameModule: sender and receiver in one module share
+    one running-ratio column, so the product bus has one end; receiving a
+    value that is not sent is rejected."""
+    from loom_b200.program import bus, col
+    n = 8
+    b = _one_module(n)
+    ends = bus(b, [col("m.s")], [col("m.r")], [([col("m.x")], "m")], [([col("m.y")], "m")])
+    compiled = b.compile()
+    assert compiled.product_buses == [ends] and len(ends) == 1
+    pad = lambda *v: list(v) + [0] * (n - len(v))
+    trace = {"m.x": pad(5, 6, 7, 0, 9), "m.s": pad(1, 1, 1, 0, 0),
+             "m.y": pad(0, 7, 6, 9 if bad else 5), "m.r": pad(0, 1, 1, 1)}
+    pb = _prove(compiled, _witness(b, compiled, trace), 8)
+    if bad:
+        with pytest.raises(oracle.VerifyError, match="do not multiply to one"):
+            oracle.verify(compiled.words, pb, 8, product_buses=compiled.product_buses)
+    else:
+        oracle.verify(compiled.words, pb, 8, product_buses=compiled.product_buses)
+
+
+@pytest.mark.parametrize("bad", [False, True])
+def test_lookup_source_and_target_in_one_module(bad):
+    """lookup_test.go TestSourceAndTargetShareColumn: source and table in one
+    module give one logup column and one total; a source value outside the
+    table is refused by the prover."""
+    from loom_b200.program import col, lookup
+    n = 8
+    b = _one_module(n)
+    totals = lookup(b, [(col("m.s"), "m")], [(col("m.t"), "m")])
+    compiled = b.compile()
+    assert compiled.logup_buses == [list(totals)] and len(totals) == 1
+    src = [(3 * i) % n for i in range(n)]
+    if bad:
+        src[2] = 100
+    wit = _witness(b, compiled, {"m.t": list(range(n)), "m.s": src})
+    if bad:
+        with pytest.raises(RuntimeError, match="not in the table"):
+            _prove(compiled, wit, 8)
+    else:
+        oracle.verify(compiled.words, _prove(compiled, wit, 8), 8, compiled.logup_buses)
