@@ -261,3 +261,58 @@ def test_lookup_source_and_target_in_one_module(bad):
             _prove(compiled, wit, 8)
     else:
         oracle.verify(compiled.words, _prove(compiled, wit, 8), 8, compiled.logup_buses)
+
+
+def _exposed_offsets(pb):
+    """Byte offset of the first word of each exposed value's first entry
+    (the encoding: backend string, then per name: string, entry count,
+    entries of index, field kind and six words)."""
+    o = 4 + struct.unpack_from(">I", pb, 0)[0]
+    count = struct.unpack_from(">I", pb, o)[0]
+    o += 4
+    offs = {}
+    for _ in range(count):
+        ln = struct.unpack_from(">I", pb, o)[0]
+        name = pb[o + 4:o + 4 + ln].decode()
+        o += 4 + ln
+        entries = struct.unpack_from(">I", pb, o)[0]
+        o += 4
+        offs[name] = o + 8
+        o += entries * 32
+    return offs
+
+
+@pytest.mark.parametrize("bad", [False, True])
+def test_batched_cyclic_lookup(bad):
+    """lookup_test.go TestBatchedCyclicLookup and
+    TestBatchedCyclicLookupRejectsMissingValue: four sources of module m
+    looked up in one table share one logup column of m; the two exposed
+    totals are bound to the transcript, so changing either is rejected; a
+    source value outside the table is refused by the prover."""
+    from loom_b200.program import Builder, Module, col, lookup
+    n = 16
+    b = Builder()
+    b.add_module(Module("m", n))
+    b.add_module(Module("tab", n))
+    totals = lookup(b, [(col(f"m.s{k}"), "m") for k in range(4)], [(col("tab.t"), "tab")])
+    assert [t.split(".")[0] for t in totals] == ["m", "tab"]  # one logup column per module
+    compiled = b.compile()
+    s2 = [3] * n
+    if bad:
+        s2[5] = 100
+    trace = {"tab.t": list(range(n)), "m.s0": list(range(n)), "m.s1": [n - 1 - i for i in range(n)],
+             "m.s2": s2, "m.s3": [i // 2 for i in range(n)]}
+    wit = _witness(b, compiled, trace)
+    if bad:
+        with pytest.raises(RuntimeError, match="not in the table"):
+            _prove(compiled, wit, 8)
+        return
+    pb = _prove(compiled, wit, 8)
+    oracle.verify(compiled.words, pb, 8, compiled.logup_buses)
+    offs = _exposed_offsets(pb)
+    assert len(offs) == 2 and set(proof.decode(pb).exposed) == set(offs)
+    for name, at in offs.items():
+        tampered = bytearray(pb)
+        struct.pack_into(">I", tampered, at, (struct.unpack_from(">I", pb, at)[0] + 1) % F.P)
+        with pytest.raises(oracle.VerifyError):
+            oracle.verify(compiled.words, bytes(tampered), 8, compiled.logup_buses)
