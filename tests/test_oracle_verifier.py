@@ -316,3 +316,30 @@ def test_batched_cyclic_lookup(bad):
         struct.pack_into(">I", tampered, at, (struct.unpack_from(">I", pb, at)[0] + 1) % F.P)
         with pytest.raises(oracle.VerifyError):
             oracle.verify(compiled.words, bytes(tampered), 8, compiled.logup_buses)
+
+
+@pytest.mark.parametrize("bad", [False, True])
+def test_lookup_selectors(bad):
+    """lookups_test.go TestLookupsSelectors: two selected sources of module a
+    into one selected table (one logup column per module); unselected source rows
+    hold anything; a selected source equal to an unselected table row is
+    refused."""
+    from loom_b200.program import Builder, Module, col, lookup_tuple
+    n = 8
+    b = Builder()
+    for name in ("a", "tab"):
+        b.add_module(Module(name, n))
+    totals = lookup_tuple(b, [([col("a.s0")], "a"), ([col("a.s1")], "a")], [([col("tab.t")], "tab")],
+                          sel_s=[col("a.sels0"), col("a.sels1")], sel_t=[col("tab.sel")])
+    compiled = b.compile()
+    assert compiled.logup_buses == [list(totals)] and [t.split(".")[0] for t in totals] == ["a", "tab"]
+    pad = lambda *v: list(v) + [0] * (n - len(v))
+    trace = {"tab.t": pad(10, 11, 12, 13), "tab.sel": pad(1, 1, 1, 0),
+             "a.s0": pad(10, 99, 12, 12), "a.sels0": pad(1, 0, 1, 1),
+             "a.s1": pad(11, 77, 13 if bad else 11), "a.sels1": pad(1, 0, 1)}
+    wit = _witness(b, compiled, trace)
+    if bad:
+        with pytest.raises(RuntimeError, match="not in the table"):
+            _prove(compiled, wit, 8)
+    else:
+        oracle.verify(compiled.words, _prove(compiled, wit, 8), 8, compiled.logup_buses)
