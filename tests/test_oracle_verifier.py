@@ -163,7 +163,8 @@ def test_conditional_tuple_lookup():
 
 
 def test_mixed_trace_round_trip_and_tampered_injection_row():
-    """verifier_test.go TestVerifyMixedTraceRoundTrip: a Fibonacci module of 4
+    """verifier_test.go TestVerifyMixedTraceRoundTrip (the fixture of
+    prover_test.go TestVanishingRelationsAndLogupBus): a Fibonacci module of 4
     rows (shifted columns, constraints except at the last row) looks up A, B
     and C in a range module of 8 rows, so the trace tree injects the smaller
     group; the proof verifies with its logup buses, and a tampered injection
@@ -189,6 +190,12 @@ def test_mixed_trace_round_trip_and_tampered_injection_row():
     oracle.verify(compiled.words, pb, 8, compiled.logup_buses)
 
     p = proof.decode(pb)
+    # prover_test.go TestVanishingRelationsAndLogupBus: every logup total is
+    # exposed with exactly one entry, and the totals of each bus sum to zero
+    for bus_totals in compiled.logup_buses:
+        assert all(len(p.exposed[name]) == 1 for name in bus_totals)
+        sums = [sum(p.exposed[name][0][2][k] for name in bus_totals) % F.P for k in range(6)]
+        assert sums == [0] * 6
     rows = [inj[0] for per in p.point_samplings for wp in per for inj in wp.injections]
     assert rows, "the mixed-size trace tree opens injection rows"
     words = rows[0].base
