@@ -350,3 +350,29 @@ def test_lookup_selectors(bad):
             _prove(compiled, wit, 8)
     else:
         oracle.verify(compiled.words, _prove(compiled, wit, 8), 8, compiled.logup_buses)
+
+
+@pytest.mark.parametrize("bad", [False, True])
+def test_lookups_share_target(bad):
+    """lookups_test.go TestLookupsShareTarget (grouped form): a.s0, a.s1 and
+    b.s looked up in one table give one bus with three totals (a, b, tab),
+    the two sources of module a batched in one logup column; a source value
+    outside the table is refused."""
+    from loom_b200.program import Builder, Module, col, lookup
+    n = 8
+    b = Builder()
+    for name in ("a", "b", "tab"):
+        b.add_module(Module(name, n))
+    totals = lookup(b, [(col("a.s0"), "a"), (col("a.s1"), "a"), (col("b.s"), "b")], [(col("tab.t"), "tab")])
+    compiled = b.compile()
+    assert compiled.logup_buses == [list(totals)] and [t.split(".")[0] for t in totals] == ["a", "b", "tab"]
+    bs = [5] * n
+    if bad:
+        bs[3] = 100
+    wit = _witness(b, compiled, {"tab.t": list(range(n)), "a.s0": [i // 2 for i in range(n)],
+                                 "a.s1": [n - 1 - i for i in range(n)], "b.s": bs})
+    if bad:
+        with pytest.raises(RuntimeError, match="not in the table"):
+            _prove(compiled, wit, 8)
+    else:
+        oracle.verify(compiled.words, _prove(compiled, wit, 8), 8, compiled.logup_buses)
