@@ -95,3 +95,42 @@ def test_bus_packs_factors_by_degree():
     assert all(e.startswith("m.busratio_") and e.endswith("_end") for e in ends)
     staged = b.rounds[0]["staged"]
     assert {"a0", "b2", "x1", "y0", "s2", "r1"} <= set(staged)
+
+
+def _lookup_shaped():
+    """rounds_test.go lookupShapedBuilder in spirit: sources s0, s1 of module m
+    looked up in t0, t1 of module tab, staged at the fold round."""
+    from loom_b200.program import Builder, Module, col, lookup
+    b = Builder()
+    b.add_module(Module("m", 8))
+    b.add_module(Module("tab", 8))
+    lookup(b, [(col("s0"), "m"), (col("s1"), "m")], [(col("t0"), "tab"), (col("t1"), "tab")])
+    return b
+
+
+def test_compile_rejects_double_staging():
+    """rounds_test.go TestCompileRoundsRejectsDoubleStaging."""
+    import pytest
+    from loom_b200.program import ROUND_LOG_DERIVATIVE
+    b = _lookup_shaped()
+    b.stage_columns(ROUND_LOG_DERIVATIVE, "s0")  # already staged at the fold round
+    with pytest.raises(ValueError, match="staged twice"):
+        b.compile()
+
+
+def test_staging_in_the_same_round_is_idempotent():
+    """rounds_test.go TestStageColumnsSameRoundIsIdempotent."""
+    from loom_b200.program import ROUND_FOLD
+    a, b = _lookup_shaped(), _lookup_shaped()
+    b.stage_columns(ROUND_FOLD, "s0", "t1")
+    assert np.array_equal(a.compile().words, b.compile().words)
+
+
+def test_compile_rejects_unknown_staged_column():
+    """rounds_test.go TestCompileRoundsRejectsUnknownColumn."""
+    import pytest
+    from loom_b200.program import ROUND_FOLD
+    b = _lookup_shaped()
+    b.stage_columns(ROUND_FOLD, "not_in_any_relation")
+    with pytest.raises(ValueError, match="not referenced by any relation"):
+        b.compile()
