@@ -2,8 +2,8 @@
  * loom_gpu.h — C ABI of the B200 (sm_100a) implementation of loom's
  * Poseidon2-backend prove phase (github.com/consensys/loom).
  *
- * The Go prover binds these functions through cgo;
- * Python binds them through ctypes.  Signatures use plain pointers and
+ * The Go prover binds these functions through a cgo shim package; Python
+ * binds them through ctypes (loom_b200/_lib.py).  Signatures use plain pointers and
  * sizes only.  Every function returns an int status (LG_OK = 0) and never
  * aborts; lg_last_error() describes the last failure on a context.
  *
@@ -86,11 +86,21 @@ enum {
 };
 
 typedef struct lg_ctx lg_ctx;
+/* A committed batch kept on the device: every group's LDE, coefficients and
+ * the Merkle tree (fri.Committed, internal/fri/pcs.go:131-168). */
+typedef struct lg_committed lg_committed;
+/* One prove of one program in progress, driven phase by phase by a caller
+ * that keeps the Fiat-Shamir transcript (the Go prover's runtime,
+ * prover/prover.go:142-719). */
+typedef struct lg_session lg_session;
 
 /* Creates a context (one CUDA stream, twiddle caches, memory pool) on
- * `device`.  Replaces nothing in the reference: the Go prover has no device
- * state; the cgo shim creates one context per GPU. */
-int lg_ctx_create(int device, lg_ctx** out);
+ * `device`.  `hbm_budget` caps the device bytes the context may hold at once
+ * (0: no cap); an allocation past it fails with LG_ERR_OOM.  Replaces nothing
+ * in the reference: the Go prover has no device state; the cgo shim creates
+ * one context per GPU.  Release every handle made on a context before
+ * destroying it. */
+int lg_ctx_create(int device, size_t hbm_budget, lg_ctx** out);
 void lg_ctx_destroy(lg_ctx* ctx);
 /* Launch partitioning of every phase: batched (1, the default) launches each
  * kernel once over all groups / modules of a size class; plain (0) launches
@@ -109,17 +119,31 @@ int lg_ctx_set_leaf_mapping(lg_ctx* ctx, int lanes_per_permutation);
  *   "p2_leaf_min_per_sm"  one thread per leaf / injection chain when a launch
  *                         has at least this many per SM (else six lanes)
  *   "p2_node_min_per_sm"  the same for one-permutation Merkle levels
+ *   "p2_inject_min_per_sm" the same for the injection chains
  *   "merkle_tail"         levels narrower than this (power of two, 2..1024)
  *                         run in one block
  *   "merkle_subtree"      above that, one launch builds the levels over
  *                         this many nodes per block (power of two, 2..1024;
  *                         0: a launch per level)
  *   "inject_block", "leaf_block"  threads per block (power of two, 32..1024)
+ *   "lde_split"           1: the LDE of 2^4..2^14 rows as an inverse launch
+ *                         plus one block per (lane, coset); 0: one block per
+ *                         lane for all of it
+ *   "lde_fwd_threads"     threads per coset block (256, 512 or 1024)
  * Unknown names or values out of range return LG_ERR_INVALID. */
 int lg_ctx_set_tuning(lg_ctx* ctx, const char* name, int64_t value);
 int lg_ctx_get_tuning(lg_ctx* ctx, const char* name, int64_t* value);
-/* Free and total device memory of the context's GPU (serving admission). */
+/* Free and total device memory of the context's GPU. */
 int lg_mem_info(lg_ctx* ctx, uint64_t* free_bytes, uint64_t* total_bytes);
+/* Device bytes a new allocation on `device` can get now — free memory plus
+ * the unused reserve of the device's default memory pool, which every context
+ * allocates from — and the total.  Needs no context and waits for no stream,
+ * so a serving loop calls it at admission time while other proves run. */
+int lg_device_mem_info(int device, uint64_t* available_bytes, uint64_t* total_bytes);
+/* Device bytes the context holds now (buffers, caches, arena chunks) and
+ * their high-water mark; reset_peak != 0 restarts the mark from now.  A
+ * serving loop reads the mark around a prove to learn that prove's peak. */
+int lg_ctx_mem_usage(lg_ctx* ctx, uint64_t* held_bytes, uint64_t* peak_bytes, int reset_peak);
 /* NUL-terminated description of the last failure on `ctx` (never NULL). */
 const char* lg_last_error(lg_ctx* ctx);
 
@@ -161,15 +185,108 @@ int lg_verify(lg_ctx* ctx, const uint32_t* program, size_t program_words, const 
 int lg_setup(lg_ctx* ctx, const uint32_t* program, size_t program_words, const uint32_t* const* setup_cols,
              int on_device, uint32_t root[8]);
 
-/* PCS.Commit of one batch (internal/fri/pcs.go:145-168 →
+/* ---- Phase-level entry points: the prover's phases with the transcript
+ * kept by the caller.  Challenges go in by their transcript names; every
+ * phase checks that the challenges it needs were given.  lg_prove runs the
+ * same phases with the library's own transcript, so both routes give the
+ * same proof bytes. */
+
+/* PCS.Commit of one batch (internal/fri/pcs.go:145-168 ->
  * internal/fri/commitment.go:259-386): RS-encode every polynomial at rate 4,
  * hash adjacent row pairs into leaves with Poseidon2LeafHasher.HashLeafPairs
  * (internal/fri/hash.go:63-120) and build the mixed-height tree
- * (internal/merkle/tree.go:117-327).  Group g has rows[g] Lagrange rows,
- * n_base[g] base columns then n_ext[g] ext columns (6 words per row) in
- * `cols`, group by group.  Writes the root. */
+ * (internal/merkle/tree.go:117-327), groups sorted by size, the largest the
+ * leaf level.  Group g has rows[g] Lagrange rows, n_base[g] base columns then
+ * n_ext[g] ext columns (ext.E6 rows, 6 words each) in `cols`, group by group.
+ * Writes the root, and in *out a handle that keeps LDE, coefficients and tree
+ * on the device for lg_committed_eval and lg_open_batches (PCS.Open,
+ * internal/fri/open.go:98-105) until lg_release. */
+int lg_commit(lg_ctx* ctx, uint32_t n_groups, const uint64_t* rows, const uint32_t* n_base, const uint32_t* n_ext,
+              const uint32_t* const* cols, int on_device, lg_committed** out, uint32_t root[8]);
+/* The root alone of the same commitment (nothing kept: no opening can
+ * follow). */
 int lg_commit_root(lg_ctx* ctx, uint32_t n_groups, const uint64_t* rows, const uint32_t* n_base,
                    const uint32_t* n_ext, const uint32_t* const* cols, int on_device, uint32_t root[8]);
+/* Values of a committed batch's polynomials at zeta * w_N^s for each shift s
+ * (w_N of the group's own size): computeClaimedValues
+ * (internal/fri/values.go:46-110) for one batch.  out (E6, 6 words each):
+ * group by group in declaration order, base polynomials then extension
+ * polynomials, each at every shift. */
+int lg_committed_eval(lg_ctx* ctx, const lg_committed* batch, const uint32_t zeta[6], uint32_t n_shifts,
+                      const int32_t* shifts, uint32_t* out);
+/* Openings of committed batches at FRI query positions s < 2^24
+ * (openCommittedAt, internal/fri/open.go:290-378): per position the batch
+ * count, then per batch the row pair of its largest group, that tree's
+ * Merkle path with its injected leaves, and the other groups' row pairs —
+ * in the canonical proof encoding.  LG_ERR_BUFFER writes the size needed. */
+int lg_open_batches(lg_ctx* ctx, uint32_t n_batches, const lg_committed* const* batches, const uint32_t* positions,
+                    uint32_t n_positions, uint8_t* out, size_t* out_len);
+
+/* Starts a prove of `program` (descriptor as for lg_prove) over `witness`
+ * (descriptor order; device witness columns are used in place and must stay
+ * unchanged until lg_release of the session) with num_queries FRI queries:
+ * newProverRuntime (prover/prover.go:142-275) without its transcript.  The
+ * caller binds "poseidon2", the module sizes in layout order and, for a
+ * program with setup columns, the setup root (lg_session_setup_root) to the
+ * first challenge, as the reference does. */
+int lg_session_begin(lg_ctx* ctx, const char* hash_backend, const uint32_t* program, size_t program_words,
+                     const uint32_t* const* witness, int witness_on_device, uint32_t num_queries, lg_session** out);
+/* The precommitted setup root of the session's program (*has_root = 0 when it
+ * has no setup columns). */
+int lg_session_setup_root(lg_session* s, uint32_t root[8], int* has_root);
+/* A challenge the caller's transcript computed (fiatshamir ComputeChallenge,
+ * internal/fiat-shamir/transcript.go:221-315), as its 8-word digest:
+ * "challenge@loom_<r>", "__zeta", "alpha_DEEP", "fri_level_<l>_gamma",
+ * "fri_fold_<j>". */
+int lg_session_challenge(lg_session* s, const char* name, const uint32_t digest[8]);
+/* Round r: ExecuteSteps and commitTraceRound (prover/prover.go:291-411) —
+ * the round's generated columns, then its batch commitment (*committed = 1
+ * and the root, which the caller binds to challenge@loom_<r>), then the
+ * round's exposed values (6 words each, step order; capacity *n_exposed, the
+ * count written back), which the caller binds after the root.  Needs the
+ * challenges of rounds < r. */
+int lg_commit_round(lg_session* s, uint32_t round, uint32_t root[8], int* committed, uint32_t* exposed,
+                    uint32_t* n_exposed);
+/* ComputeAIRQuotients (prover/prover.go:461-561 ->
+ * poly.ComputeQuotientMixed, internal/poly/compute_quotient.go:223-424) and
+ * the commitment of the quotient chunks; the caller binds the root to
+ * __zeta.  Needs every round's challenge. */
+int lg_quotient(lg_session* s, uint32_t root[8], int* committed);
+/* computeClaimedValues (internal/fri/values.go:46-110) at zeta, written in
+ * the order bindClaimedValuesByPolynomialOrder binds them to alpha_DEEP
+ * (internal/fri/open.go:223-285): 6 words each; capacity *n_values, the
+ * count written back. */
+int lg_claimed_values(lg_session* s, uint32_t* values, size_t* n_values);
+/* computeDeepQuotientCodewordsByPolynomial (internal/fri/deep.go:71-266) with
+ * alpha_DEEP. */
+int lg_deep(lg_session* s);
+/* fri.Prove's levels tree over the DEEP codewords (internal/fri/fri.go:
+ * 294-317,352-365): its root (the caller binds it to fri_level_1_gamma when
+ * there are several levels, and to fri_fold_<first_round>), the level count
+ * and the first round with a layer. */
+int lg_fri_commit_levels(lg_session* s, uint32_t root[8], uint32_t* n_levels, uint32_t* first_round);
+/* FRI round j (proveExt, internal/fri/fri.go:606-736): folds layer j with
+ * challenge fri_fold_<j> (foldLayerExt, fri.go:1177-1198), adds the levels
+ * that enter at j + 1 (their gammas must be set) and commits layer j + 1:
+ * *committed = 1 with its root, which the caller binds to fri_fold_<j+1>;
+ * 0 after the last round. */
+int lg_fri_fold_round(lg_session* s, uint32_t round, uint32_t root[8], int* committed);
+/* The FRI final polynomial after the last round (E6 values, 6 words each;
+ * capacity *n_values, the count written back); the caller binds it to
+ * fri_query_0 and derives the query positions. */
+int lg_fri_final(lg_session* s, uint32_t* values, size_t* n_values);
+/* The query openings at the caller's positions (openQueryExt,
+ * internal/fri/fri.go:1251-1272; openCommittedAt, internal/fri/open.go:
+ * 290-378) and the whole proof in the canonical encoding, as lg_prove writes
+ * it (on LG_ERR_BUFFER lg_last_proof copies it out). */
+int lg_open(lg_session* s, const uint32_t* positions, uint32_t n_positions, uint8_t* proof, size_t* proof_len);
+/* A handle to the session's committed batch `index` (layout order: the setup
+ * tree first when there is one, then the rounds' trees, then the AIR tree),
+ * for lg_committed_eval and lg_open_batches; it keeps the batch's device
+ * buffers after the session is released. */
+int lg_session_committed(lg_session* s, uint32_t index, lg_committed** out);
+/* Frees a handle (lg_committed or lg_session); NULL is ignored. */
+void lg_release(void* handle);
 
 /* reedsolomon.Encoder.Encode (internal/reedsolomon/rs.go:52-70) on
  * `n_cols` base columns of n_rows rows stored one after another in `in`;
@@ -222,7 +339,10 @@ int lg_grand_product(lg_ctx* ctx, const uint32_t* num, const uint32_t* den, uint
  * returns LG_ERR_UNSUPPORTED.  The first call on a device looks up that
  * array's address (make it before any stream capture); calls whose work
  * overlaps on the GPU share the array and race, so serialize them.  It calls
- * no cudaMalloc, cudaFree or other allocating routine. */
+ * no cudaMalloc, cudaFree or other allocating routine.  An error already
+ * pending on the calling thread is left in place and returns LG_ERR_CUDA
+ * before anything is launched; its four launches count in
+ * lg_kernel_launches(). */
 int lg_grand_product_noalloc(const uint32_t* num, const uint32_t* den, uint64_t n, uint32_t* out, void* cuda_stream);
 
 /* Measurement hooks (no counterpart in the reference, which times phases

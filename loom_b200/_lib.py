@@ -8,6 +8,7 @@ from __future__ import annotations
 import ctypes
 import os
 import threading
+import weakref
 from typing import List, Optional, Sequence
 
 import numpy as np
@@ -19,7 +20,11 @@ LG_OK, LG_ERR_INVALID, LG_ERR_CUDA, LG_ERR_OOM, LG_ERR_UNSUPPORTED, LG_ERR_BUFFE
 EXPORTS = ["lg_ctx_create", "lg_ctx_destroy", "lg_ctx_set_batched", "lg_ctx_set_leaf_mapping", "lg_ctx_set_tuning",
            "lg_ctx_get_tuning", "lg_mem_info", "lg_last_error", "lg_prove", "lg_last_proof", "lg_setup", "lg_verify", "lg_commit_root",
            "lg_rs_encode", "lg_poseidon2_permute", "lg_merkle_root", "lg_fri_fold", "lg_timer_mark",
-           "lg_timer_elapsed", "lg_kernel_launches", "lg_profile", "lg_profile_report", "lg_grand_product", "lg_grand_product_noalloc", "lg_deep_quotient"]
+           "lg_timer_elapsed", "lg_kernel_launches", "lg_profile", "lg_profile_report", "lg_grand_product", "lg_grand_product_noalloc", "lg_deep_quotient",
+           "lg_ctx_mem_usage", "lg_device_mem_info", "lg_commit", "lg_committed_eval", "lg_open_batches", "lg_session_begin",
+           "lg_session_setup_root", "lg_session_challenge", "lg_commit_round", "lg_quotient", "lg_claimed_values",
+           "lg_deep", "lg_fri_commit_levels", "lg_fri_fold_round", "lg_fri_final", "lg_open", "lg_session_committed",
+           "lg_release"]
 
 u32p = ctypes.POINTER(ctypes.c_uint32)
 u64p = ctypes.POINTER(ctypes.c_uint64)
@@ -42,7 +47,31 @@ def load():
             raise LoomError(LG_ERR_UNSUPPORTED, f"{LIB_PATH} is not built; run python -m loom_b200.build")
         L = ctypes.CDLL(LIB_PATH)
         vp = ctypes.c_void_p
-        L.lg_ctx_create.argtypes = [ctypes.c_int, ctypes.POINTER(vp)]
+        L.lg_ctx_create.argtypes = [ctypes.c_int, ctypes.c_size_t, ctypes.POINTER(vp)]
+        L.lg_ctx_mem_usage.argtypes = [vp, u64p, u64p, ctypes.c_int]
+        L.lg_device_mem_info.argtypes = [ctypes.c_int, u64p, u64p]
+        szp = ctypes.POINTER(ctypes.c_size_t)
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.lg_commit.argtypes = [vp, ctypes.c_uint32, u64p, u32p, u32p, ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
+                                ctypes.POINTER(vp), u32p]
+        L.lg_committed_eval.argtypes = [vp, vp, u32p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_int32), u32p]
+        L.lg_open_batches.argtypes = [vp, ctypes.c_uint32, ctypes.POINTER(vp), u32p, ctypes.c_uint32,
+                                      ctypes.POINTER(ctypes.c_uint8), szp]
+        L.lg_session_begin.argtypes = [vp, ctypes.c_char_p, u32p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p),
+                                       ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(vp)]
+        L.lg_session_setup_root.argtypes = [vp, u32p, ip]
+        L.lg_session_challenge.argtypes = [vp, ctypes.c_char_p, u32p]
+        L.lg_commit_round.argtypes = [vp, ctypes.c_uint32, u32p, ip, u32p, u32p]
+        L.lg_quotient.argtypes = [vp, u32p, ip]
+        L.lg_claimed_values.argtypes = [vp, u32p, szp]
+        L.lg_deep.argtypes = [vp]
+        L.lg_fri_commit_levels.argtypes = [vp, u32p, u32p, u32p]
+        L.lg_fri_fold_round.argtypes = [vp, ctypes.c_uint32, u32p, ip]
+        L.lg_fri_final.argtypes = [vp, u32p, szp]
+        L.lg_open.argtypes = [vp, u32p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint8), szp]
+        L.lg_session_committed.argtypes = [vp, ctypes.c_uint32, ctypes.POINTER(vp)]
+        L.lg_release.argtypes = [vp]
+        L.lg_release.restype = None
         L.lg_ctx_destroy.argtypes = [vp]
         L.lg_ctx_destroy.restype = None
         L.lg_ctx_set_batched.argtypes = [vp, ctypes.c_int]
@@ -90,22 +119,26 @@ def _ptr(a: np.ndarray):
 class Context:
     """A device context (lg_ctx): one CUDA stream, caches and memory pool."""
 
-    def __init__(self, device: int = 0, tuning: Optional[dict] = None):
+    def __init__(self, device: int = 0, tuning: Optional[dict] = None, hbm_budget: int = 0):
         """`tuning`: launch-shape values to apply (see set_tuning), e.g. the
-        "params" of loom_b200.autotune.autotune()."""
+        "params" of loom_b200.autotune.autotune().  `hbm_budget`: device
+        bytes this context may hold at once (0: no cap)."""
         self.L = load()
         self.device = device
         self.h = ctypes.c_void_p()
-        rc = self.L.lg_ctx_create(device, ctypes.byref(self.h))
+        rc = self.L.lg_ctx_create(device, int(hbm_budget), ctypes.byref(self.h))
         if rc != LG_OK:
             raise LoomError(rc, f"lg_ctx_create failed on device {device}")
         self._proof_cap = 1 << 22
         self._proof_buf = (ctypes.c_uint8 * self._proof_cap)()
+        self._handles = weakref.WeakSet()  # sessions and committed batches made on this context
         if tuning:
             self.apply_tuning(tuning)
 
     def close(self):
         if self.h:
+            for hd in list(self._handles):  # handles go before their context
+                hd.release()
             self.L.lg_ctx_destroy(self.h)
             self.h = ctypes.c_void_p()
 
@@ -130,8 +163,24 @@ class Context:
         self._check(self.L.lg_mem_info(self.h, ctypes.byref(f), ctypes.byref(t)))
         return int(f.value), int(t.value)
 
-    TUNING_NAMES = ("p2_leaf_min_per_sm", "p2_node_min_per_sm", "merkle_tail", "merkle_subtree", "inject_block",
-                    "leaf_block")
+    def device_available(self) -> int:
+        """Device bytes a new allocation can get now (free memory plus the
+        memory pool's unused reserve); waits for no stream."""
+        a, t = ctypes.c_uint64(), ctypes.c_uint64()
+        rc = self.L.lg_device_mem_info(self.device, ctypes.byref(a), ctypes.byref(t))
+        if rc != LG_OK:
+            raise LoomError(rc, "lg_device_mem_info failed")
+        return int(a.value)
+
+    def mem_usage(self, reset_peak: bool = False):
+        """(held, peak) device bytes of this context; reset_peak restarts the
+        high-water mark from the bytes held now."""
+        h, pk = ctypes.c_uint64(), ctypes.c_uint64()
+        self._check(self.L.lg_ctx_mem_usage(self.h, ctypes.byref(h), ctypes.byref(pk), int(reset_peak)))
+        return int(h.value), int(pk.value)
+
+    TUNING_NAMES = ("p2_leaf_min_per_sm", "p2_node_min_per_sm", "p2_inject_min_per_sm", "merkle_tail",
+                    "merkle_subtree", "inject_block", "leaf_block", "lde_split", "lde_fwd_threads")
 
     def set_tuning(self, name: str, value: int):
         """Launch-shape choice (see include/loom_gpu.h); proofs do not depend on it."""
@@ -266,6 +315,45 @@ class Context:
                                           ne.ctypes.data_as(u32p), arr, 0, root.ctypes.data_as(u32p)))
         return root
 
+    def _batch_args(self, groups: List[dict]):
+        rows = np.array([g["rows"] for g in groups], dtype=np.uint64)
+        nb = np.array([len(g.get("base", [])) for g in groups], dtype=np.uint32)
+        ne = np.array([len(g.get("ext", [])) for g in groups], dtype=np.uint32)
+        cols = []
+        for g in groups:
+            cols += [_u32(c) for c in g.get("base", [])] + [_u32(c).reshape(-1) for c in g.get("ext", [])]
+        arr = (ctypes.c_void_p * max(1, len(cols)))(*[c.ctypes.data for c in cols])
+        return rows, nb, ne, cols, arr
+
+    def commit(self, groups: List[dict]) -> "Committed":
+        """PCS.Commit keeping the batch on the device: groups of
+        {"rows": N, "base": [N words], "ext": [N x 6 words]} (Montgomery)."""
+        rows, nb, ne, cols, arr = self._batch_args(groups)
+        root = np.zeros(8, dtype=np.uint32)
+        h = ctypes.c_void_p()
+        self._check(self.L.lg_commit(self.h, len(groups), rows.ctypes.data_as(u64p), nb.ctypes.data_as(u32p),
+                                     ne.ctypes.data_as(u32p), arr, 0, ctypes.byref(h), root.ctypes.data_as(u32p)))
+        return Committed(self, h, root, [int(x) for x in nb], [int(x) for x in ne])
+
+    def open_batches(self, batches: Sequence["Committed"], positions: Sequence[int]) -> bytes:
+        """Openings of committed batches at FRI positions, in the proof's
+        encoding (openCommittedAt for every position)."""
+        hs = (ctypes.c_void_p * len(batches))(*[b.h.value for b in batches])
+        pos = _u32(positions)
+        n = ctypes.c_size_t(0)
+        rc = self.L.lg_open_batches(self.h, len(batches), hs, pos.ctypes.data_as(u32p), pos.size, None, ctypes.byref(n))
+        if rc != LG_ERR_BUFFER:
+            self._check(rc)
+        buf = (ctypes.c_uint8 * max(1, n.value))()
+        self._check(self.L.lg_open_batches(self.h, len(batches), hs, pos.ctypes.data_as(u32p), pos.size, buf,
+                                           ctypes.byref(n)))
+        return bytes(memoryview(buf)[:n.value])
+
+    def session(self, program_words: np.ndarray, witness: Sequence, num_queries: int, on_device: bool = False,
+                hash_backend: str = "poseidon2") -> "Session":
+        """A prove driven phase by phase with the caller's transcript."""
+        return Session(self, program_words, witness, num_queries, on_device, hash_backend)
+
     def rs_encode(self, cols: np.ndarray) -> np.ndarray:
         c = _u32(cols)
         if c.ndim == 1:
@@ -309,3 +397,143 @@ class Context:
         out = np.zeros((x.shape[0] // 2, 6), dtype=np.uint32)
         self._check(self.L.lg_fri_fold(self.h, _ptr(x), x.shape[0], a.ctypes.data_as(u32p), _ptr(out), 0))
         return out
+
+
+class Committed:
+    """A committed batch on the device (lg_committed)."""
+
+    def __init__(self, ctx: Context, h, root: np.ndarray, nb: List[int], ne: List[int]):
+        self.ctx, self.h, self.root, self.nb, self.ne = ctx, h, root, nb, ne
+        ctx._handles.add(self)
+
+    def eval(self, zeta, shifts: Sequence[int]) -> np.ndarray:
+        """Values at zeta w^s of every polynomial (group by group, base then
+        ext), each at every shift: (polys, shifts, 6) Montgomery words."""
+        z = _u32(zeta)
+        sh = np.ascontiguousarray(shifts, dtype=np.int32)
+        npoly = sum(self.nb) + sum(self.ne)
+        out = np.zeros((npoly, len(sh), 6), dtype=np.uint32)
+        self.ctx._check(self.ctx.L.lg_committed_eval(self.ctx.h, self.h, z.ctypes.data_as(u32p), len(sh),
+                                                     sh.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                                     out.ctypes.data_as(u32p)))
+        return out
+
+    def release(self):
+        if self.h and self.h.value:
+            self.ctx.L.lg_release(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+
+class Session:
+    """One prove driven phase by phase (lg_session_*): the caller keeps the
+    Fiat-Shamir transcript and hands each challenge in by name."""
+
+    def __init__(self, ctx: Context, program_words, witness, num_queries: int, on_device: bool, hash_backend: str):
+        self.ctx, self.L = ctx, ctx.L
+        prog = _u32(program_words)
+        if on_device:
+            self._arr = (ctypes.c_void_p * max(1, len(witness)))(*[int(p) for p in witness])
+        else:
+            self._cols = [_u32(c) for c in witness]
+            self._arr = (ctypes.c_void_p * max(1, len(self._cols)))(*[c.ctypes.data for c in self._cols])
+        self.h = ctypes.c_void_p()
+        ctx._check(self.L.lg_session_begin(ctx.h, hash_backend.encode(), prog.ctypes.data_as(u32p), prog.size,
+                                           self._arr, int(on_device), num_queries, ctypes.byref(self.h)))
+        ctx._handles.add(self)
+
+    def _ck(self, rc):
+        self.ctx._check(rc)
+
+    def setup_root(self):
+        root = np.zeros(8, dtype=np.uint32)
+        has = ctypes.c_int()
+        self._ck(self.L.lg_session_setup_root(self.h, root.ctypes.data_as(u32p), ctypes.byref(has)))
+        return root if has.value else None
+
+    def challenge(self, name: str, digest) -> None:
+        d = _u32(digest)
+        assert d.size == 8
+        self._ck(self.L.lg_session_challenge(self.h, name.encode(), d.ctypes.data_as(u32p)))
+
+    def commit_round(self, r: int):
+        """(root or None, exposed values as an (n, 6) array)."""
+        root = np.zeros(8, dtype=np.uint32)
+        com = ctypes.c_int()
+        cap = 4096
+        ex = np.zeros((cap, 6), dtype=np.uint32)
+        n = ctypes.c_uint32(cap)
+        self._ck(self.L.lg_commit_round(self.h, r, root.ctypes.data_as(u32p), ctypes.byref(com),
+                                        ex.ctypes.data_as(u32p), ctypes.byref(n)))
+        return (root if com.value else None), ex[:n.value].copy()
+
+    def quotient(self):
+        root = np.zeros(8, dtype=np.uint32)
+        com = ctypes.c_int()
+        self._ck(self.L.lg_quotient(self.h, root.ctypes.data_as(u32p), ctypes.byref(com)))
+        return root if com.value else None
+
+    def _values(self, fn) -> np.ndarray:
+        n = ctypes.c_size_t(0)
+        rc = fn(None, ctypes.byref(n))
+        if rc != LG_ERR_BUFFER:
+            self._ck(rc)
+        out = np.zeros((max(1, n.value), 6), dtype=np.uint32)
+        self._ck(fn(out.ctypes.data_as(u32p), ctypes.byref(n)))
+        return out[:n.value]
+
+    def claimed_values(self) -> np.ndarray:
+        return self._values(lambda p, n: self.L.lg_claimed_values(self.h, p, n))
+
+    def deep(self):
+        self._ck(self.L.lg_deep(self.h))
+
+    def fri_commit_levels(self):
+        """(levels root, level count, first round with a layer)."""
+        root = np.zeros(8, dtype=np.uint32)
+        nl, r0 = ctypes.c_uint32(), ctypes.c_uint32()
+        self._ck(self.L.lg_fri_commit_levels(self.h, root.ctypes.data_as(u32p), ctypes.byref(nl), ctypes.byref(r0)))
+        return root, int(nl.value), int(r0.value)
+
+    def fri_fold_round(self, j: int):
+        root = np.zeros(8, dtype=np.uint32)
+        com = ctypes.c_int()
+        self._ck(self.L.lg_fri_fold_round(self.h, j, root.ctypes.data_as(u32p), ctypes.byref(com)))
+        return root if com.value else None
+
+    def fri_final(self) -> np.ndarray:
+        return self._values(lambda p, n: self.L.lg_fri_final(self.h, p, n))
+
+    def open(self, positions: Sequence[int]) -> bytes:
+        pos = _u32(positions)
+        n = ctypes.c_size_t(0)
+        rc = self.L.lg_open(self.h, pos.ctypes.data_as(u32p), pos.size, None, ctypes.byref(n))
+        if rc == LG_ERR_BUFFER:
+            buf = (ctypes.c_uint8 * n.value)()
+            self._ck(self.L.lg_last_proof(self.ctx.h, buf, ctypes.byref(n)))
+            return bytes(memoryview(buf)[:n.value])
+        self._ck(rc)
+        return b""
+
+    def committed(self, index: int, nb: Sequence[int] = (), ne: Sequence[int] = ()) -> Committed:
+        """Handle to committed batch `index` (layout order); nb / ne: its
+        groups' polynomial counts, for Committed.eval's output shape."""
+        h = ctypes.c_void_p()
+        self._ck(self.L.lg_session_committed(self.h, index, ctypes.byref(h)))
+        return Committed(self.ctx, h, None, list(nb), list(ne))
+
+    def release(self):
+        if self.h and self.h.value:
+            self.L.lg_release(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass

@@ -1,14 +1,16 @@
 """Autotuner for the launch-shape choices of libloom_gpu (lg_ctx_set_tuning in
-include/loom_gpu.h): the Poseidon2 lane mapping thresholds, the width below
-which Merkle levels run in one block, and block sizes.  Proof bytes never
-depend on them; only time does.
+include/loom_gpu.h): the Poseidon2 lane mapping thresholds (leaves, injection
+chains, Merkle levels), the width below which Merkle levels run in one block,
+block sizes, and the NTT's launch structure (the LDE fused into one block per
+lane or split into an inverse launch and one block per coset, and the coset
+blocks' thread count).  Proof bytes never depend on them; only time does.
 
 For each parameter in turn (coordinate descent from the current values), every
-candidate value is timed on representative Poseidon2 commits: the round
-commit of many equal modules (leaf hashing plus a long injection chain per
-node), one wide column batch, and small trees whose top levels are latency
-bound.  Times are the library's CUDA events around its Poseidon2 kernels
-(median of a few runs), summed over the shapes.  The winner of every parameter
+candidate value is timed on representative commits: the round commit of many
+equal modules (LDE, leaf hashing plus a long injection chain per node), one
+wide column batch, and small trees whose top levels are latency bound.  Times
+are the library's CUDA events around its LDE and Poseidon2 kernels (median of
+a few runs), summed over the shapes.  The winner of every parameter
 is kept, and the result is cached per GPU (name, SM count) and library build
 in a JSON file: $LOOM_B200_TUNING, else ~/.cache/loom_b200/tuning.json.
 """
@@ -27,14 +29,17 @@ from . import _lib
 from . import field as F
 
 CANDIDATES: Dict[str, Sequence[int]] = {
+    "lde_split": (0, 1),
+    "lde_fwd_threads": (256, 512, 1024),
     "p2_leaf_min_per_sm": (32, 64, 128, 256, 512),
+    "p2_inject_min_per_sm": (64, 128, 256, 512, 1 << 20),
     "p2_node_min_per_sm": (128, 256, 512, 1024, 2048),
     "merkle_tail": (16, 32, 64, 128),
     "merkle_subtree": (0, 8, 16, 32, 64),
     "inject_block": (32, 64, 128),
     "leaf_block": (64, 128, 256),
 }
-P2_KERNELS = ("hash_leaves", "merkle_level", "merkle_inject", "merkle_tail")
+TIMED_KERNELS = ("lde", "lde_inv", "hash_leaves", "merkle_level", "merkle_inject", "merkle_tail")
 # (groups, log2 rows per group, base columns per group): the round commit of
 # 40 plonk modules of 2^14 rows, a wide batch, a mid-size batch, small trees
 SHAPES: Tuple[Tuple[int, int, int], ...] = ((40, 14, 3), (1, 16, 16), (8, 12, 3), (4, 9, 4))
@@ -91,7 +96,7 @@ def _time_shapes(ctx, shapes: List[List[dict]], runs: int) -> float:
             ctx.commit_root(gs)
             rep = ctx.profile_report()
             ctx.profile(False)
-            samples.append(sum(rep[k]["ms"] for k in P2_KERNELS if k in rep))
+            samples.append(sum(rep[k]["ms"] for k in TIMED_KERNELS if k in rep))
         total += statistics.median(samples)
     return total
 

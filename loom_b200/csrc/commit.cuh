@@ -135,17 +135,62 @@ inline void launch_lde(Ctx& c, const std::vector<LdeLane>& lanes, uint32_t log_n
     big_ntt(c, fwd_jobs, (int)log_n, false, "lde", 20.0 * n / (1 << RATE_LOG));
     return;
   }
-  auto tab = upload_vec(c, lanes);
   const uint32_t* twn = c.twiddles((int)log_n);
   const uint32_t* tw4 = c.twiddles((int)log_n + RATE_LOG);
-  size_t smem = 2 * pad16_words((int)log_n) * 4;
-  with_ntt_size((int)log_n, [&](auto L) {
-    allow_smem(k_lde<decltype(L)::value>, smem);
-    c.timed("lde", 20.0 * n * lanes.size(), 0, [&] {
-      k_lde<decltype(L)::value><<<(unsigned)lanes.size(), ntt_threads((int)log_n), smem, c.stream>>>(
-          (const LdeLane*)tab->p, (int)log_n, from_coeffs ? 1 : 0, twn, tw4, inv(to_mont((uint32_t)n)));
-      LG_LAUNCH();
+  const size_t smem = 2 * pad16_words((int)log_n) * 4;
+  const double bytes = 20.0 * n * lanes.size();
+  if (!c.tune.lde_split || log_n < 4) {
+    // one block per lane: inverse transform and the coset transforms
+    auto tab = upload_vec(c, lanes);
+    with_ntt_size((int)log_n, [&](auto L) {
+      allow_smem(k_lde<decltype(L)::value>, smem);
+      c.timed("lde", bytes, 0, [&] {
+        k_lde<decltype(L)::value><<<(unsigned)lanes.size(), ntt_threads((int)log_n), smem, c.stream>>>(
+            (const LdeLane*)tab->p, (int)log_n, from_coeffs ? 1 : 0, twn, tw4, inv(to_mont((uint32_t)n)));
+        LG_LAUNCH();
+      });
     });
+    return;
+  }
+  // split: the inverse transforms (coset 0 and the coefficients) in one
+  // launch, then the coset transforms, one block per (lane, coset)
+  std::vector<LdeLane> lv = lanes;
+  DBufP tmp;
+  size_t missing = 0;
+  for (auto& L : lv) missing += !from_coeffs && !L.coef;
+  if (missing) tmp = std::make_shared<DBuf>(missing * n, c.stream);
+  for (size_t i = 0, k = 0; i < lv.size(); i++)
+    if (!from_coeffs && !lv[i].coef) lv[i].coef = tmp->p + (k++) * n;
+  auto tab = upload_vec(c, lv);
+  if (from_coeffs)  // the coefficients themselves are kept when asked for
+    for (auto& L : lv)
+      if (L.coef) LG_CK(cudaMemcpyAsync(L.coef, L.src, n * 4, cudaMemcpyDeviceToDevice, c.stream));
+  with_ntt_size((int)log_n, [&](auto L) {
+    constexpr int LG = decltype(L)::value;
+    if (!from_coeffs) {
+      allow_smem(k_lde<LG>, smem);
+      c.timed("lde_inv", 8.0 * n * lv.size(), 0, [&] {
+        k_lde<LG><<<(unsigned)lv.size(), ntt_threads((int)log_n), smem, c.stream>>>(
+            (const LdeLane*)tab->p, (int)log_n, 0, twn, tw4, inv(to_mont((uint32_t)n)), 0);
+        LG_LAUNCH();
+      });
+    }
+    const int first = from_coeffs ? 0 : 1;
+    const dim3 grid((unsigned)lv.size(), (unsigned)((1 << RATE_LOG) - first));
+    const size_t fsmem = pad16_words((int)log_n) * 4;
+    const unsigned thr = (unsigned)std::min<int>(ntt_threads((int)log_n), (int)c.tune.lde_fwd_threads);
+    auto go = [&](auto kern) {
+      allow_smem(kern, fsmem);
+      c.timed("lde", bytes - (from_coeffs ? 0.0 : 8.0 * n * lv.size()), 0, [&] {
+        kern<<<grid, thr, fsmem, c.stream>>>((const LdeLane*)tab->p, first, twn, tw4);
+        LG_LAUNCH();
+      });
+    };
+    if constexpr (LG >= 4) {
+      if (thr <= 256) go(k_lde_fwd<LG, 256>);
+      else if (thr <= 512) go(k_lde_fwd<LG, 512>);
+      else go(k_lde_fwd<LG, 1024>);
+    }
   });
 }
 
@@ -264,7 +309,7 @@ inline void build_tree(Ctx& c, TreeDev& t, bool read_root = true) {
     const uint32_t* const* tab = (const uint32_t* const*)t.inj_ptrs->p + first;
     uint32_t cnt = (uint32_t)(next - first);
     c.timed("merkle_inject", 96.0 * start * cnt, (double)start * cnt, [&] {
-      if (p2_per_thread(c, start, c.tune.p2_leaf_min_per_sm)) {
+      if (p2_per_thread(c, start, c.tune.p2_inject_min_per_sm)) {
         // small blocks (one warp by default): chains are few (down to ~200
         // per SM) and long, so small blocks spread them evenly over the SMs
         const unsigned ib = c.tune.inject_block;

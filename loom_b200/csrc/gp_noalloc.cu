@@ -16,6 +16,12 @@
 #include "../../include/loom_gpu.h"
 #include "field.cuh"
 
+namespace lg {
+// Kernel launch counter of the library (lg_kernel_launches), defined with the
+// other entry points.
+void note_launches(uint64_t k);
+}  // namespace lg
+
 namespace {
 
 using namespace lg;
@@ -118,6 +124,9 @@ extern "C" int lg_grand_product_noalloc(const uint32_t* num, const uint32_t* den
                                         void* stream) {
   if (!num || !den || !out || n == 0) return LG_ERR_INVALID;
   if (n > NOALLOC_GP_MAX_ROWS) return LG_ERR_UNSUPPORTED;
+  // An error already pending on this thread (from the caller's own work) is
+  // left in place and reported, not cleared and taken for one of ours.
+  if (cudaPeekAtLastError() != cudaSuccess) return LG_ERR_CUDA;
   uint32_t* scratch = nullptr;
   int rc = scratch_for_current_device(&scratch);
   if (rc != LG_OK) return rc;
@@ -130,5 +139,6 @@ extern "C" int lg_grand_product_noalloc(const uint32_t* num, const uint32_t* den
   k_na_scan<<<nt, NA_THREADS, 0, st>>>(out, n, totals);
   k_na_prefix<<<1, 1, 0, st>>>(totals, nt, pre);
   k_na_apply<<<g, 256, 0, st>>>(out, n, pre);
+  note_launches(4);
   return cudaGetLastError() == cudaSuccess ? LG_OK : LG_ERR_CUDA;
 }

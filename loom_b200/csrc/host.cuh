@@ -44,6 +44,34 @@ inline std::atomic<uint64_t> g_launches{0};
     ::lg::g_launches.fetch_add(1);  \
   } while (0)
 
+// Device bytes held by one context (its DBuf allocations and arena chunks),
+// their high-water mark, and an optional cap (lg_ctx_create's hbm_budget:
+// an allocation past it fails with LG_ERR_OOM).  Calls on a context charge
+// their allocations to it through g_mem_acct.
+struct MemAcct {
+  std::atomic<int64_t> held{0}, peak{0};
+  int64_t budget = 0;  // bytes; 0 = no cap
+  void charge(int64_t b) {
+    const int64_t now = held.fetch_add(b) + b;
+    if (budget && now > budget) {
+      held.fetch_sub(b);
+      throw Error(LG_ERR_OOM, "context HBM budget of " + std::to_string(budget) + " bytes exceeded (" +
+                                  std::to_string(now) + " bytes needed)");
+    }
+    int64_t p = peak.load();
+    while (now > p && !peak.compare_exchange_weak(p, now)) {}
+  }
+  void refund(int64_t b) { held.fetch_sub(b); }
+};
+inline thread_local MemAcct* g_mem_acct = nullptr;
+struct AcctScope {
+  MemAcct* prev;
+  explicit AcctScope(MemAcct* a) : prev(g_mem_acct) { g_mem_acct = a; }
+  ~AcctScope() { g_mem_acct = prev; }
+  AcctScope(const AcctScope&) = delete;
+  AcctScope& operator=(const AcctScope&) = delete;
+};
+
 // Prove-scoped device memory: the small buffers of one prove (upload tables,
 // per-group scratch; about a thousand per prove) come from a bump arena of
 // retained chunks instead of one stream-ordered pool allocation and free
@@ -53,6 +81,7 @@ struct DevArena {
   static constexpr size_t MAX_OBJ = (size_t)1 << 20, CHUNK = (size_t)32 << 20, ALIGN = 256;
   std::vector<std::pair<uint8_t*, size_t>> chunks;
   size_t cur = 0, off = 0;
+  MemAcct* acct = nullptr;  // charged for the chunks
   void* take(size_t bytes, cudaStream_t s) {
     bytes = (bytes + ALIGN - 1) & ~(ALIGN - 1);
     while (cur < chunks.size() && off + bytes > chunks[cur].second) {
@@ -62,7 +91,16 @@ struct DevArena {
     if (cur == chunks.size()) {
       uint8_t* p = nullptr;
       size_t sz = std::max(CHUNK, bytes);
-      LG_CK(cudaMallocAsync((void**)&p, sz, s));
+      if (g_mem_acct) {
+        if (acct && acct != g_mem_acct) throw Error(LG_ERR_INVALID, "device arena shared between contexts");
+        g_mem_acct->charge((int64_t)sz);
+        acct = g_mem_acct;
+      }
+      if (cudaMallocAsync((void**)&p, sz, s) != cudaSuccess) {
+        cudaGetLastError();
+        if (g_mem_acct) g_mem_acct->refund((int64_t)sz);
+        throw Error(LG_ERR_OOM, "device arena chunk allocation failed");
+      }
       chunks.push_back({p, sz});
       off = 0;
     }
@@ -72,7 +110,10 @@ struct DevArena {
   }
   void rewind() { cur = 0; off = 0; }
   void release(cudaStream_t s) {
-    for (auto& c : chunks) cudaFreeAsync(c.first, s);
+    for (auto& c : chunks) {
+      cudaFreeAsync(c.first, s);
+      if (acct) acct->refund((int64_t)c.second);
+    }
     chunks.clear();
     rewind();
   }
@@ -94,6 +135,7 @@ struct DBuf {
   size_t words = 0;
   cudaStream_t st = nullptr;
   bool borrowed = false;  // caller-owned memory: never freed here
+  MemAcct* acct = nullptr;  // charged for this allocation
   DBuf() = default;
   DBuf(size_t w, cudaStream_t s) : words(w), st(s) {
     if (!w) return;
@@ -101,7 +143,19 @@ struct DBuf {
       p = (uint32_t*)g_dev_arena->take(w * 4, s);
       borrowed = true;  // the arena owns it
     } else {
-      LG_CK(cudaMallocAsync((void**)&p, w * 4, s));
+      if (g_mem_acct) {
+        g_mem_acct->charge((int64_t)(w * 4));
+        acct = g_mem_acct;
+      }
+      const cudaError_t e = cudaMallocAsync((void**)&p, w * 4, s);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        if (acct) acct->refund((int64_t)(w * 4));
+        acct = nullptr;
+        p = nullptr;
+        throw Error(e == cudaErrorMemoryAllocation ? LG_ERR_OOM : LG_ERR_CUDA,
+                    std::string("device allocation of ") + std::to_string(w * 4) + " bytes: " + cudaGetErrorString(e));
+      }
     }
   }
   DBuf(const DBuf&) = delete;
@@ -110,16 +164,20 @@ struct DBuf {
   DBuf& operator=(DBuf&& o) noexcept {
     if (this != &o) {
       release();
-      p = o.p; words = o.words; st = o.st; borrowed = o.borrowed;
-      o.p = nullptr; o.words = 0;
+      p = o.p; words = o.words; st = o.st; borrowed = o.borrowed; acct = o.acct;
+      o.p = nullptr; o.words = 0; o.acct = nullptr;
     }
     return *this;
   }
   ~DBuf() { release(); }
   void release() {
-    if (p && !borrowed) cudaFreeAsync(p, st);
+    if (p && !borrowed) {
+      cudaFreeAsync(p, st);
+      if (acct) acct->refund((int64_t)(words * 4));
+    }
     p = nullptr;
     words = 0;
+    acct = nullptr;
   }
 };
 using DBufP = std::shared_ptr<DBuf>;
@@ -146,6 +204,7 @@ struct Ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   DevArena dev_arena;            // prove-scoped small device buffers
+  MemAcct mem;                   // device bytes this context holds (lg_ctx_mem_usage)
   std::map<int, DBufP> tw;       // log n -> w_n^j, j < n
   std::map<int, DBufP> gpow;     // log n -> g^k, k < n
   std::map<int, DBufP> ginvpow;  // log n -> g^-k, k < n
@@ -289,10 +348,13 @@ struct Ctx {
   struct Tuning {
     uint32_t p2_leaf_min_per_sm = 128;  // one thread per leaf / injection chain from this many per SM
     uint32_t p2_node_min_per_sm = 512;  // one thread per node of a Merkle level from this many per SM
+    uint32_t p2_inject_min_per_sm = 128;  // one thread per injection chain from this many per SM
     uint32_t merkle_tail = 32;          // levels narrower than this run in one block
     uint32_t merkle_subtree = 16;       // nodes a block reduces to one in the levels above (0: a launch per level)
     uint32_t inject_block = 32;         // threads per block, one-thread injection chains
     uint32_t leaf_block = 128;          // threads per block, one-thread leaf hashing
+    uint32_t lde_split = 1;             // LDE as an inverse launch plus one block per (lane, coset)
+    uint32_t lde_fwd_threads = 512;     // threads per block of the coset transforms (split LDE)
   } tune;
 };
 

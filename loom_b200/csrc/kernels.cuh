@@ -95,9 +95,11 @@ __global__ void k_intt(uint32_t* const* lanes, int logn_rt, const uint32_t* tw_n
 // Optionally writes the coefficients.  Shared memory: A (coefficients) and B
 // (work), pad16 layout.
 struct LdeLane { const uint32_t* src; uint32_t* out; uint32_t* coef; };
+// fwd = 0: only the inverse transform, coset 0 and the coefficients (L.coef,
+// which must be set); k_lde_fwd then runs the other cosets.
 template <int LOGN>
 __global__ void k_lde(const LdeLane* lanes, int logn_rt, int from_coeffs, const uint32_t* tw_n, const uint32_t* tw_4n,
-                      uint32_t n_inv) {
+                      uint32_t n_inv, int fwd = 1) {
   const int logn = LOGN ? LOGN : logn_rt;
   extern __shared__ uint32_t sm[];
   const uint32_t n = 1u << logn;
@@ -163,6 +165,7 @@ __global__ void k_lde(const LdeLane* lanes, int logn_rt, int from_coeffs, const 
     };
     ntt16<false>(A, logn, tw_n, true, first, store, coset0);  // A is both work and result
   }
+  if (!fwd) return;
   for (int a = from_coeffs ? 0 : 1; a < (1 << RATE_LOG); a++) {
     const uint32_t e = bitrev32((uint32_t)a, RATE_LOG);
     uint32_t* o = L.out + (uint64_t)a * n;
@@ -180,6 +183,40 @@ __global__ void k_lde(const LdeLane* lanes, int logn_rt, int from_coeffs, const 
     };
     ntt16<true>(B, logn, tw_n, false, first, store);
   }
+}
+
+// The coset transforms of the LDE as blocks of their own: block (x, y) runs
+// coset a = first + y of lane x from its coefficients (L.coef, or L.src when
+// the lane is given as coefficients), written bit-reversed as in k_lde.  One
+// shared-memory array per block (the coefficients are read from global
+// memory, where the inverse transform left them, rather than kept in shared
+// memory), so several blocks share an SM and overlap one another's barriers
+// and shared-memory round trips.  MAXT: the block size the kernel is built
+// for (registers capped so that 1024 / MAXT blocks fit: 32 warps per SM
+// without spills).
+template <int LOGN, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1024 / MAXT)
+    k_lde_fwd(const LdeLane* lanes, int first, const uint32_t* tw_n, const uint32_t* tw_4n) {
+  static_assert(LOGN >= 4, "radix-16 passes");
+  extern __shared__ uint32_t sm[];
+  constexpr uint32_t n = 1u << LOGN, big = n << RATE_LOG;
+  const LdeLane L = lanes[blockIdx.x];
+  const uint32_t a = first + blockIdx.y;
+  const uint32_t e = bitrev32(a, RATE_LOG);
+  const uint32_t* coef = L.coef ? L.coef : L.src;
+  uint32_t* o = L.out + (uint64_t)a * n;
+  auto first_pass = [&](uint32_t t, uint32_t r, int lo) {
+    const uint32_t i = grp_index(t, r, lo);
+    return mul(__ldg(coef + i), __ldg(tw_4n + ((e * i) & (big - 1))));
+  };
+  auto store = [&](uint32_t t, int lo, const uint32_t* v) {
+    uint4* q = reinterpret_cast<uint4*>(o + ((uint64_t)t << 4));
+    q[0] = make_uint4(v[0], v[1], v[2], v[3]);
+    q[1] = make_uint4(v[4], v[5], v[6], v[7]);
+    q[2] = make_uint4(v[8], v[9], v[10], v[11]);
+    q[3] = make_uint4(v[12], v[13], v[14], v[15]);
+  };
+  ntt16<true>(sm, LOGN, tw_n, false, first_pass, store);
 }
 
 // Evaluations of a coefficient lane on the cosets s_c <w_n>, s_c = g w_4n^c,

@@ -6,6 +6,10 @@
 
 using namespace lg;
 
+namespace lg {
+void note_launches(uint64_t k) { g_launches.fetch_add(k); }
+}  // namespace lg
+
 struct lg_ctx {
   Ctx c;
   size_t last_proof_len = 0;  // bytes of the last proof in c.proof_buf
@@ -36,6 +40,7 @@ __global__ void k_e6_div_soa(const uint32_t* num, const uint32_t* den, uint64_t 
 template <class F> int guarded(lg_ctx* ctx, F f) {
   if (!ctx) return LG_ERR_INVALID;
   try {
+    AcctScope acct(&ctx->c.mem);
     LG_CK(cudaSetDevice(ctx->c.device));
     if (ctx->c.stream) {
       LG_CK(cudaStreamSynchronize(ctx->c.stream));
@@ -69,11 +74,12 @@ void from_device(Ctx& c, uint32_t* dst, const uint32_t* src, size_t words, int o
 
 extern "C" {
 
-int lg_ctx_create(int device, lg_ctx** out) {
+int lg_ctx_create(int device, size_t hbm_budget, lg_ctx** out) {
   if (!out) return LG_ERR_INVALID;
   *out = nullptr;
   lg_ctx* ctx = new lg_ctx();
   ctx->c.device = device;
+  ctx->c.mem.budget = (int64_t)hbm_budget;
   int rc = guarded(ctx, [&] {
     LG_CK(cudaStreamCreateWithFlags(&ctx->c.stream, cudaStreamNonBlocking));
     cudaMemPool_t pool;
@@ -116,6 +122,34 @@ int lg_ctx_set_batched(lg_ctx* ctx, int batched) {
   return guarded(ctx, [&] { ctx->c.batched = batched != 0; });
 }
 
+int lg_ctx_mem_usage(lg_ctx* ctx, uint64_t* held_bytes, uint64_t* peak_bytes, int reset_peak) {
+  if (!ctx) return LG_ERR_INVALID;
+  const int64_t h = ctx->c.mem.held.load();
+  if (held_bytes) *held_bytes = (uint64_t)std::max<int64_t>(h, 0);
+  if (peak_bytes) *peak_bytes = (uint64_t)std::max<int64_t>(ctx->c.mem.peak.load(), 0);
+  if (reset_peak) ctx->c.mem.peak.store(h);
+  return LG_OK;
+}
+
+int lg_device_mem_info(int device, uint64_t* available_bytes, uint64_t* total_bytes) {
+  int prev = 0;
+  if (cudaGetDevice(&prev) != cudaSuccess) return LG_ERR_CUDA;
+  if (cudaSetDevice(device) != cudaSuccess) return LG_ERR_CUDA;
+  size_t f = 0, t = 0;
+  cudaMemPool_t pool;
+  uint64_t reserved = 0, used = 0;
+  int rc = LG_OK;
+  if (cudaMemGetInfo(&f, &t) != cudaSuccess || cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess ||
+      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) != cudaSuccess ||
+      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess)
+    rc = LG_ERR_CUDA;
+  cudaSetDevice(prev);
+  if (rc != LG_OK) return rc;
+  if (available_bytes) *available_bytes = (uint64_t)f + (reserved > used ? reserved - used : 0);
+  if (total_bytes) *total_bytes = (uint64_t)t;
+  return LG_OK;
+}
+
 int lg_mem_info(lg_ctx* ctx, uint64_t* free_bytes, uint64_t* total_bytes) {
   return guarded(ctx, [&] {
     size_t f = 0, t = 0;
@@ -146,12 +180,15 @@ int lg_ctx_set_tuning(lg_ctx* ctx, const char* name, int64_t value) {
     Ctx::Tuning& t = ctx->c.tune;
     if (n == "p2_leaf_min_per_sm") { in(0, 1 << 20); t.p2_leaf_min_per_sm = (uint32_t)value; }
     else if (n == "p2_node_min_per_sm") { in(0, 1 << 20); t.p2_node_min_per_sm = (uint32_t)value; }
+    else if (n == "p2_inject_min_per_sm") { in(0, 1 << 20); t.p2_inject_min_per_sm = (uint32_t)value; }
     else if (n == "merkle_tail") { in(2, 1024); pow2(); t.merkle_tail = (uint32_t)value; }
     else if (n == "merkle_subtree") {
       if (value != 0) { in(2, 1024); pow2(); }
       t.merkle_subtree = (uint32_t)value;
     } else if (n == "inject_block") { in(32, 1024); pow2(); t.inject_block = (uint32_t)value; }
     else if (n == "leaf_block") { in(32, 1024); pow2(); t.leaf_block = (uint32_t)value; }
+    else if (n == "lde_split") { in(0, 1); t.lde_split = (uint32_t)value; }
+    else if (n == "lde_fwd_threads") { in(256, 1024); pow2(); t.lde_fwd_threads = (uint32_t)value; }
     else throw Error(LG_ERR_INVALID, "unknown tuning " + n);
   });
 }
@@ -163,10 +200,13 @@ int lg_ctx_get_tuning(lg_ctx* ctx, const char* name, int64_t* value) {
     const Ctx::Tuning& t = ctx->c.tune;
     if (n == "p2_leaf_min_per_sm") *value = t.p2_leaf_min_per_sm;
     else if (n == "p2_node_min_per_sm") *value = t.p2_node_min_per_sm;
+    else if (n == "p2_inject_min_per_sm") *value = t.p2_inject_min_per_sm;
     else if (n == "merkle_tail") *value = t.merkle_tail;
     else if (n == "merkle_subtree") *value = t.merkle_subtree;
     else if (n == "inject_block") *value = t.inject_block;
     else if (n == "leaf_block") *value = t.leaf_block;
+    else if (n == "lde_split") *value = t.lde_split;
+    else if (n == "lde_fwd_threads") *value = t.lde_fwd_threads;
     else throw Error(LG_ERR_INVALID, "unknown tuning " + n);
   });
 }
@@ -225,42 +265,382 @@ int lg_last_proof(lg_ctx* ctx, uint8_t* proof, size_t* proof_len) {
   return LG_OK;
 }
 
+}  // extern "C"
+
+// ---------------------------------------------------------------- handles
+// Every handle starts with a tag, so lg_release takes any of them.
+constexpr uint32_t LG_HANDLE_MAGIC = 0x4c474844u;  // "LGHD"
+enum : uint32_t { HK_COMMITTED = 1, HK_SESSION = 2 };
+
+struct lg_committed {
+  uint32_t magic = LG_HANDLE_MAGIC, kind = HK_COMMITTED;
+  lg_ctx* ctx = nullptr;
+  Committed cm;                // LDE, coefficients and tree on the device (shared buffers)
+  std::vector<uint32_t> nb, ne;  // per group, declaration order
+};
+
+struct lg_session {
+  uint32_t magic = LG_HANDLE_MAGIC, kind = HK_SESSION;
+  lg_ctx* ctx = nullptr;
+  std::unique_ptr<Prover> pr;
+};
+
+namespace {
+
+// Groups of a batch given as PCS.Commit's columns (internal/fri/pcs.go:145-168):
+// rows[g] Lagrange rows, n_base[g] base columns then n_ext[g] extension
+// columns (ext.E6 rows, 6 words each) in `cols`, group by group.  Extension
+// columns are laid out as six lanes on the device.
+std::vector<GroupSpec> batch_groups(Ctx& c, uint32_t n_groups, const uint64_t* rows, const uint32_t* n_base,
+                                    const uint32_t* n_ext, const uint32_t* const* cols, int on_device,
+                                    std::vector<DBufP>& keep) {
+  if (!n_groups || !rows || !n_base || !n_ext || !cols) throw Error(LG_ERR_INVALID, "null argument");
+  std::vector<GroupSpec> gs;
+  size_t ci = 0;
+  for (uint32_t g = 0; g < n_groups; g++) {
+    uint64_t n = rows[g];
+    if (n < 2 || (n & (n - 1))) throw Error(LG_ERR_INVALID, "group rows must be a power of two >= 2");
+    GroupSpec s;
+    s.log_n = 0;
+    while ((1ull << s.log_n) < n) s.log_n++;
+    s.nb = n_base[g];
+    s.ne = n_ext[g];
+    s.from_coeffs = false;
+    for (uint32_t i = 0; i < s.nb; i++) {
+      if (!cols[ci]) throw Error(LG_ERR_INVALID, "null column");
+      auto b = to_device(c, cols[ci++], n, on_device);
+      s.lanes.push_back(b->p);
+      keep.push_back(b);
+    }
+    for (uint32_t i = 0; i < s.ne; i++) {
+      if (!cols[ci]) throw Error(LG_ERR_INVALID, "null column");
+      auto a = to_device(c, cols[ci++], 6 * n, on_device);
+      auto b = std::make_shared<DBuf>(6 * n, c.stream);
+      k_aos_to_soa<<<(unsigned)((6 * n + 255) / 256), 256, 0, c.stream>>>(a->p, n, 6, b->p);
+      LG_LAUNCH();
+      for (int w = 0; w < 6; w++) s.lanes.push_back(b->p + (size_t)w * n);
+      keep.push_back(a);
+      keep.push_back(b);
+    }
+    gs.push_back(s);
+  }
+  return gs;
+}
+
+lg_committed* as_committed(const void* h) {
+  auto* c = (lg_committed*)h;
+  if (!c || c->magic != LG_HANDLE_MAGIC || c->kind != HK_COMMITTED) return nullptr;
+  return c;
+}
+lg_session* as_session(const void* h) {
+  auto* s = (lg_session*)h;
+  if (!s || s->magic != LG_HANDLE_MAGIC || s->kind != HK_SESSION) return nullptr;
+  return s;
+}
+// Runs one phase of a session: the context's guard (status codes, device,
+// idle stream) with the session's prover; phases allocate from the
+// context's memory pool only (no per-call arena), so what one phase leaves
+// on the device stays valid for the next.
+template <class F> int session_phase(lg_session* s, F f) {
+  if (!as_session(s) || !s->pr) return LG_ERR_INVALID;
+  return guarded(s->ctx, [&] {
+    ArenaScope pool_only(nullptr);
+    f(*s->pr);
+  });
+}
+
+}  // namespace
+
+extern "C" {
+
 int lg_commit_root(lg_ctx* ctx, uint32_t n_groups, const uint64_t* rows, const uint32_t* n_base,
                    const uint32_t* n_ext, const uint32_t* const* cols, int on_device, uint32_t root[8]) {
   return guarded(ctx, [&] {
-    Ctx& c = ctx->c;
-    if (!n_groups || !rows || !n_base || !n_ext || !cols || !root) throw Error(LG_ERR_INVALID, "null argument");
+    if (!root) throw Error(LG_ERR_INVALID, "null argument");
     std::vector<DBufP> keep;
-    std::vector<GroupSpec> gs;
-    size_t ci = 0;
-    for (uint32_t g = 0; g < n_groups; g++) {
-      uint64_t n = rows[g];
-      if (n < 2 || (n & (n - 1))) throw Error(LG_ERR_INVALID, "group rows must be a power of two >= 2");
-      GroupSpec s;
-      s.log_n = 0;
-      while ((1ull << s.log_n) < n) s.log_n++;
-      s.nb = n_base[g];
-      s.ne = n_ext[g];
-      s.from_coeffs = false;
-      for (uint32_t i = 0; i < s.nb; i++) {
-        auto b = to_device(c, cols[ci++], n, on_device);
-        s.lanes.push_back(b->p);
-        keep.push_back(b);
-      }
-      for (uint32_t i = 0; i < s.ne; i++) {
-        auto a = to_device(c, cols[ci++], 6 * n, on_device);
-        auto b = std::make_shared<DBuf>(6 * n, c.stream);
-        k_aos_to_soa<<<(unsigned)((6 * n + 255) / 256), 256, 0, c.stream>>>(a->p, n, 6, b->p);
-        LG_LAUNCH();
-        for (int w = 0; w < 6; w++) s.lanes.push_back(b->p + (size_t)w * n);
-        keep.push_back(a);
-        keep.push_back(b);
-      }
-      gs.push_back(s);
-    }
-    Committed cm = commit(c, gs, false);
+    std::vector<GroupSpec> gs = batch_groups(ctx->c, n_groups, rows, n_base, n_ext, cols, on_device, keep);
+    Committed cm = commit(ctx->c, gs, false);
     memcpy(root, cm.tree.root.v, 32);
   });
+}
+
+int lg_commit(lg_ctx* ctx, uint32_t n_groups, const uint64_t* rows, const uint32_t* n_base, const uint32_t* n_ext,
+              const uint32_t* const* cols, int on_device, lg_committed** out, uint32_t root[8]) {
+  if (out) *out = nullptr;
+  return guarded(ctx, [&] {
+    if (!root || !out) throw Error(LG_ERR_INVALID, "null argument");
+    ArenaScope pool_only(nullptr);  // everything here outlives the call
+    std::vector<DBufP> keep;
+    std::vector<GroupSpec> gs = batch_groups(ctx->c, n_groups, rows, n_base, n_ext, cols, on_device, keep);
+    auto h = std::make_unique<lg_committed>();
+    h->ctx = ctx;
+    h->cm = commit(ctx->c, gs, true);
+    for (auto& g : gs) { h->nb.push_back(g.nb); h->ne.push_back(g.ne); }
+    memcpy(root, h->cm.tree.root.v, 32);
+    LG_CK(cudaStreamSynchronize(ctx->c.stream));
+    *out = h.release();
+  });
+}
+
+int lg_committed_eval(lg_ctx* ctx, const lg_committed* batch, const uint32_t zeta[6], uint32_t n_shifts,
+                      const int32_t* shifts, uint32_t* out) {
+  return guarded(ctx, [&] {
+    const lg_committed* h = as_committed(batch);
+    if (!h || !zeta || !out || (n_shifts && !shifts)) throw Error(LG_ERR_INVALID, "null or invalid argument");
+    if (h->ctx != ctx) throw Error(LG_ERR_INVALID, "handle belongs to another context");
+    Ctx& c = ctx->c;
+    ArenaScope arena(&c.dev_arena);
+    E6 z;
+    for (int k = 0; k < 6; k++) z.c[k] = zeta[k];
+    std::vector<DotJob> jobs;
+    std::vector<DBufP> keep;
+    std::map<std::pair<uint32_t, int32_t>, const uint32_t*> zp;
+    for (size_t g = 0; g < h->cm.groups.size(); g++) {
+      const LdeOut& l = h->cm.groups[g];
+      if (!l.coef) throw Error(LG_ERR_UNSUPPORTED, "this batch keeps no coefficients");
+      const size_t n = (size_t)1 << l.log_n;
+      for (uint32_t si = 0; si < n_shifts; si++) {
+        auto key = std::make_pair(l.log_n, shifts[si]);
+        if (!zp.count(key)) {
+          const int64_t e = ((int64_t)shifts[si] % (int64_t)n + (int64_t)n) % (int64_t)n;
+          E6 zs = e6_mul_base(z, mont_pow(root_of_unity_mont((int)l.log_n), (uint64_t)e));
+          auto b = std::make_shared<DBuf>(6 * n, c.stream);
+          k_e6_powers<<<(unsigned)((n + 127) / 128), 128, 0, c.stream>>>(zs, (uint32_t)n, b->p);
+          LG_LAUNCH();
+          keep.push_back(b);
+          zp[key] = b->p;
+        }
+      }
+    }
+    // one dot product per (group, polynomial lane, shift)
+    for (size_t g = 0; g < h->cm.groups.size(); g++) {
+      const LdeOut& l = h->cm.groups[g];
+      const uint32_t n = 1u << l.log_n;
+      for (uint32_t lane = 0; lane < l.lanes; lane++)
+        for (uint32_t si = 0; si < n_shifts; si++)
+          jobs.push_back(DotJob{l.coef->p + (size_t)lane * n, zp.at({l.log_n, shifts[si]}), n, (uint32_t)jobs.size()});
+    }
+    std::vector<uint32_t> dots(6 * jobs.size());
+    if (!jobs.empty()) {
+      auto jd = upload_vec(c, jobs);
+      auto od = std::make_shared<DBuf>(6 * jobs.size(), c.stream);
+      k_dot<<<(unsigned)jobs.size(), 256, 0, c.stream>>>((const DotJob*)jd->p, od->p);
+      LG_LAUNCH();
+      uint32_t* hst = c.host_staging(dots.size());
+      c.d2h(hst, od->p, dots.size());
+      memcpy(dots.data(), hst, dots.size() * 4);
+    }
+    // per group: base polynomials, then extension polynomials (their six
+    // lanes' values recombined on the E6 basis), each at every shift
+    size_t j = 0, o = 0;
+    for (size_t g = 0; g < h->cm.groups.size(); g++) {
+      const uint32_t nb = h->nb[g], ne = h->ne[g];
+      for (uint32_t i = 0; i < nb; i++)
+        for (uint32_t si = 0; si < n_shifts; si++, j++, o++)
+          for (int q = 0; q < 6; q++) out[6 * o + q] = dots[6 * j + q];
+      for (uint32_t i = 0; i < ne; i++) {
+        std::vector<E6> acc(n_shifts, e6_zero());
+        for (uint32_t w = 0; w < 6; w++)
+          for (uint32_t si = 0; si < n_shifts; si++, j++) {
+            E6 d, basis = e6_zero();
+            for (int q = 0; q < 6; q++) d.c[q] = dots[6 * j + q];
+            basis.c[w] = MONT_ONE;
+            acc[si] = e6_add(acc[si], e6_mul(d, basis));
+          }
+        for (uint32_t si = 0; si < n_shifts; si++, o++)
+          for (int q = 0; q < 6; q++) out[6 * o + q] = acc[si].c[q];
+      }
+    }
+  });
+}
+
+int lg_open_batches(lg_ctx* ctx, uint32_t n_batches, const lg_committed* const* batches, const uint32_t* positions,
+                    uint32_t n_positions, uint8_t* out, size_t* out_len) {
+  return guarded(ctx, [&] {
+    if (!batches || !positions || !out_len || !n_batches || !n_positions) throw Error(LG_ERR_INVALID, "null or empty argument");
+    Ctx& c = ctx->c;
+    ArenaScope arena(&c.dev_arena);
+    std::vector<OpenBatch> obs;
+    for (uint32_t b = 0; b < n_batches; b++) {
+      const lg_committed* h = as_committed(batches[b]);
+      if (!h) throw Error(LG_ERR_INVALID, "not a committed-batch handle");
+      if (h->ctx != ctx) throw Error(LG_ERR_INVALID, "handle belongs to another context");
+      obs.push_back(OpenBatch{&h->cm, h->nb, h->ne});
+    }
+    std::vector<uint32_t> pos(positions, positions + n_positions);
+    for (uint32_t s : pos)
+      if (s >= (1u << LOG_N_FRI)) throw Error(LG_ERR_INVALID, "query position out of range");
+    OpenPlan OP;
+    const SectionSrc sec = OP.batches_section(obs, n_positions);
+    const size_t need = 4 * (size_t)n_positions * sec.q_words;
+    if (!out || *out_len < need) {
+      *out_len = need;
+      throw Error(LG_ERR_BUFFER, "output buffer too small");
+    }
+    const uint32_t* A = OP.run(c, pos);
+    memcpy(out, A + sec.out_off, need);
+    *out_len = need;
+  });
+}
+
+// ---------------------------------------------------------------- sessions
+int lg_session_begin(lg_ctx* ctx, const char* hash_backend, const uint32_t* program, size_t program_words,
+                     const uint32_t* const* witness, int witness_on_device, uint32_t num_queries, lg_session** out) {
+  if (out) *out = nullptr;
+  return guarded(ctx, [&] {
+    std::string hb = hash_backend ? hash_backend : "";
+    if (hb != "" && hb != "poseidon2")
+      throw Error(LG_ERR_UNSUPPORTED, "hash backend \"" + hb + "\" is not available on the GPU path (poseidon2 only)");
+    if (!program || !out) throw Error(LG_ERR_INVALID, "null argument");
+    ArenaScope pool_only(nullptr);
+    auto s = std::make_unique<lg_session>();
+    s->ctx = ctx;
+    s->pr = std::make_unique<Prover>(ctx->c, program, program_words, num_queries);
+    s->pr->c.phase_start();
+    s->pr->begin(witness, witness_on_device != 0);
+    LG_CK(cudaStreamSynchronize(ctx->c.stream));
+    *out = s.release();
+  });
+}
+
+int lg_session_setup_root(lg_session* s, uint32_t root[8], int* has_root) {
+  return session_phase(s, [&](Prover& p) {
+    if (!root || !has_root) throw Error(LG_ERR_INVALID, "null argument");
+    *has_root = p.has_setup_tree() ? 1 : 0;
+    if (*has_root) memcpy(root, p.prog->setup->root.v, 32);
+  });
+}
+
+int lg_session_challenge(lg_session* s, const char* name, const uint32_t digest[8]) {
+  return session_phase(s, [&](Prover& p) {
+    if (!name || !digest) throw Error(LG_ERR_INVALID, "null argument");
+    p.set_challenge(name, digest);
+  });
+}
+
+int lg_commit_round(lg_session* s, uint32_t round, uint32_t root[8], int* committed, uint32_t* exposed,
+                    uint32_t* n_exposed) {
+  return session_phase(s, [&](Prover& p) {
+    if (!root || !committed || !n_exposed) throw Error(LG_ERR_INVALID, "null argument");
+    Digest d{};
+    *committed = p.commit_round(round, &d) ? 1 : 0;
+    memcpy(root, d.v, 32);
+    const std::vector<E6> ev = p.round_exposed(round);
+    const uint32_t cap = *n_exposed;
+    *n_exposed = (uint32_t)ev.size();
+    if (ev.size() > cap || (ev.size() && !exposed)) throw Error(LG_ERR_BUFFER, "exposed-value buffer too small");
+    for (size_t i = 0; i < ev.size(); i++) memcpy(exposed + 6 * i, ev[i].c, 24);
+  });
+}
+
+int lg_quotient(lg_session* s, uint32_t root[8], int* committed) {
+  return session_phase(s, [&](Prover& p) {
+    if (!root || !committed) throw Error(LG_ERR_INVALID, "null argument");
+    Digest d{};
+    *committed = p.commit_quotient(&d) ? 1 : 0;
+    memcpy(root, d.v, 32);
+  });
+}
+
+int lg_claimed_values(lg_session* s, uint32_t* values, size_t* n_values) {
+  return session_phase(s, [&](Prover& p) {
+    if (!n_values) throw Error(LG_ERR_INVALID, "null argument");
+    if (p.cv.empty()) p.claimed_values();
+    const std::vector<E6> v = p.claimed_values_bind_order();
+    const size_t cap = *n_values;
+    *n_values = v.size();
+    if (v.size() > cap || !values) throw Error(LG_ERR_BUFFER, "claimed-value buffer too small");
+    for (size_t i = 0; i < v.size(); i++) memcpy(values + 6 * i, v[i].c, 24);
+  });
+}
+
+int lg_deep(lg_session* s) {
+  return session_phase(s, [&](Prover& p) { p.deep_codewords(); });
+}
+
+int lg_fri_commit_levels(lg_session* s, uint32_t root[8], uint32_t* n_levels, uint32_t* first_round) {
+  return session_phase(s, [&](Prover& p) {
+    if (!root || !n_levels || !first_round) throw Error(LG_ERR_INVALID, "null argument");
+    const Digest d = p.commit_levels();
+    memcpy(root, d.v, 32);
+    *n_levels = (uint32_t)p.L;
+    *first_round = (uint32_t)p.r0;
+  });
+}
+
+int lg_fri_fold_round(lg_session* s, uint32_t round, uint32_t root[8], int* committed) {
+  return session_phase(s, [&](Prover& p) {
+    if (!root || !committed) throw Error(LG_ERR_INVALID, "null argument");
+    Digest d{};
+    *committed = p.fri_fold_round((int)round, true, &d) ? 1 : 0;
+    memcpy(root, d.v, 32);
+  });
+}
+
+int lg_fri_final(lg_session* s, uint32_t* values, size_t* n_values) {
+  return session_phase(s, [&](Prover& p) {
+    if (!n_values) throw Error(LG_ERR_INVALID, "null argument");
+    if (p.final_poly.empty()) p.read_final_poly();
+    const size_t n = p.nj, cap = *n_values;
+    *n_values = n;
+    if (n > cap || !values) throw Error(LG_ERR_BUFFER, "final-polynomial buffer too small");
+    for (size_t i = 0; i < n; i++)
+      for (int w = 0; w < 6; w++) values[6 * i + w] = p.final_poly[w * n + i];
+  });
+}
+
+int lg_open(lg_session* s, const uint32_t* positions, uint32_t n_positions, uint8_t* proof, size_t* proof_len) {
+  lg_session* ss = as_session(s);
+  if (!ss) return LG_ERR_INVALID;
+  return session_phase(s, [&](Prover& p) {
+    if (!positions || !proof_len) throw Error(LG_ERR_INVALID, "null argument");
+    std::vector<uint32_t> pos(positions, positions + n_positions);
+    bool direct = false;
+    ss->ctx->last_proof_len = 0;
+    size_t need = p.open_and_encode(pos, proof, proof ? *proof_len : 0, &direct);
+    *proof_len = need;
+    if (!direct) {
+      ss->ctx->last_proof_len = need;
+      throw Error(LG_ERR_BUFFER, "proof buffer too small");
+    }
+  });
+}
+
+int lg_session_committed(lg_session* s, uint32_t index, lg_committed** out) {
+  if (out) *out = nullptr;
+  return session_phase(s, [&](Prover& p) {
+    if (!out) throw Error(LG_ERR_INVALID, "null argument");
+    if (index >= p.committed.size()) throw Error(LG_ERR_INVALID, "no committed batch at this index");
+    auto h = std::make_unique<lg_committed>();
+    h->ctx = s->ctx;
+    h->cm = p.committed[index];
+    const auto& T = p.trees[index];
+    for (size_t g = 0; g < T.groups.size(); g++) {
+      h->nb.push_back((uint32_t)T.groups[g].bcols.size());
+      h->ne.push_back((uint32_t)T.groups[g].ecols.size());
+      // the AIR batch keeps its coefficients with the quotient chunks
+      if (T.air && !h->cm.groups[g].coef) h->cm.groups[g].coef = p.chunk_coef.at(T.groups[g].module);
+    }
+    *out = h.release();
+  });
+}
+
+void lg_release(void* handle) {
+  if (lg_committed* c = as_committed(handle)) {
+    lg_ctx* ctx = c->ctx;
+    cudaSetDevice(ctx->c.device);
+    cudaStreamSynchronize(ctx->c.stream);
+    c->magic = 0;
+    delete c;  // device buffers free on the context's stream
+    return;
+  }
+  if (lg_session* s = as_session(handle)) {
+    lg_ctx* ctx = s->ctx;
+    cudaSetDevice(ctx->c.device);
+    cudaStreamSynchronize(ctx->c.stream);
+    s->magic = 0;
+    delete s;
+  }
 }
 
 int lg_rs_encode(lg_ctx* ctx, const uint32_t* in, uint64_t n_rows, uint32_t n_cols, uint32_t* out, int on_device) {

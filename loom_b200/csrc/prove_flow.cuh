@@ -1,75 +1,262 @@
-// Prover::prove: the ordered sequence of device phases and transcript steps.
-// Order of transcript operations follows prover/prover.go:142-719,
-// internal/fri/open.go:98-285 and internal/fri/fri.go:606-736.
+// The prove as a sequence of device phases, and Prover::prove, which runs
+// them with the host transcript.  Order of transcript operations follows
+// prover/prover.go:142-719, internal/fri/open.go:98-285 and
+// internal/fri/fri.go:606-736.  The phases themselves read no transcript:
+// every challenge comes in through set_challenge, so a caller that keeps its
+// own transcript (the Go prover through the session entry points of the C
+// ABI) drives the same code.
 #pragma once
 #include "prover.cuh"
 
 namespace lg {
 
-inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint8_t* out, size_t out_cap,
-                            bool* in_out) {
-  ArenaScope arena(&c.dev_arena);  // rewound by the next call on the context
-  c.phase_start();
-  setup(witness, on_device);
-  c.phase("setup+upload");
-  const uint32_t R = pg.n_rounds;
-  for (uint32_t r = 0; r < R; r++) fs.add(coin_name(r));
-  fs.add("__zeta");
-  {
-    const std::string first = coin_name(0);
-    auto hb = string_to_elements(0x48415348u, "poseidon2");
-    fs.bind(first, hb.data(), hb.size());
-    std::vector<uint32_t> sz = {to_mont(0x53495a45u), to_mont((uint32_t)mod_order.size())};
-    for (uint32_t m : mod_order) sz.push_back(to_mont((uint32_t)mod_n(m)));
-    fs.bind(first, sz.data(), sz.size());
-  }
-  // ---- the precommitted setup tree: its root binds to the first challenge
-  // and stays out of the proof's commitments (prover/prover.go:175-229)
-  size_t ti = 0;
-  if (!trees.empty() && trees[0].setup) {
-    committed.push_back(prog->setup->committed);
-    fs.bind(coin_name(0), prog->setup->root.v, 8);
-    ti = 1;
-  }
-  // ---- rounds: steps, commit, bind root, sample coin (prover/prover.go:360-411)
-  coins.assign(R, e6_zero());
-  for (uint32_t r = 0; r < R; r++) {
-    run_steps(r);
-    if (ti < trees.size() && !trees[ti].air && trees[ti].round == (int)r) {
-      committed.push_back(commit_tree(trees[ti]));
-      Digest root = committed.back().tree.root;
-      commitments.push_back(root);
-      fs.bind(coin_name(r), root.v, 8);
-      ti++;
-    }
-    // BindExposedValues (prover/prover.go:386-396): the round's logup totals
-    // in step order, each as its entry index then six elements
-    // (board/logup.go:218-225)
-    read_exposed(r);
-    for (const Step& st : pg.steps) {
-      if (st.round != r || !exposes(st.type)) continue;
-      uint32_t w[7] = {0};
-      for (int k = 0; k < 6; k++) w[1 + k] = exposed[st.exposed].c[k];
-      fs.bind(coin_name(r), w, 7);
-    }
-    coins[r] = digest_e6(fs.compute(coin_name(r)));
-    c.phase(("round " + std::to_string(r)).c_str());
-  }
-  // ---- AIR quotients and their commitment (prover/prover.go:461-561)
-  quotient_all();
-  if (ti < trees.size() && trees[ti].air) {
-    committed.push_back(commit_tree(trees[ti]));
-    Digest root = committed.back().tree.root;
-    commitments.push_back(root);
-    fs.bind("__zeta", root.v, 8);
-    ti++;
-  }
-  zeta = digest_e6(fs.compute("__zeta"));
-  c.phase("quotient+air commit");
+// A committed batch as the openings see it: its groups' base and extension
+// polynomial counts in declaration order.
+struct OpenBatch {
+  const Committed* cm;
+  std::vector<uint32_t> nb, ne;
+};
 
-  // ---- claimed values P(zeta w^s) from coefficients (internal/fri/values.go:46-110)
-  struct Poly { size_t t, g; bool ext; const uint32_t* coef; uint32_t logn; std::vector<int> shifts; };
-  std::vector<std::vector<std::vector<Poly>>> polys(trees.size());  // [tree][group] base polys then ext polys
+// Query openings gathered on the device: row pairs and Merkle paths go to one
+// staging buffer (per query, per_q words), then per-query sections are laid
+// out in proof order and encoding (big-endian canonical words) by k_assemble
+// from a word map, and read back once.
+struct OpenPlan {
+  std::vector<RowSrc> rows;
+  std::vector<PathSrc> paths;
+  uint64_t per_q = 0;
+  std::vector<uint32_t> map, consts;
+  std::vector<PosOp> pops;
+  std::vector<SectionSrc> secs;
+  uint64_t total = 0;
+  size_t start = 0;
+
+  uint64_t add_rows(const uint32_t* lane0, uint64_t stride, uint32_t nl, uint32_t shift) {
+    rows.push_back(RowSrc{lane0, stride, nl, shift, per_q});
+    uint64_t o = per_q;
+    per_q += 2ull * nl;
+    return o;
+  }
+  uint64_t add_path(const TreeDev& t, uint32_t shift, bool with_inj) {
+    PathSrc p{};
+    p.nodes = t.nodes->p;
+    p.inj = with_inj ? (const uint32_t* const*)t.inj_ptrs->p : nullptr;
+    p.inj_shift = with_inj ? t.inj_shift->p : nullptr;
+    p.log_leaves = t.log_leaves;
+    p.n_inj = with_inj ? (uint32_t)t.inj.size() : 0;
+    p.shift = shift;
+    p.off = per_q;
+    paths.push_back(p);
+    uint64_t o = per_q;
+    per_q += 8ull * (p.log_leaves + p.n_inj);
+    return o;
+  }
+  // section words: constants, the query position (shifted; as a leaf index
+  // when `leaf`), copies from the staging buffer
+  void begin() { start = map.size(); }
+  void konst(uint32_t v) {
+    map.push_back((SEC_CONST << 30) | (uint32_t)consts.size());
+    consts.push_back(v);
+  }
+  void posw(uint32_t shift, bool leaf) {
+    map.push_back((SEC_POS << 30) | (uint32_t)pops.size());
+    pops.push_back(PosOp{shift, leaf ? 1u : 0u});
+  }
+  void copy(uint64_t off, size_t n) {
+    if (off + n > 0x3fffffffu) throw Error(LG_ERR_UNSUPPORTED, "opening block too large");
+    for (size_t i = 0; i < n; i++) map.push_back((uint32_t)(off + i));
+  }
+  SectionSrc end(uint32_t nq) {
+    SectionSrc sc{start, total, (uint32_t)(map.size() - start)};
+    secs.push_back(sc);
+    total += (uint64_t)nq * sc.q_words;
+    return sc;
+  }
+
+  // The commitment openings of one query (openCommittedAt,
+  // internal/fri/open.go:290-378): the batch count, then per batch the row
+  // pair of its largest group, that tree's path with its injected leaves,
+  // and the row pairs of the other groups (sorted order).
+  SectionSrc batches_section(const std::vector<OpenBatch>& bs, uint32_t nq) {
+    struct BatchOff { std::vector<uint64_t> rows; uint64_t path; };
+    std::vector<BatchOff> boff(bs.size());
+    for (size_t b = 0; b < bs.size(); b++) {
+      const Committed& cm = *bs[b].cm;
+      for (int gi : cm.order) {
+        const LdeOut& l = cm.groups[gi];
+        uint32_t log_rows = l.log_n + RATE_LOG;
+        boff[b].rows.push_back(add_rows(l.lde->p, (size_t)1 << log_rows, l.lanes, (uint32_t)(LOG_N_FRI - log_rows)));
+      }
+      const LdeOut& top = cm.groups[cm.order[0]];
+      boff[b].path = add_path(cm.tree, (uint32_t)(LOG_N_FRI - (top.log_n + RATE_LOG)), true);
+    }
+    begin();
+    konst((uint32_t)bs.size());
+    for (size_t b = 0; b < bs.size(); b++) {
+      const Committed& cm = *bs[b].cm;
+      auto rowpair = [&](int gi, uint64_t off) {
+        const LdeOut& l = cm.groups[gi];
+        uint32_t nb = bs[b].nb[gi], ne = bs[b].ne[gi];
+        if (l.lanes != nb + 6 * ne) throw Error(LG_ERR_INVALID, "opening row width");
+        for (int h = 0; h < 2; h++) {
+          konst(nb);
+          copy(off + (uint64_t)h * l.lanes, nb);
+          konst(ne);
+          copy(off + (uint64_t)h * l.lanes + nb, 6 * (size_t)ne);
+        }
+      };
+      const LdeOut& top = cm.groups[cm.order[0]];
+      rowpair(cm.order[0], boff[b].rows[0]);
+      posw((uint32_t)(LOG_N_FRI - (top.log_n + RATE_LOG)), true);
+      konst(cm.tree.log_leaves);
+      copy(boff[b].path, 8 * (size_t)cm.tree.log_leaves);
+      konst((uint32_t)cm.tree.inj.size());
+      copy(boff[b].path + 8 * (size_t)cm.tree.log_leaves, 8 * cm.tree.inj.size());
+      konst((uint32_t)(cm.order.size() - 1));
+      for (size_t s = 1; s < cm.order.size(); s++) rowpair(cm.order[s], boff[b].rows[s]);
+    }
+    return end(nq);
+  }
+
+  // Gathers and lays out every section at the query positions; returns the
+  // host copy (the context's pinned staging, valid until its next use).
+  const uint32_t* run(Ctx& c, const std::vector<uint32_t>& pos) {
+    const uint32_t nq = (uint32_t)pos.size();
+    auto pos_d = upload_vec(c, pos);
+    auto out_d = std::make_shared<DBuf>(per_q * nq, c.stream);
+    {
+      auto rd = upload_vec(c, rows);
+      uint32_t max_l = 1;
+      for (auto& r : rows) max_l = std::max(max_l, r.n_lanes);
+      auto pd = upload_vec(c, paths);
+      uint32_t max_t = 1;
+      for (auto& p : paths) max_t = std::max(max_t, p.log_leaves + p.n_inj);
+      c.timed("openings", 8.0 * per_q * nq, 0, [&] {
+        if (!rows.empty()) {
+          k_gather_rows<<<dim3((max_l + 63) / 64, nq, (unsigned)rows.size()), 64, 0, c.stream>>>(
+              (const RowSrc*)rd->p, (uint32_t)rows.size(), pos_d->p, nq, per_q, out_d->p);
+          LG_LAUNCH();
+        }
+        if (!paths.empty()) {
+          k_gather_paths<<<dim3((max_t + 31) / 32, nq, (unsigned)paths.size()), 32, 0, c.stream>>>(
+              (const PathSrc*)pd->p, pos_d->p, nq, per_q, out_d->p);
+          LG_LAUNCH();
+        }
+        if (per_q) {
+          k_proof_words<<<(unsigned)((per_q * nq + 255) / 256), 256, 0, c.stream>>>(out_d->p, per_q * nq);
+          LG_LAUNCH();
+        }
+      });
+    }
+    auto asm_d = std::make_shared<DBuf>(total, c.stream);
+    {
+      auto map_d = upload_vec(c, map), consts_d = upload_vec(c, consts);
+      auto pops_d = upload_vec(c, pops), secs_d = upload_vec(c, secs);
+      uint32_t max_q = 1;
+      for (auto& sc : secs) max_q = std::max(max_q, sc.q_words);
+      c.timed("openings", 8.0 * total, 0, [&] {
+        k_assemble<<<dim3((max_q + 255) / 256, nq, (unsigned)secs.size()), 256, 0, c.stream>>>(
+            (const SectionSrc*)secs_d->p, map_d->p, consts_d->p, (const PosOp*)pops_d->p, pos_d->p, out_d->p, per_q, nq,
+            asm_d->p);
+        LG_LAUNCH();
+      });
+    }
+    uint32_t* A = c.host_staging(total);
+    c.d2h(A, asm_d->p, total);
+    return A;
+  }
+};
+
+inline void Prover::begin(const uint32_t* const* witness, bool on_device) {
+  setup(witness, on_device);
+  coins.assign(pg.n_rounds, e6_zero());
+  coin_ready.assign(pg.n_rounds, 0);
+  tree_next = 0;
+  // the precommitted setup tree (prover/prover.go:175-229): its root binds
+  // to the first challenge and stays out of the proof's commitments
+  if (has_setup_tree()) {
+    committed.push_back(prog->setup->committed);
+    tree_next = 1;
+  }
+}
+
+inline void Prover::set_challenge(const std::string& name, const uint32_t* d) {
+  E6 e = e6_zero();
+  for (int k = 0; k < 6; k++) e.c[k] = d[k];
+  for (uint32_t r = 0; r < pg.n_rounds; r++)
+    if (name == coin_name(r)) {
+      coins[r] = e;
+      coin_ready[r] = 1;
+      return;
+    }
+  if (name == "__zeta") { zeta = e; zeta_ready = true; return; }
+  if (name == "alpha_DEEP") { alpha = e; alpha_ready = true; return; }
+  const std::string lp = "fri_level_", fp = "fri_fold_";
+  if (name.compare(0, lp.size(), lp) == 0 && name.size() > lp.size() + 6 &&
+      name.compare(name.size() - 6, 6, "_gamma") == 0) {
+    if (fri_next < 0) throw Error(LG_ERR_INVALID, name + ": the FRI levels are not committed yet");
+    const size_t l = std::stoul(name.substr(lp.size(), name.size() - lp.size() - 6));
+    if (l < 1 || l >= L) throw Error(LG_ERR_INVALID, "no FRI level for " + name);
+    gam[l] = e;
+    gam_ready[l] = 1;
+    return;
+  }
+  if (name.compare(0, fp.size(), fp) == 0 && name.size() > fp.size()) {
+    if (fri_next < 0) throw Error(LG_ERR_INVALID, name + ": the FRI levels are not committed yet");
+    const int j = std::stoi(name.substr(fp.size()));
+    if (j < r0 || j >= NR) throw Error(LG_ERR_INVALID, name + " has no layer to fold");
+    c.h2d(chal->p + 8 * (size_t)j, d, 32);
+    chal_ready[j] = 1;
+    return;
+  }
+  throw Error(LG_ERR_INVALID, "unknown challenge " + name);
+}
+
+// ---- rounds: steps, commit (prover/prover.go:321-411)
+inline bool Prover::commit_round(uint32_t r, Digest* root) {
+  if (r >= pg.n_rounds) throw Error(LG_ERR_INVALID, "round out of range");
+  need_coins(r);
+  run_steps(r);
+  bool has = false;
+  if (tree_next < trees.size() && !trees[tree_next].air && trees[tree_next].round == (int)r) {
+    committed.push_back(commit_tree(trees[tree_next]));
+    *root = committed.back().tree.root;
+    commitments.push_back(*root);
+    tree_next++;
+    has = true;
+  }
+  read_exposed(r);
+  return has;
+}
+
+inline std::vector<E6> Prover::round_exposed(uint32_t r) const {
+  std::vector<E6> v;
+  for (const Step& st : pg.steps)
+    if (st.round == r && exposes(st.type)) v.push_back(exposed[st.exposed]);
+  return v;
+}
+
+// ---- AIR quotients and their commitment (prover/prover.go:461-561)
+inline bool Prover::commit_quotient(Digest* root) {
+  need_coins(pg.n_rounds);
+  if (tree_next < trees.size() && !trees[tree_next].air)
+    throw Error(LG_ERR_INVALID, "the rounds are not all committed yet");
+  quotient_all();
+  if (tree_next < trees.size() && trees[tree_next].air) {
+    committed.push_back(commit_tree(trees[tree_next]));
+    *root = committed.back().tree.root;
+    commitments.push_back(*root);
+    tree_next++;
+    return true;
+  }
+  return false;
+}
+
+// ---- claimed values P(zeta w^s) from coefficients (internal/fri/values.go:46-110)
+inline void Prover::claimed_values() {
+  if (!zeta_ready) throw Error(LG_ERR_INVALID, "challenge __zeta has not been set");
+  if (tree_next != trees.size()) throw Error(LG_ERR_INVALID, "the quotient is not committed yet");
+  polys.assign(trees.size(), {});
   for (size_t t = 0; t < trees.size(); t++) {
     polys[t].resize(trees[t].groups.size());
     for (size_t g = 0; g < trees[t].groups.size(); g++) {
@@ -91,7 +278,6 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
     }
   }
   std::map<std::pair<uint32_t, int>, DBufP> zp;  // (log n, shift) -> powers of zeta w^shift
-  std::map<std::pair<uint32_t, int>, E6> zpoint;
   std::vector<DotJob> jobs;
   for (auto& pt : polys)
     for (auto& pgp : pt)
@@ -101,7 +287,6 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
           if (!zp.count(key)) {
             uint32_t n = 1u << p.logn;
             E6 z = e6_mul_base(zeta, mont_pow(root_of_unity_mont((int)p.logn), (uint64_t)s));
-            zpoint[key] = z;
             auto b = std::make_shared<DBuf>(6 * (size_t)n, c.stream);
             c.timed("claimed_values", 0, 0, [&] {
               k_e6_powers<<<(n + 127) / 128, 128, 0, c.stream>>>(z, n, b->p);
@@ -125,49 +310,52 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
     c.d2h(h, od->p, dots.size());
     memcpy(dots.data(), h, dots.size() * 4);
   }
-  // values[t][g][poly][shift]
-  std::vector<std::vector<std::vector<std::vector<E6>>>> cv(trees.size());
-  {
-    size_t j = 0;
-    for (size_t t = 0; t < trees.size(); t++) {
-      cv[t].resize(polys[t].size());
-      for (size_t g = 0; g < polys[t].size(); g++)
-        for (auto& p : polys[t][g]) {
-          std::vector<E6> vals;
-          for (size_t si = 0; si < p.shifts.size(); si++) {
-            E6 v = e6_zero();
-            for (uint32_t w = 0; w < (p.ext ? 6u : 1u); w++, j++) {
-              E6 d;
-              for (int q = 0; q < 6; q++) d.c[q] = dots[6 * j + q];
-              E6 basis = e6_zero();
-              basis.c[w] = MONT_ONE;
-              v = e6_add(v, p.ext ? e6_mul(d, basis) : d);
-            }
-            vals.push_back(v);
+  cv.assign(trees.size(), {});
+  size_t j = 0;
+  for (size_t t = 0; t < trees.size(); t++) {
+    cv[t].resize(polys[t].size());
+    for (size_t g = 0; g < polys[t].size(); g++)
+      for (auto& p : polys[t][g]) {
+        std::vector<E6> vals;
+        for (size_t si = 0; si < p.shifts.size(); si++) {
+          E6 v = e6_zero();
+          for (uint32_t w = 0; w < (p.ext ? 6u : 1u); w++, j++) {
+            E6 d;
+            for (int q = 0; q < 6; q++) d.c[q] = dots[6 * j + q];
+            E6 basis = e6_zero();
+            basis.c[w] = MONT_ONE;
+            v = e6_add(v, p.ext ? e6_mul(d, basis) : d);
           }
-          cv[t][g].push_back(vals);
+          vals.push_back(v);
         }
-    }
+        cv[t][g].push_back(vals);
+      }
   }
   // DEEP classes = modules with committed groups, in sorted order
-  std::vector<uint32_t> classes;
+  classes.clear();
   for (uint32_t m : mod_order) {
     bool has = false;
     for (auto& t : trees) for (auto& g : t.groups) if (g.module == m) has = true;
     if (has) classes.push_back(m);
   }
-  fs.add("alpha_DEEP");
+}
+
+inline std::vector<E6> Prover::claimed_values_bind_order() const {
+  std::vector<E6> out;
   for (uint32_t m : classes)
     for (size_t t = 0; t < trees.size(); t++)
       for (size_t g = 0; g < trees[t].groups.size(); g++) {
         if (trees[t].groups[g].module != m) continue;
-        for (auto& vals : cv[t][g]) for (auto& v : vals) fs.bind("alpha_DEEP", v.c, 6);
+        for (auto& vals : cv[t][g]) for (auto& v : vals) out.push_back(v);
       }
-  E6 alpha = digest_e6(fs.compute("alpha_DEEP"));
-  c.phase("claimed values+bind");
+  return out;
+}
 
-  // ---- DEEP codewords on the LDE rows (internal/fri/deep.go:71-266)
-  std::vector<DBufP> deep(classes.size());
+// ---- DEEP codewords on the LDE rows (internal/fri/deep.go:71-266)
+inline void Prover::deep_codewords() {
+  if (cv.empty()) throw Error(LG_ERR_INVALID, "the claimed values are not computed yet");
+  if (!alpha_ready) throw Error(LG_ERR_INVALID, "challenge alpha_DEEP has not been set");
+  deep.assign(classes.size(), nullptr);
   DBufP deep_all;  // one allocation for every class's codeword
   {
     size_t words = 0;
@@ -247,24 +435,21 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
   };
   if (c.batched) launch_deep(0, djobs.size());
   else for (size_t i = 0; i < djobs.size(); i++) launch_deep(i, 1);
+}
 
-  c.phase("deep");
-  // ---- FRI (internal/fri/fri.go:352-365,606-736)
+// ---- FRI levels tree (internal/fri/fri.go:294-317,352-365)
+inline Digest Prover::commit_levels() {
+  if (deep.empty()) throw Error(LG_ERR_INVALID, "nothing to open: the DEEP codewords are not computed");
   std::vector<size_t> class_at(classes.size());
   for (size_t i = 0; i < class_at.size(); i++) class_at[i] = i;
   std::stable_sort(class_at.begin(), class_at.end(), [&](size_t a, size_t b) { return mod_n(classes[a]) > mod_n(classes[b]); });
-  const size_t L = class_at.size();
-  if (L == 0) throw Error(LG_ERR_INVALID, "nothing to open");
-  std::vector<uint32_t> lvl_log(L);
-  std::vector<DBufP> lvl(L);
+  L = class_at.size();
+  lvl_log.assign(L, 0);
+  lvl.assign(L, nullptr);
   for (size_t l = 0; l < L; l++) { lvl_log[l] = pg.modules[classes[class_at[l]]].log_n; lvl[l] = deep[class_at[l]]; }
-  const int NR = MAX_LOG_MODULE;
-  const int r0 = MAX_LOG_MODULE - (int)lvl_log[0];
-  auto jl = [&](size_t l) { return MAX_LOG_MODULE - (int)lvl_log[l]; };
-  for (size_t l = 1; l < L; l++) fs.add("fri_level_" + std::to_string(l) + "_gamma");
-  for (int j = 0; j < NR; j++) fs.add("fri_fold_" + std::to_string(j));
-  for (uint32_t k = 0; k < num_queries; k++) fs.add("fri_query_" + std::to_string(k));
-  TreeDev levels_tree;
+  NR = MAX_LOG_MODULE;
+  r0 = MAX_LOG_MODULE - (int)lvl_log[0];
+  levels_tree = TreeDev();
   levels_tree.log_leaves = lvl_log[0] + RATE_LOG - 1;
   levels_tree.nodes = std::make_shared<DBuf>((size_t)16 << levels_tree.log_leaves, c.stream);
   {
@@ -281,283 +466,138 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
     else for (auto& g : lgs) launch_leaves(c, {g});
   }
   build_tree(c, levels_tree);
-  c.phase("levels tree");
-  std::vector<E6> gam(L);
-  for (size_t l = 1; l < L; l++) {
-    std::string nm = "fri_level_" + std::to_string(l) + "_gamma";
-    if (l == 1) fs.bind(nm, levels_tree.root.v, 8);
-    gam[l] = digest_e6(fs.compute(nm));
-  }
-  Digest zero{};
-  for (int j = 0; j < r0; j++) {
-    fs.bind("fri_fold_" + std::to_string(j), zero.v, 8);
-    fs.compute("fri_fold_" + std::to_string(j));
-  }
-  std::vector<DBufP> layers(NR + 1);
-  std::vector<TreeDev> ftrees(NR);
-  std::vector<Digest> fri_roots;
-  // Fold challenges after the first are computed on the device from the
-  // layer roots (k_fs_challenge), so the rounds run without a host round
-  // trip; the host replays them after the loop and checks every digest.
-  auto chal = std::make_shared<DBuf>((size_t)8 * NR, c.stream);
-  std::vector<uint32_t> pre_all;
-  std::vector<uint32_t> pre_off(NR), pre_len(NR);
-  for (int j = r0 + 1; j < NR; j++) {
-    auto pe = string_to_elements(0x46534944u, "fri_fold_" + std::to_string(j));
-    if (pe.size() > 48) throw Error(LG_ERR_UNSUPPORTED, "challenge name too long");
-    pre_off[j] = (uint32_t)pre_all.size();
-    pre_len[j] = (uint32_t)pe.size();
-    pre_all.insert(pre_all.end(), pe.begin(), pe.end());
-  }
-  auto pre_d = upload_vec(c, pre_all.empty() ? std::vector<uint32_t>{0} : pre_all);
-  size_t nj = (size_t)1 << (LOG_N_FRI - r0);
-  auto running = std::make_shared<DBuf>(6 * nj, c.stream);
-  LG_CK(cudaMemcpyAsync(running->p, lvl[0]->p, 6 * nj * 4, cudaMemcpyDeviceToDevice, c.stream));
-  const uint32_t inv2 = inv(to_mont(2));
-  for (int j = r0; j < NR; j++) {
-    if (j == r0) layers[j] = lvl[0];
-    {
-      std::vector<AxpyTerm> terms;
-      for (size_t l = 1; l < L; l++)
-        if (jl(l) == j) terms.push_back(AxpyTerm{lvl[l]->p, gam[l]});
-      auto axpy = [&](const std::vector<AxpyTerm>& tv) {
-        auto td = upload_vec(c, tv);
-        c.timed("fri_axpy", 0, 0, [&] {
-          k_axpy_e6<<<(unsigned)((nj + 255) / 256), 256, 0, c.stream>>>(running->p, nj, (const AxpyTerm*)td->p,
-                                                                         (uint32_t)tv.size());
-          LG_LAUNCH();
-        });
-      };
-      if (!terms.empty()) {
-        if (c.batched) axpy(terms);
-        else for (auto& tm : terms) axpy({tm});
+  gam.assign(L, e6_zero());
+  gam_ready.assign(L, 0);
+  layers.assign(NR + 1, nullptr);
+  ftrees.assign(NR, TreeDev());
+  fri_roots.clear();
+  chal = std::make_shared<DBuf>((size_t)8 * NR, c.stream);
+  chal_ready.assign(NR, 0);
+  nj = (size_t)1 << (LOG_N_FRI - r0);
+  fri_next = r0;
+  return levels_tree.root;
+}
+
+// ---- one FRI round: fold layer j (internal/fri/fri.go:1177-1198), then the
+// levels that enter at round j + 1 and the next layer's tree
+inline bool Prover::fri_fold_round(int j, bool read_root, Digest* next_root) {
+  if (fri_next < 0) throw Error(LG_ERR_INVALID, "the FRI levels are not committed yet");
+  if (j != fri_next) throw Error(LG_ERR_INVALID, "FRI rounds run in order: the next one is fri_fold_" + std::to_string(fri_next));
+  if (!chal_ready[j]) throw Error(LG_ERR_INVALID, "challenge fri_fold_" + std::to_string(j) + " has not been set");
+  auto jl = [&](size_t l) { return MAX_LOG_MODULE - (int)lvl_log[l]; };
+  auto add_levels = [&](int round) {  // running += gamma_l level_l for the levels entering at `round`
+    std::vector<AxpyTerm> terms;
+    for (size_t l = 1; l < L; l++)
+      if (jl(l) == round) {
+        if (!gam_ready[l]) throw Error(LG_ERR_INVALID, "challenge fri_level_" + std::to_string(l) + "_gamma has not been set");
+        terms.push_back(AxpyTerm{lvl[l]->p, gam[l]});
       }
-    }
-    if (j > r0) layers[j] = running;
-    if (j == r0) {
-      ftrees[j] = levels_tree;
-      const std::string nm = "fri_fold_" + std::to_string(j);
-      fs.bind(nm, levels_tree.root.v, 8);
-      Digest d = fs.compute(nm);
-      c.h2d(chal->p + 8 * (size_t)j, d.v, 32);
-    } else {
-      TreeDev& t = ftrees[j];
-      t.log_leaves = (uint32_t)(LOG_N_FRI - j - 1);
-      t.nodes = std::make_shared<DBuf>((size_t)16 << t.log_leaves, c.stream);
-      launch_leaves(c, {leaf_group(running->p, 0, 1, (uint32_t)(LOG_N_FRI - j), t.nodes->p + ((size_t)8 << t.log_leaves))});
-      build_tree(c, t, false);
-      c.timed("fri_challenge", 0, 0, [&] {
-        k_fs_challenge<<<1, 32, 0, c.stream>>>(pre_d->p + pre_off[j], pre_len[j], chal->p + 8 * (size_t)(j - 1),
-                                               t.nodes->p + 8, chal->p + 8 * (size_t)j);
+    auto axpy = [&](const std::vector<AxpyTerm>& tv) {
+      auto td = upload_vec(c, tv);
+      c.timed("fri_axpy", 0, 0, [&] {
+        k_axpy_e6<<<(unsigned)((nj + 255) / 256), 256, 0, c.stream>>>(running->p, nj, (const AxpyTerm*)td->p,
+                                                                       (uint32_t)tv.size());
         LG_LAUNCH();
       });
-    }
-    auto next = std::make_shared<DBuf>(3 * nj, c.stream);
-    const uint32_t* twj = c.twiddles(LOG_N_FRI - j);
-    c.timed("fri_fold", 36.0 * nj, 0, [&] {
-      k_fold<<<(unsigned)((nj / 2 + 255) / 256), 256, 0, c.stream>>>(running->p, nj, chal->p + 8 * (size_t)j, twj, inv2,
-                                                                     next->p);
-      LG_LAUNCH();
-    });
-    running = next;
-    nj /= 2;
+    };
+    if (terms.empty()) return;
+    if (c.batched) axpy(terms);
+    else for (auto& tm : terms) axpy({tm});
+  };
+  if (j == r0) {
+    layers[j] = lvl[0];
+    ftrees[j] = levels_tree;
+    running = std::make_shared<DBuf>(6 * nj, c.stream);
+    LG_CK(cudaMemcpyAsync(running->p, lvl[0]->p, 6 * nj * 4, cudaMemcpyDeviceToDevice, c.stream));
+    add_levels(j);
   }
-  std::vector<uint32_t> final_poly(6 * nj);
-  {
-    // one read-back: final polynomial, device challenges, layer roots
-    const size_t nroot = (size_t)(NR > r0 + 1 ? NR - r0 - 1 : 0);
-    uint32_t* h = c.host_staging(6 * nj + 8 * (size_t)NR + 8 * nroot);
-    LG_CK(cudaMemcpyAsync(h, running->p, 6 * nj * 4, cudaMemcpyDeviceToHost, c.stream));
-    LG_CK(cudaMemcpyAsync(h + 6 * nj, chal->p, 8 * (size_t)NR * 4, cudaMemcpyDeviceToHost, c.stream));
-    for (int j = r0 + 1; j < NR; j++)
-      LG_CK(cudaMemcpyAsync(h + 6 * nj + 8 * (size_t)NR + 8 * (size_t)(j - r0 - 1), ftrees[j].nodes->p + 8, 32,
-                            cudaMemcpyDeviceToHost, c.stream));
-    LG_CK(cudaStreamSynchronize(c.stream));
-    memcpy(final_poly.data(), h, 6 * nj * 4);
-    for (int j = r0 + 1; j < NR; j++) {
-      Digest root;
-      memcpy(root.v, h + 6 * nj + 8 * (size_t)NR + 8 * (size_t)(j - r0 - 1), 32);
-      ftrees[j].root = root;
-      fri_roots.push_back(root);
-      const std::string nm = "fri_fold_" + std::to_string(j);
-      fs.bind(nm, root.v, 8);
-      Digest d = fs.compute(nm);
-      if (memcmp(d.v, h + 6 * nj + 8 * (size_t)j, 32) != 0)
-        throw Error(LG_ERR_CUDA, "device and host transcripts disagree at " + nm);
-    }
-    std::vector<uint32_t> fin = {to_mont(0x45585450u), to_mont((uint32_t)nj)};
-    for (size_t i = 0; i < nj; i++) for (int w = 0; w < 6; w++) fin.push_back(final_poly[w * nj + i]);
-    fs.bind("fri_query_0", fin.data(), fin.size());
+  auto next = std::make_shared<DBuf>(3 * nj, c.stream);
+  const uint32_t* twj = c.twiddles(LOG_N_FRI - j);
+  const uint32_t inv2 = inv(to_mont(2));
+  c.timed("fri_fold", 36.0 * nj, 0, [&] {
+    k_fold<<<(unsigned)((nj / 2 + 255) / 256), 256, 0, c.stream>>>(running->p, nj, chal->p + 8 * (size_t)j, twj, inv2,
+                                                                   next->p);
+    LG_LAUNCH();
+  });
+  running = next;
+  nj /= 2;
+  fri_next = j + 1;
+  if (j + 1 >= NR) return false;
+  add_levels(j + 1);
+  layers[j + 1] = running;
+  TreeDev& t = ftrees[j + 1];
+  t.log_leaves = (uint32_t)(LOG_N_FRI - (j + 1) - 1);
+  t.nodes = std::make_shared<DBuf>((size_t)16 << t.log_leaves, c.stream);
+  launch_leaves(c, {leaf_group(running->p, 0, 1, (uint32_t)(LOG_N_FRI - (j + 1)), t.nodes->p + ((size_t)8 << t.log_leaves))});
+  build_tree(c, t, read_root);
+  if (read_root) {
+    fri_roots.push_back(t.root);
+    *next_root = t.root;
   }
-  c.phase("fri rounds");
-  std::vector<uint32_t> pos(num_queries);
-  for (uint32_t k = 0; k < num_queries; k++) {
-    Digest ch = fs.compute("fri_query_" + std::to_string(k));
-    uint64_t s = (((uint64_t)from_mont(ch.v[0]) << 31) ^ (uint64_t)from_mont(ch.v[1])) % (1ull << LOG_N_FRI);
-    pos[k] = (uint32_t)s;
-    if (k + 1 < num_queries) fs.bind("fri_query_" + std::to_string(k + 1), ch.v, 8);
-  }
+  return true;
+}
 
-  c.phase("query challenges");
-  // ---- openings: one gather into a staging buffer, one read-back
-  std::vector<RowSrc> rows;
-  std::vector<PathSrc> paths;
-  uint64_t per_q = 0;
-  auto add_rows = [&](const uint32_t* lane0, uint64_t stride, uint32_t nl, uint32_t shift) {
-    rows.push_back(RowSrc{lane0, stride, nl, shift, per_q});
-    uint64_t o = per_q;
-    per_q += 2ull * nl;
-    return o;
-  };
-  auto add_path = [&](const TreeDev& t, uint32_t shift, bool with_inj) {
-    PathSrc p{};
-    p.nodes = t.nodes->p;
-    p.inj = with_inj ? (const uint32_t* const*)t.inj_ptrs->p : nullptr;
-    p.inj_shift = with_inj ? t.inj_shift->p : nullptr;
-    p.log_leaves = t.log_leaves;
-    p.n_inj = with_inj ? (uint32_t)t.inj.size() : 0;
-    p.shift = shift;
-    p.off = per_q;
-    paths.push_back(p);
-    uint64_t o = per_q;
-    per_q += 8ull * (p.log_leaves + p.n_inj);
-    return o;
-  };
+inline void Prover::read_final_poly() {
+  if (fri_next != NR) throw Error(LG_ERR_INVALID, "the FRI rounds are not all folded yet");
+  final_poly.assign(6 * nj, 0);
+  uint32_t* h = c.host_staging(6 * nj);
+  c.d2h(h, running->p, 6 * nj);
+  memcpy(final_poly.data(), h, 6 * nj * 4);
+}
+
+// ---- openings: one gather into a staging buffer, one read-back; then the
+// canonical encoding (same order as the proof structs)
+inline size_t Prover::open_and_encode(const std::vector<uint32_t>& pos, uint8_t* out, size_t out_cap, bool* in_out) {
+  if (final_poly.empty()) throw Error(LG_ERR_INVALID, "the FRI final polynomial is not computed yet");
+  if (pos.size() != num_queries) throw Error(LG_ERR_INVALID, "one position per query is needed");
+  for (uint32_t s : pos)
+    if (s >= (1u << LOG_N_FRI)) throw Error(LG_ERR_INVALID, "query position out of range");
+  auto jl = [&](size_t l) { return MAX_LOG_MODULE - (int)lvl_log[l]; };
+  OpenPlan OP;
   std::vector<uint64_t> fri_row_off(NR), fri_path_off(NR), lvl_row_off(L);
   for (int j = r0; j < NR; j++) {
     size_t n_j = (size_t)1 << (LOG_N_FRI - j);
-    fri_row_off[j] = add_rows(layers[j]->p, n_j, 6, (uint32_t)j);
-    fri_path_off[j] = add_path(ftrees[j], (uint32_t)j, false);
+    fri_row_off[j] = OP.add_rows(layers[j]->p, n_j, 6, (uint32_t)j);
+    fri_path_off[j] = OP.add_path(ftrees[j], (uint32_t)j, false);
   }
-  for (size_t l = 1; l < L; l++) lvl_row_off[l] = add_rows(lvl[l]->p, (size_t)1 << (lvl_log[l] + RATE_LOG), 6, (uint32_t)jl(l));
-  struct BatchOff { std::vector<uint64_t> rows; uint64_t path; };
-  std::vector<BatchOff> boff(committed.size());
-  for (size_t b = 0; b < committed.size(); b++) {
-    const Committed& cm = committed[b];
-    for (int gi : cm.order) {
-      const LdeOut& l = cm.groups[gi];
-      uint32_t log_rows = l.log_n + RATE_LOG;
-      boff[b].rows.push_back(add_rows(l.lde->p, (size_t)1 << log_rows, l.lanes, (uint32_t)(LOG_N_FRI - log_rows)));
-    }
-    const LdeOut& top = cm.groups[cm.order[0]];
-    boff[b].path = add_path(cm.tree, (uint32_t)(LOG_N_FRI - (top.log_n + RATE_LOG)), true);
-  }
-  auto pos_d = upload_vec(c, pos);
-  auto out_d = std::make_shared<DBuf>(per_q * num_queries, c.stream);
-  {
-    auto rd = upload_vec(c, rows);
-    uint32_t max_l = 1;
-    for (auto& r : rows) max_l = std::max(max_l, r.n_lanes);
-    auto pd = upload_vec(c, paths);
-    uint32_t max_t = 1;
-    for (auto& p : paths) max_t = std::max(max_t, p.log_leaves + p.n_inj);
-    c.timed("openings", 8.0 * per_q * num_queries, 0, [&] {
-      k_gather_rows<<<dim3((max_l + 63) / 64, num_queries, (unsigned)rows.size()), 64, 0, c.stream>>>(
-          (const RowSrc*)rd->p, (uint32_t)rows.size(), pos_d->p, num_queries, per_q, out_d->p);
-      LG_LAUNCH();
-      k_gather_paths<<<dim3((max_t + 31) / 32, num_queries, (unsigned)paths.size()), 32, 0, c.stream>>>(
-          (const PathSrc*)pd->p, pos_d->p, num_queries, per_q, out_d->p);
-      LG_LAUNCH();
-      k_proof_words<<<(unsigned)((per_q * num_queries + 255) / 256), 256, 0, c.stream>>>(out_d->p,
-                                                                                         per_q * num_queries);
-      LG_LAUNCH();
-    });
-  }
-  // ---- per-query sections, laid out on the GPU in proof order and encoding
-  struct SecBuild {
-    std::vector<uint32_t> map, consts;
-    std::vector<PosOp> pops;
-    std::vector<SectionSrc> secs;
-    uint64_t total = 0;
-    size_t start = 0;
-    void begin() { start = map.size(); }
-    void konst(uint32_t v) {
-      map.push_back((SEC_CONST << 30) | (uint32_t)consts.size());
-      consts.push_back(v);
-    }
-    void posw(uint32_t shift, bool leaf) {
-      map.push_back((SEC_POS << 30) | (uint32_t)pops.size());
-      pops.push_back(PosOp{shift, leaf ? 1u : 0u});
-    }
-    void copy(uint64_t off, size_t n) {
-      if (off + n > 0x3fffffffu) throw Error(LG_ERR_UNSUPPORTED, "opening block too large");
-      for (size_t i = 0; i < n; i++) map.push_back((uint32_t)(off + i));
-    }
-    SectionSrc end(uint32_t nq) {
-      SectionSrc sc{start, total, (uint32_t)(map.size() - start)};
-      secs.push_back(sc);
-      total += (uint64_t)nq * sc.q_words;
-      return sc;
-    }
-  } SB;
+  for (size_t l = 1; l < L; l++)
+    lvl_row_off[l] = OP.add_rows(lvl[l]->p, (size_t)1 << (lvl_log[l] + RATE_LOG), 6, (uint32_t)jl(l));
   std::vector<SectionSrc> lvl_sec(L);
   for (size_t l = 1; l < L; l++) {  // FRI level openings (one section per level)
-    SB.begin();
-    SB.konst(1);
-    SB.posw((uint32_t)jl(l), false);
-    SB.copy(lvl_row_off[l], 12);
-    SB.konst(0); SB.konst(0); SB.konst(0);
-    lvl_sec[l] = SB.end(num_queries);
+    OP.begin();
+    OP.konst(1);
+    OP.posw((uint32_t)jl(l), false);
+    OP.copy(lvl_row_off[l], 12);
+    OP.konst(0); OP.konst(0); OP.konst(0);
+    lvl_sec[l] = OP.end(num_queries);
   }
-  SB.begin();  // FRI fold openings
-  SB.konst((uint32_t)(NR - r0));
+  OP.begin();  // FRI fold openings
+  OP.konst((uint32_t)(NR - r0));
   for (int j = r0; j < NR; j++) {
-    SB.konst(1);
-    SB.posw((uint32_t)j, false);
-    SB.copy(fri_row_off[j], 12);
-    SB.posw((uint32_t)j, true);
-    SB.konst(ftrees[j].log_leaves);
-    SB.copy(fri_path_off[j], 8 * (size_t)ftrees[j].log_leaves);
-    SB.konst(0);
+    OP.konst(1);
+    OP.posw((uint32_t)j, false);
+    OP.copy(fri_row_off[j], 12);
+    OP.posw((uint32_t)j, true);
+    OP.konst(ftrees[j].log_leaves);
+    OP.copy(fri_path_off[j], 8 * (size_t)ftrees[j].log_leaves);
+    OP.konst(0);
   }
-  const SectionSrc fri_sec = SB.end(num_queries);
-  SB.begin();  // batch openings: rows of every group, the batch tree's path
-  SB.konst((uint32_t)committed.size());
+  const SectionSrc fri_sec = OP.end(num_queries);
+  std::vector<OpenBatch> obs;
   for (size_t b = 0; b < committed.size(); b++) {
-    const Committed& cm = committed[b];
-    auto rowpair = [&](int gi, uint64_t off) {
-      const LdeOut& l = cm.groups[gi];
-      const Group& G2 = trees[b].groups[gi];
-      uint32_t nb = (uint32_t)G2.bcols.size(), ne = (uint32_t)G2.ecols.size();
-      if (l.lanes != nb + 6 * ne) throw Error(LG_ERR_INVALID, "opening row width");
-      for (int h = 0; h < 2; h++) {
-        SB.konst(nb);
-        SB.copy(off + (uint64_t)h * l.lanes, nb);
-        SB.konst(ne);
-        SB.copy(off + (uint64_t)h * l.lanes + nb, 6 * (size_t)ne);
-      }
-    };
-    const LdeOut& top = cm.groups[cm.order[0]];
-    rowpair(cm.order[0], boff[b].rows[0]);
-    SB.posw((uint32_t)(LOG_N_FRI - (top.log_n + RATE_LOG)), true);
-    SB.konst(cm.tree.log_leaves);
-    SB.copy(boff[b].path, 8 * (size_t)cm.tree.log_leaves);
-    SB.konst((uint32_t)cm.tree.inj.size());
-    SB.copy(boff[b].path + 8 * (size_t)cm.tree.log_leaves, 8 * cm.tree.inj.size());
-    SB.konst((uint32_t)(cm.order.size() - 1));
-    for (size_t s = 1; s < cm.order.size(); s++) rowpair(cm.order[s], boff[b].rows[s]);
+    OpenBatch ob{&committed[b], {}, {}};
+    for (const Group& G2 : trees[b].groups) {
+      ob.nb.push_back((uint32_t)G2.bcols.size());
+      ob.ne.push_back((uint32_t)G2.ecols.size());
+    }
+    obs.push_back(ob);
   }
-  const SectionSrc batch_sec = SB.end(num_queries);
-  auto asm_d = std::make_shared<DBuf>(SB.total, c.stream);
-  {
-    auto map_d = upload_vec(c, SB.map), consts_d = upload_vec(c, SB.consts);
-    auto pops_d = upload_vec(c, SB.pops), secs_d = upload_vec(c, SB.secs);
-    uint32_t max_q = 1;
-    for (auto& sc : SB.secs) max_q = std::max(max_q, sc.q_words);
-    c.timed("openings", 8.0 * SB.total, 0, [&] {
-      k_assemble<<<dim3((max_q + 255) / 256, num_queries, (unsigned)SB.secs.size()), 256, 0, c.stream>>>(
-          (const SectionSrc*)secs_d->p, map_d->p, consts_d->p, (const PosOp*)pops_d->p, pos_d->p, out_d->p, per_q,
-          num_queries, asm_d->p);
-      LG_LAUNCH();
-    });
-  }
-  uint32_t* A = c.host_staging(SB.total);
-  c.d2h(A, asm_d->p, SB.total);
+  const SectionSrc batch_sec = OP.batches_section(obs, num_queries);
+  const uint32_t* A = OP.run(c, pos);
 
   c.phase("openings gather");
-  // ---- canonical encoding (same order as the proof structs)
   Writer W(c.proof_buf, out, out_cap);
-  W.expect((size_t)4 * SB.total + (1 << 20));
+  W.expect((size_t)4 * OP.total + (1 << 20));
   W.str("poseidon2");
   {  // exposed values by name: name, one entry (index 0, extension kind 1, value)
     std::vector<std::pair<std::string, size_t>> ev;
@@ -609,6 +649,141 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
   c.phase("serialize");
   *in_out = W.in_caller_buffer();
   return W.length();
+}
+
+// ---- the whole prove with the host transcript (prover/prover.go:655-719)
+inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint8_t* out, size_t out_cap,
+                            bool* in_out) {
+  ArenaScope arena(&c.dev_arena);  // rewound by the next call on the context
+  c.phase_start();
+  begin(witness, on_device);
+  c.phase("setup+upload");
+  const uint32_t R = pg.n_rounds;
+  for (uint32_t r = 0; r < R; r++) fs.add(coin_name(r));
+  fs.add("__zeta");
+  {
+    const std::string first = coin_name(0);
+    auto hb = string_to_elements(0x48415348u, "poseidon2");
+    fs.bind(first, hb.data(), hb.size());
+    std::vector<uint32_t> sz = {to_mont(0x53495a45u), to_mont((uint32_t)mod_order.size())};
+    for (uint32_t m : mod_order) sz.push_back(to_mont((uint32_t)mod_n(m)));
+    fs.bind(first, sz.data(), sz.size());
+  }
+  if (has_setup_tree()) fs.bind(coin_name(0), prog->setup->root.v, 8);
+  // ---- rounds: steps, commit, bind root, sample coin (prover/prover.go:360-411)
+  for (uint32_t r = 0; r < R; r++) {
+    Digest root;
+    if (commit_round(r, &root)) fs.bind(coin_name(r), root.v, 8);
+    // BindExposedValues (prover/prover.go:386-396): the round's logup totals
+    // in step order, each as its entry index then six elements
+    // (board/logup.go:218-225)
+    for (const E6& e : round_exposed(r)) {
+      uint32_t w[7] = {0};
+      for (int k = 0; k < 6; k++) w[1 + k] = e.c[k];
+      fs.bind(coin_name(r), w, 7);
+    }
+    set_challenge(coin_name(r), fs.compute(coin_name(r)).v);
+    c.phase(("round " + std::to_string(r)).c_str());
+  }
+  // ---- AIR quotients and their commitment
+  {
+    Digest root;
+    if (commit_quotient(&root)) fs.bind("__zeta", root.v, 8);
+  }
+  set_challenge("__zeta", fs.compute("__zeta").v);
+  c.phase("quotient+air commit");
+  // ---- claimed values and alpha_DEEP
+  claimed_values();
+  fs.add("alpha_DEEP");
+  for (const E6& v : claimed_values_bind_order()) fs.bind("alpha_DEEP", v.c, 6);
+  set_challenge("alpha_DEEP", fs.compute("alpha_DEEP").v);
+  c.phase("claimed values+bind");
+  deep_codewords();
+  c.phase("deep");
+  // ---- FRI
+  const Digest lroot = commit_levels();
+  c.phase("levels tree");
+  for (size_t l = 1; l < L; l++) fs.add("fri_level_" + std::to_string(l) + "_gamma");
+  for (int j = 0; j < NR; j++) fs.add("fri_fold_" + std::to_string(j));
+  for (uint32_t k = 0; k < num_queries; k++) fs.add("fri_query_" + std::to_string(k));
+  for (size_t l = 1; l < L; l++) {
+    std::string nm = "fri_level_" + std::to_string(l) + "_gamma";
+    if (l == 1) fs.bind(nm, lroot.v, 8);
+    set_challenge(nm, fs.compute(nm).v);
+  }
+  Digest zero{};
+  for (int j = 0; j < r0; j++) {
+    fs.bind("fri_fold_" + std::to_string(j), zero.v, 8);
+    fs.compute("fri_fold_" + std::to_string(j));
+  }
+  {
+    const std::string nm = "fri_fold_" + std::to_string(r0);
+    fs.bind(nm, lroot.v, 8);
+    set_challenge(nm, fs.compute(nm).v);
+  }
+  // Fold challenges after the first are computed on the device from the
+  // layer roots (k_fs_challenge), so the rounds run without a host round
+  // trip; the host replays them after the loop and checks every digest.
+  std::vector<uint32_t> pre_all;
+  std::vector<uint32_t> pre_off(NR), pre_len(NR);
+  for (int j = r0 + 1; j < NR; j++) {
+    auto pe = string_to_elements(0x46534944u, "fri_fold_" + std::to_string(j));
+    if (pe.size() > 48) throw Error(LG_ERR_UNSUPPORTED, "challenge name too long");
+    pre_off[j] = (uint32_t)pre_all.size();
+    pre_len[j] = (uint32_t)pe.size();
+    pre_all.insert(pre_all.end(), pe.begin(), pe.end());
+  }
+  auto pre_d = upload_vec(c, pre_all.empty() ? std::vector<uint32_t>{0} : pre_all);
+  for (int j = r0; j < NR; j++) {
+    if (j > r0) {
+      c.timed("fri_challenge", 0, 0, [&] {
+        k_fs_challenge<<<1, 32, 0, c.stream>>>(pre_d->p + pre_off[j], pre_len[j], chal->p + 8 * (size_t)(j - 1),
+                                               ftrees[j].nodes->p + 8, chal->p + 8 * (size_t)j);
+        LG_LAUNCH();
+      });
+      chal_ready[j] = 1;
+    }
+    Digest unused;
+    fri_fold_round(j, false, &unused);
+  }
+  {
+    // one read-back: final polynomial, device challenges, layer roots
+    const size_t nroot = (size_t)(NR > r0 + 1 ? NR - r0 - 1 : 0);
+    uint32_t* h = c.host_staging(6 * nj + 8 * (size_t)NR + 8 * nroot);
+    LG_CK(cudaMemcpyAsync(h, running->p, 6 * nj * 4, cudaMemcpyDeviceToHost, c.stream));
+    LG_CK(cudaMemcpyAsync(h + 6 * nj, chal->p, 8 * (size_t)NR * 4, cudaMemcpyDeviceToHost, c.stream));
+    for (int j = r0 + 1; j < NR; j++)
+      LG_CK(cudaMemcpyAsync(h + 6 * nj + 8 * (size_t)NR + 8 * (size_t)(j - r0 - 1), ftrees[j].nodes->p + 8, 32,
+                            cudaMemcpyDeviceToHost, c.stream));
+    LG_CK(cudaStreamSynchronize(c.stream));
+    final_poly.assign(6 * nj, 0);
+    memcpy(final_poly.data(), h, 6 * nj * 4);
+    fri_roots.clear();
+    for (int j = r0 + 1; j < NR; j++) {
+      Digest root;
+      memcpy(root.v, h + 6 * nj + 8 * (size_t)NR + 8 * (size_t)(j - r0 - 1), 32);
+      ftrees[j].root = root;
+      fri_roots.push_back(root);
+      const std::string nm = "fri_fold_" + std::to_string(j);
+      fs.bind(nm, root.v, 8);
+      Digest d = fs.compute(nm);
+      if (memcmp(d.v, h + 6 * nj + 8 * (size_t)j, 32) != 0)
+        throw Error(LG_ERR_CUDA, "device and host transcripts disagree at " + nm);
+    }
+    std::vector<uint32_t> fin = {to_mont(0x45585450u), to_mont((uint32_t)nj)};
+    for (size_t i = 0; i < nj; i++) for (int w = 0; w < 6; w++) fin.push_back(final_poly[w * nj + i]);
+    fs.bind("fri_query_0", fin.data(), fin.size());
+  }
+  c.phase("fri rounds");
+  std::vector<uint32_t> pos(num_queries);
+  for (uint32_t k = 0; k < num_queries; k++) {
+    Digest ch = fs.compute("fri_query_" + std::to_string(k));
+    uint64_t s = (((uint64_t)from_mont(ch.v[0]) << 31) ^ (uint64_t)from_mont(ch.v[1])) % (1ull << LOG_N_FRI);
+    pos[k] = (uint32_t)s;
+    if (k + 1 < num_queries) fs.bind("fri_query_" + std::to_string(k + 1), ch.v, 8);
+  }
+  c.phase("query challenges");
+  return open_and_encode(pos, out, out_cap, in_out);
 }
 
 }  // namespace lg

@@ -76,6 +76,35 @@ struct Prover {
   E6 zeta;
 
   ProgCache* prog = nullptr;  // compiled code of this program, kept on the context
+  std::shared_ptr<ProgCache> prog_keep;  // ... and alive while this prove lasts
+
+  // ---- state of the phases (prove_flow.cuh), in the order they run
+  struct Poly { size_t t, g; bool ext; const uint32_t* coef; uint32_t logn; std::vector<int> shifts; };
+  size_t tree_next = 0;                     // next entry of `trees` to commit
+  std::vector<char> coin_ready;             // per round: its challenge is known
+  bool zeta_ready = false, alpha_ready = false;
+  E6 alpha;
+  std::vector<std::vector<std::vector<Poly>>> polys;                  // [tree][group] base then ext polys
+  std::vector<std::vector<std::vector<std::vector<E6>>>> cv;          // claimed values [tree][group][poly][shift]
+  std::vector<uint32_t> classes;            // DEEP classes: modules with committed groups, layout order
+  std::vector<DBufP> deep;                  // DEEP codeword per class (6 lanes x 4n)
+  // FRI (internal/fri/fri.go:352-365,606-736)
+  size_t L = 0;                             // levels, sorted by size (descending, stable)
+  int NR = 0, r0 = 0;                       // rounds; the first round with a layer
+  std::vector<uint32_t> lvl_log;
+  std::vector<DBufP> lvl;
+  TreeDev levels_tree;
+  std::vector<E6> gam;                      // level weights (gam[0] unused)
+  std::vector<char> gam_ready;
+  std::vector<DBufP> layers;                // layer j (E6 lanes), r0 <= j < NR
+  std::vector<TreeDev> ftrees;
+  std::vector<Digest> fri_roots;            // layer roots after the first
+  DBufP chal;                               // fold challenge j at chal + 8 j (digest words)
+  std::vector<char> chal_ready;
+  DBufP running;                            // the layer being folded
+  size_t nj = 0;                            // its length
+  int fri_next = -1;                        // next round to fold (-1: levels not committed)
+  std::vector<uint32_t> final_poly;         // 6 lanes of nj words, once read back
 
   Prover(Ctx& ctx, const uint32_t* words, size_t nwords, uint32_t q) : c(ctx), num_queries(q) {
     pg = parse_program(words, nwords);
@@ -93,7 +122,8 @@ struct Prover {
       L.push_front(e);
       while (L.size() > Ctx::MAX_PROGRAMS) L.pop_back();
     }
-    prog = L.front().get();
+    prog_keep = L.front();
+    prog = prog_keep.get();
   }
 
   // The bytecode of `roots` compiled in order against one lane table
@@ -1174,8 +1204,46 @@ struct Prover {
     }
   }
 
-  // Returns the proof length.  The bytes go to out[0, out_cap) when they fit
-  // (*in_out = true), else to c.proof_buf.
+  // ------------------------------------------------------------ phases
+  // The prove as a sequence of device phases (prove_flow.cuh).  Each phase
+  // needs the challenges that the transcript derives from the results of the
+  // phases before it; the caller keeps the transcript (lg_prove: the host
+  // Transcript below; the session entry points: the caller of the C ABI)
+  // and hands the challenges in with set_challenge.
+  void begin(const uint32_t* const* witness, bool on_device);
+  bool has_setup_tree() const { return !trees.empty() && trees[0].setup; }
+  // ExecuteSteps + commitTraceRound of round r (prover/prover.go:321-411):
+  // true with the root when the round commits a tree.
+  bool commit_round(uint32_t r, Digest* root);
+  // the exposed values of round r's steps, in step order (Montgomery E6)
+  std::vector<E6> round_exposed(uint32_t r) const;
+  // ComputeAIRQuotients and the AIR commitment (prover/prover.go:461-561)
+  bool commit_quotient(Digest* root);
+  // claimed values at zeta (internal/fri/values.go:46-110), and the order
+  // bindClaimedValuesByPolynomialOrder binds them (internal/fri/open.go:223-285)
+  void claimed_values();
+  std::vector<E6> claimed_values_bind_order() const;
+  void deep_codewords();                  // internal/fri/deep.go:71-266
+  Digest commit_levels();                 // fri.Prove's levels tree (internal/fri/fri.go:294-317)
+  // fold round j (foldLayerExt) with the challenge at chal + 8 j, then the
+  // next layer's commitment; true with its root (read back when read_root)
+  bool fri_fold_round(int j, bool read_root, Digest* next_root);
+  void read_final_poly();
+  // query openings at positions (openQueryExt, openCommittedAt) and the
+  // canonical encoding of the whole proof
+  size_t open_and_encode(const std::vector<uint32_t>& pos, uint8_t* out, size_t out_cap, bool* in_out);
+  // challenge by its transcript name: challenge@loom_<r> and __zeta (E6 from
+  // the digest's first six words), alpha_DEEP, fri_level_<l>_gamma,
+  // fri_fold_<j> (the whole digest)
+  void set_challenge(const std::string& name, const uint32_t* digest);
+  void need_coins(uint32_t r) const {
+    for (uint32_t k = 0; k < r; k++)
+      if (!coin_ready[k]) throw Error(LG_ERR_INVALID, "challenge " + coin_name(k) + " has not been set");
+  }
+
+  // Whole prove with the host transcript (lg_prove).  Returns the proof
+  // length.  The bytes go to out[0, out_cap) when they fit (*in_out = true),
+  // else to c.proof_buf.
   size_t prove(const uint32_t* const* witness, bool on_device, uint8_t* out, size_t out_cap, bool* in_out);
 };
 

@@ -35,6 +35,7 @@ def lib():
         L.oracle_last_error.restype = ctypes.c_char_p
         L.oracle_prove.argtypes = [u32p, ctypes.c_size_t, ctypes.POINTER(u32p), ctypes.c_uint32,
                                    ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_size_t)]
+        L.oracle_last_proof.argtypes = [ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_size_t)]
         L.oracle_verify.argtypes = [u32p, ctypes.c_size_t, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_uint32,
                                     ctypes.c_char_p, u32p, ctypes.c_uint32]
         L.oracle_setup.argtypes = [u32p, ctypes.c_size_t, ctypes.POINTER(u32p), u32p]
@@ -106,17 +107,15 @@ def prove(program_words: np.ndarray, witness_mont: Sequence[np.ndarray], num_que
     prog = _u32(program_words)
     cols = [_u32(c) for c in list(witness_mont) + list(setup_mont)]
     arr = (u32p * max(1, len(cols)))(*[_p(c) for c in cols])
-    cap = ctypes.c_size_t(1 << 20)
-    while True:
-        buf = (ctypes.c_uint8 * cap.value)()
-        need = ctypes.c_size_t(cap.value)
-        rc = L.oracle_prove(_p(prog), prog.size, arr, num_queries, buf, ctypes.byref(need))
-        if rc == 0:
-            return bytes(buf[:need.value])
-        if rc == 1:
-            cap = ctypes.c_size_t(need.value)
-            continue
-        raise RuntimeError("oracle_prove: " + L.oracle_last_error().decode())
+    buf = (ctypes.c_uint8 * (1 << 20))()
+    need = ctypes.c_size_t(1 << 20)
+    rc = L.oracle_prove(_p(prog), prog.size, arr, num_queries, buf, ctypes.byref(need))
+    if rc == 1:  # larger than the first buffer: the oracle kept it
+        buf = (ctypes.c_uint8 * need.value)()
+        rc = L.oracle_last_proof(buf, ctypes.byref(need))
+    if rc == 0:
+        return bytes(buf[:need.value])
+    raise RuntimeError("oracle_prove: " + L.oracle_last_error().decode())
 
 
 def p2_permute(state, width: int = 24) -> np.ndarray:

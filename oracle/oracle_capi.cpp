@@ -28,14 +28,22 @@ extern "C" {
 
 const char* oracle_last_error() { return g_err.c_str(); }
 
+// The last proof made on this thread, for oracle_last_proof.
+static thread_local std::vector<uint8_t> g_last_proof;
+
 // Full prove; proof bytes in the canonical encoding.  Returns 0 on success,
-// 1 when *out_len is too small (required size written back), 2 on error.
+// 1 when *out_len is too small (required size written back; the proof is
+// kept for oracle_last_proof), 2 on error.
 int oracle_prove(const uint32_t* program, size_t nwords, const uint32_t* const* witness, uint32_t num_queries,
                  uint8_t* out, size_t* out_len) {
   try {
     Program pg = parse_program(program, nwords);
     std::vector<uint8_t> b = oracle_prove_bytes(pg, witness, num_queries);
-    if (*out_len < b.size()) { *out_len = b.size(); return 1; }
+    if (*out_len < b.size()) {
+      *out_len = b.size();
+      g_last_proof = std::move(b);
+      return 1;
+    }
     memcpy(out, b.data(), b.size());
     *out_len = b.size();
     return 0;
@@ -43,6 +51,16 @@ int oracle_prove(const uint32_t* program, size_t nwords, const uint32_t* const* 
     g_err = e.what();
     return 2;
   }
+}
+
+// Copies out the proof that the last oracle_prove on this thread kept
+// because its buffer was too small.  Returns 0, or 1 with the size written
+// back when *out_len is still too small.
+int oracle_last_proof(uint8_t* out, size_t* out_len) {
+  if (*out_len < g_last_proof.size()) { *out_len = g_last_proof.size(); return 1; }
+  memcpy(out, g_last_proof.data(), g_last_proof.size());
+  *out_len = g_last_proof.size();
+  return 0;
 }
 
 // Verifies proof bytes against the program (verifier/verifier.go:487-533).

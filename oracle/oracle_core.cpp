@@ -372,14 +372,21 @@ Tree build_tree(const std::vector<Digest>& leaves, const std::vector<Injection>&
   t.nodes.assign(2 * n, Digest{});
   for (size_t i = 0; i < n; i++) t.nodes[n + i] = leaves[i];
   size_t next = 0;
+  // Nodes of one level are independent, and so are the injection chains of
+  // one width (each node folds its own chain in schedule order): both run
+  // over the host threads.
   auto fold = [&](size_t start) {
-    while (next < inj.size() && inj[next].leaves.size() == start) {
-      for (size_t j = 0; j < start; j++) t.nodes[start + j] = node_compress(NODE_TAG, t.nodes[start + j], inj[next].leaves[j]);
-      next++;
-    }
+    size_t first = next;
+    while (next < inj.size() && inj[next].leaves.size() == start) next++;
+    if (next == first) return;
+#pragma omp parallel for schedule(static) if (start >= 256)
+    for (size_t j = 0; j < start; j++)
+      for (size_t k = first; k < next; k++)
+        t.nodes[start + j] = node_compress(NODE_TAG, t.nodes[start + j], inj[k].leaves[j]);
   };
   fold(n);
   for (size_t start = n >> 1; start >= 1; start >>= 1) {
+#pragma omp parallel for schedule(static) if (start >= 256)
     for (size_t i = start; i < 2 * start; i++) t.nodes[i] = node_compress(NODE_TAG, t.nodes[2 * i], t.nodes[2 * i + 1]);
     fold(start);
   }

@@ -309,19 +309,30 @@ struct Prover {
     std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return groups[a].n > groups[b].n; });
     Committed c;
     std::vector<std::vector<Digest>> leaves;
-    for (size_t gi : order) {
-      const GroupData& g = groups[gi];
-      Source s;
+    // every column of every group is encoded independently: one parallel
+    // loop over all of them (the reference fans out per column,
+    // internal/fri/commitment.go:303-331)
+    c.sources.resize(order.size());
+    struct Job { size_t k, i; bool ext; };
+    std::vector<Job> jobs;
+    for (size_t k = 0; k < order.size(); k++) {
+      const GroupData& g = groups[order[k]];
+      Source& s = c.sources[k];
       s.rows = RATE * g.n;
       s.b.resize(g.b.size());
       s.e.resize(g.e.size());
-#pragma omp parallel for schedule(dynamic)
-      for (size_t i = 0; i < g.b.size(); i++) s.b[i] = rs_encode(g.b[i], g.n, s.rows);
-#pragma omp parallel for schedule(dynamic)
-      for (size_t i = 0; i < g.e.size(); i++) s.e[i] = rs_encode_e6(g.e[i], g.n, s.rows);
-      leaves.push_back(hash_leaf_pairs(s));
-      c.sources.push_back(std::move(s));
+      for (size_t i = 0; i < g.b.size(); i++) jobs.push_back({k, i, false});
+      for (size_t i = 0; i < g.e.size(); i++) jobs.push_back({k, i, true});
     }
+#pragma omp parallel for schedule(dynamic)
+    for (size_t q = 0; q < jobs.size(); q++) {
+      const Job& jb = jobs[q];
+      const GroupData& g = groups[order[jb.k]];
+      Source& s = c.sources[jb.k];
+      if (jb.ext) s.e[jb.i] = rs_encode_e6(g.e[jb.i], g.n, s.rows);
+      else s.b[jb.i] = rs_encode(g.b[jb.i], g.n, s.rows);
+    }
+    for (size_t k = 0; k < order.size(); k++) leaves.push_back(hash_leaf_pairs(c.sources[k]));
     std::vector<Injection> inj;
     for (size_t k = 1; k < leaves.size(); k++) inj.push_back(Injection{leaves[k]});
     c.tree = build_tree(leaves[0], inj);
@@ -572,7 +583,9 @@ struct Prover {
   // Q = V / (X^N - 1) evaluated on g<w_big> as rho cosets of size N, then
   // coset-Lagrange -> canonical (iFFT, x g^-k), chunked, FFT_DIF+BitReverse
   // (internal/poly/compute_quotient.go:223-424,484-499; prover/prover.go:422-440).
-  void quotient(uint32_t m) {
+  // Returns the rho chunk columns (E6; base-field relations keep only
+  // coordinate 0 when stored).
+  std::vector<std::vector<E6>> quotient(uint32_t m) {
     size_t n = mod_n(m);
     uint32_t rho = chunk_count(m);
     size_t big = rho * n;
@@ -631,15 +644,34 @@ struct Prover {
     bit_reverse_e6(num.data(), big);
     uint32_t gi = inv(g), acc = 1;
     for (size_t k = 0; k < big; k++) { num[k] = e6_mul_base(num[k], acc); acc = mul(acc, gi); }
+    std::vector<std::vector<E6>> chunks(rho);
     for (uint32_t c = 0; c < rho; c++) {
       std::vector<E6> ch(num.begin() + c * n, num.begin() + (c + 1) * n);
       fft_dif_e6(ch.data(), n);
       bit_reverse_e6(ch.data(), n);
-      if (root_ext[m]) air_ext[{m, c}] = ch;
-      else {
-        std::vector<uint32_t> b(n);
-        for (size_t k = 0; k < n; k++) b[k] = ch[k].c[0];
-        air_base[{m, c}] = b;
+      chunks[c] = std::move(ch);
+    }
+    return chunks;
+  }
+  // Quotients of every module with a relation: modules run in parallel
+  // (largest first), each serially inside.
+  void quotients() {
+    std::vector<uint32_t> ms;
+    for (uint32_t m : mod_order) if (chunk_count(m)) ms.push_back(m);
+    std::stable_sort(ms.begin(), ms.end(), [&](uint32_t a, uint32_t b) { return mod_n(a) > mod_n(b); });
+    std::vector<std::vector<std::vector<E6>>> res(ms.size());
+#pragma omp parallel for schedule(dynamic) if (ms.size() > 1)
+    for (size_t i = 0; i < ms.size(); i++) res[i] = quotient(ms[i]);
+    for (size_t i = 0; i < ms.size(); i++) {
+      const uint32_t m = ms[i];
+      const size_t n = mod_n(m);
+      for (uint32_t c = 0; c < res[i].size(); c++) {
+        if (root_ext[m]) air_ext[{m, c}] = res[i][c];
+        else {
+          std::vector<uint32_t> b(n);
+          for (size_t k = 0; k < n; k++) b[k] = res[i][c][k].c[0];
+          air_base[{m, c}] = b;
+        }
       }
     }
   }
@@ -648,11 +680,12 @@ struct Prover {
   // L_i(zeta) = (zeta^n - 1)/n * w^i / (zeta - w^i)  (internal/poly/utils.go:66-104)
   std::vector<E6> lagranges_at(const E6& z, size_t n) {
     std::vector<E6> res(n);
-    uint32_t w = root_of_unity(n), wi = 1;
-    E6 common = e6_mul_base(e6_sub(e6_pow(z, n), e6_one()), inv((uint32_t)(n % P)));
+    const uint32_t w = root_of_unity(n);
+    const E6 common = e6_mul_base(e6_sub(e6_pow(z, n), e6_one()), inv((uint32_t)(n % P)));
+#pragma omp parallel for schedule(static)
     for (size_t i = 0; i < n; i++) {
+      const uint32_t wi = pow(w, i);
       res[i] = e6_mul(e6_mul_base(common, wi), e6_inv(e6_sub(z, e6_from_base(wi))));
-      wi = mul(wi, w);
     }
     return res;
   }
@@ -742,7 +775,7 @@ struct Prover {
       coins[r] = digest_to_e6(fs.compute(coin_name(r)));
     }
     // AIR quotients (prover/prover.go:461-561)
-    for (uint32_t m : mod_order) if (chunk_count(m)) quotient(m);
+    quotients();
     if (tree_idx < trees.size() && trees[tree_idx].air) {
       committed.push_back(commit(tree_groups(trees[tree_idx])));
       Digest root = committed.back().tree.root();
@@ -754,11 +787,21 @@ struct Prover {
     // claimed values (internal/fri/values.go:46-110)
     std::map<size_t, std::vector<E6>> lag;
     std::vector<std::vector<GroupCV>> cv(trees.size());
+    std::vector<std::pair<size_t, size_t>> tg;  // (tree, group), evaluated in parallel
     for (size_t t = 0; t < trees.size(); t++) {
-      for (const Group& g : trees[t].groups) {
-        size_t n = mod_n(g.module);
+      cv[t].resize(trees[t].groups.size());
+      for (size_t g = 0; g < trees[t].groups.size(); g++) {
+        const size_t n = mod_n(trees[t].groups[g].module);
         if (!lag.count(n)) lag[n] = lagranges_at(zeta, n);
-        const auto& L = lag[n];
+        tg.push_back({t, g});
+      }
+    }
+#pragma omp parallel for schedule(dynamic)
+    for (size_t q = 0; q < tg.size(); q++) {
+      const size_t t = tg[q].first;
+      {
+        const Group& g = trees[t].groups[tg[q].second];
+        const auto& L = lag.at(mod_n(g.module));
         GroupCV gv;
         for (uint32_t c : g.bcols) {
           const uint32_t* p = trees[t].air ? air_base.at({g.module, c}).data() : base.at(c).data();
@@ -772,7 +815,7 @@ struct Prover {
           for (int s : shifts_of(trees[t], c)) vals.push_back(eval_lagrange_e6(p, L, (size_t)s));
           gv.e.push_back(vals);
         }
-        cv[t].push_back(gv);
+        cv[t][tg[q].second] = gv;
       }
     }
     // DEEP classes = modules in sorted order (internal/protocol/layout.go:90-103,
@@ -795,6 +838,9 @@ struct Prover {
 
     // DEEP codewords (internal/fri/deep.go:71-266)
     std::vector<std::vector<E6>> deep(classes.size());
+    // classes are independent: they run in parallel, each serially inside
+    // (with few classes, serially with the rows in parallel)
+#pragma omp parallel for schedule(dynamic) if (classes.size() >= 4)
     for (size_t ci = 0; ci < classes.size(); ci++) {
       uint32_t m = classes[ci];
       size_t n = mod_n(m);
@@ -886,6 +932,7 @@ struct Prover {
       if (j == r0) layers[j] = *lvl[0];
       for (size_t l = 1; l < L; l++) {
         if (lg2(((uint64_t)1 << MAX_LOG) / lvl_d[l]) != j) continue;
+#pragma omp parallel for schedule(static)
         for (size_t k = 0; k < running.size(); k++) running[k] = e6_add(running[k], e6_mul((*lvl[l])[k], gam[l]));
       }
       if (j > r0) layers[j] = running;

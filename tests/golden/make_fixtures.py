@@ -15,7 +15,9 @@ import os
 import re
 import sys
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/make_fixtures.py <path of the loom checkout>")
+ref = sys.argv[1]
 path = os.path.join(ref, "integration_test/zkc/riscv/zkc/lib/poseidon2/constants.zkc")
 txt = open(path).read()
 keys_txt = txt[txt.index("static round_keys"):txt.index("static internal_diag")]

@@ -10,8 +10,9 @@ from loom_b200 import autotune as AT
 class FakeContext:
     """Commit time is a fixed function of the tuning values; minimum at
     p2_leaf_min_per_sm=64, merkle_tail=128, everything else at its default."""
-    DEFAULTS = {"p2_leaf_min_per_sm": 128, "p2_node_min_per_sm": 512, "merkle_tail": 32, "merkle_subtree": 16,
-                "inject_block": 32, "leaf_block": 128}
+    DEFAULTS = {"p2_leaf_min_per_sm": 128, "p2_node_min_per_sm": 512, "p2_inject_min_per_sm": 128,
+                "merkle_tail": 32, "merkle_subtree": 16, "inject_block": 32, "leaf_block": 128, "lde_split": 1,
+                "lde_fwd_threads": 512}
 
     def __init__(self):
         self.t = dict(self.DEFAULTS)
@@ -42,7 +43,10 @@ class FakeContext:
     def profile_report(self):
         cost = 1.0 + abs(self.t["p2_leaf_min_per_sm"] - 64) / 100 + abs(self.t["merkle_tail"] - 128) / 100
         cost += 0.5 * (self.t["inject_block"] != 32) + 0.5 * (self.t["leaf_block"] != 128)
-        return {"hash_leaves": {"ms": cost, "launches": 1, "bytes": 0, "perms": 0}}
+        # the NTT: the split LDE with 1024-thread coset blocks is fastest here
+        lde = 1.0 if self.t["lde_split"] == 0 else 0.6 + 0.1 * (self.t["lde_fwd_threads"] != 1024)
+        return {"hash_leaves": {"ms": cost, "launches": 1, "bytes": 0, "perms": 0},
+                "lde": {"ms": lde, "launches": 1, "bytes": 0, "perms": 0}}
 
 
 def test_coordinate_descent_and_cache(tmp_path, monkeypatch):
@@ -53,6 +57,7 @@ def test_coordinate_descent_and_cache(tmp_path, monkeypatch):
     assert res["source"] == "measured"
     assert res["params"]["p2_leaf_min_per_sm"] == 64 and res["params"]["merkle_tail"] == 128
     assert res["params"]["inject_block"] == 32 and res["params"]["leaf_block"] == 128
+    assert res["params"]["lde_split"] == 1 and res["params"]["lde_fwd_threads"] == 1024
     assert res["ms_tuned"] < res["ms_default"]
     saved = json.load(open(tmp_path / "t.json"))
     assert saved["fake-gpu|sm148|build"]["params"] == res["params"]
@@ -72,3 +77,7 @@ def test_candidates_are_valid_library_values():
                 assert v == 0 or (2 <= v <= 1024 and v & (v - 1) == 0)
             if name in ("inject_block", "leaf_block"):
                 assert 32 <= v <= 1024
+            if name == "lde_split":
+                assert v in (0, 1)
+            if name == "lde_fwd_threads":
+                assert v in (256, 512, 1024)

@@ -59,14 +59,16 @@ def test_reference_arm_line_contract():
     """`bench.py --impl reference` times the CPU restatement on the host cores
     and prints the same metric, unit and config as the GPU arm, with the
     reference-arm keys (impl, cpu_baseline, e2e with no host<->device bytes)."""
-    args = ["--impl", "reference", "--steps", "1", "--warmup", "1", "--instances", "2", "--log-n", "8",
-            "--cpu-sample", "1", "--queries", "8"]
+    args = ["--impl", "reference", "--steps", "2", "--warmup", "1", "--instances", "2", "--log-n", "8",
+            "--queries", "8"]
     (line,) = _run_bench(args)
     assert line["impl"] == "reference" and line["unit"] == "ms" and line["higher_is_better"] is False
     assert line["value"] > 0 and line["value"] == line["ms_per_step"] == line["e2e"]["value"]
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
     base = line["cpu_baseline"]
-    assert base["kind"] == "port" and base["cores"] >= 1 and "1 of 2 instances" in base["sample"]
+    # each step proves the whole workload (no sample scaled up)
+    assert base["kind"] == "port" and base["cores"] >= 1 and "whole workload (2 instances" in base["sample"]
+    assert len(base["steps_ms"]) == 2 and line["value"] == base["value"]
     assert line["config"]["instances"] == 2 and line["config"]["log_rows"] == 8
     # under torchrun only rank 0 runs and prints; the other ranks exit 0 without work
     assert _run_bench(args, {"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"}) == []

@@ -218,6 +218,32 @@ def test_mixed_lookup_full_size_properties(ctx):
     oracle.verify(compiled.words, a, 32, compiled.logup_buses)
 
 
+def test_mixed_lookup_full_size_equals_oracle_digest(ctx):
+    """The batched form at full size against the oracle, byte for byte: 40
+    modules with log2 rows 10-20 drawn with seed 0xC4, plonk gates, a copy
+    constraint and a range lookup, 200 queries.  The oracle's proof (several
+    minutes on the CPU) is recorded as its length and SHA-256 by
+    tests/golden/make_c4_digest.py; batched and plain GPU proofs must hash
+    to the same."""
+    import hashlib
+    import json
+    import os
+    fx = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "c4_mixed_lookup_digest.json")))
+    sizes = plonk.mixed_sizes(40, 10, 20, fx["seed"])
+    assert sizes == fx["log_sizes"]
+    compiled, wit = plonk.build_mixed(sizes, seed=fx["seed"])
+    assert hashlib.sha256(compiled.words.astype("<u4").tobytes()).hexdigest() == fx["program_sha256"]
+    mont = [F.to_mont(w) for w in wit]
+    for batched in (True, False):
+        ctx.set_batched(batched)
+        try:
+            got = ctx.prove(compiled.words, mont, fx["queries"])
+        finally:
+            ctx.set_batched(True)
+        assert len(got) == fx["proof_len"], batched
+        assert hashlib.sha256(got).hexdigest() == fx["proof_sha256"], batched
+
+
 @pytest.mark.parametrize("permuted", [True, False])
 @pytest.mark.parametrize("logn", [6, 12])
 def test_prove_running_ratio_equals_oracle(ctx, logn, permuted):

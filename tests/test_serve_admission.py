@@ -101,3 +101,74 @@ def test_close_waits_for_requests_in_flight():
         mine = [e for e, i in events if i == ctx_id]
         assert mine == ["proved", "closed"]
     assert len(srv.finished) == 2 and srv.queue == [rs[2]]  # the third was never admitted
+
+
+class DeviceModel:
+    """A fake device for the admission tests: bytes in use, and a total."""
+
+    def __init__(self, total):
+        self.total, self.used = total, 0
+        self.lock = threading.Lock()
+
+    def available(self):
+        with self.lock:
+            return self.total - self.used
+
+
+def test_waits_for_live_memory_and_learns_the_measured_need():
+    """Admission reads the device's allocatable bytes when it decides: a
+    request whose measured need does not fit next to a running prove waits
+    for that prove to free its memory, then starts; the need it learns is the
+    peak each prove took (the contexts' high-water marks)."""
+    dev = DeviceModel(total=1000)
+    starts, ends = {}, {}
+
+    class MemContext(FakeContext):
+        def __init__(self, device):
+            super().__init__(device)
+            self.held = self.peak_mark = 0
+
+        def mem_usage(self, reset_peak=False):
+            if reset_peak:
+                self.peak_mark = self.held
+            return self.held, self.peak_mark
+
+        def device_available(self):
+            return dev.available()
+
+        def prove(self, words, witness, q):
+            rid = int(words[0])
+            starts[rid] = time.perf_counter()
+            with dev.lock:
+                dev.used += 600  # each prove takes 600 of the 1000 bytes at its peak
+                self.held += 600
+                self.peak_mark = max(self.peak_mark, self.held)
+            time.sleep(0.05)
+            with dev.lock:
+                dev.used -= 600
+                self.held -= 600
+            ends[rid] = time.perf_counter()
+            return b"p"
+
+    rs = [S.Request(i, np.array([i], np.uint32), [], 1, 16) for i in range(3)]
+    srv = S.Server(streams=3, hbm_budget=None, context_factory=MemContext, margin=0)
+    srv.measured[rs[0].shape()] = 600  # as a warm-up would have measured
+    srv.measured[rs[1].shape()] = 600
+    srv.measured[rs[2].shape()] = 600
+    for r in rs:
+        srv.submit(r)
+    srv.wait(3, timeout=10)
+    srv.close()
+    # three free streams, yet the memory admits one prove at a time
+    assert starts[1] >= ends[0] and starts[2] >= ends[1]
+    assert srv.waits_for_memory >= 2
+    assert all(r.peak_bytes == 600 for r in srv.finished)
+    # a shape seen for the first time starts from the per-row prior, then
+    # runs on what it measured
+    srv2 = S.Server(streams=1, context_factory=MemContext, margin=0)
+    r = S.Request(9, np.array([9], np.uint32), [], 1, 1 << 12)
+    assert srv2.need(r) == S.device_bytes_estimate(1 << 12)
+    srv2.submit(r)
+    srv2.wait(1, timeout=10)
+    srv2.close()
+    assert srv2.need(r) == 600
