@@ -65,13 +65,16 @@ inline void check_ntt_size(int logn) {
 inline void big_ntt(Ctx& c, std::vector<BigNtt> jobs, int logn, bool inverse, const char* tag, double bytes_per_job) {
   if (jobs.empty()) return;
   const int logr = logn / 2, logc = logn - logr;
+  if (logr < 7 || logc > 11) throw Error(LG_ERR_UNSUPPORTED, "four-step transform size out of range");
   const size_t n = (size_t)1 << logn;
   const uint32_t* tw_n = c.twiddles(logn);
   const uint32_t* tw_c = c.twiddles(logc);
   const uint32_t* tw_r = c.twiddles(logr);
+  // scratch chunks of 2^26 words at most (256 MiB)
   const size_t per = std::max<size_t>(1, ((size_t)1 << 26) / n);
-  allow_smem(k_big_pass_a, ((size_t)BIG_TILE << logc) * 4);
-  allow_smem(k_big_pass_b, ((size_t)BIG_TILE << logr) * 4);
+  const size_t smem_a = tile_words(logc) * 4, smem_b = tile_words(logr) * 4;
+  const unsigned thr_a = (unsigned)std::min<size_t>(512, (size_t)1 << logc);
+  const unsigned thr_b = (unsigned)std::min<size_t>(512, (size_t)1 << logr);
   for (size_t first = 0; first < jobs.size(); first += per) {
     size_t cnt = std::min(per, jobs.size() - first);
     auto scratch = std::make_shared<DBuf>(cnt * n, c.stream);
@@ -79,12 +82,20 @@ inline void big_ntt(Ctx& c, std::vector<BigNtt> jobs, int logn, bool inverse, co
     for (size_t i = 0; i < cnt; i++) v[i].scratch = scratch->p + i * n;
     auto jd = upload_vec(c, v);
     c.timed(tag, bytes_per_job * cnt, 0, [&] {
-      k_big_pass_a<<<dim3((1u << logr) / BIG_TILE, (unsigned)cnt), 512, ((size_t)BIG_TILE << logc) * 4, c.stream>>>(
-          (const BigNtt*)jd->p, logn, logr, logc, inverse ? 1 : 0, tw_n, tw_c);
-      LG_LAUNCH();
-      k_big_pass_b<<<dim3((1u << logc) / BIG_TILE, (unsigned)cnt), 512, ((size_t)BIG_TILE << logr) * 4, c.stream>>>(
-          (const BigNtt*)jd->p, logr, logc, inverse ? 1 : 0, tw_r);
-      LG_LAUNCH();
+      with_tile_size(logc, [&](auto LC) {
+        constexpr int C_ = decltype(LC)::value;
+        allow_smem(k_big_pass_a<C_>, smem_a);
+        k_big_pass_a<C_><<<dim3((1u << logr) / BIG_TILE, (unsigned)cnt), thr_a, smem_a, c.stream>>>(
+            (const BigNtt*)jd->p, logn, logr, inverse ? 1 : 0, tw_n, tw_c);
+        LG_LAUNCH();
+      });
+      with_tile_size(logr, [&](auto LR) {
+        constexpr int R_ = decltype(LR)::value;
+        allow_smem(k_big_pass_b<R_>, smem_b);
+        k_big_pass_b<R_><<<dim3((1u << logc) / BIG_TILE, (unsigned)cnt), thr_b, smem_b, c.stream>>>(
+            (const BigNtt*)jd->p, logc, inverse ? 1 : 0, tw_r);
+        LG_LAUNCH();
+      });
     });
   }
 }
@@ -167,18 +178,24 @@ inline void launch_lde(Ctx& c, const std::vector<LdeLane>& lanes, uint32_t log_n
       if (L.coef) LG_CK(cudaMemcpyAsync(L.coef, L.src, n * 4, cudaMemcpyDeviceToDevice, c.stream));
   with_ntt_size((int)log_n, [&](auto L) {
     constexpr int LG = decltype(L)::value;
+    const size_t fsmem = pad16_words((int)log_n) * 4;
+    const unsigned thr = (unsigned)std::min<int>(ntt_threads((int)log_n), (int)c.tune.lde_fwd_threads);
     if (!from_coeffs) {
-      allow_smem(k_lde<LG>, smem);
-      c.timed("lde_inv", 8.0 * n * lv.size(), 0, [&] {
-        k_lde<LG><<<(unsigned)lv.size(), ntt_threads((int)log_n), smem, c.stream>>>(
-            (const LdeLane*)tab->p, (int)log_n, 0, twn, tw4, inv(to_mont((uint32_t)n)), 0);
-        LG_LAUNCH();
-      });
+      auto go_inv = [&](auto kern) {
+        allow_smem(kern, fsmem);
+        c.timed("lde_inv", 8.0 * n * lv.size(), 0, [&] {
+          kern<<<(unsigned)lv.size(), thr, fsmem, c.stream>>>((const LdeLane*)tab->p, twn, inv(to_mont((uint32_t)n)));
+          LG_LAUNCH();
+        });
+      };
+      if constexpr (LG >= 4) {
+        if (thr <= 256) go_inv(k_lde_inv<LG, 256>);
+        else if (thr <= 512) go_inv(k_lde_inv<LG, 512>);
+        else go_inv(k_lde_inv<LG, 1024>);
+      }
     }
     const int first = from_coeffs ? 0 : 1;
     const dim3 grid((unsigned)lv.size(), (unsigned)((1 << RATE_LOG) - first));
-    const size_t fsmem = pad16_words((int)log_n) * 4;
-    const unsigned thr = (unsigned)std::min<int>(ntt_threads((int)log_n), (int)c.tune.lde_fwd_threads);
     auto go = [&](auto kern) {
       allow_smem(kern, fsmem);
       c.timed("lde", bytes - (from_coeffs ? 0.0 : 8.0 * n * lv.size()), 0, [&] {

@@ -219,6 +219,33 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT)
   ntt16<true>(sm, LOGN, tw_n, false, first_pass, store);
 }
 
+// The inverse transform of the split LDE, one lane per block with a single
+// shared-memory array: the first pass gathers its bit-reversed inputs from
+// global memory (the lane's few tens of KB stay in L1 while the block reads
+// them), writes coset 0 (the input in bit-reversed order) from those
+// registers, and the last pass writes the coefficients to global memory,
+// where k_lde_fwd reads them.
+template <int LOGN, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1024 / MAXT)
+    k_lde_inv(const LdeLane* lanes, const uint32_t* tw_n, uint32_t n_inv) {
+  static_assert(LOGN >= 4, "radix-16 passes");
+  extern __shared__ uint32_t sm[];
+  const LdeLane L = lanes[blockIdx.x];
+  auto first = [&](uint32_t t, uint32_t r, int lo) { return __ldg(L.src + bitrev32(grp_index(t, r, lo), LOGN)); };
+  auto coset0 = [&](uint32_t t, const uint32_t* v) {
+    uint4* q = reinterpret_cast<uint4*>(L.out + ((uint64_t)t << 4));
+    q[0] = make_uint4(v[0], v[1], v[2], v[3]);
+    q[1] = make_uint4(v[4], v[5], v[6], v[7]);
+    q[2] = make_uint4(v[8], v[9], v[10], v[11]);
+    q[3] = make_uint4(v[12], v[13], v[14], v[15]);
+  };
+  auto store = [&](uint32_t t, int lo, const uint32_t* v) {
+#pragma unroll
+    for (uint32_t r = 0; r < 16; r++) L.coef[grp_index(t, r, lo)] = mul(v[r], n_inv);
+  };
+  ntt16<false>(sm, LOGN, tw_n, true, first, store, coset0);
+}
+
 // Evaluations of a coefficient lane on the cosets s_c <w_n>, s_c = g w_4n^c,
 // c = blockIdx.y < 4, in natural order: out[c n + j] = P(s_c w_n^j).
 // n >= 16: the scaled coefficients coef[k] s_c^k (shift: the table of s_c^k,

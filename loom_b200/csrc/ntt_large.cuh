@@ -2,13 +2,20 @@
 // buffer.  With n = R C (R = 2^floor(log n / 2), C = 2^ceil(log n / 2)),
 // k = k1 + R k2 and j = C j1 + j2:
 //   X[C j1 + j2] = sum_k1 w_R^(j1 k1) w_n^(j2 k1) sum_k2 w_C^(j2 k2) x[k1 + R k2].
-// Pass A: for a tile of TILE consecutive k1, the length-C transforms over k2
-// (rows of the input are contiguous in k1), times w_n^(j2 k1), into
-// scratch[j2 R + k1].  Pass B: for a tile of TILE consecutive j2, the
-// length-R transforms over k1, stored in natural order (X[j]) or in
-// bit-reversed order (out[bitrev(j)], what reedsolomon.Encode produces).
-// Input scaling x[k] * c0 * t1[k] * t2[(e k) mod m2] covers 1/n and the
-// coset shifts.  All sub-transforms run in shared memory.
+// Pass A: for a tile of 16 consecutive k1, the length-C transforms over k2
+// (the tile's 16 columns are read 64 bytes at a time), times w_n^(j2 k1), into
+// scratch[j2 R + k1].  Pass B: for a tile of 16 consecutive j2, the length-R
+// transforms over k1 (scratch rows, contiguous), stored in natural order
+// (X[j]) or in bit-reversed order (out[bitrev(j)], what reedsolomon.Encode
+// produces).  Input scaling x[k] * c0 * t1[k] * t2[(e k) mod m2] covers 1/n
+// and the coset shifts.
+//
+// The 16 sub-transforms of a tile run together in shared memory with the
+// radix-16 register passes of ntt16.cuh (16 elements of one column per thread,
+// four stages per shared-memory round trip), the columns interleaved: element
+// (row, col) at 16 (row + row / 16) + (col ^ (row mod 16)).  The row padding
+// keeps the two half-warps of a pass in different banks, the column swizzle
+// keeps the row-wise staging of pass B conflict-free.
 #pragma once
 #include "kernels.cuh"
 
@@ -27,73 +34,110 @@ struct BigNtt {
   int out_bitrev;
 };
 
-// Radix-2 DIF over `len` = 2^lg rows of a [len][TILE] shared array (all TILE
-// columns at once); position p ends up holding output index bitrev(p).
-__device__ void smem_dif_cols(uint32_t* S, int lg, const uint32_t* tw_len, bool inverse) {
-  const uint32_t len = 1u << lg, mask = len - 1;
-  for (int s = lg; s >= 1; s--) {
-    const uint32_t half = 1u << (s - 1);
-    for (uint32_t b = threadIdx.x; b < (len / 2) * BIG_TILE; b += blockDim.x) {
-      uint32_t kl = b % BIG_TILE, p = b / BIG_TILE;
-      uint32_t jj = p & (half - 1);
-      uint32_t i0 = ((p >> (s - 1)) << s) | jj, i1 = i0 + half;
-      uint32_t w = tw_at(tw_len, jj << (lg - s), mask, inverse);
-      uint32_t u = S[i0 * BIG_TILE + kl], v = S[i1 * BIG_TILE + kl];
-      S[i0 * BIG_TILE + kl] = add(u, v);
-      S[i1 * BIG_TILE + kl] = mul(sub(u, v), w);
+__device__ __forceinline__ uint32_t tile_addr(uint32_t row, uint32_t col) {
+  return ((row + (row >> 4)) << 4) + (col ^ (row & 15u));
+}
+// words of one tile of 16 columns of 2^logl rows
+__host__ __device__ constexpr size_t tile_words(int logl) {
+  return (((size_t)1 << logl) + ((size_t)1 << logl) / 16) * 16;
+}
+
+// The 16 column transforms of a tile, 2^LOGL rows each.  Pass 0 takes its
+// inputs from first(col, row) (global memory, or the staged tile), every pass
+// but the last writes back to S, the last hands each element to
+// store(col, row, value).  DIF: natural rows in, bit-reversed rows out.
+template <bool DIF, int LOGL, class First, class Store>
+__device__ __forceinline__ void ntt16_tile(uint32_t* S, const uint32_t* tw, bool inverse, First first, Store store) {
+  constexpr uint32_t groups = (1u << LOGL) >> 4;  // per column
+  constexpr int np = (LOGL - ((LOGL & 3) ? (LOGL & 3) : 4)) / 4 + 1;
+#pragma unroll
+  for (int p = 0; p < np; p++) {
+    int lo, s_lo, s_hi;
+    pass_plan<DIF>(p, LOGL, lo, s_lo, s_hi);
+    for (uint32_t u = threadIdx.x; u < groups * BIG_TILE; u += blockDim.x) {
+      const uint32_t col = u & (BIG_TILE - 1), t = u >> 4;
+      uint32_t v[16];
+#pragma unroll
+      for (uint32_t r = 0; r < 16; r++) {
+        const uint32_t row = grp_index(t, r, lo);
+        v[r] = p == 0 ? first(col, row) : S[tile_addr(row, col)];
+      }
+      pass16<DIF>(v, t, lo, s_lo, s_hi, LOGL, tw, inverse);
+#pragma unroll
+      for (uint32_t r = 0; r < 16; r++) {
+        const uint32_t row = grp_index(t, r, lo);
+        if (p == np - 1) store(col, row, v[r]);
+        else S[tile_addr(row, col)] = v[r];
+      }
     }
     __syncthreads();
   }
 }
 
-// tw_n / tw_c / tw_r: tables of w_n^j, w_C^j, w_R^j.
-__global__ void k_big_pass_a(const BigNtt* jobs, int logn, int logr, int logc, int inverse, const uint32_t* tw_n,
-                             const uint32_t* tw_c) {
+// tw_n / tw_c: tables of w_n^j, w_C^j.  Block (x, y): tile x of job y.
+template <int LOGC>
+__global__ void __launch_bounds__(512) k_big_pass_a(const BigNtt* jobs, int logn, int logr, int inverse,
+                                                    const uint32_t* tw_n, const uint32_t* tw_c) {
   extern __shared__ uint32_t S[];
   const BigNtt J = jobs[blockIdx.y];
-  const uint32_t R = 1u << logr, C = 1u << logc, n = 1u << logn;
+  const uint32_t R = 1u << logr, n = 1u << logn;
   const uint32_t k1_0 = blockIdx.x * BIG_TILE;
-  for (uint32_t idx = threadIdx.x; idx < C * BIG_TILE; idx += blockDim.x) {
-    uint32_t k2 = idx / BIG_TILE, kl = idx % BIG_TILE;
-    uint32_t k = (k1_0 + kl) + R * k2;
+  auto first = [&](uint32_t col, uint32_t k2) {
+    const uint32_t k = (k1_0 + col) + R * k2;
     uint32_t v = J.in[k];
     if (J.c0 != MONT_ONE) v = mul(v, J.c0);
     if (J.t1) v = mul(v, __ldg(J.t1 + k));
     if (J.t2) v = mul(v, __ldg(J.t2 + ((J.e2 * k) & J.m2_mask)));
-    S[k2 * BIG_TILE + kl] = v;
+    return v;
+  };
+  auto store = [&](uint32_t col, uint32_t p, uint32_t v) {
+    const uint32_t j2 = bitrev32(p, LOGC), k1 = k1_0 + col;
+    const uint32_t e = (uint32_t)(((uint64_t)j2 * k1) & (n - 1));
+    J.scratch[(uint64_t)j2 * R + k1] = mul(v, tw_at(tw_n, e, n - 1, inverse != 0));
+  };
+  ntt16_tile<true, LOGC>(S, tw_c, inverse != 0, first, store);
+}
+
+// Block (x, y): rows [16 x, 16 x + 16) of job y's scratch.
+template <int LOGR>
+__global__ void __launch_bounds__(512) k_big_pass_b(const BigNtt* jobs, int logc, int inverse,
+                                                    const uint32_t* tw_r) {
+  extern __shared__ uint32_t S[];
+  const BigNtt J = jobs[blockIdx.y];
+  constexpr uint32_t R = 1u << LOGR;
+  const uint32_t C = 1u << logc;
+  const uint32_t j2_0 = blockIdx.x * BIG_TILE;
+  // stage the 16 scratch rows (contiguous, coalesced) into the tile
+  for (uint32_t idx = threadIdx.x; idx < R * BIG_TILE; idx += blockDim.x) {
+    const uint32_t jl = idx / R, k1 = idx % R;
+    S[tile_addr(k1, jl)] = J.scratch[(uint64_t)(j2_0 + jl) * R + k1];
   }
   __syncthreads();
-  smem_dif_cols(S, logc, tw_c, inverse != 0);
-  for (uint32_t idx = threadIdx.x; idx < C * BIG_TILE; idx += blockDim.x) {
-    uint32_t p = idx / BIG_TILE, kl = idx % BIG_TILE;
-    uint32_t j2 = bitrev32(p, logc), k1 = k1_0 + kl;
-    uint32_t e = (uint32_t)(((uint64_t)j2 * k1) & (n - 1));
-    J.scratch[(uint64_t)j2 * R + k1] = mul(S[p * BIG_TILE + kl], tw_at(tw_n, e, n - 1, inverse != 0));
+  auto first = [&](uint32_t col, uint32_t k1) { return S[tile_addr(k1, col)]; };
+  if (J.out_bitrev) {
+    // out[bitrev_C(j2) R + q] = X[C bitrev_R(q) + j2]: position q holds j1 = bitrev_R(q)
+    auto store = [&](uint32_t col, uint32_t q, uint32_t v) {
+      J.out[(uint64_t)bitrev32(j2_0 + col, logc) * R + q] = v;
+    };
+    ntt16_tile<true, LOGR>(S, tw_r, inverse != 0, first, store);
+  } else {
+    auto store = [&](uint32_t col, uint32_t q, uint32_t v) {
+      J.out[(uint64_t)C * bitrev32(q, LOGR) + j2_0 + col] = v;
+    };
+    ntt16_tile<true, LOGR>(S, tw_r, inverse != 0, first, store);
   }
 }
 
-__global__ void k_big_pass_b(const BigNtt* jobs, int logr, int logc, int inverse, const uint32_t* tw_r) {
-  extern __shared__ uint32_t S[];
-  const BigNtt J = jobs[blockIdx.y];
-  const uint32_t R = 1u << logr, C = 1u << logc;
-  const uint32_t j2_0 = blockIdx.x * BIG_TILE;
-  for (uint32_t idx = threadIdx.x; idx < R * BIG_TILE; idx += blockDim.x) {
-    uint32_t jl = idx / R, k1 = idx % R;
-    S[k1 * BIG_TILE + jl] = J.scratch[(uint64_t)(j2_0 + jl) * R + k1];
-  }
-  __syncthreads();
-  smem_dif_cols(S, logr, tw_r, inverse != 0);
-  if (J.out_bitrev) {
-    // out[bitrev_C(j2) R + bitrev_R(j1)] = X[C j1 + j2], and position q holds j1 = bitrev_R(q)
-    for (uint32_t idx = threadIdx.x; idx < R * BIG_TILE; idx += blockDim.x) {
-      uint32_t jl = idx / R, q = idx % R;
-      J.out[(uint64_t)bitrev32(j2_0 + jl, logc) * R + q] = S[q * BIG_TILE + jl];
-    }
-  } else {
-    for (uint32_t idx = threadIdx.x; idx < R * BIG_TILE; idx += blockDim.x) {
-      uint32_t q = idx / BIG_TILE, jl = idx % BIG_TILE;
-      J.out[(uint64_t)C * bitrev32(q, logr) + j2_0 + jl] = S[q * BIG_TILE + jl];
-    }
+// Calls f(std::integral_constant<int, L>{}) for the sub-transform sizes of
+// the four-step path, 2^7 .. 2^11 rows.
+template <class F> inline void with_tile_size(int logl, F&& f) {
+  switch (logl) {
+    case 7: f(std::integral_constant<int, 7>{}); break;
+    case 8: f(std::integral_constant<int, 8>{}); break;
+    case 9: f(std::integral_constant<int, 9>{}); break;
+    case 10: f(std::integral_constant<int, 10>{}); break;
+    case 11: f(std::integral_constant<int, 11>{}); break;
+    default: break;
   }
 }
 

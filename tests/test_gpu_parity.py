@@ -400,12 +400,34 @@ def test_grand_product(ctx, n):
     assert np.array_equal(ctx.grand_product(num, den), oracle.grand_product(num, den))
 
 
-@pytest.mark.parametrize("logn,cols", [(15, 3), (16, 2), (17, 1), (20, 1)])
+@pytest.mark.parametrize("logn,cols", [(15, 3), (16, 2), (17, 1), (18, 1), (20, 1), (21, 1), (22, 1)])
 def test_rs_encode_large(ctx, logn, cols):
     c = F.to_mont(rnd((cols, 1 << logn), 300 + logn))
     got = ctx.rs_encode(c)
     for i in range(cols):
         assert np.array_equal(got[i], oracle.rs_encode(c[i], 4 << logn)), (logn, i)
+
+
+def test_lde_launch_shapes_give_identical_results(ctx):
+    """The LDE's launch structure is a tuning choice: fused (one block per
+    lane) or split (inverse launch, then one block per lane and coset, with
+    256, 512 or 1024 threads); outputs and proofs must not depend on it."""
+    cols = F.to_mont(rnd((5, 1 << 14), 77))
+    want = [oracle.rs_encode(cols[i], 4 << 14) for i in range(5)]
+    compiled, wit = plonk.build(3, 1 << 12, seed=9)
+    mont = [F.to_mont(w) for w in wit]
+    base = ctx.prove(compiled.words, mont, 16)
+    saved = {k: ctx.get_tuning(k) for k in ("lde_split", "lde_fwd_threads")}
+    try:
+        for split, thr in ((0, 512), (1, 256), (1, 512), (1, 1024)):
+            ctx.set_tuning("lde_split", split)
+            ctx.set_tuning("lde_fwd_threads", thr)
+            got = ctx.rs_encode(cols)
+            assert all(np.array_equal(got[i], want[i]) for i in range(5)), (split, thr)
+            assert ctx.prove(compiled.words, mont, 16) == base, (split, thr)
+    finally:
+        ctx.apply_tuning(saved)
+    assert base == oracle.prove(compiled.words, mont, 16)
 
 
 def test_commit_root_large_and_small(ctx):
