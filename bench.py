@@ -44,9 +44,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sweep", action="store_true",
                     help="kernel roofline sweep (LDE, Merkle commit, FRI fold, DEEP) instead of the prove bench")
-    ap.add_argument("--serve-requests", type=int, default=48, help="requests in the serving measurement (0 = skip)")
+    ap.add_argument("--serve-requests", type=int, default=2000, help="requests in the serving measurement (0 = skip)")
     ap.add_argument("--serve-shapes", type=int, default=8, help="distinct request shapes, replayed in turn")
-    ap.add_argument("--serve-rate", type=str, default="8,16", help="Poisson arrival rates (requests/s) to sweep")
+    ap.add_argument("--serve-rate", type=str, default="32,64", help="Poisson arrival rates (requests/s) to sweep")
     ap.add_argument("--serve-streams", type=int, default=4)
     ap.add_argument("--no-c4", action="store_true",
                     help="skip the mixed-size lookup workload (40 modules, log2 rows 10-20, range lookup)")
@@ -555,7 +555,9 @@ def main():
             sweeps.append({"rate_per_s": rate, "requests": res["requests"], "p50_ms": round(res["p50_ms"], 2),
                            "p99_ms": round(res["p99_ms"], 2), "proofs_per_s": round(res["proofs_per_s"], 2),
                            "errors": res["errors"], "first_error": res["first_error"],
-                           "proofs_identical_to_alone": same})
+                           "proofs_identical_to_alone": same,
+                           "measured_need_mb": [round(x / 2**20, 1) for x in res["measured_need_bytes"]],
+                           "admissions_deferred_for_memory": res["admissions_deferred_for_memory"]})
         serve_res = {"shapes": [{"log_rows": lg, "instances": ins} for lg, ins in shapes],
                      "streams": a.serve_streams, "queries": a.queries,
                      "sequential_plain_proofs_per_s": round(len(plain_one) * 1e3 / sum(plain_one), 2),

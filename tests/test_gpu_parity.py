@@ -350,20 +350,23 @@ def test_tuning_never_changes_proofs(ctx):
     ref = ctx.prove(compiled.words, mont, 16)
     try:
         for params in ({"merkle_tail": 2, "merkle_subtree": 2, "p2_leaf_min_per_sm": 0, "p2_node_min_per_sm": 0,
-                        "inject_block": 1024, "leaf_block": 32},
+                        "p2_inject_min_per_sm": 0, "inject_block": 1024, "leaf_block": 32, "lde_split": 0,
+                        "lde_fwd_threads": 256},
                        {"merkle_tail": 1024, "merkle_subtree": 1024, "p2_leaf_min_per_sm": 1 << 20,
-                        "p2_node_min_per_sm": 1 << 20, "inject_block": 32, "leaf_block": 1024},
+                        "p2_node_min_per_sm": 1 << 20, "p2_inject_min_per_sm": 1 << 20, "inject_block": 32,
+                        "leaf_block": 1024, "lde_split": 1, "lde_fwd_threads": 1024},
                        {"merkle_tail": 64, "merkle_subtree": 0, "p2_leaf_min_per_sm": 128,
                         "p2_node_min_per_sm": 512, "inject_block": 32, "leaf_block": 128},
                        {"merkle_tail": 4, "merkle_subtree": 8, "p2_leaf_min_per_sm": 128,
                         "p2_node_min_per_sm": 512, "inject_block": 32, "leaf_block": 128}):
             ctx.apply_tuning(params)
-            assert ctx.tuning() == params
+            got = ctx.tuning()
+            assert {k: got[k] for k in params} == params
             assert ctx.prove(compiled.words, mont, 16) == ref
     finally:
         ctx.apply_tuning(defaults)
     for name, value in (("merkle_tail", 48), ("merkle_tail", 2048), ("merkle_subtree", 1), ("merkle_subtree", 48),
-                        ("leaf_block", 16), ("no_such", 1)):
+                        ("leaf_block", 16), ("lde_split", 2), ("lde_fwd_threads", 128), ("no_such", 1)):
         with pytest.raises(LoomError) as e:
             ctx.set_tuning(name, value)
         assert e.value.code == 1
