@@ -68,8 +68,8 @@ inline void big_ntt(Ctx& c, std::vector<BigNtt> jobs, int logn, bool inverse, co
   if (logr < 7 || logc > 11) throw Error(LG_ERR_UNSUPPORTED, "four-step transform size out of range");
   const size_t n = (size_t)1 << logn;
   const uint32_t* tw_n = c.twiddles(logn);
-  const uint32_t* tw_c = c.twiddles(logc);
-  const uint32_t* tw_r = c.twiddles(logr);
+  const uint32_t* tw_c = c.twiddles16(logc);
+  const uint32_t* tw_r = c.twiddles16(logr);
   // scratch chunks of 2^26 words at most (256 MiB)
   const size_t per = std::max<size_t>(1, ((size_t)1 << 26) / n);
   const size_t smem_a = tile_words(logc) * 4, smem_b = tile_words(logr) * 4;
@@ -146,7 +146,7 @@ inline void launch_lde(Ctx& c, const std::vector<LdeLane>& lanes, uint32_t log_n
     big_ntt(c, fwd_jobs, (int)log_n, false, "lde", 20.0 * n / (1 << RATE_LOG));
     return;
   }
-  const uint32_t* twn = c.twiddles((int)log_n);
+  const uint32_t* twn = c.ntt_twiddles((int)log_n);
   const uint32_t* tw4 = c.twiddles((int)log_n + RATE_LOG);
   const size_t smem = 2 * pad16_words((int)log_n) * 4;
   const double bytes = 20.0 * n * lanes.size();

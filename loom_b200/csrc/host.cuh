@@ -206,6 +206,7 @@ struct Ctx {
   DevArena dev_arena;            // prove-scoped small device buffers
   MemAcct mem;                   // device bytes this context holds (lg_ctx_mem_usage)
   std::map<int, DBufP> tw;       // log n -> w_n^j, j < n
+  std::map<int, DBufP> tw16;     // log n -> the radix-16 passes' twiddle tables (tw16 layout, ntt16.cuh)
   std::map<int, DBufP> gpow;     // log n -> g^k, k < n
   std::map<int, DBufP> ginvpow;  // log n -> g^-k, k < n
   std::map<int, DBufP> cshift;   // log n -> (g w_4n^c)^k, k < n, for c = 0..3 (4 tables back to back)
@@ -268,6 +269,43 @@ struct Ctx {
     tw[logn] = b;
     return b->p;
   }
+  // Twiddles of the radix-16 passes for 2^logn points (4 <= logn), pass by
+  // pass in the tw16 layout of ntt16.cuh; built on the host once per size.
+  const uint32_t* twiddles16(int logn) {
+    auto it = tw16.find(logn);
+    if (it != tw16.end()) return it->second->p;
+    const uint32_t n = 1u << logn;
+    std::vector<uint32_t> pw(n);
+    const uint32_t w = root_of_unity_mont(logn);
+    pw[0] = MONT_ONE;
+    for (uint32_t k = 1; k < n; k++) pw[k] = mul(pw[k - 1], w);
+    std::vector<uint32_t> tab(tw16_words(logn), 0);
+    for (int dif = 0; dif < 2; dif++)
+      for (int invd = 0; invd < 2; invd++)
+        for (int p = 0; p < pass_count(logn); p++) {
+          int lo = 0, s_lo = 0, s_hi = 0;
+          if (dif) pass_plan<true>(p, logn, lo, s_lo, s_hi);
+          else pass_plan<false>(p, logn, lo, s_lo, s_hi);
+          const uint32_t base = tw16_pass_offset(logn, dif != 0, invd != 0, p);
+          for (int st = s_lo; st <= s_hi; st++) {
+            const uint32_t m = 1u << (st - lo), off = base + tw16_stage_offset(s_lo, st);
+            for (uint32_t tl = 0; tl < (1u << lo); tl++)
+              for (uint32_t rl = 0; rl < m; rl++) {
+                const uint32_t e = ((tl + (rl << lo)) << (logn - st - 1)) & (n - 1);
+                tab[off + tl * m + rl] = pw[invd ? (n - e) & (n - 1) : e];
+              }
+          }
+        }
+    ArenaScope cached(nullptr);  // kept across proves: never from the arena
+    auto b = std::make_shared<DBuf>(tab.size(), stream);
+    LG_CK(cudaMemcpyAsync(b->p, tab.data(), tab.size() * 4, cudaMemcpyHostToDevice, stream));
+    LG_CK(cudaStreamSynchronize(stream));  // the host table goes out of scope
+    tw16[logn] = b;
+    return b->p;
+  }
+  // the table a transform kernel takes: tw16 for the radix-16 passes, the
+  // plain powers below 16 points (radix-2 stages)
+  const uint32_t* ntt_twiddles(int logn) { return logn >= 4 ? twiddles16(logn) : twiddles(logn); }
   const uint32_t* gpowers(int logn, bool inverse) {
     auto& m = inverse ? ginvpow : gpow;
     auto it = m.find(logn);

@@ -7,6 +7,8 @@
 // Shared memory is addressed with one pad word per 16 (pad16) so that the
 // 16-element groups of a warp fall into distinct banks in every pass.
 #pragma once
+#include <type_traits>
+
 #include "field.cuh"
 
 namespace lg {
@@ -18,67 +20,123 @@ __device__ __forceinline__ uint32_t grp_index(uint32_t t, uint32_t r, int lo) {
   return ((t >> lo) << (lo + 4)) | (r << lo) | (t & ((1u << lo) - 1));
 }
 
-__device__ __forceinline__ uint32_t twid(const uint32_t* tw, uint32_t e, uint32_t mask, bool inverse) {
-  return __ldg(tw + (inverse ? ((0u - e) & mask) : e));
+// Pass plan.  DIF: the first pass takes the top logn mod 4 stages (or 4) with
+// local bits [logn-4, logn); then four stages per pass.  DIT mirrors it from
+// the bottom.
+LG_HD constexpr int pass_count(int logn) {
+  return (logn - ((logn & 3) ? (logn & 3) : 4)) / 4 + 1;
+}
+template <bool DIF>
+LG_HD constexpr void pass_plan(int p, int logn, int& lo, int& s_lo, int& s_hi) {
+  const int rem = (logn & 3) ? (logn & 3) : 4;
+  if (DIF) {
+    if (p == 0) { lo = logn - 4; s_hi = logn - 1; s_lo = logn - rem; }
+    else { s_hi = logn - rem - 4 * (p - 1) - 1; s_lo = s_hi - 3; lo = s_lo; }
+  } else {
+    const int np = pass_count(logn);
+    if (p < np - 1) { s_lo = 4 * p; s_hi = s_lo + 3; lo = s_lo; }
+    else { s_lo = 4 * p; s_hi = logn - 1; lo = logn - 4; }
+  }
+}
+
+// Twiddle tables laid out pass by pass.  Stage s of a pass with local bits
+// [lo, lo + 4) multiplies by w_{2^(s+1)}^j, j = (t mod 2^lo) + r 2^lo for the
+// thread's group t and the register pair r < 2^(s-lo): for each t mod 2^lo
+// those 2^(s-lo) values sit next to each other, so a thread reads a stage's
+// twiddles with one or two vector loads (one table entry per (t mod 2^lo, r):
+// 2^s words per stage, each stage's block rounded up to 8 words).  Four
+// regions: DIF forward, DIF inverse, DIT forward, DIT inverse.
+LG_HD constexpr uint32_t tw16_round8(uint32_t w) { return (w + 7u) & ~7u; }
+LG_HD constexpr uint32_t tw16_pass_words(int logn, bool dif, int p) {
+  int lo = 0, s_lo = 0, s_hi = 0;
+  if (dif) pass_plan<true>(p, logn, lo, s_lo, s_hi);
+  else pass_plan<false>(p, logn, lo, s_lo, s_hi);
+  uint32_t w = 0;
+  for (int s = s_lo; s <= s_hi; s++) w += tw16_round8(1u << s);
+  return w;
+}
+LG_HD constexpr uint32_t tw16_region_words(int logn, bool dif) {
+  uint32_t w = 0;
+  for (int p = 0; p < pass_count(logn); p++) w += tw16_pass_words(logn, dif, p);
+  return w;
+}
+LG_HD constexpr uint32_t tw16_words(int logn) { return 2 * tw16_region_words(logn, true) + 2 * tw16_region_words(logn, false); }
+// offset of pass p's table
+LG_HD constexpr uint32_t tw16_pass_offset(int logn, bool dif, bool inverse, int p) {
+  uint32_t off = dif ? 0u : 2 * tw16_region_words(logn, true);
+  if (inverse) off += tw16_region_words(logn, dif);
+  for (int q = 0; q < p; q++) off += tw16_pass_words(logn, dif, q);
+  return off;
+}
+// offset of stage s's block inside its pass's table
+LG_HD constexpr uint32_t tw16_stage_offset(int s_lo, int s) {
+  uint32_t off = 0;
+  for (int q = s_lo; q < s; q++) off += tw16_round8(1u << q);
+  return off;
+}
+
+// m consecutive words from an m-aligned offset (m = 1, 2, 4, 8)
+template <int M> __device__ __forceinline__ void ld_tw(const uint32_t* p, uint32_t* w) {
+  if constexpr (M == 1) {
+    w[0] = __ldg(p);
+  } else if constexpr (M == 2) {
+    const uint2 a = __ldg(reinterpret_cast<const uint2*>(p));
+    w[0] = a.x; w[1] = a.y;
+  } else {
+    const uint4 a = __ldg(reinterpret_cast<const uint4*>(p));
+    w[0] = a.x; w[1] = a.y; w[2] = a.z; w[3] = a.w;
+    if constexpr (M == 8) {
+      const uint4 b = __ldg(reinterpret_cast<const uint4*>(p) + 1);
+      w[4] = b.x; w[5] = b.y; w[6] = b.z; w[7] = b.w;
+    }
+  }
 }
 
 // Stages s in [s_lo, s_hi] on the 16 registers of group t (local bits
 // [lo, lo+4)).  DIF: (u, v) -> (u + v, (u - v) w), stages descending;
 // DIT: (u, v) -> (u + v w, u - v w), stages ascending.  w = w_{2^(s+1)}^j,
-// j = index mod 2^s.
-template <bool DIF>
-__device__ __forceinline__ void pass16(uint32_t v[16], uint32_t t, int lo, int s_lo, int s_hi, int logn,
-                                       const uint32_t* tw, bool inverse) {
-  const uint32_t mask = (1u << logn) - 1;
+// j = index mod 2^s; `ptab`: this pass's twiddle table (tw16 layout).
+template <bool DIF, int LS>
+__device__ __forceinline__ void stage16(uint32_t v[16], uint32_t t, int lo, int s_lo, const uint32_t* ptab) {
+  constexpr uint32_t m = 1u << LS;
+  const int s = lo + LS;
+  uint32_t w[m];
+  ld_tw<m>(ptab + tw16_stage_offset(s_lo, s) + (t & ((1u << lo) - 1)) * m, w);
 #pragma unroll
-  for (int k = 0; k < 4; k++) {
-    const int ls = DIF ? 3 - k : k;  // local bit of this stage
-    const int s = lo + ls;
-    if (s < s_lo || s > s_hi) continue;
-    const uint32_t m = 1u << ls;
-    // twiddle depends on the index bits below s: thread bits below lo and local bits below ls
+  for (uint32_t rl = 0; rl < m; rl++) {
 #pragma unroll
-    for (uint32_t rl = 0; rl < m; rl++) {
-      const uint32_t i0 = grp_index(t, rl, lo);
-      const uint32_t j = i0 & ((1u << s) - 1);
-      const uint32_t w = twid(tw, j << (logn - s - 1), mask, inverse);
-#pragma unroll
-      for (uint32_t rh = 0; rh < 16; rh += 2 * m) {
-        uint32_t& a = v[rh + rl];
-        uint32_t& b = v[rh + rl + m];
-        if (DIF) {
-          uint32_t u = a, x = b;
-          a = add(u, x);
-          b = mul(sub(u, x), w);
-        } else {
-          uint32_t u = a, x = mul(b, w);
-          a = add(u, x);
-          b = sub(u, x);
-        }
+    for (uint32_t rh = 0; rh < 16; rh += 2 * m) {
+      uint32_t& a = v[rh + rl];
+      uint32_t& b = v[rh + rl + m];
+      if (DIF) {
+        uint32_t u = a, x = b;
+        a = add(u, x);
+        b = mul(sub(u, x), w[rl]);
+      } else {
+        uint32_t u = a, x = mul(b, w[rl]);
+        a = add(u, x);
+        b = sub(u, x);
       }
     }
   }
 }
-
-// Pass plan.  DIF: the first pass takes the top logn mod 4 stages (or 4) with
-// local bits [logn-4, logn); then four stages per pass.  DIT mirrors it from
-// the bottom.  Returns the number of passes.
-__device__ __forceinline__ int pass_count(int logn) {
-  int rem = logn & 3;
-  if (!rem) rem = 4;
-  return (logn - rem) / 4 + 1;
-}
 template <bool DIF>
-__device__ __forceinline__ void pass_plan(int p, int logn, int& lo, int& s_lo, int& s_hi) {
-  int rem = logn & 3;
-  if (!rem) rem = 4;
+__device__ __forceinline__ void pass16(uint32_t v[16], uint32_t t, int lo, int s_lo, int s_hi, const uint32_t* ptab) {
+  auto one = [&](auto LSC) {
+    constexpr int LS = decltype(LSC)::value;
+    const int s = lo + LS;
+    if (s >= s_lo && s <= s_hi) stage16<DIF, LS>(v, t, lo, s_lo, ptab);
+  };
   if (DIF) {
-    if (p == 0) { lo = logn - 4; s_hi = logn - 1; s_lo = logn - rem; }
-    else { s_hi = logn - rem - 4 * (p - 1) - 1; s_lo = s_hi - 3; lo = s_lo; }
+    one(std::integral_constant<int, 3>{});
+    one(std::integral_constant<int, 2>{});
+    one(std::integral_constant<int, 1>{});
+    one(std::integral_constant<int, 0>{});
   } else {
-    int np = pass_count(logn);
-    if (p < np - 1) { s_lo = 4 * p; s_hi = s_lo + 3; lo = s_lo; }
-    else { s_lo = 4 * p; s_hi = logn - 1; lo = logn - 4; }
+    one(std::integral_constant<int, 0>{});
+    one(std::integral_constant<int, 1>{});
+    one(std::integral_constant<int, 2>{});
+    one(std::integral_constant<int, 3>{});
   }
 }
 
@@ -86,7 +144,8 @@ struct NoHook {
   __device__ void operator()(uint32_t, const uint32_t*) const {}
 };
 
-// Full transform of n = 2^logn >= 16 points.  Pass 0 takes its inputs from
+// Full transform of n = 2^logn >= 16 points; `tw`: the size's radix-16
+// twiddle tables (tw16 layout, Ctx::twiddles16).  Pass 0 takes its inputs from
 // `first(t, r, lo)` (a global gather, or a shared-memory read with a scale)
 // and shows them to `loaded(t, v)` before its butterflies; every pass but the
 // last writes back to S (pad16 layout); the last pass hands its 16 registers
@@ -102,8 +161,9 @@ __device__ __forceinline__ void ntt16(uint32_t* S, int logn, const uint32_t* tw,
   const int np = pass_count(logn);
 #pragma unroll
   for (int p = 0; p < np; p++) {
-    int lo, s_lo, s_hi;
+    int lo = 0, s_lo = 0, s_hi = 0;
     pass_plan<DIF>(p, logn, lo, s_lo, s_hi);
+    const uint32_t* ptab = tw + tw16_pass_offset(logn, DIF, inverse, p);
     for (uint32_t t = threadIdx.x; t < groups; t += blockDim.x) {
       uint32_t v[16];
       if (p == 0) {
@@ -114,7 +174,7 @@ __device__ __forceinline__ void ntt16(uint32_t* S, int logn, const uint32_t* tw,
 #pragma unroll
         for (uint32_t r = 0; r < 16; r++) v[r] = S[pad16(grp_index(t, r, lo))];
       }
-      pass16<DIF>(v, t, lo, s_lo, s_hi, logn, tw, inverse);
+      pass16<DIF>(v, t, lo, s_lo, s_hi, ptab);
       if (p == np - 1) {
         store(t, lo, v);
       } else {

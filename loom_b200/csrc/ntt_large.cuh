@@ -42,7 +42,8 @@ __host__ __device__ constexpr size_t tile_words(int logl) {
   return (((size_t)1 << logl) + ((size_t)1 << logl) / 16) * 16;
 }
 
-// The 16 column transforms of a tile, 2^LOGL rows each.  Pass 0 takes its
+// The 16 column transforms of a tile, 2^LOGL rows each (`tw`: the tw16
+// tables of 2^LOGL points).  Pass 0 takes its
 // inputs from first(col, row) (global memory, or the staged tile), every pass
 // but the last writes back to S, the last hands each element to
 // store(col, row, value).  DIF: natural rows in, bit-reversed rows out.
@@ -52,8 +53,9 @@ __device__ __forceinline__ void ntt16_tile(uint32_t* S, const uint32_t* tw, bool
   constexpr int np = (LOGL - ((LOGL & 3) ? (LOGL & 3) : 4)) / 4 + 1;
 #pragma unroll
   for (int p = 0; p < np; p++) {
-    int lo, s_lo, s_hi;
+    int lo = 0, s_lo = 0, s_hi = 0;
     pass_plan<DIF>(p, LOGL, lo, s_lo, s_hi);
+    const uint32_t* ptab = tw + tw16_pass_offset(LOGL, DIF, inverse, p);
     for (uint32_t u = threadIdx.x; u < groups * BIG_TILE; u += blockDim.x) {
       const uint32_t col = u & (BIG_TILE - 1), t = u >> 4;
       uint32_t v[16];
@@ -62,7 +64,7 @@ __device__ __forceinline__ void ntt16_tile(uint32_t* S, const uint32_t* tw, bool
         const uint32_t row = grp_index(t, r, lo);
         v[r] = p == 0 ? first(col, row) : S[tile_addr(row, col)];
       }
-      pass16<DIF>(v, t, lo, s_lo, s_hi, LOGL, tw, inverse);
+      pass16<DIF>(v, t, lo, s_lo, s_hi, ptab);
 #pragma unroll
       for (uint32_t r = 0; r < 16; r++) {
         const uint32_t row = grp_index(t, r, lo);
@@ -74,7 +76,7 @@ __device__ __forceinline__ void ntt16_tile(uint32_t* S, const uint32_t* tw, bool
   }
 }
 
-// tw_n / tw_c: tables of w_n^j, w_C^j.  Block (x, y): tile x of job y.
+// tw_n: w_n^j; tw_c: the tw16 tables of C points.  Block (x, y): tile x of job y.
 template <int LOGC>
 __global__ void __launch_bounds__(512) k_big_pass_a(const BigNtt* jobs, int logn, int logr, int inverse,
                                                     const uint32_t* tw_n, const uint32_t* tw_c) {

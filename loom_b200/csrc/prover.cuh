@@ -1069,7 +1069,7 @@ struct Prover {
       }
       auto tab = upload_vec(c, lanes);
       keep.push_back(tab);
-      const uint32_t* twn = c.twiddles((int)logn);
+      const uint32_t* twn = c.ntt_twiddles((int)logn);
       with_ntt_size((int)logn, [&](auto L) {
         allow_smem(k_intt<decltype(L)::value>, pad16_words((int)logn) * 4);
         c.timed("quotient_intt", 8.0 * n * lanes.size(), 0, [&] {
@@ -1116,7 +1116,7 @@ struct Prover {
           continue;
         }
         auto tab = upload_vec(c, kv.second);
-        const uint32_t* twn = c.twiddles((int)logn);
+        const uint32_t* twn = c.ntt_twiddles((int)logn);
         const uint32_t* shifts = c.coset_shifts((int)logn);
         const size_t smem = 2 * pad16_words((int)logn) * 4;
         with_ntt_size((int)logn, [&](auto L) {
@@ -1169,7 +1169,7 @@ struct Prover {
           continue;
         }
         auto tab = upload_vec(c, kv.second);
-        const uint32_t* twn = c.twiddles((int)kv.first);
+        const uint32_t* twn = c.ntt_twiddles((int)kv.first);
         with_ntt_size((int)kv.first, [&](auto L) {
           allow_smem(k_intt<decltype(L)::value>, pad16_words((int)kv.first) * 4);
           c.timed("quotient_intt", 8.0 * n * kv.second.size(), 0, [&] {
