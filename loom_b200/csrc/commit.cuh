@@ -70,6 +70,13 @@ inline void big_ntt(Ctx& c, std::vector<BigNtt> jobs, int logn, bool inverse, co
   const uint32_t* tw_n = c.twiddles(logn);
   const uint32_t* tw_c = c.twiddles16(logc);
   const uint32_t* tw_r = c.twiddles16(logr);
+  // the large roots' powers as two small tables (tw_split): w_n and, for the
+  // coset shifts, w_{4n} (every job's t2 table is the w_{4n} powers)
+  const uint32_t* tw_n_hi = c.twiddles(logn - TW_SPLIT);
+  const uint32_t* t2_hi = c.twiddles(logn + RATE_LOG - TW_SPLIT);
+  for (auto& j : jobs)
+    if (j.t2 && j.m2_mask != (uint32_t)((n << RATE_LOG) - 1))
+      throw Error(LG_ERR_INVALID, "four-step coset table of another size");
   // scratch chunks of 2^26 words at most (256 MiB)
   const size_t per = std::max<size_t>(1, ((size_t)1 << 26) / n);
   const size_t smem_a = tile_words(logc) * 4, smem_b = tile_words(logr) * 4;
@@ -86,7 +93,7 @@ inline void big_ntt(Ctx& c, std::vector<BigNtt> jobs, int logn, bool inverse, co
         constexpr int C_ = decltype(LC)::value;
         allow_smem(k_big_pass_a<C_>, smem_a);
         k_big_pass_a<C_><<<dim3((1u << logr) / BIG_TILE, (unsigned)cnt), thr_a, smem_a, c.stream>>>(
-            (const BigNtt*)jd->p, logn, logr, inverse ? 1 : 0, tw_n, tw_c);
+            (const BigNtt*)jd->p, logn, logr, inverse ? 1 : 0, tw_n, tw_n_hi, t2_hi, tw_c);
         LG_LAUNCH();
       });
       with_tile_size(logr, [&](auto LR) {

@@ -638,6 +638,14 @@ struct Writer {
     }
     off += 4 * n;
   }
+  // n bytes at the current offset, filled by the caller (a copy that lands
+  // later); only while writing to the caller's buffer, which must hold them
+  uint8_t* claim(size_t n) {
+    if (!external || off + n > cap) throw Error(LG_ERR_INVALID, "proof writer: claimed bytes outside the caller's buffer");
+    uint8_t* q = p + off;
+    off += n;
+    return q;
+  }
   // words already in proof encoding (big-endian canonical bytes); large
   // blocks (the per-query sections, megabytes) are copied by four threads
   void bytes(const uint32_t* be, size_t n) {

@@ -8,6 +8,7 @@
 // 16-element groups of a warp fall into distinct banks in every pass.
 #pragma once
 #include <type_traits>
+#include <utility>
 
 #include "field.cuh"
 
@@ -92,18 +93,41 @@ template <int M> __device__ __forceinline__ void ld_tw(const uint32_t* p, uint32
   }
 }
 
+// w_{2^(S+1)}^RL (or its inverse) in Montgomery form, as a compile-time
+// constant: the pass whose local bits are the lowest four (lo = 0) has the
+// same twiddles in every thread, j = RL.
+template <int S, int RL, bool INV> struct TwConst {
+  static constexpr uint32_t order = 2u << S;
+  static constexpr uint32_t w = cx_pow(3, (uint64_t)127 << (24 - (S + 1)));  // canonical, order 2^(S+1)
+  static constexpr uint32_t value = cx_mulmod(cx_pow(w, INV ? (order - RL) % order : RL), MONT_ONE);
+};
+
+template <int LS, bool INV, size_t... R>
+__device__ __forceinline__ void tw_consts(uint32_t* w, std::index_sequence<R...>) {
+  ((w[R] = TwConst<LS, (int)R, INV>::value), ...);
+}
+
 // Stages s in [s_lo, s_hi] on the 16 registers of group t (local bits
 // [lo, lo+4)).  DIF: (u, v) -> (u + v, (u - v) w), stages descending;
 // DIT: (u, v) -> (u + v w, u - v w), stages ascending.  w = w_{2^(s+1)}^j,
-// j = index mod 2^s; `ptab`: this pass's twiddle table (tw16 layout).
+// j = index mod 2^s; `ptab`: this pass's twiddle table (tw16 layout).  When
+// lo = 0 the twiddles are constants (j = r) and w = 1 (r = 0) costs no
+// product.
 template <bool DIF, int LS>
-__device__ __forceinline__ void stage16(uint32_t v[16], uint32_t t, int lo, int s_lo, const uint32_t* ptab) {
+__device__ __forceinline__ void stage16(uint32_t v[16], uint32_t t, int lo, int s_lo, const uint32_t* ptab,
+                                        bool inverse) {
   constexpr uint32_t m = 1u << LS;
   const int s = lo + LS;
   uint32_t w[m];
-  ld_tw<m>(ptab + tw16_stage_offset(s_lo, s) + (t & ((1u << lo) - 1)) * m, w);
+  if (lo == 0) {
+    if (inverse) tw_consts<LS, true>(w, std::make_index_sequence<m>{});
+    else tw_consts<LS, false>(w, std::make_index_sequence<m>{});
+  } else {
+    ld_tw<m>(ptab + tw16_stage_offset(s_lo, s) + (t & ((1u << lo) - 1)) * m, w);
+  }
 #pragma unroll
   for (uint32_t rl = 0; rl < m; rl++) {
+    const bool unit = lo == 0 && rl == 0;
 #pragma unroll
     for (uint32_t rh = 0; rh < 16; rh += 2 * m) {
       uint32_t& a = v[rh + rl];
@@ -111,9 +135,9 @@ __device__ __forceinline__ void stage16(uint32_t v[16], uint32_t t, int lo, int 
       if (DIF) {
         uint32_t u = a, x = b;
         a = add(u, x);
-        b = mul(sub(u, x), w[rl]);
+        b = unit ? sub(u, x) : mul(sub(u, x), w[rl]);
       } else {
-        uint32_t u = a, x = mul(b, w[rl]);
+        uint32_t u = a, x = unit ? b : mul(b, w[rl]);
         a = add(u, x);
         b = sub(u, x);
       }
@@ -121,11 +145,12 @@ __device__ __forceinline__ void stage16(uint32_t v[16], uint32_t t, int lo, int 
   }
 }
 template <bool DIF>
-__device__ __forceinline__ void pass16(uint32_t v[16], uint32_t t, int lo, int s_lo, int s_hi, const uint32_t* ptab) {
+__device__ __forceinline__ void pass16(uint32_t v[16], uint32_t t, int lo, int s_lo, int s_hi, const uint32_t* ptab,
+                                       bool inverse) {
   auto one = [&](auto LSC) {
     constexpr int LS = decltype(LSC)::value;
     const int s = lo + LS;
-    if (s >= s_lo && s <= s_hi) stage16<DIF, LS>(v, t, lo, s_lo, ptab);
+    if (s >= s_lo && s <= s_hi) stage16<DIF, LS>(v, t, lo, s_lo, ptab, inverse);
   };
   if (DIF) {
     one(std::integral_constant<int, 3>{});
@@ -174,7 +199,7 @@ __device__ __forceinline__ void ntt16(uint32_t* S, int logn, const uint32_t* tw,
 #pragma unroll
         for (uint32_t r = 0; r < 16; r++) v[r] = S[pad16(grp_index(t, r, lo))];
       }
-      pass16<DIF>(v, t, lo, s_lo, s_hi, ptab);
+      pass16<DIF>(v, t, lo, s_lo, s_hi, ptab, inverse);
       if (p == np - 1) {
         store(t, lo, v);
       } else {

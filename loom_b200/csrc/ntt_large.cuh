@@ -64,7 +64,7 @@ __device__ __forceinline__ void ntt16_tile(uint32_t* S, const uint32_t* tw, bool
         const uint32_t row = grp_index(t, r, lo);
         v[r] = p == 0 ? first(col, row) : S[tile_addr(row, col)];
       }
-      pass16<DIF>(v, t, lo, s_lo, s_hi, ptab);
+      pass16<DIF>(v, t, lo, s_lo, s_hi, ptab, inverse);
 #pragma unroll
       for (uint32_t r = 0; r < 16; r++) {
         const uint32_t row = grp_index(t, r, lo);
@@ -76,10 +76,21 @@ __device__ __forceinline__ void ntt16_tile(uint32_t* S, const uint32_t* tw, bool
   }
 }
 
-// tw_n: w_n^j; tw_c: the tw16 tables of C points.  Block (x, y): tile x of job y.
+// A power w^e of a root w of order 2^(11 + k) from two small tables that
+// stay in L1: lo[i] = w^i (i < 2^11, the first entries of the full table) and
+// hi[i] = w^(2^11 i); one product instead of a load from a table of megabytes.
+constexpr int TW_SPLIT = 11;
+__device__ __forceinline__ uint32_t tw_split(const uint32_t* lo, const uint32_t* hi, uint32_t e) {
+  return mul(__ldg(lo + (e & ((1u << TW_SPLIT) - 1))), __ldg(hi + (e >> TW_SPLIT)));
+}
+
+// tw_n: w_n^j (its first 2^11 entries are read), tw_n_hi: w_n^(2^11 j);
+// t2_hi: the same split of the jobs' t2 tables (w_{m2}^(2^11 j)); tw_c: the
+// tw16 tables of C points.  Block (x, y): tile x of job y.
 template <int LOGC>
-__global__ void __launch_bounds__(512) k_big_pass_a(const BigNtt* jobs, int logn, int logr, int inverse,
-                                                    const uint32_t* tw_n, const uint32_t* tw_c) {
+__global__ void __launch_bounds__(512, 2) k_big_pass_a(const BigNtt* jobs, int logn, int logr, int inverse,
+                                                    const uint32_t* tw_n, const uint32_t* tw_n_hi,
+                                                    const uint32_t* t2_hi, const uint32_t* tw_c) {
   extern __shared__ uint32_t S[];
   const BigNtt J = jobs[blockIdx.y];
   const uint32_t R = 1u << logr, n = 1u << logn;
@@ -89,20 +100,21 @@ __global__ void __launch_bounds__(512) k_big_pass_a(const BigNtt* jobs, int logn
     uint32_t v = J.in[k];
     if (J.c0 != MONT_ONE) v = mul(v, J.c0);
     if (J.t1) v = mul(v, __ldg(J.t1 + k));
-    if (J.t2) v = mul(v, __ldg(J.t2 + ((J.e2 * k) & J.m2_mask)));
+    if (J.t2) v = mul(v, tw_split(J.t2, t2_hi, (J.e2 * k) & J.m2_mask));
     return v;
   };
   auto store = [&](uint32_t col, uint32_t p, uint32_t v) {
     const uint32_t j2 = bitrev32(p, LOGC), k1 = k1_0 + col;
-    const uint32_t e = (uint32_t)(((uint64_t)j2 * k1) & (n - 1));
-    J.scratch[(uint64_t)j2 * R + k1] = mul(v, tw_at(tw_n, e, n - 1, inverse != 0));
+    uint32_t e = (uint32_t)(((uint64_t)j2 * k1) & (n - 1));
+    if (inverse) e = (n - e) & (n - 1);
+    J.scratch[(uint64_t)j2 * R + k1] = mul(v, tw_split(tw_n, tw_n_hi, e));
   };
   ntt16_tile<true, LOGC>(S, tw_c, inverse != 0, first, store);
 }
 
 // Block (x, y): rows [16 x, 16 x + 16) of job y's scratch.
 template <int LOGR>
-__global__ void __launch_bounds__(512) k_big_pass_b(const BigNtt* jobs, int logc, int inverse,
+__global__ void __launch_bounds__(512, 2) k_big_pass_b(const BigNtt* jobs, int logc, int inverse,
                                                     const uint32_t* tw_r) {
   extern __shared__ uint32_t S[];
   const BigNtt J = jobs[blockIdx.y];

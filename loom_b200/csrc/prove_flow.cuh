@@ -121,6 +121,13 @@ struct OpenPlan {
   // Gathers and lays out every section at the query positions; returns the
   // host copy (the context's pinned staging, valid until its next use).
   const uint32_t* run(Ctx& c, const std::vector<uint32_t>& pos) {
+    DBufP asm_d = run_device(c, pos);
+    uint32_t* A = c.host_staging(total);
+    c.d2h(A, asm_d->p, total);
+    return A;
+  }
+  // The same, left on the device (encoded words, sections at out_off).
+  DBufP run_device(Ctx& c, const std::vector<uint32_t>& pos) {
     const uint32_t nq = (uint32_t)pos.size();
     auto pos_d = upload_vec(c, pos);
     auto out_d = std::make_shared<DBuf>(per_q * nq, c.stream);
@@ -161,10 +168,18 @@ struct OpenPlan {
         LG_LAUNCH();
       });
     }
-    uint32_t* A = c.host_staging(total);
-    c.d2h(A, asm_d->p, total);
-    return A;
+    return asm_d;
   }
+};
+
+// Length of an encoding, counted without writing (the Writer's methods).
+struct Sizer {
+  size_t off = 0;
+  void u32(uint32_t) { off += 4; }
+  void e6(const E6&) { off += 24; }
+  void e6w(const uint32_t*) { off += 24; }
+  void dg(const Digest&) { off += 32; }
+  void str(const std::string& s) { off += 4 + s.size(); }
 };
 
 inline void Prover::begin(const uint32_t* const* witness, bool on_device) {
@@ -593,58 +608,82 @@ inline size_t Prover::open_and_encode(const std::vector<uint32_t>& pos, uint8_t*
     obs.push_back(ob);
   }
   const SectionSrc batch_sec = OP.batches_section(obs, num_queries);
-  const uint32_t* A = OP.run(c, pos);
-
+  DBufP asm_d = OP.run_device(c, pos);
   c.phase("openings gather");
-  Writer W(c.proof_buf, out, out_cap);
-  W.expect((size_t)4 * OP.total + (1 << 20));
-  W.str("poseidon2");
-  {  // exposed values by name: name, one entry (index 0, extension kind 1, value)
-    std::vector<std::pair<std::string, size_t>> ev;
-    for (const Step& st : pg.steps)
-      if (exposes(st.type))
-        ev.push_back({pg.columns[st.out].name + (st.type == STEP_LOGUP ? "_total" : "_end"), st.exposed});
-    std::sort(ev.begin(), ev.end());
-    W.u32((uint32_t)ev.size());
-    for (auto& e : ev) {
-      W.str(e.first);
-      W.u32(1);
-      W.u32(0);
-      W.u32(1);
-      W.e6(exposed[e.second]);
+  // The encoding in proof order; `section(W, sc)` appends a per-query
+  // section of the gathered words.
+  auto emit = [&](auto& W, auto section) {
+    W.str("poseidon2");
+    {  // exposed values by name: name, one entry (index 0, extension kind 1, value)
+      std::vector<std::pair<std::string, size_t>> ev;
+      for (const Step& st : pg.steps)
+        if (exposes(st.type))
+          ev.push_back({pg.columns[st.out].name + (st.type == STEP_LOGUP ? "_total" : "_end"), st.exposed});
+      std::sort(ev.begin(), ev.end());
+      W.u32((uint32_t)ev.size());
+      for (auto& e : ev) {
+        W.str(e.first);
+        W.u32(1);
+        W.u32(0);
+        W.u32(1);
+        W.e6(exposed[e.second]);
+      }
     }
-  }
-  W.u32((uint32_t)commitments.size());
-  for (auto& d : commitments) W.dg(d);
-  W.u32((uint32_t)trees.size());
-  for (size_t t = 0; t < trees.size(); t++) {
-    W.u32((uint32_t)trees[t].groups.size());
-    for (size_t g = 0; g < trees[t].groups.size(); g++) {
-      const Group& G2 = trees[t].groups[g];
-      size_t nbp = G2.bcols.size();
-      W.u32((uint32_t)nbp);
-      for (size_t i = 0; i < nbp; i++) { W.u32((uint32_t)cv[t][g][i].size()); for (auto& v : cv[t][g][i]) W.e6(v); }
-      W.u32((uint32_t)G2.ecols.size());
-      for (size_t i = nbp; i < cv[t][g].size(); i++) { W.u32((uint32_t)cv[t][g][i].size()); for (auto& v : cv[t][g][i]) W.e6(v); }
+    W.u32((uint32_t)commitments.size());
+    for (auto& d : commitments) W.dg(d);
+    W.u32((uint32_t)trees.size());
+    for (size_t t = 0; t < trees.size(); t++) {
+      W.u32((uint32_t)trees[t].groups.size());
+      for (size_t g = 0; g < trees[t].groups.size(); g++) {
+        const Group& G2 = trees[t].groups[g];
+        size_t nbp = G2.bcols.size();
+        W.u32((uint32_t)nbp);
+        for (size_t i = 0; i < nbp; i++) { W.u32((uint32_t)cv[t][g][i].size()); for (auto& v : cv[t][g][i]) W.e6(v); }
+        W.u32((uint32_t)G2.ecols.size());
+        for (size_t i = nbp; i < cv[t][g].size(); i++) { W.u32((uint32_t)cv[t][g][i].size()); for (auto& v : cv[t][g][i]) W.e6(v); }
+      }
     }
-  }
-  auto section = [&](const SectionSrc& sc) { W.bytes(A + sc.out_off, (size_t)num_queries * sc.q_words); };
-  W.dg(levels_tree.root);
-  W.u32((uint32_t)(L - 1));
-  for (size_t l = 1; l < L; l++) {
+    W.dg(levels_tree.root);
+    W.u32((uint32_t)(L - 1));
+    for (size_t l = 1; l < L; l++) {
+      W.u32(num_queries);
+      section(W, lvl_sec[l]);
+    }
+    W.u32((uint32_t)fri_roots.size());
+    for (auto& d : fri_roots) W.dg(d);
+    W.u32(1);
+    W.u32((uint32_t)nj);
+    for (size_t i = 0; i < nj; i++) { uint32_t e[6]; for (int w = 0; w < 6; w++) e[w] = final_poly[w * nj + i]; W.e6w(e); }
     W.u32(num_queries);
-    section(lvl_sec[l]);
+    section(W, fri_sec);
+    W.u32(0);
+    W.u32(num_queries);
+    section(W, batch_sec);
+  };
+  const auto sec_bytes = [&](const SectionSrc& sc) { return (size_t)4 * num_queries * sc.q_words; };
+  Sizer sz;
+  emit(sz, [&](Sizer& S, const SectionSrc& sc) { S.off += sec_bytes(sc); });
+  // A caller buffer in page-locked host memory that holds the whole proof
+  // takes the sections straight from the device (no staging copy).
+  bool pinned = false;
+  if (out && out_cap >= sz.off) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, out) == cudaSuccess) pinned = at.type == cudaMemoryTypeHost;
+    else cudaGetLastError();
   }
-  W.u32((uint32_t)fri_roots.size());
-  for (auto& d : fri_roots) W.dg(d);
-  W.u32(1);
-  W.u32((uint32_t)nj);
-  for (size_t i = 0; i < nj; i++) { uint32_t e[6]; for (int w = 0; w < 6; w++) e[w] = final_poly[w * nj + i]; W.e6w(e); }
-  W.u32(num_queries);
-  section(fri_sec);
-  W.u32(0);
-  W.u32(num_queries);
-  section(batch_sec);
+  Writer W(c.proof_buf, out, out_cap);
+  if (pinned) {
+    emit(W, [&](Writer& Wr, const SectionSrc& sc) {
+      const size_t n = sec_bytes(sc);
+      uint8_t* dst = Wr.claim(n);
+      LG_CK(cudaMemcpyAsync(dst, asm_d->p + sc.out_off, n, cudaMemcpyDeviceToHost, c.stream));
+    });
+  } else {
+    uint32_t* A = c.host_staging(OP.total);
+    c.d2h(A, asm_d->p, OP.total);
+    W.expect(sz.off);
+    emit(W, [&](Writer& Wr, const SectionSrc& sc) { Wr.bytes(A + sc.out_off, (size_t)num_queries * sc.q_words); });
+  }
   LG_CK(cudaStreamSynchronize(c.stream));
   c.phase("serialize");
   *in_out = W.in_caller_buffer();
@@ -694,10 +733,11 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
   c.phase("quotient+air commit");
   // ---- claimed values and alpha_DEEP
   claimed_values();
+  c.phase("claimed values");
   fs.add("alpha_DEEP");
   for (const E6& v : claimed_values_bind_order()) fs.bind("alpha_DEEP", v.c, 6);
   set_challenge("alpha_DEEP", fs.compute("alpha_DEEP").v);
-  c.phase("claimed values+bind");
+  c.phase("alpha bind");
   deep_codewords();
   c.phase("deep");
   // ---- FRI
