@@ -130,6 +130,9 @@ int lg_ctx_set_leaf_mapping(lg_ctx* ctx, int lanes_per_permutation);
  *                         plus one block per (lane, coset); 0: one block per
  *                         lane for all of it
  *   "lde_fwd_threads"     threads per coset block (256, 512 or 1024)
+ *   "fri_tail_leaves"     the FRI rounds whose layer tree has at most this many
+ *                         leaves run in one block, back to back (power of two,
+ *                         2..65536; 0: a launch per step of every round)
  * Unknown names or values out of range return LG_ERR_INVALID. */
 int lg_ctx_set_tuning(lg_ctx* ctx, const char* name, int64_t value);
 int lg_ctx_get_tuning(lg_ctx* ctx, const char* name, int64_t* value);

@@ -1103,6 +1103,125 @@ __global__ void k_fold(const uint32_t* layer, uint64_t n, const uint32_t* alpha_
   st6(next, half, i, e6_add(s, d));
 }
 
+// The last FRI rounds in one block: for each round j, the fold of layer j
+// with challenge j (as k_fold), the levels that enter at j + 1 (as
+// k_axpy_e6), then, unless j is the last round, layer j + 1's commitment —
+// pair leaves (one permutation each, as k_hash_leaves), the tree level by
+// level — and challenge j + 1 from its root (as k_fs_challenge).  These
+// layers are small (at most a few thousand leaves), so their launches were
+// latency bound: one block runs them back to back with barriers instead,
+// every value written where the per-round launches write it.  Six lanes per
+// permutation, five permutations per warp.
+struct FriRound {
+  const uint32_t* cur;     // layer j: 6 lanes of n words (bit-reversed rows)
+  uint32_t* next;          // layer j + 1: 6 lanes of n / 2 words
+  const uint32_t* tw;      // w_n^k, k < n
+  uint32_t* nodes;         // layer j + 1's tree (2 leaves digests, 1-indexed); null after the last fold
+  uint64_t n;              // rows of layer j
+  uint32_t log_leaves;     // of that tree
+  uint32_t pre_off, pre_len;      // challenge j + 1's name elements in `pre`
+  uint32_t term_first, term_count;  // levels added to layer j + 1
+};
+__global__ void __launch_bounds__(1024) k_fri_tail(const FriRound* rounds, uint32_t n_rounds, uint32_t j0,
+                                                   const AxpyTerm* terms, const uint32_t* pre, uint32_t* chal,
+                                                   uint32_t inv2) {
+  __shared__ uint32_t keys[144];
+  __shared__ uint32_t msg[64];
+  p2_load_full_keys(keys);  // ends with a barrier
+  P2Lane L;
+  L.init();
+  const uint32_t warps = blockDim.x >> 5, per = warps * P2_GROUPS_PER_WARP;
+  const uint32_t slot = (threadIdx.x >> 5) * P2_GROUPS_PER_WARP + (uint32_t)L.base / 6;
+  for (uint32_t r = 0; r < n_rounds; r++) {
+    const FriRound R = rounds[r];
+    const uint32_t j = j0 + r;
+    const uint64_t half = R.n / 2;
+    // fold
+    {
+      E6 alpha;
+#pragma unroll
+      for (int w = 0; w < 6; w++) alpha.c[w] = chal[8 * (size_t)j + w];
+      int lg = 0;
+      while ((1ull << lg) < half) lg++;
+      for (uint64_t i = threadIdx.x; i < half; i += blockDim.x) {
+        const uint32_t e = bitrev32((uint32_t)i, lg);
+        const uint32_t xinv = __ldg(R.tw + ((R.n - e) & (R.n - 1)));
+        const E6 p = ld6(R.cur, R.n, 2 * i), q = ld6(R.cur, R.n, 2 * i + 1);
+        const E6 sm = e6_mul_base(e6_add(p, q), inv2);
+        const E6 d = e6_mul(e6_mul_base(e6_mul_base(e6_sub(p, q), inv2), xinv), alpha);
+        E6 v = e6_add(sm, d);
+        for (uint32_t t = 0; t < R.term_count; t++) {
+          const AxpyTerm T = terms[R.term_first + t];
+          v = e6_add(v, e6_mul(ld6(T.lvl, half, i), T.gamma));
+        }
+        st6(R.next, half, i, v);
+      }
+    }
+    __syncthreads();
+    if (!R.nodes) break;
+    // leaves of layer j + 1: Sponge(LEAF, 0, 2, row 2k, row 2k + 1), 15 elements
+    const uint32_t nl = 1u << R.log_leaves;
+    {
+      LeafGroup g;
+      g.base = nullptr;
+      g.ext = R.next;
+      g.stride = half;
+      g.nb = 0;
+      g.ne = 1;
+      g.n_leaves = nl;
+      g.out = R.nodes + (size_t)8 * nl;
+      const uint32_t h0 = to_mont(LEAF_TAG), h1 = to_mont(0), h2 = to_mont(2);
+      for (uint32_t k0 = 0; k0 < nl; k0 += per) {
+        const uint32_t k = k0 + slot;
+        const bool active = L.lane < 30 && k < nl;
+        uint32_t x[4] = {0, 0, 0, 0};
+        if (active && L.idx < 4) {
+#pragma unroll
+          for (uint32_t i = 0; i < 4; i++) {
+            const uint32_t e = 4 * L.idx + i;
+            if (e < 15) x[i] = leaf_elem(g, e, k, h0, h1, h2);
+          }
+        }
+        p2c_permute(x, L, keys);
+        if (active && L.idx < 2) {
+          uint32_t* o = g.out + (size_t)k * 8 + 4 * L.idx;
+#pragma unroll
+          for (int i = 0; i < 4; i++) o[i] = x[i];
+        }
+      }
+    }
+    __syncthreads();
+    for (uint32_t w = nl >> 1; w >= 1; w >>= 1) {
+      for (uint32_t i0 = 0; i0 < w; i0 += per) {
+        const uint32_t i = i0 + slot;
+        merkle_node(R.nodes, (uint64_t)w + i, L, keys, L.lane < 30 && i < w);
+      }
+      __syncthreads();
+    }
+    // challenge j + 1 = sponge(name elements || challenge j || root)
+    const uint32_t total = R.pre_len + 16;
+    for (uint32_t i = threadIdx.x; i < total; i += blockDim.x)
+      msg[i] = i < R.pre_len ? pre[R.pre_off + i] : (i < R.pre_len + 8 ? chal[8 * (size_t)j + (i - R.pre_len)]
+                                                                          : R.nodes[8 + (i - R.pre_len - 8)]);
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      uint32_t x[4] = {0, 0, 0, 0};
+      for (uint32_t b = 0; b < total; b += 16) {
+        const uint32_t len = min(16u, total - b);
+        if (L.idx < 4)
+#pragma unroll
+          for (int k = 0; k < 4; k++)
+            if (4 * (uint32_t)L.idx + k < len) x[k] = msg[b + 4 * L.idx + k];
+        p2c_permute(x, L, keys);
+      }
+      if (L.lane < 2)
+#pragma unroll
+        for (int k = 0; k < 4; k++) chal[8 * (size_t)(j + 1) + 4 * L.lane + k] = x[k];
+    }
+    __syncthreads();
+  }
+}
+
 // One Fiat-Shamir challenge on the device, for challenges whose bindings are
 // already in device memory (the FRI layer roots): digest = state[0..8) of
 // the width-24 sponge (rate 16, overwrite, no padding) over

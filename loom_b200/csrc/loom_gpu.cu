@@ -190,6 +190,10 @@ int lg_ctx_set_tuning(lg_ctx* ctx, const char* name, int64_t value) {
     else if (n == "leaf_block") { in(32, 1024); pow2(); t.leaf_block = (uint32_t)value; }
     else if (n == "lde_split") { in(0, 1); t.lde_split = (uint32_t)value; }
     else if (n == "lde_fwd_threads") { in(256, 1024); pow2(); t.lde_fwd_threads = (uint32_t)value; }
+    else if (n == "fri_tail_leaves") {
+      if (value != 0) { in(2, 1 << 16); pow2(); }
+      t.fri_tail_leaves = (uint32_t)value;
+    }
     else throw Error(LG_ERR_INVALID, "unknown tuning " + n);
   });
 }
@@ -208,6 +212,7 @@ int lg_ctx_get_tuning(lg_ctx* ctx, const char* name, int64_t* value) {
     else if (n == "leaf_block") *value = t.leaf_block;
     else if (n == "lde_split") *value = t.lde_split;
     else if (n == "lde_fwd_threads") *value = t.lde_fwd_threads;
+    else if (n == "fri_tail_leaves") *value = t.fri_tail_leaves;
     else throw Error(LG_ERR_INVALID, "unknown tuning " + n);
   });
 }

@@ -552,6 +552,58 @@ inline bool Prover::fri_fold_round(int j, bool read_root, Digest* next_root) {
   return true;
 }
 
+inline void Prover::fri_tail(int j0, const DBufP& pre_d, const std::vector<uint32_t>& pre_off,
+                             const std::vector<uint32_t>& pre_len) {
+  if (fri_next != j0 || j0 <= r0 || j0 >= NR) throw Error(LG_ERR_INVALID, "FRI tail out of order");
+  auto jl = [&](size_t l) { return MAX_LOG_MODULE - (int)lvl_log[l]; };
+  std::vector<FriRound> rr;
+  std::vector<AxpyTerm> terms;
+  DBufP cur = running;
+  std::vector<DBufP> keep;
+  size_t n = nj;
+  for (int j = j0; j < NR; j++) {
+    FriRound R{};
+    R.cur = cur->p;
+    auto next = std::make_shared<DBuf>(3 * n, c.stream);
+    R.next = next->p;
+    R.n = n;
+    R.tw = c.twiddles(LOG_N_FRI - j);
+    R.term_first = (uint32_t)terms.size();
+    for (size_t l = 1; l < L; l++)
+      if (jl(l) == j + 1) {
+        if (!gam_ready[l]) throw Error(LG_ERR_INVALID, "challenge fri_level_" + std::to_string(l) + "_gamma has not been set");
+        terms.push_back(AxpyTerm{lvl[l]->p, gam[l]});
+      }
+    R.term_count = (uint32_t)terms.size() - R.term_first;
+    if (j + 1 < NR) {
+      TreeDev& t = ftrees[j + 1];
+      t.log_leaves = (uint32_t)(LOG_N_FRI - (j + 1) - 1);
+      t.nodes = std::make_shared<DBuf>((size_t)16 << t.log_leaves, c.stream);
+      R.nodes = t.nodes->p;
+      R.log_leaves = t.log_leaves;
+      R.pre_off = pre_off[j + 1];
+      R.pre_len = pre_len[j + 1];
+      layers[j + 1] = next;
+    }
+    rr.push_back(R);
+    keep.push_back(next);
+    cur = next;
+    n /= 2;
+  }
+  auto rd = upload_vec(c, rr);
+  auto td = upload_vec(c, terms.empty() ? std::vector<AxpyTerm>(1) : terms);
+  double perms = 0;
+  for (auto& R : rr) if (R.nodes) perms += 2.0 * (1u << R.log_leaves);
+  c.timed("fri_tail", 0, perms, [&] {
+    k_fri_tail<<<1, 1024, 0, c.stream>>>((const FriRound*)rd->p, (uint32_t)rr.size(), (uint32_t)j0,
+                                          (const AxpyTerm*)td->p, pre_d->p, chal->p, inv(to_mont(2)));
+    LG_LAUNCH();
+  });
+  running = cur;
+  nj = n;
+  fri_next = NR;
+}
+
 inline void Prover::read_final_poly() {
   if (fri_next != NR) throw Error(LG_ERR_INVALID, "the FRI rounds are not all folded yet");
   final_poly.assign(6 * nj, 0);
@@ -774,6 +826,12 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
     pre_all.insert(pre_all.end(), pe.begin(), pe.end());
   }
   auto pre_d = upload_vec(c, pre_all.empty() ? std::vector<uint32_t>{0} : pre_all);
+  // the rounds whose next layer has at most fri_tail_leaves leaves run in
+  // one block (k_fri_tail); 0 leaves them to the per-round launches
+  int j_tail = NR;
+  if (c.tune.fri_tail_leaves)
+    for (int j = r0 + 1; j < NR; j++)
+      if (((size_t)1 << (LOG_N_FRI - (j + 1) - 1)) <= c.tune.fri_tail_leaves) { j_tail = j; break; }
   for (int j = r0; j < NR; j++) {
     if (j > r0) {
       c.timed("fri_challenge", 0, 0, [&] {
@@ -782,6 +840,11 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
         LG_LAUNCH();
       });
       chal_ready[j] = 1;
+    }
+    if (j == j_tail) {
+      for (int k = j + 1; k < NR; k++) chal_ready[k] = 1;
+      fri_tail(j, pre_d, pre_off, pre_len);
+      break;
     }
     Digest unused;
     fri_fold_round(j, false, &unused);

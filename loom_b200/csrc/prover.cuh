@@ -1229,6 +1229,9 @@ struct Prover {
   // next layer's commitment; true with its root (read back when read_root)
   bool fri_fold_round(int j, bool read_root, Digest* next_root);
   void read_final_poly();
+  // rounds j0 .. NR - 1 in one block (k_fri_tail), challenge j0 already on
+  // the device; the same layers, trees and challenges as fri_fold_round
+  void fri_tail(int j0, const DBufP& pre_d, const std::vector<uint32_t>& pre_off, const std::vector<uint32_t>& pre_len);
   // query openings at positions (openQueryExt, openCommittedAt) and the
   // canonical encoding of the whole proof
   size_t open_and_encode(const std::vector<uint32_t>& pos, uint8_t* out, size_t out_cap, bool* in_out);

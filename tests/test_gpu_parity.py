@@ -351,10 +351,10 @@ def test_tuning_never_changes_proofs(ctx):
     try:
         for params in ({"merkle_tail": 2, "merkle_subtree": 2, "p2_leaf_min_per_sm": 0, "p2_node_min_per_sm": 0,
                         "p2_inject_min_per_sm": 0, "inject_block": 1024, "leaf_block": 32, "lde_split": 0,
-                        "lde_fwd_threads": 256},
+                        "lde_fwd_threads": 256, "fri_tail_leaves": 0},
                        {"merkle_tail": 1024, "merkle_subtree": 1024, "p2_leaf_min_per_sm": 1 << 20,
                         "p2_node_min_per_sm": 1 << 20, "p2_inject_min_per_sm": 1 << 20, "inject_block": 32,
-                        "leaf_block": 1024, "lde_split": 1, "lde_fwd_threads": 1024},
+                        "leaf_block": 1024, "lde_split": 1, "lde_fwd_threads": 1024, "fri_tail_leaves": 65536},
                        {"merkle_tail": 64, "merkle_subtree": 0, "p2_leaf_min_per_sm": 128,
                         "p2_node_min_per_sm": 512, "inject_block": 32, "leaf_block": 128},
                        {"merkle_tail": 4, "merkle_subtree": 8, "p2_leaf_min_per_sm": 128,
@@ -366,7 +366,8 @@ def test_tuning_never_changes_proofs(ctx):
     finally:
         ctx.apply_tuning(defaults)
     for name, value in (("merkle_tail", 48), ("merkle_tail", 2048), ("merkle_subtree", 1), ("merkle_subtree", 48),
-                        ("leaf_block", 16), ("lde_split", 2), ("lde_fwd_threads", 128), ("no_such", 1)):
+                        ("leaf_block", 16), ("lde_split", 2), ("lde_fwd_threads", 128), ("fri_tail_leaves", 3),
+                        ("no_such", 1)):
         with pytest.raises(LoomError) as e:
             ctx.set_tuning(name, value)
         assert e.value.code == 1
@@ -409,6 +410,22 @@ def test_rs_encode_large(ctx, logn, cols):
     got = ctx.rs_encode(c)
     for i in range(cols):
         assert np.array_equal(got[i], oracle.rs_encode(c[i], 4 << logn)), (logn, i)
+
+
+@pytest.mark.parametrize("tail", [0, 2, 512, 65536])
+def test_fri_tail_block_gives_identical_proofs(ctx, tail):
+    """The last FRI rounds in one block (k_fri_tail) or one launch per step:
+    the same proof, including levels that enter inside the tail (modules of
+    uneven sizes)."""
+    compiled, wit = plonk.build_mixed([12, 5, 9, 7, 4], seed=23)
+    mont = [F.to_mont(w) for w in wit]
+    saved = ctx.get_tuning("fri_tail_leaves")
+    try:
+        ctx.set_tuning("fri_tail_leaves", tail)
+        got = ctx.prove(compiled.words, mont, 20)
+    finally:
+        ctx.set_tuning("fri_tail_leaves", saved)
+    assert got == oracle.prove(compiled.words, mont, 20)
 
 
 def test_lde_launch_shapes_give_identical_results(ctx):
