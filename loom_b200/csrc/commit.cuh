@@ -423,7 +423,8 @@ struct Committed {
 
 // RSCommit.Commit: groups sorted by size (stable, descending); the largest
 // is the leaf level, the others fold in as level injections.
-inline Committed commit(Ctx& c, const std::vector<GroupSpec>& gs, bool keep_coef) {
+// read_root = false leaves the root on the device (tree.nodes[1]), unread.
+inline Committed commit(Ctx& c, const std::vector<GroupSpec>& gs, bool keep_coef, bool read_root = true) {
   if (gs.empty()) throw Error(LG_ERR_INVALID, "commit: empty batch");
   Committed cm;
   for (size_t i = 0; i < gs.size(); i++) {
@@ -487,7 +488,7 @@ inline Committed commit(Ctx& c, const std::vector<GroupSpec>& gs, bool keep_coef
   }
   if (c.batched) launch_leaves(c, lg);
   else for (auto& g : lg) launch_leaves(c, {g});
-  build_tree(c, t);
+  build_tree(c, t, read_root);
   return cm;
 }
 

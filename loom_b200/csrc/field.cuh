@@ -38,6 +38,8 @@ LG_HD uint32_t umin(uint32_t a, uint32_t b) {
 LG_HD uint32_t add(uint32_t a, uint32_t b) { uint32_t s = a + b; return umin(s, s - P); }
 LG_HD uint32_t sub(uint32_t a, uint32_t b) { uint32_t d = a - b; return umin(d, d + P); }
 LG_HD uint32_t neg(uint32_t a) { return a ? P - a : 0; }
+// a - b + p, in (0, 2p) for a, b < p: unreduced, for the first operand of mul
+LG_HD uint32_t sub_lazy(uint32_t a, uint32_t b) { return a + (P - b); }
 // x in [0, 2p) -> [0, p)
 LG_HD uint32_t red(uint32_t x) { return umin(x, x - P); }
 LG_HD uint32_t dbl(uint32_t a) { return add(a, a); }
@@ -110,7 +112,7 @@ LG_HD E2 e2_sub(E2 x, E2 y) { return {sub(x.a0, y.a0), sub(x.a1, y.a1)}; }
 LG_HD uint32_t triple(uint32_t a) { return add(add(a, a), a); }
 LG_HD E2 e2_mul(E2 x, E2 y) {
   uint32_t v0 = mul(x.a0, y.a0), v1 = mul(x.a1, y.a1);
-  uint32_t m = mul(add(x.a0, x.a1), add(y.a0, y.a1));
+  uint32_t m = mul(x.a0 + x.a1, add(y.a0, y.a1));  // first operand unreduced: < 2p
   return {add(v0, triple(v1)), sub(sub(m, v0), v1)};
 }
 // (p + q u)(1 + u) = (p + 3q) + (p + q) u

@@ -571,6 +571,24 @@ struct Transcript {
     if (chs[it->second].done) throw Error(LG_ERR_INVALID, "challenge already computed " + n);
     chs[it->second].bindings.insert(chs[it->second].bindings.end(), v, v + len);
   }
+  // What challenge n will hash, as far as the host has it: the name's
+  // elements, whether a previous challenge exists and whether the host has
+  // computed it (then its digest), and the bindings so far.
+  struct Known { std::vector<uint32_t> name; bool has_prev = false, prev_done = false; Digest prev{}; std::vector<uint32_t> binds; };
+  Known known(const std::string& n) const {
+    auto it = index.find(n);
+    if (it == index.end()) throw Error(LG_ERR_INVALID, "unknown challenge " + n);
+    const size_t i = it->second;
+    Known k;
+    k.name = string_to_elements(0x46534944u, n);
+    if (i) {
+      k.has_prev = true;
+      k.prev_done = chs[i - 1].done;
+      if (k.prev_done) k.prev = chs[i - 1].value;
+    }
+    k.binds = chs[i].bindings;
+    return k;
+  }
   Digest compute(const std::string& n) {
     auto it = index.find(n);
     if (it == index.end()) throw Error(LG_ERR_INVALID, "unknown challenge " + n);

@@ -56,7 +56,7 @@ __device__ void smem_dif(uint32_t* A, int logn, const uint32_t* tw, bool inverse
       uint32_t w = tw_at(tw, j << (logn - s), mask, inverse);
       uint32_t u = A[i0], v = A[i1];
       A[i0] = add(u, v);
-      A[i1] = mul(sub(u, v), w);
+      A[i1] = mul(sub_lazy(u, v), w);
     }
     __syncthreads();
   }
@@ -984,10 +984,13 @@ __global__ void k_eval_base(const EvalJob* jobs, const E6* coins) {
 
 // ---------------------------------------------------------------- claimed values
 // zp[k] = z^k, k < n.
-__global__ void k_e6_powers(E6 z, uint32_t n, uint32_t* zp) {
+__global__ void k_e6_powers(const uint32_t* zw, uint32_t ws, uint32_t n, uint32_t* zp) {
   uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
-  E6 v = e6_pow(z, k);
+  E6 z;
+#pragma unroll
+  for (int w = 0; w < 6; w++) z.c[w] = zw[w];
+  E6 v = e6_pow(e6_mul_base(z, ws), k);
   st6(zp, n, k, v);
 }
 
@@ -1073,12 +1076,19 @@ __global__ void k_deep(const DeepJob* jobs) {
 // ---------------------------------------------------------------- FRI
 // running += sum_t gamma_t * level_t (6 lanes each, lane stride n), the
 // levels entering FRI at this round in level order.
-struct AxpyTerm { const uint32_t* lvl; E6 gamma; };
+// gamma: device words (the first six words of the challenge's digest).
+struct AxpyTerm { const uint32_t* lvl; const uint32_t* gamma; };
+__device__ __forceinline__ E6 ld_e6w(const uint32_t* w) {
+  E6 r;
+#pragma unroll
+  for (int k = 0; k < 6; k++) r.c[k] = w[k];
+  return r;
+}
 __global__ void k_axpy_e6(uint32_t* run, uint64_t n, const AxpyTerm* terms, uint32_t n_terms) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   E6 a = ld6(run, n, i);
-  for (uint32_t t = 0; t < n_terms; t++) a = e6_add(a, e6_mul(ld6(terms[t].lvl, n, i), terms[t].gamma));
+  for (uint32_t t = 0; t < n_terms; t++) a = e6_add(a, e6_mul(ld6(terms[t].lvl, n, i), ld_e6w(terms[t].gamma)));
   st6(run, n, i, a);
 }
 
@@ -1152,7 +1162,7 @@ __global__ void __launch_bounds__(1024) k_fri_tail(const FriRound* rounds, uint3
         E6 v = e6_add(sm, d);
         for (uint32_t t = 0; t < R.term_count; t++) {
           const AxpyTerm T = terms[R.term_first + t];
-          v = e6_add(v, e6_mul(ld6(T.lvl, half, i), T.gamma));
+          v = e6_add(v, e6_mul(ld6(T.lvl, half, i), ld_e6w(T.gamma)));
         }
         st6(R.next, half, i, v);
       }
@@ -1250,6 +1260,70 @@ __global__ void k_fs_challenge(const uint32_t* pre, uint32_t n_pre, const uint32
   if (L.lane < 2)
 #pragma unroll
     for (int k = 0; k < 4; k++) out[4 * L.lane + k] = x[k];
+}
+
+// A chain of Fiat-Shamir challenges on the device, computed in order:
+// challenge i hashes msg[moff, moff + total) as k_fs_challenge does and
+// writes its 8 digest words to `out`.  The message words come from segments
+// — host constants uploaded with the descriptors (names' elements, known
+// bindings) and words already in device memory (roots, exposed values, the
+// digest of a challenge computed by an earlier launch) — all read up front,
+// one segment per thread at a time; a digest that the next challenge of the
+// same chain hashes is forwarded from registers to msg[fwd] instead.  One
+// warp, six lanes per permutation; the chain's messages hold at most
+// FS_MAX_MSG words (checked by the host).
+constexpr uint32_t FS_MAX_MSG = 4096;
+struct FsSeg { const uint32_t* src; uint32_t len, off; };
+struct FsChal { uint32_t moff, total; uint32_t* out; int32_t fwd; };
+__global__ void __launch_bounds__(32) k_fs_chain(const FsChal* chals, uint32_t n_chals, const FsSeg* segs,
+                                                 uint32_t n_segs) {
+  __shared__ uint32_t keys[144];
+  __shared__ uint32_t msg[FS_MAX_MSG];
+  for (uint32_t s = threadIdx.x; s < n_segs; s += blockDim.x) {
+    const FsSeg sg = segs[s];
+    for (uint32_t k = 0; k < sg.len; k++) msg[sg.off + k] = sg.src[k];
+  }
+  p2_load_full_keys(keys);  // ends with a barrier
+  P2Lane L;
+  L.init();
+  for (uint32_t i = 0; i < n_chals; i++) {
+    const FsChal ch = chals[i];
+    uint32_t x[4] = {0, 0, 0, 0};
+    for (uint32_t b = 0; b < ch.total; b += 16) {
+      const uint32_t len = min(16u, ch.total - b);  // words 0..len of the state are overwritten
+      if (L.idx < 4)
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+          if (4 * (uint32_t)L.idx + k < len) x[k] = msg[ch.moff + b + 4 * L.idx + k];
+      p2c_permute(x, L, keys);
+    }
+    if (L.lane < 2)
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        ch.out[4 * L.lane + k] = x[k];
+        if (ch.fwd >= 0) msg[ch.fwd + 4 * L.lane + k] = x[k];
+      }
+    __syncwarp();
+  }
+}
+
+// The challenge table of the step and quotient kernels: the round coins (the
+// first six words of each digest slot, slot stride 8), then the exposed
+// values times ninv[e] (1/n of the producing module; 0 while entry e is not
+// produced yet, which zeroes it) and the exposed values themselves.
+__global__ void k_coins_assemble(const uint32_t* slots, uint32_t n_coins, const uint32_t* exposed,
+                                 const uint32_t* ninv, uint32_t n_exp, uint32_t* out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t nc = 6 * n_coins, ne = 6 * n_exp;
+  if (i < nc) {
+    out[i] = slots[8 * (i / 6) + i % 6];
+  } else if (i < nc + ne) {
+    const uint32_t k = i - nc, f = ninv[k / 6];
+    out[i] = f ? mul(exposed[k], f) : 0u;
+  } else if (i < nc + 2 * ne) {
+    const uint32_t k = i - nc - ne;
+    out[i] = ninv[k / 6] ? exposed[k] : 0u;
+  }
 }
 
 // ---------------------------------------------------------------- openings

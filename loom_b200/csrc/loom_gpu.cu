@@ -396,8 +396,7 @@ int lg_committed_eval(lg_ctx* ctx, const lg_committed* batch, const uint32_t zet
     if (h->ctx != ctx) throw Error(LG_ERR_INVALID, "handle belongs to another context");
     Ctx& c = ctx->c;
     ArenaScope arena(&c.dev_arena);
-    E6 z;
-    for (int k = 0; k < 6; k++) z.c[k] = zeta[k];
+    auto zd = upload_vec(c, std::vector<uint32_t>(zeta, zeta + 6));
     std::vector<DotJob> jobs;
     std::vector<DBufP> keep;
     std::map<std::pair<uint32_t, int32_t>, const uint32_t*> zp;
@@ -409,9 +408,9 @@ int lg_committed_eval(lg_ctx* ctx, const lg_committed* batch, const uint32_t zet
         auto key = std::make_pair(l.log_n, shifts[si]);
         if (!zp.count(key)) {
           const int64_t e = ((int64_t)shifts[si] % (int64_t)n + (int64_t)n) % (int64_t)n;
-          E6 zs = e6_mul_base(z, mont_pow(root_of_unity_mont((int)l.log_n), (uint64_t)e));
+          const uint32_t ws = mont_pow(root_of_unity_mont((int)l.log_n), (uint64_t)e);
           auto b = std::make_shared<DBuf>(6 * n, c.stream);
-          k_e6_powers<<<(unsigned)((n + 127) / 128), 128, 0, c.stream>>>(zs, (uint32_t)n, b->p);
+          k_e6_powers<<<(unsigned)((n + 127) / 128), 128, 0, c.stream>>>(zd->p, ws, (uint32_t)n, b->p);
           LG_LAUNCH();
           keep.push_back(b);
           zp[key] = b->p;

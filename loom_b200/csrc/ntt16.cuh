@@ -135,7 +135,7 @@ __device__ __forceinline__ void stage16(uint32_t v[16], uint32_t t, int lo, int 
       if (DIF) {
         uint32_t u = a, x = b;
         a = add(u, x);
-        b = unit ? sub(u, x) : mul(sub(u, x), w[rl]);
+        b = unit ? sub(u, x) : mul(sub_lazy(u, x), w[rl]);
       } else {
         uint32_t u = a, x = unit ? b : mul(b, w[rl]);
         a = add(u, x);

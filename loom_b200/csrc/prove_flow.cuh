@@ -186,6 +186,11 @@ inline void Prover::begin(const uint32_t* const* witness, bool on_device) {
   setup(witness, on_device);
   coins.assign(pg.n_rounds, e6_zero());
   coin_ready.assign(pg.n_rounds, 0);
+  fs_slots = std::make_shared<DBuf>(8 * ((size_t)pg.n_rounds + 2), c.stream);
+  LG_CK(cudaMemsetAsync(fs_slots->p, 0, 32 * ((size_t)pg.n_rounds + 2), c.stream));
+  dev_fs = false;
+  pending_roots.clear();
+  pending_coins.clear();
   tree_next = 0;
   // the precommitted setup tree (prover/prover.go:175-229): its root binds
   // to the first challenge and stays out of the proof's commitments
@@ -202,9 +207,15 @@ inline void Prover::set_challenge(const std::string& name, const uint32_t* d) {
     if (name == coin_name(r)) {
       coins[r] = e;
       coin_ready[r] = 1;
+      c.h2d(fs_slot(r), d, 32);
       return;
     }
-  if (name == "__zeta") { zeta = e; zeta_ready = true; return; }
+  if (name == "__zeta") {
+    zeta = e;
+    zeta_ready = true;
+    c.h2d(fs_slot(pg.n_rounds), d, 32);
+    return;
+  }
   if (name == "alpha_DEEP") { alpha = e; alpha_ready = true; return; }
   const std::string lp = "fri_level_", fp = "fri_fold_";
   if (name.compare(0, lp.size(), lp) == 0 && name.size() > lp.size() + 6 &&
@@ -214,6 +225,7 @@ inline void Prover::set_challenge(const std::string& name, const uint32_t* d) {
     if (l < 1 || l >= L) throw Error(LG_ERR_INVALID, "no FRI level for " + name);
     gam[l] = e;
     gam_ready[l] = 1;
+    c.h2d(gam_d->p + 8 * l, d, 32);
     return;
   }
   if (name.compare(0, fp.size(), fp) == 0 && name.size() > fp.size()) {
@@ -234,13 +246,19 @@ inline bool Prover::commit_round(uint32_t r, Digest* root) {
   run_steps(r);
   bool has = false;
   if (tree_next < trees.size() && !trees[tree_next].air && trees[tree_next].round == (int)r) {
-    committed.push_back(commit_tree(trees[tree_next]));
-    *root = committed.back().tree.root;
+    committed.push_back(commit_tree(trees[tree_next], !dev_fs));
+    if (dev_fs) pending_roots.push_back({commitments.size(), committed.size() - 1});
+    *root = committed.back().tree.root;  // zeros while pending
     commitments.push_back(*root);
     tree_next++;
     has = true;
   }
-  read_exposed(r);
+  if (dev_fs) {  // the values stay on the device until sync_transcript
+    for (const Step& st : pg.steps)
+      if (st.round == r && exposes(st.type)) exposed_ready[st.exposed] = 1;
+  } else {
+    read_exposed(r);
+  }
   return has;
 }
 
@@ -258,7 +276,8 @@ inline bool Prover::commit_quotient(Digest* root) {
     throw Error(LG_ERR_INVALID, "the rounds are not all committed yet");
   quotient_all();
   if (tree_next < trees.size() && trees[tree_next].air) {
-    committed.push_back(commit_tree(trees[tree_next]));
+    committed.push_back(commit_tree(trees[tree_next], !dev_fs));
+    if (dev_fs) pending_roots.push_back({commitments.size(), committed.size() - 1});
     *root = committed.back().tree.root;
     commitments.push_back(*root);
     tree_next++;
@@ -301,10 +320,11 @@ inline void Prover::claimed_values() {
           auto key = std::make_pair(p.logn, s);
           if (!zp.count(key)) {
             uint32_t n = 1u << p.logn;
-            E6 z = e6_mul_base(zeta, mont_pow(root_of_unity_mont((int)p.logn), (uint64_t)s));
+            // zeta w^s with zeta read from its device slot
+            const uint32_t ws = mont_pow(root_of_unity_mont((int)p.logn), (uint64_t)s);
             auto b = std::make_shared<DBuf>(6 * (size_t)n, c.stream);
             c.timed("claimed_values", 0, 0, [&] {
-              k_e6_powers<<<(n + 127) / 128, 128, 0, c.stream>>>(z, n, b->p);
+              k_e6_powers<<<(n + 127) / 128, 128, 0, c.stream>>>(fs_slot(pg.n_rounds), ws, n, b->p);
               LG_LAUNCH();
             });
             zp[key] = b;
@@ -480,9 +500,10 @@ inline Digest Prover::commit_levels() {
     if (c.batched) launch_leaves(c, lgs);
     else for (auto& g : lgs) launch_leaves(c, {g});
   }
-  build_tree(c, levels_tree);
+  build_tree(c, levels_tree, !dev_fs);  // dev_fs: the root is read back after the FRI rounds
   gam.assign(L, e6_zero());
   gam_ready.assign(L, 0);
+  gam_d = std::make_shared<DBuf>(8 * L, c.stream);
   layers.assign(NR + 1, nullptr);
   ftrees.assign(NR, TreeDev());
   fri_roots.clear();
@@ -505,7 +526,7 @@ inline bool Prover::fri_fold_round(int j, bool read_root, Digest* next_root) {
     for (size_t l = 1; l < L; l++)
       if (jl(l) == round) {
         if (!gam_ready[l]) throw Error(LG_ERR_INVALID, "challenge fri_level_" + std::to_string(l) + "_gamma has not been set");
-        terms.push_back(AxpyTerm{lvl[l]->p, gam[l]});
+        terms.push_back(AxpyTerm{lvl[l]->p, gam_d->p + 8 * l});
       }
     auto axpy = [&](const std::vector<AxpyTerm>& tv) {
       auto td = upload_vec(c, tv);
@@ -572,7 +593,7 @@ inline void Prover::fri_tail(int j0, const DBufP& pre_d, const std::vector<uint3
     for (size_t l = 1; l < L; l++)
       if (jl(l) == j + 1) {
         if (!gam_ready[l]) throw Error(LG_ERR_INVALID, "challenge fri_level_" + std::to_string(l) + "_gamma has not been set");
-        terms.push_back(AxpyTerm{lvl[l]->p, gam[l]});
+        terms.push_back(AxpyTerm{lvl[l]->p, gam_d->p + 8 * l});
       }
     R.term_count = (uint32_t)terms.size() - R.term_first;
     if (j + 1 < NR) {
@@ -742,6 +763,104 @@ inline size_t Prover::open_and_encode(const std::vector<uint32_t>& pos, uint8_t*
   return W.length();
 }
 
+// ---- the device transcript
+inline bool Prover::fs_queue(FsQueue& q, const std::string& name, const uint32_t* prev_dev, const DevWords& dev,
+                             uint32_t* out) {
+  const Transcript::Known k = fs.known(name);
+  size_t total = k.name.size() + (k.has_prev ? 8 : 0) + k.binds.size();
+  for (auto& d : dev) total += d.second;
+  if (total > FS_MAX_MSG) return false;
+  if (q.words + total > FS_MAX_MSG) fs_launch(q);  // that chain's digests are then in device memory
+  uint32_t pos = q.words;
+  auto host = [&](const uint32_t* v, size_t n) {
+    if (!n) return;
+    q.segs.push_back({nullptr, q.consts.size(), (uint32_t)n, pos});
+    q.consts.insert(q.consts.end(), v, v + n);
+    pos += (uint32_t)n;
+  };
+  auto device = [&](const uint32_t* p, uint32_t n) {
+    q.segs.push_back({p, 0, n, pos});
+    pos += n;
+  };
+  host(k.name.data(), k.name.size());
+  if (k.has_prev) {
+    if (k.prev_done) {
+      host(k.prev.v, 8);
+    } else if (prev_dev && !q.chs.empty() && q.chs.back().out == prev_dev) {
+      q.chs.back().fwd = (int32_t)pos;  // forwarded from the previous challenge of the chain
+      pos += 8;
+    } else if (prev_dev) {
+      device(prev_dev, 8);
+    } else {
+      throw Error(LG_ERR_INVALID, "device transcript: the challenge before " + name + " is not computed");
+    }
+  }
+  host(k.binds.data(), k.binds.size());
+  for (auto& d : dev) device(d.first, d.second);
+  q.chs.push_back(FsChal{q.words, (uint32_t)total, out, -1});
+  q.words += (uint32_t)total;
+  return true;
+}
+
+inline void Prover::fs_launch(FsQueue& q) {
+  if (q.chs.empty()) return;
+  auto cd = upload_vec(c, q.consts.empty() ? std::vector<uint32_t>{0} : q.consts);
+  std::vector<FsSeg> segs;
+  for (auto& sg : q.segs) segs.push_back(FsSeg{sg.dev ? sg.dev : cd->p + sg.off, sg.len, sg.moff});
+  auto sd = upload_vec(c, segs.empty() ? std::vector<FsSeg>(1) : segs);
+  auto hd = upload_vec(c, q.chs);
+  c.timed("fs_chain", 0, 0, [&] {
+    k_fs_chain<<<1, 32, 0, c.stream>>>((const FsChal*)hd->p, (uint32_t)q.chs.size(), (const FsSeg*)sd->p,
+                                       (uint32_t)segs.size());
+    LG_LAUNCH();
+  });
+  q.chs.clear();
+  q.segs.clear();
+  q.consts.clear();
+  q.words = 0;
+}
+
+inline void Prover::sync_transcript() {
+  const uint32_t R = pg.n_rounds;
+  const size_t X = exposed_d ? n_exposed() : 0, np = pending_roots.size();
+  uint32_t* h = c.host_staging(8 * np + 6 * X + 8 * ((size_t)R + 1));
+  for (size_t i = 0; i < np; i++)
+    LG_CK(cudaMemcpyAsync(h + 8 * i, committed[pending_roots[i].tree].tree.nodes->p + 8, 32, cudaMemcpyDeviceToHost,
+                          c.stream));
+  if (X) LG_CK(cudaMemcpyAsync(h + 8 * np, exposed_d->p, 24 * X, cudaMemcpyDeviceToHost, c.stream));
+  uint32_t* slots = h + 8 * np + 6 * X;
+  LG_CK(cudaMemcpyAsync(slots, fs_slots->p, 32 * ((size_t)R + 1), cudaMemcpyDeviceToHost, c.stream));
+  LG_CK(cudaStreamSynchronize(c.stream));
+  for (size_t i = 0; i < np; i++) {
+    Digest d;
+    memcpy(d.v, h + 8 * i, 32);
+    commitments[pending_roots[i].commitment] = d;
+    committed[pending_roots[i].tree].tree.root = d;
+  }
+  for (const Step& st : pg.steps)
+    if (exposes(st.type) && exposed_ready[st.exposed] && X)
+      for (int w = 0; w < 6; w++) exposed[st.exposed].c[w] = h[8 * np + 6 * st.exposed + w];
+  for (const PendingCoin& pc : pending_coins) {
+    const std::string nm = pc.round < R ? coin_name(pc.round) : std::string("__zeta");
+    if (pc.commitment >= 0) fs.bind(nm, commitments[pc.commitment].v, 8);
+    if (pc.round < R)
+      for (const E6& e : round_exposed(pc.round)) {  // entry index, then the value
+        uint32_t w[7] = {0};
+        for (int k = 0; k < 6; k++) w[1 + k] = e.c[k];
+        fs.bind(nm, w, 7);
+      }
+    const Digest d = fs.compute(nm);
+    if (memcmp(d.v, slots + 8 * (size_t)pc.round, 32) != 0)
+      throw Error(LG_ERR_CUDA, "device and host transcripts disagree at " + nm);
+    E6 e;
+    for (int k = 0; k < 6; k++) e.c[k] = d.v[k];
+    if (pc.round < R) coins[pc.round] = e;
+    else zeta = e;
+  }
+  pending_roots.clear();
+  pending_coins.clear();
+}
+
 // ---- the whole prove with the host transcript (prover/prover.go:655-719)
 inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint8_t* out, size_t out_cap,
                             bool* in_out) {
@@ -761,10 +880,49 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
     fs.bind(first, sz.data(), sz.size());
   }
   if (has_setup_tree()) fs.bind(coin_name(0), prog->setup->root.v, 8);
+  // The round coins and zeta come from the device transcript (k_fs_chain)
+  // over the roots and exposed values where the commits left them: the host
+  // queues every phase up to the claimed values without waiting for the
+  // device, then replays those challenges (sync_transcript).  A message too
+  // long for k_fs_chain switches back to the host transcript.
+  dev_fs = true;
+  FsQueue q;
+  auto to_host = [&] {
+    if (!dev_fs) return;
+    sync_transcript();
+    dev_fs = false;
+  };
   // ---- rounds: steps, commit, bind root, sample coin (prover/prover.go:360-411)
+  // Queued challenges run as one chain right before the first kernel that
+  // reads them: a round's steps, the quotient, the claimed values.
+  auto round_has_steps = [&](uint32_t r) {
+    for (const Step& st : pg.steps) if (st.round == r) return true;
+    return false;
+  };
   for (uint32_t r = 0; r < R; r++) {
     Digest root;
-    if (commit_round(r, &root)) fs.bind(coin_name(r), root.v, 8);
+    const size_t ci = commitments.size();
+    if (round_has_steps(r)) fs_launch(q);
+    const bool has = commit_round(r, &root);
+    if (dev_fs) {
+      DevWords dv;
+      if (has) dv.push_back({committed.back().tree.nodes->p + 8, 8});
+      for (const Step& st : pg.steps)  // exposed values: entry index 0, then six words
+        if (st.round == r && exposes(st.type)) {
+          dv.push_back({fs_slot(R + 1), 1});
+          dv.push_back({exposed_d->p + 6 * (size_t)st.exposed, 6});
+        }
+      if (fs_queue(q, coin_name(r), r ? fs_slot(r - 1) : nullptr, dv, fs_slot(r))) {
+        pending_coins.push_back({r, has ? (int)ci : -1});
+        coin_ready[r] = 1;
+        c.phase(("round " + std::to_string(r)).c_str());
+        continue;
+      }
+      fs_launch(q);
+      to_host();
+      if (has) root = commitments[ci];
+    }
+    if (has) fs.bind(coin_name(r), root.v, 8);
     // BindExposedValues (prover/prover.go:386-396): the round's logup totals
     // in step order, each as its entry index then six elements
     // (board/logup.go:218-225)
@@ -779,12 +937,33 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
   // ---- AIR quotients and their commitment
   {
     Digest root;
-    if (commit_quotient(&root)) fs.bind("__zeta", root.v, 8);
+    const size_t ci = commitments.size();
+    fs_launch(q);
+    const bool has = commit_quotient(&root);
+    bool queued = false;
+    if (dev_fs) {
+      DevWords dv;
+      if (has) dv.push_back({committed.back().tree.nodes->p + 8, 8});
+      if (fs_queue(q, "__zeta", R ? fs_slot(R - 1) : nullptr, dv, fs_slot(R))) {
+        fs_launch(q);
+        pending_coins.push_back({R, has ? (int)ci : -1});
+        zeta_ready = true;
+        queued = true;
+      } else {
+        to_host();
+        if (has) root = commitments[ci];
+      }
+    }
+    if (!queued) {
+      if (has) fs.bind("__zeta", root.v, 8);
+      set_challenge("__zeta", fs.compute("__zeta").v);
+    }
   }
-  set_challenge("__zeta", fs.compute("__zeta").v);
   c.phase("quotient+air commit");
   // ---- claimed values and alpha_DEEP
   claimed_values();
+  to_host();  // the claimed values are read back: replay the device's challenges
+  dev_fs = true;  // the FRI levels' challenges again come from the device
   c.phase("claimed values");
   fs.add("alpha_DEEP");
   for (const E6& v : claimed_values_bind_order()) fs.bind("alpha_DEEP", v.c, 6);
@@ -798,17 +977,47 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
   for (size_t l = 1; l < L; l++) fs.add("fri_level_" + std::to_string(l) + "_gamma");
   for (int j = 0; j < NR; j++) fs.add("fri_fold_" + std::to_string(j));
   for (uint32_t k = 0; k < num_queries; k++) fs.add("fri_query_" + std::to_string(k));
-  for (size_t l = 1; l < L; l++) {
-    std::string nm = "fri_level_" + std::to_string(l) + "_gamma";
-    if (l == 1) fs.bind(nm, lroot.v, 8);
-    set_challenge(nm, fs.compute(nm).v);
-  }
   Digest zero{};
-  for (int j = 0; j < r0; j++) {
-    fs.bind("fri_fold_" + std::to_string(j), zero.v, 8);
-    fs.compute("fri_fold_" + std::to_string(j));
-  }
-  {
+  if (dev_fs) {
+    // the level weights and the folds up to the first layer's, chained on
+    // the device from the levels root where the tree left it; replayed with
+    // the layer roots' challenges after the rounds
+    const uint32_t* lroot_d = levels_tree.nodes->p + 8;
+    const uint32_t* prev = nullptr;  // alpha_DEEP: on the host
+    for (size_t l = 1; l < L; l++) {
+      uint32_t* out = gam_d->p + 8 * l;
+      if (!fs_queue(q, "fri_level_" + std::to_string(l) + "_gamma", prev,
+                    l == 1 ? DevWords{{lroot_d, 8}} : DevWords{}, out))
+        throw Error(LG_ERR_UNSUPPORTED, "level weight message too long");
+      gam_ready[l] = 1;
+      prev = out;
+    }
+    fold_dev.assign(r0 + 1, 0);
+    for (int j = 0; j <= r0; j++) {
+      const std::string nm = "fri_fold_" + std::to_string(j);
+      if (j < r0) fs.bind(nm, zero.v, 8);
+      if (j < r0 && !prev) {  // nothing from the device in the chain yet: the host has it
+        fs.compute(nm);
+        continue;
+      }
+      fold_dev[j] = 1;
+      uint32_t* out = chal->p + 8 * (size_t)j;
+      if (!fs_queue(q, nm, prev, j == r0 ? DevWords{{lroot_d, 8}} : DevWords{}, out))
+        throw Error(LG_ERR_UNSUPPORTED, "fold challenge message too long");
+      prev = out;
+    }
+    chal_ready[r0] = 1;
+    fs_launch(q);
+  } else {
+    for (size_t l = 1; l < L; l++) {
+      std::string nm = "fri_level_" + std::to_string(l) + "_gamma";
+      if (l == 1) fs.bind(nm, lroot.v, 8);
+      set_challenge(nm, fs.compute(nm).v);
+    }
+    for (int j = 0; j < r0; j++) {
+      fs.bind("fri_fold_" + std::to_string(j), zero.v, 8);
+      fs.compute("fri_fold_" + std::to_string(j));
+    }
     const std::string nm = "fri_fold_" + std::to_string(r0);
     fs.bind(nm, lroot.v, 8);
     set_challenge(nm, fs.compute(nm).v);
@@ -852,15 +1061,41 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
   {
     // one read-back: final polynomial, device challenges, layer roots
     const size_t nroot = (size_t)(NR > r0 + 1 ? NR - r0 - 1 : 0);
-    uint32_t* h = c.host_staging(6 * nj + 8 * (size_t)NR + 8 * nroot);
+    uint32_t* h = c.host_staging(6 * nj + 8 * (size_t)NR + 8 * nroot + 8 + 8 * L);
     LG_CK(cudaMemcpyAsync(h, running->p, 6 * nj * 4, cudaMemcpyDeviceToHost, c.stream));
     LG_CK(cudaMemcpyAsync(h + 6 * nj, chal->p, 8 * (size_t)NR * 4, cudaMemcpyDeviceToHost, c.stream));
     for (int j = r0 + 1; j < NR; j++)
       LG_CK(cudaMemcpyAsync(h + 6 * nj + 8 * (size_t)NR + 8 * (size_t)(j - r0 - 1), ftrees[j].nodes->p + 8, 32,
                             cudaMemcpyDeviceToHost, c.stream));
+    uint32_t* hl = h + 6 * nj + 8 * (size_t)NR + 8 * nroot;  // levels root, then the level weights
+    if (dev_fs) {
+      LG_CK(cudaMemcpyAsync(hl, levels_tree.nodes->p + 8, 32, cudaMemcpyDeviceToHost, c.stream));
+      LG_CK(cudaMemcpyAsync(hl + 8, gam_d->p, 32 * L, cudaMemcpyDeviceToHost, c.stream));
+    }
     LG_CK(cudaStreamSynchronize(c.stream));
     final_poly.assign(6 * nj, 0);
     memcpy(final_poly.data(), h, 6 * nj * 4);
+    if (dev_fs) {  // replay the level weights and the folds up to r0
+      memcpy(levels_tree.root.v, hl, 32);
+      ftrees[r0].root = levels_tree.root;
+      auto check = [&](const std::string& nm, const uint32_t* dev) {
+        const Digest d = fs.compute(nm);
+        if (memcmp(d.v, dev, 32) != 0) throw Error(LG_ERR_CUDA, "device and host transcripts disagree at " + nm);
+        return d;
+      };
+      for (size_t l = 1; l < L; l++) {
+        const std::string nm = "fri_level_" + std::to_string(l) + "_gamma";
+        if (l == 1) fs.bind(nm, levels_tree.root.v, 8);
+        gam[l] = digest_e6(check(nm, hl + 8 + 8 * l));
+      }
+      for (int j = 0; j <= r0; j++) {
+        if (!fold_dev[j]) continue;
+        const std::string nm = "fri_fold_" + std::to_string(j);
+        if (j == r0) fs.bind(nm, levels_tree.root.v, 8);
+        check(nm, h + 6 * nj + 8 * (size_t)j);
+      }
+      dev_fs = false;
+    }
     fri_roots.clear();
     for (int j = r0 + 1; j < NR; j++) {
       Digest root;

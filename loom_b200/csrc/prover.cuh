@@ -74,6 +74,30 @@ struct Prover {
   std::vector<Digest> commitments;
   std::map<uint32_t, DBufP> chunk_coef;  // module -> chunks (d * lanes + w) * n
   E6 zeta;
+  // Device copies of the challenges the kernels read: slot r (8 words) for
+  // round coin r, slot n_rounds for __zeta.  With dev_fs (the whole prove,
+  // lg_prove) the device computes them itself from roots and exposed values
+  // still in device memory (k_fs_chain), and the host transcript replays and
+  // checks them at the next read-back (sync_transcript); otherwise
+  // set_challenge uploads the caller's values.
+  // Slot n_rounds + 1 holds zeros (the entry-index word of exposed bindings).
+  DBufP fs_slots;
+  bool dev_fs = false;
+  struct PendingRoot { size_t commitment, tree; };      // root still on the device
+  struct PendingCoin { uint32_t round; int commitment; };  // round n_rounds: __zeta
+  std::vector<PendingRoot> pending_roots;
+  std::vector<PendingCoin> pending_coins;
+  uint32_t* fs_slot(uint32_t k) const { return fs_slots->p + 8 * (size_t)k; }
+  // challenges queued for the device (k_fs_chain)
+  struct FsQueue {
+    struct Seg { const uint32_t* dev; size_t off; uint32_t len, moff; };  // dev null: consts[off, off + len)
+    std::vector<uint32_t> consts;
+    std::vector<Seg> segs;
+    std::vector<FsChal> chs;
+    uint32_t words = 0;  // message words of the queued challenges
+  };
+  using DevWords = std::vector<std::pair<const uint32_t*, uint32_t>>;
+  std::vector<char> fold_dev;               // fold challenges up to r0 the device computed (lg_prove)
 
   ProgCache* prog = nullptr;  // compiled code of this program, kept on the context
   std::shared_ptr<ProgCache> prog_keep;  // ... and alive while this prove lasts
@@ -95,6 +119,7 @@ struct Prover {
   std::vector<DBufP> lvl;
   TreeDev levels_tree;
   std::vector<E6> gam;                      // level weights (gam[0] unused)
+  DBufP gam_d;                              // their device slots (8 words each)
   std::vector<char> gam_ready;
   std::vector<DBufP> layers;                // layer j (E6 lanes), r0 <= j < NR
   std::vector<TreeDev> ftrees;
@@ -516,18 +541,24 @@ struct Prover {
   // Round coins, then per exposed value its average value / N (N: the size of
   // the exposing step's module), then the exposed values themselves, as E6
   // Montgomery words.
+  // The kernels' challenge table, assembled on the device from the coin
+  // slots and the exposed values (k_coins_assemble): no host round trip, so
+  // it works the same whether the coins came from the host transcript or
+  // from the device's (fs_slots).
   DBufP coins_on_device() {
-    std::vector<uint32_t> w;
-    for (auto& e : coins) for (int i = 0; i < 6; i++) w.push_back(e.c[i]);
-    std::vector<E6> avg(n_exposed(), e6_zero()), val(n_exposed(), e6_zero());
-    for (const Step& st : pg.steps) {
-      if (!exposes(st.type) || !exposed_ready[st.exposed]) continue;
-      val[st.exposed] = exposed[st.exposed];
-      avg[st.exposed] = e6_mul_base(exposed[st.exposed], inv(to_mont((uint32_t)mod_n(st.module))));
+    const uint32_t R = pg.n_rounds, X = (uint32_t)n_exposed();
+    std::vector<uint32_t> ninv(std::max<uint32_t>(X, 1), 0);
+    for (const Step& st : pg.steps)
+      if (exposes(st.type) && exposed_ready[st.exposed]) ninv[st.exposed] = inv(to_mont((uint32_t)mod_n(st.module)));
+    auto nd = upload_vec(c, ninv);
+    const size_t words = 6 * ((size_t)R + 2 * (size_t)X);
+    auto out = std::make_shared<DBuf>(std::max<size_t>(words, 1), c.stream);
+    if (words) {
+      k_coins_assemble<<<(unsigned)((words + 255) / 256), 256, 0, c.stream>>>(
+          fs_slots->p, R, exposed_d ? exposed_d->p : nd->p, nd->p, X, out->p);
+      LG_LAUNCH();
     }
-    for (auto& e : avg) for (int i = 0; i < 6; i++) w.push_back(e.c[i]);
-    for (auto& e : val) for (int i = 0; i < 6; i++) w.push_back(e.c[i]);
-    return upload_vec(c, w);
+    return out;
   }
 
   // ------------------------------------------------------------ steps
@@ -920,7 +951,7 @@ struct Prover {
   }
 
   // ------------------------------------------------------------ commits
-  Committed commit_tree(const TreeL& t) {
+  Committed commit_tree(const TreeL& t, bool read_root = true) {
     std::vector<GroupSpec> gs;
     for (const Group& g : t.groups) {
       GroupSpec s;
@@ -941,7 +972,7 @@ struct Prover {
       }
       gs.push_back(s);
     }
-    Committed cm = commit(c, gs, !t.air);
+    Committed cm = commit(c, gs, !t.air, read_root);
     if (!t.air) {
       for (size_t gi = 0; gi < t.groups.size(); gi++) {
         const Group& g = t.groups[gi];
@@ -1239,6 +1270,17 @@ struct Prover {
   // the digest's first six words), alpha_DEEP, fri_level_<l>_gamma,
   // fri_fold_<j> (the whole digest)
   void set_challenge(const std::string& name, const uint32_t* digest);
+  // Device transcript (dev_fs): appends challenge `name` to q — the words
+  // the host transcript already has for it, the previous challenge's digest
+  // from prev_dev when the host does not have it yet, then `dev` (device
+  // words, in order) — with its digest going to `out`; false when the
+  // message is longer than k_fs_chain takes.
+  bool fs_queue(FsQueue& q, const std::string& name, const uint32_t* prev_dev, const DevWords& dev, uint32_t* out);
+  void fs_launch(FsQueue& q);
+  // Reads back the pending roots, the exposed values and the coin and zeta
+  // slots, and replays the pending challenges on the host transcript; each
+  // digest must equal the device's.
+  void sync_transcript();
   void need_coins(uint32_t r) const {
     for (uint32_t k = 0; k < r; k++)
       if (!coin_ready[k]) throw Error(LG_ERR_INVALID, "challenge " + coin_name(k) + " has not been set");
