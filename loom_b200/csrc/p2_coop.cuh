@@ -62,8 +62,11 @@ __device__ __forceinline__ void p2c_permute(uint32_t x[4], const P2Lane& L, cons
 #pragma unroll
   for (int r = 0; r < 3; r++) p2c_full(x, L, smem_keys + 24 * r);
   // Partial rounds as p2_partial_rounds: R = s_1 + ... + s_23 is carried,
-  // the group sum of d_i s_i runs while lane idx 0 computes the S-box, and
-  // only the S-box output crosses lanes on the dependent chain.
+  // and every lane of the group carries its own copy of s_0 (the same
+  // values in all six), so the S-box output needs no broadcast: a round's
+  // dependent chain is the S-box and two additions, while the group sum of
+  // d_i s_i for the next R runs beside it.
+  uint32_t s0 = __shfl_sync(0xffffffffu, x[0], L.base & 31);
   uint32_t R = L.allreduce(add(add(L.idx ? x[0] : 0u, x[1]), add(x[2], x[3])));
 #pragma unroll 3
   for (int r = 0; r < 21; r++) {
@@ -71,10 +74,10 @@ __device__ __forceinline__ void p2c_permute(uint32_t x[4], const P2Lane& L, cons
 #pragma unroll
     for (int i = 0; i < 4; i++) p[i] = mulc(x[i], L.dw[i], L.dws[i]);
     const uint32_t D = L.allreduce(add(add(L.idx ? p[0] : 0u, p[1]), add(p[2], p[3])));
-    const uint32_t u = p2_cube(add(x[0], P2_PARTIAL_RK_D[r]));  // meaningful in lane idx 0
-    const uint32_t sum = add(__shfl_sync(0xffffffffu, u, L.base & 31), R);
-    const uint32_t pu = mulc(u, L.dw[0], L.dws[0]);
-    x[0] = add(sum, L.idx ? p[0] : pu);
+    const uint32_t u = p2_cube(add(s0, P2_PARTIAL_RK_D[r]));
+    const uint32_t sum = add(u, R);
+    s0 = add(sum, mulc(u, P2_DSH_D.w[0], P2_DSH_D.ws[0]));
+    x[0] = L.idx ? add(sum, p[0]) : s0;
 #pragma unroll
     for (int i = 1; i < 4; i++) x[i] = sum + p[i];  // unreduced in [0, 2p) until the next product
     R = add(mulc(sum, C23, C23_SH), D);
