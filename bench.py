@@ -44,6 +44,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sweep", action="store_true",
                     help="kernel roofline sweep (LDE, Merkle commit, FRI fold, DEEP) instead of the prove bench")
+    ap.add_argument("--sweep-only", type=str, default="",
+                    help="comma-separated sweep items to run: lde, commit, fold, deep, or one size as kind:log2 "
+                         "(lde:20 = the LDE of 2^20 output rows)")
     ap.add_argument("--serve-requests", type=int, default=2000, help="requests in the serving measurement (0 = skip)")
     ap.add_argument("--serve-shapes", type=int, default=8, help="distinct request shapes, replayed in turn")
     ap.add_argument("--serve-rate", type=str, default="32,64", help="Poisson arrival rates (requests/s) to sweep")
@@ -238,7 +241,14 @@ def sweep(a):
         if rc != 0:
             raise RuntimeError(L.lg_last_error(ctx.h).decode())
 
+    only = [w for w in a.sweep_only.split(",") if w]
+
+    def want(kind, log):
+        return not only or kind in only or f"{kind}:{log}" in only
+
     for log_out, cols in [(16, 1024), (18, 512), (20, 256), (22, 128), (24, 64)]:
+        if not want("lde", log_out):
+            continue
         n = 1 << (log_out - 2)
         x = field(n * cols)
         y = torch.empty(4 * n * cols, dtype=torch.int32, device=dev)
@@ -246,6 +256,8 @@ def sweep(a):
         emit("lde", "lde", rep, rows_out=1 << log_out, cols=cols)
         del x, y
     for log_out, cols in [(16, 256), (20, 64), (22, 16)]:
+        if not want("commit", log_out):
+            continue
         n = 1 << (log_out - 2)
         x = field(n * cols)
         ptrs = (ctypes.c_void_p * cols)(*[x.data_ptr() + 4 * n * i for i in range(cols)])
@@ -258,6 +270,8 @@ def sweep(a):
         del x
     alpha = (ctypes.c_uint32 * 6)(*[12345 + i for i in range(6)])
     for logn in (18, 20, 22, 24):
+        if not want("fold", logn):
+            continue
         n = 1 << logn
         x = field(6 * n)
         y = torch.empty(3 * n, dtype=torch.int32, device=dev)
@@ -265,6 +279,8 @@ def sweep(a):
         emit("fri_fold", "fri_fold", rep, n_e6=n)
         del x, y
     for logr, cols in [(20, 256), (22, 64)]:
+        if not want("deep", logr):
+            continue
         rows = 1 << logr
         x = field(rows * cols)
         vals = field(6 * cols)

@@ -46,9 +46,13 @@ __host__ __device__ constexpr size_t tile_words(int logl) {
 // tables of 2^LOGL points).  Pass 0 takes its
 // inputs from first(col, row) (global memory, or the staged tile), every pass
 // but the last writes back to S, the last hands each element to
-// store(col, row, value).  DIF: natural rows in, bit-reversed rows out.
-template <bool DIF, int LOGL, class First, class Store>
+// store(col, row, value) — or, with STORE16 (DIF only: the last pass's local
+// bits are the lowest four), a thread's 16 consecutive rows 16 t .. 16 t + 15
+// of one column at once to store(col, t, v).  DIF: natural rows in,
+// bit-reversed rows out.
+template <bool DIF, int LOGL, bool STORE16 = false, class First, class Store>
 __device__ __forceinline__ void ntt16_tile(uint32_t* S, const uint32_t* tw, bool inverse, First first, Store store) {
+  static_assert(!STORE16 || DIF, "16-row stores follow the DIF pass plan");
   constexpr uint32_t groups = (1u << LOGL) >> 4;  // per column
   constexpr int np = (LOGL - ((LOGL & 3) ? (LOGL & 3) : 4)) / 4 + 1;
 #pragma unroll
@@ -65,11 +69,22 @@ __device__ __forceinline__ void ntt16_tile(uint32_t* S, const uint32_t* tw, bool
         v[r] = p == 0 ? first(col, row) : S[tile_addr(row, col)];
       }
       pass16<DIF>(v, t, lo, s_lo, s_hi, ptab, inverse);
+      if constexpr (STORE16) {
+        if (p == np - 1) {
+          store(col, t, v);
+          continue;
+        }
+      }
 #pragma unroll
       for (uint32_t r = 0; r < 16; r++) {
         const uint32_t row = grp_index(t, r, lo);
-        if (p == np - 1) store(col, row, v[r]);
-        else S[tile_addr(row, col)] = v[r];
+        if constexpr (!STORE16) {
+          if (p == np - 1) {
+            store(col, row, v[r]);
+            continue;
+          }
+        }
+        S[tile_addr(row, col)] = v[r];
       }
     }
     __syncthreads();
@@ -112,6 +127,14 @@ __global__ void __launch_bounds__(512, 2) k_big_pass_a(const BigNtt* jobs, int l
   ntt16_tile<true, LOGC>(S, tw_c, inverse != 0, first, store);
 }
 
+// 4-byte asynchronous copy global -> shared (cp.async, no register staging):
+// a thread issues all of its copies before waiting for any.
+__device__ __forceinline__ void cp_async4(uint32_t* smem, const uint32_t* gmem) {
+  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // Block (x, y): rows [16 x, 16 x + 16) of job y's scratch.
 template <int LOGR>
 __global__ void __launch_bounds__(512, 2) k_big_pass_b(const BigNtt* jobs, int logc, int inverse,
@@ -121,19 +144,27 @@ __global__ void __launch_bounds__(512, 2) k_big_pass_b(const BigNtt* jobs, int l
   constexpr uint32_t R = 1u << LOGR;
   const uint32_t C = 1u << logc;
   const uint32_t j2_0 = blockIdx.x * BIG_TILE;
-  // stage the 16 scratch rows (contiguous, coalesced) into the tile
+  // stage the 16 scratch rows (contiguous, coalesced) into the tile, every
+  // copy in flight before the first wait
   for (uint32_t idx = threadIdx.x; idx < R * BIG_TILE; idx += blockDim.x) {
     const uint32_t jl = idx / R, k1 = idx % R;
-    S[tile_addr(k1, jl)] = J.scratch[(uint64_t)(j2_0 + jl) * R + k1];
+    cp_async4(&S[tile_addr(k1, jl)], J.scratch + (uint64_t)(j2_0 + jl) * R + k1);
   }
+  cp_async_wait_all();
   __syncthreads();
   auto first = [&](uint32_t col, uint32_t k1) { return S[tile_addr(k1, col)]; };
   if (J.out_bitrev) {
-    // out[bitrev_C(j2) R + q] = X[C bitrev_R(q) + j2]: position q holds j1 = bitrev_R(q)
-    auto store = [&](uint32_t col, uint32_t q, uint32_t v) {
-      J.out[(uint64_t)bitrev32(j2_0 + col, logc) * R + q] = v;
+    // out[bitrev_C(j2) R + q] = X[C bitrev_R(q) + j2]: position q holds
+    // j1 = bitrev_R(q); a thread's rows q = 16 t .. 16 t + 15 are 64
+    // contiguous bytes of one output row
+    auto store = [&](uint32_t col, uint32_t t, const uint32_t* v) {
+      uint4* o = reinterpret_cast<uint4*>(J.out + (uint64_t)bitrev32(j2_0 + col, logc) * R + 16 * t);
+      o[0] = make_uint4(v[0], v[1], v[2], v[3]);
+      o[1] = make_uint4(v[4], v[5], v[6], v[7]);
+      o[2] = make_uint4(v[8], v[9], v[10], v[11]);
+      o[3] = make_uint4(v[12], v[13], v[14], v[15]);
     };
-    ntt16_tile<true, LOGR>(S, tw_r, inverse != 0, first, store);
+    ntt16_tile<true, LOGR, true>(S, tw_r, inverse != 0, first, store);
   } else {
     auto store = [&](uint32_t col, uint32_t q, uint32_t v) {
       J.out[(uint64_t)C * bitrev32(q, LOGR) + j2_0 + col] = v;
