@@ -94,6 +94,14 @@ __global__ void k_intt(uint32_t* const* lanes, int logn_rt, const uint32_t* tw_n
 // evaluations on <w_4n> of reedsolomon.Encode (internal/reedsolomon/rs.go:52-70).
 // Optionally writes the coefficients.  Shared memory: A (coefficients) and B
 // (work), pad16 layout.
+// 4-byte asynchronous copy global -> shared (cp.async, no register staging):
+// a thread issues all of its copies before waiting for any.
+__device__ __forceinline__ void cp_async4(uint32_t* smem, const uint32_t* gmem) {
+  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 struct LdeLane { const uint32_t* src; uint32_t* out; uint32_t* coef; };
 // fwd = 0: only the inverse transform, coset 0 and the coefficients (L.coef,
 // which must be set); k_lde_fwd then runs the other cosets.
@@ -205,9 +213,14 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT)
   const uint32_t e = bitrev32(a, RATE_LOG);
   const uint32_t* coef = L.coef ? L.coef : L.src;
   uint32_t* o = L.out + (uint64_t)a * n;
+  // the coefficients go to shared memory first (cp.async, coalesced, all in
+  // flight at once); the first pass reads and overwrites its own positions
+  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) cp_async4(&sm[pad16(k)], coef + k);
+  cp_async_wait_all();
+  __syncthreads();
   auto first_pass = [&](uint32_t t, uint32_t r, int lo) {
     const uint32_t i = grp_index(t, r, lo);
-    return mul(__ldg(coef + i), __ldg(tw_4n + ((e * i) & (big - 1))));
+    return mul(sm[pad16(i)], __ldg(tw_4n + ((e * i) & (big - 1))));
   };
   auto store = [&](uint32_t t, int lo, const uint32_t* v) {
     uint4* q = reinterpret_cast<uint4*>(o + ((uint64_t)t << 4));

@@ -127,14 +127,6 @@ __global__ void __launch_bounds__(512, 2) k_big_pass_a(const BigNtt* jobs, int l
   ntt16_tile<true, LOGC>(S, tw_c, inverse != 0, first, store);
 }
 
-// 4-byte asynchronous copy global -> shared (cp.async, no register staging):
-// a thread issues all of its copies before waiting for any.
-__device__ __forceinline__ void cp_async4(uint32_t* smem, const uint32_t* gmem) {
-  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-
 // Block (x, y): rows [16 x, 16 x + 16) of job y's scratch.
 template <int LOGR>
 __global__ void __launch_bounds__(512, 2) k_big_pass_b(const BigNtt* jobs, int logc, int inverse,
