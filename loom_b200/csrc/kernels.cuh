@@ -281,8 +281,16 @@ __global__ void k_coset_eval(const CosetLane* lanes, int logn_rt, const uint32_t
     for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) o[j] = sm[bitrev32(j, logn)];
     return;
   }
+  // the coefficients (to S2) and the shift powers (to the work half, free
+  // until the first pass) arrive by cp.async, all copies in flight at once;
+  // then each thread scales its own words
   uint32_t* S2 = sm + pad16(n) + 1;
-  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) S2[pad16(k)] = mul(L.src[k], sh[k]);
+  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) {
+    cp_async4(&S2[pad16(k)], L.src + k);
+    cp_async4(&sm[pad16(k)], sh + k);
+  }
+  cp_async_wait_all();
+  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) S2[pad16(k)] = mul(S2[pad16(k)], sm[pad16(k)]);
   __syncthreads();
   auto first = [&](uint32_t t, uint32_t r, int lo) { return S2[pad16(bitrev32(grp_index(t, r, lo), logn))]; };
   auto store = [&](uint32_t t, int lo, const uint32_t* v) {
