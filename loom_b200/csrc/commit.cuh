@@ -202,12 +202,14 @@ inline void launch_lde(Ctx& c, const std::vector<LdeLane>& lanes, uint32_t log_n
       }
     }
     const int first = from_coeffs ? 0 : 1;
-    const dim3 grid((unsigned)lv.size(), (unsigned)((1 << RATE_LOG) - first));
     auto go = [&](auto kern) {
       allow_smem(kern, fsmem);
       c.timed("lde", bytes - (from_coeffs ? 0.0 : 8.0 * n * lv.size()), 0, [&] {
-        kern<<<grid, thr, fsmem, c.stream>>>((const LdeLane*)tab->p, first, twn, tw4);
-        LG_LAUNCH();
+        for (size_t l0 = 0; l0 < lv.size(); l0 += 65535) {  // grid y: lanes, at most 65535 a launch
+          const dim3 grid((unsigned)((1 << RATE_LOG) - first), (unsigned)std::min<size_t>(65535, lv.size() - l0));
+          kern<<<grid, thr, fsmem, c.stream>>>((const LdeLane*)tab->p, (uint32_t)l0, first, twn, tw4);
+          LG_LAUNCH();
+        }
       });
     };
     if constexpr (LG >= 4) {

@@ -194,7 +194,9 @@ __global__ void k_lde(const LdeLane* lanes, int logn_rt, int from_coeffs, const 
 }
 
 // The coset transforms of the LDE as blocks of their own: block (x, y) runs
-// coset a = first + y of lane x from its coefficients (L.coef, or L.src when
+// coset a = first + x of lane lane0 + y (the cosets of a lane side by side,
+// so its coefficients come from DRAM once and from L2 after) from its
+// coefficients (L.coef, or L.src when
 // the lane is given as coefficients), written bit-reversed as in k_lde.  One
 // shared-memory array per block (the coefficients are read from global
 // memory, where the inverse transform left them, rather than kept in shared
@@ -204,12 +206,12 @@ __global__ void k_lde(const LdeLane* lanes, int logn_rt, int from_coeffs, const 
 // without spills).
 template <int LOGN, int MAXT>
 __global__ void __launch_bounds__(MAXT, 1024 / MAXT)
-    k_lde_fwd(const LdeLane* lanes, int first, const uint32_t* tw_n, const uint32_t* tw_4n) {
+    k_lde_fwd(const LdeLane* lanes, uint32_t lane0, int first, const uint32_t* tw_n, const uint32_t* tw_4n) {
   static_assert(LOGN >= 4, "radix-16 passes");
   extern __shared__ uint32_t sm[];
   constexpr uint32_t n = 1u << LOGN, big = n << RATE_LOG;
-  const LdeLane L = lanes[blockIdx.x];
-  const uint32_t a = first + blockIdx.y;
+  const LdeLane L = lanes[lane0 + blockIdx.y];
+  const uint32_t a = first + blockIdx.x;
   const uint32_t e = bitrev32(a, RATE_LOG);
   const uint32_t* coef = L.coef ? L.coef : L.src;
   uint32_t* o = L.out + (uint64_t)a * n;
