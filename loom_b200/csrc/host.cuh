@@ -203,6 +203,11 @@ struct ProgCache;  // compiled bytecode of one program (prover.cuh)
 struct Ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // Work that overlaps a host wait on `stream` (the DEEP denominators while
+  // the host hashes the claimed values): forked after fork_ev, joined back
+  // through join_ev.
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   DevArena dev_arena;            // prove-scoped small device buffers
   MemAcct mem;                   // device bytes this context holds (lg_ctx_mem_usage)
   std::map<int, DBufP> tw;       // log n -> w_n^j, j < n
@@ -249,12 +254,13 @@ struct Ctx {
     phases.emplace_back(name, std::chrono::duration<double, std::milli>(now - phase_t0).count());
     phase_t0 = now;
   }
-  template <class F> void timed(const char* name, double bytes, double perms, F launch) {
+  template <class F> void timed(const char* name, double bytes, double perms, F launch, cudaStream_t on = nullptr) {
     if (!profiling) { launch(); return; }
+    if (!on) on = stream;
     KRec r{name, pooled_event(), pooled_event(), bytes, perms, phases.size()};
-    LG_CK(cudaEventRecord(r.a, stream));
+    LG_CK(cudaEventRecord(r.a, on));
     launch();
-    LG_CK(cudaEventRecord(r.b, stream));
+    LG_CK(cudaEventRecord(r.b, on));
     recs.push_back(r);
   }
 

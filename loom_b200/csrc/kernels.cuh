@@ -1053,7 +1053,43 @@ struct DeepJob {
   int logn4;            // log2 of the LDE size
   const uint32_t* tw;   // w_4n^j table
   uint32_t* out;        // 6 lanes, lane stride 4n
+  const uint32_t* den;  // 1/(z_s - x) from k_deep_den (null: computed here)
 };
+
+// The DEEP denominators 1/(z_s - x) of every LDE row r of a class (x =
+// w_4n^bitrev(r)), one inversion per row for all its points (Montgomery's
+// trick), stored as six lanes per point: den[(6 s + w) 4n + r].  z_s =
+// zeta ws[s] with zeta read from its device slot, so the kernel runs as
+// soon as zeta is known, beside the claimed values and the host's
+// alpha_DEEP transcript.
+struct DenJob { uint32_t n_points; uint32_t ws[DEEP_MAX_POINTS]; int logn4; const uint32_t* tw; uint32_t* den; };
+__global__ void k_deep_den(const DenJob* jobs, const uint32_t* zeta_w) {
+  const DenJob& jb = jobs[blockIdx.y];
+  const uint32_t big = 1u << jb.logn4;
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= big) return;
+  E6 zeta;
+#pragma unroll
+  for (int w = 0; w < 6; w++) zeta.c[w] = zeta_w[w];
+  const uint32_t x = __ldg(jb.tw + bitrev32(r, jb.logn4));
+  const uint32_t np = jb.n_points;
+  E6 d[DEEP_MAX_POINTS], pre[DEEP_MAX_POINTS];
+  for (uint32_t s = 0; s < np; s++) {
+    d[s] = e6_mul_base(zeta, jb.ws[s]);
+    d[s].c[0] = sub(d[s].c[0], x);
+    pre[s] = s ? e6_mul(pre[s - 1], d[s]) : d[s];
+  }
+  auto put = [&](uint32_t s, const E6& v) {
+#pragma unroll
+    for (int w = 0; w < 6; w++) jb.den[(uint64_t)(6 * s + w) * big + r] = v.c[w];
+  };
+  E6 inv_run = e6_inv(pre[np - 1]);
+  for (uint32_t s = np - 1; s > 0; s--) {
+    put(s, e6_mul(inv_run, pre[s - 1]));
+    inv_run = e6_mul(inv_run, d[s]);
+  }
+  put(0, inv_run);
+}
 __global__ void k_deep(const DeepJob* jobs) {
   const DeepJob& jb = jobs[blockIdx.y];
   const uint32_t big = 1u << jb.logn4;
@@ -1074,11 +1110,22 @@ __global__ void k_deep(const DeepJob* jobs) {
     for (uint32_t s = 0; s < jb.n_points; s++)
       if (bu.mask >> s & 1) acc[s] = e6_sub(acc[s], v);
   }
+  const uint32_t np = jb.n_points;
+  if (jb.den) {  // the denominators are precomputed
+    E6 dq = e6_zero();
+    for (uint32_t s = 0; s < np; s++) {
+      E6 is;
+#pragma unroll
+      for (int w = 0; w < 6; w++) is.c[w] = jb.den[(uint64_t)(6 * s + w) * big + r];
+      dq = e6_add(dq, e6_mul(acc[s], is));
+    }
+    for (int w = 0; w < 6; w++) jb.out[(uint64_t)w * big + r] = dq.c[w];
+    return;
+  }
   uint32_t x = __ldg(jb.tw + bitrev32(r, jb.logn4));
   // sum_s acc_s / (z_s - x) with one inversion (Montgomery's trick over the
   // points): pre_s = d_0 ... d_s, then 1/d_s = pre_(s-1) / pre_s from the top
   E6 d[DEEP_MAX_POINTS], pre[DEEP_MAX_POINTS];
-  const uint32_t np = jb.n_points;
   for (uint32_t s = 0; s < np; s++) {
     d[s] = jb.z[s];
     d[s].c[0] = sub(d[s].c[0], x);

@@ -44,6 +44,7 @@ template <class F> int guarded(lg_ctx* ctx, F f) {
     LG_CK(cudaSetDevice(ctx->c.device));
     if (ctx->c.stream) {
       LG_CK(cudaStreamSynchronize(ctx->c.stream));
+      if (ctx->c.side) LG_CK(cudaStreamSynchronize(ctx->c.side));  // its work reads the arena too
       ctx->c.arena_reset();
       ctx->c.dev_arena.rewind();
     }
@@ -82,6 +83,9 @@ int lg_ctx_create(int device, size_t hbm_budget, lg_ctx** out) {
   ctx->c.mem.budget = (int64_t)hbm_budget;
   int rc = guarded(ctx, [&] {
     LG_CK(cudaStreamCreateWithFlags(&ctx->c.stream, cudaStreamNonBlocking));
+    LG_CK(cudaStreamCreateWithFlags(&ctx->c.side, cudaStreamNonBlocking));
+    LG_CK(cudaEventCreateWithFlags(&ctx->c.fork_ev, cudaEventDisableTiming));
+    LG_CK(cudaEventCreateWithFlags(&ctx->c.join_ev, cudaEventDisableTiming));
     cudaMemPool_t pool;
     LG_CK(cudaDeviceGetDefaultMemPool(&pool, device));
     uint64_t keep = UINT64_MAX;  // keep freed blocks for the next prove
@@ -115,6 +119,12 @@ void lg_ctx_destroy(lg_ctx* ctx) {
     cudaStreamSynchronize(ctx->c.stream);
     cudaStreamDestroy(ctx->c.stream);
   }
+  if (ctx->c.side) {
+    cudaStreamSynchronize(ctx->c.side);
+    cudaStreamDestroy(ctx->c.side);
+  }
+  if (ctx->c.fork_ev) cudaEventDestroy(ctx->c.fork_ev);
+  if (ctx->c.join_ev) cudaEventDestroy(ctx->c.join_ev);
   if (ctx->c.pinned) cudaFreeHost(ctx->c.pinned);
   delete ctx;
 }

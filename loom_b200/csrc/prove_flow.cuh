@@ -341,6 +341,10 @@ inline void Prover::claimed_values() {
       k_dot<<<(unsigned)jobs.size(), 256, 0, c.stream>>>((const DotJob*)jd->p, od->p);
       LG_LAUNCH();
     });
+    // the DEEP denominators depend on zeta alone: forked after the dot
+    // products, they run on the side stream while the host reads the claimed
+    // values back and hashes them
+    launch_deep_den();
     uint32_t* h = c.host_staging(dots.size());
     c.d2h(h, od->p, dots.size());
     memcpy(dots.data(), h, dots.size() * 4);
@@ -366,13 +370,72 @@ inline void Prover::claimed_values() {
         cv[t][g].push_back(vals);
       }
   }
-  // DEEP classes = modules with committed groups, in sorted order
-  classes.clear();
+  classes = deep_class_list();
+}
+
+inline std::vector<uint32_t> Prover::deep_class_list() const {
+  std::vector<uint32_t> cl;
   for (uint32_t m : mod_order) {
     bool has = false;
     for (auto& t : trees) for (auto& g : t.groups) if (g.module == m) has = true;
-    if (has) classes.push_back(m);
+    if (has) cl.push_back(m);
   }
+  return cl;
+}
+
+inline std::vector<uint32_t> Prover::class_point_factors(uint32_t m) const {
+  const uint32_t w_n = root_of_unity_mont((int)pg.modules[m].log_n);
+  std::vector<uint32_t> ws;
+  for (size_t t = 0; t < trees.size(); t++)
+    for (size_t g = 0; g < trees[t].groups.size(); g++) {
+      if (trees[t].groups[g].module != m) continue;
+      for (const Poly& p : polys[t][g])
+        for (int sh : p.shifts) {
+          const uint32_t f = mont_pow(w_n, (uint64_t)sh);
+          if (std::find(ws.begin(), ws.end(), f) == ws.end()) ws.push_back(f);
+        }
+    }
+  if (ws.size() > DEEP_MAX_POINTS) throw Error(LG_ERR_UNSUPPORTED, "too many distinct opening points");
+  return ws;
+}
+
+inline void Prover::launch_deep_den() {
+  const std::vector<uint32_t> cl = deep_class_list();
+  std::vector<DenJob> jobs;
+  std::vector<size_t> off;
+  size_t words = 0;
+  uint32_t max_big = 0;
+  for (uint32_t m : cl) {
+    DenJob j{};
+    const std::vector<uint32_t> ws = class_point_factors(m);
+    j.n_points = (uint32_t)ws.size();
+    for (size_t k = 0; k < ws.size(); k++) j.ws[k] = ws[k];
+    j.logn4 = (int)pg.modules[m].log_n + RATE_LOG;
+    j.tw = c.twiddles(j.logn4);
+    off.push_back(words);
+    words += 6 * (size_t)j.n_points << j.logn4;
+    max_big = std::max(max_big, 1u << j.logn4);
+    jobs.push_back(j);
+  }
+  deep_den.assign(cl.size(), nullptr);
+  if (cl.empty() || !words) return;
+  auto all = std::make_shared<DBuf>(words, c.stream);
+  for (size_t i = 0; i < jobs.size(); i++) {
+    deep_den[i] = dbuf_slice(all, off[i], 6 * (size_t)jobs[i].n_points << jobs[i].logn4);
+    jobs[i].den = deep_den[i]->p;
+  }
+  auto jd = upload_vec(c, jobs);
+  // everything the side stream reads (zeta's slot, tables, job list) is
+  // ordered before fork_ev on the main stream
+  LG_CK(cudaEventRecord(c.fork_ev, c.stream));
+  LG_CK(cudaStreamWaitEvent(c.side, c.fork_ev, 0));
+  c.timed("deep_den", 24.0 * (double)words / 6, 0, [&] {
+    k_deep_den<<<dim3((max_big + 127) / 128, (unsigned)jobs.size()), 128, 0, c.side>>>((const DenJob*)jd->p,
+                                                                                      fs_slot(pg.n_rounds));
+    LG_LAUNCH();
+  }, c.side);
+  LG_CK(cudaEventRecord(c.join_ev, c.side));
+  den_pending = true;
 }
 
 inline std::vector<E6> Prover::claimed_values_bind_order() const {
@@ -410,6 +473,7 @@ inline void Prover::deep_codewords() {
     DeepJob jb{};
     std::vector<DeepBundle> bundles;
     std::vector<E6> pts;
+    std::vector<uint32_t> pts_w;  // their factors w_n^shift (first-use order, as k_deep_den)
     E6 run = e6_one();
     for (size_t t = 0; t < trees.size(); t++)
       for (size_t g = 0; g < trees[t].groups.size(); g++) {
@@ -425,12 +489,13 @@ inline void Prover::deep_codewords() {
           bu.scale = run;
           lane += p.ext ? 6 : 1;
           for (size_t si = 0; si < p.shifts.size(); si++) {
-            E6 z = e6_mul_base(zeta, mont_pow(w_n, (uint64_t)p.shifts[si]));
+            const uint32_t f = mont_pow(w_n, (uint64_t)p.shifts[si]);
             size_t k = 0;
-            while (k < pts.size() && !e6_eq(pts[k], z)) k++;
+            while (k < pts_w.size() && pts_w[k] != f) k++;
             if (k == pts.size()) {
               if (pts.size() == DEEP_MAX_POINTS) throw Error(LG_ERR_UNSUPPORTED, "too many distinct opening points");
-              pts.push_back(z);
+              pts.push_back(e6_mul_base(zeta, f));
+              pts_w.push_back(f);
               jb.a[k] = e6_zero();
             }
             jb.a[k] = e6_add(jb.a[k], e6_mul(run, cv[t][g][i][si]));
@@ -450,6 +515,7 @@ inline void Prover::deep_codewords() {
     deep[ci] = dbuf_slice(deep_all, deep_off, 6 * big);
     deep_off += 6 * big;
     jb.out = deep[ci]->p;
+    if (den_pending && ci < deep_den.size() && deep_den[ci]) jb.den = deep_den[ci]->p;
     djobs.push_back(jb);
     double row_bytes = 24.0;
     for (auto& bu : bundles) row_bytes += bu.ext ? 24.0 : 4.0;
@@ -457,6 +523,10 @@ inline void Prover::deep_codewords() {
   }
   auto bundles_d = upload_vec(c, all_bundles);
   for (size_t i = 0; i < djobs.size(); i++) djobs[i].bundles = (const DeepBundle*)bundles_d->p + bundle_off[i];
+  if (den_pending) {  // join the side stream's denominators
+    LG_CK(cudaStreamWaitEvent(c.stream, c.join_ev, 0));
+    den_pending = false;
+  }
   auto launch_deep = [&](size_t first, size_t count) {
     std::vector<DeepJob> v(djobs.begin() + first, djobs.begin() + first + count);
     uint32_t max_big = 0;

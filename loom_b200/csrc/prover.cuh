@@ -112,6 +112,8 @@ struct Prover {
   std::vector<std::vector<std::vector<std::vector<E6>>>> cv;          // claimed values [tree][group][poly][shift]
   std::vector<uint32_t> classes;            // DEEP classes: modules with committed groups, layout order
   std::vector<DBufP> deep;                  // DEEP codeword per class (6 lanes x 4n)
+  std::vector<DBufP> deep_den;              // per class: 1/(z_s - x) per point (k_deep_den), or empty
+  bool den_pending = false;                 // k_deep_den queued on the side stream, not yet joined
   // FRI (internal/fri/fri.go:352-365,606-736)
   size_t L = 0;                             // levels, sorted by size (descending, stable)
   int NR = 0, r0 = 0;                       // rounds; the first round with a layer
@@ -131,6 +133,14 @@ struct Prover {
   int fri_next = -1;                        // next round to fold (-1: levels not committed)
   std::vector<uint32_t> final_poly;         // 6 lanes of nj words, once read back
 
+  // A prover dropped with the DEEP denominators still queued (a session
+  // released before its DEEP phase) orders the frees of its buffers, which
+  // run on the main stream, after that work.
+  ~Prover() {
+    if (den_pending) cudaStreamWaitEvent(c.stream, c.join_ev, 0);
+  }
+  Prover(const Prover&) = delete;
+  Prover& operator=(const Prover&) = delete;
   Prover(Ctx& ctx, const uint32_t* words, size_t nwords, uint32_t q) : c(ctx), num_queries(q) {
     pg = parse_program(words, nwords);
     if (q == 0) throw Error(LG_ERR_INVALID, "num_queries must be positive");
@@ -1254,6 +1264,13 @@ struct Prover {
   // bindClaimedValuesByPolynomialOrder binds them (internal/fri/open.go:223-285)
   void claimed_values();
   std::vector<E6> claimed_values_bind_order() const;
+  // DEEP classes (modules with committed groups, layout order) and, per
+  // class, its opening points as the factors w_n^shift of z = zeta w_n^shift
+  // in first-use order (the order k_deep's points take)
+  std::vector<uint32_t> deep_class_list() const;
+  std::vector<uint32_t> class_point_factors(uint32_t m) const;
+  // k_deep_den for every class on the side stream (needs zeta in its slot)
+  void launch_deep_den();
   void deep_codewords();                  // internal/fri/deep.go:71-266
   Digest commit_levels();                 // fri.Prove's levels tree (internal/fri/fri.go:294-317)
   // fold round j (foldLayerExt) with the challenge at chal + 8 j, then the
