@@ -133,6 +133,9 @@ int lg_ctx_set_leaf_mapping(lg_ctx* ctx, int lanes_per_permutation);
  *   "fri_tail_leaves"     the FRI rounds whose layer tree has at most this many
  *                         leaves run in one block, back to back (power of two,
  *                         2..65536; 0: a launch per step of every round)
+ *   "quotient_jit"        1: each module's constraint bytecode is compiled to a
+ *                         kernel of its own at run time (NVRTC, cached per
+ *                         program); 0: the bytecode interpreter
  * Unknown names or values out of range return LG_ERR_INVALID. */
 int lg_ctx_set_tuning(lg_ctx* ctx, const char* name, int64_t value);
 int lg_ctx_get_tuning(lg_ctx* ctx, const char* name, int64_t* value);
@@ -357,6 +360,9 @@ int lg_timer_mark(lg_ctx* ctx, uint32_t slot);
 int lg_timer_elapsed(lg_ctx* ctx, uint32_t from, uint32_t to, float* ms);
 /* Number of kernels this library has launched since it was loaded. */
 uint64_t lg_kernel_launches(void);
+/* Number of constraint kernels compiled at run time (tuning "quotient_jit")
+ * that this process holds, over all devices. */
+uint64_t lg_jit_kernels(void);
 /* Per-kernel event profiler: enable (1) clears and starts recording events
  * around the main kernels; lg_profile_report writes a JSON object
  * {kernel: {launches, ms, bytes, perms}} with algorithmic bytes and Poseidon2

@@ -20,7 +20,7 @@ LG_OK, LG_ERR_INVALID, LG_ERR_CUDA, LG_ERR_OOM, LG_ERR_UNSUPPORTED, LG_ERR_BUFFE
 EXPORTS = ["lg_ctx_create", "lg_ctx_destroy", "lg_ctx_set_batched", "lg_ctx_set_leaf_mapping", "lg_ctx_set_tuning",
            "lg_ctx_get_tuning", "lg_mem_info", "lg_last_error", "lg_prove", "lg_last_proof", "lg_setup", "lg_verify", "lg_commit_root",
            "lg_rs_encode", "lg_poseidon2_permute", "lg_merkle_root", "lg_fri_fold", "lg_timer_mark",
-           "lg_timer_elapsed", "lg_kernel_launches", "lg_profile", "lg_profile_report", "lg_grand_product", "lg_grand_product_noalloc", "lg_deep_quotient",
+           "lg_timer_elapsed", "lg_kernel_launches", "lg_jit_kernels", "lg_profile", "lg_profile_report", "lg_grand_product", "lg_grand_product_noalloc", "lg_deep_quotient",
            "lg_ctx_mem_usage", "lg_device_mem_info", "lg_commit", "lg_committed_eval", "lg_open_batches", "lg_session_begin",
            "lg_session_setup_root", "lg_session_challenge", "lg_commit_round", "lg_quotient", "lg_claimed_values",
            "lg_deep", "lg_fri_commit_levels", "lg_fri_fold_round", "lg_fri_final", "lg_open", "lg_session_committed",
@@ -102,6 +102,8 @@ def load():
         L.lg_timer_elapsed.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(ctypes.c_float)]
         L.lg_kernel_launches.argtypes = []
         L.lg_kernel_launches.restype = ctypes.c_uint64
+        L.lg_jit_kernels.argtypes = []
+        L.lg_jit_kernels.restype = ctypes.c_uint64
         L.lg_profile.argtypes = [vp, ctypes.c_int]
         L.lg_profile_report.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_size_t)]
         _lib = L
@@ -180,7 +182,7 @@ class Context:
         return int(h.value), int(pk.value)
 
     TUNING_NAMES = ("p2_leaf_min_per_sm", "p2_node_min_per_sm", "p2_inject_min_per_sm", "merkle_tail",
-                    "merkle_subtree", "inject_block", "leaf_block", "lde_split", "lde_fwd_threads", "fri_tail_leaves")
+                    "merkle_subtree", "inject_block", "leaf_block", "lde_split", "lde_fwd_threads", "fri_tail_leaves", "quotient_jit")
 
     def set_tuning(self, name: str, value: int):
         """Launch-shape choice (see include/loom_gpu.h); proofs do not depend on it."""

@@ -16,7 +16,7 @@ FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std
 
 def sources():
     d = os.path.join(HERE, "csrc")
-    return [os.path.join(d, f) for f in sorted(os.listdir(d)) if f.endswith((".cu", ".cuh", ".h", ".cpp"))] + \
+    return [os.path.join(d, f) for f in sorted(os.listdir(d)) if f.endswith((".cu", ".cuh", ".h", ".cpp", ".inc"))] + \
         [os.path.join(HERE, "..", "include", "loom_gpu.h")]
 
 
@@ -27,7 +27,29 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(s) <= t for s in sources())
 
 
+FIELD_SRC = os.path.join(HERE, "csrc", "field.cuh")
+FIELD_INC = os.path.join(HERE, "csrc", "field_src.inc")
+
+
+def write_field_inc() -> None:
+    """field.cuh as a C++ raw string literal: the run-time compiler of the
+    constraint kernels (csrc/xjit.cuh) includes it from memory."""
+    with open(FIELD_SRC) as f:
+        text = f.read()
+    if ')LGFIELD"' in text:
+        raise RuntimeError("field.cuh contains the raw-string delimiter")
+    body = 'R"LGFIELD(' + text + ')LGFIELD"\n'
+    old = None
+    if os.path.exists(FIELD_INC):
+        with open(FIELD_INC) as f:
+            old = f.read()
+    if old != body:
+        with open(FIELD_INC, "w") as f:
+            f.write(body)
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
+    write_field_inc()
     if not force and up_to_date():
         return OUT
     cmd = [NVCC] + FLAGS + ["-o", OUT] + SRC

@@ -10,7 +10,15 @@
 // Every function is __host__ __device__: the host-side Fiat-Shamir transcript
 // uses the same code as the kernels.
 #pragma once
+#ifdef __CUDACC_RTC__  // compiled at run time (the constraint kernels, xjit.cuh): no host headers
+typedef unsigned char uint8_t;
+typedef unsigned int uint32_t;
+typedef int int32_t;
+typedef unsigned long long uint64_t;
+typedef long long int64_t;
+#else
 #include <cstdint>
+#endif
 
 #ifdef __CUDACC__
 #define LG_HD __host__ __device__ __forceinline__

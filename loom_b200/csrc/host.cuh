@@ -38,10 +38,13 @@ struct Error : std::runtime_error {
 // Every kernel launch is followed by LG_LAUNCH(): it checks the launch and
 // counts it (lg_kernel_launches).
 inline std::atomic<uint64_t> g_launches{0};
-#define LG_LAUNCH()                 \
-  do {                              \
-    LG_CK(cudaGetLastError());      \
-    ::lg::g_launches.fetch_add(1);  \
+#define LG_LAUNCH()                                                                                 \
+  do {                                                                                              \
+    const cudaError_t e_ = cudaGetLastError();                                                      \
+    if (e_ != cudaSuccess)                                                                          \
+      throw ::lg::Error(LG_ERR_CUDA, std::string("kernel launch at ") + __FILE__ + ":" +              \
+                                         std::to_string(__LINE__) + ": " + cudaGetErrorString(e_)); \
+    ::lg::g_launches.fetch_add(1);                                                                  \
   } while (0)
 
 // Device bytes held by one context (its DBuf allocations and arena chunks),
@@ -399,6 +402,7 @@ struct Ctx {
     uint32_t leaf_block = 128;          // threads per block, one-thread leaf hashing
     uint32_t lde_split = 1;             // LDE as an inverse launch plus one block per (lane, coset)
     uint32_t lde_fwd_threads = 512;     // threads per block of the coset transforms (split LDE)
+    uint32_t quotient_jit = 1;          // the quotient's constraint bytecode as a compiled kernel (0: interpreter)
     uint32_t fri_tail_leaves = 0;       // FRI rounds whose layer tree has at most this many leaves: one block (0: none;
                                         // 512 measured 14.09 ms against 13.65 ms per 40 x 2^14 prove)
   } tune;

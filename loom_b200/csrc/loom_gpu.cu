@@ -204,6 +204,10 @@ int lg_ctx_set_tuning(lg_ctx* ctx, const char* name, int64_t value) {
       if (value != 0) { in(2, 1 << 16); pow2(); }
       t.fri_tail_leaves = (uint32_t)value;
     }
+    else if (n == "quotient_jit") {
+      in(0, 1);
+      t.quotient_jit = (uint32_t)value;
+    }
     else throw Error(LG_ERR_INVALID, "unknown tuning " + n);
   });
 }
@@ -223,6 +227,7 @@ int lg_ctx_get_tuning(lg_ctx* ctx, const char* name, int64_t* value) {
     else if (n == "lde_split") *value = t.lde_split;
     else if (n == "lde_fwd_threads") *value = t.lde_fwd_threads;
     else if (n == "fri_tail_leaves") *value = t.fri_tail_leaves;
+    else if (n == "quotient_jit") *value = t.quotient_jit;
     else throw Error(LG_ERR_INVALID, "unknown tuning " + n);
   });
 }
@@ -856,6 +861,7 @@ int lg_timer_elapsed(lg_ctx* ctx, uint32_t from, uint32_t to, float* ms) {
 }
 
 uint64_t lg_kernel_launches(void) { return g_launches.load(); }
+uint64_t lg_jit_kernels(void) { return xjit_compiled(); }
 
 int lg_profile(lg_ctx* ctx, int enable) {
   return guarded(ctx, [&] {

@@ -6,6 +6,7 @@
 #include <set>
 
 #include "commit.cuh"
+#include "xjit.cuh"
 
 namespace lg {
 
@@ -17,8 +18,7 @@ inline std::string coin_name(uint32_t r) { return "challenge@loom_" + std::to_st
 
 struct ProveStats { double ms_total = 0; };
 
-// Register bytecode of one expression (compile_expr).
-struct XCode { std::vector<XInst> code; uint32_t n_regs = 0, result = 0, result_ext = 0; };
+
 
 // The bytecode of one compile site (a step's expressions, a module's folded
 // relation) depends only on the program and on the order in which the site's
@@ -1170,10 +1170,22 @@ struct Prover {
         });
       }
       // 2. bytecode evaluation on the 4n coset points of every module
+      // modules whose bytecode compiles to a kernel of its own (xjit.cuh) run
+      // it, one launch per distinct program; the others the interpreter
       std::vector<QJob> qj;
+      std::map<CUfunction, std::pair<std::vector<QxJob>, uint32_t>> jit;  // jobs, largest n
       uint32_t max_regs = 1, max_n = 0;
       double qbytes = 0;
       for (ModQ* q : ms) {
+        qbytes += (4.0 * q->lanes.size() + 24.0) * (4.0 * (1u << q->logn));
+        max_n = std::max(max_n, 1u << q->logn);  // the chunk step below covers every module
+        if (CUfunction f = c.tune.quotient_jit ? xjit_quotient(q->xc) : nullptr) {
+          QxJob x{q->cv->p, q->qv->p, (int)q->logn, {q->zinv[0], q->zinv[1], q->zinv[2], q->zinv[3]}};
+          auto& g = jit[f];
+          g.first.push_back(x);
+          g.second = std::max(g.second, 1u << q->logn);
+          continue;
+        }
         QJob j{};
         j.p = q->prog;
         j.cv = q->cv->p;
@@ -1182,16 +1194,24 @@ struct Prover {
         for (int k = 0; k < 4; k++) j.zinv[k] = q->zinv[k];
         qj.push_back(j);
         max_regs = std::max(max_regs, q->xc.n_regs);
-        max_n = std::max(max_n, 1u << q->logn);
-        qbytes += (4.0 * q->lanes.size() + 24.0) * (4.0 * (1u << q->logn));
       }
-      auto qd = upload_vec(c, qj);
+      std::vector<std::pair<CUfunction, DBufP>> jit_d;
+      for (auto& kv : jit) jit_d.push_back({kv.first, upload_vec(c, kv.second.first)});
+      DBufP qd = qj.empty() ? DBufP() : upload_vec(c, qj);
       size_t smem = (size_t)max_regs * 6 * T * 4;
-      allow_smem(k_quotient_eval, smem);
+      if (!qj.empty()) allow_smem(k_quotient_eval, smem);
       c.timed("quotient_eval", qbytes, 0, [&] {
-        k_quotient_eval<<<dim3((max_n + T - 1) / T, 4, (unsigned)qj.size()), T, smem, c.stream>>>((const QJob*)qd->p,
-                                                                                                  (const E6*)coins_d->p);
-        LG_LAUNCH();
+        for (auto& fd : jit_d) {
+          const auto& g = jit.at(fd.first);
+          xjit_launch(fd.first, dim3((g.second + 127) / 128, 4, (unsigned)g.first.size()), (const QxJob*)fd.second->p,
+                      (const E6*)coins_d->p, c.stream);
+          g_launches.fetch_add(1);
+        }
+        if (!qj.empty()) {
+          k_quotient_eval<<<dim3((max_n + T - 1) / T, 4, (unsigned)qj.size()), T, smem, c.stream>>>(
+              (const QJob*)qd->p, (const E6*)coins_d->p);
+          LG_LAUNCH();
+        }
       });
       // 3. per-coset inverse transforms, one launch per size
       std::map<uint32_t, std::vector<uint32_t*>> intt;

@@ -1,0 +1,210 @@
+// The quotient's constraint bytecode (XCode below, XInst in kernels.cuh) compiled to a
+// kernel of its own at run time.  The interpreter (k_quotient_eval) keeps
+// its register file in shared memory (6 words per register per thread, up
+// to 72 KB per block) and decodes every instruction per row; the generated
+// kernel names every register word as a local, so the compiler allocates
+// real registers and the instruction stream is straight-line code.  The
+// semantics are the interpreter's word for word: a base write sets word 0
+// of its register and leaves the other five as they were, a base read
+// takes word 0.
+//
+// The run-time compiler (NVRTC) is loaded with dlopen and the driver's
+// module calls come through cudaGetDriverEntryPoint, so the library links
+// neither; where either is missing, or a program is too long, the
+// interpreter runs instead.  Kernels are cached per device and source.
+#pragma once
+#include <cuda.h>
+#include <dlfcn.h>
+#include <nvrtc.h>
+
+#include <array>
+#include <mutex>
+#include <sstream>
+
+#include "host.cuh"
+
+namespace lg {
+
+// Register bytecode of one expression (compile_expr, prover.cuh).
+struct XCode { std::vector<XInst> code; uint32_t n_regs = 0, result = 0, result_ext = 0; };
+
+// Job of a generated kernel (the QJob fields it needs); the generated
+// source declares the same struct.
+struct QxJob { const uint32_t* cv; uint32_t* qv; int logn; uint32_t zinv[4]; };
+static_assert(sizeof(QxJob) == 40, "QxJob layout is shared with the generated source");
+constexpr uint32_t XJIT_MAX_INST = 4096;
+
+inline const char* xjit_field_src() {
+  static const char* s =
+#include "field_src.inc"
+      ;
+  return s;
+}
+
+// CUDA source of the quotient kernel of one bytecode program.
+inline std::string xjit_source(const XCode& xc) {
+  std::ostringstream o;
+  o << "#include \"field.cuh\"\nusing namespace lg;\n"
+       "struct QxJob { const uint32_t* cv; uint32_t* qv; int logn; uint32_t zinv[4]; };\n"
+       "extern \"C\" __global__ void __launch_bounds__(128) lg_qx(const QxJob* jobs, const E6* coins) {\n"
+       "  const QxJob J = jobs[blockIdx.z];\n"
+       "  const uint32_t n = 1u << J.logn, c = blockIdx.y, m = n - 1;\n"
+       "  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;\n"
+       "  if (j >= n) return;\n"
+       "  const uint64_t big = (uint64_t)n << 2;\n"
+       "  const uint32_t* cv = J.cv + (uint64_t)c * n;\n";
+  std::vector<std::array<std::string, 6>> reg(std::max<uint32_t>(xc.n_regs, 1));
+  for (auto& r : reg) r.fill("0u");
+  auto e6lit = [&](uint32_t r) {
+    std::string s = "E6{{";
+    for (int w = 0; w < 6; w++) s += (w ? ", " : "") + reg[r][w];
+    return s + "}}";
+  };
+  auto lane = [&](uint32_t l, int32_t shift) {
+    std::ostringstream q;
+    q << "cv[" << l << "ull * big + ((j + " << (uint32_t)shift << "u) & m)]";
+    return q.str();
+  };
+  for (size_t i = 0; i < xc.code.size(); i++) {
+    const XInst& in = xc.code[i];
+    const std::string v = "v" + std::to_string(i);
+    auto base = [&](const std::string& expr) {
+      o << "  const uint32_t " << v << " = " << expr << ";\n";
+      reg[in.d][0] = v;
+    };
+    auto ext = [&](const std::string& expr) {
+      o << "  const E6 " << v << " = " << expr << ";\n";
+      for (int w = 0; w < 6; w++) reg[in.d][w] = v + ".c[" + std::to_string(w) + "]";
+    };
+    const std::string a0 = reg[in.a][0], b0 = reg[in.b][0];
+    switch (in.op) {
+      case X_LOAD_B: base(lane(in.imm, in.shift)); break;
+      case X_LOAD_E: {
+        std::string s = "E6{{";
+        for (int w = 0; w < 6; w++) s += (w ? ", " : "") + lane(in.imm + w, in.shift);
+        ext(s + "}}");
+        break;
+      }
+      case X_COIN: ext("coins[" + std::to_string(in.imm) + "]"); break;
+      case X_CONST: base(std::to_string(in.imm) + "u"); break;
+      case X_ADD_BB: base("add(" + a0 + ", " + b0 + ")"); break;
+      case X_SUB_BB: base("sub(" + a0 + ", " + b0 + ")"); break;
+      case X_MUL_BB: base("mul(" + a0 + ", " + b0 + ")"); break;
+      case X_ADD_EE: ext("e6_add(" + e6lit(in.a) + ", " + e6lit(in.b) + ")"); break;
+      case X_SUB_EE: ext("e6_sub(" + e6lit(in.a) + ", " + e6lit(in.b) + ")"); break;
+      case X_MUL_EE: ext("e6_mul(" + e6lit(in.a) + ", " + e6lit(in.b) + ")"); break;
+      case X_MUL_EB: ext("e6_mul_base(" + e6lit(in.a) + ", " + b0 + ")"); break;
+      case X_ADD_EB: case X_SUB_EB: {
+        std::string s = "E6{{" + std::string(in.op == X_ADD_EB ? "add(" : "sub(") + a0 + ", " + b0 + ")";
+        for (int w = 1; w < 6; w++) s += ", " + reg[in.a][w];
+        ext(s + "}}");
+        break;
+      }
+      case X_SUB_BE: {
+        std::string s = "E6{{sub(" + a0 + ", " + b0 + ")";
+        for (int w = 1; w < 6; w++) s += ", neg(" + reg[in.b][w] + ")";
+        ext(s + "}}");
+        break;
+      }
+      default: throw Error(LG_ERR_INVALID, "bytecode: unknown instruction");
+    }
+  }
+  o << "  const E6 r = e6_mul_base(" << (xc.result_ext ? e6lit(xc.result) : "e6_base(" + reg[xc.result][0] + ")")
+    << ", J.zinv[c]);\n";
+  const int lw = xc.result_ext ? 6 : 1;
+  for (int w = 0; w < lw; w++)
+    o << "  J.qv[" << w << "ull * big + (uint64_t)c * n + j] = r.c[" << w << "];\n";
+  o << "}\n";
+  return o.str();
+}
+
+// NVRTC entry points (dlopen) and the driver's module calls.
+struct XjitApi {
+  bool ok = false;
+  decltype(&nvrtcCreateProgram) create = nullptr;
+  decltype(&nvrtcCompileProgram) compile = nullptr;
+  decltype(&nvrtcGetProgramLogSize) log_size = nullptr;
+  decltype(&nvrtcGetProgramLog) log = nullptr;
+  decltype(&nvrtcGetCUBINSize) cubin_size = nullptr;
+  decltype(&nvrtcGetCUBIN) cubin = nullptr;
+  decltype(&nvrtcDestroyProgram) destroy = nullptr;
+  decltype(&cuModuleLoadData) load = nullptr;
+  decltype(&cuModuleGetFunction) get = nullptr;
+  decltype(&cuLaunchKernel) launch = nullptr;
+};
+inline const XjitApi& xjit_api() {
+  static XjitApi a = [] {
+    XjitApi r;
+    void* h = dlopen("libnvrtc.so.12", RTLD_NOW | RTLD_LOCAL);
+    if (!h) h = dlopen("libnvrtc.so", RTLD_NOW | RTLD_LOCAL);
+    if (!h) return r;
+    r.create = (decltype(r.create))dlsym(h, "nvrtcCreateProgram");
+    r.compile = (decltype(r.compile))dlsym(h, "nvrtcCompileProgram");
+    r.log_size = (decltype(r.log_size))dlsym(h, "nvrtcGetProgramLogSize");
+    r.log = (decltype(r.log))dlsym(h, "nvrtcGetProgramLog");
+    r.cubin_size = (decltype(r.cubin_size))dlsym(h, "nvrtcGetCUBINSize");
+    r.cubin = (decltype(r.cubin))dlsym(h, "nvrtcGetCUBIN");
+    r.destroy = (decltype(r.destroy))dlsym(h, "nvrtcDestroyProgram");
+    auto entry = [](const char* name, void** fn) {
+      cudaDriverEntryPointQueryResult q;
+      return cudaGetDriverEntryPoint(name, fn, cudaEnableDefault, &q) == cudaSuccess &&
+             q == cudaDriverEntryPointSuccess && *fn;
+    };
+    void *l = nullptr, *g = nullptr, *k = nullptr;
+    const bool drv = entry("cuModuleLoadData", &l) && entry("cuModuleGetFunction", &g) && entry("cuLaunchKernel", &k);
+    cudaGetLastError();
+    r.load = (decltype(r.load))l;
+    r.get = (decltype(r.get))g;
+    r.launch = (decltype(r.launch))k;
+    r.ok = drv && r.create && r.compile && r.log_size && r.log && r.cubin_size && r.cubin && r.destroy;
+    return r;
+  }();
+  return a;
+}
+
+inline std::atomic<uint64_t> g_xjit_compiled{0};
+inline uint64_t xjit_compiled() { return g_xjit_compiled.load(); }
+
+// The compiled quotient kernel of `xc` on the current device (compiled on
+// first use, then cached); null when it cannot be had (the interpreter runs).
+inline CUfunction xjit_quotient(const XCode& xc) {
+  if (xc.code.empty() || xc.code.size() > XJIT_MAX_INST) return nullptr;
+  const XjitApi& api = xjit_api();
+  if (!api.ok) return nullptr;
+  int dev = 0;
+  LG_CK(cudaGetDevice(&dev));
+  const std::string src = xjit_source(xc);
+  static std::mutex mu;
+  static std::map<std::pair<int, std::string>, CUfunction> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  auto key = std::make_pair(dev, src);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  CUfunction fn = nullptr;
+  nvrtcProgram prog = nullptr;
+  const char* hdr[] = {xjit_field_src()};
+  const char* hname[] = {"field.cuh"};
+  if (api.create(&prog, src.c_str(), "lg_qx.cu", 1, hdr, hname) == NVRTC_SUCCESS) {
+    const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device"};
+    size_t sz = 0;
+    if (api.compile(prog, 3, opts) == NVRTC_SUCCESS && api.cubin_size(prog, &sz) == NVRTC_SUCCESS && sz) {
+      std::vector<char> bin(sz);
+      CUmodule mod = nullptr;
+      if (api.cubin(prog, bin.data()) == NVRTC_SUCCESS && api.load(&mod, bin.data()) == CUDA_SUCCESS &&
+          api.get(&fn, mod, "lg_qx") != CUDA_SUCCESS)
+        fn = nullptr;
+    }
+    api.destroy(&prog);
+  }
+  cache[key] = fn;  // a failure is remembered too: the interpreter serves that program
+  if (fn) g_xjit_compiled.fetch_add(1);
+  return fn;
+}
+
+inline void xjit_launch(CUfunction fn, dim3 grid, const QxJob* jobs_d, const E6* coins_d, cudaStream_t s) {
+  void* args[] = {(void*)&jobs_d, (void*)&coins_d};
+  if (xjit_api().launch(fn, grid.x, grid.y, grid.z, 128, 1, 1, 0, (CUstream)s, args, nullptr) != CUDA_SUCCESS)
+    throw Error(LG_ERR_CUDA, "launch of a compiled constraint kernel failed");
+}
+
+}  // namespace lg

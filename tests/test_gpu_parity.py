@@ -351,7 +351,7 @@ def test_tuning_never_changes_proofs(ctx):
     try:
         for params in ({"merkle_tail": 2, "merkle_subtree": 2, "p2_leaf_min_per_sm": 0, "p2_node_min_per_sm": 0,
                         "p2_inject_min_per_sm": 0, "inject_block": 1024, "leaf_block": 32, "lde_split": 0,
-                        "lde_fwd_threads": 256, "fri_tail_leaves": 0},
+                        "lde_fwd_threads": 256, "fri_tail_leaves": 0, "quotient_jit": 0},
                        {"merkle_tail": 1024, "merkle_subtree": 1024, "p2_leaf_min_per_sm": 1 << 20,
                         "p2_node_min_per_sm": 1 << 20, "p2_inject_min_per_sm": 1 << 20, "inject_block": 32,
                         "leaf_block": 1024, "lde_split": 1, "lde_fwd_threads": 1024, "fri_tail_leaves": 65536},
@@ -366,7 +366,7 @@ def test_tuning_never_changes_proofs(ctx):
     finally:
         ctx.apply_tuning(defaults)
     for name, value in (("merkle_tail", 48), ("merkle_tail", 2048), ("merkle_subtree", 1), ("merkle_subtree", 48),
-                        ("leaf_block", 16), ("lde_split", 2), ("lde_fwd_threads", 128), ("fri_tail_leaves", 3),
+                        ("leaf_block", 16), ("lde_split", 2), ("lde_fwd_threads", 128), ("fri_tail_leaves", 3), ("quotient_jit", 2),
                         ("no_such", 1)):
         with pytest.raises(LoomError) as e:
             ctx.set_tuning(name, value)
@@ -426,6 +426,30 @@ def test_fri_tail_block_gives_identical_proofs(ctx, tail):
     finally:
         ctx.set_tuning("fri_tail_leaves", saved)
     assert got == oracle.prove(compiled.words, mont, 20)
+
+
+@pytest.mark.parametrize("build", ["plonk", "mixed_lookup"])
+def test_compiled_constraint_kernels_give_identical_proofs(ctx, build):
+    """The quotient's constraint bytecode compiled to kernels at run time
+    (tuning quotient_jit = 1, the default) against the bytecode interpreter
+    (0): the same proof, equal to the oracle's, with compiled kernels in use."""
+    from loom_b200 import _lib
+    L = _lib.load()
+    if build == "plonk":
+        compiled, wit = plonk.build(3, 1 << 9, seed=31)
+    else:
+        compiled, wit = plonk.build_mixed([7, 5, 9, 5], seed=11)
+    mont = [F.to_mont(w) for w in wit]
+    saved = ctx.get_tuning("quotient_jit")
+    try:
+        ctx.set_tuning("quotient_jit", 0)
+        interp = ctx.prove(compiled.words, mont, 16)
+        ctx.set_tuning("quotient_jit", 1)
+        jit = ctx.prove(compiled.words, mont, 16)
+    finally:
+        ctx.set_tuning("quotient_jit", saved)
+    assert jit == interp == oracle.prove(compiled.words, mont, 16)
+    assert L.lg_jit_kernels() >= 1
 
 
 def test_lde_launch_shapes_give_identical_results(ctx):
