@@ -234,13 +234,16 @@ struct Prover {
       else ext_of[i] = node_ext((uint32_t)i);
     }
   }
-  void collect(uint32_t id, std::vector<char>& seen) {
+  // Marks the nodes under id in `seen`; appends each newly marked one to
+  // `order` when given.
+  void collect(uint32_t id, std::vector<char>& seen, std::vector<uint32_t>* order = nullptr) {
     std::vector<uint32_t> st = {id};
     while (!st.empty()) {
       uint32_t x = st.back();
       st.pop_back();
       if (seen[x]) continue;
       seen[x] = 1;
+      if (order) order->push_back(x);
       if (is_binary(pg.nodes[x].op)) { st.push_back(pg.nodes[x].a); st.push_back(pg.nodes[x].b); }
     }
   }
@@ -466,20 +469,25 @@ struct Prover {
       fold_root[m] = (int)res;
     }
     compute_ext();
+    std::vector<int> memo(pg.nodes.size(), INT32_MIN);  // a node's degree does not depend on the module
     for (uint32_t m = 0; m < pg.modules.size(); m++) {
       if (fold_root[m] < 0) continue;
-      std::vector<int> memo(pg.nodes.size(), INT32_MIN);
       degree[m] = node_degree((uint32_t)fold_root[m], memo);
       root_ext[m] = ext_of[fold_root[m]];
     }
     // shift schedule (internal/protocol/schedule.go:92-157)
+    std::vector<char> seen(pg.nodes.size(), 0);
+    std::vector<uint32_t> reach;
     for (uint32_t m : mod_order) {
       if (fold_root[m] < 0) continue;
-      std::vector<char> seen(pg.nodes.size(), 0);
-      collect((uint32_t)fold_root[m], seen);
+      // the nodes under this module's relation only (marks cleared after)
+      reach.clear();
+      collect((uint32_t)fold_root[m], seen, &reach);
       int64_t n = (int64_t)mod_n(m);
-      for (uint32_t id = 0; id < pg.nodes.size(); id++) {
-        if (!seen[id] || pg.nodes[id].op != OP_COL) continue;
+      std::sort(reach.begin(), reach.end());  // node order, as a full scan visits them
+      for (uint32_t id : reach) seen[id] = 0;
+      for (uint32_t id : reach) {
+        if (pg.nodes[id].op != OP_COL) continue;
         const Column& cl = pg.columns[pg.nodes[id].a];
         if (cl.kind == KIND_LAGRANGE) continue;
         int64_t sh = (int32_t)pg.nodes[id].b;
