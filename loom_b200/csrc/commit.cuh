@@ -311,7 +311,10 @@ inline unsigned tail_threads(uint32_t top, int fold_first) {
 
 // nodes must already hold the leaves at [n_leaves, 2 n_leaves).  Reads the
 // root back (the transcript needs it) unless read_root is false.
-inline void build_tree(Ctx& c, TreeDev& t, bool read_root = true) {
+// With fs, a tree whose top runs as one k_merkle_tail block also gets the
+// challenge over its root there (fs->out); returns whether it did (else the
+// caller computes it).
+inline bool build_tree(Ctx& c, TreeDev& t, bool read_root = true, const FsTail* fs = nullptr) {
   const uint32_t nl = 1u << t.log_leaves;
   for (size_t k = 0; k < t.inj.size(); k++)
     if (t.inj_log_w[k] > t.log_leaves || (k && t.inj_log_w[k] > t.inj_log_w[k - 1]))
@@ -354,6 +357,7 @@ inline void build_tree(Ctx& c, TreeDev& t, bool read_root = true) {
       LG_LAUNCH();
     });
   };
+  bool fused = false;
   // blocks = 1: the tree top from width `top` (k_merkle_tail); blocks > 1:
   // the levels top/2 .. blocks, one subtree per block
   auto subtrees = [&](uint32_t top, int fold_first, uint32_t blocks) {
@@ -362,9 +366,13 @@ inline void build_tree(Ctx& c, TreeDev& t, bool read_root = true) {
       const uint32_t w = 1u << t.inj_log_w[k];
       if ((w < top && w >= blocks) || (fold_first && w == top)) perms += w;
     }
+    const bool with_fs = blocks == 1 && fs;
+    if (with_fs) fused = true;
     c.timed(blocks == 1 ? "merkle_tail" : "merkle_level", 96.0 * perms, perms, [&] {
-      k_merkle_tail<<<blocks, tail_threads(top / blocks, fold_first), 0, c.stream>>>(
-          t.nodes->p, top, fold_first, (const InjRef*)ref_tab->p, (uint32_t)refs.size());
+      // at least one warp: the challenge needs one
+      const unsigned thr = std::max(32u, tail_threads(top / blocks, fold_first));
+      k_merkle_tail<<<blocks, thr, 0, c.stream>>>(t.nodes->p, top, fold_first, (const InjRef*)ref_tab->p,
+                                                  (uint32_t)refs.size(), with_fs ? *fs : FsTail{});
       LG_LAUNCH();
     });
   };
@@ -405,10 +413,11 @@ inline void build_tree(Ctx& c, TreeDev& t, bool read_root = true) {
     }
     subtrees(start, 0, 1);
   }
-  if (!read_root) return;  // the root stays on the device (nodes[1])
+  if (!read_root) return fused;  // the root stays on the device (nodes[1])
   uint32_t* h = c.host_staging(8);
   c.d2h(h, t.nodes->p + 8, 8);
   memcpy(t.root.v, h, 32);
+  return fused;
 }
 
 struct GroupSpec {

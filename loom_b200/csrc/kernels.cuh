@@ -494,10 +494,16 @@ __global__ void k_merkle_inject1(uint32_t* nodes, uint32_t start, const uint32_t
 // launches of the levels top/2 .. B, which are latency bound, by one.  When
 // fold_first, the injections of width `top` fold first (a tree whose leaf
 // level fits in one block).
+// With fs.out set (one block only), the block then hashes the challenge that
+// binds the root: fs.out = sponge(fs.pre[0..n_pre) || fs.prev[0..8) || root),
+// as k_fs_challenge, which it replaces for the FRI layer trees.
 struct InjRef { const uint32_t* leaves; uint32_t width; };
-__global__ void k_merkle_tail(uint32_t* nodes, uint32_t top, int fold_first, const InjRef* inj, uint32_t n_inj) {
+struct FsTail { const uint32_t* pre; uint32_t n_pre; const uint32_t* prev; uint32_t* out; };
+__global__ void k_merkle_tail(uint32_t* nodes, uint32_t top, int fold_first, const InjRef* inj, uint32_t n_inj,
+                              FsTail fs) {
   __shared__ uint32_t keys[144];
   __shared__ const uint32_t* chain[64];
+  __shared__ uint32_t msg[64];
   p2_load_full_keys(keys);
   P2Lane L;
   L.init();
@@ -528,6 +534,24 @@ __global__ void k_merkle_tail(uint32_t* nodes, uint32_t top, int fold_first, con
     }
     __syncthreads();
     fold(w);
+  }
+  if (fs.out && warp == 0) {  // the root is nodes[1], written before the last barrier
+    const uint32_t total = fs.n_pre + 16;
+    for (uint32_t i = L.lane; i < total; i += 32)
+      msg[i] = i < fs.n_pre ? fs.pre[i] : (i < fs.n_pre + 8 ? fs.prev[i - fs.n_pre] : nodes[8 + i - fs.n_pre - 8]);
+    __syncwarp();
+    uint32_t x[4] = {0, 0, 0, 0};
+    for (uint32_t b0 = 0; b0 < total; b0 += 16) {
+      const uint32_t len = min(16u, total - b0);
+      if (L.idx < 4)
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+          if (4 * (uint32_t)L.idx + k < len) x[k] = msg[b0 + 4 * L.idx + k];
+      p2c_permute(x, L, keys);
+    }
+    if (L.lane < 2)
+#pragma unroll
+      for (int k = 0; k < 4; k++) fs.out[4 * L.lane + k] = x[k];
   }
 }
 

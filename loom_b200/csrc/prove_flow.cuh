@@ -586,7 +586,7 @@ inline Digest Prover::commit_levels() {
 
 // ---- one FRI round: fold layer j (internal/fri/fri.go:1177-1198), then the
 // levels that enter at round j + 1 and the next layer's tree
-inline bool Prover::fri_fold_round(int j, bool read_root, Digest* next_root) {
+inline bool Prover::fri_fold_round(int j, bool read_root, Digest* next_root, const FsTail* next_fs, bool* fused) {
   if (fri_next < 0) throw Error(LG_ERR_INVALID, "the FRI levels are not committed yet");
   if (j != fri_next) throw Error(LG_ERR_INVALID, "FRI rounds run in order: the next one is fri_fold_" + std::to_string(fri_next));
   if (!chal_ready[j]) throw Error(LG_ERR_INVALID, "challenge fri_fold_" + std::to_string(j) + " has not been set");
@@ -635,7 +635,8 @@ inline bool Prover::fri_fold_round(int j, bool read_root, Digest* next_root) {
   t.log_leaves = (uint32_t)(LOG_N_FRI - (j + 1) - 1);
   t.nodes = std::make_shared<DBuf>((size_t)16 << t.log_leaves, c.stream);
   launch_leaves(c, {leaf_group(running->p, 0, 1, (uint32_t)(LOG_N_FRI - (j + 1)), t.nodes->p + ((size_t)8 << t.log_leaves))});
-  build_tree(c, t, read_root);
+  const bool f = build_tree(c, t, read_root, next_fs);
+  if (fused) *fused = f;
   if (read_root) {
     fri_roots.push_back(t.root);
     *next_root = t.root;
@@ -1111,13 +1112,15 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
   if (c.tune.fri_tail_leaves)
     for (int j = r0 + 1; j < NR; j++)
       if (((size_t)1 << (LOG_N_FRI - (j + 1) - 1)) <= c.tune.fri_tail_leaves) { j_tail = j; break; }
+  bool fused = false;  // challenge j already hashed by the block that built tree j's top
   for (int j = r0; j < NR; j++) {
     if (j > r0) {
-      c.timed("fri_challenge", 0, 0, [&] {
-        k_fs_challenge<<<1, 32, 0, c.stream>>>(pre_d->p + pre_off[j], pre_len[j], chal->p + 8 * (size_t)(j - 1),
-                                               ftrees[j].nodes->p + 8, chal->p + 8 * (size_t)j);
-        LG_LAUNCH();
-      });
+      if (!fused)
+        c.timed("fri_challenge", 0, 0, [&] {
+          k_fs_challenge<<<1, 32, 0, c.stream>>>(pre_d->p + pre_off[j], pre_len[j], chal->p + 8 * (size_t)(j - 1),
+                                                 ftrees[j].nodes->p + 8, chal->p + 8 * (size_t)j);
+          LG_LAUNCH();
+        });
       chal_ready[j] = 1;
     }
     if (j == j_tail) {
@@ -1126,7 +1129,11 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
       break;
     }
     Digest unused;
-    fri_fold_round(j, false, &unused);
+    FsTail ft{};
+    if (j + 1 < NR)
+      ft = FsTail{pre_d->p + pre_off[j + 1], pre_len[j + 1], chal->p + 8 * (size_t)j, chal->p + 8 * (size_t)(j + 1)};
+    fused = false;
+    fri_fold_round(j, false, &unused, j + 1 < NR ? &ft : nullptr, &fused);
   }
   {
     // one read-back: final polynomial, device challenges, layer roots

@@ -1303,7 +1303,10 @@ struct Prover {
   Digest commit_levels();                 // fri.Prove's levels tree (internal/fri/fri.go:294-317)
   // fold round j (foldLayerExt) with the challenge at chal + 8 j, then the
   // next layer's commitment; true with its root (read back when read_root)
-  bool fri_fold_round(int j, bool read_root, Digest* next_root);
+  // next_fs: hash the next fold challenge with the new tree's top when that
+  // runs as one block (*fused says whether it did)
+  bool fri_fold_round(int j, bool read_root, Digest* next_root, const FsTail* next_fs = nullptr,
+                      bool* fused = nullptr);
   void read_final_poly();
   // rounds j0 .. NR - 1 in one block (k_fri_tail), challenge j0 already on
   // the device; the same layers, trees and challenges as fri_fold_round
