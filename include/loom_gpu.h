@@ -133,7 +133,8 @@ int lg_ctx_set_leaf_mapping(lg_ctx* ctx, int lanes_per_permutation);
  *   "fri_tail_leaves"     the FRI rounds whose layer tree has at most this many
  *                         leaves run in one block, back to back (power of two,
  *                         2..65536; 0: a launch per step of every round)
- *   "quotient_jit"        1: each module's constraint bytecode is compiled to a
+ *   "quotient_jit"        1: the constraint bytecode of each module's quotient
+ *                         and of each grand product's ratio is compiled to a
  *                         kernel of its own at run time (NVRTC, cached per
  *                         program); 0: the bytecode interpreter
  * Unknown names or values out of range return LG_ERR_INVALID. */

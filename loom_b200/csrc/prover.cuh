@@ -903,6 +903,7 @@ struct Prover {
     std::vector<const uint32_t*> all_lanes;  // every step's lane table, one upload
     std::vector<size_t> lane_off;
     uint32_t max_regs = 1;
+    std::vector<std::pair<const XCode*, const XCode*>> codes;  // per job: numerator, denominator bytecode
     for (const Step* st : steps) {
       uint32_t logn = pg.modules[st->module].log_n;
       size_t n = (size_t)1 << logn;
@@ -927,6 +928,7 @@ struct Prover {
       auto res = std::make_shared<DBuf>(6 * n, c.stream);
       keep.insert(keep.end(), {ratio, totals, pre});
       jobs.push_back(GpJob{cs.dev[0], cs.dev[1], nullptr, ratio->p, (int)logn});
+      codes.push_back({&cs.xc[0], &cs.xc[1]});
       ScanJob sj{ratio->p, n, totals->p, pre->p, res->p, nt};
       if (st->type == STEP_RATIO) {  // inclusive products; the end is exposed
         if (pg.columns[st->out].field != 1 || pg.columns[st->out].module != st->module)
@@ -949,13 +951,39 @@ struct Prover {
         max_n = std::max<uint32_t>(max_n, (uint32_t)scans[i].n);
         max_nt = std::max(max_nt, scans[i].nt);
       }
-      std::vector<GpJob> jv(jobs.begin() + first, jobs.begin() + first + count);
+      // ratios: compiled kernels per distinct (numerator, denominator)
+      // program (xjit.cuh), the interpreter for the rest
+      std::vector<GpJob> jv;
+      std::map<CUfunction, std::pair<std::vector<GpxJob>, uint32_t>> jit;  // jobs, largest n
+      uint32_t max_ni = 0;
+      for (size_t i = first; i < first + count; i++) {
+        const uint32_t ni = (uint32_t)scans[i].n;
+        if (CUfunction f = c.tune.quotient_jit ? xjit_gp(*codes[i].first, *codes[i].second) : nullptr) {
+          auto& g = jit[f];
+          g.first.push_back(GpxJob{jobs[i].lanes, jobs[i].ratio, jobs[i].logn});
+          g.second = std::max(g.second, ni);
+        } else {
+          jv.push_back(jobs[i]);
+          max_ni = std::max(max_ni, ni);
+        }
+      }
       std::vector<ScanJob> sv(scans.begin() + first, scans.begin() + first + count);
-      auto jd = upload_vec(c, jv), sd = upload_vec(c, sv);
+      std::vector<std::pair<CUfunction, DBufP>> jit_d;
+      for (auto& kv : jit) jit_d.push_back({kv.first, upload_vec(c, kv.second.first)});
+      DBufP jd = jv.empty() ? DBufP() : upload_vec(c, jv);
+      auto sd = upload_vec(c, sv);
       c.timed("grand_product", 0, 0, [&] {
-        k_gp_ratio<<<dim3((max_n + T - 1) / T, (unsigned)count), T, smem, c.stream>>>((const GpJob*)jd->p,
-                                                                                      (const E6*)coins_d->p);
-        LG_LAUNCH();
+        for (auto& fd : jit_d) {
+          const auto& g = jit.at(fd.first);
+          xjit_launch(fd.first, dim3((g.second + 127) / 128, (unsigned)g.first.size()), fd.second->p,
+                      (const E6*)coins_d->p, c.stream);
+          g_launches.fetch_add(1);
+        }
+        if (!jv.empty()) {
+          k_gp_ratio<<<dim3((max_ni + T - 1) / T, (unsigned)jv.size()), T, smem, c.stream>>>((const GpJob*)jd->p,
+                                                                                            (const E6*)coins_d->p);
+          LG_LAUNCH();
+        }
         k_scan_tiles<<<dim3(max_nt, (unsigned)count), SCAN_BLOCK, 0, c.stream>>>((const ScanJob*)sd->p);
         LG_LAUNCH();
         k_tile_prefix<<<(unsigned)((count + 63) / 64), 64, 0, c.stream>>>((const ScanJob*)sd->p, (uint32_t)count);
