@@ -602,18 +602,32 @@ struct Transcript {
   Digest compute(const std::string& n) {
     auto it = index.find(n);
     if (it == index.end()) throw Error(LG_ERR_INVALID, "unknown challenge " + n);
-    size_t i = it->second;
-    if (chs[i].done) return chs[i].value;
+    return compute_at(it->second);
+  }
+  // By position in declaration order (a long chain such as the query
+  // challenges, without a lookup per step).
+  size_t at(const std::string& n) const {
+    auto it = index.find(n);
+    if (it == index.end()) throw Error(LG_ERR_INVALID, "unknown challenge " + n);
+    return it->second;
+  }
+  void bind_at(size_t i, const uint32_t* v, size_t len) {
+    if (chs.at(i).done) throw Error(LG_ERR_INVALID, "challenge already computed " + chs[i].name);
+    chs[i].bindings.insert(chs[i].bindings.end(), v, v + len);
+  }
+  Digest compute_at(size_t i) {
+    Ch& ch = chs.at(i);
+    if (ch.done) return ch.value;
     HostSponge h;
-    for (uint32_t x : string_to_elements(0x46534944u, n)) h.write(x);
+    for (uint32_t x : string_to_elements(0x46534944u, ch.name)) h.write(x);
     if (i) {
-      if (!chs[i - 1].done) throw Error(LG_ERR_INVALID, "previous challenge not computed for " + n);
+      if (!chs[i - 1].done) throw Error(LG_ERR_INVALID, "previous challenge not computed for " + ch.name);
       for (int k = 0; k < 8; k++) h.write(chs[i - 1].value.v[k]);
     }
-    for (uint32_t x : chs[i].bindings) h.write(x);
-    h.sum(chs[i].value.v);
-    chs[i].done = true;
-    return chs[i].value;
+    for (uint32_t x : ch.bindings) h.write(x);
+    h.sum(ch.value.v);
+    ch.done = true;
+    return ch.value;
   }
 };
 inline E6 digest_e6(const Digest& d) { E6 r; for (int i = 0; i < 6; i++) r.c[i] = d.v[i]; return r; }

@@ -1191,11 +1191,12 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
   }
   c.phase("fri rounds");
   std::vector<uint32_t> pos(num_queries);
+  const size_t q0 = num_queries ? fs.at("fri_query_0") : 0;  // declared one after another
   for (uint32_t k = 0; k < num_queries; k++) {
-    Digest ch = fs.compute("fri_query_" + std::to_string(k));
+    Digest ch = fs.compute_at(q0 + k);
     uint64_t s = (((uint64_t)from_mont(ch.v[0]) << 31) ^ (uint64_t)from_mont(ch.v[1])) % (1ull << LOG_N_FRI);
     pos[k] = (uint32_t)s;
-    if (k + 1 < num_queries) fs.bind("fri_query_" + std::to_string(k + 1), ch.v, 8);
+    if (k + 1 < num_queries) fs.bind_at(q0 + k + 1, ch.v, 8);
   }
   c.phase("query challenges");
   return open_and_encode(pos, out, out_cap, in_out);
