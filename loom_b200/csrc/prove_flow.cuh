@@ -172,6 +172,12 @@ struct OpenPlan {
   }
 };
 
+struct Prover::OpenPrep {
+  OpenPlan op;
+  std::vector<SectionSrc> lvl_sec;
+  SectionSrc fri_sec{}, batch_sec{};
+};
+
 // Length of an encoding, counted without writing (the Writer's methods).
 struct Sizer {
   size_t off = 0;
@@ -706,13 +712,15 @@ inline void Prover::read_final_poly() {
 
 // ---- openings: one gather into a staging buffer, one read-back; then the
 // canonical encoding (same order as the proof structs)
-inline size_t Prover::open_and_encode(const std::vector<uint32_t>& pos, uint8_t* out, size_t out_cap, bool* in_out) {
-  if (final_poly.empty()) throw Error(LG_ERR_INVALID, "the FRI final polynomial is not computed yet");
-  if (pos.size() != num_queries) throw Error(LG_ERR_INVALID, "one position per query is needed");
-  for (uint32_t s : pos)
-    if (s >= (1u << LOG_N_FRI)) throw Error(LG_ERR_INVALID, "query position out of range");
+// The openings' word map (rows, paths, sections) needs only where the
+// layers, trees and batches live, not the positions: lg_prove builds it while
+// the device finishes the FRI rounds.
+inline void Prover::plan_openings() {
+  if (fri_next != NR) throw Error(LG_ERR_INVALID, "the FRI rounds are not all folded yet");
+  oplan = std::make_shared<OpenPrep>();
+  OpenPlan& OP = oplan->op;
+  std::vector<SectionSrc>& lvl_sec = oplan->lvl_sec;
   auto jl = [&](size_t l) { return MAX_LOG_MODULE - (int)lvl_log[l]; };
-  OpenPlan OP;
   std::vector<uint64_t> fri_row_off(NR), fri_path_off(NR), lvl_row_off(L);
   for (int j = r0; j < NR; j++) {
     size_t n_j = (size_t)1 << (LOG_N_FRI - j);
@@ -721,7 +729,7 @@ inline size_t Prover::open_and_encode(const std::vector<uint32_t>& pos, uint8_t*
   }
   for (size_t l = 1; l < L; l++)
     lvl_row_off[l] = OP.add_rows(lvl[l]->p, (size_t)1 << (lvl_log[l] + RATE_LOG), 6, (uint32_t)jl(l));
-  std::vector<SectionSrc> lvl_sec(L);
+  lvl_sec.assign(L, SectionSrc{});
   for (size_t l = 1; l < L; l++) {  // FRI level openings (one section per level)
     OP.begin();
     OP.konst(1);
@@ -741,7 +749,7 @@ inline size_t Prover::open_and_encode(const std::vector<uint32_t>& pos, uint8_t*
     OP.copy(fri_path_off[j], 8 * (size_t)ftrees[j].log_leaves);
     OP.konst(0);
   }
-  const SectionSrc fri_sec = OP.end(num_queries);
+  oplan->fri_sec = OP.end(num_queries);
   std::vector<OpenBatch> obs;
   for (size_t b = 0; b < committed.size(); b++) {
     OpenBatch ob{&committed[b], {}, {}};
@@ -751,7 +759,19 @@ inline size_t Prover::open_and_encode(const std::vector<uint32_t>& pos, uint8_t*
     }
     obs.push_back(ob);
   }
-  const SectionSrc batch_sec = OP.batches_section(obs, num_queries);
+  oplan->batch_sec = OP.batches_section(obs, num_queries);
+}
+
+inline size_t Prover::open_and_encode(const std::vector<uint32_t>& pos, uint8_t* out, size_t out_cap, bool* in_out) {
+  if (final_poly.empty()) throw Error(LG_ERR_INVALID, "the FRI final polynomial is not computed yet");
+  if (pos.size() != num_queries) throw Error(LG_ERR_INVALID, "one position per query is needed");
+  for (uint32_t s : pos)
+    if (s >= (1u << LOG_N_FRI)) throw Error(LG_ERR_INVALID, "query position out of range");
+  if (!oplan) plan_openings();
+  std::shared_ptr<OpenPrep> prep = std::move(oplan);
+  OpenPlan& OP = prep->op;
+  const std::vector<SectionSrc>& lvl_sec = prep->lvl_sec;
+  const SectionSrc fri_sec = prep->fri_sec, batch_sec = prep->batch_sec;
   DBufP asm_d = OP.run_device(c, pos);
   c.phase("openings gather");
   // The encoding in proof order; `section(W, sc)` appends a per-query
@@ -1135,6 +1155,7 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
     fused = false;
     fri_fold_round(j, false, &unused, j + 1 < NR ? &ft : nullptr, &fused);
   }
+  plan_openings();  // host work while the device finishes the rounds
   {
     // one read-back: final polynomial, device challenges, layer roots
     const size_t nroot = (size_t)(NR > r0 + 1 ? NR - r0 - 1 : 0);

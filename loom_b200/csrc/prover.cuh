@@ -132,6 +132,8 @@ struct Prover {
   size_t nj = 0;                            // its length
   int fri_next = -1;                        // next round to fold (-1: levels not committed)
   std::vector<uint32_t> final_poly;         // 6 lanes of nj words, once read back
+  struct OpenPrep;                          // the openings' word map (prove_flow.cuh)
+  std::shared_ptr<OpenPrep> oplan;  // (shared_ptr: complete only in prove_flow.cuh)
 
   // A prover dropped with the DEEP denominators still queued (a session
   // released before its DEEP phase) orders the frees of its buffers, which
@@ -1342,6 +1344,7 @@ struct Prover {
   // query openings at positions (openQueryExt, openCommittedAt) and the
   // canonical encoding of the whole proof
   size_t open_and_encode(const std::vector<uint32_t>& pos, uint8_t* out, size_t out_cap, bool* in_out);
+  void plan_openings();
   // challenge by its transcript name: challenge@loom_<r> and __zeta (E6 from
   // the digest's first six words), alpha_DEEP, fri_level_<l>_gamma,
   // fri_fold_<j> (the whole digest)
