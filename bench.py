@@ -16,6 +16,7 @@ same workload per step.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -382,6 +383,11 @@ def main():
     assert all(v == p.final_poly[0] for v in p.final_poly), "final FRI polynomial is not constant"
 
     # ---- timed: witness resident in HBM
+    # Python's cyclic garbage collector stays off through the timed loops: a
+    # full collection of this process's heap, triggered by the few objects a
+    # call allocates, stalled single steps by up to hundreds of milliseconds
+    gc.collect()
+    gc.disable()
     barrier()
     clocks = ClockSampler(device)
     clocks.start()
@@ -425,6 +431,7 @@ def main():
     pbp = bytes(out[:n])
     ctx.set_batched(True)
     clk = clocks.stop()
+    gc.enable()
     barrier()
     assert pbh == pb, "host-buffer and device-buffer proofs differ"
     assert pbp == pb, "plain and batched proofs differ"
@@ -436,6 +443,8 @@ def main():
     # ---- throughput: several proofs in flight, one context + stream each
     from loom_b200.pool import ProverPool
     thr = []
+    gc.collect()
+    gc.disable()  # as in the timed loops above
     for S in [int(x) for x in a.streams.split(",") if x]:
         with ProverPool(S, device, tparams) as pool:
             for _ in range(2):  # warm every context (buffers, pools, tables), twice
@@ -453,10 +462,12 @@ def main():
                 e1.record()
                 torch.cuda.synchronize()
                 assert all(o == pb for o in outs), "concurrent proofs differ from the single-stream proof"
+                del outs, futs
                 walls.append(e0.elapsed_time(e1))
             wall = statistics.median(walls)
             thr.append({"streams": S, "proofs": jobs, "ms": round(wall, 3), "proofs_per_s": round(jobs * 1e3 / wall, 3),
                         "ms_each_batch": [round(w, 3) for w in walls]})
+    gc.enable()
 
     # ---- batched form: 40 modules of uneven sizes (log2 rows 10-20, seeded)
     # with plonk gates, a copy constraint and a range lookup into a shared 2^8
