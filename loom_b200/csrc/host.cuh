@@ -279,7 +279,8 @@ struct Ctx {
     return b->p;
   }
   // Twiddles of the radix-16 passes for 2^logn points (4 <= logn), pass by
-  // pass in the tw16 layout of ntt16.cuh; built on the host once per size.
+  // pass in the tw16 layout of ntt16.cuh (canonical words, then their Shoup
+  // companions); built on the host once per size.
   const uint32_t* twiddles16(int logn) {
     auto it = tw16.find(logn);
     if (it != tw16.end()) return it->second->p;
@@ -288,7 +289,8 @@ struct Ctx {
     const uint32_t w = root_of_unity_mont(logn);
     pw[0] = MONT_ONE;
     for (uint32_t k = 1; k < n; k++) pw[k] = mul(pw[k - 1], w);
-    std::vector<uint32_t> tab(tw16_words(logn), 0);
+    const uint32_t W = tw16_words(logn);  // canonical twiddles, then their Shoup companions
+    std::vector<uint32_t> tab(2 * (size_t)W, 0);
     for (int dif = 0; dif < 2; dif++)
       for (int invd = 0; invd < 2; invd++)
         for (int p = 0; p < pass_count(logn); p++) {
@@ -301,7 +303,9 @@ struct Ctx {
             for (uint32_t tl = 0; tl < (1u << lo); tl++)
               for (uint32_t rl = 0; rl < m; rl++) {
                 const uint32_t e = ((tl + (rl << lo)) << (logn - st - 1)) & (n - 1);
-                tab[off + tl * m + rl] = pw[invd ? (n - e) & (n - 1) : e];
+                const uint32_t wc = from_mont(pw[invd ? (n - e) & (n - 1) : e]);
+                tab[off + tl * m + rl] = wc;
+                tab[W + off + tl * m + rl] = shoup(wc);
               }
           }
         }

@@ -55,6 +55,7 @@ __device__ __forceinline__ void ntt16_tile(uint32_t* S, const uint32_t* tw, bool
   static_assert(!STORE16 || DIF, "16-row stores follow the DIF pass plan");
   constexpr uint32_t groups = (1u << LOGL) >> 4;  // per column
   constexpr int np = (LOGL - ((LOGL & 3) ? (LOGL & 3) : 4)) / 4 + 1;
+  constexpr uint32_t comp = tw16_words(LOGL);
 #pragma unroll
   for (int p = 0; p < np; p++) {
     int lo = 0, s_lo = 0, s_hi = 0;
@@ -68,7 +69,7 @@ __device__ __forceinline__ void ntt16_tile(uint32_t* S, const uint32_t* tw, bool
         const uint32_t row = grp_index(t, r, lo);
         v[r] = p == 0 ? first(col, row) : S[tile_addr(row, col)];
       }
-      pass16<DIF>(v, t, lo, s_lo, s_hi, ptab, inverse);
+      pass16<DIF>(v, t, lo, s_lo, s_hi, ptab, comp, inverse);
       if constexpr (STORE16) {
         if (p == np - 1) {
           store(col, t, v);
