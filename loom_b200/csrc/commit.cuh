@@ -67,16 +67,18 @@ inline void big_ntt(Ctx& c, std::vector<BigNtt> jobs, int logn, bool inverse, co
   const int logr = logn / 2, logc = logn - logr;
   if (logr < 7 || logc > 11) throw Error(LG_ERR_UNSUPPORTED, "four-step transform size out of range");
   const size_t n = (size_t)1 << logn;
-  const uint32_t* tw_n = c.twiddles(logn);
   const uint32_t* tw_c = c.twiddles16(logc);
   const uint32_t* tw_r = c.twiddles16(logr);
-  // the large roots' powers as two small tables (tw_split): w_n and, for the
-  // coset shifts, w_{4n} (every job's t2 table is the w_{4n} powers)
-  const uint32_t* tw_n_hi = c.twiddles(logn - TW_SPLIT);
-  const uint32_t* t2_hi = c.twiddles(logn + RATE_LOG - TW_SPLIT);
-  for (auto& j : jobs)
+  // the large roots' powers as two small tables each (mul_split): w_n and,
+  // for the coset shifts, w_{4n}
+  const uint2* tw_n = c.split_powers(logn);
+  const uint2* t2s = c.split_powers(logn + RATE_LOG);
+  for (auto& j : jobs) {
     if (j.t2 && j.m2_mask != (uint32_t)((n << RATE_LOG) - 1))
       throw Error(LG_ERR_INVALID, "four-step coset table of another size");
+    j.c0c = from_mont(j.c0);
+    j.c0s = shoup(j.c0c);
+  }
   // scratch chunks of 2^26 words at most (256 MiB)
   const size_t per = std::max<size_t>(1, ((size_t)1 << 26) / n);
   const size_t smem_a = tile_words(logc) * 4, smem_b = tile_words(logr) * 4;
@@ -93,7 +95,7 @@ inline void big_ntt(Ctx& c, std::vector<BigNtt> jobs, int logn, bool inverse, co
         constexpr int C_ = decltype(LC)::value;
         allow_smem(k_big_pass_a<C_>, smem_a);
         k_big_pass_a<C_><<<dim3((1u << logr) / BIG_TILE, (unsigned)cnt), thr_a, smem_a, c.stream>>>(
-            (const BigNtt*)jd->p, logn, logr, inverse ? 1 : 0, tw_n, tw_n_hi, t2_hi, tw_c);
+            (const BigNtt*)jd->p, logn, logr, inverse ? 1 : 0, tw_n, t2s, tw_c);
         LG_LAUNCH();
       });
       with_tile_size(logr, [&](auto LR) {

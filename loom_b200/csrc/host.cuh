@@ -215,6 +215,7 @@ struct Ctx {
   MemAcct mem;                   // device bytes this context holds (lg_ctx_mem_usage)
   std::map<int, DBufP> tw;       // log n -> w_n^j, j < n
   std::map<int, DBufP> tw16;     // log n -> the radix-16 passes' twiddle tables (tw16 layout, ntt16.cuh)
+  std::map<int, DBufP> tw_split; // log n -> w_n's powers as two small Shoup tables (split_powers)
   std::map<int, DBufP> gpow;     // log n -> g^k, k < n
   std::map<int, DBufP> ginvpow;  // log n -> g^-k, k < n
   std::map<int, DBufP> cshift;   // log n -> (g w_4n^c)^k, k < n, for c = 0..3 (4 tables back to back)
@@ -315,6 +316,36 @@ struct Ctx {
     LG_CK(cudaStreamSynchronize(stream));  // the host table goes out of scope
     tw16[logn] = b;
     return b->p;
+  }
+  // Powers of w = w_{2^logw} (logw > 11) for mul_split (ntt_large.cuh):
+  // 2^11 pairs (w^i canonical, its Shoup companion), then 2^(logw - 11)
+  // pairs for w^(2^11 i); built on the host once per size.
+  const uint2* split_powers(int logw) {
+    auto it = tw_split.find(logw);
+    if (it != tw_split.end()) return reinterpret_cast<const uint2*>(it->second->p);
+    if (logw <= 11 || logw > 30) throw Error(LG_ERR_INVALID, "split powers of an unsupported order");
+    const uint32_t nlo = 1u << 11, nhi = 1u << (logw - 11);
+    std::vector<uint32_t> tab(2 * (size_t)(nlo + nhi));
+    const uint32_t w = root_of_unity_mont(logw);
+    uint32_t x = MONT_ONE;
+    for (uint32_t i = 0; i < nlo; i++) {
+      tab[2 * i] = from_mont(x);
+      tab[2 * i + 1] = shoup(tab[2 * i]);
+      x = mul(x, w);
+    }
+    const uint32_t step = x;  // w^(2^11)
+    x = MONT_ONE;
+    for (uint32_t i = 0; i < nhi; i++) {
+      tab[2 * (nlo + i)] = from_mont(x);
+      tab[2 * (nlo + i) + 1] = shoup(tab[2 * (nlo + i)]);
+      x = mul(x, step);
+    }
+    ArenaScope cached(nullptr);  // kept across proves: never from the arena
+    auto b = std::make_shared<DBuf>(tab.size(), stream);
+    LG_CK(cudaMemcpyAsync(b->p, tab.data(), tab.size() * 4, cudaMemcpyHostToDevice, stream));
+    LG_CK(cudaStreamSynchronize(stream));  // the host table goes out of scope
+    tw_split[logw] = b;
+    return reinterpret_cast<const uint2*>(b->p);
   }
   // the table a transform kernel takes: tw16 for the radix-16 passes, the
   // plain powers below 16 points (radix-2 stages)

@@ -107,6 +107,7 @@ void lg_ctx_destroy(lg_ctx* ctx) {
   // every cached device buffer frees on the stream: release them while it exists
   ctx->c.tw.clear();
   ctx->c.tw16.clear();
+  ctx->c.tw_split.clear();
   ctx->c.gpow.clear();
   ctx->c.ginvpow.clear();
   ctx->c.cshift.clear();

@@ -27,10 +27,11 @@ struct BigNtt {
   const uint32_t* in;
   uint32_t* out;
   uint32_t* scratch;       // n words
-  const uint32_t* t1;      // optional table of n words
-  const uint32_t* t2;      // optional table of m2 words (a power of two)
+  const uint32_t* t1;      // optional table of n words (Montgomery)
+  const uint32_t* t2;      // optional: the coset shift w_4n^((e2 k) mod 4n) (set: the w_4n table)
   uint32_t m2_mask, e2;    // t2 index = (e2 * k) & m2_mask
   uint32_t c0;             // constant factor (Montgomery)
+  uint32_t c0c, c0s;       // c0 canonical and its Shoup companion (big_ntt sets them)
   int out_bitrev;
 };
 
@@ -92,21 +93,21 @@ __device__ __forceinline__ void ntt16_tile(uint32_t* S, const uint32_t* tw, bool
   }
 }
 
-// A power w^e of a root w of order 2^(11 + k) from two small tables that
-// stay in L1: lo[i] = w^i (i < 2^11, the first entries of the full table) and
-// hi[i] = w^(2^11 i); one product instead of a load from a table of megabytes.
+// A product v w^e by a power of a root w of order 2^(11 + k), from two small
+// tables that stay in L1: lo[i] = w^i (i < 2^11) and hi[i] = w^(2^11 i), each
+// entry a canonical word with its Shoup companion (Ctx::split_powers): two
+// Shoup products instead of a table product and a Montgomery product.
 constexpr int TW_SPLIT = 11;
-__device__ __forceinline__ uint32_t tw_split(const uint32_t* lo, const uint32_t* hi, uint32_t e) {
-  return mul(__ldg(lo + (e & ((1u << TW_SPLIT) - 1))), __ldg(hi + (e >> TW_SPLIT)));
+__device__ __forceinline__ uint32_t mul_split(uint32_t v, const uint2* tab, uint32_t e) {
+  const uint2 a = __ldg(tab + (e & ((1u << TW_SPLIT) - 1))), b = __ldg(tab + (1u << TW_SPLIT) + (e >> TW_SPLIT));
+  return mulc(mulc_lazy(v, a.x, a.y), b.x, b.y);
 }
 
-// tw_n: w_n^j (its first 2^11 entries are read), tw_n_hi: w_n^(2^11 j);
-// t2_hi: the same split of the jobs' t2 tables (w_{m2}^(2^11 j)); tw_c: the
-// tw16 tables of C points.  Block (x, y): tile x of job y.
+// tw_n: w_n split (mul_split layout); t2s: the same for w_4n (the coset
+// shifts); tw_c: the tw16 tables of C points.  Block (x, y): tile x of job y.
 template <int LOGC>
 __global__ void __launch_bounds__(512, 2) k_big_pass_a(const BigNtt* jobs, int logn, int logr, int inverse,
-                                                    const uint32_t* tw_n, const uint32_t* tw_n_hi,
-                                                    const uint32_t* t2_hi, const uint32_t* tw_c) {
+                                                    const uint2* tw_n, const uint2* t2s, const uint32_t* tw_c) {
   extern __shared__ uint32_t S[];
   const BigNtt J = jobs[blockIdx.y];
   const uint32_t R = 1u << logr, n = 1u << logn;
@@ -114,16 +115,16 @@ __global__ void __launch_bounds__(512, 2) k_big_pass_a(const BigNtt* jobs, int l
   auto first = [&](uint32_t col, uint32_t k2) {
     const uint32_t k = (k1_0 + col) + R * k2;
     uint32_t v = J.in[k];
-    if (J.c0 != MONT_ONE) v = mul(v, J.c0);
+    if (J.c0 != MONT_ONE) v = mulc(v, J.c0c, J.c0s);
     if (J.t1) v = mul(v, __ldg(J.t1 + k));
-    if (J.t2) v = mul(v, tw_split(J.t2, t2_hi, (J.e2 * k) & J.m2_mask));
+    if (J.t2) v = mul_split(v, t2s, (J.e2 * k) & J.m2_mask);
     return v;
   };
   auto store = [&](uint32_t col, uint32_t p, uint32_t v) {
     const uint32_t j2 = bitrev32(p, LOGC), k1 = k1_0 + col;
     uint32_t e = (uint32_t)(((uint64_t)j2 * k1) & (n - 1));
     if (inverse) e = (n - e) & (n - 1);
-    J.scratch[(uint64_t)j2 * R + k1] = mul(v, tw_split(tw_n, tw_n_hi, e));
+    J.scratch[(uint64_t)j2 * R + k1] = mul_split(v, tw_n, e);
   };
   ntt16_tile<true, LOGC>(S, tw_c, inverse != 0, first, store);
 }
