@@ -137,6 +137,10 @@ int lg_ctx_set_leaf_mapping(lg_ctx* ctx, int lanes_per_permutation);
  *                         and of each grand product's ratio is compiled to a
  *                         kernel of its own at run time (NVRTC, cached per
  *                         program); 0: the bytecode interpreter
+ *   "upload_split"        1: lg_prove with a host witness copies the columns
+ *                         the first round commits first and the others on a
+ *                         second stream while that round runs; 0: every
+ *                         column before the prove starts
  * Unknown names or values out of range return LG_ERR_INVALID. */
 int lg_ctx_set_tuning(lg_ctx* ctx, const char* name, int64_t value);
 int lg_ctx_get_tuning(lg_ctx* ctx, const char* name, int64_t* value);

@@ -182,7 +182,8 @@ class Context:
         return int(h.value), int(pk.value)
 
     TUNING_NAMES = ("p2_leaf_min_per_sm", "p2_node_min_per_sm", "p2_inject_min_per_sm", "merkle_tail",
-                    "merkle_subtree", "inject_block", "leaf_block", "lde_split", "lde_fwd_threads", "fri_tail_leaves", "quotient_jit")
+                    "merkle_subtree", "inject_block", "leaf_block", "lde_split", "lde_fwd_threads", "fri_tail_leaves", "quotient_jit",
+                    "upload_split")
 
     def set_tuning(self, name: str, value: int):
         """Launch-shape choice (see include/loom_gpu.h); proofs do not depend on it."""

@@ -211,6 +211,9 @@ struct Ctx {
   // through join_ev.
   cudaStream_t side = nullptr;
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+  // A host witness's columns that the first commitment does not take go up
+  // on `side` after the others, while round 0 runs; upload_ev marks the end.
+  cudaEvent_t upload_ev = nullptr;
   DevArena dev_arena;            // prove-scoped small device buffers
   MemAcct mem;                   // device bytes this context holds (lg_ctx_mem_usage)
   std::map<int, DBufP> tw;       // log n -> w_n^j, j < n
@@ -438,6 +441,8 @@ struct Ctx {
     uint32_t lde_split = 1;             // LDE as an inverse launch plus one block per (lane, coset)
     uint32_t lde_fwd_threads = 512;     // threads per block of the coset transforms (split LDE)
     uint32_t quotient_jit = 1;          // constraint bytecode (quotient, grand-product ratios) as compiled kernels (0: interpreter)
+    uint32_t upload_split = 1;          // host witness: round 0's columns first, the rest on the side stream while
+                                        // round 0 runs (0: every column before the prove starts)
     uint32_t fri_tail_leaves = 0;       // FRI rounds whose layer tree has at most this many leaves: one block (0: none;
                                         // 512 measured 14.09 ms against 13.65 ms per 40 x 2^14 prove)
   } tune;

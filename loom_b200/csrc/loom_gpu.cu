@@ -86,6 +86,7 @@ int lg_ctx_create(int device, size_t hbm_budget, lg_ctx** out) {
     LG_CK(cudaStreamCreateWithFlags(&ctx->c.side, cudaStreamNonBlocking));
     LG_CK(cudaEventCreateWithFlags(&ctx->c.fork_ev, cudaEventDisableTiming));
     LG_CK(cudaEventCreateWithFlags(&ctx->c.join_ev, cudaEventDisableTiming));
+    LG_CK(cudaEventCreateWithFlags(&ctx->c.upload_ev, cudaEventDisableTiming));
     cudaMemPool_t pool;
     LG_CK(cudaDeviceGetDefaultMemPool(&pool, device));
     uint64_t keep = UINT64_MAX;  // keep freed blocks for the next prove
@@ -126,6 +127,7 @@ void lg_ctx_destroy(lg_ctx* ctx) {
   }
   if (ctx->c.fork_ev) cudaEventDestroy(ctx->c.fork_ev);
   if (ctx->c.join_ev) cudaEventDestroy(ctx->c.join_ev);
+  if (ctx->c.upload_ev) cudaEventDestroy(ctx->c.upload_ev);
   if (ctx->c.pinned) cudaFreeHost(ctx->c.pinned);
   delete ctx;
 }
@@ -209,6 +211,7 @@ int lg_ctx_set_tuning(lg_ctx* ctx, const char* name, int64_t value) {
       in(0, 1);
       t.quotient_jit = (uint32_t)value;
     }
+    else if (n == "upload_split") { in(0, 1); t.upload_split = (uint32_t)value; }
     else throw Error(LG_ERR_INVALID, "unknown tuning " + n);
   });
 }
@@ -229,6 +232,7 @@ int lg_ctx_get_tuning(lg_ctx* ctx, const char* name, int64_t* value) {
     else if (n == "lde_fwd_threads") *value = t.lde_fwd_threads;
     else if (n == "fri_tail_leaves") *value = t.fri_tail_leaves;
     else if (n == "quotient_jit") *value = t.quotient_jit;
+    else if (n == "upload_split") *value = t.upload_split;
     else throw Error(LG_ERR_INVALID, "unknown tuning " + n);
   });
 }

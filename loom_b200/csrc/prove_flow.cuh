@@ -188,8 +188,8 @@ struct Sizer {
   void str(const std::string& s) { off += 4 + s.size(); }
 };
 
-inline void Prover::begin(const uint32_t* const* witness, bool on_device) {
-  setup(witness, on_device);
+inline void Prover::begin(const uint32_t* const* witness, bool on_device, bool split_upload) {
+  setup(witness, on_device, split_upload);
   coins.assign(pg.n_rounds, e6_zero());
   coin_ready.assign(pg.n_rounds, 0);
   fs_slots = std::make_shared<DBuf>(8 * ((size_t)pg.n_rounds + 2), c.stream);
@@ -249,6 +249,11 @@ inline void Prover::set_challenge(const std::string& name, const uint32_t* d) {
 inline bool Prover::commit_round(uint32_t r, Digest* root) {
   if (r >= pg.n_rounds) throw Error(LG_ERR_INVALID, "round out of range");
   need_coins(r);
+  // a split upload's late columns: round 0's commitment does not read them,
+  // everything after it (round 0's own steps included) may
+  bool steps_now = false;
+  for (const Step& st : pg.steps) steps_now = steps_now || st.round == r;
+  if (r > 0 || steps_now) await_upload();
   run_steps(r);
   bool has = false;
   if (tree_next < trees.size() && !trees[tree_next].air && trees[tree_next].round == (int)r) {
@@ -278,6 +283,7 @@ inline std::vector<E6> Prover::round_exposed(uint32_t r) const {
 // ---- AIR quotients and their commitment (prover/prover.go:461-561)
 inline bool Prover::commit_quotient(Digest* root) {
   need_coins(pg.n_rounds);
+  await_upload();
   if (tree_next < trees.size() && !trees[tree_next].air)
     throw Error(LG_ERR_INVALID, "the rounds are not all committed yet");
   quotient_all();
@@ -957,7 +963,7 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
                             bool* in_out) {
   ArenaScope arena(&c.dev_arena);  // rewound by the next call on the context
   c.phase_start();
-  begin(witness, on_device);
+  begin(witness, on_device, true);
   c.phase("setup+upload");
   const uint32_t R = pg.n_rounds;
   for (uint32_t r = 0; r < R; r++) fs.add(coin_name(r));

@@ -65,6 +65,7 @@ struct Prover {
   // column data on the device: lane pointer = buf + w * n
   std::map<uint32_t, DBufP> col_buf;
   DBufP witness_dev;  // host witness columns, uploaded into one buffer
+  bool upload_pending = false;  // late columns of a split upload still on the side stream (await_upload)
   std::map<uint32_t, const uint32_t*> col_coef;  // committed columns: coefficient lane 0
 
   struct Group { uint32_t module; std::vector<uint32_t> bcols, ecols; };
@@ -140,6 +141,7 @@ struct Prover {
   // run on the main stream, after that work.
   ~Prover() {
     if (den_pending) cudaStreamWaitEvent(c.stream, c.join_ev, 0);
+    if (upload_pending) cudaStreamWaitEvent(c.stream, c.upload_ev, 0);
   }
   Prover(const Prover&) = delete;
   Prover& operator=(const Prover&) = delete;
@@ -394,22 +396,21 @@ struct Prover {
     prog->setup = sd;
   }
 
-  void setup(const uint32_t* const* witness, bool on_device) {
+  // Host witness: one device buffer for all columns, in column order.  With
+  // `split` (lg_prove, tuning upload_split), the columns round 0 commits go
+  // up first on the main stream and the others on the side stream right
+  // after them, while round 0 runs (await_upload joins them); otherwise
+  // every column goes up on the main stream.  Copies of columns that follow
+  // one another in host and device memory merge.
+  void setup(const uint32_t* const* witness, bool on_device, bool split = false) {
     init_order();
-    // Host witness: one device buffer for all columns; columns that follow
-    // one another in host memory go up in a single copy.
     size_t total_words = 0;
     for (const Column& cl : pg.columns)
       if (cl.kind == KIND_WITNESS) total_words += mod_n(cl.module);
     if (!on_device && total_words) witness_dev = std::make_shared<DBuf>(total_words, c.stream);
+    upload_pending = false;
+    std::vector<const uint32_t*> src(pg.columns.size(), nullptr);
     size_t wi = 0, woff = 0;
-    const uint32_t* run_src = nullptr;
-    uint32_t* run_dst = nullptr;
-    size_t run_words = 0;
-    auto flush = [&]() {
-      if (run_words) LG_CK(cudaMemcpyAsync(run_dst, run_src, run_words * 4, cudaMemcpyHostToDevice, c.stream));
-      run_words = 0;
-    };
     for (uint32_t col = 0; col < pg.columns.size(); col++) {
       const Column& cl = pg.columns[col];
       size_t n = mod_n(cl.module);
@@ -418,14 +419,12 @@ struct Prover {
         auto b = std::make_shared<DBuf>();
         b->words = n;
         b->borrowed = true;
-        const uint32_t* src = witness[wi++];
+        src[col] = witness[wi++];
         if (on_device) {
           // read-only input: use the caller's device buffer as it is
-          b->p = const_cast<uint32_t*>(src);
+          b->p = const_cast<uint32_t*>(src[col]);
         } else {
           b->p = witness_dev->p + woff;
-          if (run_words && src == run_src + run_words) run_words += n;
-          else { flush(); run_src = src; run_dst = b->p; run_words = n; }
           woff += n;
         }
         col_buf[col] = b;
@@ -448,8 +447,53 @@ struct Prover {
         col_coef[col] = prog->setup->coef.at(col);
       }
     }
-    flush();
+    if (!on_device && total_words) {
+      // early: the witness columns round 0 commits (all of them unless split)
+      std::vector<char> early(pg.columns.size(), 1);
+      bool any_late = false;
+      if (split && c.tune.upload_split && c.side && c.upload_ev && !pg.staged.empty()) {
+        std::fill(early.begin(), early.end(), 0);
+        for (uint32_t col : pg.staged[0]) early.at(col) = 1;
+        for (uint32_t col = 0; col < pg.columns.size(); col++)
+          any_late = any_late || (pg.columns[col].kind == KIND_WITNESS && !early[col]);
+        if (!any_late) std::fill(early.begin(), early.end(), 1);
+      }
+      auto copy = [&](bool want, cudaStream_t s) {
+        const uint32_t* run_src = nullptr;
+        uint32_t* run_dst = nullptr;
+        size_t run_words = 0;
+        auto flush = [&]() {
+          if (run_words) LG_CK(cudaMemcpyAsync(run_dst, run_src, run_words * 4, cudaMemcpyHostToDevice, s));
+          run_words = 0;
+        };
+        for (uint32_t col = 0; col < pg.columns.size(); col++) {
+          if (pg.columns[col].kind != KIND_WITNESS || (early[col] != 0) != want) continue;
+          const size_t n = mod_n(pg.columns[col].module);
+          uint32_t* dst = col_buf[col]->p;
+          if (run_words && src[col] == run_src + run_words && dst == run_dst + run_words) run_words += n;
+          else { flush(); run_src = src[col]; run_dst = dst; run_words = n; }
+        }
+        flush();
+      };
+      copy(true, c.stream);
+      if (any_late) {
+        // after the early copies (no contention for the link), on the side
+        // stream; the main stream waits for upload_ev before round 1
+        LG_CK(cudaEventRecord(c.fork_ev, c.stream));
+        LG_CK(cudaStreamWaitEvent(c.side, c.fork_ev, 0));
+        copy(false, c.side);
+        LG_CK(cudaEventRecord(c.upload_ev, c.side));
+        upload_pending = true;
+      }
+    }
     setup_layout();
+  }
+
+  // The main stream waits for the late columns of a split upload.
+  void await_upload() {
+    if (!upload_pending) return;
+    LG_CK(cudaStreamWaitEvent(c.stream, c.upload_ev, 0));
+    upload_pending = false;
   }
 
   // Module order is set; folded relations, degrees, shift schedule and the
@@ -1309,7 +1353,7 @@ struct Prover {
   // phases before it; the caller keeps the transcript (lg_prove: the host
   // Transcript below; the session entry points: the caller of the C ABI)
   // and hands the challenges in with set_challenge.
-  void begin(const uint32_t* const* witness, bool on_device);
+  void begin(const uint32_t* const* witness, bool on_device, bool split_upload = false);
   bool has_setup_tree() const { return !trees.empty() && trees[0].setup; }
   // ExecuteSteps + commitTraceRound of round r (prover/prover.go:321-411):
   // true with the root when the round commits a tree.

@@ -351,7 +351,7 @@ def test_tuning_never_changes_proofs(ctx):
     try:
         for params in ({"merkle_tail": 2, "merkle_subtree": 2, "p2_leaf_min_per_sm": 0, "p2_node_min_per_sm": 0,
                         "p2_inject_min_per_sm": 0, "inject_block": 1024, "leaf_block": 32, "lde_split": 0,
-                        "lde_fwd_threads": 256, "fri_tail_leaves": 0, "quotient_jit": 0},
+                        "lde_fwd_threads": 256, "fri_tail_leaves": 0, "quotient_jit": 0, "upload_split": 0},
                        {"merkle_tail": 1024, "merkle_subtree": 1024, "p2_leaf_min_per_sm": 1 << 20,
                         "p2_node_min_per_sm": 1 << 20, "p2_inject_min_per_sm": 1 << 20, "inject_block": 32,
                         "leaf_block": 1024, "lde_split": 1, "lde_fwd_threads": 1024, "fri_tail_leaves": 65536},
@@ -366,7 +366,7 @@ def test_tuning_never_changes_proofs(ctx):
     finally:
         ctx.apply_tuning(defaults)
     for name, value in (("merkle_tail", 48), ("merkle_tail", 2048), ("merkle_subtree", 1), ("merkle_subtree", 48),
-                        ("leaf_block", 16), ("lde_split", 2), ("lde_fwd_threads", 128), ("fri_tail_leaves", 3), ("quotient_jit", 2),
+                        ("leaf_block", 16), ("lde_split", 2), ("lde_fwd_threads", 128), ("fri_tail_leaves", 3), ("quotient_jit", 2), ("upload_split", 2),
                         ("no_such", 1)):
         with pytest.raises(LoomError) as e:
             ctx.set_tuning(name, value)
@@ -450,6 +450,39 @@ def test_compiled_constraint_kernels_give_identical_proofs(ctx, build):
         ctx.set_tuning("quotient_jit", saved)
     assert jit == interp == oracle.prove(compiled.words, mont, 16)
     assert L.lg_jit_kernels() >= 1
+
+
+@pytest.mark.parametrize("build", ["plonk", "mixed_lookup"])
+def test_split_witness_upload_gives_identical_proofs(ctx, build):
+    """A host witness's columns that round 0 does not commit go up on a second
+    stream while round 0 runs (tuning upload_split = 1, the default; a first
+    round with witness steps waits for all of them): the proof of a
+    device-resident witness with the split and without, from pageable arrays
+    and from one page-locked buffer whose columns are adjacent."""
+    import torch
+    if build == "plonk":
+        compiled, wit = plonk.build(5, 1 << 9, seed=41)
+    else:
+        compiled, wit = plonk.build_mixed([7, 5, 9, 5, 8], seed=13)
+    mont = [np.ascontiguousarray(F.to_mont(w), dtype=np.uint32) for w in wit]
+    dev = [torch.from_numpy(m.astype(np.int64)).to(torch.int32).cuda() for m in mont]
+    ref = ctx.prove(compiled.words, [t.data_ptr() for t in dev], 16, on_device=True)
+    pinned = torch.empty(sum(m.size for m in mont), dtype=torch.int32).pin_memory()
+    flat = pinned.numpy().view(np.uint32)
+    views, off = [], 0
+    for m in mont:
+        flat[off:off + m.size] = m
+        views.append(flat[off:off + m.size])
+        off += m.size
+    saved = ctx.get_tuning("upload_split")
+    try:
+        for split in (1, 0):
+            ctx.set_tuning("upload_split", split)
+            assert ctx.prove(compiled.words, mont, 16) == ref
+            assert ctx.prove(compiled.words, views, 16) == ref
+    finally:
+        ctx.set_tuning("upload_split", saved)
+    assert ref == oracle.prove(compiled.words, mont, 16)
 
 
 def test_lde_launch_shapes_give_identical_results(ctx):
