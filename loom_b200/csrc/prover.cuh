@@ -30,6 +30,11 @@ struct CodeSet {
   std::vector<XProgram> dev;   // device copies, in xc order
   std::vector<uint32_t> cols;  // columns in first-use order
   DBufP code;                  // every xc back to back (kept across proves)
+  // The kernel compiled from xc at run time (xjit.cuh: the quotient's program,
+  // or a grand product's numerator and denominator), looked up once: later
+  // proves skip generating its source to find it in the compile cache.
+  mutable bool jit_done = false;
+  mutable CUfunction jit = nullptr;
 };
 // A program's precommitted setup tree (lg_setup; setup/setup.go:68-124): the
 // committed LDE and tree, the setup columns' values and coefficients, and the
@@ -167,6 +172,15 @@ struct Prover {
 
   // The bytecode of `roots` compiled in order against one lane table
   // (lane_of), from the program's cache when this site was compiled before.
+  // The run-time compiled kernel of a cached code set (null: the interpreter
+  // runs it), found once per code set.
+  static CUfunction jit_of(const CodeSet& cs, bool grand_product) {
+    if (!cs.jit_done) {
+      cs.jit = grand_product ? xjit_gp(cs.xc.at(0), cs.xc.at(1)) : xjit_quotient(cs.xc.at(0));
+      cs.jit_done = true;
+    }
+    return cs.jit;
+  }
   template <class LaneOf> const CodeSet& compiled(const std::string& site, LaneOf& lane_of, const std::vector<uint32_t>& roots) {
     auto it = prog->sites.find(site);
     if (it != prog->sites.end()) {
@@ -949,7 +963,7 @@ struct Prover {
     std::vector<const uint32_t*> all_lanes;  // every step's lane table, one upload
     std::vector<size_t> lane_off;
     uint32_t max_regs = 1;
-    std::vector<std::pair<const XCode*, const XCode*>> codes;  // per job: numerator, denominator bytecode
+    std::vector<const CodeSet*> codes;  // per job: numerator and denominator bytecode
     for (const Step* st : steps) {
       uint32_t logn = pg.modules[st->module].log_n;
       size_t n = (size_t)1 << logn;
@@ -974,7 +988,7 @@ struct Prover {
       auto res = std::make_shared<DBuf>(6 * n, c.stream);
       keep.insert(keep.end(), {ratio, totals, pre});
       jobs.push_back(GpJob{cs.dev[0], cs.dev[1], nullptr, ratio->p, (int)logn});
-      codes.push_back({&cs.xc[0], &cs.xc[1]});
+      codes.push_back(&cs);
       ScanJob sj{ratio->p, n, totals->p, pre->p, res->p, nt};
       if (st->type == STEP_RATIO) {  // inclusive products; the end is exposed
         if (pg.columns[st->out].field != 1 || pg.columns[st->out].module != st->module)
@@ -1004,7 +1018,7 @@ struct Prover {
       uint32_t max_ni = 0;
       for (size_t i = first; i < first + count; i++) {
         const uint32_t ni = (uint32_t)scans[i].n;
-        if (CUfunction f = c.tune.quotient_jit ? xjit_gp(*codes[i].first, *codes[i].second) : nullptr) {
+        if (CUfunction f = c.tune.quotient_jit ? jit_of(*codes[i], true) : nullptr) {
           auto& g = jit[f];
           g.first.push_back(GpxJob{jobs[i].lanes, jobs[i].ratio, jobs[i].logn});
           g.second = std::max(g.second, ni);
@@ -1088,7 +1102,7 @@ struct Prover {
       std::vector<const uint32_t*> coef_lanes;
       std::vector<CosetLane> lanes;
       DBufP cv, qv, chunks;
-      XCode xc;
+      const CodeSet* cs;
       XProgram prog;
       uint32_t zinv[4];
     };
@@ -1151,7 +1165,7 @@ struct Prover {
         return f;
       };
       const CodeSet& cs = compiled("q" + std::to_string(m), lane_of, {(uint32_t)fold_root[m]});
-      q.xc = cs.xc[0];
+      q.cs = &cs;
       q.prog = cs.dev[0];
       q.coef_lanes = coef_lanes;
       uint32_t g = to_mont(3), w4n = root_of_unity_mont((int)logn + RATE_LOG);
@@ -1261,7 +1275,7 @@ struct Prover {
       for (ModQ* q : ms) {
         qbytes += (4.0 * q->lanes.size() + 24.0) * (4.0 * (1u << q->logn));
         max_n = std::max(max_n, 1u << q->logn);  // the chunk step below covers every module
-        if (CUfunction f = c.tune.quotient_jit ? xjit_quotient(q->xc) : nullptr) {
+        if (CUfunction f = c.tune.quotient_jit ? jit_of(*q->cs, false) : nullptr) {
           QxJob x{q->cv->p, q->qv->p, (int)q->logn, {q->zinv[0], q->zinv[1], q->zinv[2], q->zinv[3]}};
           auto& g = jit[f];
           g.first.push_back(x);
@@ -1275,7 +1289,7 @@ struct Prover {
         j.logn = (int)q->logn;
         for (int k = 0; k < 4; k++) j.zinv[k] = q->zinv[k];
         qj.push_back(j);
-        max_regs = std::max(max_regs, q->xc.n_regs);
+        max_regs = std::max(max_regs, q->cs->xc[0].n_regs);
       }
       std::vector<std::pair<CUfunction, DBufP>> jit_d;
       for (auto& kv : jit) jit_d.push_back({kv.first, upload_vec(c, kv.second.first)});
