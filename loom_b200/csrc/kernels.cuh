@@ -204,6 +204,22 @@ __global__ void k_lde(const LdeLane* lanes, int logn_rt, int from_coeffs, const 
 // and shared-memory round trips.  MAXT: the block size the kernel is built
 // for (registers capped so that 1024 / MAXT blocks fit: 32 warps per SM
 // without spills).
+// The coset shifts of the first DIF pass: its element i = r 2^(logn-4) + t
+// (t < 2^(logn-4)) takes w_4n^(e i) = w_4n^(e t) w_64^(e r), since
+// w_4n^(2^(logn-4)) = w_64 for every size; w_64^(e r) for e < 4, r < 16 as
+// canonical words with their Shoup companions.
+struct CosetSteps { uint32_t w[4][16], ws[4][16]; };
+constexpr CosetSteps make_coset_steps() {
+  CosetSteps c{};
+  for (uint32_t e = 0; e < 4; e++)
+    for (uint32_t r = 0; r < 16; r++) {
+      c.w[e][r] = cx_pow(3, (uint64_t)((P - 1) / 64) * ((e * r) % 64));
+      c.ws[e][r] = shoup(c.w[e][r]);
+    }
+  return c;
+}
+__constant__ CosetSteps COSET_STEPS_D = make_coset_steps();
+
 template <int LOGN, int MAXT>
 __global__ void __launch_bounds__(MAXT, 1024 / MAXT)
     k_lde_fwd(const LdeLane* lanes, uint32_t lane0, int first, const uint32_t* tw_n, const uint32_t* tw_4n) {
@@ -220,9 +236,14 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT)
   for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) cp_async4(&sm[pad16(k)], coef + k);
   cp_async_wait_all();
   __syncthreads();
+  // one table load per group for w_4n^(e t); the 15 other shifts of the group
+  // are Shoup products by constants (r is a compile-time index after unrolling)
+  uint32_t shift_t = 0;
   auto first_pass = [&](uint32_t t, uint32_t r, int lo) {
     const uint32_t i = grp_index(t, r, lo);
-    return mul(sm[pad16(i)], __ldg(tw_4n + ((e * i) & (big - 1))));
+    if (r == 0) shift_t = __ldg(tw_4n + ((e * t) & (big - 1)));
+    const uint32_t x = mul(sm[pad16(i)], shift_t);
+    return r ? mulc(x, COSET_STEPS_D.w[e][r], COSET_STEPS_D.ws[e][r]) : x;
   };
   auto store = [&](uint32_t t, int lo, const uint32_t* v) {
     uint4* q = reinterpret_cast<uint4*>(o + ((uint64_t)t << 4));
