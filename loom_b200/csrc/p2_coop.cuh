@@ -76,7 +76,7 @@ __device__ __forceinline__ void p2c_permute(uint32_t x[4], const P2Lane& L, cons
     const uint32_t D = L.allreduce(add(add(L.idx ? p[0] : 0u, p[1]), add(p[2], p[3])));
     const uint32_t u = p2_cube(add(s0, P2_PARTIAL_RK_D[r]));
     const uint32_t sum = add(u, R);
-    s0 = add(sum, mulc(u, P2_DSH_D.w[0], P2_DSH_D.ws[0]));
+    s0 = sub(R, u);  // sum + d_0 u with d_0 = -2
     x[0] = L.idx ? add(sum, p[0]) : s0;
 #pragma unroll
     for (int i = 1; i < 4; i++) x[i] = sum + p[i];  // unreduced in [0, 2p) until the next product

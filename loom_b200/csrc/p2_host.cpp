@@ -82,20 +82,23 @@ LG_AVX2 void p2_permute_avx2(uint32_t s[24]) {
   vexternal(v);
   for (int r = 0; r < 3; r++) vfull_round(v, P2_FULL_RK_H[r]);
   // partial rounds, carried R = s_1 + ... + s_23 (as p2_partial_rounds)
+  // s_0 stays a scalar through the rounds (lane 0 of v[0] is not read until
+  // the end); with d_0 = -2 its update sum + d_0 u is R - u, no product
   uint32_t R = vhsum(vadd(_mm256_blend_epi32(v[0], zero, 0x01), vadd(v[1], v[2])));
+  uint32_t s0 = (uint32_t)_mm256_cvtsi256_si32(v[0]);
   for (int r = 0; r < 21; r++) {
-    const uint32_t s0 = (uint32_t)_mm256_cvtsi256_si32(v[0]);
     const uint32_t u = p2_cube(add(s0, P2_PARTIAL_RK_H[r]));
     const __m256i p0 = vmul(v[0], dg[0]), p1 = vmul(v[1], dg[1]), p2 = vmul(v[2], dg[2]);
     const uint32_t D = vhsum(vadd(_mm256_blend_epi32(p0, zero, 0x01), vadd(p1, p2)));
     const uint32_t sum = add(u, R);
     const __m256i sv = _mm256_set1_epi32((int)sum);
-    const uint32_t s0n = add(sum, mul(u, P2_DIAG_H[0]));
-    v[0] = _mm256_blend_epi32(_mm256_add_epi32(sv, p0), _mm256_set1_epi32((int)s0n), 0x01);
-    v[1] = _mm256_add_epi32(sv, p1);  // unreduced in [0, 2p) until the next product
+    s0 = sub(R, u);
+    v[0] = _mm256_add_epi32(sv, p0);  // unreduced in [0, 2p) until the next product
+    v[1] = _mm256_add_epi32(sv, p1);
     v[2] = _mm256_add_epi32(sv, p2);
     R = add(mul(sum, MONT_23), D);
   }
+  v[0] = _mm256_blend_epi32(v[0], _mm256_set1_epi32((int)s0), 0x01);
   for (int k = 0; k < 3; k++) v[k] = vred(v[k]);
   for (int r = 3; r < 6; r++) vfull_round(v, P2_FULL_RK_H[r]);
   for (int k = 0; k < 3; k++) _mm256_storeu_si256(reinterpret_cast<__m256i*>(s + 8 * k), v[k]);
@@ -158,21 +161,22 @@ LG_AVX512 void p2_permute_avx512(uint32_t s[24]) {
   zexternal(a, b);
   for (int r = 0; r < 3; r++) zfull_round(a, b, P2_FULL_RK_H[r]);
   // partial rounds, carried R = s_1 + ... + s_23 (as p2_partial_rounds)
+  // s_0 as a scalar through the rounds, updated as R - u (d_0 = -2)
   uint32_t R = zsum_tail(a, b);
+  uint32_t s0 = (uint32_t)_mm_cvtsi128_si32(_mm512_castsi512_si128(a));
   for (int r = 0; r < 21; r++) {
-    const uint32_t s0 = (uint32_t)_mm_cvtsi128_si32(_mm512_castsi512_si128(a));
     const uint32_t u = p2_cube(add(s0, P2_PARTIAL_RK_H[r]));
     const __m512i pa = zmul(a, da);
     const __m256i pb = vmul(b, db);
     const uint32_t D = zsum_tail(pa, pb);
     const uint32_t sum = add(u, R);
     const __m512i sv = _mm512_set1_epi32((int)sum);
-    const uint32_t s0n = add(sum, mul(u, P2_DIAG_H[0]));
-    a = _mm512_mask_blend_epi32((__mmask16)0x0001, _mm512_add_epi32(sv, pa), _mm512_set1_epi32((int)s0n));
-    b = _mm256_add_epi32(_mm512_castsi512_si256(sv), pb);  // unreduced in [0, 2p) until the next product
+    s0 = sub(R, u);
+    a = _mm512_add_epi32(sv, pa);  // unreduced in [0, 2p) until the next product
+    b = _mm256_add_epi32(_mm512_castsi512_si256(sv), pb);
     R = add(mul(sum, MONT_23), D);
   }
-  a = zred(a);
+  a = _mm512_mask_blend_epi32((__mmask16)0x0001, zred(a), _mm512_set1_epi32((int)s0));
   b = vred(b);
   for (int r = 3; r < 6; r++) zfull_round(a, b, P2_FULL_RK_H[r]);
   _mm512_storeu_si512(s, a);

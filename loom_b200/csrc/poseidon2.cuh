@@ -127,6 +127,7 @@ constexpr P2DiagShoup make_p2_diag_shoup() {
 }
 constexpr P2DiagShoup P2_DSH_H = make_p2_diag_shoup();
 static_assert(P2_DSH_H.w[1] == 1, "internal diagonal entry 1 is 1");
+static_assert(P2_DSH_H.w[0] == P - 2, "internal diagonal entry 0 is -2: s_0 <- sum + d_0 u = R - u");
 #ifdef __CUDACC__
 __constant__ P2DiagShoup P2_DSH_D = make_p2_diag_shoup();
 #endif
@@ -222,7 +223,7 @@ LG_HD void p2_partial_rounds(uint32_t s[24]) {
     p2_diag_products(s, p);
     const uint32_t D = wide_sum<23>(p + 1);
     const uint32_t sum = add(u, R);
-    s[0] = add(sum, mulc(u, LG_P2_DSH.w[0], LG_P2_DSH.ws[0]));
+    s[0] = sub(R, u);  // sum + d_0 u with d_0 = -2
 #pragma unroll
     for (int i = 1; i < 24; i++) s[i] = sum + p[i];
     R = add(mulc(sum, C23, C23_SH), D);
