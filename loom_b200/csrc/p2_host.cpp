@@ -17,6 +17,30 @@
 namespace lg {
 namespace {
 
+// The scalar S-box chain of the partial rounds, shortened for the host: the
+// cube of a Montgomery word x (x^3 R after the reduction) as one 93-bit
+// product reduced once by Montgomery's method with 2^64 (x^3 R^3 2^-64 =
+// x^3 R for R = 2^32) instead of two reductions by 2^32; and the additions
+// on the chain as the minimum of two independent sums.
+constexpr uint64_t neg_inv64() {  // -p^-1 mod 2^64 (Newton's iteration)
+  uint64_t v = 1;
+  for (int i = 0; i < 7; i++) v *= 2 - (uint64_t)P * v;
+  return 0 - v;
+}
+constexpr uint64_t P_INV_NEG64 = neg_inv64();
+static_assert((uint64_t)P * P_INV_NEG64 == ~(uint64_t)0, "-p^-1 mod 2^64");
+inline uint32_t cube_host(uint32_t x) {
+  const uint64_t x2 = (uint64_t)x * x;                               // < 2^62
+  const unsigned __int128 t = (unsigned __int128)x2 * x;            // < 2^93 < p 2^64
+  const uint64_t m = (uint64_t)t * P_INV_NEG64;
+  const uint32_t r = (uint32_t)((t + (unsigned __int128)m * P) >> 64);  // < 2p
+  return umin(r, r - P);
+}
+// a + k and a - b for reduced words, each a minimum of two sums that do not
+// wait for each other (k - p and b: prepared off the chain)
+inline uint32_t add_pre(uint32_t a, uint32_t k, uint32_t k_minus_p) { return umin(a + k, a + k_minus_p); }
+inline uint32_t sub_pre(uint32_t a_plus_p, uint32_t a, uint32_t b) { return umin(a - b, a_plus_p - b); }
+
 LG_AVX2 inline __m256i vp() { return _mm256_set1_epi32((int)P); }
 
 // a + b mod p for a, b in [0, p)
@@ -87,12 +111,13 @@ LG_AVX2 void p2_permute_avx2(uint32_t s[24]) {
   uint32_t R = vhsum(vadd(_mm256_blend_epi32(v[0], zero, 0x01), vadd(v[1], v[2])));
   uint32_t s0 = (uint32_t)_mm256_cvtsi256_si32(v[0]);
   for (int r = 0; r < 21; r++) {
-    const uint32_t u = p2_cube(add(s0, P2_PARTIAL_RK_H[r]));
+    const uint32_t k = P2_PARTIAL_RK_H[r];
+    const uint32_t u = cube_host(add_pre(s0, k, k - P));
     const __m256i p0 = vmul(v[0], dg[0]), p1 = vmul(v[1], dg[1]), p2 = vmul(v[2], dg[2]);
     const uint32_t D = vhsum(vadd(_mm256_blend_epi32(p0, zero, 0x01), vadd(p1, p2)));
     const uint32_t sum = add(u, R);
     const __m256i sv = _mm256_set1_epi32((int)sum);
-    s0 = sub(R, u);
+    s0 = sub_pre(R + P, R, u);
     v[0] = _mm256_add_epi32(sv, p0);  // unreduced in [0, 2p) until the next product
     v[1] = _mm256_add_epi32(sv, p1);
     v[2] = _mm256_add_epi32(sv, p2);
@@ -165,13 +190,14 @@ LG_AVX512 void p2_permute_avx512(uint32_t s[24]) {
   uint32_t R = zsum_tail(a, b);
   uint32_t s0 = (uint32_t)_mm_cvtsi128_si32(_mm512_castsi512_si128(a));
   for (int r = 0; r < 21; r++) {
-    const uint32_t u = p2_cube(add(s0, P2_PARTIAL_RK_H[r]));
+    const uint32_t k = P2_PARTIAL_RK_H[r];
+    const uint32_t u = cube_host(add_pre(s0, k, k - P));
     const __m512i pa = zmul(a, da);
     const __m256i pb = vmul(b, db);
     const uint32_t D = zsum_tail(pa, pb);
     const uint32_t sum = add(u, R);
     const __m512i sv = _mm512_set1_epi32((int)sum);
-    s0 = sub(R, u);
+    s0 = sub_pre(R + P, R, u);
     a = _mm512_add_epi32(sv, pa);  // unreduced in [0, 2p) until the next product
     b = _mm256_add_epi32(_mm512_castsi512_si256(sv), pb);
     R = add(mul(sum, MONT_23), D);
