@@ -61,8 +61,23 @@ LG_AVX2 inline __m256i vmul(__m256i a, __m256i b) {
   const __m256i uo = _mm256_add_epi64(to, _mm256_mul_epu32(mo, p));
   return vred(_mm256_blend_epi32(_mm256_srli_epi64(ue, 32), uo, 0xAA));
 }
+// the same without the final reduction: [0, 2p), a valid first operand of vmul
+LG_AVX2 inline __m256i vmul_lazy(__m256i a, __m256i b) {
+  const __m256i p = vp(), pinv = _mm256_set1_epi32((int)P_INV_NEG);
+  const __m256i te = _mm256_mul_epu32(a, b);
+  const __m256i to = _mm256_mul_epu32(_mm256_srli_epi64(a, 32), _mm256_srli_epi64(b, 32));
+  const __m256i me = _mm256_mul_epu32(te, pinv), mo = _mm256_mul_epu32(to, pinv);
+  const __m256i ue = _mm256_add_epi64(te, _mm256_mul_epu32(me, p));
+  const __m256i uo = _mm256_add_epi64(to, _mm256_mul_epu32(mo, p));
+  return _mm256_blend_epi32(_mm256_srli_epi64(ue, 32), uo, 0xAA);
+}
 
-LG_AVX2 inline __m256i vcube(__m256i x) { return vmul(vmul(x, x), x); }
+LG_AVX2 inline __m256i vcube(__m256i x) { return vmul(vmul_lazy(x, x), x); }
+// x + k for a constant vector k, as the minimum of two sums that do not wait
+// for each other
+LG_AVX2 inline __m256i vadd_k(__m256i x, __m256i k) {
+  return _mm256_min_epu32(_mm256_add_epi32(x, k), _mm256_add_epi32(x, _mm256_sub_epi32(k, vp())));
+}
 
 // M4 on the two 4-word blocks of v: y_i = x_i + 2 x_{i+1} + (x_0 + x_1 + x_2 + x_3),
 // indices mod 4 -- the matrix of p2_m4's addition chain.
@@ -91,7 +106,7 @@ LG_AVX2 inline uint32_t vhsum(__m256i x) {
 
 LG_AVX2 inline void vfull_round(__m256i v[3], const uint32_t* rk) {
   for (int k = 0; k < 3; k++)
-    v[k] = vcube(vadd(v[k], _mm256_loadu_si256(reinterpret_cast<const __m256i*>(rk + 8 * k))));
+    v[k] = vcube(vadd_k(v[k], _mm256_loadu_si256(reinterpret_cast<const __m256i*>(rk + 8 * k))));
   vexternal(v);
 }
 
@@ -148,7 +163,19 @@ LG_AVX512 inline __m512i zmul(__m512i a, __m512i b) {
   const __m512i uo = _mm512_add_epi64(to, _mm512_mul_epu32(mo, p));
   return zred(_mm512_mask_blend_epi32((__mmask16)0xAAAA, _mm512_srli_epi64(ue, 32), uo));
 }
-LG_AVX512 inline __m512i zcube(__m512i x) { return zmul(zmul(x, x), x); }
+LG_AVX512 inline __m512i zmul_lazy(__m512i a, __m512i b) {  // [0, 2p)
+  const __m512i p = zp(), pinv = _mm512_set1_epi32((int)P_INV_NEG);
+  const __m512i te = _mm512_mul_epu32(a, b);
+  const __m512i to = _mm512_mul_epu32(_mm512_srli_epi64(a, 32), _mm512_srli_epi64(b, 32));
+  const __m512i me = _mm512_mul_epu32(te, pinv), mo = _mm512_mul_epu32(to, pinv);
+  const __m512i ue = _mm512_add_epi64(te, _mm512_mul_epu32(me, p));
+  const __m512i uo = _mm512_add_epi64(to, _mm512_mul_epu32(mo, p));
+  return _mm512_mask_blend_epi32((__mmask16)0xAAAA, _mm512_srli_epi64(ue, 32), uo);
+}
+LG_AVX512 inline __m512i zcube(__m512i x) { return zmul(zmul_lazy(x, x), x); }
+LG_AVX512 inline __m512i zadd_k(__m512i x, __m512i k) {  // as vadd_k
+  return _mm512_min_epu32(_mm512_add_epi32(x, k), _mm512_add_epi32(x, _mm512_sub_epi32(k, zp())));
+}
 LG_AVX512 inline __m512i zm4(__m512i v) {  // p2_m4 on each 128-bit lane, as vm4
   const __m512i r = _mm512_shuffle_epi32(v, (_MM_PERM_ENUM)_MM_SHUFFLE(0, 3, 2, 1));
   const __m512i e = zadd(v, zadd(r, r));
@@ -167,8 +194,8 @@ LG_AVX512 inline void zexternal(__m512i& a, __m256i& b) {
   b = vadd(b, _mm512_castsi512_si256(tot));
 }
 LG_AVX512 inline void zfull_round(__m512i& a, __m256i& b, const uint32_t* rk) {
-  a = zcube(zadd(a, _mm512_loadu_si512(rk)));
-  b = vcube(vadd(b, _mm256_loadu_si256(reinterpret_cast<const __m256i*>(rk + 16))));
+  a = zcube(zadd_k(a, _mm512_loadu_si512(rk)));
+  b = vcube(vadd_k(b, _mm256_loadu_si256(reinterpret_cast<const __m256i*>(rk + 16))));
   zexternal(a, b);
 }
 
