@@ -607,13 +607,18 @@ inline std::vector<uint32_t> string_to_elements(uint32_t tag, const std::string&
 struct Digest { uint32_t v[8]; };
 
 struct Transcript {
-  struct Ch { std::string name; std::vector<uint32_t> bindings; Digest value; bool done = false; };
+  // name_el: the name's field elements (string_to_elements), made once when
+  // the challenge is declared
+  struct Ch { std::string name; std::vector<uint32_t> name_el, bindings; Digest value; bool done = false; };
   std::vector<Ch> chs;
   std::map<std::string, size_t> index;
   void add(const std::string& n) {
     if (index.count(n)) throw Error(LG_ERR_INVALID, "duplicate challenge " + n);
     index[n] = chs.size();
-    Ch c; c.name = n; chs.push_back(c);
+    Ch c;
+    c.name = n;
+    c.name_el = string_to_elements(0x46534944u, n);
+    chs.push_back(std::move(c));
   }
   void bind(const std::string& n, const uint32_t* v, size_t len) {
     auto it = index.find(n);
@@ -630,7 +635,7 @@ struct Transcript {
     if (it == index.end()) throw Error(LG_ERR_INVALID, "unknown challenge " + n);
     const size_t i = it->second;
     Known k;
-    k.name = string_to_elements(0x46534944u, n);
+    k.name = chs[i].name_el;
     if (i) {
       k.has_prev = true;
       k.prev_done = chs[i - 1].done;
@@ -659,7 +664,7 @@ struct Transcript {
     Ch& ch = chs.at(i);
     if (ch.done) return ch.value;
     HostSponge h;
-    for (uint32_t x : string_to_elements(0x46534944u, ch.name)) h.write(x);
+    for (uint32_t x : ch.name_el) h.write(x);
     if (i) {
       if (!chs[i - 1].done) throw Error(LG_ERR_INVALID, "previous challenge not computed for " + ch.name);
       for (int k = 0; k < 8; k++) h.write(chs[i - 1].value.v[k]);
