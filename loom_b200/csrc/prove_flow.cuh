@@ -1063,8 +1063,13 @@ inline size_t Prover::prove(const uint32_t* const* witness, bool on_device, uint
   dev_fs = true;  // the FRI levels' challenges again come from the device
   c.phase("claimed values");
   fs.add("alpha_DEEP");
-  for (const E6& v : claimed_values_bind_order()) fs.bind("alpha_DEEP", v.c, 6);
-  set_challenge("alpha_DEEP", fs.compute("alpha_DEEP").v);
+  {
+    const std::vector<E6> vals = claimed_values_bind_order();
+    const size_t ia = fs.at("alpha_DEEP");
+    fs.chs[ia].bindings.reserve(6 * vals.size());
+    for (const E6& v : vals) fs.bind_at(ia, v.c, 6);
+    set_challenge("alpha_DEEP", fs.compute_at(ia).v);
+  }
   c.phase("alpha bind");
   deep_codewords();
   c.phase("deep");
